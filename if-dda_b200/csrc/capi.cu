@@ -1,0 +1,487 @@
+// C-ABI of libifdda_gpu.so (declarations and reference seams: include/ifdda_gpu.h).
+#include <cstring>
+#include <memory>
+#include <string>
+#include "../../include/ifdda_gpu.h"
+#include "post.cuh"
+
+using namespace ifdda;
+
+struct ifdda_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    DevBuf<int> flag;  // device error flag for post kernels
+    DevBuf<double2> partials;
+    DevBuf<unsigned> tickets;
+    DevBuf<KState> st;
+    DevBuf<int> zstatus;
+};
+
+struct ifdda_green {
+    ifdda_ctx* ctx = nullptr;
+    Green G;
+    SolverWork SW;
+    // per-call device copies
+    DevBuf<int> tab;
+    DevBuf<double2> alpha, ff0, x, ffx, ffb;
+    DevBuf<float2> ffx32, ffb32, alpha32;
+};
+
+static void set_info(char* infostr, const char* msg) {
+    if (!infostr) return;
+    const size_t L = std::min<size_t>(strlen(msg), 64);
+    memset(infostr, ' ', 64);
+    memcpy(infostr, msg, L);
+}
+
+#define IFDDA_GUARD_BEGIN try {
+#define IFDDA_GUARD_END(ctxp, info)                           \
+    }                                                         \
+    catch (const EngineError& e) {                            \
+        if (ctxp) (ctxp)->last_error = e.msg;                 \
+        set_info(info, e.msg.c_str());                        \
+        return 1;                                             \
+    }                                                         \
+    catch (const std::exception& e) {                         \
+        if (ctxp) (ctxp)->last_error = e.what();              \
+        set_info(info, e.what());                             \
+        return 1;                                             \
+    }
+
+namespace {
+struct DeviceScope {
+    int prev = -1;
+    explicit DeviceScope(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) IFDDA_CUDA(cudaSetDevice(dev));
+    }
+    ~DeviceScope() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// A polarisability is stored compactly when every dipole's tensor is the
+// same complex number times the identity (every object of the reference
+// built with trope = 'iso').
+int pola_mode(const ifdda_dcmplx* pol, int nb, long nmax) {
+    for (long i = 0; i < nb; i++) {
+        const ifdda_dcmplx d0 = pol[i];
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+                const ifdda_dcmplx v = pol[i + nmax * (a + 3 * b)];
+                if (a == b) {
+                    if (v.re != d0.re || v.im != d0.im) return ALPHA_FULL;
+                } else if (v.re != 0.0 || v.im != 0.0) {
+                    return ALPHA_FULL;
+                }
+            }
+    }
+    return ALPHA_ISO;
+}
+
+int method_code(const char* m) {
+    char buf[13];
+    memset(buf, ' ', 12);
+    buf[12] = 0;
+    if (m) memcpy(buf, m, std::min<size_t>(strnlen(m, 12), 12));
+    if (!strncmp(buf, "GPBICG1", 7)) return 1;
+    if (!strncmp(buf, "QMRBICGSTAB1", 12)) return 2;
+    if (!strncmp(buf, "QMRBICGSTAB2", 12)) return 3;
+    return 0;
+}
+
+SolveSpec make_spec(int method, int nrhs, int nb, double tol, const ifdda_solve_options* opt) {
+    SolveSpec sp;
+    sp.method = method;
+    sp.nrhs = nrhs;
+    sp.n3 = 3L * nb;
+    sp.tol = tol;
+    if (opt) {
+        if (opt->check_every > 0) sp.check_every = opt->check_every;
+        if (opt->max_outer > 0) sp.max_outer = opt->max_outer;
+        if (opt->inner_floor > 0) sp.inner_floor = opt->inner_floor;
+    }
+    return sp;
+}
+
+// Runs a (batched) solve whose inputs are already on the device.
+int solve_device(ifdda_green* g, int nrhs, int nb, int nmax, const int* tab_dev, const double2* alpha_dev, int amode,
+                 const double2* ff0_dev, const char* methodeit, double tol, double2* ff_dev, double2* loc_dev,
+                 double* tol1, int* nloop, int* ncompte, int* nstop, char* infostr, const ifdda_solve_options* opt) {
+    ifdda_ctx* ctx = g->ctx;
+    const int method = method_code(methodeit);
+    if (method == 0) {
+        if (nstop) *nstop = 1;
+        set_info(infostr, "Iterative method not correct!");
+        return 1;
+    }
+    if (tol < 1e-12 || tol > 0.5) {
+        // cdmlib/cdmlib.f:462-471 rejects tolerances outside this range
+        if (nstop) *nstop = 1;
+        set_info(infostr, "Tolerance out of range [1e-12, 0.5]");
+        return 1;
+    }
+    SolveSpec sp = make_spec(method, nrhs, nb, tol, opt);
+    sp.tabdip = tab_dev;
+    sp.amode = amode;
+    sp.alpha = alpha_dev;
+    sp.nmax = amode == ALPHA_FULL ? nmax : nb;
+    sp.cancel = (volatile int*)nstop;
+    if (nstop && *nstop == -1) {
+        set_info(infostr, "Calculation cancelled during iterative method");
+        return -1;
+    }
+    const int prec = opt ? opt->precision : IFDDA_FP64;
+    std::vector<SolveResult> res;
+    if (prec == IFDDA_MIXED) solve_mixed(g->G, g->SW, sp, ff0_dev, loc_dev, res, ctx->stream);
+    else solve_fp64(g->G, g->SW, sp, ff0_dev, loc_dev, res, ctx->stream);
+    // FF = polarisa . E (cdmlib/inverserigopt.f:92-97)
+    apply_alpha_dev(loc_dev, ff_dev, nb, nrhs, 3L * nb, amode, alpha_dev, sp.nmax, ctx->stream);
+    IFDDA_CUDA(cudaStreamSynchronize(ctx->stream));
+    int rc = 0;
+    const char* msg = nullptr;
+    for (int r = 0; r < nrhs; r++) {
+        if (tol1) tol1[r] = res[r].tol1;
+        if (nloop) nloop[r] = res[r].nloop;
+        if (ncompte) ncompte[r] = res[r].ncompte;
+        if (rc) continue;
+        if (res[r].cancelled) {
+            rc = -1;
+            msg = "Calculation cancelled during iterative method";
+        } else if (res[r].status < 0) {
+            rc = 1;
+            msg = "Problem to solve Ax=b!";
+        } else if (!(res[r].tol1 < tol)) {
+            rc = 1;
+            msg = "Converge do not reach!";
+        }
+    }
+    if (nstop) *nstop = rc;
+    if (msg) set_info(infostr, msg);
+    else if (infostr) memset(infostr, ' ', 64);
+    return rc;
+}
+}  // namespace
+
+extern "C" {
+
+int ifdda_abi_version(void) { return IFDDA_GPU_ABI_VERSION; }
+
+int ifdda_ctx_create(int device, ifdda_ctx** out) {
+    if (!out) return 1;
+    *out = nullptr;
+    auto* c = new ifdda_ctx();
+    try {
+        int n = 0;
+        IFDDA_CUDA(cudaGetDeviceCount(&n));
+        if (device < 0 || device >= n) throw EngineError{1, "no such CUDA device"};
+        c->device = device;
+        DeviceScope ds(device);
+        IFDDA_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->flag.ensure(1);
+        c->st.ensure(1);
+        c->zstatus.ensure(1);
+        c->tickets.ensure(1);
+        IFDDA_CUDA(cudaMemset(c->zstatus.p, 0, sizeof(int)));
+        IFDDA_CUDA(cudaMemset(c->tickets.p, 0, sizeof(unsigned)));
+        c->partials.ensure(1024 * 4);
+    } catch (const EngineError& e) {
+        delete c;
+        return 1;
+    }
+    *out = c;
+    return 0;
+}
+
+int ifdda_ctx_destroy(ifdda_ctx* ctx) {
+    if (!ctx) return 0;
+    {
+        DeviceScope ds(ctx->device);
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
+        ctx->flag.release();
+        ctx->partials.release();
+        ctx->tickets.release();
+        ctx->st.release();
+        ctx->zstatus.release();
+    }
+    delete ctx;
+    return 0;
+}
+
+const char* ifdda_ctx_last_error(const ifdda_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int ifdda_ctx_synchronize(ifdda_ctx* ctx) {
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(ctx->device);
+    IFDDA_CUDA(cudaStreamSynchronize(ctx->stream));
+    return 0;
+    IFDDA_GUARD_END(ctx, nullptr)
+}
+
+void* ifdda_ctx_stream(ifdda_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int ifdda_green_create(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, ifdda_green** out) {
+    if (!ctx || !out) return 1;
+    *out = nullptr;
+    std::unique_ptr<ifdda_green> g(new ifdda_green());
+    g->ctx = ctx;
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(ctx->device);
+    green_build(g->G, nx, ny, nz, aretecube, k0, ctx->stream);
+    *out = g.release();
+    return 0;
+    IFDDA_GUARD_END(ctx, nullptr)
+}
+
+int ifdda_green_destroy(ifdda_green* g) {
+    if (!g) return 0;
+    {
+        DeviceScope ds(g->ctx->device);
+        cudaStreamSynchronize(g->ctx->stream);
+        delete g;
+    }
+    return 0;
+}
+
+int ifdda_green_export(ifdda_green* g, ifdda_dcmplx* xx, ifdda_dcmplx* xy, ifdda_dcmplx* xz, ifdda_dcmplx* yy,
+                       ifdda_dcmplx* yz, ifdda_dcmplx* zz) {
+    if (!g) return 1;
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(g->ctx->device);
+    double2* out[6] = {(double2*)xx, (double2*)xy, (double2*)xz, (double2*)yy, (double2*)yz, (double2*)zz};
+    green_export(g->G, out, g->ctx->stream);
+    return 0;
+    IFDDA_GUARD_END(g->ctx, nullptr)
+}
+
+int ifdda_matvec(ifdda_green* g, int precision, int ndip, const int* tabdip, const ifdda_dcmplx* FFX,
+                 ifdda_dcmplx* FFB) {
+    if (!g || !FFX || !FFB) return 1;
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(g->ctx->device);
+    cudaStream_t st = g->ctx->stream;
+    const MvGeom& geo = g->G.g;
+    if (!tabdip && ndip != geo.N) throw EngineError{1, "ifdda_matvec: ndip must be nx*ny*nz without tabdip"};
+    const long n3 = 3L * ndip;
+    const int* tab = nullptr;
+    if (tabdip) {
+        g->tab.ensure(geo.N);
+        IFDDA_CUDA(cudaMemcpyAsync(g->tab.p, tabdip, geo.N * sizeof(int), cudaMemcpyHostToDevice, st));
+        tab = g->tab.p;
+    }
+    g->ffx.ensure(n3);
+    g->ffb.ensure(n3);
+    IFDDA_CUDA(cudaMemcpyAsync(g->ffx.p, FFX, n3 * sizeof(double2), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(g->ffb.p, FFB, n3 * sizeof(double2), cudaMemcpyHostToDevice, st));
+    if (precision == IFDDA_FP32) {
+        g->ffx32.ensure(n3);
+        g->ffb32.ensure(n3);
+        cast_dev<float>(g->ffx.p, g->ffx32.p, n3, st);
+        cast_dev<float>(g->ffb.p, g->ffb32.p, n3, st);
+        MvArgs<float> a = mv_args<float>(g->G, 1, g->ffx32.p, g->ffb32.p, g->ffb32.p, n3, ALPHA_NONE, nullptr, 0, tab,
+                                         nullptr);
+        if (!matvec_launch<float>(a, 1, tab != nullptr, st)) throw EngineError{1, "FFT size not supported"};
+        std::vector<float2> h(n3);
+        IFDDA_CUDA(cudaMemcpyAsync(h.data(), g->ffb32.p, n3 * sizeof(float2), cudaMemcpyDeviceToHost, st));
+        IFDDA_CUDA(cudaStreamSynchronize(st));
+        for (long i = 0; i < n3; i++) FFB[i] = ifdda_dcmplx{h[i].x, h[i].y};
+    } else {
+        MvArgs<double> a = mv_args<double>(g->G, 1, g->ffx.p, g->ffb.p, g->ffb.p, n3, ALPHA_NONE, nullptr, 0, tab,
+                                           nullptr);
+        if (!matvec_launch<double>(a, 1, tab != nullptr, st)) throw EngineError{1, "FFT size not supported"};
+        IFDDA_CUDA(cudaMemcpyAsync(FFB, g->ffb.p, n3 * sizeof(double2), cudaMemcpyDeviceToHost, st));
+        IFDDA_CUDA(cudaStreamSynchronize(st));
+    }
+    return 0;
+    IFDDA_GUARD_END(g->ctx, nullptr)
+}
+
+int ifdda_matvec_device(ifdda_green* g, int precision, int nrhs, int ndip, const int* tabdip_dev,
+                        const void* FFX_dev, void* FFB_dev) {
+    if (!g || !FFX_dev || !FFB_dev || nrhs < 1 || ndip < 1) return 1;
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(g->ctx->device);
+    cudaStream_t st = g->ctx->stream;
+    if (!tabdip_dev && ndip != g->G.g.N) throw EngineError{1, "ifdda_matvec_device: ndip must be nx*ny*nz"};
+    const long n3 = 3L * ndip;
+    bool ok;
+    if (precision == IFDDA_FP32) {
+        MvArgs<float> a = mv_args<float>(g->G, nrhs, (const float2*)FFX_dev, (const float2*)FFB_dev, (float2*)FFB_dev,
+                                         n3, ALPHA_NONE, nullptr, 0, tabdip_dev, nullptr);
+        ok = matvec_launch<float>(a, nrhs, tabdip_dev != nullptr, st);
+    } else {
+        MvArgs<double> a = mv_args<double>(g->G, nrhs, (const double2*)FFX_dev, (const double2*)FFB_dev,
+                                           (double2*)FFB_dev, n3, ALPHA_NONE, nullptr, 0, tabdip_dev, nullptr);
+        ok = matvec_launch<double>(a, nrhs, tabdip_dev != nullptr, st);
+    }
+    if (!ok) throw EngineError{1, "FFT size not supported"};
+    return 0;
+    IFDDA_GUARD_END(g->ctx, nullptr)
+}
+
+int ifdda_inverserig_batch(ifdda_green* g, int nrhs, int nbsphere, int nmax, const int* tabdip,
+                           const ifdda_dcmplx* polarisa, const ifdda_dcmplx* FF0, const char* methodeit, double tol,
+                           ifdda_dcmplx* FF, ifdda_dcmplx* FFloc, double* tol1, int* nloop, int* ncompte,
+                           int* nstop, char* infostr, const ifdda_solve_options* opt) {
+    if (!g || !polarisa || !FF0 || !FF || !FFloc || nrhs < 1 || nbsphere < 1) {
+        if (nstop) *nstop = 1;
+        set_info(infostr, "invalid argument");
+        return 1;
+    }
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(g->ctx->device);
+    cudaStream_t st = g->ctx->stream;
+    const MvGeom& geo = g->G.g;
+    if (!tabdip && nbsphere != geo.N)
+        throw EngineError{1, "full-box solve: nbsphere must equal nx*ny*nz (or pass tabdip)"};
+    if (nmax < nbsphere) throw EngineError{1, "nmax smaller than nbsphere"};
+    const long n3 = 3L * nbsphere, tot = n3 * nrhs;
+    const int* tab = nullptr;
+    if (tabdip) {
+        g->tab.ensure(geo.N);
+        IFDDA_CUDA(cudaMemcpyAsync(g->tab.p, tabdip, geo.N * sizeof(int), cudaMemcpyHostToDevice, st));
+        tab = g->tab.p;
+    }
+    const int amode = pola_mode(polarisa, nbsphere, nmax);
+    if (amode == ALPHA_ISO) {
+        std::vector<double2> h(nbsphere);
+        for (int i = 0; i < nbsphere; i++) h[i] = make_double2(polarisa[i].re, polarisa[i].im);
+        g->alpha.ensure(nbsphere);
+        IFDDA_CUDA(cudaMemcpyAsync(g->alpha.p, h.data(), nbsphere * sizeof(double2), cudaMemcpyHostToDevice, st));
+        IFDDA_CUDA(cudaStreamSynchronize(st));
+    } else {
+        g->alpha.ensure((size_t)9 * nmax);
+        IFDDA_CUDA(cudaMemcpyAsync(g->alpha.p, polarisa, (size_t)9 * nmax * sizeof(double2), cudaMemcpyHostToDevice,
+                                   st));
+    }
+    g->ff0.ensure(tot);
+    g->x.ensure(tot);
+    g->ffb.ensure(tot);
+    IFDDA_CUDA(cudaMemcpyAsync(g->ff0.p, FF0, tot * sizeof(double2), cudaMemcpyHostToDevice, st));
+    const int rc = solve_device(g, nrhs, nbsphere, nmax, tab, g->alpha.p, amode, g->ff0.p, methodeit, tol, g->ffb.p,
+                                g->x.p, tol1, nloop, ncompte, nstop, infostr, opt);
+    IFDDA_CUDA(cudaMemcpyAsync(FFloc, g->x.p, tot * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaMemcpyAsync(FF, g->ffb.p, tot * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    return rc;
+    IFDDA_GUARD_END(g->ctx, infostr)
+}
+
+int ifdda_inverserig(ifdda_green* g, int nbsphere, int nmax, const int* tabdip, const ifdda_dcmplx* polarisa,
+                     const ifdda_dcmplx* FF0, const char* methodeit, double tol, ifdda_dcmplx* FF,
+                     ifdda_dcmplx* FFloc, double* tol1, int* nloop, int* ncompte, int* nstop, char* infostr,
+                     const ifdda_solve_options* opt) {
+    return ifdda_inverserig_batch(g, 1, nbsphere, nmax, tabdip, polarisa, FF0, methodeit, tol, FF, FFloc, tol1, nloop,
+                                  ncompte, nstop, infostr, opt);
+}
+
+int ifdda_inverserig_batch_device(ifdda_green* g, int nrhs, int nbsphere, int nmax, const int* tabdip_dev,
+                                  const ifdda_dcmplx* polarisa_dev, const ifdda_dcmplx* FF0_dev,
+                                  const char* methodeit, double tol, ifdda_dcmplx* FF_dev, ifdda_dcmplx* FFloc_dev,
+                                  double* tol1, int* nloop, int* ncompte, int* nstop, char* infostr,
+                                  const ifdda_solve_options* opt) {
+    if (!g || !polarisa_dev || !FF0_dev || !FF_dev || !FFloc_dev || nrhs < 1 || nbsphere < 1) {
+        if (nstop) *nstop = 1;
+        set_info(infostr, "invalid argument");
+        return 1;
+    }
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(g->ctx->device);
+    if (!tabdip_dev && nbsphere != g->G.g.N)
+        throw EngineError{1, "full-box solve: nbsphere must equal nx*ny*nz (or pass tabdip)"};
+    return solve_device(g, nrhs, nbsphere, nmax, tabdip_dev, (const double2*)polarisa_dev, ALPHA_FULL,
+                        (const double2*)FF0_dev, methodeit, tol, (double2*)FF_dev, (double2*)FFloc_dev, tol1, nloop,
+                        ncompte, nstop, infostr, opt);
+    IFDDA_GUARD_END(g->ctx, infostr)
+}
+
+int ifdda_local_macro(ifdda_ctx* ctx, int nbsphere, int nmax, const ifdda_dcmplx* epsilon,
+                      const ifdda_dcmplx* FFloc, double aretecube, double k0, ifdda_dcmplx* Em) {
+    if (!ctx || !epsilon || !FFloc || !Em || nbsphere < 1 || nmax < nbsphere) return 1;
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(ctx->device);
+    cudaStream_t st = ctx->stream;
+    DevBuf<double2> eps, loc, em;
+    eps.ensure((size_t)9 * nmax);
+    loc.ensure(3L * nbsphere);
+    em.ensure(3L * nbsphere);
+    IFDDA_CUDA(cudaMemcpyAsync(eps.p, epsilon, (size_t)9 * nmax * sizeof(double2), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(loc.p, FFloc, 3L * nbsphere * sizeof(double2), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemsetAsync(ctx->flag.p, 0, sizeof(int), st));
+    local_macro_dev(nbsphere, nmax, eps.p, loc.p, aretecube, k0, em.p, ctx->flag.p, st);
+    int bad = 0;
+    IFDDA_CUDA(cudaMemcpyAsync(Em, em.p, 3L * nbsphere * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaMemcpyAsync(&bad, ctx->flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    if (bad) throw EngineError{1, "problem in local-macro: singular 3x3 matrix"};
+    return 0;
+    IFDDA_GUARD_END(ctx, nullptr)
+}
+
+int ifdda_cross_sections(ifdda_ctx* ctx, int nbsphere, const ifdda_dcmplx* FF0, const ifdda_dcmplx* FF,
+                         const ifdda_dcmplx* FFloc, double k0, double I0, double* Cext, double* Cabs) {
+    if (!ctx || !FF0 || !FF || !FFloc || nbsphere < 1) return 1;
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(ctx->device);
+    cudaStream_t st = ctx->stream;
+    const long n3 = 3L * nbsphere;
+    DevBuf<double2> a, b, c;
+    a.ensure(n3);
+    b.ensure(n3);
+    c.ensure(n3);
+    IFDDA_CUDA(cudaMemcpyAsync(a.p, FF0, n3 * sizeof(double2), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(b.p, FF, n3 * sizeof(double2), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(c.p, FFloc, n3 * sizeof(double2), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemsetAsync(ctx->tickets.p, 0, sizeof(unsigned), st));
+    cross_sections_dev(nbsphere, a.p, b.p, c.p, k0, ctx->partials.p, ctx->tickets.p, ctx->st.p, ctx->zstatus.p, st);
+    KState h;
+    IFDDA_CUDA(cudaMemcpyAsync(&h, ctx->st.p, sizeof(KState), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    const double pi = 3.14159265358979323846;
+    if (Cext) *Cext = 4.0 * pi * k0 * h.alpha.x / I0;
+    if (Cabs) *Cabs = 4.0 * pi * k0 * h.beta.x / I0;
+    return 0;
+    IFDDA_GUARD_END(ctx, nullptr)
+}
+
+int ifdda_incident_planewaves(ifdda_ctx* ctx, int nbsphere, const double* xs, const double* ys, const double* zs,
+                              double k0, ifdda_dcmplx E0, int nrhs, const int* beam, const double* a1,
+                              const double* a2, const double* pp, ifdda_dcmplx* FF0) {
+    if (!ctx || !xs || !ys || !zs || !beam || !a1 || !a2 || !pp || !FF0 || nbsphere < 1 || nrhs < 1) return 1;
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(ctx->device);
+    cudaStream_t st = ctx->stream;
+    DevBuf<double> dx, dy, dz, d1, d2, dp;
+    DevBuf<int> db;
+    DevBuf<double2> out;
+    dx.ensure(nbsphere);
+    dy.ensure(nbsphere);
+    dz.ensure(nbsphere);
+    d1.ensure(nrhs);
+    d2.ensure(nrhs);
+    dp.ensure(nrhs);
+    db.ensure(nrhs);
+    out.ensure(3L * nbsphere * nrhs);
+    IFDDA_CUDA(cudaMemcpyAsync(dx.p, xs, nbsphere * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(dy.p, ys, nbsphere * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(dz.p, zs, nbsphere * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(d1.p, a1, nrhs * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(d2.p, a2, nrhs * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(dp.p, pp, nrhs * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(db.p, beam, nrhs * sizeof(int), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemsetAsync(ctx->flag.p, 0, sizeof(int), st));
+    planewaves_dev(nbsphere, dx.p, dy.p, dz.p, k0, make_double2(E0.re, E0.im), nrhs, db.p, d1.p, d2.p, dp.p, out.p,
+                   ctx->flag.p, st);
+    int bad = 0;
+    IFDDA_CUDA(cudaMemcpyAsync(FF0, out.p, 3L * nbsphere * nrhs * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaMemcpyAsync(&bad, ctx->flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    if (bad) throw EngineError{1, "problem in plance incident wave"};
+    return 0;
+    IFDDA_GUARD_END(ctx, nullptr)
+}
+
+}  // extern "C"

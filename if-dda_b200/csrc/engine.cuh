@@ -1,0 +1,132 @@
+// Host-side engine types shared by the translation units of libifdda_gpu.so.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+#include <atomic>
+#include "matvec_kernels.cuh"
+
+// FFT lengths (padded grid edges 2n) with compiled kernels.  A lattice edge n
+// is supported when 2n is in this list; the reference's own FFT accepts any
+// length but warns above prime factor 5 (cdmlib/primefactor.f).
+#define IFDDA_FFT_LENGTHS(X) \
+    X(2) X(4) X(6) X(8) X(10) X(12) X(16) X(20) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(160) X(192) X(256) X(320) X(384)
+
+namespace ifdda {
+
+bool fft_length_supported(int L);
+
+struct EngineError {
+    int code;
+    std::string msg;
+};
+
+#define IFDDA_CUDA(call)                                                                          \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            throw ::ifdda::EngineError{1, std::string("CUDA error: ") + cudaGetErrorString(e_) + \
+                                              " at " + __FILE__ + ":" + std::to_string(__LINE__)}; \
+    } while (0)
+
+// Set the dynamic shared-memory limit of a kernel once per device.
+template <class K> inline void ensure_smem(K kernel, size_t bytes) {
+    static std::atomic<uint64_t> done{0};
+    if (bytes <= 48 * 1024) return;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = 1ull << (dev & 63);
+    if (done.load() & bit) return;
+    IFDDA_CUDA(cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    done.fetch_or(bit);
+}
+
+template <class T> struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void ensure(size_t count) {
+        if (count <= n) return;
+        release();
+        IFDDA_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
+        n = count;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevBuf() { release(); }
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+};
+
+// mat-vec scratch for one precision: B1 and B2 for up to `cap` right-hand sides
+template <class T> struct MvWork {
+    DevBuf<cplx<T>> B1, B2;
+    void ensure(const MvGeom& g, int nrhs) {
+        B1.ensure((size_t)g.b1_rhs * nrhs);
+        B2.ensure((size_t)g.b2_rhs * nrhs);
+    }
+};
+
+// Green spectrum of one (lattice, spacing, wavenumber), device resident.
+struct Green {
+    int device = 0;
+    MvGeom g{};
+    double d = 0, k0 = 0;
+    DevBuf<double2> gc64;
+    DevBuf<float2> gc32;
+    DevBuf<double2> tw64[3];
+    DevBuf<float2> tw32[3];
+    MvWork<float> w32;
+    MvWork<double> w64;
+    template <class T> const cplx<T>* gc() const;
+    template <class T> const cplx<T>* tw(int axis) const;
+    template <class T> MvWork<T>& work();
+};
+template <> inline const float2* Green::gc<float>() const { return gc32.p; }
+template <> inline const double2* Green::gc<double>() const { return gc64.p; }
+template <> inline const float2* Green::tw<float>(int a) const { return tw32[a].p; }
+template <> inline const double2* Green::tw<double>(int a) const { return tw64[a].p; }
+template <> inline MvWork<float>& Green::work<float>() { return w32; }
+template <> inline MvWork<double>& Green::work<double>() { return w64; }
+
+MvGeom make_geom(int nx, int ny, int nz);
+// builds the spectrum (FP64, plus an FP32 copy) on `st`; throws EngineError
+void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStream_t st);
+// full FFTTENSOR arrays (6 x 8N) on the host, expanded from the compressed octant
+void green_export(const Green& G, double2* const out[6], cudaStream_t st);
+
+// The five mat-vec passes.  Returns false if a length has no compiled kernel.
+template <class T> bool matvec_launch(const MvArgs<T>& a, int nrhs, bool tab, cudaStream_t st);
+
+// fill MvArgs from a Green object and the caller's vectors
+template <class T>
+MvArgs<T> mv_args(Green& G, int nrhs, const cplx<T>* x, const cplx<T>* b, cplx<T>* y, long xstride, int amode,
+                  const cplx<T>* alpha, long nmax, const int* tabdip, const int* status) {
+    MvArgs<T> a{};
+    a.g = G.g;
+    a.x = x;
+    a.b = b;
+    a.y = y;
+    a.xstride = xstride;
+    a.amode = amode;
+    a.alpha = alpha;
+    a.nmax = nmax;
+    a.tabdip = tabdip;
+    MvWork<T>& w = G.work<T>();
+    w.ensure(G.g, nrhs);
+    a.B1 = w.B1.p;
+    a.B2 = w.B2.p;
+    a.Gc = G.gc<T>();
+    a.twx = G.tw<T>(0);
+    a.twy = G.tw<T>(1);
+    a.twz = G.tw<T>(2);
+    a.status = status;
+    a.inv_m = (T)(1.0 / ((double)G.g.X * G.g.Y * G.g.Z));
+    return a;
+}
+
+}  // namespace ifdda

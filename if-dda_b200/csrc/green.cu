@@ -1,0 +1,145 @@
+// Green spectrum build (replaces greencalculfft, cdmlib/calculgreenfft.f:1-104).
+#include <cmath>
+#include "engine.cuh"
+#include "green_kernels.cuh"
+
+namespace ifdda {
+
+bool fft_length_supported(int L) {
+    switch (L) {
+#define IFDDA_CASE_OK(L) case L:
+        IFDDA_FFT_LENGTHS(IFDDA_CASE_OK)
+        return true;
+#undef IFDDA_CASE_OK
+        default:
+            return false;
+    }
+}
+
+MvGeom make_geom(int nx, int ny, int nz) {
+    MvGeom g{};
+    g.nx = nx;
+    g.ny = ny;
+    g.nz = nz;
+    g.X = 2 * nx;
+    g.Y = 2 * ny;
+    g.Z = 2 * nz;
+    g.N = (long)nx * ny * nz;
+    g.b1_rhs = 3L * nz * ny * g.X;
+    g.b2_rhs = 3L * nz * g.Y * g.X;
+    g.gc_comp = (long)(nx + 1) * (ny + 1) * (nz + 1);
+    return g;
+}
+
+// twiddle table exp(+2 pi i j / L), j < L, computed in FP64 on the host
+static void upload_twiddles(int L, DevBuf<double2>& t64, DevBuf<float2>& t32, cudaStream_t st) {
+    std::vector<double2> h(L);
+    std::vector<float2> hf(L);
+    const double two_pi = 6.283185307179586476925286766559;
+    for (int j = 0; j < L; j++) {
+        // reduce the angle to the first octant-free form exactly where possible
+        const double a = two_pi * (double)j / (double)L;
+        h[j] = make_double2(std::cos(a), std::sin(a));
+        if (4 * j == L) h[j] = make_double2(0.0, 1.0);
+        if (2 * j == L) h[j] = make_double2(-1.0, 0.0);
+        if (4 * j == 3 * L) h[j] = make_double2(0.0, -1.0);
+        if (j == 0) h[j] = make_double2(1.0, 0.0);
+        hf[j] = make_float2((float)h[j].x, (float)h[j].y);
+    }
+    t64.ensure(L);
+    t32.ensure(L);
+    IFDDA_CUDA(cudaMemcpyAsync(t64.p, h.data(), L * sizeof(double2), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(t32.p, hf.data(), L * sizeof(float2), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+}
+
+template <int L> static void launch_gx(const GreenGeom& gg, double2* GA, const double2* tw, cudaStream_t st) {
+    using TT = GreenTiles<L>;
+    dim3 grid((gg.Y + TT::TLX - 1) / TT::TLX, gg.Z, 1);
+    ensure_smem(k_green_x<L>, TT::smem_x);
+    k_green_x<L><<<grid, TT::NT, TT::smem_x, st>>>(gg, GA, tw);
+}
+
+template <int L, int AXIS>
+static void launch_gyz(const GreenGeom& gg, const double2* src, double2* d64, float2* d32, const double2* tw,
+                       cudaStream_t st) {
+    using TT = GreenTiles<L>;
+    const int W = gg.nx + 1;
+    dim3 grid((W + TT::TLY - 1) / TT::TLY, AXIS == 1 ? gg.Z : gg.ny + 1, 6);
+    ensure_smem(k_green_yz<L, AXIS>, TT::smem_y);
+    k_green_yz<L, AXIS><<<grid, TT::NT, TT::smem_y, st>>>(gg, src, d64, d32, tw);
+}
+
+void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStream_t st) {
+    if (nx < 1 || ny < 1 || nz < 1) throw EngineError{1, "Green: lattice dimensions must be positive"};
+    G.g = make_geom(nx, ny, nz);
+    if (!fft_length_supported(G.g.X) || !fft_length_supported(G.g.Y) || !fft_length_supported(G.g.Z))
+        throw EngineError{1, "FFT size not supported: 2*nx, 2*ny and 2*nz must be compiled lengths"};
+    G.d = d;
+    G.k0 = k0;
+    cudaGetDevice(&G.device);
+    upload_twiddles(G.g.X, G.tw64[0], G.tw32[0], st);
+    upload_twiddles(G.g.Y, G.tw64[1], G.tw32[1], st);
+    upload_twiddles(G.g.Z, G.tw64[2], G.tw32[2], st);
+    GreenGeom gg{nx, ny, nz, G.g.X, G.g.Y, G.g.Z, d, k0};
+    const long W = nx + 1;
+    DevBuf<double2> GA, GB;
+    GA.ensure((size_t)6 * G.g.Z * G.g.Y * W);
+    GB.ensure((size_t)6 * G.g.Z * (ny + 1) * W);
+    G.gc64.ensure((size_t)6 * G.g.gc_comp);
+    G.gc32.ensure((size_t)6 * G.g.gc_comp);
+    switch (G.g.X) {
+#define IFDDA_CASE_GX(L) \
+    case L: launch_gx<L>(gg, GA.p, G.tw64[0].p, st); break;
+        IFDDA_FFT_LENGTHS(IFDDA_CASE_GX)
+#undef IFDDA_CASE_GX
+    }
+    switch (G.g.Y) {
+#define IFDDA_CASE_GY(L) \
+    case L: launch_gyz<L, 1>(gg, GA.p, GB.p, nullptr, G.tw64[1].p, st); break;
+        IFDDA_FFT_LENGTHS(IFDDA_CASE_GY)
+#undef IFDDA_CASE_GY
+    }
+    switch (G.g.Z) {
+#define IFDDA_CASE_GZ(L) \
+    case L: launch_gyz<L, 2>(gg, GB.p, G.gc64.p, G.gc32.p, G.tw64[2].p, st); break;
+        IFDDA_FFT_LENGTHS(IFDDA_CASE_GZ)
+#undef IFDDA_CASE_GZ
+    }
+    IFDDA_CUDA(cudaGetLastError());
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+}
+
+// parity of component c along axis a: +1 even, -1 odd (xx,xy,xz,yy,yz,zz)
+static inline int parity(int c, int axis) {
+    static const int P[6][3] = {{1, 1, 1}, {-1, -1, 1}, {-1, 1, -1}, {1, 1, 1}, {1, -1, -1}, {1, 1, 1}};
+    return P[c][axis];
+}
+
+void green_export(const Green& G, double2* const out[6], cudaStream_t st) {
+    const MvGeom& g = G.g;
+    std::vector<double2> h((size_t)6 * g.gc_comp);
+    IFDDA_CUDA(cudaMemcpyAsync(h.data(), G.gc64.p, h.size() * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    const int W = g.nx + 1, H = g.ny + 1;
+    for (int c = 0; c < 6; c++) {
+        const double2* src = h.data() + (size_t)c * g.gc_comp;
+        for (int kz = 0; kz < g.Z; kz++) {
+            const int qz = kz <= g.nz ? kz : g.Z - kz;
+            const int sz = kz <= g.nz ? 1 : parity(c, 2);
+            for (int jy = 0; jy < g.Y; jy++) {
+                const int qy = jy <= g.ny ? jy : g.Y - jy;
+                const int sy = jy <= g.ny ? 1 : parity(c, 1);
+                for (int ix = 0; ix < g.X; ix++) {
+                    const int qx = ix <= g.nx ? ix : g.X - ix;
+                    const int sx = ix <= g.nx ? 1 : parity(c, 0);
+                    const double s = (double)(sx * sy * sz);
+                    const double2 v = src[((size_t)qz * H + qy) * W + qx];
+                    out[c][((size_t)kz * g.Y + jy) * g.X + ix] = make_double2(s * v.x, s * v.y);
+                }
+            }
+        }
+    }
+}
+
+}  // namespace ifdda

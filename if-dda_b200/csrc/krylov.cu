@@ -1,0 +1,408 @@
+// Host orchestration of the device Krylov solvers and of the mixed-precision
+// (FP32 inner / FP64 outer) iterative refinement.
+#include <algorithm>
+#include <cmath>
+#include "solver.cuh"
+
+namespace ifdda {
+
+// ---------------------------------------------------------------- kernels --
+__global__ void k_apply_alpha(const double2* __restrict__ x, double2* __restrict__ y, long nd, int nrhs, long stride,
+                              int amode, const double2* __restrict__ alpha, long nmax) {
+    const long tot = nd * nrhs;
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += (long)gridDim.x * blockDim.x) {
+        const long r = q / nd, d = q - r * nd;
+        const double2* xv = x + r * stride + 3 * d;
+        double2* yv = y + r * stride + 3 * d;
+        const double2 v[3] = {xv[0], xv[1], xv[2]};
+        for (int a = 0; a < 3; a++) {
+            double2 acc = make_double2(0, 0);
+            if (amode == ALPHA_ISO) acc = zmul(alpha[d], v[a]);
+            else if (amode == ALPHA_FULL)
+                for (int b = 0; b < 3; b++) acc = zadd(acc, zmul(alpha[d + nmax * (a + 3 * b)], v[b]));
+            else acc = v[a];
+            yv[a] = acc;
+        }
+    }
+}
+
+// outer residual of the refinement: r = b - A x (A x in ax), relative norm, and
+// the FP32 right-hand side of the next inner solve
+struct ResidualOp {
+    const double2* b;
+    const double2* ax;
+    float2* b32;
+    long n3;
+    KState* stt;     // outer state: norm, residu, tol
+    KState* inner;   // inner state: tol set here
+    int* inner_status;
+    double inner_floor;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const long o = (long)r * n3 + i;
+        const double2 rv = zsub(b[o], ax[o]);
+        b32[o] = make_float2((float)rv.x, (float)rv.y);
+        acc[0].x += rv.x * rv.x + rv.y * rv.y;
+    }
+    __device__ void finish(int r, KState& s, int& status, const double2* a) const {
+        s.residu = sqrt(a[0].x) / s.norm;
+        if (s.residu <= s.tol) {
+            status = 1;
+            inner_status[r] = 1;
+            return;
+        }
+        // ask the inner solve for half of the remaining reduction, but no less
+        // than FP32 vectors can deliver
+        inner[r].tol = fmax(0.5 * s.tol / s.residu, inner_floor);
+        inner[r].maxit = s.maxit;
+        inner_status[r] = 0;
+        s.itno += 1;
+    }
+};
+
+struct NormOp {  // ||b|| of the outer problem, x = b
+    const double2* b;
+    double2* x;
+    long n3;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const long o = (long)r * n3 + i;
+        const double2 v = b[o];
+        x[o] = v;
+        acc[0].x += v.x * v.x + v.y * v.y;
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.norm = sqrt(a[0].x);
+        s.itno = 0;
+    }
+};
+
+struct TrueResOp {  // tol1 = ||A x - b|| / NORM (cdmlib/inverserigopt.f:92-102)
+    const double2* b;
+    const double2* ax;
+    long n3;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const long o = (long)r * n3 + i;
+        const double2 rv = zsub(ax[o], b[o]);
+        acc[0].x += rv.x * rv.x + rv.y * rv.y;
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const { s.residu = sqrt(a[0].x) / s.norm; }
+};
+
+template <class T>
+__global__ void k_axpy_outer(double2* __restrict__ x, const cplx<T>* __restrict__ d, long n3, int nrhs,
+                             const int* __restrict__ ostatus) {
+    const long tot = n3 * nrhs;
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < tot; q += (long)gridDim.x * blockDim.x) {
+        const long r = q / n3;
+        if (ostatus[r]) continue;
+        const double2 v = to_d(d[q]);
+        x[q] = make_double2(x[q].x + v.x, x[q].y + v.y);
+    }
+}
+
+template <class T> __global__ void k_cast(const double2* __restrict__ a, cplx<T>* __restrict__ b, long n) {
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+        b[q] = from_d<cplx<T>>(a[q]);
+}
+
+template <class T> __global__ void k_uncast(const cplx<T>* __restrict__ a, double2* __restrict__ b, long n) {
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+        b[q] = to_d(a[q]);
+}
+
+static inline int grid_for(long n, int nt = 256) { return (int)std::max<long>(1, std::min<long>((n + nt - 1) / nt, 148L * 16)); }
+
+void apply_alpha_dev(const double2* x, double2* y, long nd, int nrhs, long stride, int amode, const double2* alpha,
+                     long nmax, cudaStream_t st) {
+    k_apply_alpha<<<grid_for(nd * nrhs), 256, 0, st>>>(x, y, nd, nrhs, stride, amode, alpha, nmax);
+    IFDDA_CUDA(cudaGetLastError());
+}
+
+template <class T> void cast_dev(const double2* a, cplx<T>* b, long n, cudaStream_t st) {
+    k_cast<T><<<grid_for(n), 256, 0, st>>>(a, b, n);
+    IFDDA_CUDA(cudaGetLastError());
+}
+template void cast_dev<float>(const double2*, float2*, long, cudaStream_t);
+template void cast_dev<double>(const double2*, double2*, long, cudaStream_t);
+
+// ------------------------------------------------------------- solver ----
+int reduction_blocks(long n3) { return (int)std::max<long>(1, std::min<long>((n3 + KNT * 4 - 1) / (KNT * 4), 1024)); }
+
+template <class T> void KrylovWork<T>::ensure(int method, int nrhs_, long n3_) {
+    nslot = method == 1 ? (int)G_NSLOT : (int)Q_NSLOT;
+    nrhs = nrhs_;
+    n3 = n3_;
+    nblk = reduction_blocks(n3);
+    vecs.ensure((size_t)nslot * nrhs * n3);
+    st.ensure(nrhs);
+    status.ensure(nrhs);
+    zstatus.ensure(nrhs);
+    partials.ensure((size_t)nrhs * nblk * 4);
+    tickets.ensure(nrhs);
+    hstatus.resize(nrhs);
+}
+
+template <class T> Slots<T> KrylovWork<T>::slots() const { return Slots<T>{vecs.p, n3, nrhs}; }
+
+template <int ND, class Op>
+static void vec_launch(const Op& op, long n3, int nblk, int nrhs, const RedSlots& rs, int* status, cudaStream_t st) {
+    k_vec<ND, Op><<<dim3(nblk, nrhs), KNT, 0, st>>>(op, n3, nblk, rs, status);
+}
+
+template <class T>
+static void mv_solver(Green& G, const SolveSpec& sp, KrylovWork<T>& W, int sx, int sy, const int* status,
+                      cudaStream_t st) {
+    Slots<T> V = W.slots();
+    const cplx<T>* x = V.base + (long)sx * W.nrhs * W.n3;
+    cplx<T>* y = V.base + (long)sy * W.nrhs * W.n3;
+    MvArgs<T> a = mv_args<T>(G, W.nrhs, x, x, y, W.n3, sp.amode, (const cplx<T>*)sp.alpha, sp.nmax, sp.tabdip, status);
+    if (!matvec_launch<T>(a, W.nrhs, sp.tabdip != nullptr, st))
+        throw EngineError{1, "FFT size not supported by the compiled kernels"};
+}
+
+template <class T> static bool poll(KrylovWork<T>& W, const SolveSpec& sp, cudaStream_t st, bool& cancelled) {
+    IFDDA_CUDA(cudaMemcpyAsync(W.hstatus.data(), W.status.p, W.nrhs * sizeof(int), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    if (sp.cancel && *sp.cancel == -1) {
+        cancelled = true;
+        return true;
+    }
+    for (int r = 0; r < W.nrhs; r++)
+        if (W.hstatus[r] == 0) return false;
+    return true;
+}
+
+// Runs the Krylov loop on slot B (right-hand sides) into slot X.  The state
+// (tol, maxit) must be set for each right-hand side before the call when
+// sp.preset_state is true; otherwise tol/maxit come from sp.
+template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>& W, cudaStream_t st) {
+    Slots<T> V = W.slots();
+    const long n3 = W.n3;
+    const int nrhs = W.nrhs, nblk = W.nblk;
+    RedSlots rs{W.partials.p, W.tickets.p, nblk};
+    if (!sp.preset_state) {
+        std::vector<KState> h(nrhs);
+        for (auto& s : h) {
+            s = KState{};
+            s.tol = sp.tol;
+            s.maxit = sp.maxit;
+        }
+        IFDDA_CUDA(cudaMemcpyAsync(W.st.p, h.data(), nrhs * sizeof(KState), cudaMemcpyHostToDevice, st));
+        IFDDA_CUDA(cudaMemsetAsync(W.status.p, 0, nrhs * sizeof(int), st));
+    }
+    IFDDA_CUDA(cudaMemsetAsync(W.tickets.p, 0, nrhs * sizeof(unsigned), st));
+    int* status = W.status.p;
+    KState* S = W.st.p;
+    bool cancelled = false;
+    const int every = std::max(1, sp.check_every);
+    if (sp.method == 1) {
+        vec_launch<1>(GpStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
+        if (!sp.zero_guess) mv_solver<T>(G, sp, W, G_X, G_XR, status, st);
+        vec_launch<1>(GpInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+        int tcur = G_TA, tnew = G_TB;
+        for (long it = 0;; it++) {
+            vec_launch<0>(GpP<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            mv_solver<T>(G, sp, W, G_P, G_AP, status, st);
+            vec_launch<1>(GpAlpha<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<2>(GpYT<T>{V, S, tcur, tnew}, n3, nblk, nrhs, rs, status, st);
+            mv_solver<T>(G, sp, W, tnew, G_AT, status, st);
+            vec_launch<3>(GpZeta<T>{V, S, tnew}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<2>(GpUpdate<T>{V, S, tcur, tnew}, n3, nblk, nrhs, rs, status, st);
+            std::swap(tcur, tnew);
+            IFDDA_CUDA(cudaGetLastError());
+            if ((it + 1) % every == 0 || it < 2) {
+                if (poll(W, sp, st, cancelled)) break;
+            }
+            if (it > (long)sp.maxit + 4) break;
+        }
+    } else {
+        const int methode = sp.method == 2 ? 1 : 2;
+        vec_launch<1>(QStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
+        if (!sp.zero_guess) mv_solver<T>(G, sp, W, Q_X, Q_XR, status, st);
+        vec_launch<1>(QInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+        for (long it = 0;; it++) {
+            vec_launch<0>(QP<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            mv_solver<T>(G, sp, W, Q_P, Q_V, status, st);
+            vec_launch<1>(QAlpha<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<1>(QS<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            mv_solver<T>(G, sp, W, Q_S, Q_T, status, st);
+            vec_launch<2>(QOmega<T>{V, S, methode}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<2>(QR<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<1>(QX<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            IFDDA_CUDA(cudaGetLastError());
+            if ((it + 1) % every == 0 || it < 2) {
+                if (poll(W, sp, st, cancelled)) break;
+            }
+            if (it > (long)sp.maxit + 4) break;
+        }
+    }
+    return !cancelled;
+}
+
+template <class T> int KrylovWork<T>::x_slot(int method) const { return method == 1 ? (int)G_X : (int)Q_X; }
+template <class T> int KrylovWork<T>::b_slot(int method) const { return method == 1 ? (int)G_B : (int)Q_B; }
+template <class T> int KrylovWork<T>::xr_slot(int method) const { return method == 1 ? (int)G_XR : (int)Q_XR; }
+
+template struct KrylovWork<float>;
+template struct KrylovWork<double>;
+template bool krylov_run<float>(Green&, const SolveSpec&, KrylovWork<float>&, cudaStream_t);
+template bool krylov_run<double>(Green&, const SolveSpec&, KrylovWork<double>&, cudaStream_t);
+
+// ------------------------------------------------------ public drivers ----
+// Plain FP64 solve (the drop-in for inverserig/inverserigopt): the solution
+// x, then A x and the true residual, all FP64.
+void solve_fp64(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b_dev, double2* x_out, std::vector<SolveResult>& res,
+                cudaStream_t st) {
+    KrylovWork<double>& W = SW.kw64;
+    W.ensure(sp.method, sp.nrhs, sp.n3);
+    const long tot = (long)sp.nrhs * sp.n3;
+    Slots<double> V = W.slots();
+    const int bs = W.b_slot(sp.method), xs = W.x_slot(sp.method), xrs = W.xr_slot(sp.method);
+    IFDDA_CUDA(cudaMemcpyAsync(V.v(bs, 0), b_dev, tot * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+    const bool ok = krylov_run<double>(G, sp, W, st);
+    res.assign(sp.nrhs, SolveResult{});
+    std::vector<KState> hs(sp.nrhs);
+    IFDDA_CUDA(cudaMemcpyAsync(hs.data(), W.st.p, sp.nrhs * sizeof(KState), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaMemcpyAsync(W.hstatus.data(), W.status.p, sp.nrhs * sizeof(int), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    // final A x and true residual, for every right-hand side that did not break down
+    IFDDA_CUDA(cudaMemsetAsync(W.zstatus.p, 0, sp.nrhs * sizeof(int), st));
+    {
+        MvArgs<double> a = mv_args<double>(G, sp.nrhs, V.v(xs, 0), V.v(xs, 0), V.v(xrs, 0), sp.n3, sp.amode,
+                                           (const double2*)sp.alpha, sp.nmax, sp.tabdip, W.zstatus.p);
+        if (!matvec_launch<double>(a, sp.nrhs, sp.tabdip != nullptr, st))
+            throw EngineError{1, "FFT size not supported by the compiled kernels"};
+        RedSlots rs{W.partials.p, W.tickets.p, W.nblk};
+        vec_launch<1>(TrueResOp{V.v(bs, 0), V.v(xrs, 0), sp.n3, W.st.p}, sp.n3, W.nblk, sp.nrhs, rs, W.zstatus.p, st);
+    }
+    IFDDA_CUDA(cudaMemcpyAsync(x_out, V.v(xs, 0), tot * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+    std::vector<KState> hf(sp.nrhs);
+    IFDDA_CUDA(cudaMemcpyAsync(hf.data(), W.st.p, sp.nrhs * sizeof(KState), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    for (int r = 0; r < sp.nrhs; r++) {
+        SolveResult& o = res[r];
+        o.status = W.hstatus[r];
+        o.steperr = hs[r].steperr;
+        o.cancelled = !ok;
+        o.tol1 = hf[r].residu;
+        if (sp.method == 1) {
+            o.nloop = hs[r].itno + 1;
+            o.ncompte = 1 + 2 * (hs[r].itno + 1) + 1;
+        } else {
+            o.nloop = hs[r].itno;
+            o.ncompte = 2 + 2 * hs[r].itno;
+        }
+        o.ncompte64 = o.ncompte;
+        o.outer = 0;
+    }
+}
+
+// Mixed precision: FP32 mat-vec and inner Krylov vectors (FP64 scalars)
+// inside FP64 iterative refinement on the true residual.
+void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b_dev, double2* x_out, std::vector<SolveResult>& res,
+                 cudaStream_t st) {
+    const int nrhs = sp.nrhs;
+    const long n3 = sp.n3, tot = (long)nrhs * n3;
+    MixedWork& M = SW.mixed;
+    M.x.ensure(tot);
+    M.ax.ensure(tot);
+    M.alpha32.ensure(sp.amode == ALPHA_FULL ? (size_t)9 * sp.nmax : (size_t)std::max<long>(1, sp.nmax));
+    M.ost.ensure(nrhs);
+    M.ostatus.ensure(nrhs);
+    M.partials.ensure((size_t)nrhs * reduction_blocks(n3) * 4);
+    M.tickets.ensure(nrhs);
+    KrylovWork<float>& W = SW.kw32;
+    W.ensure(sp.method, nrhs, n3);
+    const int nblk = reduction_blocks(n3);
+    RedSlots rs{M.partials.p, M.tickets.p, nblk};
+    // FP32 copy of the polarisability
+    if (sp.amode != ALPHA_NONE) {
+        const long na = sp.amode == ALPHA_FULL ? 9 * sp.nmax : sp.nmax;
+        cast_dev<float>((const double2*)sp.alpha, M.alpha32.p, na, st);
+    }
+    std::vector<KState> ho(nrhs);
+    for (auto& s : ho) {
+        s = KState{};
+        s.tol = sp.tol;
+        s.maxit = sp.maxit;
+    }
+    IFDDA_CUDA(cudaMemcpyAsync(M.ost.p, ho.data(), nrhs * sizeof(KState), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemsetAsync(M.ostatus.p, 0, nrhs * sizeof(int), st));
+    IFDDA_CUDA(cudaMemsetAsync(M.tickets.p, 0, nrhs * sizeof(unsigned), st));
+    // inner state defaults
+    std::vector<KState> hi(nrhs);
+    for (auto& s : hi) {
+        s = KState{};
+        s.tol = sp.tol;
+        s.maxit = sp.maxit;
+    }
+    IFDDA_CUDA(cudaMemcpyAsync(W.st.p, hi.data(), nrhs * sizeof(KState), cudaMemcpyHostToDevice, st));
+    vec_launch<1>(NormOp{b_dev, M.x.p, n3, M.ost.p}, n3, nblk, nrhs, rs, M.ostatus.p, st);
+    Slots<float> V = W.slots();
+    const int bs = W.b_slot(sp.method), xs = W.x_slot(sp.method);
+    SolveSpec isp = sp;
+    isp.zero_guess = 1;
+    isp.preset_state = true;
+    isp.alpha = M.alpha32.p;
+    std::vector<int> ost(nrhs, 0), done_before(nrhs, 0);
+    res.assign(nrhs, SolveResult{});
+    std::vector<long> inner_iters(nrhs, 0), inner_mv(nrhs, 0), outer_mv(nrhs, 0), inner_runs(nrhs, 0);
+    bool ok = true;
+    int outer = 0;
+    for (;; outer++) {
+        MvArgs<double> a = mv_args<double>(G, nrhs, M.x.p, M.x.p, M.ax.p, n3, sp.amode, (const double2*)sp.alpha,
+                                           sp.nmax, sp.tabdip, M.ostatus.p);
+        if (!matvec_launch<double>(a, nrhs, sp.tabdip != nullptr, st))
+            throw EngineError{1, "FFT size not supported by the compiled kernels"};
+        vec_launch<1>(ResidualOp{b_dev, M.ax.p, V.v(bs, 0), n3, M.ost.p, W.st.p, W.status.p, sp.inner_floor}, n3,
+                      nblk, nrhs, rs, M.ostatus.p, st);
+        IFDDA_CUDA(cudaMemcpyAsync(ost.data(), M.ostatus.p, nrhs * sizeof(int), cudaMemcpyDeviceToHost, st));
+        IFDDA_CUDA(cudaStreamSynchronize(st));
+        bool all = true;
+        for (int r = 0; r < nrhs; r++) {
+            if (!done_before[r]) outer_mv[r]++;
+            done_before[r] = ost[r];
+            if (!ost[r]) all = false;
+        }
+        if (all) break;
+        if (outer >= sp.max_outer) break;
+        if (sp.cancel && *sp.cancel == -1) {
+            ok = false;
+            break;
+        }
+        if (!krylov_run<float>(G, isp, W, st)) {
+            ok = false;
+            break;
+        }
+        std::vector<KState> hs(nrhs);
+        IFDDA_CUDA(cudaMemcpyAsync(hs.data(), W.st.p, nrhs * sizeof(KState), cudaMemcpyDeviceToHost, st));
+        IFDDA_CUDA(cudaStreamSynchronize(st));
+        for (int r = 0; r < nrhs; r++) {
+            if (ost[r]) continue;
+            const long its = sp.method == 1 ? hs[r].itno + 1 : hs[r].itno;
+            inner_iters[r] += its;
+            inner_mv[r] += 2 * its;
+            inner_runs[r] += 1;
+        }
+        k_axpy_outer<float><<<grid_for(tot), 256, 0, st>>>(M.x.p, V.v(xs, 0), n3, nrhs, M.ostatus.p);
+        IFDDA_CUDA(cudaGetLastError());
+    }
+    std::vector<KState> hf(nrhs);
+    IFDDA_CUDA(cudaMemcpyAsync(hf.data(), M.ost.p, nrhs * sizeof(KState), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaMemcpyAsync(x_out, M.x.p, tot * sizeof(double2), cudaMemcpyDeviceToDevice, st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    for (int r = 0; r < nrhs; r++) {
+        SolveResult& o = res[r];
+        o.status = ost[r] ? 1 : 0;
+        o.steperr = 0;
+        o.cancelled = !ok;
+        o.tol1 = hf[r].residu;
+        o.nloop = (int)inner_iters[r];
+        o.ncompte = (int)(inner_mv[r] + outer_mv[r]);
+        o.ncompte64 = (int)outer_mv[r];
+        o.outer = (int)inner_runs[r];
+    }
+}
+
+}  // namespace ifdda

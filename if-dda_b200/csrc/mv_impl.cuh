@@ -1,0 +1,70 @@
+// Launch wrappers for the mat-vec passes, dispatched on the FFT length of each
+// axis.  Included by one translation unit per precision.
+#pragma once
+#include "engine.cuh"
+
+namespace ifdda {
+
+template <class T, int L> void launch_fwd_x(const MvArgs<T>& a, int nrhs, bool tab, cudaStream_t st) {
+    using TT = MvTiles<T, L>;
+    dim3 grid((a.g.ny + TT::TLX - 1) / TT::TLX, a.g.nz, nrhs);
+    if (tab) {
+        ensure_smem(k_fwd_x<T, L, true>, TT::smem_x);
+        k_fwd_x<T, L, true><<<grid, TT::NT, TT::smem_x, st>>>(a);
+    } else {
+        ensure_smem(k_fwd_x<T, L, false>, TT::smem_x);
+        k_fwd_x<T, L, false><<<grid, TT::NT, TT::smem_x, st>>>(a);
+    }
+}
+
+template <class T, int L, int DIR> void launch_pass_y(const MvArgs<T>& a, int nrhs, cudaStream_t st) {
+    using TT = MvTiles<T, L>;
+    dim3 grid((a.g.X + TT::TLY - 1) / TT::TLY, a.g.nz, 3 * nrhs);
+    ensure_smem(k_pass_y<T, L, DIR>, TT::smem_y);
+    k_pass_y<T, L, DIR><<<grid, TT::NT, TT::smem_y, st>>>(a);
+}
+
+template <class T, int L> void launch_zconv(const MvArgs<T>& a, int nrhs, cudaStream_t st) {
+    using TT = MvTiles<T, L>;
+    dim3 grid((a.g.X + TT::TLZ - 1) / TT::TLZ, a.g.Y, nrhs);
+    ensure_smem(k_zconv<T, L>, TT::smem_z);
+    k_zconv<T, L><<<grid, TT::NT, TT::smem_z, st>>>(a);
+}
+
+template <class T, int L, class Epi>
+void launch_inv_x(const MvArgs<T>& a, const Epi& epi, int nrhs, bool tab, cudaStream_t st) {
+    using TT = MvTiles<T, L>;
+    dim3 grid((a.g.ny + TT::TLX - 1) / TT::TLX, a.g.nz, nrhs);
+    if (tab) {
+        ensure_smem(k_inv_x<T, L, true, Epi>, TT::smem_x);
+        k_inv_x<T, L, true, Epi><<<grid, TT::NT, TT::smem_x, st>>>(a, epi);
+    } else {
+        ensure_smem(k_inv_x<T, L, false, Epi>, TT::smem_x);
+        k_inv_x<T, L, false, Epi><<<grid, TT::NT, TT::smem_x, st>>>(a, epi);
+    }
+}
+
+#define IFDDA_CASE_FWDX(L) \
+    case L: launch_fwd_x<T, L>(a, nrhs, tab, st); break;
+#define IFDDA_CASE_FWDY(L) \
+    case L: launch_pass_y<T, L, +1>(a, nrhs, st); break;
+#define IFDDA_CASE_INVY(L) \
+    case L: launch_pass_y<T, L, -1>(a, nrhs, st); break;
+#define IFDDA_CASE_ZC(L) \
+    case L: launch_zconv<T, L>(a, nrhs, st); break;
+#define IFDDA_CASE_INVX(L) \
+    case L: launch_inv_x<T, L, Epi>(a, epi, nrhs, tab, st); break;
+
+template <class T, class Epi>
+bool matvec_launch_epi(const MvArgs<T>& a, const Epi& epi, int nrhs, bool tab, cudaStream_t st) {
+    if (!fft_length_supported(a.g.X) || !fft_length_supported(a.g.Y) || !fft_length_supported(a.g.Z)) return false;
+    switch (a.g.X) { IFDDA_FFT_LENGTHS(IFDDA_CASE_FWDX) default: return false; }
+    switch (a.g.Y) { IFDDA_FFT_LENGTHS(IFDDA_CASE_FWDY) default: return false; }
+    switch (a.g.Z) { IFDDA_FFT_LENGTHS(IFDDA_CASE_ZC) default: return false; }
+    switch (a.g.Y) { IFDDA_FFT_LENGTHS(IFDDA_CASE_INVY) default: return false; }
+    switch (a.g.X) { IFDDA_FFT_LENGTHS(IFDDA_CASE_INVX) default: return false; }
+    IFDDA_CUDA(cudaGetLastError());
+    return true;
+}
+
+}  // namespace ifdda

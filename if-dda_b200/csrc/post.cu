@@ -1,0 +1,161 @@
+// Post-step and incident-field kernels.
+//   local_macro  : cdmlib/local-macro.f:3-71 over every dipole (cdmlib/cdmlib.f:2595-2655)
+//   cross sections: cdmlib/cdmlib.f:2730-2746
+//   plane waves  : cdmlib/ondeplane.f:1-50, cdmlib/ondeplanekxky.f:1-60
+#include "post.cuh"
+#include "krylov_kernels.cuh"
+
+namespace ifdda {
+
+// closed-form 3x3 complex inverse by cofactors; returns false when singular
+__device__ __forceinline__ bool inv33(const double2 (&m)[9], double2 (&o)[9]) {
+#define A(i, j) m[(i) + 3 * (j)]
+    const double2 c00 = zsub(zmul(A(1, 1), A(2, 2)), zmul(A(1, 2), A(2, 1)));
+    const double2 c01 = zsub(zmul(A(1, 2), A(2, 0)), zmul(A(1, 0), A(2, 2)));
+    const double2 c02 = zsub(zmul(A(1, 0), A(2, 1)), zmul(A(1, 1), A(2, 0)));
+    const double2 det = zadd(zadd(zmul(A(0, 0), c00), zmul(A(0, 1), c01)), zmul(A(0, 2), c02));
+    if (zisnull(det)) return false;
+    const double2 cof[9] = {
+        c00,
+        c01,
+        c02,
+        zsub(zmul(A(0, 2), A(2, 1)), zmul(A(0, 1), A(2, 2))),
+        zsub(zmul(A(0, 0), A(2, 2)), zmul(A(0, 2), A(2, 0))),
+        zsub(zmul(A(0, 1), A(2, 0)), zmul(A(0, 0), A(2, 1))),
+        zsub(zmul(A(0, 1), A(1, 2)), zmul(A(0, 2), A(1, 1))),
+        zsub(zmul(A(0, 2), A(1, 0)), zmul(A(0, 0), A(1, 2))),
+        zsub(zmul(A(0, 0), A(1, 1)), zmul(A(0, 1), A(1, 0))),
+    };
+#undef A
+    // cof[] is listed column by column of the inverse: (0,0),(1,0),(2,0),(0,1),...
+    for (int q = 0; q < 9; q++) o[q] = zdiv(cof[q], det);
+    return true;
+}
+
+__global__ void k_local_macro(int nb, long nmax, const double2* __restrict__ eps, const double2* __restrict__ loc,
+                              double cst, double2* __restrict__ em, int* __restrict__ bad) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += (long)gridDim.x * blockDim.x) {
+        double2 m[9], mi[9];
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+                const double2 e = eps[i + nmax * (a + 3 * b)];
+                const double d0 = a == b ? 2.0 : 0.0, d1 = a == b ? 1.0 : 0.0;
+                // eps + 2I - i cst (eps - I)
+                const double2 m1 = make_double2(e.x - d1, e.y);
+                m[a + 3 * b] = make_double2(e.x + d0 + cst * m1.y, e.y - cst * m1.x);
+            }
+        if (!inv33(m, mi)) {
+            atomicOr(bad, 1);
+            continue;
+        }
+        for (int a = 0; a < 3; a++) {
+            double2 acc = make_double2(0, 0);
+            for (int b = 0; b < 3; b++) acc = zadd(acc, zmul(mi[a + 3 * b], loc[3 * i + b]));
+            em[3 * i + a] = make_double2(3.0 * acc.x, 3.0 * acc.y);
+        }
+    }
+}
+
+struct CrossOp {
+    const double2* ff0;
+    const double2* ff;
+    const double2* loc;
+    double k03;
+    KState* stt;
+    __device__ void elem(const KState&, int, long i, double2* acc) const {
+        // i runs over 3*nb components
+        const double2 e0 = ff0[i], p = ff[i], l = loc[i];
+        acc[0].x += zconjmul(e0, p).y;                              // Im(conj(E0) p)
+        acc[1].x += zmul(p, zconj(l)).y - 2.0 / 3.0 * k03 * (p.x * p.x + p.y * p.y);
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.alpha = a[0];
+        s.beta = a[1];
+    }
+};
+
+void local_macro_dev(int nb, long nmax, const double2* eps, const double2* loc, double d, double k0, double2* em,
+                     int* bad_dev, cudaStream_t st) {
+    const double pi = 3.14159265358979323846;
+    const double cst = k0 * k0 * k0 * d * d * d / 2.0 / pi;
+    const int grid = (int)std::max(1L, std::min<long>((nb + 255) / 256, 148L * 8));
+    k_local_macro<<<grid, 256, 0, st>>>(nb, nmax, eps, loc, cst, em, bad_dev);
+    IFDDA_CUDA(cudaGetLastError());
+}
+
+void cross_sections_dev(int nb, const double2* ff0, const double2* ff, const double2* loc, double k0,
+                        double2* partials, unsigned* tickets, KState* stt, int* zstatus, cudaStream_t st) {
+    const long n3 = 3L * nb;
+    const int nblk = reduction_blocks(n3);
+    RedSlots rs{partials, tickets, nblk};
+    k_vec<2, CrossOp><<<dim3(nblk, 1), KNT, 0, st>>>(CrossOp{ff0, ff, loc, k0 * k0 * k0, stt}, n3, nblk, rs, zstatus);
+    IFDDA_CUDA(cudaGetLastError());
+}
+
+// one incidence per blockIdx.y; beam 0 ondeplane(theta, phi [deg]); 1 ondeplanekxky(kx, ky)
+__global__ void k_planewaves(int nb, const double* __restrict__ xs, const double* __restrict__ ys,
+                             const double* __restrict__ zs, double k0, double2 E0, const int* __restrict__ beam,
+                             const double* __restrict__ a1, const double* __restrict__ a2,
+                             const double* __restrict__ pp, double2* __restrict__ out, int* __restrict__ bad) {
+    const int r = blockIdx.y;
+    const double ppr = pp[r];
+    if (ppr < 0.0 || ppr > 1.0) {
+        if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(bad, 1);
+        return;
+    }
+    const double p = sqrt(ppr), s = sqrt(1.0 - ppr);
+    double kx, ky, kz;
+    double2 ex, ey, ez;
+    if (beam[r] == 0) {
+        const double pi = 3.14159265358979323846;
+        const double th = a1[r] * pi / 180.0, ph = a2[r] * pi / 180.0;
+        const double sg = copysign(1.0, th);
+        const double2 E0s = make_double2(E0.x * s * sg, E0.y * s * sg), E0p = make_double2(E0.x * p * sg, E0.y * p * sg);
+        kx = k0 * sin(th) * cos(ph);
+        ky = k0 * sin(th) * sin(ph);
+        kz = k0 * cos(th);
+        ey = make_double2(E0s.x * cos(ph) + E0p.x * cos(th) * sin(ph), E0s.y * cos(ph) + E0p.y * cos(th) * sin(ph));
+        ex = make_double2(-E0s.x * sin(ph) + E0p.x * cos(th) * cos(ph), -E0s.y * sin(ph) + E0p.y * cos(th) * cos(ph));
+        ez = make_double2(-E0p.x * sin(th), -E0p.y * sin(th));
+    } else {
+        kx = a1[r];
+        ky = a2[r];
+        kz = sqrt(k0 * k0 - kx * kx - ky * ky);
+        const double2 E0s = make_double2(E0.x * s, E0.y * s), E0p = make_double2(E0.x * p, E0.y * p);
+        if (kz >= 0.99999 * k0) {
+            ex = E0p;
+            ey = E0s;
+            ez = make_double2(0, 0);
+        } else {
+            const double kp = sqrt(kx * kx + ky * ky);
+            const double nsx = -ky / kp, nsy = kx / kp;
+            double npx = kz * nsy, npy = -kz * nsx, npz = -kx * nsy + ky * nsx;
+            const double np = sqrt(npx * npx + npy * npy + npz * npz);
+            npx /= np;
+            npy /= np;
+            npz /= np;
+            ex = make_double2(E0s.x * nsx + E0p.x * npx, E0s.y * nsx + E0p.y * npx);
+            ey = make_double2(E0s.x * nsy + E0p.x * npy, E0s.y * nsy + E0p.y * npy);
+            ez = make_double2(E0p.x * npz, E0p.y * npz);
+        }
+    }
+    double2* o = out + (long)r * 3 * nb;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += (long)gridDim.x * blockDim.x) {
+        double sn, cs;
+        sincos(xs[i] * kx + ys[i] * ky + zs[i] * kz, &sn, &cs);
+        const double2 e = make_double2(cs, sn);
+        o[3 * i] = zmul(ex, e);
+        o[3 * i + 1] = zmul(ey, e);
+        o[3 * i + 2] = zmul(ez, e);
+    }
+}
+
+void planewaves_dev(int nb, const double* xs, const double* ys, const double* zs, double k0, double2 E0, int nrhs,
+                    const int* beam, const double* a1, const double* a2, const double* pp, double2* out, int* bad,
+                    cudaStream_t st) {
+    const int gx = (int)std::max(1L, std::min<long>((nb + 255) / 256, 148L * 4));
+    k_planewaves<<<dim3(gx, nrhs), 256, 0, st>>>(nb, xs, ys, zs, k0, E0, beam, a1, a2, pp, out, bad);
+    IFDDA_CUDA(cudaGetLastError());
+}
+
+}  // namespace ifdda

@@ -1,0 +1,17 @@
+// Post-step and incident-field launchers (device pointers).
+#pragma once
+#include <algorithm>
+#include "solver.cuh"
+
+namespace ifdda {
+
+void local_macro_dev(int nb, long nmax, const double2* eps, const double2* loc, double d, double k0, double2* em,
+                     int* bad_dev, cudaStream_t st);
+// sums land in stt->alpha.x (Cext sum) and stt->beta.x (Cabs sum)
+void cross_sections_dev(int nb, const double2* ff0, const double2* ff, const double2* loc, double k0,
+                        double2* partials, unsigned* tickets, KState* stt, int* zstatus, cudaStream_t st);
+void planewaves_dev(int nb, const double* xs, const double* ys, const double* zs, double k0, double2 E0, int nrhs,
+                    const int* beam, const double* a1, const double* a2, const double* pp, double2* out, int* bad,
+                    cudaStream_t st);
+
+}  // namespace ifdda

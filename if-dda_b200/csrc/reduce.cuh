@@ -1,0 +1,84 @@
+// Deterministic two-stage reductions of complex FP64 sums.
+//
+// Every block reduces its ND running sums in a fixed tree (warp shuffles, then
+// one warp over the warp partials), writes them to partials[rhs][blk][ND],
+// fences, and takes a ticket.  The block that takes the last ticket sums the
+// partials of all blocks in a fixed order and calls the finisher (thread 0),
+// which updates the solver scalars on the device.  The result does not depend
+// on block scheduling, so repeated runs -- and a right-hand side solved alone
+// or inside a batch -- give bit-identical scalars.
+#pragma once
+#include "cplx.cuh"
+
+namespace ifdda {
+
+__device__ __forceinline__ double2 dadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+__device__ __forceinline__ double2 shfl_down2(double2 v, int o) {
+    return make_double2(__shfl_down_sync(0xffffffffu, v.x, o), __shfl_down_sync(0xffffffffu, v.y, o));
+}
+
+// Sum acc over the block; the result is valid in thread 0.  scratch holds
+// ND * 32 double2.
+template <int NT, int ND>
+__device__ __forceinline__ void block_sum(double2 (&acc)[ND], double2* scratch) {
+    static_assert(NT % 32 == 0, "block size must be a multiple of 32");
+    constexpr int NW = NT / 32;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int m = 0; m < ND; m++) {
+        double2 v = acc[m];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = dadd(v, shfl_down2(v, o));
+        if (lane == 0) scratch[m * 32 + w] = v;
+    }
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+        for (int m = 0; m < ND; m++) {
+            double2 v = lane < NW ? scratch[m * 32 + lane] : make_double2(0, 0);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v = dadd(v, shfl_down2(v, o));
+            acc[m] = v;
+        }
+    }
+    __syncthreads();
+}
+
+struct RedSlots {
+    double2* partials;   // [nrhs][maxblk][ND]
+    unsigned* tickets;   // [nrhs]
+    int maxblk;          // stride between right-hand sides, in blocks
+};
+
+// Stage 2.  Returns true in the one block that finished the reduction; the
+// final sums are then in `acc` of thread 0.
+template <int NT, int ND>
+__device__ __forceinline__ bool reduce_across_blocks(double2 (&acc)[ND], int rhs, int blk, int nblk,
+                                                     const RedSlots& rs) {
+    __shared__ double2 scratch[ND * 32];
+    __shared__ bool am_last;
+    block_sum<NT, ND>(acc, scratch);
+    double2* part = rs.partials + ((long)rhs * rs.maxblk) * ND;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int m = 0; m < ND; m++) part[(long)blk * ND + m] = acc[m];
+        __threadfence();
+        const unsigned t = atomicAdd(&rs.tickets[rhs], 1u);
+        am_last = (t == (unsigned)(nblk - 1));
+    }
+    __syncthreads();
+    if (!am_last) return false;
+    __threadfence();
+#pragma unroll
+    for (int m = 0; m < ND; m++) acc[m] = make_double2(0, 0);
+    for (int q = threadIdx.x; q < nblk; q += NT) {
+#pragma unroll
+        for (int m = 0; m < ND; m++) acc[m] = dadd(acc[m], __ldcg(part + (long)q * ND + m));
+    }
+    block_sum<NT, ND>(acc, scratch);
+    if (threadIdx.x == 0) rs.tickets[rhs] = 0u;
+    return true;
+}
+
+}  // namespace ifdda

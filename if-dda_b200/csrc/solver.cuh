@@ -1,0 +1,79 @@
+// Solver workspaces and entry points (host side).
+#pragma once
+#include "engine.cuh"
+#include "krylov_kernels.cuh"
+
+namespace ifdda {
+
+struct SolveSpec {
+    int method = 1;        // 1 GPBICG1, 2 QMRBICGSTAB1, 3 QMRBICGSTAB2
+    int nrhs = 1;
+    long n3 = 0;           // 3 * dipoles
+    double tol = 1e-4;
+    int maxit = 10000;     // nlim of cdmlib/inverserigopt.f:30
+    int check_every = 4;   // iterations launched between status polls
+    int zero_guess = 0;    // x0 = 0 instead of x0 = b
+    bool preset_state = false;
+    const int* tabdip = nullptr;  // device, lattice -> 1-based dipole, or null (full box)
+    int amode = ALPHA_ISO;
+    const void* alpha = nullptr;  // device polarisability (precision of the vectors)
+    long nmax = 0;
+    volatile int* cancel = nullptr;  // host word, -1 cancels (the reference's nstop)
+    // mixed precision
+    int max_outer = 12;
+    double inner_floor = 1e-6;
+};
+
+struct SolveResult {
+    int status = 0;     // 1 converged, 0 not converged, -1 breakdown
+    int steperr = 0;
+    bool cancelled = false;
+    double tol1 = 0;    // true FP64 residual ||A x - b|| / ||b||
+    int nloop = 0;      // iterations (inner iterations for mixed)
+    int ncompte = 0;    // mat-vecs
+    int ncompte64 = 0;  // of which FP64
+    int outer = 0;      // refinement steps (mixed)
+};
+
+template <class T> struct KrylovWork {
+    DevBuf<cplx<T>> vecs;
+    DevBuf<KState> st;
+    DevBuf<int> status, zstatus;
+    DevBuf<double2> partials;
+    DevBuf<unsigned> tickets;
+    std::vector<int> hstatus;
+    int nslot = 0, nrhs = 0, nblk = 1;
+    long n3 = 0;
+    void ensure(int method, int nrhs, long n3);
+    Slots<T> slots() const;
+    int x_slot(int method) const;
+    int b_slot(int method) const;
+    int xr_slot(int method) const;
+};
+
+struct MixedWork {
+    DevBuf<double2> x, ax;
+    DevBuf<float2> alpha32;
+    DevBuf<KState> ost;
+    DevBuf<int> ostatus;
+    DevBuf<double2> partials;
+    DevBuf<unsigned> tickets;
+};
+
+struct SolverWork {
+    KrylovWork<double> kw64;
+    KrylovWork<float> kw32;
+    MixedWork mixed;
+};
+
+int reduction_blocks(long n3);
+template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>& W, cudaStream_t st);
+void solve_fp64(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b_dev, double2* x_out,
+                std::vector<SolveResult>& res, cudaStream_t st);
+void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b_dev, double2* x_out,
+                 std::vector<SolveResult>& res, cudaStream_t st);
+void apply_alpha_dev(const double2* x, double2* y, long nd, int nrhs, long stride, int amode, const double2* alpha,
+                     long nmax, cudaStream_t st);
+template <class T> void cast_dev(const double2* a, cplx<T>* b, long n, cudaStream_t st);
+
+}  // namespace ifdda

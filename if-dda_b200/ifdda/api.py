@@ -1,0 +1,210 @@
+"""Object interface over the C-ABI (numpy in, numpy out).
+
+Errors follow the reference's nstop/infostr convention: a failing solve
+returns nstop = 1 and the reference's message in ``infostr`` ("Problem to
+solve Ax=b!", "Converge do not reach!", "Iterative method not correct!");
+a failing library call (bad argument, CUDA error) raises IfddaError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _capi
+from ._capi import IFDDA_FP32, IFDDA_FP64, IFDDA_MIXED, DComplex, SolveOptions
+
+
+class IfddaError(RuntimeError):
+    pass
+
+
+def _p(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data)
+
+
+def _zc(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+@dataclass
+class SolveResult:
+    FF: np.ndarray            # dipole moments polarisa . E
+    FFloc: np.ndarray         # local field E
+    tol1: np.ndarray          # true residual per right-hand side
+    nloop: np.ndarray
+    ncompte: np.ndarray
+    nstop: int
+    infostr: str
+    extra: dict = field(default_factory=dict)
+
+
+class Context:
+    """One CUDA device and stream (ifdda_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _capi.load()
+        h = C.c_void_p()
+        if self.lib.ifdda_ctx_create(int(device), C.byref(h)) != 0:
+            raise IfddaError(f"ifdda_ctx_create failed for device {device}")
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ifdda_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def last_error(self) -> str:
+        return (self.lib.ifdda_ctx_last_error(self.h) or b"").decode()
+
+    def stream(self) -> int:
+        return self.lib.ifdda_ctx_stream(self.h) or 0
+
+    def synchronize(self):
+        self._check(self.lib.ifdda_ctx_synchronize(self.h))
+
+    def _check(self, rc):
+        if rc != 0:
+            raise IfddaError(self.last_error() or f"ifdda call failed ({rc})")
+
+    def green(self, nx, ny, nz, aretecube, k0) -> "GreenSpectrum":
+        return GreenSpectrum(self, nx, ny, nz, aretecube, k0)
+
+    # -- post-step ------------------------------------------------------
+    def local_macro(self, nbsphere, nmax, epsilon, FFloc, aretecube, k0) -> np.ndarray:
+        eps = _zc(epsilon)
+        loc = _zc(FFloc)
+        em = np.zeros(3 * nbsphere, np.complex128)
+        self._check(self.lib.ifdda_local_macro(self.h, nbsphere, nmax, _p(eps), _p(loc), aretecube, k0, _p(em)))
+        return em
+
+    def cross_sections(self, FF0, FF, FFloc, k0, I0):
+        a, b, c = _zc(FF0), _zc(FF), _zc(FFloc)
+        ce, ca = C.c_double(0), C.c_double(0)
+        self._check(self.lib.ifdda_cross_sections(self.h, len(a) // 3, _p(a), _p(b), _p(c), k0, I0, C.byref(ce),
+                                                  C.byref(ca)))
+        return ce.value, ca.value
+
+    def planewaves(self, xs, ys, zs, k0, E0, beam, a1, a2, pp) -> np.ndarray:
+        """FF0 for a batch of plane waves: beam 0 = ondeplane(theta, phi deg),
+        1 = ondeplanekxky(kx, ky).  Returns (nrhs, 3*nbsphere)."""
+        xs = np.ascontiguousarray(xs, np.float64)
+        ys = np.ascontiguousarray(ys, np.float64)
+        zs = np.ascontiguousarray(zs, np.float64)
+        beam = np.ascontiguousarray(np.atleast_1d(beam), np.int32)
+        a1 = np.ascontiguousarray(np.atleast_1d(a1), np.float64)
+        a2 = np.ascontiguousarray(np.atleast_1d(a2), np.float64)
+        pp = np.ascontiguousarray(np.atleast_1d(pp), np.float64)
+        nrhs = len(beam)
+        out = np.zeros((nrhs, 3 * len(xs)), np.complex128)
+        e0 = complex(E0)
+        self._check(self.lib.ifdda_incident_planewaves(self.h, len(xs), _p(xs), _p(ys), _p(zs), k0,
+                                                       DComplex(e0.real, e0.imag), nrhs, _p(beam), _p(a1),
+                                                       _p(a2), _p(pp), _p(out)))
+        return out
+
+
+class GreenSpectrum:
+    """Device-resident Green spectrum of one lattice (greencalculfft) plus the
+    solver workspace that uses it."""
+
+    def __init__(self, ctx: Context, nx, ny, nz, aretecube, k0):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
+        self.aretecube, self.k0 = float(aretecube), float(k0)
+        h = C.c_void_p()
+        rc = self.lib.ifdda_green_create(ctx.h, self.nx, self.ny, self.nz, self.aretecube, self.k0, C.byref(h))
+        if rc != 0:
+            raise IfddaError(ctx.last_error() or "ifdda_green_create failed")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ifdda_green_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def ntotal(self):
+        return 8 * self.nx * self.ny * self.nz
+
+    def export(self) -> np.ndarray:
+        """The six FFTTENSOR arrays, shape (6, 2nz, 2ny, 2nx)."""
+        M = self.ntotal
+        out = np.zeros((6, M), np.complex128)
+        self.ctx._check(self.lib.ifdda_green_export(self.h, *[_p(out[c]) for c in range(6)]))
+        return out.reshape(6, 2 * self.nz, 2 * self.ny, 2 * self.nx)
+
+    def matvec(self, FFX, FFB, tabdip=None, precision=IFDDA_FP64) -> np.ndarray:
+        """FFB - (1/ntotal) IFFT(G~ FFT(pad FFX)): produitfftmatvectopt (tabdip
+        None) or produitfftmatvect3.  Returns the new FFB."""
+        x = _zc(FFX)
+        b = _zc(FFB).copy()
+        nd = len(x) // 3
+        tab = None if tabdip is None else np.ascontiguousarray(tabdip, np.int32)
+        self.ctx._check(self.lib.ifdda_matvec(self.h, precision, nd, _p(tab) if tab is not None else None, _p(x),
+                                              _p(b)))
+        return b
+
+    def matvec_device(self, nrhs, ndip, FFX_ptr, FFB_ptr, tabdip_ptr=None, precision=IFDDA_FP64):
+        """In-place FFB -= conv(FFX) on device pointers (asynchronous on the
+        context's stream)."""
+        self.ctx._check(self.lib.ifdda_matvec_device(self.h, precision, nrhs, ndip,
+                                                     C.c_void_p(tabdip_ptr) if tabdip_ptr else None,
+                                                     C.c_void_p(FFX_ptr), C.c_void_p(FFB_ptr)))
+
+    def inverserig(self, nbsphere, polarisa, nmax, FF0, methodeit="GPBICG1", tol=1e-4, tabdip=None,
+                   precision=IFDDA_FP64, check_every=0, max_outer=0, inner_floor=0.0, nstop_in=0) -> SolveResult:
+        """Rigorous solve (inverserig / inverserigopt) for one or a batch of
+        right-hand sides.  FF0: (3*nbsphere,) or (nrhs, 3*nbsphere)."""
+        ff0 = _zc(FF0)
+        single = ff0.ndim == 1
+        ff0 = ff0.reshape(-1, 3 * nbsphere)
+        nrhs = ff0.shape[0]
+        pol = _zc(polarisa)
+        FF = np.zeros_like(ff0)
+        FFloc = np.zeros_like(ff0)
+        tol1 = np.zeros(nrhs)
+        nloop = np.zeros(nrhs, np.int32)
+        ncompte = np.zeros(nrhs, np.int32)
+        nstop = C.c_int(nstop_in)
+        info = C.create_string_buffer(b" " * 64, 65)
+        opt = SolveOptions(precision, check_every, max_outer, inner_floor)
+        tab = None if tabdip is None else np.ascontiguousarray(tabdip, np.int32)
+        self.lib.ifdda_inverserig_batch(self.h, nrhs, nbsphere, nmax, _p(tab) if tab is not None else None,
+                                        _p(pol), _p(ff0), methodeit.encode(), tol, _p(FF), _p(FFloc), _p(tol1),
+                                        _p(nloop), _p(ncompte), C.byref(nstop), info, C.byref(opt))
+        r = SolveResult(FF=FF[0] if single else FF, FFloc=FFloc[0] if single else FFloc, tol1=tol1, nloop=nloop,
+                        ncompte=ncompte, nstop=nstop.value, infostr=info.raw[:64].decode(errors="replace"))
+        return r
+
+    def inverserig_device(self, nrhs, nbsphere, nmax, tabdip_ptr, polarisa_ptr, FF0_ptr, FF_ptr, FFloc_ptr,
+                          methodeit="GPBICG1", tol=1e-4, precision=IFDDA_FP64, check_every=0, max_outer=0,
+                          inner_floor=0.0):
+        """Batched solve on device pointers (ints, e.g. torch data_ptr())."""
+        tol1 = np.zeros(nrhs)
+        nloop = np.zeros(nrhs, np.int32)
+        ncompte = np.zeros(nrhs, np.int32)
+        nstop = C.c_int(0)
+        info = C.create_string_buffer(b" " * 64, 65)
+        opt = SolveOptions(precision, check_every, max_outer, inner_floor)
+        self.lib.ifdda_inverserig_batch_device(self.h, nrhs, nbsphere, nmax, C.c_void_p(tabdip_ptr or 0) if tabdip_ptr else None,
+                                               C.c_void_p(polarisa_ptr), C.c_void_p(FF0_ptr), methodeit.encode(),
+                                               tol, C.c_void_p(FF_ptr), C.c_void_p(FFloc_ptr), _p(tol1), _p(nloop),
+                                               _p(ncompte), C.byref(nstop), info, C.byref(opt))
+        return dict(tol1=tol1, nloop=nloop, ncompte=ncompte, nstop=nstop.value,
+                    infostr=info.raw[:64].decode(errors="replace"))

@@ -1,0 +1,138 @@
+/*
+ * ifdda_gpu.h -- C-ABI of libifdda_gpu.so, the sm_100a drop-in for the
+ * FFT-accelerated dipole solve of IF-DDA's cdmlib.
+ *
+ * Conventions are the reference's (cdmlib/cdmlib.h, cdmlib/cdmlib.f):
+ *   - double complex = { double re, im } (ifdda_dcmplx);
+ *   - field vectors are AoS: dipole n (0-based) at 3n+{0,1,2};
+ *   - lattice site (i,j,k) (0-based) has index i + nx*j + nx*ny*k;
+ *   - tabdip[site] is the 1-based dipole number, 0 for an empty site;
+ *   - polarisa / epsilon are column-major (nmax,3,3): (n,a,b) at n + nmax*(a + 3*b);
+ *   - infostr is a Fortran character(64): space padded, not NUL terminated.
+ * Every entry point returns the reference's nstop convention: 0 success,
+ * 1 error (infostr or ifdda_ctx_last_error says why), -1 cancelled.
+ * Nothing here aborts the process (unlike cdmlib/local-macro.f:41-48).
+ */
+#ifndef IFDDA_GPU_H
+#define IFDDA_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IFDDA_GPU_ABI_VERSION 1
+
+typedef struct {
+    double re, im;
+} ifdda_dcmplx;
+
+typedef struct ifdda_ctx ifdda_ctx;     /* one device + one CUDA stream */
+typedef struct ifdda_green ifdda_green; /* device-resident Green spectrum + solver workspace */
+
+/* arithmetic of a solve */
+enum { IFDDA_FP64 = 0, IFDDA_MIXED = 1, IFDDA_FP32 = 2 };
+
+typedef struct {
+    int precision;      /* IFDDA_FP64 (plain drop-in) or IFDDA_MIXED (FP32 inner, FP64 refinement) */
+    int check_every;    /* iterations launched between status polls; 0 = 4 */
+    int max_outer;      /* refinement steps of IFDDA_MIXED; 0 = 12 */
+    double inner_floor; /* smallest relative tolerance asked of an FP32 inner solve; 0 = 1e-6 */
+} ifdda_solve_options;
+
+int ifdda_abi_version(void);
+
+/* Context: device ordinal, owns a CUDA stream.  No counterpart in the
+   reference (which has no device); cdmlib's FFTW plan set-up
+   (cdmlib/cdmlib.f:1150-1165) is the closest analogue. */
+int ifdda_ctx_create(int device, ifdda_ctx** out);
+int ifdda_ctx_destroy(ifdda_ctx* ctx);
+const char* ifdda_ctx_last_error(const ifdda_ctx* ctx);
+int ifdda_ctx_synchronize(ifdda_ctx* ctx);
+/* the context's CUDA stream, as a cudaStream_t cast to void* */
+void* ifdda_ctx_stream(ifdda_ctx* ctx);
+
+/* Green spectrum.  Replaces greencalculfft (cdmlib/calculgreenfft.f:1-104,
+   called at cdmlib/cdmlib.f:1529-1531) with nquad = 0: the six components of
+   the free-space dyadic on the (2nx,2ny,2nz) circulant grid, FFT sign +1.
+   aretecube in metres, k0 in 1/m.  The spectrum stays on the device. */
+int ifdda_green_create(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, ifdda_green** out);
+int ifdda_green_destroy(ifdda_green* g);
+/* Writes the six FFTTENSOR arrays (xx,xy,xz,yy,yz,zz, 8*nx*ny*nz each, x
+   fastest) exactly as greencalculfft leaves them. */
+int ifdda_green_export(ifdda_green* g, ifdda_dcmplx* xx, ifdda_dcmplx* xy, ifdda_dcmplx* xz, ifdda_dcmplx* yy,
+                       ifdda_dcmplx* yz, ifdda_dcmplx* zz);
+
+/* Mat-vec FFB <- FFB - (1/ntotal) IFFT(G~ . FFT(pad FFX)).  Replaces
+   produitfftmatvectopt (cdmlib/produitfftmatvectopt.f:3-121, tabdip == NULL,
+   ndip = nx*ny*nz) and produitfftmatvect3 (cdmlib/produitfftmatvect3.f:2-127,
+   tabdip != NULL, ndip = dipole count).  precision: IFDDA_FP64 or IFDDA_FP32. */
+int ifdda_matvec(ifdda_green* g, int precision, int ndip, const int* tabdip, const ifdda_dcmplx* FFX,
+                 ifdda_dcmplx* FFB);
+
+/* Same operation on nrhs vectors already in device memory, in place on
+   FFB_dev: complex128 vectors for IFDDA_FP64, complex64 for IFDDA_FP32
+   (3*ndip per right-hand side, contiguous).  Asynchronous on the context's
+   stream. */
+int ifdda_matvec_device(ifdda_green* g, int precision, int nrhs, int ndip, const int* tabdip_dev,
+                        const void* FFX_dev, void* FFB_dev);
+
+/* Rigorous solve.  Replaces inverserigopt (cdmlib/inverserigopt.f:1-1085,
+   tabdip == NULL) and inverserig (cdmlib/inverserig.f:1-1090, tabdip != NULL),
+   called at cdmlib/cdmlib.f:1565-1581: initial guess FF0, methodeit
+   "GPBICG1" | "QMRBICGSTAB1" | "QMRBICGSTAB2" (others: nstop = 1,
+   "Iterative method not correct!"), on return FFloc = E (local field),
+   FF = polarisa . E (dipole moments), tol1 = ||A E - FF0|| / ||FF0||
+   (FP64), nloop iterations, ncompte mat-vecs.  *nstop is read during the
+   solve: a value of -1 written by another thread cancels it, as in the
+   reference (cdm/cdmRunWidget.cpp:156).  A converged tol1 >= tol is reported
+   as nstop = 1 "Converge do not reach!" (cdmlib/cdmlib.f:1586-1591).
+   opt may be NULL (plain FP64). */
+int ifdda_inverserig(ifdda_green* g, int nbsphere, int nmax, const int* tabdip, const ifdda_dcmplx* polarisa,
+                     const ifdda_dcmplx* FF0, const char* methodeit, double tol, ifdda_dcmplx* FF,
+                     ifdda_dcmplx* FFloc, double* tol1, int* nloop, int* ncompte, int* nstop, char* infostr,
+                     const ifdda_solve_options* opt);
+
+/* Batched solve of nrhs right-hand sides sharing the object (the serial
+   incidence loop of cdmlib/microsbf.f:214-280 as one launch sequence).
+   FF0, FF, FFloc hold nrhs vectors of 3*nbsphere; tol1, nloop, ncompte hold
+   nrhs entries; nstop/infostr report the first failing right-hand side. */
+int ifdda_inverserig_batch(ifdda_green* g, int nrhs, int nbsphere, int nmax, const int* tabdip,
+                           const ifdda_dcmplx* polarisa, const ifdda_dcmplx* FF0, const char* methodeit, double tol,
+                           ifdda_dcmplx* FF, ifdda_dcmplx* FFloc, double* tol1, int* nloop, int* ncompte,
+                           int* nstop, char* infostr, const ifdda_solve_options* opt);
+
+/* Same as ifdda_inverserig_batch with every array already in device memory
+   of the context's device (inputs resident in HBM).  polarisa_dev is the
+   (nmax,3,3) tensor; tabdip_dev may be NULL. */
+int ifdda_inverserig_batch_device(ifdda_green* g, int nrhs, int nbsphere, int nmax, const int* tabdip_dev,
+                                  const ifdda_dcmplx* polarisa_dev, const ifdda_dcmplx* FF0_dev,
+                                  const char* methodeit, double tol, ifdda_dcmplx* FF_dev, ifdda_dcmplx* FFloc_dev,
+                                  double* tol1, int* nloop, int* ncompte, int* nstop, char* infostr,
+                                  const ifdda_solve_options* opt);
+
+/* Local -> macroscopic field of every dipole (nsens = 1), replacing the loop
+   of cdmlib/cdmlib.f:2595-2655 over local_macro (cdmlib/local-macro.f:3-71);
+   the 3x3 inverse is evaluated in closed form on the device.  epsilon is
+   (nmax,3,3); Em receives 3*nbsphere values. */
+int ifdda_local_macro(ifdda_ctx* ctx, int nbsphere, int nmax, const ifdda_dcmplx* epsilon,
+                      const ifdda_dcmplx* FFloc, double aretecube, double k0, ifdda_dcmplx* Em);
+
+/* Extinction and absorption cross sections (cdmlib/cdmlib.f:2730-2746):
+   Cext = 4 pi k0 / I0 sum Im(conj(FF0) . FF),
+   Cabs = 4 pi k0 / I0 sum [Im(FF . conj(FFloc)) - 2/3 k0^3 |FF|^2]. */
+int ifdda_cross_sections(ifdda_ctx* ctx, int nbsphere, const ifdda_dcmplx* FF0, const ifdda_dcmplx* FF,
+                         const ifdda_dcmplx* FFloc, double k0, double I0, double* Cext, double* Cabs);
+
+/* Incident plane waves for a batch of incidences (the OpenMP loops of
+   cdmlib/cdmlib.f:1180-1187 over ondeplane, cdmlib/ondeplane.f:1-50, and of
+   cdmlib/microsbf.f:245-253 over ondeplanekxky, cdmlib/ondeplanekxky.f:1-60).
+   beam 0: a1 = theta, a2 = phi in degrees; beam 1: a1 = kx, a2 = ky in 1/m.
+   Writes nrhs vectors of 3*nbsphere into FF0. */
+int ifdda_incident_planewaves(ifdda_ctx* ctx, int nbsphere, const double* xs, const double* ys, const double* zs,
+                              double k0, ifdda_dcmplx E0, int nrhs, const int* beam, const double* a1,
+                              const double* a2, const double* pp, ifdda_dcmplx* FF0);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

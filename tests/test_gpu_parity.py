@@ -1,0 +1,169 @@
+"""GPU parity of the sm_100a path against the FP64 oracle, through the C-ABI.
+
+Tolerances: FP64 kernels agree with the oracle to 1e-11 relative (different
+FFT factorisations round differently); FP32 mat-vecs to 2e-5; a converged
+solve reproduces the oracle's iteration and mat-vec counts exactly and its
+local field to 1e-7 relative (Krylov amplifies the 1e-15 FFT differences).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from cases import c1, rel, random_field
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(4, 3, 2), (5, 6, 3), (8, 8, 8), (12, 10, 8), (16, 16, 16), (24, 20, 12)]
+
+
+@pytest.mark.parametrize("dims", SIZES)
+def test_green_spectrum_matches_oracle(gctx, orc, dims):
+    nx, ny, nz = dims
+    d, k0 = 11e-9, 2 * math.pi / 550e-9
+    g = gctx.green(nx, ny, nz, d, k0)
+    got = g.export()
+    ref = orc.greencalculfft(nx, ny, nz, d, k0)
+    for c in range(6):
+        assert np.abs(got[c] - ref[c]).max() <= 1e-11 * np.abs(ref[c]).max(), c
+    g.close()
+
+
+@pytest.mark.parametrize("dims", SIZES)
+@pytest.mark.parametrize("inside", [False, True])
+def test_matvec_fp64_matches_oracle(gctx, orc, dims, inside):
+    nx, ny, nz = dims
+    d, k0 = 9e-9, 2 * math.pi / 480e-9
+    N = nx * ny * nz
+    tab = None
+    nb = N
+    if inside:
+        rng = np.random.default_rng(nx * 100 + ny)
+        occ = rng.uniform(size=N) < 0.6
+        tab = np.zeros(N, np.int32)
+        tab[occ] = np.arange(1, occ.sum() + 1)
+        nb = int(occ.sum())
+    x = random_field(3 * nb, 1)
+    b = random_field(3 * nb, 2)
+    g = gctx.green(nx, ny, nz, d, k0)
+    got = g.matvec(x, b, tabdip=tab)
+    G = orc.greencalculfft(nx, ny, nz, d, k0)
+    ref = orc.matvec(G, nx, ny, nz, x, b, tabdip=tab)
+    assert rel(got, ref) < 1e-11
+    from ifdda import IFDDA_FP32
+    got32 = g.matvec(x, b, tabdip=tab, precision=IFDDA_FP32)
+    assert rel(got32, ref) < 2e-5
+    g.close()
+
+
+def _c1_inputs(orc, nnnr=16):
+    ob, k0, E0 = c1(nnnr)
+    ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 1.0, 0, 0.0, 0.0)
+    G = orc.greencalculfft(ob.nx, ob.ny, ob.nz, ob.aretecube, k0)
+    return ob, k0, E0, ff0, G
+
+
+@pytest.mark.parametrize("meth", ["GPBICG1", "QMRBICGSTAB1", "QMRBICGSTAB2"])
+def test_c1_solve_fp64_matches_oracle(gctx, orc, meth):
+    ob, k0, E0, ff0, G = _c1_inputs(orc)
+    ref = orc.inverserig(G, 16, 16, 16, ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-4, tabdip=ob.tabdip)
+    g = gctx.green(16, 16, 16, ob.aretecube, k0)
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-4, tabdip=ob.tabdip)
+    assert r.nstop == ref["nstop"] == 0
+    assert int(r.nloop[0]) == ref["nloop"]
+    assert int(r.ncompte[0]) == ref["ncompte"]
+    assert abs(r.tol1[0] - ref["tol1"]) <= 1e-6 * ref["tol1"]
+    assert rel(r.FFloc, ref["FFloc"]) < 1e-7
+    assert rel(r.FF, ref["FF"]) < 1e-7
+    g.close()
+
+
+@pytest.mark.parametrize("meth", ["GPBICG1", "QMRBICGSTAB1"])
+def test_full_box_solve_matches_oracle(gctx, orc, meth):
+    """Sphere in its full box (na = 0, inverserigopt), vacuum sites alpha = 0."""
+    from ifdda import objects
+    k0 = 2 * math.pi / 500e-9
+    ob = objects.sphere(120e-9, 3.0 + 0.2j, 12, k0, "RR", na=0)
+    ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, 1.0, 0.3, 0, 30.0, 40.0)
+    G = orc.greencalculfft(12, 12, 12, ob.aretecube, k0)
+    ref = orc.inverserig(G, 12, 12, 12, ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-6)
+    g = gctx.green(12, 12, 12, ob.aretecube, k0)
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-6)
+    assert r.nstop == 0 and int(r.nloop[0]) == ref["nloop"] and int(r.ncompte[0]) == ref["ncompte"]
+    assert rel(r.FFloc, ref["FFloc"]) < 1e-7
+    g.close()
+
+
+def test_mixed_precision_meets_fp64_residual(gctx, orc):
+    from ifdda import IFDDA_MIXED
+    ob, k0, E0, ff0, G = _c1_inputs(orc)
+    tight = orc.inverserig(G, 16, 16, 16, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-10,
+                           tabdip=ob.tabdip)
+    g = gctx.green(16, 16, 16, ob.aretecube, k0)
+    for meth in ("GPBICG1", "QMRBICGSTAB1"):
+        r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-4, tabdip=ob.tabdip, precision=IFDDA_MIXED)
+        assert r.nstop == 0, r.infostr
+        assert r.tol1[0] < 1e-4
+        # local-field error of a 1e-4 solve against the converged FP64 field
+        assert rel(r.FFloc, tight["FFloc"]) < 1e-3
+    g.close()
+
+
+def test_batch_equals_single_bitwise(gctx, orc):
+    """A right-hand side gives bit-identical results alone and inside a batch
+    (fixed-order reductions, per-RHS scalars)."""
+    ob, k0, E0, _, _ = _c1_inputs(orc, nnnr=10)
+    angles = [(0.0, 0.0, 1.0), (20.0, 10.0, 0.0), (35.0, 70.0, 1.0), (10.0, 200.0, 0.5)]
+    ff0 = np.stack([orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, pp, 0, t, p) for t, p, pp in angles])
+    g = gctx.green(10, 10, 10, ob.aretecube, k0)
+    for prec in (0, 1):
+        rb = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-5, tabdip=ob.tabdip,
+                          precision=prec)
+        assert rb.nstop == 0
+        for q in range(len(angles)):
+            rs = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0[q], "GPBICG1", 1e-5, tabdip=ob.tabdip,
+                              precision=prec)
+            assert np.array_equal(rs.FFloc, rb.FFloc[q])
+            assert rs.nloop[0] == rb.nloop[q] and rs.ncompte[0] == rb.ncompte[q]
+    g.close()
+
+
+def test_post_step_matches_oracle(gctx, orc):
+    ob, k0, E0, ff0, G = _c1_inputs(orc)
+    ref = orc.inverserig(G, 16, 16, 16, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-4, tabdip=ob.tabdip)
+    em_ref = orc.local_macro_all(ob.nbsphere, ob.nmax, ob.epsilon, ref["FFloc"], ob.aretecube, k0)
+    em = gctx.local_macro(ob.nbsphere, ob.nmax, ob.epsilon, ref["FFloc"], ob.aretecube, k0)
+    assert rel(em, em_ref) < 1e-13
+    ce_r, ca_r = orc.cross_sections(ff0, ref["FF"], ref["FFloc"], k0, E0 ** 2)
+    ce, ca = gctx.cross_sections(ff0, ref["FF"], ref["FFloc"], k0, E0 ** 2)
+    assert abs(ce - ce_r) <= 1e-12 * abs(ce_r)
+    assert abs(ca - ca_r) <= 1e-9 * abs(ce_r)
+
+
+def test_planewaves_match_oracle(gctx, orc):
+    ob, k0, E0, _, _ = _c1_inputs(orc, nnnr=8)
+    beams = [(0, 0.0, 0.0, 1.0), (0, 25.0, -40.0, 0.3), (1, 0.3 * k0, -0.4 * k0, 0.0), (1, 0.0, 0.0, 1.0),
+             (1, 0.1 * k0, 0.7 * k0, 0.6)]
+    got = gctx.planewaves(ob.xs, ob.ys, ob.zs, k0, E0, [b[0] for b in beams], [b[1] for b in beams],
+                          [b[2] for b in beams], [b[3] for b in beams])
+    for q, (bm, a1, a2, pp) in enumerate(beams):
+        ref = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, pp, bm, a1, a2)
+        assert rel(got[q], ref) < 1e-13
+
+
+def test_error_paths(gctx, orc):
+    ob, k0, E0, ff0, _ = _c1_inputs(orc, nnnr=6)
+    g = gctx.green(6, 6, 6, ob.aretecube, k0)
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, "TFQMR", 1e-4, tabdip=ob.tabdip)
+    assert r.nstop == 1 and r.infostr.strip() == "Iterative method not correct!"
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, np.zeros_like(ff0), "GPBICG1", 1e-4, tabdip=ob.tabdip)
+    assert r.nstop == 1 and r.infostr.strip() == "Problem to solve Ax=b!"
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1.0, tabdip=ob.tabdip)
+    assert r.nstop == 1
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-4, tabdip=ob.tabdip, nstop_in=-1)
+    assert r.nstop == -1 and r.infostr.strip() == "Calculation cancelled during iterative method"
+    # unsupported FFT length: 2*7 = 14 has no compiled kernel
+    import ifdda
+    with pytest.raises(ifdda.IfddaError):
+        gctx.green(7, 7, 7, 10e-9, k0)
+    g.close()

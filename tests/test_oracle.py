@@ -1,0 +1,214 @@
+"""CPU tests: the oracle pinned against independent answers, and the
+product's host set-up checked against the oracle."""
+import math
+
+import numpy as np
+import pytest
+
+from cases import c1, rel, random_field
+
+
+def test_fft_sign_and_normalisation(orc):
+    rng = np.random.default_rng(0)
+    a = rng.standard_normal((6, 10, 12)) + 1j * rng.standard_normal((6, 10, 12))
+    # sign +1 is numpy's unnormalised inverse transform, sign -1 its forward one
+    assert rel(orc.fft3d(a, +1), np.fft.ifftn(a) * a.size) < 1e-14
+    assert rel(orc.fft3d(a, -1), np.fft.fftn(a)) < 1e-14
+
+
+@pytest.mark.parametrize("shape", [(7, 1, 1), (3, 5, 2), (16, 9, 25), (13, 11, 7)])
+def test_fft_any_length(orc, shape):
+    rng = np.random.default_rng(1)
+    a = rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+    assert rel(orc.fft3d(a, +1), np.fft.ifftn(a) * a.size) < 1e-13
+
+
+def test_propa_espace_libre_symmetry(orc):
+    k0 = 2 * math.pi / 500e-9
+    t = orc.propa_espace_libre((1e-8, -2e-8, 3e-8), (0, 0, 0), k0)
+    assert np.allclose(t, t.T, rtol=0, atol=1e-12 * abs(t).max())
+    t2 = orc.propa_espace_libre((-1e-8, 2e-8, -3e-8), (0, 0, 0), k0)
+    assert np.allclose(t, t2)  # even in r
+    assert np.all(orc.propa_espace_libre((0, 0, 0), (0, 0, 0), k0) == 0)
+
+
+@pytest.mark.parametrize("dims,inside", [((4, 3, 2), False), ((5, 5, 5), False), ((6, 6, 6), True)])
+def test_fft_matvec_equals_direct_sum(orc, dims, inside):
+    """Pins the circulant embedding, wrap, zero planes and 1/ntotal scaling."""
+    nx, ny, nz = dims
+    k0 = 2 * math.pi / 600e-9
+    d = 15e-9
+    G = orc.greencalculfft(nx, ny, nz, d, k0)
+    N = nx * ny * nz
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    i, j, k = (a.transpose(2, 1, 0).ravel() for a in (i, j, k))
+    tab = np.arange(1, N + 1, dtype=np.int32)
+    if inside:
+        keep = ((i - 2.5) ** 2 + (j - 2.5) ** 2 + (k - 2.5) ** 2) < 7.0
+        tab = np.zeros(N, np.int32)
+        tab[keep] = np.arange(1, keep.sum() + 1)
+        i, j, k = i[keep], j[keep], k[keep]
+    nb = len(i)
+    x = random_field(3 * nb, 5)
+    b = random_field(3 * nb, 6)
+    y = orc.matvec(G, nx, ny, nz, x, b, tabdip=tab if inside else None)
+    yd = orc.matvec_direct(i * d, j * d, k * d, k0, x, b)
+    assert rel(y, yd) < 1e-12
+
+
+def test_green_parity_octant(orc):
+    """Every FFTTENSOR component is even or odd along each axis, so the GPU
+    keeps only q <= n per axis."""
+    nx, ny, nz = 5, 4, 3
+    G = orc.greencalculfft(nx, ny, nz, 10e-9, 2 * math.pi / 500e-9)
+    par = {0: (1, 1, 1), 1: (-1, -1, 1), 2: (-1, 1, -1), 3: (1, 1, 1), 4: (1, -1, -1), 5: (1, 1, 1)}
+    for c, (px, py, pz) in par.items():
+        g = G[c]  # (Z, Y, X)
+        m = np.roll(g[::-1, ::-1, ::-1], 1, axis=(0, 1, 2))  # q -> (L - q) mod L on every axis
+        assert rel(m * (px * py * pz), g) < 1e-12
+        mx = np.roll(g[:, :, ::-1], 1, axis=2)
+        assert rel(mx * px, g) < 1e-12
+
+
+def test_gpbicg_self_test_kat(orc):
+    """The reference's own GPBICG self-test (cdmlib/gpbicg.f:1-79): diag(i*k) x = i."""
+    n = 5
+    mat = np.diag([1j * (q + 1) for q in range(n)])
+    x, st, _ = orc.gpbicg_dense(mat, np.full(n, 1j), np.zeros(n), 1e-3)
+    assert st == 1
+    # GPBICG's own stop test: relative 2-norm residual <= tol (gpbicg.f:282-296)
+    assert np.linalg.norm(mat @ x - np.full(n, 1j)) / np.linalg.norm(np.full(n, 1j)) <= 1e-3
+    assert np.allclose(x, 1.0 / np.arange(1, n + 1), rtol=2e-3)
+
+
+def test_mie_known_answer(orc):
+    """Small-sphere limit: Cext -> Rayleigh absorption/scattering."""
+    eps = 2.25 + 0.1j
+    a = 5e-9
+    lam = 600e-9
+    ce, cs, ca = orc.mie(eps, a, lam)
+    k = 2 * math.pi / lam
+    al = 4 * math.pi * a ** 3 * (eps - 1) / (eps + 2)
+    cabs_r = k * al.imag
+    csca_r = k ** 4 / (6 * math.pi) * abs(al) ** 2
+    # size parameter x = 0.05: corrections to the dipole limit are O(x^2)
+    assert abs(ca - cabs_r) / cabs_r < 5e-3
+    assert abs(cs - csca_r) / csca_r < 5e-3
+    assert abs(ce - (ca + cs)) / ce < 1e-12
+
+
+def test_c1_solution_and_mie(orc):
+    ob, k0, E0 = c1()
+    assert ob.nbsphere == 2176 and abs(ob.aretecube - 12.5e-9) < 1e-20
+    G = orc.greencalculfft(16, 16, 16, ob.aretecube, k0)
+    ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 1.0, 0, 0.0, 0.0)
+    r = orc.inverserig(G, 16, 16, 16, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-4, tabdip=ob.tabdip)
+    assert r["nstop"] == 0 and r["tol1"] < 1e-4
+    assert r["ncompte"] == 2 * r["nloop"] + 2
+    ce, ca = orc.cross_sections(ff0, r["FF"], r["FFloc"], k0, E0 ** 2)
+    me, _, _ = orc.mie(2.25, 100e-9, 632.8e-9)
+    assert abs(ce - me) / me < 0.06  # DDA discretisation error at 16 layers
+
+
+@pytest.mark.parametrize("meth", ["QMRBICGSTAB1", "QMRBICGSTAB2"])
+def test_qmr_agrees_with_gpbicg(orc, meth):
+    ob, k0, E0 = c1(nnnr=8)
+    G = orc.greencalculfft(8, 8, 8, ob.aretecube, k0)
+    ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 1.0, 0, 0.0, 0.0)
+    a = orc.inverserig(G, 8, 8, 8, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-10, tabdip=ob.tabdip)
+    b = orc.inverserig(G, 8, 8, 8, ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-10, tabdip=ob.tabdip)
+    assert b["nstop"] == 0 and b["ncompte"] == 2 * b["nloop"] + 2
+    assert rel(b["FFloc"], a["FFloc"]) < 1e-8
+
+
+def test_unknown_method_message(orc):
+    ob, k0, E0 = c1(nnnr=4)
+    G = orc.greencalculfft(4, 4, 4, ob.aretecube, k0)
+    ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 1.0, 0, 0.0, 0.0)
+    r = orc.inverserig(G, 4, 4, 4, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "TFQMRX", 1e-4, tabdip=ob.tabdip)
+    assert r["nstop"] == 1 and r["infostr"].strip() == "Iterative method not correct!"
+
+
+def test_zero_rhs_breakdown(orc):
+    ob, k0, _ = c1(nnnr=4)
+    G = orc.greencalculfft(4, 4, 4, ob.aretecube, k0)
+    r = orc.inverserig(G, 4, 4, 4, ob.nbsphere, ob.polarisa, ob.nmax, np.zeros(3 * ob.nbsphere), "GPBICG1", 1e-4,
+                       tabdip=ob.tabdip)
+    assert r["nstop"] == 1 and r["infostr"].strip() == "Problem to solve Ax=b!"
+
+
+def test_local_macro_roundtrip(orc):
+    ob, k0, E0 = c1(nnnr=6)
+    loc = random_field(3 * ob.nbsphere, 2)
+    em = orc.local_macro_all(ob.nbsphere, ob.nmax, ob.epsilon, loc, ob.aretecube, k0)
+    # nsens = -1 recovers Eloc: Eloc = M Em / 3 with M = eps + 2 - i c (eps - 1)
+    c = k0 ** 3 * ob.aretecube ** 3 / 2 / math.pi
+    e = ob.eps.repeat(3)
+    back = (e + 2 - 1j * c * (e - 1)) * em / 3
+    assert rel(back, loc) < 1e-13
+
+
+# ---- product host set-up vs oracle -------------------------------------
+def test_objects_sphere_matches_oracle(orc):
+    from ifdda import objects
+    k0 = 2 * math.pi / 632.8e-9
+    for na in (-1, 0):
+        a = objects.sphere(100e-9, 2.25, 10, k0, "RR", na=na)
+        b = orc.object_sphere(100e-9, 2.25, 10, na, k0, "RR")
+        assert a.nbsphere == b.nbsphere
+        assert np.array_equal(a.tabdip, b.tabdip)
+        assert np.array_equal(a.xs, b.xs) and np.array_equal(a.zs, b.zs)
+        assert rel(a.polarisa, b.polarisa) < 1e-15
+        assert rel(a.epsilon, b.epsilon) < 1e-15
+
+
+@pytest.mark.parametrize("meth", ["CM", "RR", "GB", "LA", "LR"])
+def test_poladiff_matches_oracle(orc, meth):
+    from ifdda import objects
+    k0 = 2 * math.pi / 500e-9
+    for eps in (2.25, 3.0 + 0.01j, 12 + 1j):
+        a = objects.poladiff(10e-9, eps, k0, meth)
+        b = orc.poladiff(10e-9, eps, k0, meth)
+        assert abs(a - b) <= 1e-14 * abs(b)
+
+
+def test_sunif_matches_oracle(orc):
+    from ifdda import objects
+    assert np.array_equal(objects.sunif_sequence(29, 1000), orc.sunif_sequence(29, 1000))
+
+
+def test_grf_cuboid_matches_oracle(orc):
+    from ifdda import objects
+    k0 = 2 * math.pi / 632.8e-9
+    a = objects.inhomocuboid(16, 12, 10, 10e-9, 2.25, 50e-9, 0.1, 3, k0, "RR")
+    b = orc.object_inhomocuboid(16, 12, 10, 10e-9, 2.25, 50e-9, 0.1, 3, k0, "RR")
+    assert rel(a.epsilon, b.epsilon) < 1e-14
+    assert rel(a.polarisa, b.polarisa) < 1e-13
+
+
+def test_grf_statistics():
+    """mean eps 2.25 and std close to hc for the C2 configuration"""
+    from ifdda import objects
+    k0 = 2 * math.pi / 632.8e-9
+    ob = objects.inhomocuboid(64, 64, 64, 10e-9, 2.25, 50e-9, 0.1, 7, k0, "RR")
+    e = ob.eps.real
+    assert abs(e.mean() - 2.25) < 0.02
+    assert 0.03 < e.std() < 0.2
+
+
+def test_concentric_matches_oracle(orc):
+    from ifdda import objects
+    k0 = 2 * math.pi / 632.8e-9
+    for na in (-1, 0):
+        a = objects.concentric([0.9e-6, 1.9e-6], [3.0 + 0.01j, 2.0], 12, k0, "RR", na=na)
+        b = orc.object_concentric([0.9e-6, 1.9e-6], [3.0 + 0.01j, 2.0], 12, na, k0, "RR")
+        assert a.nbsphere == b.nbsphere and np.array_equal(a.tabdip, b.tabdip)
+        assert rel(a.polarisa, b.polarisa) < 1e-15
+
+
+def test_cube_matches_oracle(orc):
+    from ifdda import objects
+    k0 = 2 * math.pi / 500e-9
+    a = objects.cube(200e-9, 2.0 + 0.3j, 8, k0, "CM")
+    b = orc.object_cube(200e-9, 2.0 + 0.3j, 8, k0, "CM")
+    assert np.array_equal(a.xs, b.xs) and rel(a.polarisa, b.polarisa) < 1e-15
