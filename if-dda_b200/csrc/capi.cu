@@ -82,6 +82,12 @@ int pola_mode(const ifdda_dcmplx* pol, int nb, long nmax) {
     return ALPHA_ISO;
 }
 
+// every tabdip entry must name a dipole in [1, ndip] or be 0 (empty site)
+void check_tabdip(const int* tab, long nsites, int ndip) {
+    for (long s = 0; s < nsites; s++)
+        if (tab[s] < 0 || tab[s] > ndip) throw EngineError{1, "tabdip entry out of range [0, nbsphere]"};
+}
+
 int method_code(const char* m) {
     char buf[13];
     memset(buf, ' ', 12);
@@ -268,6 +274,7 @@ int ifdda_matvec(ifdda_green* g, int precision, int ndip, const int* tabdip, con
     const long n3 = 3L * ndip;
     const int* tab = nullptr;
     if (tabdip) {
+        check_tabdip(tabdip, geo.N, ndip);
         g->tab.ensure(geo.N);
         IFDDA_CUDA(cudaMemcpyAsync(g->tab.p, tabdip, geo.N * sizeof(int), cudaMemcpyHostToDevice, st));
         tab = g->tab.p;
@@ -341,6 +348,7 @@ int ifdda_inverserig_batch(ifdda_green* g, int nrhs, int nbsphere, int nmax, con
     const long n3 = 3L * nbsphere, tot = n3 * nrhs;
     const int* tab = nullptr;
     if (tabdip) {
+        check_tabdip(tabdip, geo.N, nbsphere);
         g->tab.ensure(geo.N);
         IFDDA_CUDA(cudaMemcpyAsync(g->tab.p, tabdip, geo.N * sizeof(int), cudaMemcpyHostToDevice, st));
         tab = g->tab.p;
