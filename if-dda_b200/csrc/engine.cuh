@@ -5,6 +5,9 @@
 #include <string>
 #include <vector>
 #include <atomic>
+#include <mutex>
+#include <unordered_map>
+#include "instrument.cuh"
 #include "matvec_kernels.cuh"
 
 // FFT lengths (padded grid edges 2n) with compiled kernels.  A lattice edge n
@@ -30,17 +33,21 @@ struct EngineError {
                                               " at " + __FILE__ + ":" + std::to_string(__LINE__)}; \
     } while (0)
 
-// Set the dynamic shared-memory limit of a kernel once per device.
-template <class K> inline void ensure_smem(K kernel, size_t bytes) {
-    static std::atomic<uint64_t> done{0};
+// Set the dynamic shared-memory limit of a kernel once per (kernel, device).
+inline void ensure_smem_ptr(const void* kernel, size_t bytes) {
     if (bytes <= 48 * 1024) return;
+    static std::mutex mu;
+    static std::unordered_map<const void*, uint64_t> done;
     int dev = 0;
     cudaGetDevice(&dev);
     const uint64_t bit = 1ull << (dev & 63);
-    if (done.load() & bit) return;
-    IFDDA_CUDA(cudaFuncSetAttribute((const void*)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
-    done.fetch_or(bit);
+    std::lock_guard<std::mutex> lk(mu);
+    uint64_t& m = done[kernel];
+    if (m & bit) return;
+    IFDDA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    m |= bit;
 }
+template <class K> inline void ensure_smem(K kernel, size_t bytes) { ensure_smem_ptr((const void*)kernel, bytes); }
 
 template <class T> struct DevBuf {
     T* p = nullptr;

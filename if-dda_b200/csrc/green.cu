@@ -57,6 +57,7 @@ template <int L> static void launch_gx(const GreenGeom& gg, double2* GA, const d
     using TT = GreenTiles<L>;
     dim3 grid((gg.Y + TT::TLX - 1) / TT::TLX, gg.Z, 1);
     ensure_smem(k_green_x<L>, TT::smem_x);
+    count_launch();
     k_green_x<L><<<grid, TT::NT, TT::smem_x, st>>>(gg, GA, tw);
 }
 
@@ -67,6 +68,7 @@ static void launch_gyz(const GreenGeom& gg, const double2* src, double2* d64, fl
     const int W = gg.nx + 1;
     dim3 grid((W + TT::TLY - 1) / TT::TLY, AXIS == 1 ? gg.Z : gg.ny + 1, 6);
     ensure_smem(k_green_yz<L, AXIS>, TT::smem_y);
+    count_launch();
     k_green_yz<L, AXIS><<<grid, TT::NT, TT::smem_y, st>>>(gg, src, d64, d32, tw);
 }
 

@@ -115,11 +115,13 @@ static inline int grid_for(long n, int nt = 256) { return (int)std::max<long>(1,
 
 void apply_alpha_dev(const double2* x, double2* y, long nd, int nrhs, long stride, int amode, const double2* alpha,
                      long nmax, cudaStream_t st) {
+    count_launch();
     k_apply_alpha<<<grid_for(nd * nrhs), 256, 0, st>>>(x, y, nd, nrhs, stride, amode, alpha, nmax);
     IFDDA_CUDA(cudaGetLastError());
 }
 
 template <class T> void cast_dev(const double2* a, cplx<T>* b, long n, cudaStream_t st) {
+    count_launch();
     k_cast<T><<<grid_for(n), 256, 0, st>>>(a, b, n);
     IFDDA_CUDA(cudaGetLastError());
 }
@@ -147,6 +149,7 @@ template <class T> Slots<T> KrylovWork<T>::slots() const { return Slots<T>{vecs.
 
 template <int ND, class Op>
 static void vec_launch(const Op& op, long n3, int nblk, int nrhs, const RedSlots& rs, int* status, cudaStream_t st) {
+    count_launch();
     k_vec<ND, Op><<<dim3(nblk, nrhs), KNT, 0, st>>>(op, n3, nblk, rs, status);
 }
 
@@ -385,6 +388,7 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
             inner_mv[r] += 2 * its;
             inner_runs[r] += 1;
         }
+        count_launch();
         k_axpy_outer<float><<<grid_for(tot), 256, 0, st>>>(M.x.p, V.v(xs, 0), n3, nrhs, M.ostatus.p);
         IFDDA_CUDA(cudaGetLastError());
     }

@@ -5,9 +5,18 @@
 
 namespace ifdda {
 
+// brackets one pass launch with the optional timing events and counts it
+struct PassScope {
+    cudaEvent_t ev;
+    cudaStream_t st;
+    PassScope(int pass, int bytes, cudaStream_t s) : ev(timing_before(pass, bytes, s)), st(s) { count_launch(); }
+    ~PassScope() { timing_after(ev, st); }
+};
+
 template <class T, int L> void launch_fwd_x(const MvArgs<T>& a, int nrhs, bool tab, cudaStream_t st) {
     using TT = MvTiles<T, L>;
     dim3 grid((a.g.ny + TT::TLX - 1) / TT::TLX, a.g.nz, nrhs);
+    PassScope ps(PASS_FWD_X, TT::S, st);
     if (tab) {
         ensure_smem(k_fwd_x<T, L, true>, TT::smem_x);
         k_fwd_x<T, L, true><<<grid, TT::NT, TT::smem_x, st>>>(a);
@@ -20,6 +29,7 @@ template <class T, int L> void launch_fwd_x(const MvArgs<T>& a, int nrhs, bool t
 template <class T, int L, int DIR> void launch_pass_y(const MvArgs<T>& a, int nrhs, cudaStream_t st) {
     using TT = MvTiles<T, L>;
     dim3 grid((a.g.X + TT::TLY - 1) / TT::TLY, a.g.nz, 3 * nrhs);
+    PassScope ps(DIR > 0 ? PASS_FWD_Y : PASS_INV_Y, TT::S, st);
     ensure_smem(k_pass_y<T, L, DIR>, TT::smem_y);
     k_pass_y<T, L, DIR><<<grid, TT::NT, TT::smem_y, st>>>(a);
 }
@@ -27,6 +37,7 @@ template <class T, int L, int DIR> void launch_pass_y(const MvArgs<T>& a, int nr
 template <class T, int L> void launch_zconv(const MvArgs<T>& a, int nrhs, cudaStream_t st) {
     using TT = MvTiles<T, L>;
     dim3 grid((a.g.X + TT::TLZ - 1) / TT::TLZ, a.g.Y, nrhs);
+    PassScope ps(PASS_ZCONV, TT::S, st);
     ensure_smem(k_zconv<T, L>, TT::smem_z);
     k_zconv<T, L><<<grid, TT::NT, TT::smem_z, st>>>(a);
 }
@@ -35,6 +46,7 @@ template <class T, int L, class Epi>
 void launch_inv_x(const MvArgs<T>& a, const Epi& epi, int nrhs, bool tab, cudaStream_t st) {
     using TT = MvTiles<T, L>;
     dim3 grid((a.g.ny + TT::TLX - 1) / TT::TLX, a.g.nz, nrhs);
+    PassScope ps(PASS_INV_X, TT::S, st);
     if (tab) {
         ensure_smem(k_inv_x<T, L, true, Epi>, TT::smem_x);
         k_inv_x<T, L, true, Epi><<<grid, TT::NT, TT::smem_x, st>>>(a, epi);
@@ -59,9 +71,13 @@ template <class T, class Epi>
 bool matvec_launch_epi(const MvArgs<T>& a, const Epi& epi, int nrhs, bool tab, cudaStream_t st) {
     if (!fft_length_supported(a.g.X) || !fft_length_supported(a.g.Y) || !fft_length_supported(a.g.Z)) return false;
     switch (a.g.X) { IFDDA_FFT_LENGTHS(IFDDA_CASE_FWDX) default: return false; }
+    IFDDA_CUDA(cudaGetLastError());
     switch (a.g.Y) { IFDDA_FFT_LENGTHS(IFDDA_CASE_FWDY) default: return false; }
+    IFDDA_CUDA(cudaGetLastError());
     switch (a.g.Z) { IFDDA_FFT_LENGTHS(IFDDA_CASE_ZC) default: return false; }
+    IFDDA_CUDA(cudaGetLastError());
     switch (a.g.Y) { IFDDA_FFT_LENGTHS(IFDDA_CASE_INVY) default: return false; }
+    IFDDA_CUDA(cudaGetLastError());
     switch (a.g.X) { IFDDA_FFT_LENGTHS(IFDDA_CASE_INVX) default: return false; }
     IFDDA_CUDA(cudaGetLastError());
     return true;

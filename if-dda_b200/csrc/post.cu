@@ -79,6 +79,7 @@ void local_macro_dev(int nb, long nmax, const double2* eps, const double2* loc, 
     const double pi = 3.14159265358979323846;
     const double cst = k0 * k0 * k0 * d * d * d / 2.0 / pi;
     const int grid = (int)std::max(1L, std::min<long>((nb + 255) / 256, 148L * 8));
+    count_launch();
     k_local_macro<<<grid, 256, 0, st>>>(nb, nmax, eps, loc, cst, em, bad_dev);
     IFDDA_CUDA(cudaGetLastError());
 }
@@ -88,6 +89,7 @@ void cross_sections_dev(int nb, const double2* ff0, const double2* ff, const dou
     const long n3 = 3L * nb;
     const int nblk = reduction_blocks(n3);
     RedSlots rs{partials, tickets, nblk};
+    count_launch();
     k_vec<2, CrossOp><<<dim3(nblk, 1), KNT, 0, st>>>(CrossOp{ff0, ff, loc, k0 * k0 * k0, stt}, n3, nblk, rs, zstatus);
     IFDDA_CUDA(cudaGetLastError());
 }
@@ -154,6 +156,7 @@ void planewaves_dev(int nb, const double* xs, const double* ys, const double* zs
                     const int* beam, const double* a1, const double* a2, const double* pp, double2* out, int* bad,
                     cudaStream_t st) {
     const int gx = (int)std::max(1L, std::min<long>((nb + 255) / 256, 148L * 4));
+    count_launch();
     k_planewaves<<<dim3(gx, nrhs), 256, 0, st>>>(nb, xs, ys, zs, k0, E0, beam, a1, a2, pp, out, bad);
     IFDDA_CUDA(cudaGetLastError());
 }

@@ -57,7 +57,12 @@ SIGNATURES = {
     "ifdda_cross_sections": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_double, C.c_double, _dp, _dp]),
     "ifdda_incident_planewaves": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_double, DComplex, C.c_int, _vp, _vp,
                                             _vp, _vp, _vp]),
+    "ifdda_launch_count": (C.c_ulonglong, []),
+    "ifdda_timing_enable": (C.c_int, [C.c_int, C.c_int]),
+    "ifdda_timing_read": (C.c_int, [_ip, _dp]),
 }
+
+PASS_FWD_X, PASS_FWD_Y, PASS_ZCONV, PASS_INV_Y, PASS_INV_X = 1, 2, 3, 4, 5
 
 
 def load():

@@ -132,6 +132,19 @@ int ifdda_incident_planewaves(ifdda_ctx* ctx, int nbsphere, const double* xs, co
                               double k0, ifdda_dcmplx E0, int nrhs, const int* beam, const double* a1,
                               const double* a2, const double* pp, ifdda_dcmplx* FF0);
 
+/* Diagnostics (no counterpart in the reference, whose only instrumentation
+   is the wall/CPU-time printout of cdmlib/cdmlib.f:1956-1963 and the
+   mat-vec count ncompte).
+   ifdda_launch_count: kernels launched by this library since it was loaded.
+   ifdda_timing_enable: bracket every launch of one mat-vec pass with CUDA
+   events on its stream (pass 1 fwd_x, 2 fwd_y, 3 zconv, 4 inv_y, 5 inv_x;
+   0 disables; precision IFDDA_FP64 / IFDDA_FP32 filters, -1 both).
+   ifdda_timing_read: waits for the recorded events, returns the number of
+   timed launches and their summed duration, and clears the record. */
+unsigned long long ifdda_launch_count(void);
+int ifdda_timing_enable(int pass, int precision);
+int ifdda_timing_read(int* launches, double* total_ms);
+
 #ifdef __cplusplus
 }
 #endif
