@@ -35,7 +35,6 @@ struct EngineError {
 
 // Set the dynamic shared-memory limit of a kernel once per (kernel, device).
 inline void ensure_smem_ptr(const void* kernel, size_t bytes) {
-    if (bytes <= 48 * 1024) return;
     static std::mutex mu;
     static std::unordered_map<const void*, uint64_t> done;
     int dev = 0;
@@ -44,7 +43,11 @@ inline void ensure_smem_ptr(const void* kernel, size_t bytes) {
     std::lock_guard<std::mutex> lk(mu);
     uint64_t& m = done[kernel];
     if (m & bit) return;
-    IFDDA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    if (bytes > 48 * 1024)
+        IFDDA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    // prefer the largest shared-memory carveout: the tiles, not L1, hold the data
+    IFDDA_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    cudaSharedmemCarveoutMaxShared));
     m |= bit;
 }
 template <class K> inline void ensure_smem(K kernel, size_t bytes) { ensure_smem_ptr((const void*)kernel, bytes); }

@@ -1,9 +1,7 @@
 // Shared-memory Stockham FFT on a tile of NB independent lines of length L.
 //
-// Layout in shared memory: point p of line b sits at sm[p * LS + b] (lines
-// fastest), so a warp touching consecutive lines at one point reads
-// consecutive words.  Each pass of radix R combines R sub-transforms of length
-// Ns into one of length Ns * R (autosort Stockham, natural-order output):
+// Each pass of radix R combines R sub-transforms of length Ns into one of
+// length Ns * R (autosort Stockham, natural-order output):
 //     v[r] = x[j + r L/R] * w^(DIR * (j mod Ns) * r * L / (Ns R)),  r < R
 //     v    = DFT_R(v, DIR)
 //     x[(j / Ns) Ns R + (j mod Ns) + r Ns] = v[r]
@@ -11,22 +9,43 @@
 // transform runs in place.  DIR = +1 is exp(+i 2 pi jk / L) (the reference's
 // "forward" convention for G and x, cdmlib/calculgreenfft.f:16,76-99), DIR = -1
 // the inverse; both unnormalised.  L may be any product of 2, 3 and 5.
+//
+// The first pass may read its inputs straight from global memory (Src::GLOBAL)
+// and the last pass may write straight to global memory (Dst::GLOBAL), so a
+// transform costs one shared-memory round trip less at each end.  With
+// Src::HALF the upper half of the input is known to be zero (the padding of
+// the circulant embedding) and is neither loaded nor stored; with Dst::HALF
+// only the first half of the output is written (the crop).
+//
+// Shared-memory layout: point p of line b at sm[p * PS + b * BS].  With
+// BFAST the butterflies of consecutive threads belong to consecutive lines
+// (use with BS = 1: lines contiguous in global memory, e.g. the y and z axes);
+// otherwise consecutive threads take consecutive points of one line (PS = 1,
+// e.g. the x axis).
 #pragma once
 #include "cplx.cuh"
 
 namespace ifdda {
 
-// radix used for the pass that starts at sub-length Ns
-__host__ __device__ constexpr int pick_radix(int rem) {
+// radices 8, 4, 2, 3, 5 in that order of preference
+__host__ __device__ constexpr int pick_radix_basic(int rem) {
     return rem % 8 == 0 ? 8 : rem % 4 == 0 ? 4 : rem % 2 == 0 ? 2 : rem % 3 == 0 ? 3 : rem % 5 == 0 ? 5 : 0;
 }
-__host__ __device__ constexpr int num_passes(int L) {
+__host__ __device__ constexpr int passes_basic(int rem) {
     int n = 0;
-    for (int rem = L; rem > 1; rem /= pick_radix(rem)) {
-        if (pick_radix(rem) == 0) return -1;
+    while (rem > 1) {
+        const int r = pick_radix_basic(rem);
+        if (r == 0) return 1000;
+        rem /= r;
         n++;
     }
     return n;
+}
+// radix of the pass that has `rem` = L / Ns points left to combine: the
+// first pass takes 16 where that saves a whole pass (one shared-memory round
+// trip less; the first pass needs no table twiddles), otherwise 8, 4, 2, 3, 5
+__host__ __device__ constexpr int pick_radix(int rem, bool first = false) {
+    return (first && rem % 16 == 0 && 1 + passes_basic(rem / 16) < passes_basic(rem)) ? 16 : pick_radix_basic(rem);
 }
 __host__ __device__ constexpr bool smooth235(int L) {
     if (L < 1) return false;
@@ -35,11 +54,23 @@ __host__ __device__ constexpr bool smooth235(int L) {
     while (L % 5 == 0) L /= 5;
     return L == 1;
 }
-
 __host__ __device__ constexpr int clamp_pow2(int v, int lo, int hi) {
     int p = 1;
     while (p * 2 <= v && p * 2 <= hi) p *= 2;
     return p < lo ? lo : p;
+}
+// largest radix used by the plan of L (sets the register footprint)
+__host__ __device__ constexpr int max_radix(int L) {
+    int m = 1;
+    bool first = true;
+    for (int rem = L; rem > 1;) {
+        const int r = pick_radix(rem, first);
+        if (r == 0) return 0;
+        m = r > m ? r : m;
+        rem /= r;
+        first = false;
+    }
+    return m;
 }
 
 // Exact mathematical constants used by the radix-3/5/8 butterflies.
@@ -94,6 +125,45 @@ template <int DIR, class C> struct Dft<8, DIR, C> {
     }
 };
 
+// 16 points as 4 x 4: DFT4 over the stride-4 subsequences, the inner twiddles
+// w16^(n2 k1), then DFT4 across them; X[k1 + 4 k2]
+#define IFDDA_COS_PI8 0.92387953251128675612818318939679  // cos(pi / 8)
+#define IFDDA_SIN_PI8 0.38268343236508977172845998403040  // sin(pi / 8)
+template <int DIR, class C> struct Dft<16, DIR, C> {
+    __device__ __forceinline__ static void run(C* v) {
+        using T = decltype(C().x);
+        C a[4][4];
+#pragma unroll
+        for (int n2 = 0; n2 < 4; n2++) {
+            C t[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+            Dft<4, DIR, C>::run(t);
+#pragma unroll
+            for (int k1 = 0; k1 < 4; k1++) a[n2][k1] = t[k1];
+        }
+        const T c = (T)IFDDA_COS_PI8, s = (T)IFDDA_SIN_PI8, h = (T)IFDDA_SQRT1_2;
+        const T ds = DIR > 0 ? s : -s, dc = DIR > 0 ? c : -c, dh = DIR > 0 ? h : -h;
+        // w^1 = c + i DIR s, w^2 = (1 + i DIR)/sqrt2, w^3 = s + i DIR c,
+        // w^4 = i DIR, w^6 = (-1 + i DIR)/sqrt2, w^9 = -w^1
+        const C w1 = mk(c, ds), w2 = mk(h, dh), w3 = mk(s, dc), w6 = mk(-h, dh), w9 = mk(-c, -ds);
+        a[1][1] = cmul(a[1][1], w1);
+        a[1][2] = cmul(a[1][2], w2);
+        a[1][3] = cmul(a[1][3], w3);
+        a[2][1] = cmul(a[2][1], w2);
+        a[2][2] = cmul_i<DIR>(a[2][2]);
+        a[2][3] = cmul(a[2][3], w6);
+        a[3][1] = cmul(a[3][1], w3);
+        a[3][2] = cmul(a[3][2], w6);
+        a[3][3] = cmul(a[3][3], w9);
+#pragma unroll
+        for (int k1 = 0; k1 < 4; k1++) {
+            C t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+            Dft<4, DIR, C>::run(t);
+#pragma unroll
+            for (int k2 = 0; k2 < 4; k2++) v[k1 + 4 * k2] = t[k2];
+        }
+    }
+};
+
 template <int DIR, class C> struct Dft<3, DIR, C> {
     __device__ __forceinline__ static void run(C* v) {
         using T = decltype(C().x);
@@ -124,21 +194,47 @@ template <int DIR, class C> struct Dft<5, DIR, C> {
     }
 };
 
+// Source / destination that is the shared-memory tile itself.
+struct SmemIO {
+    static constexpr bool GLOBAL = false;
+    static constexpr bool HALF = false;
+    template <class C> __device__ C load(int, int) const { return C(); }
+    template <class C> __device__ void store(int, int, C) const {}
+};
+
+template <int PS_, int BS_, bool BFAST_> struct Layout {
+    static constexpr int PS = PS_, BS = BS_;
+    static constexpr bool BFAST = BFAST_;
+};
+
 // One Stockham pass.  tw[j] = exp(+2 pi i j / L) in shared memory.
-template <class C, int L, int Ns, int NB, int LS, int NT, int DIR>
-__device__ __forceinline__ void stockham_pass(C* sm, const C* tw) {
-    constexpr int R = pick_radix(L / Ns);
-    constexpr int NBF = NB * (L / R);
+template <class C, int L, int Ns, int NB, int NT, int DIR, class Lay, class Src, class Dst>
+__device__ __forceinline__ void stockham_pass(C* sm, const C* tw, const Src& src, const Dst& dst) {
+    constexpr int R = pick_radix(L / Ns, Ns == 1);
+    constexpr int NJ = L / R;
+    constexpr int NBF = NB * NJ;
     constexpr int PER = (NBF + NT - 1) / NT;
     constexpr int TSTEP = L / (Ns * R);
+    constexpr bool FIRST = Ns == 1, LAST = Ns * R == L;
+    constexpr bool GIN = FIRST && Src::GLOBAL, GOUT = LAST && Dst::GLOBAL;
     C v[PER][R];
 #pragma unroll
     for (int q = 0; q < PER; q++) {
         const int u = threadIdx.x + q * NT;
         if (PER * NT == NBF || u < NBF) {
-            const int b = u % NB, j = u / NB;
+            const int b = Lay::BFAST ? u % NB : u / NJ;
+            const int j = Lay::BFAST ? u / NB : u % NJ;
 #pragma unroll
-            for (int r = 0; r < R; r++) v[q][r] = sm[(j + r * (L / R)) * LS + b];
+            for (int r = 0; r < R; r++) {
+                const int p = j + r * NJ;
+                if (GIN) {
+                    // zero upper half: for an even radix p >= L/2 exactly when r >= R/2
+                    const bool zero = Src::HALF && (R % 2 == 0 ? 2 * r >= R : 2 * p >= L);
+                    v[q][r] = zero ? mk(decltype(C().x)(0), decltype(C().x)(0)) : src.template load<C>(b, p);
+                } else {
+                    v[q][r] = sm[p * Lay::PS + b * Lay::BS];
+                }
+            }
             if (Ns > 1) {
                 const int k = j % Ns;
 #pragma unroll
@@ -151,35 +247,54 @@ __device__ __forceinline__ void stockham_pass(C* sm, const C* tw) {
             Dft<R, DIR, C>::run(v[q]);
         }
     }
-    __syncthreads();
+    if (!GIN) __syncthreads();
 #pragma unroll
     for (int q = 0; q < PER; q++) {
         const int u = threadIdx.x + q * NT;
         if (PER * NT == NBF || u < NBF) {
-            const int b = u % NB, j = u / NB;
+            const int b = Lay::BFAST ? u % NB : u / NJ;
+            const int j = Lay::BFAST ? u / NB : u % NJ;
             const int k = j % Ns;
             const int d = (j / Ns) * Ns * R + k;
 #pragma unroll
-            for (int r = 0; r < R; r++) sm[(d + r * Ns) * LS + b] = v[q][r];
+            for (int r = 0; r < R; r++) {
+                const int o = d + r * Ns;
+                if (GOUT) {
+                    // last pass: o = j + r L/R; for an even radix o < L/2 exactly when r < R/2
+                    const bool keep = !Dst::HALF || (R % 2 == 0 ? 2 * r < R : 2 * o < L);
+                    if (keep) dst.template store<C>(b, o, v[q][r]);
+                } else {
+                    sm[o * Lay::PS + b * Lay::BS] = v[q][r];
+                }
+            }
         }
     }
-    __syncthreads();
+    if (!GOUT) __syncthreads();
 }
 
-template <class C, int L, int Ns, int NB, int LS, int NT, int DIR>
-__device__ __forceinline__ void stockham_chain(C* sm, const C* tw) {
+template <class C, int L, int Ns, int NB, int NT, int DIR, class Lay, class Src, class Dst>
+__device__ __forceinline__ void stockham_chain(C* sm, const C* tw, const Src& src, const Dst& dst) {
     if constexpr (Ns < L) {
-        stockham_pass<C, L, Ns, NB, LS, NT, DIR>(sm, tw);
-        stockham_chain<C, L, Ns * pick_radix(L / Ns), NB, LS, NT, DIR>(sm, tw);
+        stockham_pass<C, L, Ns, NB, NT, DIR, Lay, Src, Dst>(sm, tw, src, dst);
+        stockham_chain<C, L, Ns * pick_radix(L / Ns, Ns == 1), NB, NT, DIR, Lay, Src, Dst>(sm, tw, src, dst);
     }
 }
 
-// Full transform of the tile; callers __syncthreads() before (data in place)
-// and may read the result right after.
+// Transform NB lines.  When the source is shared memory the caller must have
+// synchronised after filling it; when the destination is shared memory the
+// result may be read right after the call (the last pass ends in a barrier).
+// The twiddle table must be resident before the second pass (the first pass
+// uses none), so a caller may start filling it together with the first pass.
+template <class C, int L, int NB, int NT, int DIR, class Lay, class Src = SmemIO, class Dst = SmemIO>
+__device__ __forceinline__ void fft_tile(C* sm, const C* tw, const Src& src = Src(), const Dst& dst = Dst()) {
+    static_assert(smooth235(L), "FFT length must be a product of 2, 3 and 5");
+    stockham_chain<C, L, 1, NB, NT, DIR, Lay, Src, Dst>(sm, tw, src, dst);
+}
+
+// shared-memory to shared-memory transform with lines fastest (LS >= NB)
 template <class C, int L, int NB, int LS, int NT, int DIR>
 __device__ __forceinline__ void tile_fft(C* sm, const C* tw) {
-    static_assert(smooth235(L), "FFT length must be a product of 2, 3 and 5");
-    stockham_chain<C, L, 1, NB, LS, NT, DIR>(sm, tw);
+    fft_tile<C, L, NB, NT, DIR, Layout<LS, 1, true>>(sm, tw);
 }
 
 // copy the twiddle table for length L into shared memory

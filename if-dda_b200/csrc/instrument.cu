@@ -45,6 +45,8 @@ cudaEvent_t timing_before(int pass, int precision_bytes, cudaStream_t st) {
     return a;
 }
 
+bool timing_active() { return timing().pass != PASS_NONE; }
+
 void timing_after(cudaEvent_t start, cudaStream_t st) {
     if (!start) return;
     Timing& t = timing();

@@ -20,5 +20,7 @@ inline void count_launch(unsigned n = 1) { launch_counter().fetch_add(n, std::me
 // pass is not being timed); timing_after() records the matching end event
 cudaEvent_t timing_before(int pass, int precision_bytes, cudaStream_t st);
 void timing_after(cudaEvent_t start, cudaStream_t st);
+// true while a pass is selected for event timing
+bool timing_active();
 
 }  // namespace ifdda

@@ -198,13 +198,13 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
     int* status = W.status.p;
     KState* S = W.st.p;
     bool cancelled = false;
-    const int every = std::max(1, sp.check_every);
-    if (sp.method == 1) {
-        vec_launch<1>(GpStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
-        if (!sp.zero_guess) mv_solver<T>(G, sp, W, G_X, G_XR, status, st);
-        vec_launch<1>(GpInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
-        int tcur = G_TA, tnew = G_TB;
-        for (long it = 0;; it++) {
+    // poll at an even number of iterations so a two-iteration graph fits
+    const int every = std::max(2, (sp.check_every + 1) / 2 * 2);
+    const int methode = sp.method == 3 ? 2 : 1;
+    // one iteration; for GPBiCG `par` selects which t buffer is current
+    auto iteration = [&](int par) {
+        if (sp.method == 1) {
+            const int tcur = par ? G_TB : G_TA, tnew = par ? G_TA : G_TB;
             vec_launch<0>(GpP<T>{V, S}, n3, nblk, nrhs, rs, status, st);
             mv_solver<T>(G, sp, W, G_P, G_AP, status, st);
             vec_launch<1>(GpAlpha<T>{V, S}, n3, nblk, nrhs, rs, status, st);
@@ -212,19 +212,7 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
             mv_solver<T>(G, sp, W, tnew, G_AT, status, st);
             vec_launch<3>(GpZeta<T>{V, S, tnew}, n3, nblk, nrhs, rs, status, st);
             vec_launch<2>(GpUpdate<T>{V, S, tcur, tnew}, n3, nblk, nrhs, rs, status, st);
-            std::swap(tcur, tnew);
-            IFDDA_CUDA(cudaGetLastError());
-            if ((it + 1) % every == 0 || it < 2) {
-                if (poll(W, sp, st, cancelled)) break;
-            }
-            if (it > (long)sp.maxit + 4) break;
-        }
-    } else {
-        const int methode = sp.method == 2 ? 1 : 2;
-        vec_launch<1>(QStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
-        if (!sp.zero_guess) mv_solver<T>(G, sp, W, Q_X, Q_XR, status, st);
-        vec_launch<1>(QInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
-        for (long it = 0;; it++) {
+        } else {
             vec_launch<0>(QP<T>{V, S}, n3, nblk, nrhs, rs, status, st);
             mv_solver<T>(G, sp, W, Q_P, Q_V, status, st);
             vec_launch<1>(QAlpha<T>{V, S}, n3, nblk, nrhs, rs, status, st);
@@ -233,12 +221,64 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
             vec_launch<2>(QOmega<T>{V, S, methode}, n3, nblk, nrhs, rs, status, st);
             vec_launch<2>(QR<T>{V, S}, n3, nblk, nrhs, rs, status, st);
             vec_launch<1>(QX<T>{V, S}, n3, nblk, nrhs, rs, status, st);
-            IFDDA_CUDA(cudaGetLastError());
-            if ((it + 1) % every == 0 || it < 2) {
-                if (poll(W, sp, st, cancelled)) break;
-            }
-            if (it > (long)sp.maxit + 4) break;
         }
+        IFDDA_CUDA(cudaGetLastError());
+    };
+    if (sp.method == 1) {
+        vec_launch<1>(GpStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
+        if (!sp.zero_guess) mv_solver<T>(G, sp, W, G_X, G_XR, status, st);
+        vec_launch<1>(GpInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+    } else {
+        vec_launch<1>(QStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
+        if (!sp.zero_guess) mv_solver<T>(G, sp, W, Q_X, Q_XR, status, st);
+        vec_launch<1>(QInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+    }
+    // the first two iterations run as plain launches (they also set the
+    // kernels' shared-memory limits before any capture)
+    long it = 0;
+    bool done = false;
+    for (; it < 2 && !done; it++) {
+        iteration((int)(it & 1));
+        done = poll(W, sp, st, cancelled);
+    }
+    const bool graphs = sp.use_graphs && !timing_active();
+    if (!done && graphs) {
+        MvWork<T>& mw = G.work<T>();
+        mw.ensure(G.g, nrhs);
+        const std::vector<const void*> key = {
+            V.base, sp.alpha, sp.tabdip, G.gc<T>(), mw.B1.p, mw.B2.p, W.partials.p, W.tickets.p, status, S,
+            (const void*)(long)sp.method, (const void*)(long)nrhs, (const void*)n3, (const void*)(long)sp.amode,
+            (const void*)sp.nmax, (const void*)(long)nblk};
+        if (!W.graph.exec || W.graph.key != key) {
+            W.graph.reset();
+            const unsigned long long c0 = launch_counter().load();
+            cudaGraph_t graph;
+            IFDDA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            iteration(0);
+            iteration(1);
+            IFDDA_CUDA(cudaStreamEndCapture(st, &graph));
+            const unsigned long long nk = launch_counter().load() - c0;
+            launch_counter().fetch_sub(nk);  // captured, not run
+            const cudaError_t e = cudaGraphInstantiate(&W.graph.exec, graph, 0);
+            cudaGraphDestroy(graph);
+            IFDDA_CUDA(e);
+            W.graph.key = key;
+            W.graph.kernels = nk;
+        }
+    }
+    while (!done) {
+        for (int k = 0; k < every; k += 2) {
+            if (graphs && W.graph.exec) {
+                IFDDA_CUDA(cudaGraphLaunch(W.graph.exec, st));
+                count_launch((unsigned)W.graph.kernels);
+            } else {
+                iteration(0);
+                iteration(1);
+            }
+            it += 2;
+        }
+        done = poll(W, sp, st, cancelled);
+        if (it > (long)sp.maxit + 4) break;
     }
     return !cancelled;
 }

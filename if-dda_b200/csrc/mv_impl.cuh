@@ -19,10 +19,10 @@ template <class T, int L> void launch_fwd_x(const MvArgs<T>& a, int nrhs, bool t
     PassScope ps(PASS_FWD_X, TT::S, st);
     if (tab) {
         ensure_smem(k_fwd_x<T, L, true>, TT::smem_x);
-        k_fwd_x<T, L, true><<<grid, TT::NT, TT::smem_x, st>>>(a);
+        k_fwd_x<T, L, true><<<grid, TT::NTX, TT::smem_x, st>>>(a);
     } else {
         ensure_smem(k_fwd_x<T, L, false>, TT::smem_x);
-        k_fwd_x<T, L, false><<<grid, TT::NT, TT::smem_x, st>>>(a);
+        k_fwd_x<T, L, false><<<grid, TT::NTX, TT::smem_x, st>>>(a);
     }
 }
 
@@ -31,15 +31,15 @@ template <class T, int L, int DIR> void launch_pass_y(const MvArgs<T>& a, int nr
     dim3 grid((a.g.X + TT::TLY - 1) / TT::TLY, a.g.nz, 3 * nrhs);
     PassScope ps(DIR > 0 ? PASS_FWD_Y : PASS_INV_Y, TT::S, st);
     ensure_smem(k_pass_y<T, L, DIR>, TT::smem_y);
-    k_pass_y<T, L, DIR><<<grid, TT::NT, TT::smem_y, st>>>(a);
+    k_pass_y<T, L, DIR><<<grid, TT::NTY, TT::smem_y, st>>>(a);
 }
 
 template <class T, int L> void launch_zconv(const MvArgs<T>& a, int nrhs, cudaStream_t st) {
     using TT = MvTiles<T, L>;
-    dim3 grid((a.g.X + TT::TLZ - 1) / TT::TLZ, a.g.Y, nrhs);
+    dim3 grid((a.g.X + TT::TLZ - 1) / TT::TLZ, a.g.ny + 1, nrhs);
     PassScope ps(PASS_ZCONV, TT::S, st);
     ensure_smem(k_zconv<T, L>, TT::smem_z);
-    k_zconv<T, L><<<grid, TT::NT, TT::smem_z, st>>>(a);
+    k_zconv<T, L><<<grid, TT::NTZ, TT::smem_z, st>>>(a);
 }
 
 template <class T, int L, class Epi>
@@ -49,10 +49,10 @@ void launch_inv_x(const MvArgs<T>& a, const Epi& epi, int nrhs, bool tab, cudaSt
     PassScope ps(PASS_INV_X, TT::S, st);
     if (tab) {
         ensure_smem(k_inv_x<T, L, true, Epi>, TT::smem_x);
-        k_inv_x<T, L, true, Epi><<<grid, TT::NT, TT::smem_x, st>>>(a, epi);
+        k_inv_x<T, L, true, Epi><<<grid, TT::NTX, TT::smem_x, st>>>(a, epi);
     } else {
         ensure_smem(k_inv_x<T, L, false, Epi>, TT::smem_x);
-        k_inv_x<T, L, false, Epi><<<grid, TT::NT, TT::smem_x, st>>>(a, epi);
+        k_inv_x<T, L, false, Epi><<<grid, TT::NTX, TT::smem_x, st>>>(a, epi);
     }
 }
 

@@ -12,6 +12,7 @@ struct SolveSpec {
     double tol = 1e-4;
     int maxit = 10000;     // nlim of cdmlib/inverserigopt.f:30
     int check_every = 4;   // iterations launched between status polls
+    bool use_graphs = true;  // replay captured iterations instead of launching kernels
     int zero_guess = 0;    // x0 = 0 instead of x0 = b
     bool preset_state = false;
     const int* tabdip = nullptr;  // device, lattice -> 1-based dipole, or null (full box)
@@ -35,7 +36,23 @@ struct SolveResult {
     int outer = 0;      // refinement steps (mixed)
 };
 
+// Two Krylov iterations captured as one CUDA graph (the t buffers alternate,
+// so two iterations bring the pointers back), reused while every pointer and
+// size baked into its kernel arguments stays the same.
+struct IterGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<const void*> key;
+    unsigned long long kernels = 0;  // kernel launches per replay
+    void reset() {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+        key.clear();
+    }
+    ~IterGraph() { reset(); }
+};
+
 template <class T> struct KrylovWork {
+    IterGraph graph;
     DevBuf<cplx<T>> vecs;
     DevBuf<KState> st;
     DevBuf<int> status, zstatus;
