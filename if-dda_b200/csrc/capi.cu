@@ -7,26 +7,7 @@
 
 using namespace ifdda;
 
-struct ifdda_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::string last_error;
-    DevBuf<int> flag;  // device error flag for post kernels
-    DevBuf<double2> partials;
-    DevBuf<unsigned> tickets;
-    DevBuf<KState> st;
-    DevBuf<int> zstatus;
-};
-
-struct ifdda_green {
-    ifdda_ctx* ctx = nullptr;
-    Green G;
-    SolverWork SW;
-    // per-call device copies
-    DevBuf<int> tab;
-    DevBuf<double2> alpha, ff0, x, ffx, ffb;
-    DevBuf<float2> ffx32, ffb32, alpha32;
-};
+#include "capi_types.cuh"
 
 static void set_info(char* infostr, const char* msg) {
     if (!infostr) return;

@@ -1,0 +1,27 @@
+// Definitions of the opaque C-ABI handles, shared by the translation units
+// that implement entry points.
+#pragma once
+#include <string>
+#include "../../include/ifdda_gpu.h"
+#include "post.cuh"
+
+struct ifdda_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    ifdda::DevBuf<int> flag;  // device error flag for post kernels
+    ifdda::DevBuf<double2> partials;
+    ifdda::DevBuf<unsigned> tickets;
+    ifdda::DevBuf<ifdda::KState> st;
+    ifdda::DevBuf<int> zstatus;
+};
+
+struct ifdda_green {
+    ifdda_ctx* ctx = nullptr;
+    ifdda::Green G;
+    ifdda::SolverWork SW;
+    // per-call device copies
+    ifdda::DevBuf<int> tab;
+    ifdda::DevBuf<double2> alpha, ff0, x, ffx, ffb;
+    ifdda::DevBuf<float2> ffx32, ffb32, alpha32;
+};
