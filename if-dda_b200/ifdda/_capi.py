@@ -46,6 +46,7 @@ SIGNATURES = {
     "ifdda_green_export": (C.c_int, [_vp] + [_vp] * 6),
     "ifdda_matvec": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, _vp]),
     "ifdda_matvec_device": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp]),
+    "ifdda_matvec_noalloc": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, _vp]),
     "ifdda_inverserig": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, _vp, C.c_char_p, C.c_double, _vp, _vp, _dp,
                                    _ip, _ip, _ip, C.c_char_p, C.POINTER(SolveOptions)]),
     "ifdda_inverserig_batch": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, C.c_char_p, C.c_double,

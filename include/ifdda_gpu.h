@@ -76,6 +76,24 @@ int ifdda_matvec(ifdda_green* g, int precision, int ndip, const int* tabdip, con
 int ifdda_matvec_device(ifdda_green* g, int precision, int nrhs, int ndip, const int* tabdip_dev,
                         const void* FFX_dev, void* FFB_dev);
 
+/* Same operation as ifdda_matvec_device for one right-hand side, for callers
+   that cannot allocate device memory while they run: a real-time loop that
+   must avoid the device-wide synchronisation of cudaMalloc/cudaFree, a
+   framework whose own caching allocator owns the GPU memory, or code running
+   under CUDA stream capture.  It has no counterpart in the reference (whose
+   buffers are static Fortran arrays).  The mat-vec scratch lives in one fixed
+   16 MiB device array inside the library (held by every GPU that loads it
+   until the process exits), so 18*nx*ny*nz complex values of the chosen
+   precision must fit in 16 MiB (e.g. 32^3 sites fit in FP64 and 40^3 in FP32,
+   48^3 does not fit in FP64);
+   larger grids return 1 with the reason in ifdda_ctx_last_error.  The first
+   call on a device looks up the array's device address; make that first call
+   before any stream capture.  All calls share the array: calls whose kernels
+   overlap on the GPU race.  The spectrum comes from ifdda_green_create, made
+   beforehand. */
+int ifdda_matvec_noalloc(ifdda_green* g, int precision, int ndip, const int* tabdip_dev, const void* FFX_dev,
+                         void* FFB_dev);
+
 /* Rigorous solve.  Replaces inverserigopt (cdmlib/inverserigopt.f:1-1085,
    tabdip == NULL) and inverserig (cdmlib/inverserig.f:1-1090, tabdip != NULL),
    called at cdmlib/cdmlib.f:1565-1581: initial guess FF0, methodeit
