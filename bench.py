@@ -1,19 +1,22 @@
 """Benchmark: solves/s of the FFT-accelerated dipole solve on one B200.
 
-Workload (one step = one complete rigorous solve):
+Default workload (one step = one complete rigorous solve):
   inhomogeneous cube 64x64x64 (262,144 dipoles), d = 10 nm, lambda 632.8 nm,
   permittivity from the seeded Gaussian random field (mean 2.25, std 0.1,
   lc = 50 nm, SUNIF seed 4*7+1), plane wave theta = 20 deg p-polarised, RR
   polarisability, FFT grid 128^3, GPBICG1 to true residual 1e-4, solved with
   the FP32 mat-vec / inner Krylov inside FP64 iterative refinement
   (headline `value`), next to the plain FP64 drop-in (`fp64` block).
-Inputs (FF0, polarisability) are resident in HBM for `value`; `e2e` runs the
-same solve through the C-ABI (ifdda_inverserig) with pinned host buffers and
-the host<->device copies inside the timed region.  L2 is flushed (256 MiB
-write) before every timed step.  `--impl reference` times the CPU
-restatement of the reference path (oracle, all host threads) on the same
-workload.  With torchrun, every rank solves its own copy (replicas, weak
-scaling); times are the max over ranks.
+Other workloads (--workload): c1 (sphere 16^3, inside-only dipoles), c3
+(128 plane waves on a 96x96x64 ellipsoid lattice, one batched solve per
+step), c5 (192^3 concentric spheres, QMR-BiCGSTAB), c4 (request stream
+through the continuous-batching server).
+Inputs are resident in HBM for `value`; `e2e` runs the same solve through the
+C-ABI (ifdda_inverserig) with pinned host inputs and the host<->device copies
+inside the timed region.  L2 is flushed (256 MiB write) before every timed
+step.  `--impl reference` times the CPU restatement of the reference path
+(oracle, all host threads) on the same workload.  With torchrun, every rank
+solves its own copy (replicas, weak scaling); times are the max over ranks.
 """
 import argparse
 import json
@@ -24,6 +27,7 @@ import subprocess
 import sys
 import threading
 import time
+from dataclasses import dataclass, field
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "if-dda_b200"))
@@ -31,21 +35,85 @@ sys.path.insert(0, os.path.join(ROOT, "if-dda_b200"))
 import numpy as np  # noqa: E402
 
 METRIC = "solves/s & p99 latency, mixed vs FP64 at rel. residual 1e-4; matvec HBM GB/s"
-WORKLOAD = ("C2 inhomogeneous GRF cube 64^3 (262,144 dipoles), d=10 nm, lambda=632.8 nm, "
-            "theta=20 deg p-pol, RR, GPBICG1 to true residual 1e-4, FFT grid 128^3")
-LAMBDA = 632.8e-9
-N_EDGE = 64
 TOL = 1e-4
 
 
-def build_object():
+# ----------------------------------------------------------------- workloads --
+@dataclass
+class Workload:
+    key: str
+    desc: str
+    ob: object
+    k0: float
+    E0: float
+    beams: list            # [(beam, a1, a2, pp)] one per right-hand side
+    method: str
+    fp64_nrhs: int         # right-hand sides solved for the FP64 comparison
+    cpu_mv: int = 4        # oracle mat-vecs timed for the CPU baseline
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def nrhs(self):
+        return len(self.beams)
+
+
+def wl_c1():
     from ifdda import objects
-    k0 = 2 * math.pi / LAMBDA
-    ob = objects.inhomocuboid(N_EDGE, N_EDGE, N_EDGE, 10e-9, 2.25 + 0j, 50e-9, 0.1, 7, k0, "RR")
-    E0, _ = objects.irradiance(1.0, 10 * LAMBDA)
-    return ob, k0, E0
+    lam = 632.8e-9
+    k0 = 2 * math.pi / lam
+    ob = objects.sphere(100e-9, 2.25 + 0j, 16, k0, "RR", na=-1)
+    E0, _ = objects.irradiance(1.0, 10 * lam)
+    return Workload("c1", "C1 sphere eps 2.25, R=100 nm, 16^3 lattice, 2176 dipoles inside, lambda=632.8 nm, "
+                    "normal incidence x-pol, RR, GPBICG1 to 1e-4, FFT grid 32^3", ob, k0, E0,
+                    [(0, 0.0, 0.0, 1.0)], "GPBICG1", 1)
 
 
+def wl_c2():
+    from ifdda import objects
+    lam = 632.8e-9
+    k0 = 2 * math.pi / lam
+    ob = objects.inhomocuboid(64, 64, 64, 10e-9, 2.25 + 0j, 50e-9, 0.1, 7, k0, "RR")
+    E0, _ = objects.irradiance(1.0, 10 * lam)
+    return Workload("c2", "C2 inhomogeneous GRF cube 64^3 (262,144 dipoles), d=10 nm, lambda=632.8 nm, "
+                    "theta=20 deg p-pol, RR, GPBICG1 to true residual 1e-4, FFT grid 128^3", ob, k0, E0,
+                    [(0, 20.0, 0.0, 1.0)], "GPBICG1", 1)
+
+
+def wl_c3(nrhs_pairs=64):
+    from ifdda import objects
+    lam = 500e-9
+    k0 = 2 * math.pi / lam
+    ob = objects.ellipsoid_lattice(96, 96, 64, 10e-9, 400e-9, 300e-9, 200e-9, 2.0, 2.6, 33, k0, "RR")
+    E0, _ = objects.irradiance(1.0, 10 * lam)
+    rng = np.random.Generator(np.random.PCG64(3))
+    r = 0.9 * k0 * np.sqrt(rng.uniform(0, 1, nrhs_pairs))
+    t = rng.uniform(0, 2 * np.pi, nrhs_pairs)
+    beams = []
+    for kx, ky in zip(r * np.cos(t), r * np.sin(t)):
+        beams.append((1, float(kx), float(ky), 0.0))  # s
+        beams.append((1, float(kx), float(ky), 1.0))  # p
+    return Workload("c3", f"C3 batched brightfield sweep: ellipsoid 400/300/200 nm on a 96x96x64 lattice, d=10 nm, "
+                    f"eps U[2.0,2.6] (seed 33), lambda=500 nm, {len(beams)} plane waves ({nrhs_pairs} (kx,ky) on the "
+                    f"NA 0.9 disk, seed 3, x s/p) in one batched solve, GPBICG1 to 1e-4, FFT grid 192x192x128",
+                    ob, k0, E0, beams, "GPBICG1", 8, cpu_mv=2)
+
+
+def wl_c5():
+    from ifdda import objects
+    lam = 632.8e-9
+    k0 = 2 * math.pi / lam
+    ob = objects.concentric([0.9e-6, 1.9e-6], [3.0 + 0.01j, 2.0 + 0j], 192, k0, "RR", na=0)
+    E0, _ = objects.irradiance(1.0, 10 * lam)
+    return Workload("c5", "C5 concentric spheres (core eps 3+0.01i r=0.9 um, shell eps 2 r=1.9 um) on the full "
+                    "192^3 lattice (7.08M dipoles, d = 2 r_out/192 = 19.79 nm as the reference sizes it), "
+                    "lambda=632.8 nm, normal incidence, QMR-BiCGSTAB1 to 1e-4, FFT grid 384^3", ob, k0, E0,
+                    [(0, 0.0, 0.0, 1.0)], "QMRBICGSTAB1", 1, cpu_mv=1)
+
+
+WORKLOADS = {"c1": wl_c1, "c2": wl_c2, "c3": wl_c3, "c5": wl_c5}
+
+
+# ------------------------------------------------------------------ helpers --
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -54,9 +122,9 @@ def measured_peaks():
     return 6650.0, "fallback 6.65 TB/s"
 
 
-def profile_traffic():
+def profile_traffic(key):
     """dram bytes per zconv launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "zconv_c2_fp32.md")
+    p = os.path.join(ROOT, "profiles", f"zconv_{key}_fp32.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -146,48 +214,56 @@ def barrier(ws):
 
 
 # ----------------------------------------------------------------- CPU arm --
-def cpu_oracle_sample(ob, k0, E0, ncompte_full, n_mv=4):
+def cpu_oracle_sample(w: Workload, ncompte_full: int, n_mv=None):
     """Times the oracle (C restatement of the reference path, FP64, OpenMP on
-    every host thread): the Green spectrum once, then GPBICG1 stopped after
-    n_mv mat-vecs; a full solve is extrapolated with the solve's mat-vec
-    count.  Returns (solves/s, seconds sampled, cores, sample string)."""
+    every host thread) on one right-hand side of the workload: the Green
+    spectrum once, then the solve stopped after n_mv mat-vecs; a full solve is
+    extrapolated with the solve's mat-vec count.  Returns (solves/s for one
+    right-hand side, cores, sample string)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
+    n_mv = n_mv or w.cpu_mv
     cores = os.cpu_count() or 1
     oracle.set_threads(cores)
-    n = ob.nx
+    ob = w.ob
     t0 = time.perf_counter()
-    G = oracle.greencalculfft(n, n, n, ob.aretecube, k0)
+    G = oracle.greencalculfft(ob.nx, ob.ny, ob.nz, ob.aretecube, w.k0)
     t_green = time.perf_counter() - t0
-    ff0 = oracle.incident(ob.xs, ob.ys, ob.zs, k0, E0, 1.0, 0, 20.0, 0.0)
+    bm, a1, a2, pp = w.beams[0]
+    ff0 = oracle.incident(ob.xs, ob.ys, ob.zs, w.k0, w.E0, pp, bm, a1, a2)
     t0 = time.perf_counter()
-    oracle.inverserig(G, n, n, n, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", TOL, max_matvecs=n_mv)
+    oracle.inverserig(G, ob.nx, ob.ny, ob.nz, ob.nbsphere, ob.polarisa, ob.nmax, ff0, w.method, TOL,
+                      tabdip=ob.tabdip_or_none, max_matvecs=n_mv)
     t_mv = (time.perf_counter() - t0) / n_mv
+    del G
     t_solve = t_green + t_mv * ncompte_full
-    sample = (f"oracle FP64 on {cores} host threads: greencalculfft 128^3 ({t_green:.2f} s) + GPBICG1 stopped "
-              f"after {n_mv} mat-vecs ({t_mv:.3f} s/mat-vec incl. Krylov vector work); full solve "
-              f"extrapolated to ncompte={ncompte_full} mat-vecs = {t_solve:.1f} s")
-    return 1.0 / t_solve, t_green + t_mv * n_mv, cores, sample
+    sample = (f"oracle FP64 on {cores} host threads, one right-hand side of {w.key}: greencalculfft "
+              f"({t_green:.2f} s) + {w.method} stopped after {n_mv} mat-vecs ({t_mv:.3f} s/mat-vec incl. Krylov "
+              f"vector work); full solve extrapolated to ncompte={ncompte_full} mat-vecs = {t_solve:.1f} s")
+    return 1.0 / t_solve, cores, sample
+
+
+# number of mat-vecs of the FP64 GPBICG1 / QMR solve of each workload, the
+# same for the oracle and the GPU drop-in (tests check the equality)
+NCOMPTE_FP64 = {"c1": 8, "c2": 34}
 
 
 def run_reference(args):
     ws, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    ob, k0, E0 = build_object()
-    # GPBICG1 on this workload needs 34 mat-vecs (16 iterations) in FP64, the
-    # same count for the oracle and the GPU drop-in
-    ncompte = 34
+    w = WORKLOADS[args.workload]()
+    ncompte = NCOMPTE_FP64.get(w.key, 40)
     vals = []
     for i in range(args.warmup + args.steps):
-        v, secs, cores, sample = cpu_oracle_sample(ob, k0, E0, ncompte, n_mv=2)
+        v, cores, sample = cpu_oracle_sample(w, ncompte, n_mv=2)
         if i >= args.warmup:
             vals.append(v)
     value = statistics.mean(vals)
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded GRF, ng=7)", "impl": "reference",
-            "config": {"workload": WORKLOAD, "precision": "fp64", "parallelism": "cpu"},
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": w.desc, "precision": "fp64", "parallelism": "cpu"},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -208,33 +284,36 @@ def run_gpu(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = torch.device("cuda", local)
-    ob, k0, E0 = build_object()
+    w = WORKLOADS[args.workload]()
+    ob, k0, E0 = w.ob, w.k0, w.E0
     ctx = ifdda.Context(local)
     lib = ctx.lib
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
     t0 = time.perf_counter()
     g = ctx.green(ob.nx, ob.ny, ob.nz, ob.aretecube, k0)
     green_ms = (time.perf_counter() - t0) * 1e3
-    ff0_h = ctx.planewaves(ob.xs, ob.ys, ob.zs, k0, E0, [0], [20.0], [0.0], [1.0])[0]
-    nb, nmax = ob.nbsphere, ob.nmax
+    ff0_h = ctx.planewaves(ob.xs, ob.ys, ob.zs, k0, E0, [b[0] for b in w.beams], [b[1] for b in w.beams],
+                           [b[2] for b in w.beams], [b[3] for b in w.beams])
+    nb, nmax, nrhs = ob.nbsphere, ob.nmax, w.nrhs
     pol_h = ob.polarisa
     ff0_d = torch.from_numpy(ff0_h).to(dev)
     pol_d = torch.from_numpy(pol_h).to(dev)
+    tab_d = torch.from_numpy(ob.tabdip).to(dev) if ob.inside_only else None
     ff_d = torch.empty_like(ff0_d)
     loc_d = torch.empty_like(ff0_d)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
     torch.cuda.synchronize()
 
-    def solve_dev(prec):
-        r = g.inverserig_device(1, nb, nmax, None, pol_d.data_ptr(), ff0_d.data_ptr(), ff_d.data_ptr(),
-                                loc_d.data_ptr(), "GPBICG1", TOL, precision=prec)
+    def solve_dev(prec, k=nrhs):
+        r = g.inverserig_device(k, nb, nmax, tab_d.data_ptr() if tab_d is not None else None, pol_d.data_ptr(),
+                                ff0_d.data_ptr(), ff_d.data_ptr(), loc_d.data_ptr(), w.method, TOL, precision=prec)
         if r["nstop"] != 0:
             raise RuntimeError(f"solve failed: {r['infostr'].strip()}")
         return r
 
-    def timed(prec, steps, warmup, count_launches=False):
+    def timed(prec, steps, warmup, k=nrhs):
         for _ in range(warmup):
-            solve_dev(prec)
+            solve_dev(prec, k)
         torch.cuda.synchronize()
         barrier(ws)
         torch.cuda.synchronize()
@@ -246,7 +325,7 @@ def run_gpu(args):
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
-            infos.append(solve_dev(prec))
+            infos.append(solve_dev(prec, k))
             with torch.cuda.stream(stream):
                 e1.record(stream)
             e1.synchronize()
@@ -262,21 +341,23 @@ def run_gpu(args):
     # the dominant kernel (zconv, FP32) bracketed by CUDA events on the
     # solver's stream during further complete solves (plain launches)
     lib.ifdda_timing_enable(_capi.PASS_ZCONV, _capi.IFDDA_FP32)
-    timed(IFDDA_MIXED, max(3, min(args.steps, 10)), 0)
+    timed(IFDDA_MIXED, max(1, min(args.steps, 5)), 0)
     nl, tot = C.c_int(0), C.c_double(0)
     lib.ifdda_timing_read(C.byref(nl), C.byref(tot))
     lib.ifdda_timing_enable(0, -1)
     zconv_ms = tot.value / max(nl.value, 1)
+    g.release_workspace()
 
     fp64_steps = max(1, min(args.steps, 5))
-    t_fp64, info_fp64, _ = timed(IFDDA_FP64, fp64_steps, min(args.warmup, 3))
+    t_fp64, info_fp64, _ = timed(IFDDA_FP64, fp64_steps, min(args.warmup, 2), k=w.fp64_nrhs)
+    g.release_workspace()
 
     total_ms = max_over_ranks(sum(t_mixed), ws, dev)
-    value = ws * args.steps / (total_ms / 1e3)
+    value = ws * args.steps * nrhs / (total_ms / 1e3)
     fp64_total = max_over_ranks(sum(t_fp64), ws, dev)
-    fp64_value = ws * fp64_steps / (fp64_total / 1e3)
+    fp64_value = ws * fp64_steps * w.fp64_nrhs / (fp64_total / 1e3)
 
-    # mat-vec throughput (whole mat-vec, algorithmic bytes) at both precisions
+    # mat-vec throughput (whole mat-vec, algorithmic bytes, one right-hand side)
     N = ob.nx * ob.ny * ob.nz
     Np = (ob.nx + 1) * (ob.ny + 1) * (ob.nz + 1)
     M = 8 * N
@@ -301,33 +382,40 @@ def run_gpu(args):
         balg = s * (7 * N + 6 * Np + 6 * M)
         mv["fp32" if prec == 2 else "fp64"] = {"ms": round(ms, 4), "alg_bytes": balg,
                                                 "GB_s": round(balg / ms / 1e6, 1)}
+        del x, b
+    g.release_workspace()
 
-    # end to end through the C-ABI with pinned host buffers
-    ff0_pin = torch.from_numpy(ff0_h).pin_memory()
-    pol_pin = torch.from_numpy(pol_h).pin_memory()
-    e2e_steps = max(1, min(args.steps, 5))
-    g.inverserig(nb, pol_pin.numpy(), nmax, ff0_pin.numpy(), "GPBICG1", TOL, precision=IFDDA_MIXED)
-    barrier(ws)
-    te = []
-    for _ in range(e2e_steps):
-        t0 = time.perf_counter()
-        r = g.inverserig(nb, pol_pin.numpy(), nmax, ff0_pin.numpy(), "GPBICG1", TOL, precision=IFDDA_MIXED)
-        te.append(time.perf_counter() - t0)
-        if r.nstop != 0:
-            raise RuntimeError(r.infostr)
-    e2e_total = max_over_ranks(sum(te), ws, dev)
-    e2e_value = ws * e2e_steps / e2e_total
-    h2d = ff0_h.nbytes + nb * 16  # FF0 + the compact isotropic polarisability
-    d2h = 2 * ff0_h.nbytes        # FF and FFloc
+    # end to end through the C-ABI with pinned host inputs
+    e2e_value, h2d, d2h = None, 0, 0
+    if not args.no_e2e:
+        ff0_pin = torch.from_numpy(ff0_h).pin_memory()
+        pol_pin = torch.from_numpy(pol_h).pin_memory()
+        e2e_steps = max(1, min(args.steps, 5 if nrhs == 1 else 2))
+        tab_h = ob.tabdip_or_none
+        g.inverserig(nb, pol_pin.numpy(), nmax, ff0_pin.numpy(), w.method, TOL, tabdip=tab_h, precision=IFDDA_MIXED)
+        barrier(ws)
+        te = []
+        for _ in range(e2e_steps):
+            t0 = time.perf_counter()
+            r = g.inverserig(nb, pol_pin.numpy(), nmax, ff0_pin.numpy(), w.method, TOL, tabdip=tab_h,
+                             precision=IFDDA_MIXED)
+            te.append(time.perf_counter() - t0)
+            if r.nstop != 0:
+                raise RuntimeError(r.infostr)
+        e2e_total = max_over_ranks(sum(te), ws, dev)
+        e2e_value = ws * e2e_steps * nrhs / e2e_total
+        h2d = ff0_h.nbytes + nb * 16 + (ob.tabdip.nbytes if ob.inside_only else 0)  # FF0, compact alpha, Tabdip
+        d2h = 2 * ff0_h.nbytes  # FF and FFloc
+        g.release_workspace()
 
     peak, peak_src = measured_peaks()
-    zc_bytes = 8 * (2 * 3 * ob.nz * (2 * ob.ny) * (2 * ob.nx) + 6 * Np)
+    Z, Y, X = 2 * ob.nz, 2 * ob.ny, 2 * ob.nx
+    zc_bytes = 8 * (2 * 3 * ob.nz * Y * X * nrhs + 6 * Np)
     achieved = zc_bytes / (zconv_ms * 1e6) if zconv_ms > 0 else None
-    traffic = profile_traffic()
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         ncompte64 = int(info_fp64[0]["ncompte"][0])
-        v, secs, cores, sample = cpu_oracle_sample(ob, k0, E0, ncompte64)
+        v, cores, sample = cpu_oracle_sample(w, ncompte64)
         cpu = {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample}
 
     lat = sorted(t_mixed)
@@ -338,19 +426,20 @@ def run_gpu(args):
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c64 inner / c128 outer", "data": "synthetic (seeded GRF, ng=7)",
-        "config": {"workload": WORKLOAD, "precision": "mixed FP32/FP64 refinement", "l2": "flushed before each step",
-                   "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+        "vs_baseline": None, "dtype": "c64 inner / c128 outer", "data": "synthetic (seeded)",
+        "config": {"workload": w.desc, "nrhs_per_step": nrhs, "precision": "mixed FP32/FP64 refinement",
+                   "l2": "flushed before each step", "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
         "latency_ms": {"p50": p50, "p99": p99},
-        "mixed": {"solves_s": value, "nloop": int(im["nloop"][0]), "ncompte": int(im["ncompte"][0]),
-                  "tol1": float(im["tol1"][0])},
-        "fp64": {"solves_s": fp64_value, "ms_per_solve": fp64_total / fp64_steps, "nloop": int(i64["nloop"][0]),
-                 "ncompte": int(i64["ncompte"][0]), "tol1": float(i64["tol1"][0])},
+        "mixed": {"solves_s": value, "nloop_max": int(np.max(im["nloop"])), "ncompte_max": int(np.max(im["ncompte"])),
+                  "tol1_max": float(np.max(im["tol1"]))},
+        "fp64": {"solves_s": fp64_value, "nrhs": w.fp64_nrhs, "ms_per_solve": fp64_total / fp64_steps,
+                 "nloop_max": int(np.max(i64["nloop"])), "ncompte_max": int(np.max(i64["ncompte"])),
+                 "tol1_max": float(np.max(i64["tol1"]))},
         "matvec": mv,
         "green_build_ms": green_ms,
-        "roofline": {"bound": "hbm", "kernel": "k_zconv<float,128> (z FFT + 3x3 spectrum multiply + inverse z FFT)",
+        "roofline": {"bound": "hbm", "kernel": f"k_zconv<float,{Z}> (z FFT + 3x3 spectrum multiply + inverse z FFT)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "frac": (achieved / peak) if achieved else None, "traffic": profile_traffic(w.key),
                      "alg_bytes_per_launch": zc_bytes, "avg_launch_ms": zconv_ms, "launches_timed": nl.value,
                      "peak_source": peak_src},
         "cpu_baseline": cpu,
@@ -368,16 +457,60 @@ def run_gpu(args):
     return 0
 
 
+def run_serving(args):
+    """Config 4: a seeded request stream through the continuous-batching
+    server, mixed precision then plain FP64 on the same stream."""
+    import torch
+    from ifdda import IFDDA_FP64, IFDDA_MIXED
+    from ifdda import serve
+
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    reqs = serve.make_stream(args.requests, args.rate, seed=4)
+    out = {}
+    for name, prec in (("mixed", IFDDA_MIXED), ("fp64", IFDDA_FP64)):
+        srv = serve.Server(slots=args.slots, device=local, precision=prec)
+        # warm-up: one request per lattice size compiles nothing but fills caches
+        srv.run(reqs[:args.slots], realtime=False)
+        t0 = time.perf_counter()
+        res = srv.run(reqs, realtime=True)
+        wall = time.perf_counter() - t0
+        srv.close()
+        out[name] = serve.latency_stats(res, wall)
+        out[name]["wall_s"] = wall
+    desc = (f"C4 serving stream: {args.requests} requests, Poisson arrivals at {args.rate}/s (seed 4), sphere or "
+            f"cube, edge in {{16..96}}, d=10 nm, eps' U[1.5,4] eps'' U[0,0.5], lambda U[400,800] nm, 1-32 "
+            f"incidences on the NA 0.9 disk, GPBICG1 to 1e-4, {args.slots} concurrent slots, HBM-budget admission")
+    m = out["mixed"]
+    line = {"metric": METRIC, "value": m["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": args.requests,
+            "warmup": args.slots, "ms_per_step": m["wall_s"] * 1e3 / args.requests, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64 inner / c128 outer", "data": "synthetic (seeded)",
+            "config": {"workload": desc, "parallelism": "single GPU"},
+            "latency_ms": {"p50": m["p50_ms"], "p99": m["p99_ms"]}, "serving": out}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ifdda", choices=["ifdda", "reference"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) measurement")
+    ap.add_argument("--requests", type=int, default=2000, help="c4: stream length")
+    ap.add_argument("--rate", type=float, default=100.0, help="c4: Poisson arrival rate (requests/s)")
+    ap.add_argument("--slots", type=int, default=4, help="c4: concurrent solver slots")
     args = ap.parse_args()
     if args.impl == "reference":
+        if args.workload == "c4":
+            args.workload = "c2"
         return run_reference(args)
+    if args.workload == "c4":
+        return run_serving(args)
     return run_gpu(args)
 
 

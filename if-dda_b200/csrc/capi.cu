@@ -90,6 +90,7 @@ SolveSpec make_spec(int method, int nrhs, int nb, double tol, const ifdda_solve_
         if (opt->check_every > 0) sp.check_every = opt->check_every;
         if (opt->max_outer > 0) sp.max_outer = opt->max_outer;
         if (opt->inner_floor > 0) sp.inner_floor = opt->inner_floor;
+        if (opt->maxit > 0) sp.maxit = opt->maxit;
     }
     return sp;
 }
@@ -105,10 +106,15 @@ int solve_device(ifdda_green* g, int nrhs, int nb, int nmax, const int* tab_dev,
         set_info(infostr, "Iterative method not correct!");
         return 1;
     }
-    if (tol < 1e-12 || tol > 0.5) {
-        // cdmlib/cdmlib.f:462-471 rejects tolerances outside this range
+    // cdmlib/cdmlib.f:462-471 rejects tolerances outside [1e-12, 0.5]
+    if (tol < 1e-12) {
         if (nstop) *nstop = 1;
-        set_info(infostr, "Tolerance out of range [1e-12, 0.5]");
+        set_info(infostr, "Tolerance for the iterative method too small!");
+        return 1;
+    }
+    if (tol > 0.5) {
+        if (nstop) *nstop = 1;
+        set_info(infostr, "Tolerance  for the iterative method too large!");
         return 1;
     }
     SolveSpec sp = make_spec(method, nrhs, nb, tol, opt);
@@ -168,6 +174,13 @@ int ifdda_ctx_create(int device, ifdda_ctx** out) {
         c->device = device;
         DeviceScope ds(device);
         IFDDA_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        AllocStreamScope as(c->stream);
+        // keep freed blocks in the device's memory pool: re-allocating a
+        // workspace then costs neither a cudaMalloc nor a device synchronisation
+        cudaMemPool_t pool;
+        IFDDA_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t keep = UINT64_MAX;
+        IFDDA_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
         c->flag.ensure(1);
         c->st.ensure(1);
         c->zstatus.ensure(1);
@@ -187,12 +200,18 @@ int ifdda_ctx_destroy(ifdda_ctx* ctx) {
     if (!ctx) return 0;
     {
         DeviceScope ds(ctx->device);
-        if (ctx->stream) cudaStreamDestroy(ctx->stream);
-        ctx->flag.release();
-        ctx->partials.release();
-        ctx->tickets.release();
-        ctx->st.release();
-        ctx->zstatus.release();
+        {
+            AllocStreamScope as(ctx->stream);
+            ctx->flag.release();
+            ctx->partials.release();
+            ctx->tickets.release();
+            ctx->st.release();
+            ctx->zstatus.release();
+        }
+        if (ctx->stream) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaStreamDestroy(ctx->stream);
+        }
     }
     delete ctx;
     return 0;
@@ -203,6 +222,7 @@ const char* ifdda_ctx_last_error(const ifdda_ctx* ctx) { return ctx ? ctx->last_
 int ifdda_ctx_synchronize(ifdda_ctx* ctx) {
     IFDDA_GUARD_BEGIN
     DeviceScope ds(ctx->device);
+    AllocStreamScope as(ctx->stream);
     IFDDA_CUDA(cudaStreamSynchronize(ctx->stream));
     return 0;
     IFDDA_GUARD_END(ctx, nullptr)
@@ -217,6 +237,7 @@ int ifdda_green_create(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube,
     g->ctx = ctx;
     IFDDA_GUARD_BEGIN
     DeviceScope ds(ctx->device);
+    AllocStreamScope as(ctx->stream);
     green_build(g->G, nx, ny, nz, aretecube, k0, ctx->stream);
     *out = g.release();
     return 0;
@@ -227,10 +248,37 @@ int ifdda_green_destroy(ifdda_green* g) {
     if (!g) return 0;
     {
         DeviceScope ds(g->ctx->device);
+        AllocStreamScope as(g->ctx->stream);
         cudaStreamSynchronize(g->ctx->stream);
         delete g;
     }
     return 0;
+}
+
+int ifdda_green_release_workspace(ifdda_green* g) {
+    if (!g) return 1;
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(g->ctx->device);
+    AllocStreamScope as(g->ctx->stream);
+    IFDDA_CUDA(cudaStreamSynchronize(g->ctx->stream));
+    g->SW.kw64.release();
+    g->SW.kw32.release();
+    g->SW.mixed.release();
+    g->G.w32.B1.release();
+    g->G.w32.B2.release();
+    g->G.w64.B1.release();
+    g->G.w64.B2.release();
+    g->alpha.release();
+    g->ff0.release();
+    g->x.release();
+    g->ffx.release();
+    g->ffb.release();
+    g->ffx32.release();
+    g->ffb32.release();
+    g->alpha32.release();
+    g->tab.release();
+    return 0;
+    IFDDA_GUARD_END(g->ctx, nullptr)
 }
 
 int ifdda_green_export(ifdda_green* g, ifdda_dcmplx* xx, ifdda_dcmplx* xy, ifdda_dcmplx* xz, ifdda_dcmplx* yy,
@@ -238,6 +286,7 @@ int ifdda_green_export(ifdda_green* g, ifdda_dcmplx* xx, ifdda_dcmplx* xy, ifdda
     if (!g) return 1;
     IFDDA_GUARD_BEGIN
     DeviceScope ds(g->ctx->device);
+    AllocStreamScope as(g->ctx->stream);
     double2* out[6] = {(double2*)xx, (double2*)xy, (double2*)xz, (double2*)yy, (double2*)yz, (double2*)zz};
     green_export(g->G, out, g->ctx->stream);
     return 0;
@@ -249,6 +298,7 @@ int ifdda_matvec(ifdda_green* g, int precision, int ndip, const int* tabdip, con
     if (!g || !FFX || !FFB) return 1;
     IFDDA_GUARD_BEGIN
     DeviceScope ds(g->ctx->device);
+    AllocStreamScope as(g->ctx->stream);
     cudaStream_t st = g->ctx->stream;
     const MvGeom& geo = g->G.g;
     if (!tabdip && ndip != geo.N) throw EngineError{1, "ifdda_matvec: ndip must be nx*ny*nz without tabdip"};
@@ -292,6 +342,7 @@ int ifdda_matvec_device(ifdda_green* g, int precision, int nrhs, int ndip, const
     if (!g || !FFX_dev || !FFB_dev || nrhs < 1 || ndip < 1) return 1;
     IFDDA_GUARD_BEGIN
     DeviceScope ds(g->ctx->device);
+    AllocStreamScope as(g->ctx->stream);
     cudaStream_t st = g->ctx->stream;
     if (!tabdip_dev && ndip != g->G.g.N) throw EngineError{1, "ifdda_matvec_device: ndip must be nx*ny*nz"};
     const long n3 = 3L * ndip;
@@ -321,6 +372,7 @@ int ifdda_inverserig_batch(ifdda_green* g, int nrhs, int nbsphere, int nmax, con
     }
     IFDDA_GUARD_BEGIN
     DeviceScope ds(g->ctx->device);
+    AllocStreamScope as(g->ctx->stream);
     cudaStream_t st = g->ctx->stream;
     const MvGeom& geo = g->G.g;
     if (!tabdip && nbsphere != geo.N)
@@ -379,9 +431,19 @@ int ifdda_inverserig_batch_device(ifdda_green* g, int nrhs, int nbsphere, int nm
     }
     IFDDA_GUARD_BEGIN
     DeviceScope ds(g->ctx->device);
+    AllocStreamScope as(g->ctx->stream);
     if (!tabdip_dev && nbsphere != g->G.g.N)
         throw EngineError{1, "full-box solve: nbsphere must equal nx*ny*nz (or pass tabdip)"};
-    return solve_device(g, nrhs, nbsphere, nmax, tabdip_dev, (const double2*)polarisa_dev, ALPHA_FULL,
+    // isotropic tensors are compacted on the device (one alpha per dipole)
+    cudaStream_t st = g->ctx->stream;
+    g->alpha.ensure(nbsphere);
+    IFDDA_CUDA(cudaMemsetAsync(g->ctx->flag.p, 0, sizeof(int), st));
+    pola_compact_dev((const double2*)polarisa_dev, nbsphere, nmax, g->alpha.p, g->ctx->flag.p, st);
+    int aniso = 0;
+    IFDDA_CUDA(cudaMemcpyAsync(&aniso, g->ctx->flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    const double2* alpha = aniso ? (const double2*)polarisa_dev : g->alpha.p;
+    return solve_device(g, nrhs, nbsphere, nmax, tabdip_dev, alpha, aniso ? ALPHA_FULL : ALPHA_ISO,
                         (const double2*)FF0_dev, methodeit, tol, (double2*)FF_dev, (double2*)FFloc_dev, tol1, nloop,
                         ncompte, nstop, infostr, opt);
     IFDDA_GUARD_END(g->ctx, infostr)
@@ -392,6 +454,7 @@ int ifdda_local_macro(ifdda_ctx* ctx, int nbsphere, int nmax, const ifdda_dcmplx
     if (!ctx || !epsilon || !FFloc || !Em || nbsphere < 1 || nmax < nbsphere) return 1;
     IFDDA_GUARD_BEGIN
     DeviceScope ds(ctx->device);
+    AllocStreamScope as(ctx->stream);
     cudaStream_t st = ctx->stream;
     DevBuf<double2> eps, loc, em;
     eps.ensure((size_t)9 * nmax);
@@ -415,6 +478,7 @@ int ifdda_cross_sections(ifdda_ctx* ctx, int nbsphere, const ifdda_dcmplx* FF0, 
     if (!ctx || !FF0 || !FF || !FFloc || nbsphere < 1) return 1;
     IFDDA_GUARD_BEGIN
     DeviceScope ds(ctx->device);
+    AllocStreamScope as(ctx->stream);
     cudaStream_t st = ctx->stream;
     const long n3 = 3L * nbsphere;
     DevBuf<double2> a, b, c;
@@ -442,6 +506,7 @@ int ifdda_incident_planewaves(ifdda_ctx* ctx, int nbsphere, const double* xs, co
     if (!ctx || !xs || !ys || !zs || !beam || !a1 || !a2 || !pp || !FF0 || nbsphere < 1 || nrhs < 1) return 1;
     IFDDA_GUARD_BEGIN
     DeviceScope ds(ctx->device);
+    AllocStreamScope as(ctx->stream);
     cudaStream_t st = ctx->stream;
     DevBuf<double> dx, dy, dz, d1, d2, dp;
     DevBuf<int> db;

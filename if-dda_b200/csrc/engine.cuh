@@ -52,17 +52,31 @@ inline void ensure_smem_ptr(const void* kernel, size_t bytes) {
 }
 template <class K> inline void ensure_smem(K kernel, size_t bytes) { ensure_smem_ptr((const void*)kernel, bytes); }
 
+// Stream on which DevBuf allocates and frees (stream-ordered, from the
+// device's memory pool): the calling entry point sets it to its context's
+// stream, so buffers are neither allocated nor freed with a device-wide
+// synchronisation and a free is ordered after the work that used the buffer.
+inline cudaStream_t& alloc_stream() {
+    static thread_local cudaStream_t s = nullptr;
+    return s;
+}
+struct AllocStreamScope {
+    cudaStream_t prev;
+    explicit AllocStreamScope(cudaStream_t s) : prev(alloc_stream()) { alloc_stream() = s; }
+    ~AllocStreamScope() { alloc_stream() = prev; }
+};
+
 template <class T> struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
     void ensure(size_t count) {
         if (count <= n) return;
         release();
-        IFDDA_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
+        IFDDA_CUDA(cudaMallocAsync((void**)&p, count * sizeof(T), alloc_stream()));
         n = count;
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, alloc_stream());
         p = nullptr;
         n = 0;
     }

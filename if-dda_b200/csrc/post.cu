@@ -161,4 +161,29 @@ void planewaves_dev(int nb, const double* xs, const double* ys, const double* zs
     IFDDA_CUDA(cudaGetLastError());
 }
 
+// Compacts an isotropic (nmax,3,3) polarisability to one value per dipole;
+// sets *aniso when any tensor is not a multiple of the identity.
+__global__ void k_pola_compact(const double2* __restrict__ pol, long nb, long nmax, double2* __restrict__ alpha,
+                               int* __restrict__ aniso) {
+    int bad = 0;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += (long)gridDim.x * blockDim.x) {
+        const double2 d0 = pol[i];
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+                const double2 v = pol[i + nmax * (a + 3 * b)];
+                if (a == b) bad |= (v.x != d0.x || v.y != d0.y);
+                else bad |= (v.x != 0.0 || v.y != 0.0);
+            }
+        alpha[i] = d0;
+    }
+    if (bad) atomicOr(aniso, 1);
+}
+
+void pola_compact_dev(const double2* pol, long nb, long nmax, double2* alpha, int* aniso, cudaStream_t st) {
+    const int grid = (int)std::max(1L, std::min<long>((nb + 255) / 256, 148L * 8));
+    count_launch();
+    k_pola_compact<<<grid, 256, 0, st>>>(pol, nb, nmax, alpha, aniso);
+    IFDDA_CUDA(cudaGetLastError());
+}
+
 }  // namespace ifdda

@@ -66,6 +66,18 @@ template <class T> struct KrylovWork {
     int x_slot(int method) const;
     int b_slot(int method) const;
     int xr_slot(int method) const;
+    void release() {
+        graph.reset();
+        vecs.release();
+        st.release();
+        status.release();
+        zstatus.release();
+        partials.release();
+        tickets.release();
+        hstatus.clear();
+        nrhs = 0;
+        n3 = 0;
+    }
 };
 
 struct MixedWork {
@@ -75,6 +87,15 @@ struct MixedWork {
     DevBuf<int> ostatus;
     DevBuf<double2> partials;
     DevBuf<unsigned> tickets;
+    void release() {
+        x.release();
+        ax.release();
+        alpha32.release();
+        ost.release();
+        ostatus.release();
+        partials.release();
+        tickets.release();
+    }
 };
 
 struct SolverWork {

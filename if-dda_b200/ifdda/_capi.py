@@ -24,7 +24,7 @@ class DComplex(C.Structure):
 
 class SolveOptions(C.Structure):
     _fields_ = [("precision", C.c_int), ("check_every", C.c_int), ("max_outer", C.c_int),
-                ("inner_floor", C.c_double)]
+                ("inner_floor", C.c_double), ("maxit", C.c_int)]
 
 
 _lib = None
@@ -43,6 +43,7 @@ SIGNATURES = {
     "ifdda_ctx_stream": (_vp, [_vp]),
     "ifdda_green_create": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.POINTER(_vp)]),
     "ifdda_green_destroy": (C.c_int, [_vp]),
+    "ifdda_green_release_workspace": (C.c_int, [_vp]),
     "ifdda_green_export": (C.c_int, [_vp] + [_vp] * 6),
     "ifdda_matvec": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, _vp]),
     "ifdda_matvec_device": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp]),

@@ -138,6 +138,10 @@ class GreenSpectrum:
         except Exception:
             pass
 
+    def release_workspace(self):
+        """Free the solver / mat-vec workspaces; the spectrum stays."""
+        self.ctx._check(self.lib.ifdda_green_release_workspace(self.h))
+
     @property
     def ntotal(self):
         return 8 * self.nx * self.ny * self.nz
@@ -168,7 +172,8 @@ class GreenSpectrum:
                                                      C.c_void_p(FFX_ptr), C.c_void_p(FFB_ptr)))
 
     def inverserig(self, nbsphere, polarisa, nmax, FF0, methodeit="GPBICG1", tol=1e-4, tabdip=None,
-                   precision=IFDDA_FP64, check_every=0, max_outer=0, inner_floor=0.0, nstop_in=0) -> SolveResult:
+                   precision=IFDDA_FP64, check_every=0, max_outer=0, inner_floor=0.0, nstop_in=0,
+                   maxit=0) -> SolveResult:
         """Rigorous solve (inverserig / inverserigopt) for one or a batch of
         right-hand sides.  FF0: (3*nbsphere,) or (nrhs, 3*nbsphere)."""
         ff0 = _zc(FF0)
@@ -183,7 +188,7 @@ class GreenSpectrum:
         ncompte = np.zeros(nrhs, np.int32)
         nstop = C.c_int(nstop_in)
         info = C.create_string_buffer(b" " * 64, 65)
-        opt = SolveOptions(precision, check_every, max_outer, inner_floor)
+        opt = SolveOptions(precision, check_every, max_outer, inner_floor, maxit)
         tab = None if tabdip is None else np.ascontiguousarray(tabdip, np.int32)
         self.lib.ifdda_inverserig_batch(self.h, nrhs, nbsphere, nmax, _p(tab) if tab is not None else None,
                                         _p(pol), _p(ff0), methodeit.encode(), tol, _p(FF), _p(FFloc), _p(tol1),
@@ -194,14 +199,14 @@ class GreenSpectrum:
 
     def inverserig_device(self, nrhs, nbsphere, nmax, tabdip_ptr, polarisa_ptr, FF0_ptr, FF_ptr, FFloc_ptr,
                           methodeit="GPBICG1", tol=1e-4, precision=IFDDA_FP64, check_every=0, max_outer=0,
-                          inner_floor=0.0):
+                          inner_floor=0.0, maxit=0):
         """Batched solve on device pointers (ints, e.g. torch data_ptr())."""
         tol1 = np.zeros(nrhs)
         nloop = np.zeros(nrhs, np.int32)
         ncompte = np.zeros(nrhs, np.int32)
         nstop = C.c_int(0)
         info = C.create_string_buffer(b" " * 64, 65)
-        opt = SolveOptions(precision, check_every, max_outer, inner_floor)
+        opt = SolveOptions(precision, check_every, max_outer, inner_floor, maxit)
         self.lib.ifdda_inverserig_batch_device(self.h, nrhs, nbsphere, nmax, C.c_void_p(tabdip_ptr or 0) if tabdip_ptr else None,
                                                C.c_void_p(polarisa_ptr), C.c_void_p(FF0_ptr), methodeit.encode(),
                                                tol, C.c_void_p(FF_ptr), C.c_void_p(FFloc_ptr), _p(tol1), _p(nloop),

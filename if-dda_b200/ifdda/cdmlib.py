@@ -1,0 +1,123 @@
+"""cdmlib -- host-side mirror of the reference's entry point for the rigorous
+solve (cdmlib/cdmlib.f:3-60, C prototype cdmlib/cdmlib.h:5-71), on the GPU.
+
+It takes the reference's option names and units (lengths in nm, angles in
+degrees, eps as complex), runs the same sequence as cdmlib.f --
+validation (:317-471), object (:661-805), padded grid (:1141-1148), incident
+field (:1172-1187), Green spectrum (:1518-1546), solve (:1555-1597), local and
+macroscopic fields (:2497-2655), cross sections (:2717-2778) -- and returns
+the reference's outputs in a dict together with nstop/infostr.  Only the
+options on the rigorous-solve path are implemented (trope 'iso', plane waves,
+nrig = 0, nquad = 0); anything else returns nstop = 1 with a message.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import objects
+from .api import Context, IfddaError
+
+_SUPPORTED_OBJECTS = ("sphere", "cube", "inhomocuboid2", "concentricsphere", "arbitrary")
+
+
+def _fail(msg, **extra):
+    d = dict(nstop=1, infostr=msg)
+    d.update(extra)
+    return d
+
+
+def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, rayons=None, epss=None,
+           nx=None, ny=None, nz=None, aretecube=None, lc=None, hc=None, ng=0, positions=None, eps_site=None,
+           beam="pwavelinear", theta=0.0, phi=0.0, pp=1.0, incidences=None, P0=1.0, w0=None,
+           tolinit=1e-4, methodeit="GPBICG1", polarizability="RR", trope="iso", nproche=0, nrig=0, nquad=0,
+           nlocal=1, nmacro=1, nsection=1, precision=0, ctx: Context | None = None, device=0):
+    """Rigorous solve of one object for one plane wave (theta, phi, pp) or a
+    batch of them (incidences = [(theta, phi, pp), ...]).  nproche follows the
+    GUI convention: 0 -> dipoles inside the object only (inverserig), >= 1 ->
+    the full box (inverserigopt).  precision: 0 plain FP64, 1 FP32 inner
+    iterations with FP64 refinement."""
+    lam = wavelength * 1e-9
+    if trope != "iso":
+        return _fail("only isotropic objects are handled by the GPU drop-in")
+    if nrig != 0:
+        return _fail("only the rigorous solve (nrig = 0) is handled by the GPU drop-in")
+    if nquad != 0:
+        return _fail("only nquad = 0 is handled by the GPU drop-in")
+    if beam != "pwavelinear":
+        return _fail("Cross section only with plane wave" if nsection else "only plane waves are handled")
+    if tolinit < 1e-12:
+        return _fail("Tolerance for the iterative method too small!")
+    if tolinit > 0.5:
+        return _fail("Tolerance  for the iterative method too large!")
+    if object not in _SUPPORTED_OBJECTS:
+        return _fail(f"object {object!r} not handled by the GPU drop-in")
+    if not (nlocal or nmacro or nsection):
+        return _fail("No calculation requested!")
+    k0 = 2 * math.pi / lam
+    inside = nproche - 1 == -1  # cdmlib.f:627 decrements the GUI value
+    # ---- object (cdmlib.f:661-805) -------------------------------------
+    try:
+        if object == "sphere":
+            ob = objects.sphere(rayon * 1e-9, complex(eps), nnnr, k0, polarizability, na=-1 if inside else 0)
+        elif object == "cube":
+            ob = objects.cube(side * 1e-9, complex(eps), nnnr, k0, polarizability)
+        elif object == "inhomocuboid2":
+            ob = objects.inhomocuboid(nx, ny, nz, aretecube * 1e-9, complex(eps), lc * 1e-9, hc, ng, k0,
+                                      polarizability)
+        elif object == "concentricsphere":
+            ob = objects.concentric([r * 1e-9 for r in rayons], epss, nnnr, k0, polarizability,
+                                    na=-1 if inside else 0)
+        else:
+            pos = np.asarray(positions, float) * 1e-9
+            ob = objects.arbitrary(nx, ny, nz, aretecube * 1e-9, pos[:, 0], pos[:, 1], pos[:, 2], eps_site, k0,
+                                   polarizability)
+    except ValueError as e:
+        return _fail(str(e))
+    if ob.nbsphere == 0:
+        return _fail("No dipole in the object!")
+    # mesh size check (cdmlib.f:994-999)
+    eps_max = np.max(np.abs(np.sqrt(ob.eps))) if len(ob.eps) else 1.0
+    if ob.aretecube > 2.5 * lam / 10.0 / eps_max:
+        return _fail("Meshsize larger than lambda/4!")
+    own = ctx is None
+    ctx = ctx or Context(device)
+    try:
+        # ---- incident field (cdmlib.f:1172-1187, irradiance.f) -----------
+        E0, irra = objects.irradiance(P0, (w0 if w0 is not None else 10 * wavelength) * 1e-9)
+        inc = incidences if incidences is not None else [(theta, phi, pp)]
+        ff0 = ctx.planewaves(ob.xs, ob.ys, ob.zs, k0, E0, [0] * len(inc), [t for t, _, _ in inc],
+                             [p for _, p, _ in inc], [q for _, _, q in inc])
+        # ---- Green spectrum and solve (cdmlib.f:1518-1597) ---------------
+        try:
+            g = ctx.green(ob.nx, ob.ny, ob.nz, ob.aretecube, k0)
+        except IfddaError as e:
+            return _fail(str(e)[:64])
+        r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0 if len(inc) > 1 else ff0[0], methodeit, tolinit,
+                         tabdip=ob.tabdip_or_none, precision=precision)
+        out = dict(nstop=r.nstop, infostr=r.infostr, nbsphere=ob.nbsphere, ndipole=ob.ndipole,
+                   aretecube=ob.aretecube, k0=k0, irra=irra, E0=E0, tol1=r.tol1, nloop=r.nloop,
+                   ncompte=r.ncompte, incidentfield=ff0, FF=r.FF, localfield=r.FFloc, xs=ob.xs, ys=ob.ys,
+                   zs=ob.zs)
+        g.close()
+        if r.nstop != 0:
+            return out
+        FF = np.atleast_2d(r.FF)
+        FFloc = np.atleast_2d(r.FFloc)
+        # ---- macroscopic field (cdmlib.f:2595-2655) ----------------------
+        if nmacro:
+            out["macroscopicfield"] = np.stack([ctx.local_macro(ob.nbsphere, ob.nmax, ob.epsilon, FFloc[q],
+                                                                ob.aretecube, k0) for q in range(len(inc))])
+        # ---- cross sections (cdmlib.f:2717-2778) -------------------------
+        if nsection:
+            cs = [ctx.cross_sections(ff0[q], FF[q], FFloc[q], k0, abs(E0) ** 2) for q in range(len(inc))]
+            cext = np.array([c[0] for c in cs])
+            cabs = np.array([c[1] for c in cs])
+            csca = cext - cabs
+            cabs = np.where(cabs <= cext * 1e-12, 0.0, cabs)
+            out.update(Cext=cext, Cabs=cabs, Csca=csca)
+        return out
+    finally:
+        if own:
+            ctx.close()

@@ -1,0 +1,217 @@
+"""Continuous-batching request loop for many solves of uneven size on one GPU.
+
+A stream of requests (object, wavelength, a few incidences each) arrives over
+time.  `SLOTS` worker threads each own an ifdda Context (one CUDA stream) and
+take the next request in arrival order as soon as they are free *and* the
+request's device footprint fits in the HBM budget next to the requests in
+flight; their solves then overlap on the GPU.  Each slot keeps an LRU cache of
+Green spectra keyed by (lattice, spacing, wavelength), so a repeated object
+size at the same wavelength skips the spectrum build.  Every request's result
+is computed by its own context with fixed-order reductions, so it is the same
+bit for bit alone and inside the mix.
+
+The reference solves one object at a time (cdmlib/cdmlib.f:3-60 called from
+the GUI's run thread, cdm/cdmRunWidget.cpp:162); this loop is the serving
+layer the batched solver is driven by.
+"""
+from __future__ import annotations
+
+import collections
+import math
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import objects
+from .api import Context, IFDDA_FP64, IFDDA_MIXED
+
+
+@dataclass
+class Request:
+    rid: int
+    shape: str             # "sphere" or "cube"
+    n: int                 # lattice edge
+    d: float               # spacing (m)
+    eps: complex
+    wavelength: float      # (m)
+    incidences: list       # [(kx/k0, ky/k0, pp)]
+    arrival: float = 0.0   # seconds after the stream start
+
+
+@dataclass
+class Result:
+    rid: int
+    FFloc: np.ndarray
+    tol1: np.ndarray
+    nloop: np.ndarray
+    ncompte: np.ndarray
+    nstop: int
+    infostr: str
+    start: float
+    end: float
+    arrival: float
+    slot: int
+    green_hit: bool
+
+
+def footprint_bytes(n: int, nrhs: int, precision: int) -> int:
+    """Device bytes one solve holds: the spectrum (FP64 + FP32), mat-vec
+    scratch, Krylov vectors and inputs."""
+    N = n ** 3
+    Np = (n + 1) ** 3
+    green = 6 * Np * (16 + 8)
+    scr64 = 18 * N * 16 * nrhs
+    vec64 = 14 * 3 * N * 16 * nrhs
+    io = 4 * 3 * N * 16 * nrhs + N * 16
+    if precision == IFDDA_MIXED:
+        return green + scr64 + 18 * N * 8 * nrhs + 14 * 3 * N * 8 * nrhs + 2 * 3 * N * 16 * nrhs + io
+    return green + scr64 + vec64 + io
+
+
+def make_stream(nreq: int, rate: float, seed: int = 4, edges=(16, 24, 32, 48, 64, 80, 96), max_inc: int = 32,
+                d: float = 10e-9):
+    """Seeded synthetic request stream: Poisson arrivals at `rate` per second,
+    sphere or cube, edge uniform in `edges`, eps' ~ U[1.5, 4], eps'' ~
+    U[0, 0.5], wavelength ~ U[400, 800] nm, 1..max_inc incidences uniform on
+    the NA 0.9 disk, s and p alternating."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    t = 0.0
+    out = []
+    for rid in range(nreq):
+        t += rng.exponential(1.0 / rate)
+        ninc = int(rng.integers(1, max_inc + 1))
+        rr = 0.9 * np.sqrt(rng.uniform(0, 1, ninc))
+        th = rng.uniform(0, 2 * np.pi, ninc)
+        inc = [(float(a * math.cos(b)), float(a * math.sin(b)), float(q % 2)) for q, (a, b) in enumerate(zip(rr, th))]
+        out.append(Request(rid=rid, shape="sphere" if rng.uniform() < 0.5 else "cube",
+                           n=int(edges[int(rng.integers(0, len(edges)))]), d=d,
+                           eps=complex(rng.uniform(1.5, 4.0), rng.uniform(0.0, 0.5)),
+                           wavelength=float(rng.uniform(400e-9, 800e-9)), incidences=inc, arrival=t))
+    return out
+
+
+def build_object(req: Request):
+    k0 = 2 * math.pi / req.wavelength
+    if req.shape == "sphere":
+        ob = objects.sphere(req.n * req.d / 2, req.eps, req.n, k0, "RR", na=-1)
+    else:
+        ob = objects.cube(req.n * req.d, req.eps, req.n, k0, "RR")
+    return ob, k0
+
+
+class _Slot:
+    def __init__(self, idx: int, device: int, cache_size: int):
+        self.idx = idx
+        self.ctx = Context(device)
+        self.cache = collections.OrderedDict()
+        self.cache_size = cache_size
+
+    def green(self, ob, k0):
+        key = (ob.nx, ob.ny, ob.nz, ob.aretecube, k0)
+        if key in self.cache:
+            self.cache.move_to_end(key)
+            return self.cache[key], True
+        g = self.ctx.green(ob.nx, ob.ny, ob.nz, ob.aretecube, k0)
+        self.cache[key] = g
+        while len(self.cache) > self.cache_size:
+            _, old = self.cache.popitem(last=False)
+            old.close()
+        return g, False
+
+    def close(self):
+        for g in self.cache.values():
+            g.close()
+        self.cache.clear()
+        self.ctx.close()
+
+
+def solve_request(slot: _Slot, req: Request, precision: int, tol: float = 1e-4, methodeit: str = "GPBICG1"):
+    ob, k0 = build_object(req)
+    E0, _ = objects.irradiance(1.0, 10 * req.wavelength)
+    kx = [a * k0 for a, _, _ in req.incidences]
+    ky = [b * k0 for _, b, _ in req.incidences]
+    pp = [c for _, _, c in req.incidences]
+    ff0 = slot.ctx.planewaves(ob.xs, ob.ys, ob.zs, k0, E0, [1] * len(kx), kx, ky, pp)
+    g, hit = slot.green(ob, k0)
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, methodeit, tol, tabdip=ob.tabdip_or_none,
+                     precision=precision)
+    # a cached spectrum keeps no workspace: the HBM budget covers in-flight solves only
+    g.release_workspace()
+    return r, hit
+
+
+class Server:
+    """Admission by HBM footprint + `slots` concurrent workers."""
+
+    def __init__(self, slots: int = 4, device: int = 0, hbm_budget: float = 120e9, precision: int = IFDDA_MIXED,
+                 cache_size: int = 4):
+        self.slots = [_Slot(i, device, cache_size) for i in range(slots)]
+        self.budget = hbm_budget
+        self.precision = precision
+        self.in_use = 0.0
+        self.cv = threading.Condition()
+
+    def close(self):
+        for s in self.slots:
+            s.close()
+
+    def run(self, requests, realtime: bool = True):
+        """Serve `requests` (sorted by arrival); returns the Results in id
+        order.  With realtime, a request becomes visible at its arrival time."""
+        pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+        results = {}
+        t0 = time.perf_counter()
+        lock = threading.Lock()
+
+        def next_request():
+            # FIFO admission: the head of the queue waits until it has arrived
+            # and its footprint fits next to the work in flight
+            with self.cv:
+                while True:
+                    if not pending:
+                        return None, 0.0
+                    head = pending[0]
+                    now = time.perf_counter() - t0
+                    fp = footprint_bytes(head.n, len(head.incidences), self.precision)
+                    arrived = (not realtime) or head.arrival <= now
+                    fits = self.in_use + fp <= self.budget or self.in_use == 0
+                    if arrived and fits:
+                        pending.popleft()
+                        self.in_use += fp
+                        return head, fp
+                    wait = max(0.0005, head.arrival - now) if not arrived else 0.05
+                    self.cv.wait(timeout=wait)
+
+        def worker(slot: _Slot):
+            while True:
+                req, fp = next_request()
+                if req is None:
+                    return
+                start = time.perf_counter() - t0
+                try:
+                    r, hit = solve_request(slot, req, self.precision)
+                finally:
+                    with self.cv:
+                        self.in_use -= fp
+                        self.cv.notify_all()
+                end = time.perf_counter() - t0
+                with lock:
+                    results[req.rid] = Result(req.rid, r.FFloc, r.tol1, r.nloop, r.ncompte, r.nstop, r.infostr,
+                                              start, end, req.arrival if realtime else 0.0, slot.idx, hit)
+
+        threads = [threading.Thread(target=worker, args=(s,), daemon=True) for s in self.slots]
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
+        return [results[k] for k in sorted(results)]
+
+
+def latency_stats(results, wall: float):
+    lat = np.array([r.end - r.arrival for r in results])
+    nrhs = sum(len(np.atleast_1d(r.tol1)) for r in results)
+    return dict(p50_ms=float(np.percentile(lat, 50) * 1e3), p99_ms=float(np.percentile(lat, 99) * 1e3),
+                requests_per_s=len(results) / wall, solves_per_s=nrhs / wall,
+                failed=int(sum(r.nstop != 0 for r in results)))

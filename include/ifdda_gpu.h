@@ -37,6 +37,7 @@ typedef struct {
     int check_every;    /* iterations launched between status polls; 0 = 4 */
     int max_outer;      /* refinement steps of IFDDA_MIXED; 0 = 12 */
     double inner_floor; /* smallest relative tolerance asked of an FP32 inner solve; 0 = 1e-6 */
+    int maxit;          /* iteration limit; 0 = 10000, the reference's nlim (cdmlib/inverserigopt.f:30) */
 } ifdda_solve_options;
 
 int ifdda_abi_version(void);
@@ -57,6 +58,10 @@ void* ifdda_ctx_stream(ifdda_ctx* ctx);
    aretecube in metres, k0 in 1/m.  The spectrum stays on the device. */
 int ifdda_green_create(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, ifdda_green** out);
 int ifdda_green_destroy(ifdda_green* g);
+/* Frees the solver and mat-vec workspaces held by g (they are re-created on
+   the next solve); the spectrum stays.  For callers that cache many spectra.
+   No counterpart in the reference. */
+int ifdda_green_release_workspace(ifdda_green* g);
 /* Writes the six FFTTENSOR arrays (xx,xy,xz,yy,yz,zz, 8*nx*ny*nz each, x
    fastest) exactly as greencalculfft leaves them. */
 int ifdda_green_export(ifdda_green* g, ifdda_dcmplx* xx, ifdda_dcmplx* xy, ifdda_dcmplx* xz, ifdda_dcmplx* yy,

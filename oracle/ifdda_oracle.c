@@ -638,9 +638,10 @@ typedef int (*orc_cancel_fn)(int ncompte);
 int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int *tabdip,
                    const zc *polarisa, int nmax, const zc *FF0, const char *methodeit,
                    double tol, zc *FF, zc *FFloc, double *tol1, int *nloop, int *ncompte,
-                   int *nstop, char *infostr, orc_cancel_fn cancel) {
+                   int *nstop, char *infostr, orc_cancel_fn cancel, int nlim_in) {
     long n3 = 3L * nbsphere;
-    int nlim = 10000;
+    /* nlim = 10000 in the reference (inverserigopt.f:30); tests may lower it */
+    int nlim = nlim_in > 0 ? nlim_in : 10000;
     int nou = 0, nstat = 0, steperr = 0;
     zc *xi = (zc *)malloc(sizeof(zc) * n3);
     zc *xr = (zc *)malloc(sizeof(zc) * n3);

@@ -111,10 +111,11 @@ _CANCEL = C.CFUNCTYPE(C.c_int, C.c_int)
 
 
 def inverserig(G6, nx, ny, nz, nbsphere, polarisa, nmax, FF0, methodeit, tol,
-               tabdip=None, max_matvecs=None):
+               tabdip=None, max_matvecs=None, nlim=0):
     """Solver driver (inverserig / inverserigopt).  Returns a dict with
     FF, FFloc, tol1, nloop, ncompte, nstop, infostr.  ``max_matvecs`` stops
-    the solve after that many mat-vecs (the bounded CPU-baseline sample)."""
+    the solve after that many mat-vecs (the bounded CPU-baseline sample);
+    ``nlim`` > 0 replaces the reference's iteration limit of 10000."""
     g = _z(G6)
     pol = _z(polarisa)
     ff0 = _z(FF0)
@@ -135,7 +136,7 @@ def inverserig(G6, nx, ny, nz, nbsphere, polarisa, nmax, FF0, methodeit, tol,
                          _p(tab) if tab is not None else None, _p(pol), C.c_int(nmax), _p(ff0),
                          methodeit.encode(), C.c_double(tol), _p(FF), _p(FFloc),
                          C.byref(tol1), C.byref(nloop), C.byref(ncompte), C.byref(nstop),
-                         info, cb)
+                         info, cb, C.c_int(nlim))
     return dict(FF=FF, FFloc=FFloc, tol1=tol1.value, nloop=nloop.value,
                 ncompte=ncompte.value, nstop=nstop.value,
                 infostr=info.raw[:64].decode(errors="replace"))

@@ -94,6 +94,46 @@ def test_full_box_solve_matches_oracle(gctx, orc, meth):
     g.close()
 
 
+def _grf(orc, n):
+    from ifdda import objects
+    k0 = 2 * math.pi / 632.8e-9
+    ob = objects.inhomocuboid(n, n, n, 10e-9, 2.25 + 0j, 50e-9, 0.1, 7, k0, "RR")
+    E0, _ = objects.irradiance(1.0, 10 * 632.8e-9)
+    ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 1.0, 0, 20.0, 0.0)
+    return ob, k0, ff0, orc.greencalculfft(n, n, n, ob.aretecube, k0)
+
+
+@pytest.mark.parametrize("n,nlim", [(40, 0), (48, 10)])
+def test_qmr_on_grf_cube_matches_oracle(gctx, orc, n, nlim):
+    """Full-box GRF cube (the config-2 object at reduced size).  At 40^3 QMR
+    converges; at 48^3 it stalls and is stopped at nlim iterations, where both
+    paths report "Converge do not reach!" with the same iterate."""
+    ob, k0, ff0, G = _grf(orc, n)
+    for meth in ("QMRBICGSTAB1", "QMRBICGSTAB2"):
+        ref = orc.inverserig(G, n, n, n, ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-4, nlim=nlim)
+        g = gctx.green(n, n, n, ob.aretecube, k0)
+        r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-4, maxit=nlim)
+        # the C-ABI adds cdmlib's own check tol1 >= tolinit (cdmlib.f:1586-1591)
+        want = (1, "Converge do not reach!") if ref["tol1"] >= 1e-4 else (ref["nstop"], ref["infostr"].strip())
+        assert (r.nstop, r.infostr.strip()) == want
+        assert int(r.nloop[0]) == ref["nloop"] and int(r.ncompte[0]) == ref["ncompte"]
+        assert rel(r.FFloc, ref["FFloc"]) < 1e-7
+        g.close()
+
+
+def test_gpbicg_iteration_limit_matches_oracle(gctx, orc):
+    ob, k0, E0, ff0, G = _c1_inputs(orc)
+    ref = orc.inverserig(G, 16, 16, 16, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-9, tabdip=ob.tabdip,
+                         nlim=2)
+    g = gctx.green(16, 16, 16, ob.aretecube, k0)
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-9, tabdip=ob.tabdip, maxit=2)
+    assert ref["nstop"] == 0 and ref["tol1"] >= 1e-9  # inverserig itself does not test tol1
+    assert r.nstop == 1 and r.infostr.strip() == "Converge do not reach!"
+    assert int(r.nloop[0]) == ref["nloop"] == 4 and int(r.ncompte[0]) == ref["ncompte"]
+    assert rel(r.FFloc, ref["FFloc"]) < 1e-9
+    g.close()
+
+
 def test_mixed_precision_meets_fp64_residual(gctx, orc):
     from ifdda import IFDDA_MIXED
     ob, k0, E0, ff0, G = _c1_inputs(orc)
@@ -167,3 +207,23 @@ def test_error_paths(gctx, orc):
     with pytest.raises(ifdda.IfddaError):
         gctx.green(7, 7, 7, 10e-9, k0)
     g.close()
+
+
+def test_cdmlib_driver_config1_matches_oracle(orc):
+    """Config 1 through the cdmlib-style entry (reference option names and
+    units) against the oracle pipeline; Cext within the DDA error of Mie."""
+    from ifdda.cdmlib import cdmlib
+    out = cdmlib(wavelength=632.8, object="sphere", rayon=100.0, eps=2.25 + 0j, nnnr=16, tolinit=1e-4,
+                 methodeit="GPBICG1", polarizability="RR", nproche=0, theta=0.0, phi=0.0, pp=1.0, P0=1.0,
+                 w0=6328.0)
+    assert out["nstop"] == 0 and out["nbsphere"] == 2176
+    ob, k0, E0, ff0, G = _c1_inputs(orc)
+    ref = orc.inverserig(G, 16, 16, 16, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-4, tabdip=ob.tabdip)
+    assert rel(out["localfield"], ref["FFloc"]) < 1e-7
+    em = orc.local_macro_all(ob.nbsphere, ob.nmax, ob.epsilon, ref["FFloc"], ob.aretecube, k0)
+    assert rel(out["macroscopicfield"][0], em) < 1e-7
+    ce, ca = orc.cross_sections(ff0, ref["FF"], ref["FFloc"], k0, E0 ** 2)
+    assert abs(out["Cext"][0] - ce) <= 1e-7 * ce
+    mie_ext, _, _ = orc.mie(2.25, 100e-9, 632.8e-9)
+    assert abs(out["Cext"][0] - mie_ext) / mie_ext < 0.06
+
