@@ -9,7 +9,7 @@ Default workload (one step = one complete rigorous solve):
   (headline `value`), next to the plain FP64 drop-in (`fp64` block).
 Other workloads (--workload): c1 (sphere 16^3, inside-only dipoles), c3
 (128 plane waves on a 96x96x64 ellipsoid lattice, one batched solve per
-step), c5 (192^3 concentric spheres, QMR-BiCGSTAB), c4 (request stream
+step), c5 (192^3 concentric spheres, GPBICG1), c4 (request stream
 through the continuous-batching server).
 Inputs are resident in HBM for `value`; `e2e` runs the same solve through the
 C-ABI (ifdda_inverserig) with pinned host inputs and the host<->device copies
@@ -106,8 +106,9 @@ def wl_c5():
     E0, _ = objects.irradiance(1.0, 10 * lam)
     return Workload("c5", "C5 concentric spheres (core eps 3+0.01i r=0.9 um, shell eps 2 r=1.9 um) on the full "
                     "192^3 lattice (7.08M dipoles, d = 2 r_out/192 = 19.79 nm as the reference sizes it), "
-                    "lambda=632.8 nm, normal incidence, QMR-BiCGSTAB1 to 1e-4, FFT grid 384^3", ob, k0, E0,
-                    [(0, 0.0, 0.0, 1.0)], "QMRBICGSTAB1", 1, cpu_mv=1)
+                    "lambda=632.8 nm, normal incidence, GPBICG1 to 1e-4 (QMR-BiCGSTAB, the configured method, "
+                    "stalls on this object in the restatement and on the GPU alike), FFT grid 384^3",
+                    ob, k0, E0, [(0, 0.0, 0.0, 1.0)], "GPBICG1", 1, cpu_mv=1)
 
 
 WORKLOADS = {"c1": wl_c1, "c2": wl_c2, "c3": wl_c3, "c5": wl_c5}
@@ -457,6 +458,54 @@ def run_gpu(args):
     return 0
 
 
+def run_matvec(args):
+    """Mat-vec only: the five passes of one right-hand side on the workload's
+    grid, FP32 then FP64, each pass timed with CUDA events on the solver
+    stream (also the target of the ncu commands in profiles/)."""
+    import ctypes as C
+    import torch
+    import ifdda
+    from ifdda import _capi
+
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = WORKLOADS[args.workload]()
+    ob = w.ob
+    ctx = ifdda.Context(local)
+    lib = ctx.lib
+    g = ctx.green(ob.nx, ob.ny, ob.nz, ob.aretecube, w.k0)
+    N = ob.nx * ob.ny * ob.nz
+    Np = (ob.nx + 1) * (ob.ny + 1) * (ob.nz + 1)
+    names = {1: "fwd_x", 2: "fwd_y", 3: "zconv", 4: "inv_y", 5: "inv_x"}
+    out = {}
+    for prec, dt, s in ((_capi.IFDDA_FP32, torch.complex64, 8), (_capi.IFDDA_FP64, torch.complex128, 16)):
+        x = torch.randn(3 * N, dtype=dt, device=dev)
+        b = torch.randn(3 * N, dtype=dt, device=dev)
+        for _ in range(args.warmup):
+            g.matvec_device(1, N, x.data_ptr(), b.data_ptr(), precision=prec)
+        ctx.synchronize()
+        balg = {1: 9 * N * s, 2: 18 * N * s, 3: (24 * N + 6 * Np) * s, 4: 18 * N * s, 5: 12 * N * s}
+        passes = {}
+        for ps in range(1, 6):
+            lib.ifdda_timing_enable(ps, prec)
+            for _ in range(args.steps):
+                g.matvec_device(1, N, x.data_ptr(), b.data_ptr(), precision=prec)
+            ctx.synchronize()
+            nl, ms = C.c_int(0), C.c_double(0)
+            lib.ifdda_timing_read(C.byref(nl), C.byref(ms))
+            avg = ms.value / max(nl.value, 1)
+            passes[names[ps]] = {"ms": round(avg, 5), "alg_GB_s": round(balg[ps] / avg / 1e6, 1)}
+        lib.ifdda_timing_enable(0, -1)
+        out["fp32" if s == 8 else "fp64"] = passes
+        del x, b
+    if rank == 0:
+        print(json.dumps({"mode": "matvec", "workload": w.desc, "passes": out}), flush=True)
+    g.close()
+    ctx.close()
+    return 0
+
+
 def run_serving(args):
     """Config 4: a seeded request stream through the continuous-batching
     server, mixed precision then plain FP64 on the same stream."""
@@ -504,6 +553,8 @@ def main():
     ap.add_argument("--requests", type=int, default=2000, help="c4: stream length")
     ap.add_argument("--rate", type=float, default=100.0, help="c4: Poisson arrival rate (requests/s)")
     ap.add_argument("--slots", type=int, default=4, help="c4: concurrent solver slots")
+    ap.add_argument("--mode", default="solve", choices=["solve", "matvec"],
+                    help="matvec: time the five mat-vec passes only")
     args = ap.parse_args()
     if args.impl == "reference":
         if args.workload == "c4":
@@ -511,6 +562,8 @@ def main():
         return run_reference(args)
     if args.workload == "c4":
         return run_serving(args)
+    if args.mode == "matvec":
+        return run_matvec(args)
     return run_gpu(args)
 
 

@@ -59,6 +59,35 @@ __host__ __device__ constexpr int clamp_pow2(int v, int lo, int hi) {
     while (p * 2 <= v && p * 2 <= hi) p *= 2;
     return p < lo ? lo : p;
 }
+// The plan of L: radix of pass q (0-based) and number of passes.  A plan
+// runs forward (q = 0 .. n-1) or reversed; any order of the radices is a
+// valid Stockham transform, and the reversed plan lets an inverse transform
+// start from the registers the forward transform ended with.
+__host__ __device__ constexpr int plan_len(int L) {
+    int n = 0;
+    bool first = true;
+    for (int rem = L; rem > 1;) {
+        const int r = pick_radix(rem, first);
+        if (r == 0) return -1;
+        rem /= r;
+        first = false;
+        n++;
+    }
+    return n;
+}
+__host__ __device__ constexpr int plan_radix(int L, int q) {
+    int rem = L;
+    bool first = true;
+    for (int i = 0; i < q; i++) {
+        rem /= pick_radix(rem, first);
+        first = false;
+    }
+    return pick_radix(rem, first);
+}
+__host__ __device__ constexpr int plan_radix_dir(int L, int q, bool rev) {
+    return rev ? plan_radix(L, plan_len(L) - 1 - q) : plan_radix(L, q);
+}
+
 // largest radix used by the plan of L (sets the register footprint)
 __host__ __device__ constexpr int max_radix(int L) {
     int m = 1;
@@ -202,15 +231,22 @@ struct SmemIO {
     template <class C> __device__ void store(int, int, C) const {}
 };
 
-template <int PS_, int BS_, bool BFAST_> struct Layout {
-    static constexpr int PS = PS_, BS = BS_;
+// PADSH > 0 inserts one padding word every 2^PADSH points, so the strided
+// writes of a radix-R pass (points j*R + r of consecutive j) spread over the
+// shared-memory banks.
+template <int PS_, int BS_, bool BFAST_, int PADSH_ = 0> struct Layout {
+    static constexpr int PS = PS_, BS = BS_, PADSH = PADSH_;
     static constexpr bool BFAST = BFAST_;
+    __device__ __forceinline__ static int addr(int p, int b) {
+        return (PADSH ? p + (p >> PADSH) : p) * PS + b * BS;
+    }
+    // points spanned by a line of length L (padding included)
+    static constexpr int span(int L) { return PADSH ? L + (L >> PADSH) : L; }
 };
 
 // One Stockham pass.  tw[j] = exp(+2 pi i j / L) in shared memory.
-template <class C, int L, int Ns, int NB, int NT, int DIR, class Lay, class Src, class Dst>
+template <class C, int L, int R, int Ns, int NB, int NT, int DIR, class Lay, class Src, class Dst>
 __device__ __forceinline__ void stockham_pass(C* sm, const C* tw, const Src& src, const Dst& dst) {
-    constexpr int R = pick_radix(L / Ns, Ns == 1);
     constexpr int NJ = L / R;
     constexpr int NBF = NB * NJ;
     constexpr int PER = (NBF + NT - 1) / NT;
@@ -232,7 +268,7 @@ __device__ __forceinline__ void stockham_pass(C* sm, const C* tw, const Src& src
                     const bool zero = Src::HALF && (R % 2 == 0 ? 2 * r >= R : 2 * p >= L);
                     v[q][r] = zero ? mk(decltype(C().x)(0), decltype(C().x)(0)) : src.template load<C>(b, p);
                 } else {
-                    v[q][r] = sm[p * Lay::PS + b * Lay::BS];
+                    v[q][r] = sm[Lay::addr(p, b)];
                 }
             }
             if (Ns > 1) {
@@ -264,7 +300,7 @@ __device__ __forceinline__ void stockham_pass(C* sm, const C* tw, const Src& src
                     const bool keep = !Dst::HALF || (R % 2 == 0 ? 2 * r < R : 2 * o < L);
                     if (keep) dst.template store<C>(b, o, v[q][r]);
                 } else {
-                    sm[o * Lay::PS + b * Lay::BS] = v[q][r];
+                    sm[Lay::addr(o, b)] = v[q][r];
                 }
             }
         }
@@ -272,11 +308,14 @@ __device__ __forceinline__ void stockham_pass(C* sm, const C* tw, const Src& src
     if (!GOUT) __syncthreads();
 }
 
-template <class C, int L, int Ns, int NB, int NT, int DIR, class Lay, class Src, class Dst>
-__device__ __forceinline__ void stockham_chain(C* sm, const C* tw, const Src& src, const Dst& dst) {
-    if constexpr (Ns < L) {
-        stockham_pass<C, L, Ns, NB, NT, DIR, Lay, Src, Dst>(sm, tw, src, dst);
-        stockham_chain<C, L, Ns * pick_radix(L / Ns, Ns == 1), NB, NT, DIR, Lay, Src, Dst>(sm, tw, src, dst);
+// Passes q in [q, Q1) of the plan (reversed when REV); Ns is the product of
+// the radices of the passes before q.
+template <class C, int L, int NB, int NT, int DIR, class Lay, bool REV, int Q1, int q, int Ns, class Src, class Dst>
+__device__ __forceinline__ void stockham_range(C* sm, const C* tw, const Src& src, const Dst& dst) {
+    if constexpr (q < Q1) {
+        constexpr int R = plan_radix_dir(L, q, REV);
+        stockham_pass<C, L, R, Ns, NB, NT, DIR, Lay, Src, Dst>(sm, tw, src, dst);
+        stockham_range<C, L, NB, NT, DIR, Lay, REV, Q1, q + 1, Ns * R, Src, Dst>(sm, tw, src, dst);
     }
 }
 
@@ -288,7 +327,7 @@ __device__ __forceinline__ void stockham_chain(C* sm, const C* tw, const Src& sr
 template <class C, int L, int NB, int NT, int DIR, class Lay, class Src = SmemIO, class Dst = SmemIO>
 __device__ __forceinline__ void fft_tile(C* sm, const C* tw, const Src& src = Src(), const Dst& dst = Dst()) {
     static_assert(smooth235(L), "FFT length must be a product of 2, 3 and 5");
-    stockham_chain<C, L, 1, NB, NT, DIR, Lay, Src, Dst>(sm, tw, src, dst);
+    stockham_range<C, L, NB, NT, DIR, Lay, false, plan_len(L), 0, 1, Src, Dst>(sm, tw, src, dst);
 }
 
 // shared-memory to shared-memory transform with lines fastest (LS >= NB)

@@ -73,20 +73,31 @@ template <class T, int L> struct MvTiles {
     static constexpr int TLY = clamp_pow2(SMEM_Y / (L * S), 32 / S > 2 ? 32 / S : 2, 32);
     static constexpr int TLZ = clamp_pow2(SMEM_Z / (6 * L * S), 32 / S > 2 ? 32 / S : 2, 16);
     static constexpr int NBX = 3 * TLX, NBY = TLY, NBZ = 6 * TLZ;
-    static constexpr int LP = L + 1;  // padded line stride of the x-pass tile
-    static constexpr int PSY = NBY + 1, PSZ = NBZ + 1;  // padded point strides (odd) of the y and z tiles
+    // x tile: points contiguous with one pad word every 16, line pitch = 8 (mod 16)
+    static constexpr int lpitch() {
+        int p = L + L / 16 + 1;
+        while (p % 16 != 8) p++;
+        return p;
+    }
+    static constexpr int LP = lpitch();
+    // y tile: odd point stride; z tile: point stride NBZ = 24 = 8 (mod 16) with
+    // one pad point every 16
+    static constexpr int PSY = NBY + 1, PSZ = NBZ;
+    using LayX = Layout<1, LP, false, 4>;
+    using LayZ = Layout<PSZ, 1, true, 4>;
     // one butterfly of the widest radix per thread
     static constexpr int nthreads(int nb) {
         int t = nb * L / max_radix(L);
         t = (t + 31) / 32 * 32;
-        return t < 64 ? 64 : (t > 256 ? 256 : t);
+        return t < 64 ? 64 : (t > 512 ? 512 : t);
     }
     static constexpr int NTX = nthreads(NBX), NTY = nthreads(NBY), NTZ = nthreads(NBZ);
+    static constexpr int MINBZ = 1;  // minimum resident blocks asked of the compiler for zconv
     static constexpr size_t smem_x = (size_t)L * S + (size_t)NBX * LP * S;
     static constexpr size_t smem_y = (size_t)L * S + (size_t)L * PSY * S;
     // twiddles, the data tile, then the compressed spectrum of the block:
     // 6 components x (L/2 + 1) z planes x TLZ columns
-    static constexpr size_t smem_z = (size_t)L * S + (size_t)L * PSZ * S + (size_t)6 * (L / 2 + 1) * TLZ * S;
+    static constexpr size_t smem_z = (size_t)L * S + (size_t)LayZ::span(L) * PSZ * S + (size_t)6 * (L / 2 + 1) * TLZ * S;
 };
 
 // asynchronous global -> shared copy of one complex element (8 or 16 bytes)
@@ -164,7 +175,7 @@ __global__ void __launch_bounds__(MvTiles<T, L>::NTX) k_fwd_x(const MvArgs<T> a)
     load_twiddles<C, L, NT>(tw, a.twx);
     FwdXLoad<T, TAB> src{&a, a.x + rhs * a.xstride, (long)k * nx * ny + (long)j0 * nx, nl, TL};
     B1RowIO<T, L, TL> dst{a.B1 + rhs * a.g.b1_rhs, nl, nz, ny, k, j0};
-    fft_tile<C, L, NB, NT, +1, Layout<1, TT::LP, false>>(sm, tw, src, dst);
+    fft_tile<C, L, NB, NT, +1, typename TT::LayX>(sm, tw, src, dst);
 }
 
 // ---- pass 2 and 4 ---------------------------------------------------------
@@ -239,74 +250,128 @@ template <class T> struct ZStore {
     }
 };
 
-template <class T, int L>
-__global__ void __launch_bounds__(MvTiles<T, L>::NTZ) k_zconv(const MvArgs<T> a) {
+// Forward z transform (passes 0 .. n-2 of the plan), then in registers: the
+// last forward pass, the 3x3 multiply and the first pass of the inverse
+// transform run on the reversed plan, so the inverse starts from the values
+// the forward one ended with (its pass 0 reads exactly the points
+// j + r L/R the forward last pass produced), then inverse passes 1 .. n-1.
+template <class T, int L, class TT = MvTiles<T, L>>
+__global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a) {
     using C = cplx<T>;
-    using TT = MvTiles<T, L>;
+    using LZ = typename TT::LayZ;
     constexpr int TL = TT::TLZ, NB = TT::NBZ, NT = TT::NTZ;
+    constexpr int NP = plan_len(L);
+    constexpr int RK = plan_radix(L, NP - 1);  // last forward radix = first inverse radix
+    constexpr int NJ = L / RK;                 // butterflies per line in that pass
+    constexpr int NG = 2 * TL * NJ;            // (row half, column, butterfly) groups
+    constexpr int PERM = (NG + NT - 1) / NT;
+    constexpr int NQ = L / 2 + 1;
     const int rhs = blockIdx.z;
     if (a.status && a.status[rhs]) return;
     C* tw = smem_base<C>();
     C* sm = tw + L;
+    C* gs = sm + LZ::span(L) * TT::PSZ;
     const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz, X = a.g.X, Y = a.g.Y;
     const int i0 = blockIdx.x * TL;
-    const int qy = blockIdx.y;                       // 0 .. ny
-    const int two = (qy > 0 && qy < ny) ? 2 : 1;     // rows qy and Y - qy
+    const int qy = blockIdx.y;                    // 0 .. ny
+    const int two = (qy > 0 && qy < ny) ? 2 : 1;  // rows qy and Y - qy
     load_twiddles<C, L, NT>(tw, a.twz);
-    // start copying this block's slice of the compressed spectrum (qy fixed,
-    // every qz, the TL columns qx(i)) into shared memory; it lands while the
-    // forward z transform runs
-    constexpr int PS = TT::PSZ;
-    C* gs = sm + L * PS;
-    constexpr int NQ = L / 2 + 1;
+    // this block's slice of the compressed spectrum (qy fixed, every qz, the
+    // TL columns qx(i)) is copied into shared memory while the forward
+    // transform runs
     const long gcs = a.g.gc_comp;
     for (int e = threadIdx.x; e < 6 * NQ * TL; e += NT) {
         const int il = e % TL, cq = e / TL;
         const int c6 = cq / NQ, qz = cq - c6 * NQ;
         const int i = min(i0 + il, X - 1);
         const int qxc = i <= nx ? i : X - i;
-        const C* src = a.Gc + c6 * gcs + ((long)qz * (ny + 1) + qy) * (nx + 1) + qxc;
-        cp_async_elem(gs + e, src);
+        cp_async_elem(gs + e, a.Gc + c6 * gcs + ((long)qz * (ny + 1) + qy) * (nx + 1) + qxc);
     }
     cp_async_commit();
     C* B2 = a.B2 + rhs * a.g.b2_rhs;
     const long rs = (long)Y * X, comp = (long)nz * Y * X;
     const long row0 = (long)qy * X, row1 = (long)(Y - qy) * X;
-    fft_tile<C, L, NB, NT, +1, Layout<PS, 1, true>>(sm, tw, ZLoad<T>{B2, rs, comp, row0, row1, X, i0, TL, two},
-                                                    SmemIO{});
+    const ZLoad<T> zload{B2, rs, comp, row0, row1, X, i0, TL, two};
+    const ZStore<T> zstore{B2, rs, comp, row0, row1, X, i0, TL, two};
+    if constexpr (NP > 1) stockham_range<C, L, NB, NT, +1, LZ, false, NP - 1, 0, 1>(sm, tw, zload, SmemIO{});
     cp_async_wait_all();
     __syncthreads();
-    // 3x3 symmetric multiply with the compressed spectrum; the mirror row
-    // uses the same values with the sign of the y-odd components flipped
-    for (int e = threadIdx.x; e < TL * L; e += NT) {
-        const int p = e / TL, il = e - p * TL;
-        const int i = i0 + il;
-        if (i >= X) continue;
-        const T sx = i <= nx ? (T)1 : (T)-1;
-        const int qzc = p <= nz ? p : L - p;
-        const T sz = p <= nz ? (T)1 : (T)-1;
-        const C* gq = gs + qzc * TL + il;
-        const C gxx = gq[0];
-        const C gxy = cscale(gq[NQ * TL], sx);
-        const C gxz = cscale(gq[2 * NQ * TL], sx * sz);
-        const C gyy = gq[3 * NQ * TL];
-        const C gyz = cscale(gq[4 * NQ * TL], sz);
-        const C gzz = gq[5 * NQ * TL];
+    // ---- fused middle: read, transform, multiply, transform (registers) ----
+    C v[PERM][3][RK];
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            if (h >= two) break;
+    for (int q = 0; q < PERM; q++) {
+        const int g = threadIdx.x + q * NT;
+        if (!(PERM * NT == NG || g < NG)) continue;
+        const int il = g % TL, j = (g / TL) % NJ, h = g / (TL * NJ);
+        const int i = i0 + il;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const int b = (h * 3 + c) * TL + il;
+#pragma unroll
+            for (int r = 0; r < RK; r++) {
+                const int p = j + r * NJ;
+                if constexpr (NP == 1) {
+                    v[q][c][r] = (2 * p >= L) ? czero<C>() : zload.template load<C>(b, p);
+                } else {
+                    v[q][c][r] = sm[LZ::addr(p, b)];
+                }
+            }
+            if constexpr (NJ > 1) {
+                // forward last pass: Ns = NJ, k = j, twiddle w^(j r)
+#pragma unroll
+                for (int r = 1; r < RK; r++) v[q][c][r] = cmul(v[q][c][r], tw[j * r]);
+            }
+            Dft<RK, +1, C>::run(v[q][c]);
+        }
+        if (h < two && i < X) {
+            const T sx = i <= nx ? (T)1 : (T)-1;
             const T sy = h ? (T)-1 : (T)1;
-            const C hxy = cscale(gxy, sy), hyz = cscale(gyz, sy);
-            C* row = sm + p * PS + h * 3 * TL + il;
-            const C vx = row[0], vy = row[TL], vz = row[2 * TL];
-            row[0] = cadd(cadd(cmul(gxx, vx), cmul(hxy, vy)), cmul(gxz, vz));
-            row[TL] = cadd(cadd(cmul(hxy, vx), cmul(gyy, vy)), cmul(hyz, vz));
-            row[2 * TL] = cadd(cadd(cmul(gxz, vx), cmul(hyz, vy)), cmul(gzz, vz));
+#pragma unroll
+            for (int r = 0; r < RK; r++) {
+                const int p = j + r * NJ;  // spectral index of this output
+                const int qzc = p <= nz ? p : L - p;
+                const T sz = p <= nz ? (T)1 : (T)-1;
+                const C* gq = gs + qzc * TL + il;
+                const C gxx = gq[0];
+                const C gxy = cscale(gq[NQ * TL], sx * sy);
+                const C gxz = cscale(gq[2 * NQ * TL], sx * sz);
+                const C gyy = gq[3 * NQ * TL];
+                const C gyz = cscale(gq[4 * NQ * TL], sy * sz);
+                const C gzz = gq[5 * NQ * TL];
+                const C vx = v[q][0][r], vy = v[q][1][r], vz = v[q][2][r];
+                v[q][0][r] = cadd(cadd(cmul(gxx, vx), cmul(gxy, vy)), cmul(gxz, vz));
+                v[q][1][r] = cadd(cadd(cmul(gxy, vx), cmul(gyy, vy)), cmul(gyz, vz));
+                v[q][2][r] = cadd(cadd(cmul(gxz, vx), cmul(gyz, vy)), cmul(gzz, vz));
+            }
+        }
+        // inverse pass 0 of the reversed plan: Ns = 1, inputs j + r NJ, no twiddles
+#pragma unroll
+        for (int c = 0; c < 3; c++) Dft<RK, -1, C>::run(v[q][c]);
+    }
+    if constexpr (NP > 1) __syncthreads();  // every read of the tile is done
+#pragma unroll
+    for (int q = 0; q < PERM; q++) {
+        const int g = threadIdx.x + q * NT;
+        if (!(PERM * NT == NG || g < NG)) continue;
+        const int il = g % TL, j = (g / TL) % NJ, h = g / (TL * NJ);
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const int b = (h * 3 + c) * TL + il;
+#pragma unroll
+            for (int r = 0; r < RK; r++) {
+                const int o = j * RK + r;
+                if constexpr (NP == 1) {
+                    if (2 * o < L) zstore.template store<C>(b, o, v[q][c][r]);
+                } else {
+                    sm[LZ::addr(o, b)] = v[q][c][r];
+                }
+            }
         }
     }
-    __syncthreads();
-    fft_tile<C, L, NB, NT, -1, Layout<PS, 1, true>>(sm, tw, SmemIO{},
-                                                    ZStore<T>{B2, rs, comp, row0, row1, X, i0, TL, two});
+    if constexpr (NP > 1) {
+        __syncthreads();
+        stockham_range<C, L, NB, NT, -1, LZ, true, NP, 1, RK>(sm, tw, SmemIO{}, zstore);
+    }
 }
 
 // ---- pass 5 -----------------------------------------------------------------
@@ -347,7 +412,7 @@ __global__ void __launch_bounds__(MvTiles<T, L>::NTX) k_inv_x(const MvArgs<T> a,
     B1RowIO<T, L, TL> src{a.B1 + rhs * a.g.b1_rhs, nl, nz, ny, k, j0};
     InvXStore<T, TAB> dst{&a, a.b + rhs * a.xstride, a.y + rhs * a.xstride, (long)k * nx * ny + (long)j0 * nx, nl,
                           TL};
-    fft_tile<C, L, NB, NT, -1, Layout<1, TT::LP, false>>(sm, tw, src, dst);
+    fft_tile<C, L, NB, NT, -1, typename TT::LayX>(sm, tw, src, dst);
     (void)epi;
 }
 
