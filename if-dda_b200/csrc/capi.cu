@@ -1,6 +1,10 @@
 // C-ABI of libifdda_gpu.so (declarations and reference seams: include/ifdda_gpu.h).
+#include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <memory>
+#include <thread>
+#include <vector>
 #include <string>
 #include "../../include/ifdda_gpu.h"
 #include "post.cuh"
@@ -47,19 +51,45 @@ struct DeviceScope {
 // A polarisability is stored compactly when every dipole's tensor is the
 // same complex number times the identity (every object of the reference
 // built with trope = 'iso').
-int pola_mode(const ifdda_dcmplx* pol, int nb, long nmax) {
-    for (long i = 0; i < nb; i++) {
+bool pola_iso_range(const ifdda_dcmplx* pol, long i0, long i1, long nmax, const std::atomic<bool>& stop) {
+    for (long i = i0; i < i1; i++) {
+        if ((i & 4095) == 0 && stop.load(std::memory_order_relaxed)) return false;
         const ifdda_dcmplx d0 = pol[i];
         for (int a = 0; a < 3; a++)
             for (int b = 0; b < 3; b++) {
                 const ifdda_dcmplx v = pol[i + nmax * (a + 3 * b)];
                 if (a == b) {
-                    if (v.re != d0.re || v.im != d0.im) return ALPHA_FULL;
+                    if (v.re != d0.re || v.im != d0.im) return false;
                 } else if (v.re != 0.0 || v.im != 0.0) {
-                    return ALPHA_FULL;
+                    return false;
                 }
             }
     }
+    return true;
+}
+
+// The scan reads 9 * nb complex numbers of host memory; large objects are
+// split over host threads (one chunk of at least 64K dipoles each).
+int pola_mode(const ifdda_dcmplx* pol, int nb, long nmax) {
+    constexpr long CHUNK = 65536;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nt = (int)std::min<long>({(long)hw, 16L, std::max(1L, (nb + CHUNK - 1) / CHUNK)});
+    std::atomic<bool> stop{false};
+    if (nt == 1) return pola_iso_range(pol, 0, nb, nmax, stop) ? ALPHA_ISO : ALPHA_FULL;
+    std::vector<std::thread> th;
+    std::vector<char> iso(nt, 1);
+    const long per = (nb + nt - 1) / nt;
+    for (int t = 0; t < nt; t++)
+        th.emplace_back([&, t] {
+            const long i0 = t * per, i1 = std::min<long>(nb, i0 + per);
+            if (i0 < i1 && !pola_iso_range(pol, i0, i1, nmax, stop)) {
+                iso[t] = 0;
+                stop.store(true, std::memory_order_relaxed);
+            }
+        });
+    for (auto& x : th) x.join();
+    for (int t = 0; t < nt; t++)
+        if (!iso[t]) return ALPHA_FULL;
     return ALPHA_ISO;
 }
 
@@ -380,28 +410,29 @@ int ifdda_inverserig_batch(ifdda_green* g, int nrhs, int nbsphere, int nmax, con
     if (nmax < nbsphere) throw EngineError{1, "nmax smaller than nbsphere"};
     const long n3 = 3L * nbsphere, tot = n3 * nrhs;
     const int* tab = nullptr;
+    if (tabdip) check_tabdip(tabdip, geo.N, nbsphere);
+    // the incident field goes first, so that its copy overlaps the host scan
+    // of the polarisability below (when FF0 is pinned)
+    g->ff0.ensure(tot);
+    g->x.ensure(tot);
+    g->ffb.ensure(tot);
+    IFDDA_CUDA(cudaMemcpyAsync(g->ff0.p, FF0, tot * sizeof(double2), cudaMemcpyHostToDevice, st));
     if (tabdip) {
-        check_tabdip(tabdip, geo.N, nbsphere);
         g->tab.ensure(geo.N);
         IFDDA_CUDA(cudaMemcpyAsync(g->tab.p, tabdip, geo.N * sizeof(int), cudaMemcpyHostToDevice, st));
         tab = g->tab.p;
     }
     const int amode = pola_mode(polarisa, nbsphere, nmax);
     if (amode == ALPHA_ISO) {
-        std::vector<double2> h(nbsphere);
-        for (int i = 0; i < nbsphere; i++) h[i] = make_double2(polarisa[i].re, polarisa[i].im);
+        // the isotropic value of dipole i is polarisa(i,1,1): the first nb
+        // entries of the (nmax,3,3) array, contiguous
         g->alpha.ensure(nbsphere);
-        IFDDA_CUDA(cudaMemcpyAsync(g->alpha.p, h.data(), nbsphere * sizeof(double2), cudaMemcpyHostToDevice, st));
-        IFDDA_CUDA(cudaStreamSynchronize(st));
+        IFDDA_CUDA(cudaMemcpyAsync(g->alpha.p, polarisa, nbsphere * sizeof(double2), cudaMemcpyHostToDevice, st));
     } else {
         g->alpha.ensure((size_t)9 * nmax);
         IFDDA_CUDA(cudaMemcpyAsync(g->alpha.p, polarisa, (size_t)9 * nmax * sizeof(double2), cudaMemcpyHostToDevice,
                                    st));
     }
-    g->ff0.ensure(tot);
-    g->x.ensure(tot);
-    g->ffb.ensure(tot);
-    IFDDA_CUDA(cudaMemcpyAsync(g->ff0.p, FF0, tot * sizeof(double2), cudaMemcpyHostToDevice, st));
     const int rc = solve_device(g, nrhs, nbsphere, nmax, tab, g->alpha.p, amode, g->ff0.p, methodeit, tol, g->ffb.p,
                                 g->x.p, tol1, nloop, ncompte, nstop, infostr, opt);
     IFDDA_CUDA(cudaMemcpyAsync(FFloc, g->x.p, tot * sizeof(double2), cudaMemcpyDeviceToHost, st));

@@ -65,14 +65,23 @@ template <class T> struct MvArgs {
     T inv_m;             // 1 / (X Y Z)
 };
 
-// Tile shapes: lines per block and threads per block for each pass.
+// Tile shapes: lines per block, threads per block and the register cap of
+// each pass.  The rules come from a sweep of every pass over tile widths,
+// thread counts and register caps on B200 at the 128^3 (FP32, FP64),
+// 192x192x128 (8 right-hand sides) and 384^3 grids:
+//  * x passes: latency-bound at small grids (every shape within 5%); a cap of
+//    80 (FP32) / 96 (FP64) registers helps the larger grids;
+//  * y passes: 16 columns per block (64 contiguous bytes per row in FP32) at
+//    every length, about 30% faster than narrower tiles at 192 and 384;
+//  * zconv: as many columns as fit in ~80 KB (FP32) / ~160 KB (FP64) of
+//    shared memory, so that two blocks (FP32) share an SM, and a register
+//    cap near 72 (FP32) / 168 (FP64) to keep more blocks resident.
 template <class T, int L> struct MvTiles {
     static constexpr int S = (int)sizeof(cplx<T>);
-    static constexpr int SMEM_X = 16384, SMEM_Y = 16384, SMEM_Z = 24576 * (S / 8);
+    static constexpr int SMEM_X = 16384;
     static constexpr int TLX = clamp_pow2(SMEM_X / (3 * (L + 1) * S), 1, 16);
-    static constexpr int TLY = clamp_pow2(SMEM_Y / (L * S), 32 / S > 2 ? 32 / S : 2, 32);
-    static constexpr int TLZ = clamp_pow2(SMEM_Z / (6 * L * S), 32 / S > 2 ? 32 / S : 2, 16);
-    static constexpr int NBX = 3 * TLX, NBY = TLY, NBZ = 6 * TLZ;
+    static constexpr int TLY = 16;
+    static constexpr int NBX = 3 * TLX, NBY = TLY;
     // x tile: points contiguous with one pad word every 16, line pitch = 8 (mod 16)
     static constexpr int lpitch() {
         int p = L + L / 16 + 1;
@@ -80,24 +89,42 @@ template <class T, int L> struct MvTiles {
         return p;
     }
     static constexpr int LP = lpitch();
-    // y tile: odd point stride; z tile: point stride NBZ = 24 = 8 (mod 16) with
-    // one pad point every 16
-    static constexpr int PSY = NBY + 1, PSZ = NBZ;
-    using LayX = Layout<1, LP, false, 4>;
-    using LayZ = Layout<PSZ, 1, true, 4>;
     // one butterfly of the widest radix per thread
     static constexpr int nthreads(int nb) {
         int t = nb * L / max_radix(L);
         t = (t + 31) / 32 * 32;
         return t < 64 ? 64 : (t > 512 ? 512 : t);
     }
+    // blocks per SM asked of the compiler so that it keeps to about cap registers
+    static constexpr int minblocks(int nt, int cap) {
+        int m = 65536 / (nt * cap);
+        if (m * nt > 2048) m = 2048 / nt;
+        return m < 1 ? 1 : (m > 32 ? 32 : m);
+    }
+    // z tile: shared memory of TL columns (twiddles, data tile with one pad
+    // point every 16, the block's slice of the compressed spectrum)
+    static constexpr size_t zbytes(int tl) {
+        return (size_t)L * S + (size_t)(L + (L >> 4)) * 6 * tl * S + (size_t)6 * (L / 2 + 1) * tl * S;
+    }
+    static constexpr int ztile() {
+        int tl = 16;
+        while (tl > 1 && zbytes(tl) > (size_t)80 * 1024 * (S / 8)) tl /= 2;
+        return tl;
+    }
+    static constexpr int TLZ = ztile(), NBZ = 6 * TLZ;
+    // y tile: odd point stride; z tile: point stride NBZ with one pad point every 16
+    static constexpr int PSY = NBY + 1, PSZ = NBZ;
+    using LayX = Layout<1, LP, false, 4>;
+    using LayY = Layout<PSY, 1, true>;
+    using LayZ = Layout<PSZ, 1, true, 4>;
     static constexpr int NTX = nthreads(NBX), NTY = nthreads(NBY), NTZ = nthreads(NBZ);
-    static constexpr int MINBZ = 1;  // minimum resident blocks asked of the compiler for zconv
+    static constexpr int MINBX = minblocks(NTX, S == 8 ? 80 : 96);
+    static constexpr int MINBY = minblocks(NTY, S == 8 ? 80 : 112);
+    static constexpr int MINBZ = minblocks(NTZ, S == 8 ? 72 : 168);
     static constexpr size_t smem_x = (size_t)L * S + (size_t)NBX * LP * S;
     static constexpr size_t smem_y = (size_t)L * S + (size_t)L * PSY * S;
-    // twiddles, the data tile, then the compressed spectrum of the block:
-    // 6 components x (L/2 + 1) z planes x TLZ columns
     static constexpr size_t smem_z = (size_t)L * S + (size_t)LayZ::span(L) * PSZ * S + (size_t)6 * (L / 2 + 1) * TLZ * S;
+    static_assert(zbytes(TLZ) == smem_z, "z tile size rule and layout disagree");
 };
 
 // asynchronous global -> shared copy of one complex element (8 or 16 bytes)
@@ -160,10 +187,9 @@ template <class T, int L, int TL> struct B1RowIO {
     }
 };
 
-template <class T, int L, bool TAB>
-__global__ void __launch_bounds__(MvTiles<T, L>::NTX) k_fwd_x(const MvArgs<T> a) {
+template <class T, int L, bool TAB, class TT = MvTiles<T, L>>
+__global__ void __launch_bounds__(TT::NTX, TT::MINBX) k_fwd_x(const MvArgs<T> a) {
     using C = cplx<T>;
-    using TT = MvTiles<T, L>;
     constexpr int TL = TT::TLX, NB = TT::NBX, NT = TT::NTX;
     const int rhs = blockIdx.z;
     if (a.status && a.status[rhs]) return;
@@ -199,10 +225,9 @@ template <class T, int DIR> struct YStore {
     }
 };
 
-template <class T, int L, int DIR>
-__global__ void __launch_bounds__(MvTiles<T, L>::NTY) k_pass_y(const MvArgs<T> a) {
+template <class T, int L, int DIR, class TT = MvTiles<T, L>>
+__global__ void __launch_bounds__(TT::NTY, TT::MINBY) k_pass_y(const MvArgs<T> a) {
     using C = cplx<T>;
-    using TT = MvTiles<T, L>;
     constexpr int TL = TT::TLY, NT = TT::NTY;
     const int rhs = blockIdx.z / 3, c = blockIdx.z - 3 * (blockIdx.z / 3);
     if (a.status && a.status[rhs]) return;
@@ -217,7 +242,7 @@ __global__ void __launch_bounds__(MvTiles<T, L>::NTY) k_pass_y(const MvArgs<T> a
     C* dstb = DIR > 0 ? a.B2 + rhs * a.g.b2_rhs : a.B1 + rhs * a.g.b1_rhs;
     YLoad<T, DIR> src{srcb + ((long)c * nz + k) * rows_in * X, X, i0};
     YStore<T, DIR> dst{dstb + ((long)c * nz + k) * rows_out * X, X, i0};
-    fft_tile<C, L, TL, NT, DIR, Layout<TT::PSY, 1, true>>(sm, tw, src, dst);
+    fft_tile<C, L, TL, NT, DIR, typename TT::LayY>(sm, tw, src, dst);
 }
 
 // ---- pass 3 -----------------------------------------------------------------
@@ -396,10 +421,9 @@ template <class T, bool TAB> struct InvXStore {
     }
 };
 
-template <class T, int L, bool TAB, class Epi>
-__global__ void __launch_bounds__(MvTiles<T, L>::NTX) k_inv_x(const MvArgs<T> a, const Epi epi) {
+template <class T, int L, bool TAB, class Epi, class TT = MvTiles<T, L>>
+__global__ void __launch_bounds__(TT::NTX, TT::MINBX) k_inv_x(const MvArgs<T> a, const Epi epi) {
     using C = cplx<T>;
-    using TT = MvTiles<T, L>;
     constexpr int TL = TT::TLX, NB = TT::NBX, NT = TT::NTX;
     const int rhs = blockIdx.z;
     if (a.status && a.status[rhs]) return;

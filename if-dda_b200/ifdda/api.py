@@ -173,16 +173,29 @@ class GreenSpectrum:
 
     def inverserig(self, nbsphere, polarisa, nmax, FF0, methodeit="GPBICG1", tol=1e-4, tabdip=None,
                    precision=IFDDA_FP64, check_every=0, max_outer=0, inner_floor=0.0, nstop_in=0,
-                   maxit=0) -> SolveResult:
+                   maxit=0, out=None) -> SolveResult:
         """Rigorous solve (inverserig / inverserigopt) for one or a batch of
-        right-hand sides.  FF0: (3*nbsphere,) or (nrhs, 3*nbsphere)."""
+        right-hand sides.  FF0: (3*nbsphere,) or (nrhs, 3*nbsphere).
+
+        out: optional (FF, FFloc) pair of C-contiguous complex128 arrays of
+        FF0's shape that receive the fields (e.g. pinned buffers reused from
+        call to call, like the reference's own FF / FFloc arrays); new arrays
+        are allocated otherwise."""
         ff0 = _zc(FF0)
         single = ff0.ndim == 1
         ff0 = ff0.reshape(-1, 3 * nbsphere)
         nrhs = ff0.shape[0]
         pol = _zc(polarisa)
-        FF = np.zeros_like(ff0)
-        FFloc = np.zeros_like(ff0)
+        if out is None:
+            FF = np.zeros_like(ff0)
+            FFloc = np.zeros_like(ff0)
+        else:
+            FF, FFloc = out
+            for a in (FF, FFloc):
+                if a.dtype != np.complex128 or not a.flags.c_contiguous or a.size != ff0.size:
+                    raise ValueError("out arrays must be C-contiguous complex128 of FF0's size")
+            FF = FF.reshape(ff0.shape)
+            FFloc = FFloc.reshape(ff0.shape)
         tol1 = np.zeros(nrhs)
         nloop = np.zeros(nrhs, np.int32)
         ncompte = np.zeros(nrhs, np.int32)
