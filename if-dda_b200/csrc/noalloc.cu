@@ -3,8 +3,8 @@
 // Some callers cannot call cudaMalloc while they solve: a real-time loop that
 // must not hit the device-wide synchronisation cudaMalloc/cudaFree imply, a
 // host framework whose own caching allocator owns the device memory and must
-// not be bypassed, or code that runs while a CUDA graph is being captured
-// (allocation calls are not allowed there).  ifdda_matvec_device needs B1/B2
+// not be bypassed, or an application that has handed its whole device memory
+// budget to another library.  ifdda_matvec_device needs B1/B2
 // scratch and grows it from the device memory pool on first use; this variant runs the
 // same five mat-vec kernels with their scratch in one fixed device array of
 // this file instead.

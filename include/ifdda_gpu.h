@@ -84,8 +84,8 @@ int ifdda_matvec_device(ifdda_green* g, int precision, int nrhs, int ndip, const
 /* Same operation as ifdda_matvec_device for one right-hand side, for callers
    that cannot allocate device memory while they run: a real-time loop that
    must avoid the device-wide synchronisation of cudaMalloc/cudaFree, a
-   framework whose own caching allocator owns the GPU memory, or code running
-   under CUDA stream capture.  It has no counterpart in the reference (whose
+   framework whose own caching allocator owns the GPU memory, or a host
+   application that has handed its whole memory budget to another library.  It has no counterpart in the reference (whose
    buffers are static Fortran arrays).  The mat-vec scratch lives in one fixed
    16 MiB device array inside the library (held by every GPU that loads it
    until the process exits), so 18*nx*ny*nz complex values of the chosen

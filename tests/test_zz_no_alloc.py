@@ -3,8 +3,8 @@ allocating one (ifdda_matvec_device).
 
 Callers that cannot allocate device memory while they run (a real-time loop
 avoiding cudaMalloc's device-wide synchronisation, a framework whose caching
-allocator owns the GPU memory, code under stream capture) use the entry point
-whose scratch is a fixed array inside the library.  Both entry points run the
+allocator owns the GPU memory, an application whose memory budget is spoken
+for) use the entry point whose scratch is a fixed array inside the library.  Both entry points run the
 same kernels, so the results must agree within the FP64/FP32 tolerances of the
 parity tests (1e-11 / 2e-5 relative); two calls in a row check that the shared
 array left by the first call does not change the second.  This file is named
