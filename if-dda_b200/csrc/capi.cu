@@ -226,10 +226,13 @@ int ifdda_ctx_create(int device, ifdda_ctx** out) {
     return 0;
 }
 
-int ifdda_ctx_destroy(ifdda_ctx* ctx) {
-    if (!ctx) return 0;
-    {
-        DeviceScope ds(ctx->device);
+namespace {
+// Frees the context's buffers and stream.  Never throws: destroy calls come
+// from finalisers and exit paths.
+void ctx_free(ifdda_ctx* ctx) {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(ctx->device) == cudaSuccess) {
         {
             AllocStreamScope as(ctx->stream);
             ctx->flag.release();
@@ -242,8 +245,20 @@ int ifdda_ctx_destroy(ifdda_ctx* ctx) {
             cudaStreamSynchronize(ctx->stream);
             cudaStreamDestroy(ctx->stream);
         }
+        if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     }
     delete ctx;
+}
+}  // namespace
+
+int ifdda_ctx_destroy(ifdda_ctx* ctx) {
+    if (!ctx) return 0;
+    if (ctx->live_greens > 0) {
+        // spectra still use the stream: the last ifdda_green_destroy frees it
+        ctx->closing = true;
+        return 0;
+    }
+    ctx_free(ctx);
     return 0;
 }
 
@@ -268,20 +283,28 @@ int ifdda_green_create(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube,
     IFDDA_GUARD_BEGIN
     DeviceScope ds(ctx->device);
     AllocStreamScope as(ctx->stream);
+    if (ctx->closing) throw EngineError{1, "context already destroyed"};
     green_build(g->G, nx, ny, nz, aretecube, k0, ctx->stream);
     *out = g.release();
+    ctx->live_greens++;
     return 0;
     IFDDA_GUARD_END(ctx, nullptr)
 }
 
 int ifdda_green_destroy(ifdda_green* g) {
     if (!g) return 0;
-    {
-        DeviceScope ds(g->ctx->device);
-        AllocStreamScope as(g->ctx->stream);
-        cudaStreamSynchronize(g->ctx->stream);
+    ifdda_ctx* ctx = g->ctx;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(ctx->device) == cudaSuccess) {
+        AllocStreamScope as(ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+        delete g;
+        if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
+    } else {
         delete g;
     }
+    if (--ctx->live_greens == 0 && ctx->closing) ctx_free(ctx);
     return 0;
 }
 

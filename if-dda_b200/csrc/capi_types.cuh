@@ -14,6 +14,10 @@ struct ifdda_ctx {
     ifdda::DevBuf<unsigned> tickets;
     ifdda::DevBuf<ifdda::KState> st;
     ifdda::DevBuf<int> zstatus;
+    // spectra created on this context and not yet destroyed; a destroy
+    // request while some are alive is carried out by the last one's destroy
+    int live_greens = 0;
+    bool closing = false;
 };
 
 struct ifdda_green {

@@ -237,12 +237,31 @@ struct SmemIO {
 template <int PS_, int BS_, bool BFAST_, int PADSH_ = 0> struct Layout {
     static constexpr int PS = PS_, BS = BS_, PADSH = PADSH_;
     static constexpr bool BFAST = BFAST_;
-    __device__ __forceinline__ static int addr(int p, int b) {
-        return (PADSH ? p + (p >> PADSH) : p) * PS + b * BS;
-    }
+    // padded position of point p
+    __host__ __device__ static constexpr int pidx(int p) { return PADSH ? p + (p >> PADSH) : p; }
+    __device__ __forceinline__ static int addr(int p, int b) { return pidx(p) * PS + b * BS; }
     // points spanned by a line of length L (padding included)
     static constexpr int span(int L) { return PADSH ? L + (L >> PADSH) : L; }
 };
+
+// True when the padded positions of a butterfly's points j + r NJ (j < NJ,
+// r < R) are pidx(j) + pidx(r NJ): the shared-memory address of every point
+// is then the thread's base address plus a compile-time offset.
+template <class Lay> constexpr bool read_split(int NJ, int R) {
+    for (int j = 0; j < NJ; j++)
+        for (int r = 0; r < R; r++)
+            if (Lay::pidx(j + r * NJ) - Lay::pidx(j) != Lay::pidx(r * NJ)) return false;
+    return true;
+}
+// The same for the outputs d + r Ns, d = (j / Ns) Ns R + j mod Ns, of a pass.
+template <class Lay> constexpr bool write_split(int NJ, int Ns, int R) {
+    for (int j = 0; j < NJ; j++) {
+        const int d = (j / Ns) * Ns * R + j % Ns;
+        for (int r = 0; r < R; r++)
+            if (Lay::pidx(d + r * Ns) - Lay::pidx(d) != Lay::pidx(r * Ns)) return false;
+    }
+    return true;
+}
 
 // One Stockham pass.  tw[j] = exp(+2 pi i j / L) in shared memory.
 template <class C, int L, int R, int Ns, int NB, int NT, int DIR, class Lay, class Src, class Dst>
@@ -253,6 +272,7 @@ __device__ __forceinline__ void stockham_pass(C* sm, const C* tw, const Src& src
     constexpr int TSTEP = L / (Ns * R);
     constexpr bool FIRST = Ns == 1, LAST = Ns * R == L;
     constexpr bool GIN = FIRST && Src::GLOBAL, GOUT = LAST && Dst::GLOBAL;
+    constexpr bool RSPLIT = read_split<Lay>(NJ, R), WSPLIT = write_split<Lay>(NJ, Ns, R);
     C v[PER][R];
 #pragma unroll
     for (int q = 0; q < PER; q++) {
@@ -267,6 +287,8 @@ __device__ __forceinline__ void stockham_pass(C* sm, const C* tw, const Src& src
                     // zero upper half: for an even radix p >= L/2 exactly when r >= R/2
                     const bool zero = Src::HALF && (R % 2 == 0 ? 2 * r >= R : 2 * p >= L);
                     v[q][r] = zero ? mk(decltype(C().x)(0), decltype(C().x)(0)) : src.template load<C>(b, p);
+                } else if constexpr (RSPLIT) {
+                    v[q][r] = sm[Lay::addr(j, b) + Lay::pidx(r * NJ) * Lay::PS];
                 } else {
                     v[q][r] = sm[Lay::addr(p, b)];
                 }
@@ -299,6 +321,8 @@ __device__ __forceinline__ void stockham_pass(C* sm, const C* tw, const Src& src
                     // last pass: o = j + r L/R; for an even radix o < L/2 exactly when r < R/2
                     const bool keep = !Dst::HALF || (R % 2 == 0 ? 2 * r < R : 2 * o < L);
                     if (keep) dst.template store<C>(b, o, v[q][r]);
+                } else if constexpr (WSPLIT) {
+                    sm[Lay::addr(d, b) + Lay::pidx(r * Ns) * Lay::PS] = v[q][r];
                 } else {
                     sm[Lay::addr(o, b)] = v[q][r];
                 }

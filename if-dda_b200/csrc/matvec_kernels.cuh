@@ -247,28 +247,28 @@ __global__ void __launch_bounds__(TT::NTY, TT::MINBY) k_pass_y(const MvArgs<T> a
 
 // ---- pass 3 -----------------------------------------------------------------
 // lines b = (h * 3 + c) * TL + il: h = 0 row qy, h = 1 the mirror row Y - qy
-template <class T> struct ZLoad {
+template <class T, int TL> struct ZLoad {
     static constexpr bool GLOBAL = true, HALF = true;  // rows >= nz are padding
     const cplx<T>* B2;
     long rs;  // elements between z rows (Y * X)
     long comp;  // elements between components (nz * Y * X)
     long row0, row1;
-    int X, i0, tl, two;
+    int X, i0, two;
     template <class C> __device__ __forceinline__ C load(int b, int p) const {
-        const int hc = b / tl, il = b - hc * tl;
+        const int hc = b / TL, il = b - hc * TL;
         const int h = hc / 3, c = hc - 3 * h;
         const int i = i0 + il;
         if (i >= X || h >= two) return czero<C>();
         return B2[c * comp + (long)p * rs + (h ? row1 : row0) + i];
     }
 };
-template <class T> struct ZStore {
+template <class T, int TL> struct ZStore {
     static constexpr bool GLOBAL = true, HALF = true;  // keep z rows < nz
     cplx<T>* B2;
     long rs, comp, row0, row1;
-    int X, i0, tl, two;
+    int X, i0, two;
     template <class C> __device__ __forceinline__ void store(int b, int p, C v) const {
-        const int hc = b / tl, il = b - hc * tl;
+        const int hc = b / TL, il = b - hc * TL;
         const int h = hc / 3, c = hc - 3 * h;
         const int i = i0 + il;
         if (i < X && h < two) B2[c * comp + (long)p * rs + (h ? row1 : row0) + i] = v;
@@ -316,8 +316,8 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
     C* B2 = a.B2 + rhs * a.g.b2_rhs;
     const long rs = (long)Y * X, comp = (long)nz * Y * X;
     const long row0 = (long)qy * X, row1 = (long)(Y - qy) * X;
-    const ZLoad<T> zload{B2, rs, comp, row0, row1, X, i0, TL, two};
-    const ZStore<T> zstore{B2, rs, comp, row0, row1, X, i0, TL, two};
+    const ZLoad<T, TL> zload{B2, rs, comp, row0, row1, X, i0, two};
+    const ZStore<T, TL> zstore{B2, rs, comp, row0, row1, X, i0, two};
     if constexpr (NP > 1) stockham_range<C, L, NB, NT, +1, LZ, false, NP - 1, 0, 1>(sm, tw, zload, SmemIO{});
     cp_async_wait_all();
     __syncthreads();
@@ -337,6 +337,8 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
                 const int p = j + r * NJ;
                 if constexpr (NP == 1) {
                     v[q][c][r] = (2 * p >= L) ? czero<C>() : zload.template load<C>(b, p);
+                } else if constexpr (read_split<LZ>(NJ, RK)) {
+                    v[q][c][r] = sm[LZ::addr(j, b) + LZ::pidx(r * NJ) * LZ::PS];
                 } else {
                     v[q][c][r] = sm[LZ::addr(p, b)];
                 }
@@ -354,8 +356,8 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
 #pragma unroll
             for (int r = 0; r < RK; r++) {
                 const int p = j + r * NJ;  // spectral index of this output
-                const int qzc = p <= nz ? p : L - p;
-                const T sz = p <= nz ? (T)1 : (T)-1;
+                const int qzc = 2 * p <= L ? p : L - p;  // nz = L / 2
+                const T sz = 2 * p <= L ? (T)1 : (T)-1;
                 const C* gq = gs + qzc * TL + il;
                 const C gxx = gq[0];
                 const C gxy = cscale(gq[NQ * TL], sx * sy);
@@ -387,6 +389,8 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
                 const int o = j * RK + r;
                 if constexpr (NP == 1) {
                     if (2 * o < L) zstore.template store<C>(b, o, v[q][c][r]);
+                } else if constexpr (write_split<LZ>(NJ, 1, RK)) {
+                    sm[LZ::addr(j * RK, b) + LZ::pidx(r) * LZ::PS] = v[q][c][r];
                 } else {
                     sm[LZ::addr(o, b)] = v[q][c][r];
                 }

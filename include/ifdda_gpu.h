@@ -46,6 +46,9 @@ int ifdda_abi_version(void);
    reference (which has no device); cdmlib's FFTW plan set-up
    (cdmlib/cdmlib.f:1150-1165) is the closest analogue. */
 int ifdda_ctx_create(int device, ifdda_ctx** out);
+/* Releases the context.  If spectra made on it are still alive, the release
+   waits until the last of them is destroyed (they keep using its stream);
+   no new spectrum can be made on it meanwhile. */
 int ifdda_ctx_destroy(ifdda_ctx* ctx);
 const char* ifdda_ctx_last_error(const ifdda_ctx* ctx);
 int ifdda_ctx_synchronize(ifdda_ctx* ctx);

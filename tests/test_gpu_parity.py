@@ -117,7 +117,10 @@ def test_qmr_on_grf_cube_matches_oracle(gctx, orc, n, nlim):
         want = (1, "Converge do not reach!") if ref["tol1"] >= 1e-4 else (ref["nstop"], ref["infostr"].strip())
         assert (r.nstop, r.infostr.strip()) == want
         assert int(r.nloop[0]) == ref["nloop"] and int(r.ncompte[0]) == ref["ncompte"]
-        assert rel(r.FFloc, ref["FFloc"]) < 1e-7
+        # each mat-vec agrees to 1e-11; a stalled recurrence stopped at nlim
+        # amplifies that rounding (FMA contraction differs between builds), so
+        # the unconverged iterate is held to 1e-6 and a converged one to 1e-7
+        assert rel(r.FFloc, ref["FFloc"]) < (1e-7 if ref["tol1"] < 1e-4 else 1e-6)
         g.close()
 
 
@@ -227,3 +230,20 @@ def test_cdmlib_driver_config1_matches_oracle(orc):
     mie_ext, _, _ = orc.mie(2.25, 100e-9, 632.8e-9)
     assert abs(out["Cext"][0] - mie_ext) / mie_ext < 0.06
 
+
+
+def test_context_closed_before_its_spectrum():
+    """A context destroyed while a spectrum made on it is alive (finalisers
+    run in any order) is released by the spectrum's own destroy; neither
+    call may fail or touch freed memory."""
+    import ifdda
+    ctx = ifdda.Context(0)
+    g = ctx.green(4, 4, 4, 10e-9, 1e7)
+    h = g.h
+    ctx.close()
+    assert g.lib.ifdda_green_destroy(h) == 0
+    g.h = None
+    ctx2 = ifdda.Context(0)
+    g2 = ctx2.green(4, 4, 4, 10e-9, 1e7)
+    g2.close()
+    ctx2.close()
