@@ -125,6 +125,11 @@ void green_export(const Green& G, double2* const out[6], cudaStream_t st);
 
 // The five mat-vec passes.  Returns false if a length has no compiled kernel.
 template <class T> bool matvec_launch(const MvArgs<T>& a, int nrhs, bool tab, cudaStream_t st);
+// The same with a solver's input functor in the first x pass and output
+// functor in the last one (gpbicg_fused.cuh); red holds their reductions.
+template <class T, class Pre, class Epi>
+bool matvec_launch_fused(const MvArgs<T>& a, const Pre& pre, const Epi& epi, const MvRed& red, int nrhs, bool tab,
+                         cudaStream_t st);
 
 // fill MvArgs from a Green object and the caller's vectors
 template <class T>

@@ -2,6 +2,7 @@
 // (FP32 inner / FP64 outer) iterative refinement.
 #include <algorithm>
 #include <cmath>
+#include "gpbicg_fused.cuh"
 #include "solver.cuh"
 
 namespace ifdda {
@@ -147,6 +148,24 @@ template <class T> void KrylovWork<T>::ensure(int method, int nrhs_, long n3_) {
 
 template <class T> Slots<T> KrylovWork<T>::slots() const { return Slots<T>{vecs.p, n3, nrhs}; }
 
+// Reduction buffers of the fused mat-vecs: x-pass grids have at most ny x nz
+// blocks per right-hand side; up to 2 partial sums per block from the first
+// x pass, 3 from the last, 5 per row.
+template <class T> MvRed KrylovWork<T>::mv_red(int ny, int nz) {
+    const long rows = (long)nrhs * nz;
+    const long np = rows * ny * 2, ne = rows * ny * 3, nr = rows * 5;
+    mvpart.ensure((size_t)(np + ne + nr));
+    mvtk.ensure((size_t)(rows + nrhs));
+    MvRed r;
+    r.ppart = mvpart.p;
+    r.epart = mvpart.p + np;
+    r.rpart = mvpart.p + np + ne;
+    r.t1 = mvtk.p;
+    r.t2 = mvtk.p + rows;
+    r.gxs = ny;
+    return r;
+}
+
 template <int ND, class Op>
 static void vec_launch(const Op& op, long n3, int nblk, int nrhs, const RedSlots& rs, int* status, cudaStream_t st) {
     count_launch();
@@ -198,12 +217,33 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
     int* status = W.status.p;
     KState* S = W.st.p;
     bool cancelled = false;
+    // GPBiCG with its vector steps folded into the mat-vecs (one element per
+    // x-pass visit needs an isotropic or absent polarisability)
+    const bool fused = sp.method == 1 && sp.fuse && sp.amode != ALPHA_FULL;
+    MvRed red{};
+    if (fused) {
+        red = W.mv_red(G.g.ny, G.g.nz);
+        IFDDA_CUDA(cudaMemsetAsync(W.mvtk.p, 0, W.mvtk.n * sizeof(unsigned), st));
+    }
+    const bool tab = sp.tabdip != nullptr;
+    const cplx<T>* alpha = (const cplx<T>*)sp.alpha;
     // poll at an even number of iterations so a two-iteration graph fits
     const int every = std::max(2, (sp.check_every + 1) / 2 * 2);
     const int methode = sp.method == 3 ? 2 : 1;
     // one iteration; for GPBiCG `par` selects which t buffer is current
     auto iteration = [&](int par) {
-        if (sp.method == 1) {
+        if (fused) {
+            const int tcur = par ? G_TB : G_TA, tnew = par ? G_TA : G_TB;
+            const MvArgs<T> a1 = mv_args<T>(G, nrhs, V.v(G_P, 0), V.v(G_P, 0), V.v(G_AP, 0), n3, sp.amode, alpha,
+                                            sp.nmax, sp.tabdip, status);
+            const MvArgs<T> a2 = mv_args<T>(G, nrhs, V.v(tnew, 0), V.v(tnew, 0), V.v(G_AT, 0), n3, sp.amode, alpha,
+                                            sp.nmax, sp.tabdip, status);
+            if (!matvec_launch_fused<T>(a1, PreGpP<T>{V, S}, EpiGpAlpha<T>{V, S, status}, red, nrhs, tab, st) ||
+                !matvec_launch_fused<T>(a2, PreGpYT<T>{V, S, tcur, tnew}, EpiGpZeta<T>{V, S, status, tnew}, red, nrhs,
+                                        tab, st))
+                throw EngineError{1, "FFT size not supported by the compiled kernels"};
+            vec_launch<2>(GpUpdate<T>{V, S, tcur, tnew}, n3, nblk, nrhs, rs, status, st);
+        } else if (sp.method == 1) {
             const int tcur = par ? G_TB : G_TA, tnew = par ? G_TA : G_TB;
             vec_launch<0>(GpP<T>{V, S}, n3, nblk, nrhs, rs, status, st);
             mv_solver<T>(G, sp, W, G_P, G_AP, status, st);
@@ -247,6 +287,7 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
         mw.ensure(G.g, nrhs);
         const std::vector<const void*> key = {
             V.base, sp.alpha, sp.tabdip, G.gc<T>(), mw.B1.p, mw.B2.p, W.partials.p, W.tickets.p, status, S,
+            W.mvpart.p, W.mvtk.p, (const void*)(long)fused,
             (const void*)(long)sp.method, (const void*)(long)nrhs, (const void*)n3, (const void*)(long)sp.amode,
             (const void*)sp.nmax, (const void*)(long)nblk};
         if (!W.graph.exec || W.graph.key != key) {

@@ -141,10 +141,24 @@ template <class C> __device__ __forceinline__ C* smem_base() {
 }
 
 // ---- pass 1 ---------------------------------------------------------------
-template <class T, bool TAB> struct FwdXLoad {
+// The mat-vec input: Pre::value(e) returns element e = 3 d + c of the vector
+// to multiply.  PreNone reads it; a solver's Pre may instead form it from its
+// own vectors (storing the result) and accumulate ND dot products, which the
+// x pass leaves as per-block partial sums.  value() is called exactly once per
+// element, except with a full polarisability tensor (three calls per
+// element), which only PreNone supports.
+template <class T> struct PreNone {
+    static constexpr int ND = 0;
+    const cplx<T>* x;
+    double2 acc[1];
+    __device__ __forceinline__ void bind(const MvArgs<T>& a, int rhs) { x = a.x + rhs * a.xstride; }
+    template <class C> __device__ __forceinline__ C value(long e) { return x[e]; }
+};
+
+template <class T, bool TAB, class Pre> struct FwdXLoad {
     static constexpr bool GLOBAL = true, HALF = true;  // points p >= nx are the padding
     const MvArgs<T>* a;
-    const cplx<T>* x;
+    mutable Pre pre;
     long site0;
     int nl, tl;
     template <class C> __device__ __forceinline__ C load(int b, int p) const {
@@ -157,14 +171,15 @@ template <class T, bool TAB> struct FwdXLoad {
             if (t == 0) return czero<C>();
             d = (long)t - 1;
         }
-        if (a->amode == ALPHA_ISO) return cmul(a->alpha[d], x[3 * d + c]);
+        if (a->amode == ALPHA_ISO) return cmul(a->alpha[d], pre.template value<C>(3 * d + c));
         if (a->amode == ALPHA_FULL) {
             C acc = czero<C>();
 #pragma unroll
-            for (int q = 0; q < 3; q++) acc = cadd(acc, cmul(a->alpha[d + a->nmax * (c + 3 * q)], x[3 * d + q]));
+            for (int q = 0; q < 3; q++)
+                acc = cadd(acc, cmul(a->alpha[d + a->nmax * (c + 3 * q)], pre.template value<C>(3 * d + q)));
             return acc;
         }
-        return x[3 * d + c];
+        return pre.template value<C>(3 * d + c);
     }
 };
 
@@ -187,8 +202,8 @@ template <class T, int L, int TL> struct B1RowIO {
     }
 };
 
-template <class T, int L, bool TAB, class TT = MvTiles<T, L>>
-__global__ void __launch_bounds__(TT::NTX, TT::MINBX) k_fwd_x(const MvArgs<T> a) {
+template <class T, int L, bool TAB, class TT = MvTiles<T, L>, class Pre = PreNone<T>>
+__global__ void __launch_bounds__(TT::NTX, TT::MINBX) k_fwd_x(const MvArgs<T> a, const Pre pre, const MvRed red) {
     using C = cplx<T>;
     constexpr int TL = TT::TLX, NB = TT::NBX, NT = TT::NTX;
     const int rhs = blockIdx.z;
@@ -199,9 +214,13 @@ __global__ void __launch_bounds__(TT::NTX, TT::MINBX) k_fwd_x(const MvArgs<T> a)
     const int j0 = blockIdx.x * TL, k = blockIdx.y;
     const int nl = min(TL, ny - j0);
     load_twiddles<C, L, NT>(tw, a.twx);
-    FwdXLoad<T, TAB> src{&a, a.x + rhs * a.xstride, (long)k * nx * ny + (long)j0 * nx, nl, TL};
+    FwdXLoad<T, TAB, Pre> src{&a, pre, (long)k * nx * ny + (long)j0 * nx, nl, TL};
+    src.pre.bind(a, rhs);
     B1RowIO<T, L, TL> dst{a.B1 + rhs * a.g.b1_rhs, nl, nz, ny, k, j0};
     fft_tile<C, L, NB, NT, +1, typename TT::LayX>(sm, tw, src, dst);
+    if constexpr (Pre::ND > 0)
+        block_partial<NT, Pre::ND>(src.pre.acc,
+                                   red.ppart + (((long)rhs * gridDim.y + k) * red.gxs + blockIdx.x) * Pre::ND);
 }
 
 // ---- pass 2 and 4 ---------------------------------------------------------
@@ -404,13 +423,26 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
 }
 
 // ---- pass 5 -----------------------------------------------------------------
-template <class T, bool TAB> struct InvXStore {
+// The mat-vec output: Epi::elem(e, y) sees every stored element y of the
+// result (e = 3 d + c) and may accumulate ND dot products; the last block of
+// the grid then holds them, with the NDP partials of the first x pass, and
+// calls Epi::finish.
+struct EpiNone {
+    static constexpr int ND = 0, NDP = 0;
+    double2 acc[1];
+    template <class T> __device__ __forceinline__ void bind(const MvArgs<T>&, int) {}
+    template <class C> __device__ __forceinline__ void elem(long, C) {}
+    __device__ __forceinline__ void finish(int, const double2*) {}
+};
+
+template <class T, bool TAB, class Epi> struct InvXStore {
     static constexpr bool GLOBAL = true, HALF = true;  // keep points < nx
     const MvArgs<T>* a;
     const cplx<T>* bv;
     cplx<T>* yv;
     long site0;
     int nl, tl;
+    mutable Epi epi;
     template <class C> __device__ __forceinline__ void store(int b, int p, C v) const {
         const int c = b / tl, jl = b - c * tl;
         if (jl >= nl) return;
@@ -421,12 +453,14 @@ template <class T, bool TAB> struct InvXStore {
             if (t == 0) return;
             d = (long)t - 1;
         }
-        yv[3 * d + c] = csub(bv[3 * d + c], cscale(v, a->inv_m));
+        const C y = csub(bv[3 * d + c], cscale(v, a->inv_m));
+        yv[3 * d + c] = y;
+        epi.elem(3 * d + c, y);
     }
 };
 
 template <class T, int L, bool TAB, class Epi, class TT = MvTiles<T, L>>
-__global__ void __launch_bounds__(TT::NTX, TT::MINBX) k_inv_x(const MvArgs<T> a, const Epi epi) {
+__global__ void __launch_bounds__(TT::NTX, TT::MINBX) k_inv_x(const MvArgs<T> a, const Epi epi, const MvRed red) {
     using C = cplx<T>;
     constexpr int TL = TT::TLX, NB = TT::NBX, NT = TT::NTX;
     const int rhs = blockIdx.z;
@@ -438,12 +472,16 @@ __global__ void __launch_bounds__(TT::NTX, TT::MINBX) k_inv_x(const MvArgs<T> a,
     const int nl = min(TL, ny - j0);
     load_twiddles<C, L, NT>(tw, a.twx);
     B1RowIO<T, L, TL> src{a.B1 + rhs * a.g.b1_rhs, nl, nz, ny, k, j0};
-    InvXStore<T, TAB> dst{&a, a.b + rhs * a.xstride, a.y + rhs * a.xstride, (long)k * nx * ny + (long)j0 * nx, nl,
-                          TL};
+    InvXStore<T, TAB, Epi> dst{&a, a.b + rhs * a.xstride, a.y + rhs * a.xstride, (long)k * nx * ny + (long)j0 * nx, nl,
+                               TL, epi};
+    dst.epi.bind(a, rhs);
     fft_tile<C, L, NB, NT, -1, typename TT::LayX>(sm, tw, src, dst);
-    (void)epi;
+    if constexpr (Epi::ND > 0) {
+        double2 tot[Epi::ND + Epi::NDP];
+        if (reduce_rows<NT, Epi::ND, Epi::NDP>(dst.epi.acc, tot, rhs, blockIdx.x, k, gridDim.x, gridDim.y, red) &&
+            threadIdx.x == 0)
+            dst.epi.finish(rhs, tot);
+    }
 }
-
-struct EpiNone {};
 
 }  // namespace ifdda

@@ -13,16 +13,17 @@ struct PassScope {
     ~PassScope() { timing_after(ev, st); }
 };
 
-template <class T, int L> void launch_fwd_x(const MvArgs<T>& a, int nrhs, bool tab, cudaStream_t st) {
+template <class T, int L, class Pre>
+void launch_fwd_x(const MvArgs<T>& a, const Pre& pre, const MvRed& red, int nrhs, bool tab, cudaStream_t st) {
     using TT = MvTiles<T, L>;
     dim3 grid((a.g.ny + TT::TLX - 1) / TT::TLX, a.g.nz, nrhs);
     PassScope ps(PASS_FWD_X, TT::S, st);
     if (tab) {
-        ensure_smem(k_fwd_x<T, L, true>, TT::smem_x);
-        k_fwd_x<T, L, true><<<grid, TT::NTX, TT::smem_x, st>>>(a);
+        ensure_smem(k_fwd_x<T, L, true, TT, Pre>, TT::smem_x);
+        k_fwd_x<T, L, true, TT, Pre><<<grid, TT::NTX, TT::smem_x, st>>>(a, pre, red);
     } else {
-        ensure_smem(k_fwd_x<T, L, false>, TT::smem_x);
-        k_fwd_x<T, L, false><<<grid, TT::NTX, TT::smem_x, st>>>(a);
+        ensure_smem(k_fwd_x<T, L, false, TT, Pre>, TT::smem_x);
+        k_fwd_x<T, L, false, TT, Pre><<<grid, TT::NTX, TT::smem_x, st>>>(a, pre, red);
     }
 }
 
@@ -43,21 +44,21 @@ template <class T, int L> void launch_zconv(const MvArgs<T>& a, int nrhs, cudaSt
 }
 
 template <class T, int L, class Epi>
-void launch_inv_x(const MvArgs<T>& a, const Epi& epi, int nrhs, bool tab, cudaStream_t st) {
+void launch_inv_x(const MvArgs<T>& a, const Epi& epi, const MvRed& red, int nrhs, bool tab, cudaStream_t st) {
     using TT = MvTiles<T, L>;
     dim3 grid((a.g.ny + TT::TLX - 1) / TT::TLX, a.g.nz, nrhs);
     PassScope ps(PASS_INV_X, TT::S, st);
     if (tab) {
-        ensure_smem(k_inv_x<T, L, true, Epi>, TT::smem_x);
-        k_inv_x<T, L, true, Epi><<<grid, TT::NTX, TT::smem_x, st>>>(a, epi);
+        ensure_smem(k_inv_x<T, L, true, Epi, TT>, TT::smem_x);
+        k_inv_x<T, L, true, Epi, TT><<<grid, TT::NTX, TT::smem_x, st>>>(a, epi, red);
     } else {
-        ensure_smem(k_inv_x<T, L, false, Epi>, TT::smem_x);
-        k_inv_x<T, L, false, Epi><<<grid, TT::NTX, TT::smem_x, st>>>(a, epi);
+        ensure_smem(k_inv_x<T, L, false, Epi, TT>, TT::smem_x);
+        k_inv_x<T, L, false, Epi, TT><<<grid, TT::NTX, TT::smem_x, st>>>(a, epi, red);
     }
 }
 
 #define IFDDA_CASE_FWDX(L) \
-    case L: launch_fwd_x<T, L>(a, nrhs, tab, st); break;
+    case L: launch_fwd_x<T, L, Pre>(a, pre, red, nrhs, tab, st); break;
 #define IFDDA_CASE_FWDY(L) \
     case L: launch_pass_y<T, L, +1>(a, nrhs, st); break;
 #define IFDDA_CASE_INVY(L) \
@@ -65,10 +66,13 @@ void launch_inv_x(const MvArgs<T>& a, const Epi& epi, int nrhs, bool tab, cudaSt
 #define IFDDA_CASE_ZC(L) \
     case L: launch_zconv<T, L>(a, nrhs, st); break;
 #define IFDDA_CASE_INVX(L) \
-    case L: launch_inv_x<T, L, Epi>(a, epi, nrhs, tab, st); break;
+    case L: launch_inv_x<T, L, Epi>(a, epi, red, nrhs, tab, st); break;
 
-template <class T, class Epi>
-bool matvec_launch_epi(const MvArgs<T>& a, const Epi& epi, int nrhs, bool tab, cudaStream_t st) {
+// The five passes with a solver's input functor (first x pass) and output
+// functor (last x pass); red holds their reduction buffers.
+template <class T, class Pre, class Epi>
+bool matvec_launch_fused(const MvArgs<T>& a, const Pre& pre, const Epi& epi, const MvRed& red, int nrhs, bool tab,
+                         cudaStream_t st) {
     if (!fft_length_supported(a.g.X) || !fft_length_supported(a.g.Y) || !fft_length_supported(a.g.Z)) return false;
     switch (a.g.X) { IFDDA_FFT_LENGTHS(IFDDA_CASE_FWDX) default: return false; }
     IFDDA_CUDA(cudaGetLastError());

@@ -81,4 +81,78 @@ __device__ __forceinline__ bool reduce_across_blocks(double2 (&acc)[ND], int rhs
     return true;
 }
 
+// Reductions over the (gx, gy) grid of a mat-vec x pass, per right-hand
+// side.  The x passes of one mat-vec have the same grid, so the first pass
+// can leave NDP partial sums per block (ppart) that the last pass folds in.
+struct MvRed {
+    double2* ppart;   // [nrhs][gy][gxs][NDP]  partials of the first x pass
+    double2* epart;   // [nrhs][gy][gxs][ND]   partials of the last x pass
+    double2* rpart;   // [nrhs][gy][ND + NDP]  row sums
+    unsigned* t1;     // [nrhs][gy]            row tickets
+    unsigned* t2;     // [nrhs]                grid tickets
+    int gxs;          // stride between rows, in blocks (>= gx)
+};
+
+// Block sum of acc written to out[0..ND) by thread 0.
+template <int NT, int ND>
+__device__ __forceinline__ void block_partial(double2 (&acc)[ND], double2* out) {
+    __shared__ double2 scratch[ND * 32];
+    block_sum<NT, ND>(acc, scratch);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int m = 0; m < ND; m++) out[m] = acc[m];
+    }
+}
+
+// Two ticket levels: the last block of a row sums that row's ND partials and
+// the row's NDP partials of the first pass; the last row sums the rows.  All
+// sums run in index order, so the result does not depend on scheduling.
+// Returns true in the one block that holds the totals (thread 0's tot).
+template <int NT, int ND, int NDP>
+__device__ __forceinline__ bool reduce_rows(double2 (&own)[ND], double2 (&tot)[ND + NDP], int rhs, int bx, int by,
+                                            int gx, int gy, const MvRed& R) {
+    constexpr int NA = ND + NDP;
+    __shared__ double2 scratch[NA * 32];
+    __shared__ bool last;
+    block_sum<NT, ND>(own, scratch);
+    const long row = (long)rhs * gy + by;
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int m = 0; m < ND; m++) R.epart[(row * R.gxs + bx) * ND + m] = own[m];
+        __threadfence();
+        last = atomicAdd(&R.t1[row], 1u) == (unsigned)(gx - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+#pragma unroll
+    for (int m = 0; m < NA; m++) tot[m] = make_double2(0, 0);
+    for (int q = threadIdx.x; q < gx; q += NT) {
+#pragma unroll
+        for (int m = 0; m < ND; m++) tot[m] = dadd(tot[m], __ldcg(R.epart + (row * R.gxs + q) * ND + m));
+#pragma unroll
+        for (int m = 0; m < NDP; m++) tot[ND + m] = dadd(tot[ND + m], __ldcg(R.ppart + (row * R.gxs + q) * NDP + m));
+    }
+    block_sum<NT, NA>(tot, scratch);
+    if (threadIdx.x == 0) {
+        R.t1[row] = 0u;
+#pragma unroll
+        for (int m = 0; m < NA; m++) R.rpart[row * NA + m] = tot[m];
+        __threadfence();
+        last = atomicAdd(&R.t2[rhs], 1u) == (unsigned)(gy - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+#pragma unroll
+    for (int m = 0; m < NA; m++) tot[m] = make_double2(0, 0);
+    for (int q = threadIdx.x; q < gy; q += NT) {
+#pragma unroll
+        for (int m = 0; m < NA; m++) tot[m] = dadd(tot[m], __ldcg(R.rpart + ((long)rhs * gy + q) * NA + m));
+    }
+    block_sum<NT, NA>(tot, scratch);
+    if (threadIdx.x == 0) R.t2[rhs] = 0u;
+    return true;
+}
+
 }  // namespace ifdda

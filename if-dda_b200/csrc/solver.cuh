@@ -12,6 +12,7 @@ struct SolveSpec {
     double tol = 1e-4;
     int maxit = 10000;     // nlim of cdmlib/inverserigopt.f:30
     int check_every = 4;   // iterations launched between status polls
+    bool fuse = true;      // GPBiCG vector steps inside the mat-vec x passes (gpbicg_fused.cuh)
     bool use_graphs = true;  // replay captured iterations instead of launching kernels
     int zero_guess = 0;    // x0 = 0 instead of x0 = b
     bool preset_state = false;
@@ -58,10 +59,13 @@ template <class T> struct KrylovWork {
     DevBuf<int> status, zstatus;
     DevBuf<double2> partials;
     DevBuf<unsigned> tickets;
+    DevBuf<double2> mvpart;  // reductions of the fused mat-vecs (MvRed)
+    DevBuf<unsigned> mvtk;
     std::vector<int> hstatus;
     int nslot = 0, nrhs = 0, nblk = 1;
     long n3 = 0;
     void ensure(int method, int nrhs, long n3);
+    MvRed mv_red(int ny, int nz);  // sized for x-pass grids of up to ny x nz blocks
     Slots<T> slots() const;
     int x_slot(int method) const;
     int b_slot(int method) const;
@@ -74,6 +78,8 @@ template <class T> struct KrylovWork {
         zstatus.release();
         partials.release();
         tickets.release();
+        mvpart.release();
+        mvtk.release();
         hstatus.clear();
         nrhs = 0;
         n3 = 0;
