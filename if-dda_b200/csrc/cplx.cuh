@@ -5,6 +5,17 @@
 
 namespace ifdda {
 
+// Programmatic dependent launch.  A kernel launched with it may start while
+// the kernel before it on the stream is still finishing: its blocks run their
+// prologue (constant tables, prefetches of constant data), then pdl_wait()
+// blocks until the previous kernel has completed and its writes are visible.
+// Every block calls pdl_wait() before it reads anything the previous kernel
+// wrote and before it exits, so the chain of dependencies stays transitive.
+// pdl_trigger() lets the next kernel's blocks be scheduled once every block
+// of this one has started.  Without the launch attribute both are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 template <typename T> struct cvec;
 template <> struct cvec<float> { using type = float2; };
 template <> struct cvec<double> { using type = double2; };

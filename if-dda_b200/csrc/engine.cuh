@@ -7,6 +7,7 @@
 #include <atomic>
 #include <mutex>
 #include <unordered_map>
+#include <utility>
 #include "instrument.cuh"
 #include "matvec_kernels.cuh"
 
@@ -51,6 +52,23 @@ inline void ensure_smem_ptr(const void* kernel, size_t bytes) {
     m |= bit;
 }
 template <class K> inline void ensure_smem(K kernel, size_t bytes) { ensure_smem_ptr((const void*)kernel, bytes); }
+
+// Launch with programmatic dependent launch allowed (see pdl_wait): the
+// kernel's blocks may be scheduled during the previous kernel's last wave.
+template <class... KP, class... A>
+inline void launch_pdl(void (*kernel)(KP...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, A&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    IFDDA_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...));
+}
 
 // Stream on which DevBuf allocates and frees (stream-ordered, from the
 // device's memory pool): the calling entry point sets it to its context's

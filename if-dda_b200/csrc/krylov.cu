@@ -169,7 +169,7 @@ template <class T> MvRed KrylovWork<T>::mv_red(int ny, int nz) {
 template <int ND, class Op>
 static void vec_launch(const Op& op, long n3, int nblk, int nrhs, const RedSlots& rs, int* status, cudaStream_t st) {
     count_launch();
-    k_vec<ND, Op><<<dim3(nblk, nrhs), KNT, 0, st>>>(op, n3, nblk, rs, status);
+    launch_pdl(k_vec<ND, Op>, dim3(nblk, nrhs), dim3(KNT), 0, st, op, n3, nblk, rs, status);
 }
 
 template <class T>

@@ -60,6 +60,8 @@ constexpr int KNT = 256;
 template <int ND, class Op>
 __global__ void __launch_bounds__(KNT) k_vec(const Op op, long n3, int nblk, RedSlots rs, int* __restrict__ status) {
     const int rhs = blockIdx.y;
+    pdl_trigger();
+    pdl_wait();
     if (status[rhs]) return;
     double2 acc[ND > 0 ? ND : 1];
 #pragma unroll

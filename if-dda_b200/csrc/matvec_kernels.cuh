@@ -207,13 +207,15 @@ __global__ void __launch_bounds__(TT::NTX, TT::MINBX) k_fwd_x(const MvArgs<T> a,
     using C = cplx<T>;
     constexpr int TL = TT::TLX, NB = TT::NBX, NT = TT::NTX;
     const int rhs = blockIdx.z;
-    if (a.status && a.status[rhs]) return;
     C* tw = smem_base<C>();
     C* sm = tw + L;
     const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
     const int j0 = blockIdx.x * TL, k = blockIdx.y;
     const int nl = min(TL, ny - j0);
     load_twiddles<C, L, NT>(tw, a.twx);
+    pdl_trigger();
+    pdl_wait();
+    if (a.status && a.status[rhs]) return;
     FwdXLoad<T, TAB, Pre> src{&a, pre, (long)k * nx * ny + (long)j0 * nx, nl, TL};
     src.pre.bind(a, rhs);
     B1RowIO<T, L, TL> dst{a.B1 + rhs * a.g.b1_rhs, nl, nz, ny, k, j0};
@@ -249,12 +251,14 @@ __global__ void __launch_bounds__(TT::NTY, TT::MINBY) k_pass_y(const MvArgs<T> a
     using C = cplx<T>;
     constexpr int TL = TT::TLY, NT = TT::NTY;
     const int rhs = blockIdx.z / 3, c = blockIdx.z - 3 * (blockIdx.z / 3);
-    if (a.status && a.status[rhs]) return;
     C* tw = smem_base<C>();
     C* sm = tw + L;
     const int X = a.g.X, ny = a.g.ny, nz = a.g.nz;
     const int i0 = blockIdx.x * TL, k = blockIdx.y;
     load_twiddles<C, L, NT>(tw, a.twy);
+    pdl_trigger();
+    pdl_wait();
+    if (a.status && a.status[rhs]) return;
     const int rows_in = DIR > 0 ? ny : L;
     const int rows_out = DIR > 0 ? L : ny;
     const C* srcb = DIR > 0 ? a.B1 + rhs * a.g.b1_rhs : a.B2 + rhs * a.g.b2_rhs;
@@ -311,7 +315,6 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
     constexpr int PERM = (NG + NT - 1) / NT;
     constexpr int NQ = L / 2 + 1;
     const int rhs = blockIdx.z;
-    if (a.status && a.status[rhs]) return;
     C* tw = smem_base<C>();
     C* sm = tw + L;
     C* gs = sm + LZ::span(L) * TT::PSZ;
@@ -332,6 +335,13 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
         cp_async_elem(gs + e, a.Gc + c6 * gcs + ((long)qz * (ny + 1) + qy) * (nx + 1) + qxc);
     }
     cp_async_commit();
+    // the spectrum and the twiddles are constant: only B2 waits for the y pass
+    pdl_trigger();
+    pdl_wait();
+    if (a.status && a.status[rhs]) {
+        cp_async_wait_all();
+        return;
+    }
     C* B2 = a.B2 + rhs * a.g.b2_rhs;
     const long rs = (long)Y * X, comp = (long)nz * Y * X;
     const long row0 = (long)qy * X, row1 = (long)(Y - qy) * X;
@@ -464,13 +474,15 @@ __global__ void __launch_bounds__(TT::NTX, TT::MINBX) k_inv_x(const MvArgs<T> a,
     using C = cplx<T>;
     constexpr int TL = TT::TLX, NB = TT::NBX, NT = TT::NTX;
     const int rhs = blockIdx.z;
-    if (a.status && a.status[rhs]) return;
     C* tw = smem_base<C>();
     C* sm = tw + L;
     const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz;
     const int j0 = blockIdx.x * TL, k = blockIdx.y;
     const int nl = min(TL, ny - j0);
     load_twiddles<C, L, NT>(tw, a.twx);
+    pdl_trigger();
+    pdl_wait();
+    if (a.status && a.status[rhs]) return;
     B1RowIO<T, L, TL> src{a.B1 + rhs * a.g.b1_rhs, nl, nz, ny, k, j0};
     InvXStore<T, TAB, Epi> dst{&a, a.b + rhs * a.xstride, a.y + rhs * a.xstride, (long)k * nx * ny + (long)j0 * nx, nl,
                                TL, epi};

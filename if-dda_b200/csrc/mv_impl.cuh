@@ -20,10 +20,10 @@ void launch_fwd_x(const MvArgs<T>& a, const Pre& pre, const MvRed& red, int nrhs
     PassScope ps(PASS_FWD_X, TT::S, st);
     if (tab) {
         ensure_smem(k_fwd_x<T, L, true, TT, Pre>, TT::smem_x);
-        k_fwd_x<T, L, true, TT, Pre><<<grid, TT::NTX, TT::smem_x, st>>>(a, pre, red);
+        launch_pdl(k_fwd_x<T, L, true, TT, Pre>, grid, TT::NTX, TT::smem_x, st, a, pre, red);
     } else {
         ensure_smem(k_fwd_x<T, L, false, TT, Pre>, TT::smem_x);
-        k_fwd_x<T, L, false, TT, Pre><<<grid, TT::NTX, TT::smem_x, st>>>(a, pre, red);
+        launch_pdl(k_fwd_x<T, L, false, TT, Pre>, grid, TT::NTX, TT::smem_x, st, a, pre, red);
     }
 }
 
@@ -32,7 +32,7 @@ template <class T, int L, int DIR> void launch_pass_y(const MvArgs<T>& a, int nr
     dim3 grid((a.g.X + TT::TLY - 1) / TT::TLY, a.g.nz, 3 * nrhs);
     PassScope ps(DIR > 0 ? PASS_FWD_Y : PASS_INV_Y, TT::S, st);
     ensure_smem(k_pass_y<T, L, DIR>, TT::smem_y);
-    k_pass_y<T, L, DIR><<<grid, TT::NTY, TT::smem_y, st>>>(a);
+    launch_pdl(k_pass_y<T, L, DIR>, grid, TT::NTY, TT::smem_y, st, a);
 }
 
 template <class T, int L> void launch_zconv(const MvArgs<T>& a, int nrhs, cudaStream_t st) {
@@ -40,7 +40,7 @@ template <class T, int L> void launch_zconv(const MvArgs<T>& a, int nrhs, cudaSt
     dim3 grid((a.g.X + TT::TLZ - 1) / TT::TLZ, a.g.ny + 1, nrhs);
     PassScope ps(PASS_ZCONV, TT::S, st);
     ensure_smem(k_zconv<T, L>, TT::smem_z);
-    k_zconv<T, L><<<grid, TT::NTZ, TT::smem_z, st>>>(a);
+    launch_pdl(k_zconv<T, L>, grid, TT::NTZ, TT::smem_z, st, a);
 }
 
 template <class T, int L, class Epi>
@@ -50,10 +50,10 @@ void launch_inv_x(const MvArgs<T>& a, const Epi& epi, const MvRed& red, int nrhs
     PassScope ps(PASS_INV_X, TT::S, st);
     if (tab) {
         ensure_smem(k_inv_x<T, L, true, Epi, TT>, TT::smem_x);
-        k_inv_x<T, L, true, Epi, TT><<<grid, TT::NTX, TT::smem_x, st>>>(a, epi, red);
+        launch_pdl(k_inv_x<T, L, true, Epi, TT>, grid, TT::NTX, TT::smem_x, st, a, epi, red);
     } else {
         ensure_smem(k_inv_x<T, L, false, Epi, TT>, TT::smem_x);
-        k_inv_x<T, L, false, Epi, TT><<<grid, TT::NTX, TT::smem_x, st>>>(a, epi, red);
+        launch_pdl(k_inv_x<T, L, false, Epi, TT>, grid, TT::NTX, TT::smem_x, st, a, epi, red);
     }
 }
 
