@@ -166,6 +166,20 @@ template <class T> MvRed KrylovWork<T>::mv_red(int ny, int nz) {
     return r;
 }
 
+// Condition of the device-side iteration loop: run another body while some
+// right-hand side is still iterating and fewer than `chunk` bodies have run
+// in this launch.  One thread; status was written by the body's last kernel.
+__global__ void k_loop_ctl(cudaGraphConditionalHandle h, const int* __restrict__ status, int nrhs, int* count,
+                           int chunk) {
+    if (threadIdx.x != 0) return;
+    const int c = *count + 1;
+    *count = c;
+    bool run = false;
+    if (c < chunk)
+        for (int r = 0; r < nrhs && !run; r++) run = status[r] == 0;
+    cudaGraphSetConditional(h, run ? 1u : 0u);
+}
+
 template <int ND, class Op>
 static void vec_launch(const Op& op, long n3, int nblk, int nrhs, const RedSlots& rs, int* status, cudaStream_t st) {
     count_launch();
@@ -282,32 +296,110 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
         done = poll(W, sp, st, cancelled);
     }
     const bool graphs = sp.use_graphs && !timing_active();
+    // Builds the device-side loop: [clear counter] -> while(cond) { two
+    // iterations; k_loop_ctl }.  Returns false (nothing kept) if the driver
+    // cannot build it; the caller then replays plain two-iteration graphs.
+    constexpr int CHUNK = 32;  // bodies (2 iterations each) per launch, between host checks
+    auto build_loop = [&]() -> bool {
+        cudaGraph_t g = nullptr;
+        if (cudaGraphCreate(&g, 0) != cudaSuccess) return false;
+        bool ok = false;
+        cudaGraphExec_t ex = nullptr;
+        unsigned long long nk = 0;
+        do {
+            cudaGraphConditionalHandle h;
+            if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) break;
+            cudaMemsetParams mp = {};
+            mp.dst = W.loopcount.p;
+            mp.value = 0;
+            mp.elementSize = sizeof(int);
+            mp.width = 1;
+            mp.height = 1;
+            cudaGraphNode_t nm, nc;
+            if (cudaGraphAddMemsetNode(&nm, g, nullptr, 0, &mp) != cudaSuccess) break;
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            if (cudaGraphAddNode(&nc, g, &nm, 1, &cp) != cudaSuccess) break;
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            if (cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+                cudaSuccess)
+                break;
+            const unsigned long long c0 = launch_counter().load();
+            bool cap_ok = true;
+            try {
+                iteration(0);
+                iteration(1);
+                count_launch();
+                k_loop_ctl<<<1, 32, 0, st>>>(h, status, nrhs, W.loopcount.p, CHUNK);
+            } catch (...) {
+                cap_ok = false;
+            }
+            nk = launch_counter().load() - c0;
+            launch_counter().fetch_sub(nk);  // captured, not run
+            cudaGraph_t out = nullptr;
+            const cudaError_t ee = cudaStreamEndCapture(st, &out);
+            if (!cap_ok || ee != cudaSuccess) break;
+            if (cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) {
+                ex = nullptr;
+                break;
+            }
+            ok = true;
+        } while (0);
+        cudaGraphDestroy(g);
+        if (!ok) {
+            cudaGetLastError();
+            return false;
+        }
+        W.graph.exec = ex;
+        W.graph.kernels = nk;
+        W.graph.loop = true;
+        W.graph.chunk = CHUNK;
+        return true;
+    };
     if (!done && graphs) {
         MvWork<T>& mw = G.work<T>();
         mw.ensure(G.g, nrhs);
+        W.loopcount.ensure(1);
         const std::vector<const void*> key = {
             V.base, sp.alpha, sp.tabdip, G.gc<T>(), mw.B1.p, mw.B2.p, W.partials.p, W.tickets.p, status, S,
-            W.mvpart.p, W.mvtk.p, (const void*)(long)fused,
+            W.mvpart.p, W.mvtk.p, W.loopcount.p, (const void*)(long)fused,
             (const void*)(long)sp.method, (const void*)(long)nrhs, (const void*)n3, (const void*)(long)sp.amode,
             (const void*)sp.nmax, (const void*)(long)nblk};
         if (!W.graph.exec || W.graph.key != key) {
             W.graph.reset();
-            const unsigned long long c0 = launch_counter().load();
-            cudaGraph_t graph;
-            IFDDA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            iteration(0);
-            iteration(1);
-            IFDDA_CUDA(cudaStreamEndCapture(st, &graph));
-            const unsigned long long nk = launch_counter().load() - c0;
-            launch_counter().fetch_sub(nk);  // captured, not run
-            const cudaError_t e = cudaGraphInstantiate(&W.graph.exec, graph, 0);
-            cudaGraphDestroy(graph);
-            IFDDA_CUDA(e);
-            W.graph.key = key;
-            W.graph.kernels = nk;
+            if (build_loop()) {
+                W.graph.key = key;
+            } else {
+                const unsigned long long c0 = launch_counter().load();
+                cudaGraph_t graph;
+                IFDDA_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                iteration(0);
+                iteration(1);
+                IFDDA_CUDA(cudaStreamEndCapture(st, &graph));
+                const unsigned long long nk = launch_counter().load() - c0;
+                launch_counter().fetch_sub(nk);  // captured, not run
+                const cudaError_t e = cudaGraphInstantiate(&W.graph.exec, graph, 0);
+                cudaGraphDestroy(graph);
+                IFDDA_CUDA(e);
+                W.graph.key = key;
+                W.graph.kernels = nk;
+            }
         }
     }
     while (!done) {
+        if (graphs && W.graph.exec && W.graph.loop) {
+            IFDDA_CUDA(cudaGraphLaunch(W.graph.exec, st));
+            int bodies = 0;
+            IFDDA_CUDA(cudaMemcpyAsync(&bodies, W.loopcount.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+            done = poll(W, sp, st, cancelled);
+            count_launch((unsigned)(W.graph.kernels * (unsigned long long)bodies));
+            it += 2L * bodies;
+            if (it > (long)sp.maxit + 4) break;
+            continue;
+        }
         for (int k = 0; k < every; k += 2) {
             if (graphs && W.graph.exec) {
                 IFDDA_CUDA(cudaGraphLaunch(W.graph.exec, st));

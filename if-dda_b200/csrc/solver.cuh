@@ -37,17 +37,24 @@ struct SolveResult {
     int outer = 0;      // refinement steps (mixed)
 };
 
-// Two Krylov iterations captured as one CUDA graph (the t buffers alternate,
-// so two iterations bring the pointers back), reused while every pointer and
-// size baked into its kernel arguments stays the same.
+// Krylov iterations as one CUDA graph, reused while every pointer and size
+// baked into its kernel arguments stays the same.  Two iterations make one
+// body (the t buffers alternate, so two iterations bring the pointers back).
+// With `loop` the body sits in a device-side while node that repeats it until
+// every right-hand side has stopped or `chunk` bodies have run (a counter in
+// device memory, cleared by the graph), so one launch replaces many host
+// polls; otherwise one launch runs the body once.
 struct IterGraph {
     cudaGraphExec_t exec = nullptr;
     std::vector<const void*> key;
-    unsigned long long kernels = 0;  // kernel launches per replay
+    unsigned long long kernels = 0;  // kernel launches per body
+    bool loop = false;
+    int chunk = 0;
     void reset() {
         if (exec) cudaGraphExecDestroy(exec);
         exec = nullptr;
         key.clear();
+        loop = false;
     }
     ~IterGraph() { reset(); }
 };
@@ -61,6 +68,7 @@ template <class T> struct KrylovWork {
     DevBuf<unsigned> tickets;
     DevBuf<double2> mvpart;  // reductions of the fused mat-vecs (MvRed)
     DevBuf<unsigned> mvtk;
+    DevBuf<int> loopcount;   // bodies run by the last device-side loop
     std::vector<int> hstatus;
     int nslot = 0, nrhs = 0, nblk = 1;
     long n3 = 0;
@@ -80,6 +88,7 @@ template <class T> struct KrylovWork {
         tickets.release();
         mvpart.release();
         mvtk.release();
+        loopcount.release();
         hstatus.clear();
         nrhs = 0;
         n3 = 0;
