@@ -38,7 +38,7 @@ template <class T> struct PreGpP {
         beta = S[rhs].beta;
         upd_w = S[rhs].itno > 0;
     }
-    template <class C> __device__ __forceinline__ C value(long e) {
+    template <class C> __device__ __forceinline__ C value(int e) {
         const C pc = from_d<C>(zadd(ld(r, e), zmul(beta, zsub(ld(p, e), ld(u, e)))));
         p[e] = pc;
         if (upd_w) st(w, e, zadd(ld(at, e), zmul(beta, ld(ap, e))));
@@ -58,7 +58,7 @@ template <class T> struct EpiGpAlpha {
         r0 = V.v(G_R0, rhs);
         acc[0] = make_double2(0, 0);
     }
-    template <class C> __device__ __forceinline__ void elem(long e, C y) {
+    template <class C> __device__ __forceinline__ void elem(int e, C y) {
         acc[0] = zadd(acc[0], zconjmul(ld(r0, e), to_d(y)));
     }
     __device__ __forceinline__ void finish(int rhs, const double2* tot) {
@@ -88,7 +88,7 @@ template <class T> struct PreGpYT {
         alpha = S[rhs].alpha;
         acc[0] = acc[1] = make_double2(0, 0);
     }
-    template <class C> __device__ __forceinline__ C value(long e) {
+    template <class C> __device__ __forceinline__ C value(int e) {
         const double2 rr = ld(r, e), apv = ld(ap, e);
         const double2 yv = zadd(zsub(ld(t, e), rr), zmul(alpha, zsub(apv, ld(w, e))));
         const double2 tv = zsub(rr, zmul(alpha, apv));
@@ -116,7 +116,7 @@ template <class T> struct EpiGpZeta {
         t = V.v(tnew, rhs);
         acc[0] = acc[1] = acc[2] = make_double2(0, 0);
     }
-    template <class C> __device__ __forceinline__ void elem(long e, C atc) {
+    template <class C> __device__ __forceinline__ void elem(int e, C atc) {
         const double2 a = to_d(atc);
         acc[0] = zadd(acc[0], zconjmul(a, a));
         acc[1] = zadd(acc[1], zconjmul(a, ld(y, e)));

@@ -152,31 +152,36 @@ template <class T> struct PreNone {
     const cplx<T>* x;
     double2 acc[1];
     __device__ __forceinline__ void bind(const MvArgs<T>& a, int rhs) { x = a.x + rhs * a.xstride; }
-    template <class C> __device__ __forceinline__ C value(long e) { return x[e]; }
+    template <class C> __device__ __forceinline__ C value(int e) { return x[e]; }
 };
 
+// Element offsets inside one right-hand side's vectors and scratch fit in 32
+// bits for every compiled FFT length (at most 3 * 192^3 dipole components,
+// 3 * 192 * 384^2 grid points), so the pass functors index with int from
+// per-block base pointers; the fields they need are copied by value.
 template <class T, bool TAB, class Pre> struct FwdXLoad {
     static constexpr bool GLOBAL = true, HALF = true;  // points p >= nx are the padding
-    const MvArgs<T>* a;
+    const int* tab;
+    const cplx<T>* alpha;
+    int amode, nmax, nx;
     mutable Pre pre;
-    long site0;
-    int nl, tl;
+    int site0, nl, tl;
     template <class C> __device__ __forceinline__ C load(int b, int p) const {
         const int c = b / tl, jl = b - c * tl;
         if (jl >= nl) return czero<C>();
-        const long site = site0 + (long)jl * a->g.nx + p;
-        long d = site;
+        const int site = site0 + jl * nx + p;
+        int d = site;
         if (TAB) {
-            const int t = a->tabdip[site];
+            const int t = tab[site];
             if (t == 0) return czero<C>();
-            d = (long)t - 1;
+            d = t - 1;
         }
-        if (a->amode == ALPHA_ISO) return cmul(a->alpha[d], pre.template value<C>(3 * d + c));
-        if (a->amode == ALPHA_FULL) {
+        if (amode == ALPHA_ISO) return cmul(alpha[d], pre.template value<C>(3 * d + c));
+        if (amode == ALPHA_FULL) {
             C acc = czero<C>();
 #pragma unroll
             for (int q = 0; q < 3; q++)
-                acc = cadd(acc, cmul(a->alpha[d + a->nmax * (c + 3 * q)], pre.template value<C>(3 * d + q)));
+                acc = cadd(acc, cmul(alpha[d + nmax * (c + 3 * q)], pre.template value<C>(3 * d + q)));
             return acc;
         }
         return pre.template value<C>(3 * d + c);
@@ -186,19 +191,19 @@ template <class T, bool TAB, class Pre> struct FwdXLoad {
 // B1 rows of one x-pass tile: line b = c * TL + jl is row ((c * nz + k) * ny + j0 + jl)
 template <class T, int L, int TL> struct B1RowIO {
     static constexpr bool GLOBAL = true, HALF = false;
-    cplx<T>* B1;
-    int nl, nz, ny, k, j0;
-    template <class C> __device__ __forceinline__ long at(int b, int p) const {
+    cplx<T>* base;  // row (c = 0, k, j0) of this right-hand side
+    int nl, cstride;  // valid rows, elements between components (nz ny L)
+    template <class C> __device__ __forceinline__ int at(int b, int p) const {
         const int c = b / TL, jl = b - c * TL;
-        return jl < nl ? (((long)c * nz + k) * ny + j0 + jl) * L + p : -1;
+        return jl < nl ? c * cstride + jl * L + p : -1;
     }
     template <class C> __device__ __forceinline__ void store(int b, int p, C v) const {
-        const long o = at<C>(b, p);
-        if (o >= 0) B1[o] = v;
+        const int o = at<C>(b, p);
+        if (o >= 0) base[o] = v;
     }
     template <class C> __device__ __forceinline__ C load(int b, int p) const {
-        const long o = at<C>(b, p);
-        return o >= 0 ? B1[o] : czero<C>();
+        const int o = at<C>(b, p);
+        return o >= 0 ? base[o] : czero<C>();
     }
 };
 
@@ -216,9 +221,9 @@ __global__ void __launch_bounds__(TT::NTX, TT::MINBX) k_fwd_x(const MvArgs<T> a,
     pdl_trigger();
     pdl_wait();
     if (a.status && a.status[rhs]) return;
-    FwdXLoad<T, TAB, Pre> src{&a, pre, (long)k * nx * ny + (long)j0 * nx, nl, TL};
+    FwdXLoad<T, TAB, Pre> src{a.tabdip, a.alpha, a.amode, (int)a.nmax, nx, pre, k * nx * ny + j0 * nx, nl, TL};
     src.pre.bind(a, rhs);
-    B1RowIO<T, L, TL> dst{a.B1 + rhs * a.g.b1_rhs, nl, nz, ny, k, j0};
+    B1RowIO<T, L, TL> dst{a.B1 + rhs * a.g.b1_rhs + ((long)k * ny + j0) * L, nl, nz * ny * L};
     fft_tile<C, L, NB, NT, +1, typename TT::LayX>(sm, tw, src, dst);
     if constexpr (Pre::ND > 0)
         block_partial<NT, Pre::ND>(src.pre.acc,
@@ -233,7 +238,7 @@ template <class T, int DIR> struct YLoad {
     int X, i0;
     template <class C> __device__ __forceinline__ C load(int b, int p) const {
         const int i = i0 + b;
-        return i < X ? src[(long)p * X + i] : czero<C>();
+        return i < X ? src[p * X + i] : czero<C>();
     }
 };
 template <class T, int DIR> struct YStore {
@@ -242,7 +247,7 @@ template <class T, int DIR> struct YStore {
     int X, i0;
     template <class C> __device__ __forceinline__ void store(int b, int p, C v) const {
         const int i = i0 + b;
-        if (i < X) dst[(long)p * X + i] = v;
+        if (i < X) dst[p * X + i] = v;
     }
 };
 
@@ -272,29 +277,26 @@ __global__ void __launch_bounds__(TT::NTY, TT::MINBY) k_pass_y(const MvArgs<T> a
 // lines b = (h * 3 + c) * TL + il: h = 0 row qy, h = 1 the mirror row Y - qy
 template <class T, int TL> struct ZLoad {
     static constexpr bool GLOBAL = true, HALF = true;  // rows >= nz are padding
-    const cplx<T>* B2;
-    long rs;  // elements between z rows (Y * X)
-    long comp;  // elements between components (nz * Y * X)
-    long row0, row1;
-    int X, i0, two;
+    const cplx<T>* base;  // B2 of this right-hand side, column i0 of row qy
+    int rs;    // elements between z rows (Y * X)
+    int comp;  // elements between components (nz * Y * X)
+    int drow;  // row Y - qy minus row qy
+    int nv, two;  // valid columns, rows in the block (1 or 2)
     template <class C> __device__ __forceinline__ C load(int b, int p) const {
         const int hc = b / TL, il = b - hc * TL;
         const int h = hc / 3, c = hc - 3 * h;
-        const int i = i0 + il;
-        if (i >= X || h >= two) return czero<C>();
-        return B2[c * comp + (long)p * rs + (h ? row1 : row0) + i];
+        if (il >= nv || h >= two) return czero<C>();
+        return base[c * comp + p * rs + h * drow + il];
     }
 };
 template <class T, int TL> struct ZStore {
     static constexpr bool GLOBAL = true, HALF = true;  // keep z rows < nz
-    cplx<T>* B2;
-    long rs, comp, row0, row1;
-    int X, i0, two;
+    cplx<T>* base;
+    int rs, comp, drow, nv, two;
     template <class C> __device__ __forceinline__ void store(int b, int p, C v) const {
         const int hc = b / TL, il = b - hc * TL;
         const int h = hc / 3, c = hc - 3 * h;
-        const int i = i0 + il;
-        if (i < X && h < two) B2[c * comp + (long)p * rs + (h ? row1 : row0) + i] = v;
+        if (il < nv && h < two) base[c * comp + p * rs + h * drow + il] = v;
     }
 };
 
@@ -326,13 +328,17 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
     // this block's slice of the compressed spectrum (qy fixed, every qz, the
     // TL columns qx(i)) is copied into shared memory while the forward
     // transform runs
-    const long gcs = a.g.gc_comp;
-    for (int e = threadIdx.x; e < 6 * NQ * TL; e += NT) {
-        const int il = e % TL, cq = e / TL;
-        const int c6 = cq / NQ, qz = cq - c6 * NQ;
+    {
+        static_assert(NT % TL == 0, "a thread keeps one column of the slice");
+        const int il = threadIdx.x % TL;
         const int i = min(i0 + il, X - 1);
         const int qxc = i <= nx ? i : X - i;
-        cp_async_elem(gs + e, a.Gc + c6 * gcs + ((long)qz * (ny + 1) + qy) * (nx + 1) + qxc);
+        const C* gsrc = a.Gc + qy * (nx + 1) + qxc;
+        const int gcs = (int)a.g.gc_comp, qzs = (ny + 1) * (nx + 1);
+        for (int cq = threadIdx.x / TL; cq < 6 * NQ; cq += NT / TL) {
+            const int c6 = cq / NQ, qz = cq - c6 * NQ;
+            cp_async_elem(gs + cq * TL + il, gsrc + c6 * gcs + qz * qzs);
+        }
     }
     cp_async_commit();
     // the spectrum and the twiddles are constant: only B2 waits for the y pass
@@ -342,11 +348,10 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
         cp_async_wait_all();
         return;
     }
-    C* B2 = a.B2 + rhs * a.g.b2_rhs;
-    const long rs = (long)Y * X, comp = (long)nz * Y * X;
-    const long row0 = (long)qy * X, row1 = (long)(Y - qy) * X;
-    const ZLoad<T, TL> zload{B2, rs, comp, row0, row1, X, i0, two};
-    const ZStore<T, TL> zstore{B2, rs, comp, row0, row1, X, i0, two};
+    C* B2 = a.B2 + rhs * a.g.b2_rhs + (long)qy * X + i0;
+    const int rs = Y * X, comp = nz * Y * X, drow = (Y - 2 * qy) * X, nv = min(TL, X - i0);
+    const ZLoad<T, TL> zload{B2, rs, comp, drow, nv, two};
+    const ZStore<T, TL> zstore{B2, rs, comp, drow, nv, two};
     if constexpr (NP > 1) stockham_range<C, L, NB, NT, +1, LZ, false, NP - 1, 0, 1>(sm, tw, zload, SmemIO{});
     cp_async_wait_all();
     __syncthreads();
@@ -441,29 +446,29 @@ struct EpiNone {
     static constexpr int ND = 0, NDP = 0;
     double2 acc[1];
     template <class T> __device__ __forceinline__ void bind(const MvArgs<T>&, int) {}
-    template <class C> __device__ __forceinline__ void elem(long, C) {}
+    template <class C> __device__ __forceinline__ void elem(int, C) {}
     __device__ __forceinline__ void finish(int, const double2*) {}
 };
 
 template <class T, bool TAB, class Epi> struct InvXStore {
     static constexpr bool GLOBAL = true, HALF = true;  // keep points < nx
-    const MvArgs<T>* a;
+    const int* tab;
     const cplx<T>* bv;
     cplx<T>* yv;
-    long site0;
-    int nl, tl;
+    T inv_m;
+    int nx, site0, nl, tl;
     mutable Epi epi;
     template <class C> __device__ __forceinline__ void store(int b, int p, C v) const {
         const int c = b / tl, jl = b - c * tl;
         if (jl >= nl) return;
-        const long site = site0 + (long)jl * a->g.nx + p;
-        long d = site;
+        const int site = site0 + jl * nx + p;
+        int d = site;
         if (TAB) {
-            const int t = a->tabdip[site];
+            const int t = tab[site];
             if (t == 0) return;
-            d = (long)t - 1;
+            d = t - 1;
         }
-        const C y = csub(bv[3 * d + c], cscale(v, a->inv_m));
+        const C y = csub(bv[3 * d + c], cscale(v, inv_m));
         yv[3 * d + c] = y;
         epi.elem(3 * d + c, y);
     }
@@ -483,9 +488,9 @@ __global__ void __launch_bounds__(TT::NTX, TT::MINBX) k_inv_x(const MvArgs<T> a,
     pdl_trigger();
     pdl_wait();
     if (a.status && a.status[rhs]) return;
-    B1RowIO<T, L, TL> src{a.B1 + rhs * a.g.b1_rhs, nl, nz, ny, k, j0};
-    InvXStore<T, TAB, Epi> dst{&a, a.b + rhs * a.xstride, a.y + rhs * a.xstride, (long)k * nx * ny + (long)j0 * nx, nl,
-                               TL, epi};
+    B1RowIO<T, L, TL> src{a.B1 + rhs * a.g.b1_rhs + ((long)k * ny + j0) * L, nl, nz * ny * L};
+    InvXStore<T, TAB, Epi> dst{a.tabdip, a.b + rhs * a.xstride, a.y + rhs * a.xstride, a.inv_m, nx,
+                               k * nx * ny + j0 * nx, nl, TL, epi};
     dst.epi.bind(a, rhs);
     fft_tile<C, L, NB, NT, -1, typename TT::LayX>(sm, tw, src, dst);
     if constexpr (Epi::ND > 0) {

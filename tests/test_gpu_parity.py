@@ -247,3 +247,30 @@ def test_context_closed_before_its_spectrum():
     g2 = ctx2.green(4, 4, 4, 10e-9, 1e7)
     g2.close()
     ctx2.close()
+
+
+@pytest.mark.parametrize("meth,prec", [("GPBICG1", 0), ("QMRBICGSTAB1", 0), ("GPBICG1", 1)])
+def test_anisotropic_polarisability_matches_oracle(gctx, orc, meth, prec):
+    """A full 3x3 polarisability per dipole (polarisa(n,a,b) with off-diagonal
+    terms) takes the mat-vec's full-tensor path and the unfused GPBiCG steps."""
+    ob, k0, E0, ff0, G = _c1_inputs(orc, nnnr=10)
+    nb, nmax = ob.nbsphere, ob.nmax
+    pol = ob.polarisa.copy()
+    rng = np.random.default_rng(11)
+    for a in range(3):
+        for b in range(3):
+            pol[np.arange(nb) + nmax * (a + 3 * b)] += 0.1 * ob.alpha * (rng.standard_normal(nb) +
+                                                                       1j * rng.standard_normal(nb))
+    ref = orc.inverserig(G, 10, 10, 10, nb, pol, nmax, ff0, meth, 1e-6, tabdip=ob.tabdip)
+    assert ref["nstop"] == 0
+    g = gctx.green(10, 10, 10, ob.aretecube, k0)
+    r = g.inverserig(nb, pol, nmax, ff0, meth, 1e-6, tabdip=ob.tabdip, precision=prec)
+    assert r.nstop == 0, r.infostr
+    if prec == 0:
+        assert int(r.nloop[0]) == ref["nloop"] and int(r.ncompte[0]) == ref["ncompte"]
+        assert rel(r.FFloc, ref["FFloc"]) < 1e-7
+        assert rel(r.FF, ref["FF"]) < 1e-7
+    else:
+        assert r.tol1[0] < 1e-6
+        assert rel(r.FFloc, ref["FFloc"]) < 1e-4
+    g.close()
