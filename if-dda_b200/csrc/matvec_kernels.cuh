@@ -300,6 +300,58 @@ template <class T, int TL> struct ZStore {
     }
 };
 
+// Group g of the fused zconv middle -> (column il, butterfly j, mirror row h):
+// order 0 takes il fastest, then j, then h; order 1 il, then h, then j.
+__host__ __device__ constexpr void zmid_map(int order, int g, int TL, int NJ, int& il, int& j, int& h) {
+    il = g % TL;
+    if (order == 0) {
+        j = (g / TL) % NJ;
+        h = g / (TL * NJ);
+    } else {
+        h = (g / TL) % 2;
+        j = g / (2 * TL);
+    }
+}
+
+// Shared-memory cost of the middle's reads (points j + r NJ) and writes
+// (points j RK + r) under a group order, for the first warps of a block: each
+// request of 32 lanes is served in phases of 128 bytes (16 lanes of 8-byte or
+// 8 lanes of 16-byte elements), and a phase costs the largest number of
+// distinct addresses that share a bank group.  Used at compile time to pick
+// the order without bank conflicts.
+template <class LZ> constexpr int zmid_cost(int order, int TL, int NJ, int RK, int NG, int S) {
+    const int per = 128 / S;
+    int total = 0;
+    for (int w = 0; w < 4 && w * 32 < NG; w++)
+        for (int pass = 0; pass < 2; pass++)
+            for (int r = 0; r < RK; r++)
+                for (int ph = 0; ph < 32 / per; ph++) {
+                    int addr[16] = {};
+                    int n = 0;
+                    for (int l = 0; l < per; l++) {
+                        const int g = w * 32 + ph * per + l;
+                        if (g >= NG) continue;
+                        int il = 0, j = 0, h = 0;
+                        zmid_map(order, g, TL, NJ, il, j, h);
+                        const int p = pass == 0 ? j + r * NJ : j * RK + r;
+                        addr[n++] = LZ::pidx(p) * LZ::PS + h * 3 * TL + il;
+                    }
+                    int worst = 0;
+                    for (int a = 0; a < n; a++) {
+                        int cnt = 0;
+                        for (int q = 0; q < n; q++) {
+                            if (addr[q] % per != addr[a] % per) continue;
+                            bool dup = false;
+                            for (int z = 0; z < q; z++) dup = dup || addr[z] == addr[q];
+                            if (!dup) cnt++;
+                        }
+                        worst = cnt > worst ? cnt : worst;
+                    }
+                    total += worst;
+                }
+    return total;
+}
+
 // Forward z transform (passes 0 .. n-2 of the plan), then in registers: the
 // last forward pass, the 3x3 multiply and the first pass of the inverse
 // transform run on the reversed plan, so the inverse starts from the values
@@ -315,6 +367,8 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
     constexpr int NJ = L / RK;                 // butterflies per line in that pass
     constexpr int NG = 2 * TL * NJ;            // (row half, column, butterfly) groups
     constexpr int PERM = (NG + NT - 1) / NT;
+    constexpr int S = (int)sizeof(C);
+    constexpr int ORDER = zmid_cost<LZ>(1, TL, NJ, RK, NG, S) < zmid_cost<LZ>(0, TL, NJ, RK, NG, S) ? 1 : 0;
     constexpr int NQ = L / 2 + 1;
     const int rhs = blockIdx.z;
     C* tw = smem_base<C>();
@@ -361,7 +415,8 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
     for (int q = 0; q < PERM; q++) {
         const int g = threadIdx.x + q * NT;
         if (!(PERM * NT == NG || g < NG)) continue;
-        const int il = g % TL, j = (g / TL) % NJ, h = g / (TL * NJ);
+        int il, j, h;
+        zmid_map(ORDER, g, TL, NJ, il, j, h);
         const int i = i0 + il;
 #pragma unroll
         for (int c = 0; c < 3; c++) {
@@ -414,7 +469,8 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
     for (int q = 0; q < PERM; q++) {
         const int g = threadIdx.x + q * NT;
         if (!(PERM * NT == NG || g < NG)) continue;
-        const int il = g % TL, j = (g / TL) % NJ, h = g / (TL * NJ);
+        int il, j, h;
+        zmid_map(ORDER, g, TL, NJ, il, j, h);
 #pragma unroll
         for (int c = 0; c < 3; c++) {
             const int b = (h * 3 + c) * TL + il;
