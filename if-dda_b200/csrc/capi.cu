@@ -68,20 +68,23 @@ bool pola_iso_range(const ifdda_dcmplx* pol, long i0, long i1, long nmax, const 
     return true;
 }
 
-// The scan reads 9 * nb complex numbers of host memory; large objects are
-// split over host threads (one chunk of at least 64K dipoles each).
-int pola_mode(const ifdda_dcmplx* pol, int nb, long nmax) {
-    constexpr long CHUNK = 65536;
+// Isotropy of dipoles [b0, b1): the scan reads 9 complex numbers of host
+// memory per dipole; large ranges are split over up to 16 host threads (one
+// chunk of at least 16K dipoles each).
+int pola_mode_range(const ifdda_dcmplx* pol, long b0, long b1, long nmax) {
+    constexpr long CHUNK = 16384;
+    const long nb = b1 - b0;
+    if (nb <= 0) return ALPHA_ISO;
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     const int nt = (int)std::min<long>({(long)hw, 16L, std::max(1L, (nb + CHUNK - 1) / CHUNK)});
     std::atomic<bool> stop{false};
-    if (nt == 1) return pola_iso_range(pol, 0, nb, nmax, stop) ? ALPHA_ISO : ALPHA_FULL;
+    if (nt == 1) return pola_iso_range(pol, b0, b1, nmax, stop) ? ALPHA_ISO : ALPHA_FULL;
     std::vector<std::thread> th;
     std::vector<char> iso(nt, 1);
     const long per = (nb + nt - 1) / nt;
     for (int t = 0; t < nt; t++)
         th.emplace_back([&, t] {
-            const long i0 = t * per, i1 = std::min<long>(nb, i0 + per);
+            const long i0 = b0 + t * per, i1 = std::min<long>(b1, i0 + per);
             if (i0 < i1 && !pola_iso_range(pol, i0, i1, nmax, stop)) {
                 iso[t] = 0;
                 stop.store(true, std::memory_order_relaxed);
@@ -445,19 +448,45 @@ int ifdda_inverserig_batch(ifdda_green* g, int nrhs, int nbsphere, int nmax, con
         IFDDA_CUDA(cudaMemcpyAsync(g->tab.p, tabdip, geo.N * sizeof(int), cudaMemcpyHostToDevice, st));
         tab = g->tab.p;
     }
-    const int amode = pola_mode(polarisa, nbsphere, nmax);
-    if (amode == ALPHA_ISO) {
-        // the isotropic value of dipole i is polarisa(i,1,1): the first nb
-        // entries of the (nmax,3,3) array, contiguous
-        g->alpha.ensure(nbsphere);
-        IFDDA_CUDA(cudaMemcpyAsync(g->alpha.p, polarisa, nbsphere * sizeof(double2), cudaMemcpyHostToDevice, st));
-    } else {
-        g->alpha.ensure((size_t)9 * nmax);
-        IFDDA_CUDA(cudaMemcpyAsync(g->alpha.p, polarisa, (size_t)9 * nmax * sizeof(double2), cudaMemcpyHostToDevice,
-                                   st));
+    // Isotropy: the first dipoles are checked here (an anisotropic object is
+    // almost always anisotropic there); if they are isotropic the solve starts
+    // with one alpha per dipole while host threads scan the rest, and it is
+    // repeated with the full tensor in the rare case that the rest is not.
+    const long head = std::min<long>(nbsphere, 4096);
+    std::atomic<bool> nostop{false};
+    const int amode = pola_iso_range(polarisa, 0, head, nmax, nostop) ? ALPHA_ISO : ALPHA_FULL;
+    std::atomic<int> tail{ALPHA_ISO};
+    std::thread scan;
+    struct Joiner {
+        std::thread& t;
+        ~Joiner() {
+            if (t.joinable()) t.join();
+        }
+    } joiner{scan};
+    if (amode == ALPHA_ISO && nbsphere > head)
+        scan = std::thread([&] { tail.store(pola_mode_range(polarisa, head, nbsphere, nmax)); });
+    auto upload_alpha = [&](int mode) {
+        if (mode == ALPHA_ISO) {
+            // the isotropic value of dipole i is polarisa(i,1,1): the first nb
+            // entries of the (nmax,3,3) array, contiguous
+            g->alpha.ensure(nbsphere);
+            IFDDA_CUDA(
+                cudaMemcpyAsync(g->alpha.p, polarisa, nbsphere * sizeof(double2), cudaMemcpyHostToDevice, st));
+        } else {
+            g->alpha.ensure((size_t)9 * nmax);
+            IFDDA_CUDA(cudaMemcpyAsync(g->alpha.p, polarisa, (size_t)9 * nmax * sizeof(double2),
+                                       cudaMemcpyHostToDevice, st));
+        }
+    };
+    upload_alpha(amode);
+    int rc = solve_device(g, nrhs, nbsphere, nmax, tab, g->alpha.p, amode, g->ff0.p, methodeit, tol, g->ffb.p, g->x.p,
+                          tol1, nloop, ncompte, nstop, infostr, opt);
+    if (scan.joinable()) scan.join();
+    if (amode == ALPHA_ISO && tail.load() == ALPHA_FULL && rc != -1) {
+        upload_alpha(ALPHA_FULL);
+        rc = solve_device(g, nrhs, nbsphere, nmax, tab, g->alpha.p, ALPHA_FULL, g->ff0.p, methodeit, tol, g->ffb.p,
+                          g->x.p, tol1, nloop, ncompte, nstop, infostr, opt);
     }
-    const int rc = solve_device(g, nrhs, nbsphere, nmax, tab, g->alpha.p, amode, g->ff0.p, methodeit, tol, g->ffb.p,
-                                g->x.p, tol1, nloop, ncompte, nstop, infostr, opt);
     IFDDA_CUDA(cudaMemcpyAsync(FFloc, g->x.p, tot * sizeof(double2), cudaMemcpyDeviceToHost, st));
     IFDDA_CUDA(cudaMemcpyAsync(FF, g->ffb.p, tot * sizeof(double2), cudaMemcpyDeviceToHost, st));
     IFDDA_CUDA(cudaStreamSynchronize(st));

@@ -274,3 +274,23 @@ def test_anisotropic_polarisability_matches_oracle(gctx, orc, meth, prec):
         assert r.tol1[0] < 1e-6
         assert rel(r.FFloc, ref["FFloc"]) < 1e-4
     g.close()
+
+
+def test_anisotropy_only_in_the_tail_matches_oracle(gctx, orc):
+    """The host entry checks the first dipoles before it starts and scans the
+    rest while an isotropic solve runs; a tensor that is anisotropic only
+    beyond that head must still give the full-tensor result."""
+    ob, k0, E0, ff0, G = _c1_inputs(orc, nnnr=24)
+    nb, nmax = ob.nbsphere, ob.nmax
+    assert nb > 5000
+    pol = ob.polarisa.copy()
+    tail = np.arange(5000, nb)
+    pol[tail + nmax * (0 + 3 * 1)] += 0.05 * ob.alpha[tail]
+    pol[tail + nmax * (1 + 3 * 0)] += 0.05 * ob.alpha[tail]
+    ref = orc.inverserig(G, 24, 24, 24, nb, pol, nmax, ff0, "GPBICG1", 1e-6, tabdip=ob.tabdip)
+    g = gctx.green(24, 24, 24, ob.aretecube, k0)
+    r = g.inverserig(nb, pol, nmax, ff0, "GPBICG1", 1e-6, tabdip=ob.tabdip)
+    assert r.nstop == ref["nstop"] == 0
+    assert int(r.nloop[0]) == ref["nloop"] and int(r.ncompte[0]) == ref["ncompte"]
+    assert rel(r.FFloc, ref["FFloc"]) < 1e-7
+    g.close()
