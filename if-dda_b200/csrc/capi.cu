@@ -107,7 +107,16 @@ int method_code(const char* m) {
     memset(buf, ' ', 12);
     buf[12] = 0;
     if (m) memcpy(buf, m, std::min<size_t>(strnlen(m, 12), 12));
+    // the reference's elseif chain (cdmlib/inverserigopt.f:42-1009) compares
+    // prefixes of the blank-padded character(12) methodeit, in this order;
+    // the methods not built here answer "Iterative method not correct!"
     if (!strncmp(buf, "GPBICG1", 7)) return 1;
+    if (!strncmp(buf, "GPBICG2", 7) || !strncmp(buf, "GPBICGsafe", 10) || !strncmp(buf, "GPBICGplus", 10) ||
+        !strncmp(buf, "GPBICGAR", 8) || !strncmp(buf, "BICGSTARPLUS", 12) || !strncmp(buf, "QMRCLA", 6) ||
+        !strncmp(buf, "TFQMR", 5))
+        return 0;
+    if (!strncmp(buf, "CG   ", 5)) return 5;
+    if (!strncmp(buf, "BICGSTAB", 8)) return 4;
     if (!strncmp(buf, "QMRBICGSTAB1", 12)) return 2;
     if (!strncmp(buf, "QMRBICGSTAB2", 12)) return 3;
     return 0;

@@ -133,7 +133,7 @@ template void cast_dev<double>(const double2*, double2*, long, cudaStream_t);
 int reduction_blocks(long n3) { return (int)std::max<long>(1, std::min<long>((n3 + KNT * 4 - 1) / (KNT * 4), 1024)); }
 
 template <class T> void KrylovWork<T>::ensure(int method, int nrhs_, long n3_) {
-    nslot = method == 1 ? (int)G_NSLOT : (int)Q_NSLOT;
+    nslot = method == 1 ? (int)G_NSLOT : method == 4 ? (int)B_NSLOT : method == 5 ? (int)C_NSLOT : (int)Q_NSLOT;
     nrhs = nrhs_;
     n3 = n3_;
     nblk = reduction_blocks(n3);
@@ -266,6 +266,18 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
             mv_solver<T>(G, sp, W, tnew, G_AT, status, st);
             vec_launch<3>(GpZeta<T>{V, S, tnew}, n3, nblk, nrhs, rs, status, st);
             vec_launch<2>(GpUpdate<T>{V, S, tcur, tnew}, n3, nblk, nrhs, rs, status, st);
+        } else if (sp.method == 4) {
+            vec_launch<0>(BP<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            mv_solver<T>(G, sp, W, B_P, B_V, status, st);
+            vec_launch<1>(BXi<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<1>(BS<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            mv_solver<T>(G, sp, W, B_S, B_T, status, st);
+            vec_launch<2>(BOmega<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<1>(BUpdate<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+        } else if (sp.method == 5) {
+            vec_launch<1>(CUpdate<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            mv_solver<T>(G, sp, W, C_R, C_S, status, st);
+            vec_launch<2>(CBeta<T>{V, S}, n3, nblk, nrhs, rs, status, st);
         } else {
             vec_launch<0>(QP<T>{V, S}, n3, nblk, nrhs, rs, status, st);
             mv_solver<T>(G, sp, W, Q_P, Q_V, status, st);
@@ -282,6 +294,16 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
         vec_launch<1>(GpStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
         if (!sp.zero_guess) mv_solver<T>(G, sp, W, G_X, G_XR, status, st);
         vec_launch<1>(GpInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+    } else if (sp.method == 4) {
+        vec_launch<1>(BStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
+        if (!sp.zero_guess) mv_solver<T>(G, sp, W, B_X, B_XR, status, st);
+        vec_launch<2>(BInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+    } else if (sp.method == 5) {
+        vec_launch<1>(CStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
+        if (!sp.zero_guess) mv_solver<T>(G, sp, W, C_X, C_XR, status, st);
+        vec_launch<2>(CInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+        mv_solver<T>(G, sp, W, C_P, C_W, status, st);
+        vec_launch<1>(CXi<T>{V, S}, n3, nblk, nrhs, rs, status, st);
     } else {
         vec_launch<1>(QStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
         if (!sp.zero_guess) mv_solver<T>(G, sp, W, Q_X, Q_XR, status, st);
@@ -416,9 +438,34 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
     return !cancelled;
 }
 
-template <class T> int KrylovWork<T>::x_slot(int method) const { return method == 1 ? (int)G_X : (int)Q_X; }
-template <class T> int KrylovWork<T>::b_slot(int method) const { return method == 1 ? (int)G_B : (int)Q_B; }
-template <class T> int KrylovWork<T>::xr_slot(int method) const { return method == 1 ? (int)G_XR : (int)Q_XR; }
+template <class T> int KrylovWork<T>::x_slot(int method) const {
+    return method == 1 ? (int)G_X : method == 4 ? (int)B_X : method == 5 ? (int)C_X : (int)Q_X;
+}
+template <class T> int KrylovWork<T>::b_slot(int method) const {
+    return method == 1 ? (int)G_B : method == 4 ? (int)B_B : method == 5 ? (int)C_B : (int)Q_B;
+}
+template <class T> int KrylovWork<T>::xr_slot(int method) const {
+    return method == 1 ? (int)G_XR : method == 4 ? (int)B_XR : method == 5 ? (int)C_XR : (int)Q_XR;
+}
+
+// Mat-vecs and iterations the reference's driver counts for a solve that
+// ended after `itno` passes of the method's loop (GPBICG: one pass less than
+// the iterations it reports, cdmlib/inverserigopt.f:42-107; QMR-BiCGSTAB and
+// BiCGSTAB: two mat-vecs per iteration plus the first and the residual one,
+// :743-942; CG: one per iteration plus A x0, A p0 and the residual one,
+// :676-742).
+void method_counts(int method, int itno, int& nloop, int& ncompte) {
+    if (method == 1) {
+        nloop = itno + 1;
+        ncompte = 1 + 2 * (itno + 1) + 1;
+    } else if (method == 5) {
+        nloop = itno;
+        ncompte = itno + 2;
+    } else {
+        nloop = itno;
+        ncompte = 2 + 2 * itno;
+    }
+}
 
 template struct KrylovWork<float>;
 template struct KrylovWork<double>;
@@ -442,6 +489,12 @@ void solve_fp64(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b_
     IFDDA_CUDA(cudaMemcpyAsync(hs.data(), W.st.p, sp.nrhs * sizeof(KState), cudaMemcpyDeviceToHost, st));
     IFDDA_CUDA(cudaMemcpyAsync(W.hstatus.data(), W.status.p, sp.nrhs * sizeof(int), cudaMemcpyDeviceToHost, st));
     IFDDA_CUDA(cudaStreamSynchronize(st));
+    // BiCGSTAB's soft breakdown returns x = p (cdmlib/pimzbicgstab.f:145-156)
+    if (sp.method == 4)
+        for (int r = 0; r < sp.nrhs; r++)
+            if (W.hstatus[r] < 0 && hs[r].steperr == 12)
+                IFDDA_CUDA(cudaMemcpyAsync(V.v(B_X, r), V.v(B_P, r), sp.n3 * sizeof(double2), cudaMemcpyDeviceToDevice,
+                                           st));
     // final A x and true residual, for every right-hand side that did not break down
     IFDDA_CUDA(cudaMemsetAsync(W.zstatus.p, 0, sp.nrhs * sizeof(int), st));
     {
@@ -462,13 +515,7 @@ void solve_fp64(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b_
         o.steperr = hs[r].steperr;
         o.cancelled = !ok;
         o.tol1 = hf[r].residu;
-        if (sp.method == 1) {
-            o.nloop = hs[r].itno + 1;
-            o.ncompte = 1 + 2 * (hs[r].itno + 1) + 1;
-        } else {
-            o.nloop = hs[r].itno;
-            o.ncompte = 2 + 2 * hs[r].itno;
-        }
+        method_counts(sp.method, hs[r].itno, o.nloop, o.ncompte);
         o.ncompte64 = o.ncompte;
         o.outer = 0;
     }
@@ -556,9 +603,10 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
         IFDDA_CUDA(cudaStreamSynchronize(st));
         for (int r = 0; r < nrhs; r++) {
             if (ost[r]) continue;
-            const long its = sp.method == 1 ? hs[r].itno + 1 : hs[r].itno;
+            int its = 0, mvs = 0;
+            method_counts(sp.method, hs[r].itno, its, mvs);
             inner_iters[r] += its;
-            inner_mv[r] += 2 * its;
+            inner_mv[r] += sp.method == 5 ? its + 1 : 2 * its;  // zero initial guess: no A x0
             inner_runs[r] += 1;
         }
         count_launch();

@@ -443,6 +443,280 @@ template <class T> struct QX {
     }
 };
 
+// -------------------------------------------------------------- BiCGSTAB ----
+// cdmlib/pimzbicgstab.f:1-216 as the reference writes it: NORM is the SQUARED
+// norm of the initial residual, rho = r^H r, the loop stops when
+// ||r||^2 / NORM <= tol / 10, and ITNO > MAXIT, a zero denominator or
+// ||s|| < 1e-15 (soft breakdown: x = p, done by the host) end it with an
+// error status.  KState: alpha, beta, omega, rho; itno = ITNO.
+// slots: 0 r, 1 rtilde, 2 p, 3 v = A p, 4 s, 5 t = A s, 6 x, 7 xr (mat-vec out), 8 b
+enum { B_R = 0, B_RT, B_P, B_V, B_S, B_T, B_X, B_XR, B_B, B_NSLOT };
+
+// x = x0 (FF0) or 0 (pimzbicgstab.f:40-47)
+template <class T> struct BStart {
+    Slots<T> V;
+    KState* stt;
+    int zero_guess;
+    __device__ void elem(const KState&, int r, long i, double2*) const {
+        st(V.v(B_X, r), i, zero_guess ? make_double2(0, 0) : ld(V.v(B_B, r), i));
+        if (zero_guess) st(V.v(B_XR, r), i, make_double2(0, 0));
+    }
+    __device__ void finish(int, KState& s, int&, const double2*) const {
+        s.steperr = -1;
+        s.itno = 0;
+    }
+};
+
+// label 10 (pimzbicgstab.f:52-72) and the first pass of label 100
+// (:76-97): r = b - A x0, rtilde = r, p = v = 0, NORM = ||r||^2,
+// rho = alpha = omega = 1, then ITNO = 1, rho = r^H r, beta = rho
+template <class T> struct BInit {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 rr = zsub(ld(V.v(B_B, r), i), ld(V.v(B_XR, r), i));
+        const double2 z = make_double2(0, 0);
+        st(V.v(B_R, r), i, rr);
+        st(V.v(B_RT, r), i, rr);
+        st(V.v(B_P, r), i, z);
+        st(V.v(B_V, r), i, z);
+        acc[0].x += rr.x * rr.x + rr.y * rr.y;
+        acc[1] = zadd(acc[1], zconjmul(rr, rr));
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.norm = a[0].x;
+        s.alpha = make_double2(1, 0);
+        s.omega = make_double2(1, 0);
+        s.itno = 1;
+        s.rho = a[1];
+        s.beta = s.rho;  // rho alpha / (rho0 omega) with rho0 = alpha = omega = 1
+    }
+};
+
+// pimzbicgstab.f:100-110: p = r + beta (p - omega v)
+template <class T> struct BP {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2*) const {
+        const double2 q = zsub(ld(V.v(B_P, r), i), zmul(s.omega, ld(V.v(B_V, r), i)));
+        st(V.v(B_P, r), i, zadd(ld(V.v(B_R, r), i), zmul(s.beta, q)));
+    }
+    __device__ void finish(int, KState&, int&, const double2*) const {}
+};
+
+// label 20 (pimzbicgstab.f:114-131): xi = rtilde^H v, alpha = rho / xi
+template <class T> struct BXi {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        acc[0] = zadd(acc[0], zconjmul(ld(V.v(B_RT, r), i), ld(V.v(B_V, r), i)));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        if (zisnull(a[0])) {
+            status = -1;
+            s.steperr = 10;
+            return;
+        }
+        s.alpha = zdiv(s.rho, a[0]);
+    }
+};
+
+// pimzbicgstab.f:133-157: s = r - alpha v, soft breakdown when ||s|| < 1e-15
+template <class T> struct BS {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2* acc) const {
+        const double2 sv = zsub(ld(V.v(B_R, r), i), zmul(s.alpha, ld(V.v(B_V, r), i)));
+        st(V.v(B_S, r), i, sv);
+        acc[0] = zadd(acc[0], zconjmul(sv, sv));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        const double2 k = zsqrt(a[0]);
+        if (hypot(k.x, k.y) < 1e-15) {
+            status = -1;
+            s.steperr = 12;
+        }
+    }
+};
+
+// label 30 (pimzbicgstab.f:169-186): omega = t^H s / t^H t
+template <class T> struct BOmega {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 t = ld(V.v(B_T, r), i);
+        acc[0] = zadd(acc[0], zconjmul(t, t));
+        acc[1] = zadd(acc[1], zconjmul(t, ld(V.v(B_S, r), i)));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        if (zisnull(a[0])) {
+            status = -1;
+            s.steperr = 14;
+            return;
+        }
+        s.omega = zdiv(a[1], a[0]);
+    }
+};
+
+// pimzbicgstab.f:188-211: x += alpha p + omega s, r = s - omega t, the stop
+// test, then the next pass of label 100: rho0 = rho, rho = r^H r,
+// beta = rho alpha / (rho0 omega)
+template <class T> struct BUpdate {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2* acc) const {
+        const double2 sv = ld(V.v(B_S, r), i);
+        st(V.v(B_X, r), i,
+           zadd(zadd(ld(V.v(B_X, r), i), zmul(s.alpha, ld(V.v(B_P, r), i))), zmul(s.omega, sv)));
+        const double2 rn = zsub(sv, zmul(s.omega, ld(V.v(B_T, r), i)));
+        st(V.v(B_R, r), i, rn);
+        acc[0] = zadd(acc[0], zconjmul(rn, rn));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        const double2 c = make_double2(a[0].x / s.norm, a[0].y / s.norm);
+        s.residu = hypot(c.x, c.y);
+        if (s.itno > s.maxit) {
+            status = -1;
+            s.steperr = 0;
+            s.itno = s.maxit;
+            return;
+        }
+        if (hypot(c.x, c.y) <= s.tol / 10.0) {
+            status = 1;
+            s.steperr = 0;
+            return;
+        }
+        s.itno += 1;
+        const double2 rho0 = s.rho;
+        s.rho = a[0];
+        const double2 kappa = zmul(rho0, s.omega);
+        if (zisnull(kappa)) {
+            status = -1;
+            s.steperr = 6;
+            return;
+        }
+        s.beta = zdiv(zmul(s.rho, s.alpha), kappa);
+    }
+};
+
+// ---------------------------------------------------------------- ZCG ----
+// Conjugate gradient for complex-symmetric systems (unconjugated dot
+// products), cdmlib/zcg.f:1-179: one mat-vec per iteration, w = A p carried
+// by w = A r + beta w.  NORM = ||b||; the loop stops when ||r|| / NORM <= tol;
+// NLOOP >= MAXIT and p^T A p = 0 (where the reference stops the program) end
+// it with an error status.  KState: alpha, beta, rho = rho0, c2 = xi;
+// itno = NLOOP.
+// slots: 0 x, 1 r, 2 p, 3 s = A r, 4 w, 5 xr (mat-vec out), 6 b
+enum { C_X = 0, C_R, C_P, C_S, C_W, C_XR, C_B, C_NSLOT };
+
+template <class T> struct CStart {
+    Slots<T> V;
+    KState* stt;
+    int zero_guess;
+    __device__ void elem(const KState&, int r, long i, double2*) const {
+        st(V.v(C_X, r), i, zero_guess ? make_double2(0, 0) : ld(V.v(C_B, r), i));
+        if (zero_guess) st(V.v(C_XR, r), i, make_double2(0, 0));
+    }
+    __device__ void finish(int, KState& s, int&, const double2*) const {
+        s.steperr = -1;
+        s.itno = 0;
+    }
+};
+
+// label 10 (zcg.f:45-64): r = b - A x0, p = r, NORM = ||b||, rho0 = r^T r
+template <class T> struct CInit {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 b = ld(V.v(C_B, r), i);
+        const double2 rr = zsub(b, ld(V.v(C_XR, r), i));
+        st(V.v(C_R, r), i, rr);
+        st(V.v(C_P, r), i, rr);
+        acc[0].x += b.x * b.x + b.y * b.y;
+        acc[1] = zadd(acc[1], zmul(rr, rr));
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.norm = sqrt(a[0].x);
+        s.rho = a[1];
+        s.itno = 0;
+    }
+};
+
+// next pass of label 50 (zcg.f:74-85): NLOOP += 1, the iteration limit, alpha
+__device__ __forceinline__ void cg_next(KState& s, int& status) {
+    s.itno += 1;
+    if (s.itno >= s.maxit) {
+        status = -1;
+        s.steperr = 0;
+        return;
+    }
+    s.alpha = zdiv(s.rho, s.c2);
+}
+
+// label 20 (zcg.f:66-73): xi = p^T w with w = A p, then label 50
+template <class T> struct CXi {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        acc[0] = zadd(acc[0], zmul(ld(V.v(C_P, r), i), ld(V.v(C_W, r), i)));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        s.c2 = a[0];
+        if (a[0].x == 0.0 && a[0].y == 0.0) {
+            status = -1;
+            s.steperr = 3;
+            return;
+        }
+        cg_next(s, status);
+    }
+};
+
+// zcg.f:154-157 (after the first iteration: p = r + beta p, w = s + beta w),
+// then zcg.f:89-110: x += alpha p, r -= alpha w, stop when ||r||/NORM <= tol
+template <class T> struct CUpdate {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2* acc) const {
+        double2 p = ld(V.v(C_P, r), i), w = ld(V.v(C_W, r), i);
+        const double2 rr = ld(V.v(C_R, r), i);
+        if (s.itno > 1) {
+            p = zadd(rr, zmul(s.beta, p));
+            w = zadd(ld(V.v(C_S, r), i), zmul(s.beta, w));
+            st(V.v(C_P, r), i, p);
+            st(V.v(C_W, r), i, w);
+        }
+        st(V.v(C_X, r), i, zadd(ld(V.v(C_X, r), i), zmul(s.alpha, p)));
+        const double2 rn = zsub(rr, zmul(s.alpha, w));
+        st(V.v(C_R, r), i, rn);
+        acc[0].x += rn.x * rn.x + rn.y * rn.y;
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        s.residu = sqrt(a[0].x) / s.norm;
+        if (s.residu <= s.tol) {
+            status = 1;
+            s.steperr = 0;
+        }
+    }
+};
+
+// label 30 (zcg.f:139-160): rho = r^T r, delta = r^T s, beta = rho / rho0,
+// xi = delta - beta^2 xi, then label 50
+template <class T> struct CBeta {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 rr = ld(V.v(C_R, r), i);
+        acc[0] = zadd(acc[0], zmul(rr, rr));
+        acc[1] = zadd(acc[1], zmul(rr, ld(V.v(C_S, r), i)));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        s.beta = zdiv(a[0], s.rho);
+        s.rho = a[0];
+        s.c2 = zsub(a[1], zmul(zmul(s.beta, s.beta), s.c2));
+        cg_next(s, status);
+    }
+};
+
 // ------------------------------------------------------------ shared ------
 // y = alpha . x (polarisability, cdmlib/inverserigopt.f:68-80) on FP64 vectors
 __global__ void k_apply_alpha(const double2* __restrict__ x, double2* __restrict__ y, long nd, int nrhs, long stride,

@@ -105,10 +105,13 @@ int ifdda_matvec_noalloc(ifdda_green* g, int precision, int ndip, const int* tab
 /* Rigorous solve.  Replaces inverserigopt (cdmlib/inverserigopt.f:1-1085,
    tabdip == NULL) and inverserig (cdmlib/inverserig.f:1-1090, tabdip != NULL),
    called at cdmlib/cdmlib.f:1565-1581: initial guess FF0, methodeit
-   "GPBICG1" | "QMRBICGSTAB1" | "QMRBICGSTAB2" (others: nstop = 1,
-   "Iterative method not correct!"), on return FFloc = E (local field),
-   FF = polarisa . E (dipole moments), tol1 = ||A E - FF0|| / ||FF0||
-   (FP64), nloop iterations, ncompte mat-vecs.  *nstop is read during the
+   "GPBICG1" | "QMRBICGSTAB1" | "QMRBICGSTAB2" | "BICGSTAB" (pimzbicgstab.f)
+   | "CG" (zcg.f), matched by prefix in the reference's order; the other
+   methods of the reference answer nstop = 1, "Iterative method not
+   correct!".  On return FFloc = E (local field), FF = polarisa . E (dipole
+   moments), tol1 = ||A E - FF0|| / NORM in FP64 with the method's NORM
+   (||FF0||; for BICGSTAB the squared norm of the initial residual, as the
+   reference computes it), nloop iterations, ncompte mat-vecs.  *nstop is read during the
    solve: a value of -1 written by another thread cancels it, as in the
    reference (cdm/cdmRunWidget.cpp:156).  A converged tol1 >= tol is reported
    as nstop = 1 "Converge do not reach!" (cdmlib/cdmlib.f:1586-1591).

@@ -609,6 +609,217 @@ L40:
 }
 
 /* ------------------------------------------------------------------------- */
+/* BiCGSTAB reverse-communication state machine: cdmlib/pimzbicgstab.f:1-216. */
+/* x is the caller's solution array (FFLOC in the reference).  Work columns:  */
+/* 0 r, 1 rtilde, 2 p, 4 s, 5 t, 6 v, 7 A x0.  The reference keeps NORM as the */
+/* SQUARED norm of the initial residual, takes rho = r^H r (not rtilde^H r),  */
+/* stops when ||r||^2 / NORM <= tol / 10 and reports ITNO > MAXIT as an error. */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    zc alpha, omega, rho;
+    double norm;
+} bicgstab_state;
+
+static void bicgstab(zc *x, zc *xi, zc *xr, const zc *B, long n, int *nou, zc *W, int *itno,
+                     int maxit, double tol, bicgstab_state *S, int *status, int *steperr) {
+#define WK(c) (W + (size_t)(c) * n)
+    zc *r = WK(0), *rt = WK(1), *p = WK(2), *s = WK(4), *t = WK(5), *v = WK(6), *ax0 = WK(7);
+#undef WK
+    if (*nou == 1) goto L10;
+    if (*nou == 2) goto L20;
+    if (*nou == 3) goto L30;
+    if (*nou == 4) goto L100;
+    *status = 0;
+    *steperr = -1;
+    for (long i = 0; i < n; i++) {
+        r[i] = B[i];
+        x[i] = xi[i];
+    }
+    *nou = 1;
+    return;
+L10: {
+    double nrm = 0;
+#pragma omp parallel for reduction(+ : nrm)
+    for (long i = 0; i < n; i++) {
+        ax0[i] = xr[i];
+        r[i] = r[i] - ax0[i];
+        nrm += creal(r[i] * conj(r[i]));
+        rt[i] = r[i];
+        p[i] = 0;
+        v[i] = 0;
+    }
+    S->norm = nrm;
+}
+    S->rho = 1;
+    S->alpha = 1;
+    S->omega = 1;
+    *itno = 0;
+L100: {
+    *itno += 1;
+    const zc rho0 = S->rho;
+    S->rho = zsum(r, r, n, 1);
+    const zc kappa = rho0 * S->omega;
+    if (cabs(kappa) == 0.0) {
+        *status = -3;
+        *steperr = 6;
+        return;
+    }
+    const zc beta = S->rho * S->alpha / kappa, om = S->omega;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        const zc q = p[i] - om * v[i];
+        p[i] = r[i] + beta * q;
+        xi[i] = p[i];
+    }
+    *nou = 2;
+    return;
+}
+L20: {
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) v[i] = xr[i];
+    const zc xxi = zsum(rt, v, n, 1);
+    if (cabs(xxi) == 0.0) {
+        *status = -3;
+        *steperr = 10;
+        return;
+    }
+    S->alpha = S->rho / xxi;
+    const zc al = S->alpha;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) s[i] = r[i] - al * v[i];
+    const zc kappa = csqrt(zsum(s, s, n, 1));
+    if (cabs(kappa) < 1e-15) {
+        *status = -2;
+        *steperr = 12;
+        for (long i = 0; i < n; i++) x[i] = p[i];
+        return;
+    }
+    for (long i = 0; i < n; i++) xi[i] = s[i];
+    *nou = 3;
+    return;
+}
+L30: {
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) t[i] = xr[i];
+    const zc c1 = zsum(t, t, n, 1), c2 = zsum(t, s, n, 1);
+    if (cabs(c1) == 0.0) {
+        *status = -3;
+        *steperr = 14;
+        return;
+    }
+    S->omega = c2 / c1;
+    const zc al = S->alpha, om = S->omega;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        x[i] = x[i] + al * p[i] + om * s[i];
+        r[i] = s[i] - om * t[i];
+    }
+    const zc c = zsum(r, r, n, 1) / S->norm;
+    if (*itno > maxit) {
+        *status = -1;
+        *itno = maxit;
+        return;
+    }
+    if (cabs(c) <= tol / 10.0) {
+        *status = 1;
+        *nou = 4;
+        return;
+    }
+    goto L100;
+}
+}
+
+/* ------------------------------------------------------------------------- */
+/* Conjugate gradient for complex-symmetric systems (dot products without     */
+/* conjugation), reverse communication: cdmlib/zcg.f:1-179.  One mat-vec per  */
+/* iteration: w = A p is carried by the recurrence w = A r + beta w.  Work    */
+/* columns: 0 x, 1 r, 2 p, 3 s = A r, 4 w.  Where the reference stops the     */
+/* program (xi = p^T A p = 0) the restatement returns status -3.              */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    zc rho0, xxi;
+    double norm;
+} cg_state;
+
+static void zcg(zc *xi, zc *xr, const zc *B, long n, int *nou, zc *W, int *nloop, int maxit,
+                double tol, cg_state *S, int *status) {
+#define WK(c) (W + (size_t)(c) * n)
+    zc *x = WK(0), *r = WK(1), *p = WK(2), *s = WK(3), *w = WK(4);
+#undef WK
+    if (*nou == 1) goto L10;
+    if (*nou == 2) goto L20;
+    if (*nou == 3) goto L30;
+    if (*nou == 4) goto L40;
+    *nou = 1;
+    *status = 0;
+    for (long i = 0; i < n; i++) x[i] = xi[i];
+    return;
+L10: {
+    double nrm = 0;
+#pragma omp parallel for reduction(+ : nrm)
+    for (long i = 0; i < n; i++) {
+        r[i] = B[i] - xr[i];
+        nrm += creal(B[i] * conj(B[i]));
+        p[i] = r[i];
+        xi[i] = p[i];
+    }
+    S->norm = sqrt(nrm);
+    S->rho0 = zsum(r, r, n, 0);
+    *nou = 2;
+    return;
+}
+L20: {
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) w[i] = xr[i];
+    S->xxi = zsum(p, w, n, 0);
+    if (S->xxi == 0) {
+        *status = -3;
+        return;
+    }
+}
+L50: {
+    *nloop += 1;
+    if (*nloop >= maxit) {
+        *status = -4;
+        *nou = 0;
+        for (long i = 0; i < n; i++) xi[i] = x[i];
+        return;
+    }
+    const zc al = S->rho0 / S->xxi;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        x[i] = x[i] + al * p[i];
+        r[i] = r[i] - al * w[i];
+    }
+    const double tole = sqrt(cabs(zsum(r, r, n, 1))) / S->norm;
+    if (tole <= tol) {
+        *status = 1;
+        for (long i = 0; i < n; i++) xi[i] = x[i];
+        *nou = 4;
+        return;
+    }
+}
+L40:
+    *nou = 3;
+    for (long i = 0; i < n; i++) xi[i] = r[i];
+    return;
+L30: {
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) s[i] = xr[i];
+    const zc rho = zsum(r, r, n, 0), delta = zsum(r, s, n, 0);
+    const zc beta = rho / S->rho0;
+    S->rho0 = rho;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        p[i] = r[i] + beta * p[i];
+        w[i] = s[i] + beta * w[i];
+    }
+    S->xxi = delta - beta * beta * S->xxi;
+    goto L50;
+}
+}
+
+/* ------------------------------------------------------------------------- */
 /* Solver driver: cdmlib/inverserigopt.f:1-107 (GPBICG1), :811-942             */
 /* (QMRBICGSTAB1/2) and cdmlib/inverserig.f (tabdip != NULL).                  */
 /* Returns nstop; infostr receives the reference's messages (space padded to   */
@@ -655,8 +866,16 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
     memset(meth, ' ', 12);
     meth[12] = 0;
     memcpy(meth, methodeit, strnlen(methodeit, 12));
+    /* the reference's elseif chain (inverserigopt.f:42-1009) compares prefixes
+       of the blank-padded character(12) methodeit, in this order */
     int kind = 0;
     if (strncmp(meth, "GPBICG1", 7) == 0) kind = 1;
+    else if (strncmp(meth, "GPBICG2", 7) == 0 || strncmp(meth, "GPBICGsafe", 10) == 0 ||
+             strncmp(meth, "GPBICGplus", 10) == 0 || strncmp(meth, "GPBICGAR", 8) == 0 ||
+             strncmp(meth, "BICGSTARPLUS", 12) == 0 || strncmp(meth, "QMRCLA", 6) == 0 ||
+             strncmp(meth, "TFQMR", 5) == 0) kind = 0;
+    else if (strncmp(meth, "CG   ", 5) == 0) kind = 5;
+    else if (strncmp(meth, "BICGSTAB", 8) == 0) kind = 4;
     else if (strncmp(meth, "QMRBICGSTAB1", 12) == 0) kind = 2;
     else if (strncmp(meth, "QMRBICGSTAB2", 12) == 0) kind = 3;
     if (kind == 0) {
@@ -667,16 +886,27 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
     }
     gpbicg_state gs;
     qmr_state qs;
+    bicgstab_state bs;
+    cg_state cs;
     memset(&gs, 0, sizeof gs);
     memset(&qs, 0, sizeof qs);
+    memset(&bs, 0, sizeof bs);
+    memset(&cs, 0, sizeof cs);
     double norm = 0;
+    /* GPBICG and CG return the solution in xi; QMR-BiCGSTAB and BiCGSTAB in
+       FFloc (the X argument), which the driver copies back to xi */
+    const int x_in_floc = kind == 2 || kind == 3 || kind == 4;
     for (;;) {
         if (kind == 1)
             gpbicg(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &gs, &nstat, &steperr);
+        else if (kind == 4)
+            bicgstab(FFloc, xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &bs, &nstat, &steperr);
+        else if (kind == 5)
+            zcg(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &cs, &nstat);
         else
             qmrbicgstab(FFloc, xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &qs,
                         kind == 2 ? 1 : 2, &nstat, &steperr);
-        norm = kind == 1 ? gs.norm : qs.norm;
+        norm = kind == 1 ? gs.norm : kind == 4 ? bs.norm : kind == 5 ? cs.norm : qs.norm;
         if (nstat < 0) {
             *nstop = 1;
             set_info(infostr, "Problem to solve Ax=b!");
@@ -684,7 +914,7 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
             return *nstop;
         }
         *ncompte += 1;
-        if (kind == 1) {
+        if (!x_in_floc) {
             memcpy(xr, xi, sizeof(zc) * n3);
             if (nstat == 1) memcpy(FFloc, xi, sizeof(zc) * n3);
         } else {

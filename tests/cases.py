@@ -45,6 +45,7 @@ def random_field(n3, seed):
 
 
 def rel(a, b):
-    a = np.asarray(a)
-    b = np.asarray(b)
+    # in FP64, whatever the inputs' precision (FP32 squares can overflow)
+    a = np.asarray(a, np.complex128)
+    b = np.asarray(b, np.complex128)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))

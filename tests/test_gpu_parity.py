@@ -294,3 +294,41 @@ def test_anisotropy_only_in_the_tail_matches_oracle(gctx, orc):
     assert int(r.nloop[0]) == ref["nloop"] and int(r.ncompte[0]) == ref["ncompte"]
     assert rel(r.FFloc, ref["FFloc"]) < 1e-7
     g.close()
+
+
+@pytest.mark.parametrize("meth", ["BICGSTAB", "CG"])
+def test_bicgstab_and_cg_match_oracle(gctx, orc, meth):
+    """The reference's BiCGSTAB (pimzbicgstab.f) and complex-symmetric CG
+    (zcg.f) on the sphere (inside-only, Tabdip) and on a full-box GRF cube:
+    identical counters, local field within 1e-7, the method's tol1."""
+    ob, k0, E0, ff0, G = _c1_inputs(orc)
+    ref = orc.inverserig(G, 16, 16, 16, ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-5, tabdip=ob.tabdip)
+    assert ref["nstop"] == 0, ref["infostr"]
+    g = gctx.green(16, 16, 16, ob.aretecube, k0)
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-5, tabdip=ob.tabdip)
+    assert r.nstop == 0, r.infostr
+    assert int(r.nloop[0]) == ref["nloop"] and int(r.ncompte[0]) == ref["ncompte"]
+    assert abs(r.tol1[0] - ref["tol1"]) <= 1e-6 * ref["tol1"]
+    assert rel(r.FFloc, ref["FFloc"]) < 1e-7 and rel(r.FF, ref["FF"]) < 1e-7
+    g.close()
+    ob, k0, ff0, G = _grf(orc, 16)
+    ref = orc.inverserig(G, 16, 16, 16, ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-5)
+    g = gctx.green(16, 16, 16, ob.aretecube, k0)
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-5)
+    assert (r.nstop, int(r.nloop[0]), int(r.ncompte[0])) == (ref["nstop"], ref["nloop"], ref["ncompte"])
+    assert rel(r.FFloc, ref["FFloc"]) < 1e-7
+    g.close()
+
+
+@pytest.mark.parametrize("meth", ["BICGSTAB", "CG"])
+def test_bicgstab_and_cg_mixed_precision(gctx, orc, meth):
+    from ifdda import IFDDA_MIXED
+    ob, k0, E0, ff0, G = _c1_inputs(orc)
+    tight = orc.inverserig(G, 16, 16, 16, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-10,
+                           tabdip=ob.tabdip)
+    g = gctx.green(16, 16, 16, ob.aretecube, k0)
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-4, tabdip=ob.tabdip, precision=IFDDA_MIXED)
+    assert r.nstop == 0, r.infostr
+    assert r.tol1[0] < 1e-4
+    assert rel(r.FFloc, tight["FFloc"]) < 1e-3
+    g.close()

@@ -21,6 +21,10 @@ pytestmark = pytest.mark.gpu
 
 
 def _rel(a, b):
+    # in FP64: without a polarisability the values reach ~1e25, whose squares
+    # overflow a single-precision norm
+    a = np.asarray(a, np.complex128)
+    b = np.asarray(b, np.complex128)
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
