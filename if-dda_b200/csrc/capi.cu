@@ -112,9 +112,9 @@ int method_code(const char* m) {
     // the methods not built here answer "Iterative method not correct!"
     if (!strncmp(buf, "GPBICG1", 7)) return 1;
     if (!strncmp(buf, "GPBICG2", 7) || !strncmp(buf, "GPBICGsafe", 10) || !strncmp(buf, "GPBICGplus", 10) ||
-        !strncmp(buf, "GPBICGAR", 8) || !strncmp(buf, "BICGSTARPLUS", 12) || !strncmp(buf, "QMRCLA", 6) ||
-        !strncmp(buf, "TFQMR", 5))
+        !strncmp(buf, "GPBICGAR", 8) || !strncmp(buf, "BICGSTARPLUS", 12) || !strncmp(buf, "QMRCLA", 6))
         return 0;
+    if (!strncmp(buf, "TFQMR", 5)) return 6;
     if (!strncmp(buf, "CG   ", 5)) return 5;
     if (!strncmp(buf, "BICGSTAB", 8)) return 4;
     if (!strncmp(buf, "QMRBICGSTAB1", 12)) return 2;
@@ -188,7 +188,9 @@ int solve_device(ifdda_green* g, int nrhs, int nb, int nmax, const int* tab_dev,
             msg = "Calculation cancelled during iterative method";
         } else if (res[r].status < 0) {
             rc = 1;
-            msg = "Problem to solve Ax=b!";
+            // the TFQMR branch of the reference words it without '!'
+            // (cdmlib/inverserigopt.f:609)
+            msg = method == 6 ? "Problem to solve Ax=b" : "Problem to solve Ax=b!";
         } else if (!(res[r].tol1 < tol)) {
             rc = 1;
             msg = "Converge do not reach!";

@@ -133,7 +133,11 @@ template void cast_dev<double>(const double2*, double2*, long, cudaStream_t);
 int reduction_blocks(long n3) { return (int)std::max<long>(1, std::min<long>((n3 + KNT * 4 - 1) / (KNT * 4), 1024)); }
 
 template <class T> void KrylovWork<T>::ensure(int method, int nrhs_, long n3_) {
-    nslot = method == 1 ? (int)G_NSLOT : method == 4 ? (int)B_NSLOT : method == 5 ? (int)C_NSLOT : (int)Q_NSLOT;
+    nslot = method == 1   ? (int)G_NSLOT
+            : method == 4 ? (int)B_NSLOT
+            : method == 5 ? (int)C_NSLOT
+            : method == 6 ? (int)T_NSLOT
+                          : (int)Q_NSLOT;
     nrhs = nrhs_;
     n3 = n3_;
     nblk = reduction_blocks(n3);
@@ -274,6 +278,21 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
             mv_solver<T>(G, sp, W, B_S, B_T, status, st);
             vec_launch<2>(BOmega<T>{V, S}, n3, nblk, nrhs, rs, status, st);
             vec_launch<1>(BUpdate<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+        } else if (sp.method == 6) {
+            if (par == 0) {
+                vec_launch<1>(TAlpha<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+                vec_launch<1>(TW<T, true>{V, S}, n3, nblk, nrhs, rs, status, st);
+                vec_launch<1>(TX<T, false>{V, S}, n3, nblk, nrhs, rs, status, st);
+                vec_launch<0>(TU<T, false>{V, S}, n3, nblk, nrhs, rs, status, st);
+                mv_solver<T>(G, sp, W, T_U, T_AU, status, st);
+                vec_launch<1>(TV<T, false>{V, S}, n3, nblk, nrhs, rs, status, st);
+            } else {
+                vec_launch<1>(TW<T, false>{V, S}, n3, nblk, nrhs, rs, status, st);
+                vec_launch<1>(TX<T, true>{V, S}, n3, nblk, nrhs, rs, status, st);
+                vec_launch<0>(TU<T, true>{V, S}, n3, nblk, nrhs, rs, status, st);
+                mv_solver<T>(G, sp, W, T_U, T_AU, status, st);
+                vec_launch<1>(TV<T, true>{V, S}, n3, nblk, nrhs, rs, status, st);
+            }
         } else if (sp.method == 5) {
             vec_launch<1>(CUpdate<T>{V, S}, n3, nblk, nrhs, rs, status, st);
             mv_solver<T>(G, sp, W, C_R, C_S, status, st);
@@ -298,6 +317,12 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
         vec_launch<1>(BStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
         if (!sp.zero_guess) mv_solver<T>(G, sp, W, B_X, B_XR, status, st);
         vec_launch<2>(BInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+    } else if (sp.method == 6) {
+        vec_launch<1>(TStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
+        if (!sp.zero_guess) mv_solver<T>(G, sp, W, T_X, T_XR, status, st);
+        vec_launch<0>(TInit1<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+        mv_solver<T>(G, sp, W, T_U, T_V, status, st);
+        vec_launch<1>(TInit2<T>{V, S}, n3, nblk, nrhs, rs, status, st);
     } else if (sp.method == 5) {
         vec_launch<1>(CStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
         if (!sp.zero_guess) mv_solver<T>(G, sp, W, C_X, C_XR, status, st);
@@ -439,13 +464,13 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
 }
 
 template <class T> int KrylovWork<T>::x_slot(int method) const {
-    return method == 1 ? (int)G_X : method == 4 ? (int)B_X : method == 5 ? (int)C_X : (int)Q_X;
+    return method == 1 ? (int)G_X : method == 4 ? (int)B_X : method == 5 ? (int)C_X : method == 6 ? (int)T_X : (int)Q_X;
 }
 template <class T> int KrylovWork<T>::b_slot(int method) const {
-    return method == 1 ? (int)G_B : method == 4 ? (int)B_B : method == 5 ? (int)C_B : (int)Q_B;
+    return method == 1 ? (int)G_B : method == 4 ? (int)B_B : method == 5 ? (int)C_B : method == 6 ? (int)T_B : (int)Q_B;
 }
 template <class T> int KrylovWork<T>::xr_slot(int method) const {
-    return method == 1 ? (int)G_XR : method == 4 ? (int)B_XR : method == 5 ? (int)C_XR : (int)Q_XR;
+    return method == 1 ? (int)G_XR : method == 4 ? (int)B_XR : method == 5 ? (int)C_XR : method == 6 ? (int)T_XR : (int)Q_XR;
 }
 
 // Mat-vecs and iterations the reference's driver counts for a solve that
@@ -453,11 +478,15 @@ template <class T> int KrylovWork<T>::xr_slot(int method) const {
 // the iterations it reports, cdmlib/inverserigopt.f:42-107; QMR-BiCGSTAB and
 // BiCGSTAB: two mat-vecs per iteration plus the first and the residual one,
 // :743-942; CG: one per iteration plus A x0, A p0 and the residual one,
-// :676-742).
+// :676-742; TFQMR: one per pass plus A x0, A u0 and the residual one, and
+// the driver adds one to ITNO, :603-675).
 void method_counts(int method, int itno, int& nloop, int& ncompte) {
     if (method == 1) {
         nloop = itno + 1;
         ncompte = 1 + 2 * (itno + 1) + 1;
+    } else if (method == 6) {
+        nloop = itno + 1;
+        ncompte = nloop + 2;
     } else if (method == 5) {
         nloop = itno;
         ncompte = itno + 2;
@@ -606,7 +635,7 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
             int its = 0, mvs = 0;
             method_counts(sp.method, hs[r].itno, its, mvs);
             inner_iters[r] += its;
-            inner_mv[r] += sp.method == 5 ? its + 1 : 2 * its;  // zero initial guess: no A x0
+            inner_mv[r] += sp.method == 5 || sp.method == 6 ? its + 1 : 2 * its;  // zero initial guess: no A x0
             inner_runs[r] += 1;
         }
         count_launch();

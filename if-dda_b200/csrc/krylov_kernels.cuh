@@ -717,6 +717,164 @@ template <class T> struct CBeta {
     }
 };
 
+// ----------------------------------------------------------------- TFQMR ----
+// cdmlib/tfqmr.f:1-218: passes alternate, an even pass forms alpha and the
+// next u, an odd one rho, beta and v; stop when sqrt(ITNO+1) |tau| / NORM <=
+// tol.  Past MAXIT the reference routine returns no status (its driver loops
+// for ever); here the solve ends there with the current iterate.  KState:
+// alpha, beta, rho, tau, theta, etaq = eta, conv; itno = ITNO.
+// slots: 0 u, 1 w, 2 r, 3 v, 4 d, 5 rtilde, 6 u next, 7 A u, 8 A u previous,
+//        9 x, 10 xr (mat-vec out), 11 b
+enum { T_U = 0, T_W, T_R, T_V, T_D, T_RT, T_U1, T_AU, T_AUP, T_X, T_XR, T_B, T_NSLOT };
+
+// tfqmr.f:45-53: x = x0 (or 0), NORM = ||b||
+template <class T> struct TStart {
+    Slots<T> V;
+    KState* stt;
+    int zero_guess;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 b = ld(V.v(T_B, r), i);
+        st(V.v(T_X, r), i, zero_guess ? make_double2(0, 0) : b);
+        if (zero_guess) st(V.v(T_XR, r), i, make_double2(0, 0));
+        acc[0].x += b.x * b.x + b.y * b.y;
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.norm = sqrt(a[0].x);
+        s.itno = 0;
+        s.steperr = -1;
+        s.conv = 0;
+    }
+};
+
+// label 10 (tfqmr.f:57-64): r = w = u = b - A x0
+template <class T> struct TInit1 {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2*) const {
+        const double2 rr = zsub(ld(V.v(T_B, r), i), ld(V.v(T_XR, r), i));
+        st(V.v(T_R, r), i, rr);
+        st(V.v(T_W, r), i, rr);
+        st(V.v(T_U, r), i, rr);
+    }
+    __device__ void finish(int, KState&, int&, const double2*) const {}
+};
+
+// label 20 (tfqmr.f:66-82): v = A u, d = 0, rtilde = r, rho = rtilde^H r,
+// tau = NORM, theta = eta = 0, ITNO = 0
+template <class T> struct TInit2 {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 rr = ld(V.v(T_R, r), i);
+        st(V.v(T_AU, r), i, ld(V.v(T_V, r), i));
+        st(V.v(T_D, r), i, make_double2(0, 0));
+        st(V.v(T_RT, r), i, rr);
+        acc[0] = zadd(acc[0], zconjmul(rr, rr));
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.rho = a[0];
+        s.tau = make_double2(s.norm, 0);
+        s.theta = make_double2(0, 0);
+        s.etaq = make_double2(0, 0);
+        s.itno = 0;
+        s.conv = 0;
+    }
+};
+
+// tfqmr.f:88-96 (even pass): alpha = rho / rtilde^H v
+template <class T> struct TAlpha {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        acc[0] = zadd(acc[0], zconjmul(ld(V.v(T_RT, r), i), ld(V.v(T_V, r), i)));
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const { s.alpha = zdiv(s.rho, a[0]); }
+};
+
+// tfqmr.f:97-125: (even) u next = u - alpha v; w -= alpha A u,
+// d = u + theta^2 / alpha eta d; theta, c, tau, eta; the stop test
+template <class T, bool EVEN> struct TW {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2* acc) const {
+        const double2 u = ld(V.v(T_U, r), i);
+        if (EVEN) st(V.v(T_U1, r), i, zsub(u, zmul(s.alpha, ld(V.v(T_V, r), i))));
+        const double2 wn = zsub(ld(V.v(T_W, r), i), zmul(s.alpha, ld(V.v(T_AU, r), i)));
+        const double2 f = zmul(zdiv(zmul(s.theta, s.theta), s.alpha), s.etaq);
+        st(V.v(T_W, r), i, wn);
+        st(V.v(T_D, r), i, zadd(u, zmul(f, ld(V.v(T_D, r), i))));
+        acc[0] = zadd(acc[0], zconjmul(wn, wn));
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.theta = zdiv(zsqrt(a[0]), s.tau);
+        const double2 c = zdiv(make_double2(1, 0), zsqrt(zadd(make_double2(1, 0), zmul(s.theta, s.theta))));
+        s.tau = zmul(zmul(s.tau, s.theta), c);
+        s.etaq = zmul(zmul(c, c), s.alpha);
+        if (sqrt((double)(s.itno + 1)) * hypot(s.tau.x, s.tau.y) / s.norm <= s.tol) s.conv = 1;
+    }
+};
+
+// tfqmr.f:127-149: x += eta d; converged -> stop; (odd) rho = rtilde^H w,
+// beta = rho / rho0
+template <class T, bool ODD> struct TX {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2* acc) const {
+        st(V.v(T_X, r), i, zadd(ld(V.v(T_X, r), i), zmul(s.etaq, ld(V.v(T_D, r), i))));
+        if (ODD) acc[0] = zadd(acc[0], zconjmul(ld(V.v(T_RT, r), i), ld(V.v(T_W, r), i)));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        if (s.conv) {
+            status = 1;
+            s.steperr = 0;
+            return;
+        }
+        if (ODD) {
+            const double2 rho0 = s.rho;
+            s.rho = a[0];
+            s.beta = zdiv(s.rho, rho0);
+        }
+    }
+};
+
+// tfqmr.f:150-163: (odd) u next = w + beta u, A u previous = A u; u = u next
+template <class T, bool ODD> struct TU {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2*) const {
+        if (ODD) {
+            const double2 un = zadd(ld(V.v(T_W, r), i), zmul(s.beta, ld(V.v(T_U, r), i)));
+            st(V.v(T_U, r), i, un);
+            st(V.v(T_AUP, r), i, ld(V.v(T_AU, r), i));
+        } else {
+            st(V.v(T_U, r), i, ld(V.v(T_U1, r), i));
+        }
+    }
+    __device__ void finish(int, KState&, int&, const double2*) const {}
+};
+
+// label 30 (tfqmr.f:166-177): (odd) v = A u + beta (A u previous + beta v);
+// next pass, or the end past MAXIT
+template <class T, bool ODD> struct TV {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2*) const {
+        if (ODD) {
+            const double2 v = ld(V.v(T_V, r), i);
+            st(V.v(T_V, r), i,
+               zadd(ld(V.v(T_AU, r), i), zmul(s.beta, zadd(ld(V.v(T_AUP, r), i), zmul(s.beta, v)))));
+        }
+    }
+    __device__ void finish(int, KState& s, int& status, const double2*) const {
+        if (s.itno <= s.maxit) {
+            s.itno += 1;
+        } else {
+            status = 1;
+            s.steperr = 0;
+        }
+    }
+};
+
 // ------------------------------------------------------------ shared ------
 // y = alpha . x (polarisability, cdmlib/inverserigopt.f:68-80) on FP64 vectors
 __global__ void k_apply_alpha(const double2* __restrict__ x, double2* __restrict__ y, long nd, int nrhs, long stride,

@@ -820,6 +820,127 @@ L30: {
 }
 
 /* ------------------------------------------------------------------------- */
+/* TFQMR reverse-communication state machine: cdmlib/tfqmr.f:1-218.  x is the */
+/* caller's solution array (FFloc).  Work columns: 0 u, 1 w, 2 r, 3 v, 4 d,   */
+/* 5 rtilde, 6 u(next), 7 A u, 8 A u (previous).  Passes alternate: an even   */
+/* pass forms alpha and the next u, an odd pass rho, beta and v.  Stop when   */
+/* sqrt(ITNO+1) |tau| / NORM <= tol.  Past MAXIT the reference routine falls  */
+/* off its end without a status and its driver loops for ever; the            */
+/* restatement ends there with status 1 and the current iterate.             */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    zc alpha, beta, rho, tau, theta, eta;
+    double norm;
+} tfqmr_state;
+
+static void tfqmr(zc *x, zc *xi, zc *xr, const zc *B, long n, int *nou, zc *W, int *itno, int maxit,
+                  double tol, tfqmr_state *S, int *status, int *steperr) {
+#define WK(c) (W + (size_t)(c) * n)
+    zc *u = WK(0), *w = WK(1), *r = WK(2), *v = WK(3), *d = WK(4), *rt = WK(5), *u1 = WK(6),
+       *au = WK(7), *aup = WK(8);
+#undef WK
+    if (*nou == 1) goto L10;
+    if (*nou == 2) goto L20;
+    if (*nou == 3) goto L30;
+    if (*nou == 4) goto L40;
+    *status = 0;
+    *steperr = -1;
+    {
+        double nrm = 0;
+#pragma omp parallel for reduction(+ : nrm)
+        for (long i = 0; i < n; i++) {
+            x[i] = xi[i];
+            nrm += creal(B[i] * conj(B[i]));
+        }
+        S->norm = sqrt(nrm);
+    }
+    *nou = 1;
+    return;
+L10:
+    *nou = 2;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        r[i] = B[i] - xr[i];
+        w[i] = r[i];
+        u[i] = r[i];
+        xi[i] = u[i];
+    }
+    return;
+L20:
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        v[i] = xr[i];
+        d[i] = 0;
+        au[i] = v[i];
+        rt[i] = r[i];
+    }
+    S->rho = zsum(rt, r, n, 1);
+    S->tau = S->norm;
+    S->theta = 0;
+    S->eta = 0;
+    *itno = -1;
+L100: {
+    *itno += 1;
+    if (*itno % 2 == 0) {
+        S->alpha = S->rho / zsum(rt, v, n, 1);
+        const zc al = S->alpha;
+#pragma omp parallel for
+        for (long i = 0; i < n; i++) u1[i] = u[i] - al * v[i];
+    }
+    const zc al = S->alpha, f = S->theta * S->theta / S->alpha * S->eta;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        w[i] = w[i] - al * au[i];
+        d[i] = u[i] + f * d[i];
+    }
+    S->theta = csqrt(zsum(w, w, n, 1)) / S->tau;
+    const zc c = 1.0 / csqrt(1.0 + S->theta * S->theta);
+    S->tau = S->tau * S->theta * c;
+    S->eta = c * c * S->alpha;
+    const zc et = S->eta;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) x[i] = x[i] + et * d[i];
+    if (sqrt((double)(*itno + 1)) * cabs(S->tau) / S->norm <= tol) {
+        *status = 1;
+        *nou = 4;
+        return;
+    }
+}
+L40:
+    if (*itno % 2 == 1) {
+        const zc rho0 = S->rho;
+        S->rho = zsum(rt, w, n, 1);
+        S->beta = S->rho / rho0;
+        const zc be = S->beta;
+#pragma omp parallel for
+        for (long i = 0; i < n; i++) {
+            u1[i] = w[i] + be * u[i];
+            aup[i] = au[i];
+        }
+    }
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        xi[i] = u1[i];
+        u[i] = u1[i];
+    }
+    *nou = 3;
+    return;
+L30:
+    *nou = 3;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) au[i] = xr[i];
+    if (*itno % 2 == 1) {
+        const zc be = S->beta;
+#pragma omp parallel for
+        for (long i = 0; i < n; i++) v[i] = au[i] + be * (aup[i] + be * v[i]);
+    }
+    if (*itno <= maxit) goto L100;
+    *status = 1;
+    *steperr = 0;
+    *nou = 4;
+}
+
+/* ------------------------------------------------------------------------- */
 /* Solver driver: cdmlib/inverserigopt.f:1-107 (GPBICG1), :811-942             */
 /* (QMRBICGSTAB1/2) and cdmlib/inverserig.f (tabdip != NULL).                  */
 /* Returns nstop; infostr receives the reference's messages (space padded to   */
@@ -872,8 +993,8 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
     if (strncmp(meth, "GPBICG1", 7) == 0) kind = 1;
     else if (strncmp(meth, "GPBICG2", 7) == 0 || strncmp(meth, "GPBICGsafe", 10) == 0 ||
              strncmp(meth, "GPBICGplus", 10) == 0 || strncmp(meth, "GPBICGAR", 8) == 0 ||
-             strncmp(meth, "BICGSTARPLUS", 12) == 0 || strncmp(meth, "QMRCLA", 6) == 0 ||
-             strncmp(meth, "TFQMR", 5) == 0) kind = 0;
+             strncmp(meth, "BICGSTARPLUS", 12) == 0 || strncmp(meth, "QMRCLA", 6) == 0) kind = 0;
+    else if (strncmp(meth, "TFQMR", 5) == 0) kind = 6;
     else if (strncmp(meth, "CG   ", 5) == 0) kind = 5;
     else if (strncmp(meth, "BICGSTAB", 8) == 0) kind = 4;
     else if (strncmp(meth, "QMRBICGSTAB1", 12) == 0) kind = 2;
@@ -888,6 +1009,8 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
     qmr_state qs;
     bicgstab_state bs;
     cg_state cs;
+    tfqmr_state ts;
+    memset(&ts, 0, sizeof ts);
     memset(&gs, 0, sizeof gs);
     memset(&qs, 0, sizeof qs);
     memset(&bs, 0, sizeof bs);
@@ -895,7 +1018,7 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
     double norm = 0;
     /* GPBICG and CG return the solution in xi; QMR-BiCGSTAB and BiCGSTAB in
        FFloc (the X argument), which the driver copies back to xi */
-    const int x_in_floc = kind == 2 || kind == 3 || kind == 4;
+    const int x_in_floc = kind == 2 || kind == 3 || kind == 4 || kind == 6;
     for (;;) {
         if (kind == 1)
             gpbicg(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &gs, &nstat, &steperr);
@@ -903,13 +1026,16 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
             bicgstab(FFloc, xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &bs, &nstat, &steperr);
         else if (kind == 5)
             zcg(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &cs, &nstat);
+        else if (kind == 6)
+            tfqmr(FFloc, xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &ts, &nstat, &steperr);
         else
             qmrbicgstab(FFloc, xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &qs,
                         kind == 2 ? 1 : 2, &nstat, &steperr);
-        norm = kind == 1 ? gs.norm : kind == 4 ? bs.norm : kind == 5 ? cs.norm : qs.norm;
+        norm = kind == 1 ? gs.norm : kind == 4 ? bs.norm : kind == 5 ? cs.norm : kind == 6 ? ts.norm : qs.norm;
         if (nstat < 0) {
             *nstop = 1;
-            set_info(infostr, "Problem to solve Ax=b!");
+            /* the TFQMR branch prints it without '!' (inverserigopt.f:609) */
+            set_info(infostr, kind == 6 ? "Problem to solve Ax=b" : "Problem to solve Ax=b!");
             free(xi); free(xr); free(W);
             return *nstop;
         }
@@ -938,7 +1064,7 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
         t += creal(xr[i] * conj(xr[i]));
     }
     *tol1 = sqrt(t) / norm;
-    if (kind == 1) *nloop += 1;
+    if (kind == 1 || kind == 6) *nloop += 1;
     free(xi); free(xr); free(W);
     return *nstop;
 }

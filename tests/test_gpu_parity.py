@@ -197,7 +197,7 @@ def test_planewaves_match_oracle(gctx, orc):
 def test_error_paths(gctx, orc):
     ob, k0, E0, ff0, _ = _c1_inputs(orc, nnnr=6)
     g = gctx.green(6, 6, 6, ob.aretecube, k0)
-    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, "TFQMR", 1e-4, tabdip=ob.tabdip)
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, "NOSUCHMETHOD", 1e-4, tabdip=ob.tabdip)
     assert r.nstop == 1 and r.infostr.strip() == "Iterative method not correct!"
     r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, np.zeros_like(ff0), "GPBICG1", 1e-4, tabdip=ob.tabdip)
     assert r.nstop == 1 and r.infostr.strip() == "Problem to solve Ax=b!"
@@ -296,7 +296,7 @@ def test_anisotropy_only_in_the_tail_matches_oracle(gctx, orc):
     g.close()
 
 
-@pytest.mark.parametrize("meth", ["BICGSTAB", "CG"])
+@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR"])
 def test_bicgstab_and_cg_match_oracle(gctx, orc, meth):
     """The reference's BiCGSTAB (pimzbicgstab.f) and complex-symmetric CG
     (zcg.f) on the sphere (inside-only, Tabdip) and on a full-box GRF cube:
@@ -320,7 +320,7 @@ def test_bicgstab_and_cg_match_oracle(gctx, orc, meth):
     g.close()
 
 
-@pytest.mark.parametrize("meth", ["BICGSTAB", "CG"])
+@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR"])
 def test_bicgstab_and_cg_mixed_precision(gctx, orc, meth):
     from ifdda import IFDDA_MIXED
     ob, k0, E0, ff0, G = _c1_inputs(orc)
