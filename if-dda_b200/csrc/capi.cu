@@ -111,7 +111,9 @@ int method_code(const char* m) {
     // prefixes of the blank-padded character(12) methodeit, in this order;
     // the methods not built here answer "Iterative method not correct!"
     if (!strncmp(buf, "GPBICG1", 7)) return 1;
-    if (!strncmp(buf, "GPBICG2", 7) || !strncmp(buf, "GPBICGsafe", 10) || !strncmp(buf, "GPBICGplus", 10) ||
+    if (!strncmp(buf, "GPBICG2", 7)) return 0;
+    if (!strncmp(buf, "GPBICGsafe", 10)) return 7;
+    if (!strncmp(buf, "GPBICGplus", 10) ||
         !strncmp(buf, "GPBICGAR", 8) || !strncmp(buf, "BICGSTARPLUS", 12) || !strncmp(buf, "QMRCLA", 6))
         return 0;
     if (!strncmp(buf, "TFQMR", 5)) return 6;

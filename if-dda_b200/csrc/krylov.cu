@@ -137,6 +137,7 @@ template <class T> void KrylovWork<T>::ensure(int method, int nrhs_, long n3_) {
             : method == 4 ? (int)B_NSLOT
             : method == 5 ? (int)C_NSLOT
             : method == 6 ? (int)T_NSLOT
+            : method == 7 ? (int)S_NSLOT
                           : (int)Q_NSLOT;
     nrhs = nrhs_;
     n3 = n3_;
@@ -145,7 +146,7 @@ template <class T> void KrylovWork<T>::ensure(int method, int nrhs_, long n3_) {
     st.ensure(nrhs);
     status.ensure(nrhs);
     zstatus.ensure(nrhs);
-    partials.ensure((size_t)nrhs * nblk * 4);
+    partials.ensure((size_t)nrhs * nblk * 8);  // up to 8 sums per reduction
     tickets.ensure(nrhs);
     hstatus.resize(nrhs);
 }
@@ -278,6 +279,13 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
             mv_solver<T>(G, sp, W, B_S, B_T, status, st);
             vec_launch<2>(BOmega<T>{V, S}, n3, nblk, nrhs, rs, status, st);
             vec_launch<1>(BUpdate<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+        } else if (sp.method == 7) {
+            vec_launch<0>(SfP<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            mv_solver<T>(G, sp, W, S_R, S_AR, status, st);
+            vec_launch<6>(SfAlpha<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<0>(SfU<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            mv_solver<T>(G, sp, W, S_U, S_AU, status, st);
+            vec_launch<2>(SfUpdate<T>{V, S}, n3, nblk, nrhs, rs, status, st);
         } else if (sp.method == 6) {
             if (par == 0) {
                 vec_launch<1>(TAlpha<T>{V, S}, n3, nblk, nrhs, rs, status, st);
@@ -317,6 +325,10 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
         vec_launch<1>(BStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
         if (!sp.zero_guess) mv_solver<T>(G, sp, W, B_X, B_XR, status, st);
         vec_launch<2>(BInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+    } else if (sp.method == 7) {
+        vec_launch<1>(SfStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
+        if (!sp.zero_guess) mv_solver<T>(G, sp, W, S_X, S_XR, status, st);
+        vec_launch<1>(SfInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
     } else if (sp.method == 6) {
         vec_launch<1>(TStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
         if (!sp.zero_guess) mv_solver<T>(G, sp, W, T_X, T_XR, status, st);
@@ -464,13 +476,13 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
 }
 
 template <class T> int KrylovWork<T>::x_slot(int method) const {
-    return method == 1 ? (int)G_X : method == 4 ? (int)B_X : method == 5 ? (int)C_X : method == 6 ? (int)T_X : (int)Q_X;
+    return method == 1 ? (int)G_X : method == 4 ? (int)B_X : method == 5 ? (int)C_X : method == 6 ? (int)T_X : method == 7 ? (int)S_X : (int)Q_X;
 }
 template <class T> int KrylovWork<T>::b_slot(int method) const {
-    return method == 1 ? (int)G_B : method == 4 ? (int)B_B : method == 5 ? (int)C_B : method == 6 ? (int)T_B : (int)Q_B;
+    return method == 1 ? (int)G_B : method == 4 ? (int)B_B : method == 5 ? (int)C_B : method == 6 ? (int)T_B : method == 7 ? (int)S_B : (int)Q_B;
 }
 template <class T> int KrylovWork<T>::xr_slot(int method) const {
-    return method == 1 ? (int)G_XR : method == 4 ? (int)B_XR : method == 5 ? (int)C_XR : method == 6 ? (int)T_XR : (int)Q_XR;
+    return method == 1 ? (int)G_XR : method == 4 ? (int)B_XR : method == 5 ? (int)C_XR : method == 6 ? (int)T_XR : method == 7 ? (int)S_XR : (int)Q_XR;
 }
 
 // Mat-vecs and iterations the reference's driver counts for a solve that
@@ -481,7 +493,7 @@ template <class T> int KrylovWork<T>::xr_slot(int method) const {
 // :676-742; TFQMR: one per pass plus A x0, A u0 and the residual one, and
 // the driver adds one to ITNO, :603-675).
 void method_counts(int method, int itno, int& nloop, int& ncompte) {
-    if (method == 1) {
+    if (method == 1 || method == 7) {  // GPBICG1, GPBICGsafe (:174-237)
         nloop = itno + 1;
         ncompte = 1 + 2 * (itno + 1) + 1;
     } else if (method == 6) {

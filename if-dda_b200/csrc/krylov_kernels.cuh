@@ -717,6 +717,166 @@ template <class T> struct CBeta {
     }
 };
 
+// ------------------------------------------------------------ GPBiCGsafe ----
+// cdmlib/gpbicgsafe.f: the mat-vecs are A r and A u; A p is carried by
+// Ap = Ar + beta (Ap - Au); zeta and eta come from five dot products.  Ends
+// like GPBICG (status 1 with the iterate past MAXIT).  KState: alpha, beta,
+// eta, dzeta, r0rn; itno = ITNO.
+// slots: 0 r0 (shadow), 1 p, 2 u, 3 r, 4 A u, 5 A r, 6 A p, 7 z, 8 y, 9 x,
+//        10 xr (mat-vec out), 11 b
+enum { S_R0 = 0, S_P, S_U, S_R, S_AU, S_AR, S_AP, S_Z, S_Y, S_X, S_XR, S_B, S_NSLOT };
+
+template <class T> struct SfStart {
+    Slots<T> V;
+    KState* stt;
+    int zero_guess;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 b = ld(V.v(S_B, r), i);
+        st(V.v(S_X, r), i, zero_guess ? make_double2(0, 0) : b);
+        if (zero_guess) st(V.v(S_XR, r), i, make_double2(0, 0));
+        acc[0].x += b.x * b.x + b.y * b.y;
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.norm = sqrt(a[0].x);
+        s.itno = 0;
+        s.steperr = -1;
+    }
+};
+
+// label 10: r0 = r = b - A x0, p = u = z = Ap = Au = y = 0, R0RN = r0^H r0
+template <class T> struct SfInit {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 rr = zsub(ld(V.v(S_B, r), i), ld(V.v(S_XR, r), i));
+        const double2 z = make_double2(0, 0);
+        st(V.v(S_R0, r), i, rr);
+        st(V.v(S_R, r), i, rr);
+        st(V.v(S_P, r), i, z);
+        st(V.v(S_U, r), i, z);
+        st(V.v(S_Z, r), i, z);
+        st(V.v(S_AP, r), i, z);
+        st(V.v(S_AU, r), i, z);
+        st(V.v(S_Y, r), i, z);
+        acc[0] = zadd(acc[0], zconjmul(rr, rr));
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.r0rn = a[0];
+        s.beta = make_double2(0, 0);
+        s.itno = 0;
+    }
+};
+
+// label 100: p = r + beta (p - u); then A r
+template <class T> struct SfP {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2*) const {
+        const double2 p = ld(V.v(S_P, r), i), u = ld(V.v(S_U, r), i);
+        st(V.v(S_P, r), i, zadd(ld(V.v(S_R, r), i), zmul(s.beta, zsub(p, u))));
+    }
+    __device__ void finish(int, KState&, int&, const double2*) const {}
+};
+
+// label 20: Ap = Ar + beta (Ap - Au), alpha = R0RN / r0^H Ap, zeta and eta
+// (first iteration: zeta = Ar^H r / Ar^H Ar, eta = 0)
+template <class T> struct SfAlpha {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2* acc) const {
+        const double2 ar = ld(V.v(S_AR, r), i), y = ld(V.v(S_Y, r), i), rr = ld(V.v(S_R, r), i);
+        const double2 ap = zadd(ar, zmul(s.beta, zsub(ld(V.v(S_AP, r), i), ld(V.v(S_AU, r), i))));
+        st(V.v(S_AP, r), i, ap);
+        acc[0] = zadd(acc[0], zconjmul(ld(V.v(S_R0, r), i), ap));
+        acc[1] = zadd(acc[1], zconjmul(y, y));
+        acc[2] = zadd(acc[2], zconjmul(ar, rr));
+        acc[3] = zadd(acc[3], zconjmul(y, rr));
+        acc[4] = zadd(acc[4], zconjmul(ar, y));
+        acc[5] = zadd(acc[5], zconjmul(ar, ar));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        if (zisnull(a[0])) {
+            status = -1;
+            s.steperr = 1;
+            return;
+        }
+        s.alpha = zdiv(s.r0rn, a[0]);
+        const double2 c1 = a[1], c2 = a[2], c3 = a[3], c4 = a[4], c5 = a[5];
+        if (s.itno == 0) {
+            s.eta = make_double2(0, 0);
+            if (zisnull(c5)) {
+                status = -1;
+                s.steperr = 2;
+                return;
+            }
+            s.dzeta = zdiv(c2, c5);
+        } else {
+            const double2 c = zsub(zmul(c5, c1), zmul(c4, zconj(c4)));
+            if (zisnull(c)) {
+                status = -1;
+                s.steperr = 3;
+                return;
+            }
+            s.dzeta = zdiv(zsub(zmul(c1, c2), zmul(c3, c4)), c);
+            s.eta = zdiv(zsub(zmul(c5, c3), zmul(zconj(c4), c2)), c);
+        }
+    }
+};
+
+// u = zeta Ap + eta (y + beta u); then A u
+template <class T> struct SfU {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2*) const {
+        const double2 u = ld(V.v(S_U, r), i);
+        st(V.v(S_U, r), i,
+           zadd(zmul(s.dzeta, ld(V.v(S_AP, r), i)), zmul(s.eta, zadd(ld(V.v(S_Y, r), i), zmul(s.beta, u)))));
+    }
+    __device__ void finish(int, KState&, int&, const double2*) const {}
+};
+
+// label 30 and 40: t = r - alpha Ap, z, y, x += alpha p + z, r = t - y, the
+// stop test on ||r|| / NORM, beta = alpha r0^H r / zeta / R0RN
+template <class T> struct SfUpdate {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2* acc) const {
+        const double2 rr = ld(V.v(S_R, r), i);
+        const double2 t = zsub(rr, zmul(s.alpha, ld(V.v(S_AP, r), i)));
+        const double2 z = zsub(zadd(zmul(s.dzeta, rr), zmul(s.eta, ld(V.v(S_Z, r), i))), zmul(s.alpha, ld(V.v(S_U, r), i)));
+        const double2 y = zsub(zadd(zmul(s.dzeta, ld(V.v(S_AR, r), i)), zmul(s.eta, ld(V.v(S_Y, r), i))),
+                               zmul(s.alpha, ld(V.v(S_AU, r), i)));
+        st(V.v(S_Z, r), i, z);
+        st(V.v(S_Y, r), i, y);
+        st(V.v(S_X, r), i, zadd(zadd(ld(V.v(S_X, r), i), zmul(s.alpha, ld(V.v(S_P, r), i))), z));
+        const double2 rn = zsub(t, y);
+        st(V.v(S_R, r), i, rn);
+        acc[0].x += rn.x * rn.x + rn.y * rn.y;
+        acc[1] = zadd(acc[1], zconjmul(ld(V.v(S_R0, r), i), rn));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        s.residu = sqrt(a[0].x) / s.norm;
+        if (s.residu <= s.tol) {
+            status = 1;
+            s.steperr = 0;
+            return;
+        }
+        if (zisnull(s.r0rn)) {
+            status = -1;
+            s.steperr = 4;
+            return;
+        }
+        s.beta = zdiv(zdiv(zmul(s.alpha, a[1]), s.dzeta), s.r0rn);
+        s.r0rn = a[1];
+        if (s.itno <= s.maxit) {
+            s.itno += 1;
+        } else {
+            status = 1;
+            s.steperr = 0;
+        }
+    }
+};
+
 // ----------------------------------------------------------------- TFQMR ----
 // cdmlib/tfqmr.f:1-218: passes alternate, an even pass forms alpha and the
 // next u, an odd one rho, beta and v; stop when sqrt(ITNO+1) |tau| / NORM <=

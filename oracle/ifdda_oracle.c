@@ -941,6 +941,146 @@ L30:
 }
 
 /* ------------------------------------------------------------------------- */
+/* GPBiCGsafe reverse-communication state machine: cdmlib/gpbicgsafe.f.       */
+/* The mat-vecs are A r and A u; A p is carried by Ap = Ar + beta (Ap - Au).  */
+/* Work columns: 0 r0 (shadow), 1 p, 2 u, 3 r, 4 A u, 5 A r, 6 A p, 7 t,     */
+/* 8 z, 9 y, 10 x.  Ends like GPBICG: status 1 past MAXIT with the iterate.   */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    zc alpha, beta, eta, dzeta, r0rn;
+    double norm;
+} gpsafe_state;
+
+static void gpbicgsafe(zc *xi, zc *xr, const zc *B, long n, int *nou, zc *W, int *itno, int maxit,
+                       double tol, gpsafe_state *S, int *status, int *steperr) {
+#define WK(c) (W + (size_t)(c) * n)
+    zc *r0 = WK(0), *p = WK(1), *u = WK(2), *r = WK(3), *au = WK(4), *ar = WK(5), *ap = WK(6), *t = WK(7),
+       *z = WK(8), *y = WK(9), *x = WK(10);
+#undef WK
+    if (*nou == 1) goto L10;
+    if (*nou == 2) goto L20;
+    if (*nou == 3) goto L30;
+    if (*nou == 4) goto L40;
+    *status = 0;
+    *steperr = -1;
+    {
+        double nrm = 0;
+#pragma omp parallel for reduction(+ : nrm)
+        for (long i = 0; i < n; i++) {
+            x[i] = xi[i];
+            nrm += creal(B[i] * conj(B[i]));
+        }
+        S->norm = sqrt(nrm);
+    }
+    *nou = 1;
+    return;
+L10:
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        r0[i] = B[i] - xr[i];
+        p[i] = 0;
+        u[i] = 0;
+        z[i] = 0;
+        ap[i] = 0;
+        au[i] = 0;
+        y[i] = 0;
+        r[i] = r0[i];
+    }
+    S->r0rn = zsum(r0, r0, n, 1);
+    S->beta = 0;
+    *itno = -1;
+L100: {
+    *itno += 1;
+    const zc be = S->beta;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        p[i] = r[i] + be * (p[i] - u[i]);
+        xi[i] = r[i];
+    }
+    *nou = 2;
+    return;
+}
+L20: {
+    const zc be = S->beta;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        ar[i] = xr[i];
+        ap[i] = ar[i] + be * (ap[i] - au[i]);
+    }
+    const zc c0 = zsum(r0, ap, n, 1);
+    if (c0 == 0) {
+        *status = -1;
+        *steperr = 1;
+        return;
+    }
+    S->alpha = S->r0rn / c0;
+    if (*itno == 0) {
+        S->eta = 0;
+        const zc num = zsum(ar, r, n, 1), den = zsum(ar, ar, n, 1);
+        if (den == 0) {
+            *status = -1;
+            *steperr = 2;
+            return;
+        }
+        S->dzeta = num / den;
+    } else {
+        const zc c1 = zsum(y, y, n, 1), c2 = zsum(ar, r, n, 1), c3 = zsum(y, r, n, 1),
+                 c4 = zsum(ar, y, n, 1), c5 = zsum(ar, ar, n, 1);
+        const zc c = c5 * c1 - c4 * conj(c4);
+        if (c == 0) {
+            *status = -1;
+            *steperr = 3;
+            return;
+        }
+        S->dzeta = (c1 * c2 - c3 * c4) / c;
+        S->eta = (c5 * c3 - conj(c4) * c2) / c;
+    }
+    const zc dz = S->dzeta, et = S->eta;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        u[i] = dz * ap[i] + et * (y[i] + be * u[i]);
+        xi[i] = u[i];
+    }
+    *nou = 3;
+    return;
+}
+L30: {
+    const zc al = S->alpha, dz = S->dzeta, et = S->eta;
+    double res = 0;
+#pragma omp parallel for reduction(+ : res)
+    for (long i = 0; i < n; i++) {
+        au[i] = xr[i];
+        t[i] = r[i] - al * ap[i];
+        z[i] = dz * r[i] + et * z[i] - al * u[i];
+        y[i] = dz * ar[i] + et * y[i] - al * au[i];
+        x[i] = x[i] + al * p[i] + z[i];
+        r[i] = t[i] - y[i];
+        res += creal(r[i] * conj(r[i]));
+    }
+    if (sqrt(res) / S->norm <= tol) {
+        *status = 1;
+        for (long i = 0; i < n; i++) xi[i] = x[i];
+        *nou = 4;
+        return;
+    }
+}
+L40: {
+    const zc c = zsum(r0, r, n, 1);
+    if (S->r0rn == 0) {
+        *status = -1;
+        *steperr = 4;
+        return;
+    }
+    S->beta = S->alpha * c / S->dzeta / S->r0rn;
+    S->r0rn = c;
+    if (*itno <= maxit) goto L100;
+    *status = 1;
+    for (long i = 0; i < n; i++) xi[i] = x[i];
+    *nou = 4;
+}
+}
+
+/* ------------------------------------------------------------------------- */
 /* Solver driver: cdmlib/inverserigopt.f:1-107 (GPBICG1), :811-942             */
 /* (QMRBICGSTAB1/2) and cdmlib/inverserig.f (tabdip != NULL).                  */
 /* Returns nstop; infostr receives the reference's messages (space padded to   */
@@ -991,8 +1131,9 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
        of the blank-padded character(12) methodeit, in this order */
     int kind = 0;
     if (strncmp(meth, "GPBICG1", 7) == 0) kind = 1;
-    else if (strncmp(meth, "GPBICG2", 7) == 0 || strncmp(meth, "GPBICGsafe", 10) == 0 ||
-             strncmp(meth, "GPBICGplus", 10) == 0 || strncmp(meth, "GPBICGAR", 8) == 0 ||
+    else if (strncmp(meth, "GPBICG2", 7) == 0) kind = 0;
+    else if (strncmp(meth, "GPBICGsafe", 10) == 0) kind = 7;
+    else if (strncmp(meth, "GPBICGplus", 10) == 0 || strncmp(meth, "GPBICGAR", 8) == 0 ||
              strncmp(meth, "BICGSTARPLUS", 12) == 0 || strncmp(meth, "QMRCLA", 6) == 0) kind = 0;
     else if (strncmp(meth, "TFQMR", 5) == 0) kind = 6;
     else if (strncmp(meth, "CG   ", 5) == 0) kind = 5;
@@ -1010,7 +1151,9 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
     bicgstab_state bs;
     cg_state cs;
     tfqmr_state ts;
+    gpsafe_state ss;
     memset(&ts, 0, sizeof ts);
+    memset(&ss, 0, sizeof ss);
     memset(&gs, 0, sizeof gs);
     memset(&qs, 0, sizeof qs);
     memset(&bs, 0, sizeof bs);
@@ -1028,10 +1171,13 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
             zcg(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &cs, &nstat);
         else if (kind == 6)
             tfqmr(FFloc, xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &ts, &nstat, &steperr);
+        else if (kind == 7)
+            gpbicgsafe(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &ss, &nstat, &steperr);
         else
             qmrbicgstab(FFloc, xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &qs,
                         kind == 2 ? 1 : 2, &nstat, &steperr);
-        norm = kind == 1 ? gs.norm : kind == 4 ? bs.norm : kind == 5 ? cs.norm : kind == 6 ? ts.norm : qs.norm;
+        norm = kind == 1 ? gs.norm : kind == 4 ? bs.norm : kind == 5 ? cs.norm : kind == 6 ? ts.norm
+             : kind == 7 ? ss.norm : qs.norm;
         if (nstat < 0) {
             *nstop = 1;
             /* the TFQMR branch prints it without '!' (inverserigopt.f:609) */
@@ -1064,7 +1210,7 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
         t += creal(xr[i] * conj(xr[i]));
     }
     *tol1 = sqrt(t) / norm;
-    if (kind == 1 || kind == 6) *nloop += 1;
+    if (kind == 1 || kind == 6 || kind == 7) *nloop += 1;
     free(xi); free(xr); free(W);
     return *nstop;
 }

@@ -296,7 +296,7 @@ def test_anisotropy_only_in_the_tail_matches_oracle(gctx, orc):
     g.close()
 
 
-@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR"])
+@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR", "GPBICGsafe"])
 def test_bicgstab_and_cg_match_oracle(gctx, orc, meth):
     """The reference's BiCGSTAB (pimzbicgstab.f) and complex-symmetric CG
     (zcg.f) on the sphere (inside-only, Tabdip) and on a full-box GRF cube:
@@ -320,7 +320,7 @@ def test_bicgstab_and_cg_match_oracle(gctx, orc, meth):
     g.close()
 
 
-@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR"])
+@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR", "GPBICGsafe"])
 def test_bicgstab_and_cg_mixed_precision(gctx, orc, meth):
     from ifdda import IFDDA_MIXED
     ob, k0, E0, ff0, G = _c1_inputs(orc)

@@ -121,7 +121,7 @@ def test_qmr_agrees_with_gpbicg(orc, meth):
     assert rel(b["FFloc"], a["FFloc"]) < 1e-8
 
 
-@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR"])
+@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR", "GPBICGsafe"])
 def test_bicgstab_and_cg_agree_with_gpbicg(orc, meth):
     """BiCGSTAB (pimzbicgstab.f) and complex-symmetric CG (zcg.f) restated:
     on the homogeneous sphere (A complex symmetric) both reach the GPBICG
@@ -137,6 +137,9 @@ def test_bicgstab_and_cg_agree_with_gpbicg(orc, meth):
     if meth in ("CG", "TFQMR"):
         assert b["ncompte"] == b["nloop"] + 2 and b["tol1"] < 1e-9
         assert rel(b["FFloc"], a["FFloc"]) < 1e-8
+    elif meth == "GPBICGsafe":
+        assert b["ncompte"] == 2 * b["nloop"] + 2 and b["tol1"] < 1e-10
+        assert rel(b["FFloc"], a["FFloc"]) < 1e-8
     else:
         assert b["ncompte"] == 2 * b["nloop"] + 2
         assert rel(b["FFloc"], a["FFloc"]) < 1e-4  # stops at ||r||^2/||r0||^2 <= tol/10
@@ -145,7 +148,8 @@ def test_bicgstab_and_cg_agree_with_gpbicg(orc, meth):
 
 
 @pytest.mark.parametrize("name,works", [("CG", True), ("CGX", False), ("BICGSTAB", True), ("GPBICGAR2", False),
-                                        ("TFQMR", True), ("BICGSTARPLUS", False), ("QMRCLA", False)])
+                                        ("TFQMR", True), ("BICGSTARPLUS", False), ("QMRCLA", False),
+                                        ("GPBICGsafe", True), ("GPBICG2", False)])
 def test_method_prefixes(orc, name, works):
     """methodeit is matched by prefix in the reference's order: 'GPBICGAR2'
     meets the 'GPBICGAR' test first, 'CGX' is not 'CG' (blank padded)."""
