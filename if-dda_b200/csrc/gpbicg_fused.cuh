@@ -109,6 +109,7 @@ template <class T> struct EpiGpZeta {
     KState* S;
     int* status;
     int tnew;
+    int every2;  // GPBICG2 (see GpZeta)
     const cplx<T>*y, *t;
     double2 acc[3];
     template <class U> __device__ __forceinline__ void bind(const MvArgs<U>&, int rhs) {
@@ -126,7 +127,7 @@ template <class T> struct EpiGpZeta {
         KState& s = S[rhs];
         s.c2 = tot[3];
         s.c5 = tot[4];
-        GpZeta<T>{V, S, tnew}.finish(rhs, s, status[rhs], tot);
+        GpZeta<T>{V, S, tnew, every2}.finish(rhs, s, status[rhs], tot);
     }
 };
 

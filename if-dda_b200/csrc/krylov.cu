@@ -133,12 +133,8 @@ template void cast_dev<double>(const double2*, double2*, long, cudaStream_t);
 int reduction_blocks(long n3) { return (int)std::max<long>(1, std::min<long>((n3 + KNT * 4 - 1) / (KNT * 4), 1024)); }
 
 template <class T> void KrylovWork<T>::ensure(int method, int nrhs_, long n3_) {
-    nslot = method == 1   ? (int)G_NSLOT
-            : method == 4 ? (int)B_NSLOT
-            : method == 5 ? (int)C_NSLOT
-            : method == 6 ? (int)T_NSLOT
-            : method == 7 ? (int)S_NSLOT
-                          : (int)Q_NSLOT;
+    static const int nslots[] = {0, G_NSLOT, Q_NSLOT, 0, B_NSLOT, C_NSLOT, T_NSLOT, S_NSLOT, A_NSLOT};
+    nslot = nslots[method_family(method)];
     nrhs = nrhs_;
     n3 = n3_;
     nblk = reduction_blocks(n3);
@@ -238,7 +234,10 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
     bool cancelled = false;
     // GPBiCG with its vector steps folded into the mat-vecs (one element per
     // x-pass visit needs an isotropic or absent polarisability)
-    const bool fused = sp.method == 1 && sp.fuse && sp.amode != ALPHA_FULL;
+    // GPBICG2 (method 8) is GPBiCG with the zeta-only step on every even iteration
+    const bool gp = sp.method == 1 || sp.method == 8;
+    const int every2 = sp.method == 8 ? 1 : 0;
+    const bool fused = gp && sp.fuse && sp.amode != ALPHA_FULL;
     MvRed red{};
     if (fused) {
         red = W.mv_red(G.g.ny, G.g.nz);
@@ -258,18 +257,18 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
             const MvArgs<T> a2 = mv_args<T>(G, nrhs, V.v(tnew, 0), V.v(tnew, 0), V.v(G_AT, 0), n3, sp.amode, alpha,
                                             sp.nmax, sp.tabdip, status);
             if (!matvec_launch_fused<T>(a1, PreGpP<T>{V, S}, EpiGpAlpha<T>{V, S, status}, red, nrhs, tab, st) ||
-                !matvec_launch_fused<T>(a2, PreGpYT<T>{V, S, tcur, tnew}, EpiGpZeta<T>{V, S, status, tnew}, red, nrhs,
+                !matvec_launch_fused<T>(a2, PreGpYT<T>{V, S, tcur, tnew}, EpiGpZeta<T>{V, S, status, tnew, every2}, red, nrhs,
                                         tab, st))
                 throw EngineError{1, "FFT size not supported by the compiled kernels"};
             vec_launch<2>(GpUpdate<T>{V, S, tcur, tnew}, n3, nblk, nrhs, rs, status, st);
-        } else if (sp.method == 1) {
+        } else if (gp) {
             const int tcur = par ? G_TB : G_TA, tnew = par ? G_TA : G_TB;
             vec_launch<0>(GpP<T>{V, S}, n3, nblk, nrhs, rs, status, st);
             mv_solver<T>(G, sp, W, G_P, G_AP, status, st);
             vec_launch<1>(GpAlpha<T>{V, S}, n3, nblk, nrhs, rs, status, st);
             vec_launch<2>(GpYT<T>{V, S, tcur, tnew}, n3, nblk, nrhs, rs, status, st);
             mv_solver<T>(G, sp, W, tnew, G_AT, status, st);
-            vec_launch<3>(GpZeta<T>{V, S, tnew}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<3>(GpZeta<T>{V, S, tnew, every2}, n3, nblk, nrhs, rs, status, st);
             vec_launch<2>(GpUpdate<T>{V, S, tcur, tnew}, n3, nblk, nrhs, rs, status, st);
         } else if (sp.method == 4) {
             vec_launch<0>(BP<T>{V, S}, n3, nblk, nrhs, rs, status, st);
@@ -279,10 +278,17 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
             mv_solver<T>(G, sp, W, B_S, B_T, status, st);
             vec_launch<2>(BOmega<T>{V, S}, n3, nblk, nrhs, rs, status, st);
             vec_launch<1>(BUpdate<T>{V, S}, n3, nblk, nrhs, rs, status, st);
-        } else if (sp.method == 7) {
+        } else if (sp.method == 10) {
+            vec_launch<6>(ArAlpha<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<0>(ArU<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            mv_solver<T>(G, sp, W, A_U, A_AU, status, st);
+            vec_launch<1>(ArUpdate<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            mv_solver<T>(G, sp, W, A_R, A_AR, status, st);
+            vec_launch<1>(ArBeta<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+        } else if (sp.method == 7 || sp.method == 9) {
             vec_launch<0>(SfP<T>{V, S}, n3, nblk, nrhs, rs, status, st);
             mv_solver<T>(G, sp, W, S_R, S_AR, status, st);
-            vec_launch<6>(SfAlpha<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<6>(SfAlpha<T>{V, S, sp.method == 9 ? 1 : 0}, n3, nblk, nrhs, rs, status, st);
             vec_launch<0>(SfU<T>{V, S}, n3, nblk, nrhs, rs, status, st);
             mv_solver<T>(G, sp, W, S_U, S_AU, status, st);
             vec_launch<2>(SfUpdate<T>{V, S}, n3, nblk, nrhs, rs, status, st);
@@ -317,7 +323,7 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
         }
         IFDDA_CUDA(cudaGetLastError());
     };
-    if (sp.method == 1) {
+    if (gp) {
         vec_launch<1>(GpStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
         if (!sp.zero_guess) mv_solver<T>(G, sp, W, G_X, G_XR, status, st);
         vec_launch<1>(GpInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
@@ -325,7 +331,12 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
         vec_launch<1>(BStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
         if (!sp.zero_guess) mv_solver<T>(G, sp, W, B_X, B_XR, status, st);
         vec_launch<2>(BInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
-    } else if (sp.method == 7) {
+    } else if (sp.method == 10) {
+        vec_launch<1>(ArStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
+        if (!sp.zero_guess) mv_solver<T>(G, sp, W, A_X, A_XR, status, st);
+        vec_launch<1>(ArInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+        mv_solver<T>(G, sp, W, A_R, A_AR, status, st);
+    } else if (sp.method == 7 || sp.method == 9) {
         vec_launch<1>(SfStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
         if (!sp.zero_guess) mv_solver<T>(G, sp, W, S_X, S_XR, status, st);
         vec_launch<1>(SfInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
@@ -475,14 +486,34 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
     return !cancelled;
 }
 
+// Method codes (capi.cu method_code) -> the state machine and slot layout
+// they run on: GPBICG2 runs on GPBiCG's (1), GPBICGplus on GPBiCGsafe's (7),
+// QMRBICGSTAB2 on QMRBICGSTAB1's (2), GPBICGAR has its own (8).
+int method_family(int method) {
+    switch (method) {
+    case 1:
+    case 8: return 1;
+    case 4: return 4;
+    case 5: return 5;
+    case 6: return 6;
+    case 7:
+    case 9: return 7;
+    case 10: return 8;
+    default: return 2;
+    }
+}
+
 template <class T> int KrylovWork<T>::x_slot(int method) const {
-    return method == 1 ? (int)G_X : method == 4 ? (int)B_X : method == 5 ? (int)C_X : method == 6 ? (int)T_X : method == 7 ? (int)S_X : (int)Q_X;
+    static const int s[] = {0, G_X, Q_X, 0, B_X, C_X, T_X, S_X, A_X};
+    return s[method_family(method)];
 }
 template <class T> int KrylovWork<T>::b_slot(int method) const {
-    return method == 1 ? (int)G_B : method == 4 ? (int)B_B : method == 5 ? (int)C_B : method == 6 ? (int)T_B : method == 7 ? (int)S_B : (int)Q_B;
+    static const int s[] = {0, G_B, Q_B, 0, B_B, C_B, T_B, S_B, A_B};
+    return s[method_family(method)];
 }
 template <class T> int KrylovWork<T>::xr_slot(int method) const {
-    return method == 1 ? (int)G_XR : method == 4 ? (int)B_XR : method == 5 ? (int)C_XR : method == 6 ? (int)T_XR : method == 7 ? (int)S_XR : (int)Q_XR;
+    static const int s[] = {0, G_XR, Q_XR, 0, B_XR, C_XR, T_XR, S_XR, A_XR};
+    return s[method_family(method)];
 }
 
 // Mat-vecs and iterations the reference's driver counts for a solve that
@@ -493,7 +524,9 @@ template <class T> int KrylovWork<T>::xr_slot(int method) const {
 // :676-742; TFQMR: one per pass plus A x0, A u0 and the residual one, and
 // the driver adds one to ITNO, :603-675).
 void method_counts(int method, int itno, int& nloop, int& ncompte) {
-    if (method == 1 || method == 7) {  // GPBICG1, GPBICGsafe (:174-237)
+    if (method == 1 || method >= 7) {
+        // GPBICG1, GPBICGsafe (:174-237), GPBICG2 (:109-173), GPBICGplus
+        // (:238-301), GPBICGAR (:302-366)
         nloop = itno + 1;
         ncompte = 1 + 2 * (itno + 1) + 1;
     } else if (method == 6) {

@@ -172,11 +172,14 @@ template <class T> struct GpYT {
     }
 };
 
-// label 30 coefficients (gpbicg.f:212-264)
+// label 30 coefficients (gpbicg.f:212-264).  every2: GPBICG2
+// (cdmlib/gpbicg2.f), which takes the zeta-only step on every even ITNO, not
+// only the first (its label 30 tests mod(ITNO,2) = 0).
 template <class T> struct GpZeta {
     Slots<T> V;
     KState* stt;
     int tnew;
+    int every2;
     __device__ void elem(const KState&, int r, long i, double2* acc) const {
         const double2 at = ld(V.v(G_AT, r), i), y = ld(V.v(G_Y, r), i), t = ld(V.v(tnew, r), i);
         acc[0] = zadd(acc[0], zconjmul(at, at));
@@ -185,7 +188,7 @@ template <class T> struct GpZeta {
     }
     __device__ void finish(int, KState& s, int& status, const double2* a) const {
         const double2 c1 = a[0], c3 = a[1], c4 = a[2], c2 = s.c2, c5 = s.c5;
-        if (s.itno == 0) {
+        if (every2 ? s.itno % 2 == 0 : s.itno == 0) {
             s.eta = make_double2(0, 0);
             if (zisnull(c1)) {
                 status = -1;
@@ -779,10 +782,13 @@ template <class T> struct SfP {
 };
 
 // label 20: Ap = Ar + beta (Ap - Au), alpha = R0RN / r0^H Ap, zeta and eta
-// (first iteration: zeta = Ar^H r / Ar^H Ar, eta = 0)
+// (first iteration: zeta = Ar^H r / Ar^H Ar, eta = 0).  plus: GPBICGplus
+// (cdmlib/gpbicgplus.f), the same iteration with zeta and eta written from
+// the same five dot products in its own form.
 template <class T> struct SfAlpha {
     Slots<T> V;
     KState* stt;
+    int plus;
     __device__ void elem(const KState& s, int r, long i, double2* acc) const {
         const double2 ar = ld(V.v(S_AR, r), i), y = ld(V.v(S_Y, r), i), rr = ld(V.v(S_R, r), i);
         const double2 ap = zadd(ar, zmul(s.beta, zsub(ld(V.v(S_AP, r), i), ld(V.v(S_AU, r), i))));
@@ -810,6 +816,17 @@ template <class T> struct SfAlpha {
                 return;
             }
             s.dzeta = zdiv(c2, c5);
+        } else if (plus) {
+            // gpbicgplus.f names: y^H y, Ar^H Ar, Ar^H r, y^H r, y^H Ar
+            const double2 p1 = c1, p2 = c5, p3 = c2, p4 = c3, p5 = zconj(c4);
+            const double2 c = zsub(zmul(p1, p2), zmul(p5, zconj(p5)));
+            if (zisnull(c)) {
+                status = -1;
+                s.steperr = 3;
+                return;
+            }
+            s.dzeta = zdiv(zsub(zmul(p1, p3), zmul(p4, zconj(p5))), c);
+            s.eta = zdiv(zsub(zmul(p2, p4), zmul(p5, p3)), c);
         } else {
             const double2 c = zsub(zmul(c5, c1), zmul(c4, zconj(c4)));
             if (zisnull(c)) {
@@ -868,6 +885,146 @@ template <class T> struct SfUpdate {
         }
         s.beta = zdiv(zdiv(zmul(s.alpha, a[1]), s.dzeta), s.r0rn);
         s.r0rn = a[1];
+        if (s.itno <= s.maxit) {
+            s.itno += 1;
+        } else {
+            status = 1;
+            s.steperr = 0;
+        }
+    }
+};
+
+// -------------------------------------------------------------- GPBiCG-AR ----
+// cdmlib/gpbicgar.f (associate residual): mat-vecs A u then A r, A p carried
+// by Ap = Ar + beta (Ap - Au), zeta and eta from the same five dot products as
+// GPBiCGsafe (SfAlpha), u = zeta Ap + eta (t - r + beta u).  'GPBICGAR2'
+// lands here too (the reference tests the 8-character prefix first).
+// slots: 0 r0, 1 p, 2 r, 3 t, 4 z, 5 A p, 6 A r, 7 u, 8 y, 9 x, 10 A u,
+//        11 xr (mat-vec out), 12 b
+enum { A_R0 = 0, A_P, A_R, A_T, A_Z, A_AP, A_AR, A_U, A_Y, A_X, A_AU, A_XR, A_B, A_NSLOT };
+
+template <class T> struct ArStart {
+    Slots<T> V;
+    KState* stt;
+    int zero_guess;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 b = ld(V.v(A_B, r), i);
+        st(V.v(A_X, r), i, zero_guess ? make_double2(0, 0) : b);
+        if (zero_guess) st(V.v(A_XR, r), i, make_double2(0, 0));
+        acc[0].x += b.x * b.x + b.y * b.y;
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.norm = sqrt(a[0].x);
+        s.itno = 0;
+        s.steperr = -1;
+    }
+};
+
+// label 10: r0 = r = b - A x0, R0RN = r0^H r0 (the other vectors start at 0);
+// then A r, and label 20: beta = 0
+template <class T> struct ArInit {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 rr = zsub(ld(V.v(A_B, r), i), ld(V.v(A_XR, r), i));
+        const double2 z = make_double2(0, 0);
+        st(V.v(A_R0, r), i, rr);
+        st(V.v(A_R, r), i, rr);
+        st(V.v(A_P, r), i, z);
+        st(V.v(A_U, r), i, z);
+        st(V.v(A_AP, r), i, z);
+        st(V.v(A_AU, r), i, z);
+        st(V.v(A_T, r), i, z);
+        st(V.v(A_Z, r), i, z);
+        st(V.v(A_Y, r), i, z);
+        acc[0] = zadd(acc[0], zconjmul(rr, rr));
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.r0rn = a[0];
+        s.beta = make_double2(0, 0);
+        s.itno = 0;
+    }
+};
+
+// label 100: p = r + beta (p - u), Ap = Ar + beta (Ap - Au), alpha, zeta, eta
+template <class T> struct ArAlpha {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2* acc) const {
+        const double2 ar = ld(V.v(A_AR, r), i), y = ld(V.v(A_Y, r), i), rr = ld(V.v(A_R, r), i);
+        st(V.v(A_P, r), i, zadd(rr, zmul(s.beta, zsub(ld(V.v(A_P, r), i), ld(V.v(A_U, r), i)))));
+        const double2 ap = zadd(ar, zmul(s.beta, zsub(ld(V.v(A_AP, r), i), ld(V.v(A_AU, r), i))));
+        st(V.v(A_AP, r), i, ap);
+        acc[0] = zadd(acc[0], zconjmul(ld(V.v(A_R0, r), i), ap));
+        acc[1] = zadd(acc[1], zconjmul(y, y));
+        acc[2] = zadd(acc[2], zconjmul(ar, rr));
+        acc[3] = zadd(acc[3], zconjmul(y, rr));
+        acc[4] = zadd(acc[4], zconjmul(ar, y));
+        acc[5] = zadd(acc[5], zconjmul(ar, ar));
+    }
+    __device__ void finish(int rhs, KState& s, int& status, const double2* a) const {
+        SfAlpha<T>{V, stt, 0}.finish(rhs, s, status, a);
+    }
+};
+
+// u = zeta Ap + eta (t - r + beta u); then A u
+template <class T> struct ArU {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2*) const {
+        const double2 q = zadd(zsub(ld(V.v(A_T, r), i), ld(V.v(A_R, r), i)), zmul(s.beta, ld(V.v(A_U, r), i)));
+        st(V.v(A_U, r), i, zadd(zmul(s.dzeta, ld(V.v(A_AP, r), i)), zmul(s.eta, q)));
+    }
+    __device__ void finish(int, KState&, int&, const double2*) const {}
+};
+
+// label 40: t, z, y, x, r = t - y and the stop test; then A r
+template <class T> struct ArUpdate {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2* acc) const {
+        const double2 rr = ld(V.v(A_R, r), i);
+        const double2 t = zsub(rr, zmul(s.alpha, ld(V.v(A_AP, r), i)));
+        const double2 z = zsub(zadd(zmul(s.dzeta, rr), zmul(s.eta, ld(V.v(A_Z, r), i))), zmul(s.alpha, ld(V.v(A_U, r), i)));
+        const double2 y = zsub(zadd(zmul(s.dzeta, ld(V.v(A_AR, r), i)), zmul(s.eta, ld(V.v(A_Y, r), i))),
+                               zmul(s.alpha, ld(V.v(A_AU, r), i)));
+        st(V.v(A_T, r), i, t);
+        st(V.v(A_Z, r), i, z);
+        st(V.v(A_Y, r), i, y);
+        st(V.v(A_X, r), i, zadd(zadd(ld(V.v(A_X, r), i), zmul(s.alpha, ld(V.v(A_P, r), i))), z));
+        const double2 rn = zsub(t, y);
+        st(V.v(A_R, r), i, rn);
+        acc[0].x += rn.x * rn.x + rn.y * rn.y;
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        s.residu = sqrt(a[0].x) / s.norm;
+        if (s.residu <= s.tol) {
+            status = 1;
+            s.steperr = 0;
+        }
+    }
+};
+
+// label 50: beta = alpha r0^H r / zeta / R0RN, the iteration limit
+template <class T> struct ArBeta {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        acc[0] = zadd(acc[0], zconjmul(ld(V.v(A_R0, r), i), ld(V.v(A_R, r), i)));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        if (zisnull(s.r0rn)) {
+            status = -1;
+            s.steperr = 5;
+            return;
+        }
+        if (zisnull(s.dzeta)) {
+            status = -1;
+            s.steperr = 6;
+            return;
+        }
+        s.beta = zdiv(zdiv(zmul(s.alpha, a[0]), s.dzeta), s.r0rn);
+        s.r0rn = a[0];
         if (s.itno <= s.maxit) {
             s.itno += 1;
         } else {

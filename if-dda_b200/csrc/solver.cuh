@@ -120,6 +120,7 @@ struct SolverWork {
 };
 
 int reduction_blocks(long n3);
+int method_family(int method);
 template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>& W, cudaStream_t st);
 void solve_fp64(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b_dev, double2* x_out,
                 std::vector<SolveResult>& res, cudaStream_t st);

@@ -300,8 +300,11 @@ typedef struct {
     double norm;
 } gpbicg_state;
 
+/* every2 = 1 is GPBICG2 (cdmlib/gpbicg2.f): the same iteration, but every
+   even ITNO (not only the first) takes the zeta-only step (gpbicg2.f, label
+   30: mod(ITNO,2) = 0). */
 static void gpbicg(zc *xi, zc *xr, const zc *B, long n, int *nou, zc *W, int *itno,
-                   int maxit, double tol, gpbicg_state *S, int *status, int *steperr) {
+                   int maxit, double tol, gpbicg_state *S, int *status, int *steperr, int every2) {
 #define WK(c) (W + (size_t)(c) * n)
     zc *r0 = WK(0), *p = WK(1), *r = WK(2), *y = WK(3), *t = WK(4), *Ap = WK(5),
        *At = WK(6), *u = WK(7), *w = WK(8), *z = WK(9), *x = WK(10), *told = WK(11);
@@ -377,7 +380,7 @@ L20: {
 L30: {
 #pragma omp parallel for
     for (long i = 0; i < n; i++) At[i] = xr[i];
-    if (*itno == 0) {
+    if (every2 ? *itno % 2 == 0 : *itno == 0) {
         double dr = 0, di = 0, cr = 0, ci = 0;
 #pragma omp parallel for reduction(+ : dr, di, cr, ci)
         for (long i = 0; i < n; i++) {
@@ -951,8 +954,12 @@ typedef struct {
     double norm;
 } gpsafe_state;
 
+/* plus = 1 is GPBICGplus (cdmlib/gpbicgplus.f): the same iteration (it forms
+   t and z before the second mat-vec instead of after), NORM summed as
+   |b_i|^2 and zeta, eta written from the same five dot products in its own
+   form. */
 static void gpbicgsafe(zc *xi, zc *xr, const zc *B, long n, int *nou, zc *W, int *itno, int maxit,
-                       double tol, gpsafe_state *S, int *status, int *steperr) {
+                       double tol, gpsafe_state *S, int *status, int *steperr, int plus) {
 #define WK(c) (W + (size_t)(c) * n)
     zc *r0 = WK(0), *p = WK(1), *u = WK(2), *r = WK(3), *au = WK(4), *ar = WK(5), *ap = WK(6), *t = WK(7),
        *z = WK(8), *y = WK(9), *x = WK(10);
@@ -968,7 +975,7 @@ static void gpbicgsafe(zc *xi, zc *xr, const zc *B, long n, int *nou, zc *W, int
 #pragma omp parallel for reduction(+ : nrm)
         for (long i = 0; i < n; i++) {
             x[i] = xi[i];
-            nrm += creal(B[i] * conj(B[i]));
+            nrm += plus ? cabs(B[i]) * cabs(B[i]) : creal(B[i] * conj(B[i]));
         }
         S->norm = sqrt(nrm);
     }
@@ -1024,16 +1031,29 @@ L20: {
         }
         S->dzeta = num / den;
     } else {
-        const zc c1 = zsum(y, y, n, 1), c2 = zsum(ar, r, n, 1), c3 = zsum(y, r, n, 1),
-                 c4 = zsum(ar, y, n, 1), c5 = zsum(ar, ar, n, 1);
-        const zc c = c5 * c1 - c4 * conj(c4);
-        if (c == 0) {
-            *status = -1;
-            *steperr = 3;
-            return;
+        if (plus) {
+            const zc c1 = zsum(y, y, n, 1), c2 = zsum(ar, ar, n, 1), c3 = zsum(ar, r, n, 1),
+                     c4 = zsum(y, r, n, 1), c5 = zsum(y, ar, n, 1);
+            const zc c = c1 * c2 - c5 * conj(c5);
+            if (c == 0) {
+                *status = -1;
+                *steperr = 3;
+                return;
+            }
+            S->dzeta = (c1 * c3 - c4 * conj(c5)) / c;
+            S->eta = (c2 * c4 - c5 * c3) / c;
+        } else {
+            const zc c1 = zsum(y, y, n, 1), c2 = zsum(ar, r, n, 1), c3 = zsum(y, r, n, 1),
+                     c4 = zsum(ar, y, n, 1), c5 = zsum(ar, ar, n, 1);
+            const zc c = c5 * c1 - c4 * conj(c4);
+            if (c == 0) {
+                *status = -1;
+                *steperr = 3;
+                return;
+            }
+            S->dzeta = (c1 * c2 - c3 * c4) / c;
+            S->eta = (c5 * c3 - conj(c4) * c2) / c;
         }
-        S->dzeta = (c1 * c2 - c3 * c4) / c;
-        S->eta = (c5 * c3 - conj(c4) * c2) / c;
     }
     const zc dz = S->dzeta, et = S->eta;
 #pragma omp parallel for
@@ -1077,6 +1097,145 @@ L40: {
     *status = 1;
     for (long i = 0; i < n; i++) xi[i] = x[i];
     *nou = 4;
+}
+}
+
+/* ------------------------------------------------------------------------- */
+/* GPBiCG-AR (associate residual) reverse communication: cdmlib/gpbicgar.f.   */
+/* Mat-vecs A u then A r; A p carried by Ap = Ar + beta (Ap - Au).  Work      */
+/* columns: 0 r0 (shadow), 1 p, 2 r, 3 t, 4 z, 5 Ap, 6 Ar, 7 u, 8 y, 10 x,    */
+/* 11 Au.  The reference never sets p, u, Ap, Au, t before the first pass     */
+/* (they are multiplied by beta = 0 there); they start at zero here.          */
+/* ------------------------------------------------------------------------- */
+static void gpbicgar(zc *xi, zc *xr, const zc *B, long n, int *nou, zc *W, int *itno, int maxit,
+                     double tol, gpsafe_state *S, int *status, int *steperr) {
+#define WK(c) (W + (size_t)(c) * n)
+    zc *r0 = WK(0), *p = WK(1), *r = WK(2), *t = WK(3), *z = WK(4), *ap = WK(5), *ar = WK(6), *u = WK(7),
+       *y = WK(8), *x = WK(10), *au = WK(11);
+#undef WK
+    if (*nou == 1) goto L10;
+    if (*nou == 2) goto L20;
+    if (*nou == 4) goto L40;
+    if (*nou == 5) goto L50;
+    if (*nou == 6) goto L60;
+    *status = 0;
+    *steperr = -1;
+    {
+        double nrm = 0;
+#pragma omp parallel for reduction(+ : nrm)
+        for (long i = 0; i < n; i++) {
+            x[i] = xi[i];
+            nrm += creal(B[i] * conj(B[i]));
+        }
+        S->norm = sqrt(nrm);
+    }
+    *nou = 1;
+    return;
+L10:
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        r0[i] = B[i] - xr[i];
+        r[i] = r0[i];
+        xi[i] = r0[i];
+        p[i] = u[i] = ap[i] = au[i] = t[i] = z[i] = y[i] = 0;
+    }
+    S->r0rn = zsum(r0, r0, n, 1);
+    *nou = 2;
+    return;
+L20:
+    S->beta = 0;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) ar[i] = xr[i];
+    *itno = -1;
+L100: {
+    *itno += 1;
+    const zc be = S->beta;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        p[i] = r[i] + be * (p[i] - u[i]);
+        ap[i] = ar[i] + be * (ap[i] - au[i]);
+    }
+    const zc c0 = zsum(r0, ap, n, 1);
+    if (cabs(c0) == 0.0) {
+        *status = -1;
+        *steperr = 1;
+        return;
+    }
+    S->alpha = S->r0rn / c0;
+    if (*itno != 0) {
+        const zc c1 = zsum(y, y, n, 1), c2 = zsum(ar, r, n, 1), c3 = zsum(y, r, n, 1),
+                 c4 = zsum(ar, y, n, 1), c5 = zsum(ar, ar, n, 1);
+        const zc c = c5 * c1 - c4 * conj(c4);
+        if (cabs(c) == 0.0) {
+            *status = -1;
+            *steperr = 3;
+            return;
+        }
+        S->dzeta = (c1 * c2 - c3 * c4) / c;
+        S->eta = (c5 * c3 - conj(c4) * c2) / c;
+    } else {
+        const zc den = zsum(ar, ar, n, 1), num = zsum(ar, r, n, 1);
+        if (cabs(den) == 0.0) {
+            *status = -1;
+            *steperr = 2;
+            return;
+        }
+        S->dzeta = num / den;
+        S->eta = 0;
+    }
+    const zc dz = S->dzeta, et = S->eta;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        u[i] = dz * ap[i] + et * (t[i] - r[i] + be * u[i]);
+        xi[i] = u[i];
+    }
+    *nou = 4;
+    return;
+}
+L40: {
+    const zc al = S->alpha, dz = S->dzeta, et = S->eta;
+    double res = 0;
+#pragma omp parallel for reduction(+ : res)
+    for (long i = 0; i < n; i++) {
+        au[i] = xr[i];
+        t[i] = r[i] - al * ap[i];
+        z[i] = dz * r[i] + et * z[i] - al * u[i];
+        y[i] = dz * ar[i] + et * y[i] - al * au[i];
+        x[i] = x[i] + al * p[i] + z[i];
+        r[i] = t[i] - y[i];
+        res += creal(r[i] * conj(r[i]));
+    }
+    if (sqrt(res) / S->norm <= tol) {
+        *status = 1;
+        for (long i = 0; i < n; i++) xi[i] = x[i];
+        *nou = 6;
+        return;
+    }
+}
+L60:
+    *nou = 5;
+    for (long i = 0; i < n; i++) xi[i] = r[i];
+    return;
+L50: {
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) ar[i] = xr[i];
+    const zc c = zsum(r0, r, n, 1);
+    if (cabs(S->r0rn) == 0.0) {
+        *status = -1;
+        *steperr = 5;
+        return;
+    }
+    if (cabs(S->dzeta) == 0.0) {
+        *status = -1;
+        *steperr = 6;
+        return;
+    }
+    S->beta = S->alpha * c / S->dzeta / S->r0rn;
+    S->r0rn = c;
+    if (*itno <= maxit) goto L100;
+    *status = 1;
+    for (long i = 0; i < n; i++) xi[i] = x[i];
+    *nou = 6;
 }
 }
 
@@ -1131,10 +1290,11 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
        of the blank-padded character(12) methodeit, in this order */
     int kind = 0;
     if (strncmp(meth, "GPBICG1", 7) == 0) kind = 1;
-    else if (strncmp(meth, "GPBICG2", 7) == 0) kind = 0;
+    else if (strncmp(meth, "GPBICG2", 7) == 0) kind = 8;
     else if (strncmp(meth, "GPBICGsafe", 10) == 0) kind = 7;
-    else if (strncmp(meth, "GPBICGplus", 10) == 0 || strncmp(meth, "GPBICGAR", 8) == 0 ||
-             strncmp(meth, "BICGSTARPLUS", 12) == 0 || strncmp(meth, "QMRCLA", 6) == 0) kind = 0;
+    else if (strncmp(meth, "GPBICGplus", 10) == 0) kind = 9;
+    else if (strncmp(meth, "GPBICGAR", 8) == 0) kind = 10;  /* 'GPBICGAR2' too: (1:8) is tested first */
+    else if (strncmp(meth, "BICGSTARPLUS", 12) == 0 || strncmp(meth, "QMRCLA", 6) == 0) kind = 0;
     else if (strncmp(meth, "TFQMR", 5) == 0) kind = 6;
     else if (strncmp(meth, "CG   ", 5) == 0) kind = 5;
     else if (strncmp(meth, "BICGSTAB", 8) == 0) kind = 4;
@@ -1163,21 +1323,23 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
        FFloc (the X argument), which the driver copies back to xi */
     const int x_in_floc = kind == 2 || kind == 3 || kind == 4 || kind == 6;
     for (;;) {
-        if (kind == 1)
-            gpbicg(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &gs, &nstat, &steperr);
+        if (kind == 1 || kind == 8)
+            gpbicg(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &gs, &nstat, &steperr, kind == 8);
         else if (kind == 4)
             bicgstab(FFloc, xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &bs, &nstat, &steperr);
         else if (kind == 5)
             zcg(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &cs, &nstat);
         else if (kind == 6)
             tfqmr(FFloc, xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &ts, &nstat, &steperr);
-        else if (kind == 7)
-            gpbicgsafe(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &ss, &nstat, &steperr);
+        else if (kind == 10)
+            gpbicgar(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &ss, &nstat, &steperr);
+        else if (kind == 7 || kind == 9)
+            gpbicgsafe(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &ss, &nstat, &steperr, kind == 9);
         else
             qmrbicgstab(FFloc, xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &qs,
                         kind == 2 ? 1 : 2, &nstat, &steperr);
-        norm = kind == 1 ? gs.norm : kind == 4 ? bs.norm : kind == 5 ? cs.norm : kind == 6 ? ts.norm
-             : kind == 7 ? ss.norm : qs.norm;
+        norm = kind == 1 || kind == 8 ? gs.norm : kind == 4 ? bs.norm : kind == 5 ? cs.norm : kind == 6 ? ts.norm
+             : kind == 7 || kind == 9 || kind == 10 ? ss.norm : qs.norm;
         if (nstat < 0) {
             *nstop = 1;
             /* the TFQMR branch prints it without '!' (inverserigopt.f:609) */
@@ -1210,7 +1372,7 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
         t += creal(xr[i] * conj(xr[i]));
     }
     *tol1 = sqrt(t) / norm;
-    if (kind == 1 || kind == 6 || kind == 7) *nloop += 1;
+    if (kind == 1 || kind >= 6) *nloop += 1;
     free(xi); free(xr); free(W);
     return *nstop;
 }
@@ -1225,7 +1387,7 @@ int orc_gpbicg_dense(int ndim, const zc *mat /* column-major ndim x ndim */, con
     gpbicg_state S;
     memset(&S, 0, sizeof S);
     for (;;) {
-        gpbicg(xi, xr, b, ndim, &nou, W, &itno, maxit, tol, &S, &st, &se);
+        gpbicg(xi, xr, b, ndim, &nou, W, &itno, maxit, tol, &S, &st, &se, 0);
         if (st < 0) break;
         for (int i = 0; i < ndim; i++) {
             zc acc = 0;

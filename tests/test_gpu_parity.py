@@ -296,11 +296,12 @@ def test_anisotropy_only_in_the_tail_matches_oracle(gctx, orc):
     g.close()
 
 
-@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR", "GPBICGsafe"])
-def test_bicgstab_and_cg_match_oracle(gctx, orc, meth):
-    """The reference's BiCGSTAB (pimzbicgstab.f) and complex-symmetric CG
-    (zcg.f) on the sphere (inside-only, Tabdip) and on a full-box GRF cube:
-    identical counters, local field within 1e-7, the method's tol1."""
+@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR", "GPBICGsafe", "GPBICG2", "GPBICGplus", "GPBICGAR"])
+def test_other_methods_match_oracle(gctx, orc, meth):
+    """The reference's other Krylov methods (pimzbicgstab.f, zcg.f, tfqmr.f,
+    gpbicgsafe.f, gpbicg2.f, gpbicgplus.f, gpbicgar.f) on the sphere
+    (inside-only, Tabdip) and on a full-box GRF cube: identical counters,
+    local field within 1e-7, the method's tol1."""
     ob, k0, E0, ff0, G = _c1_inputs(orc)
     ref = orc.inverserig(G, 16, 16, 16, ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-5, tabdip=ob.tabdip)
     assert ref["nstop"] == 0, ref["infostr"]
@@ -320,8 +321,8 @@ def test_bicgstab_and_cg_match_oracle(gctx, orc, meth):
     g.close()
 
 
-@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR", "GPBICGsafe"])
-def test_bicgstab_and_cg_mixed_precision(gctx, orc, meth):
+@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR", "GPBICGsafe", "GPBICG2"])
+def test_other_methods_mixed_precision(gctx, orc, meth):
     from ifdda import IFDDA_MIXED
     ob, k0, E0, ff0, G = _c1_inputs(orc)
     tight = orc.inverserig(G, 16, 16, 16, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-10,

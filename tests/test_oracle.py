@@ -121,13 +121,14 @@ def test_qmr_agrees_with_gpbicg(orc, meth):
     assert rel(b["FFloc"], a["FFloc"]) < 1e-8
 
 
-@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR", "GPBICGsafe"])
-def test_bicgstab_and_cg_agree_with_gpbicg(orc, meth):
-    """BiCGSTAB (pimzbicgstab.f) and complex-symmetric CG (zcg.f) restated:
-    on the homogeneous sphere (A complex symmetric) both reach the GPBICG
-    solution; their counters follow the reference drivers (BiCGSTAB: 2 + 2
-    nloop mat-vecs, CG: nloop + 2), and BiCGSTAB's tol1 is divided by the
-    squared norm of the initial residual as in the reference."""
+@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR", "GPBICGsafe", "GPBICG2", "GPBICGplus", "GPBICGAR"])
+def test_other_methods_agree_with_gpbicg(orc, meth):
+    """The other Krylov methods restated (pimzbicgstab.f, zcg.f, tfqmr.f,
+    gpbicgsafe.f, gpbicg2.f, gpbicgplus.f, gpbicgar.f): on the homogeneous
+    sphere (A complex symmetric) they reach the GPBICG solution; their
+    counters follow the reference drivers (BiCGSTAB and the GPBiCG family: 2 +
+    2 nloop mat-vecs, CG and TFQMR: nloop + 2), and BiCGSTAB's tol1 is divided
+    by the squared norm of the initial residual as in the reference."""
     ob, k0, E0 = c1(nnnr=8)
     G = orc.greencalculfft(8, 8, 8, ob.aretecube, k0)
     ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 1.0, 0, 0.0, 0.0)
@@ -137,7 +138,7 @@ def test_bicgstab_and_cg_agree_with_gpbicg(orc, meth):
     if meth in ("CG", "TFQMR"):
         assert b["ncompte"] == b["nloop"] + 2 and b["tol1"] < 1e-9
         assert rel(b["FFloc"], a["FFloc"]) < 1e-8
-    elif meth == "GPBICGsafe":
+    elif meth in ("GPBICGsafe", "GPBICG2", "GPBICGplus", "GPBICGAR"):
         assert b["ncompte"] == 2 * b["nloop"] + 2 and b["tol1"] < 1e-10
         assert rel(b["FFloc"], a["FFloc"]) < 1e-8
     else:
@@ -147,12 +148,13 @@ def test_bicgstab_and_cg_agree_with_gpbicg(orc, meth):
         assert 0 < b["tol1"] < 1e-10
 
 
-@pytest.mark.parametrize("name,works", [("CG", True), ("CGX", False), ("BICGSTAB", True), ("GPBICGAR2", False),
+@pytest.mark.parametrize("name,works", [("CG", True), ("CGX", False), ("BICGSTAB", True), ("GPBICGAR2", True),
                                         ("TFQMR", True), ("BICGSTARPLUS", False), ("QMRCLA", False),
-                                        ("GPBICGsafe", True), ("GPBICG2", False)])
+                                        ("GPBICGsafe", True), ("GPBICG2", True)])
 def test_method_prefixes(orc, name, works):
     """methodeit is matched by prefix in the reference's order: 'GPBICGAR2'
-    meets the 'GPBICGAR' test first, 'CGX' is not 'CG' (blank padded)."""
+    meets the 'GPBICGAR' test first (and runs GPBICGAR), 'CGX' is not 'CG'
+    (blank padded)."""
     ob, k0, E0 = c1(nnnr=4)
     G = orc.greencalculfft(4, 4, 4, ob.aretecube, k0)
     ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 1.0, 0, 0.0, 0.0)
