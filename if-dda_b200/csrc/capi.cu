@@ -115,12 +115,15 @@ int method_code(const char* m) {
     if (!strncmp(buf, "GPBICGsafe", 10)) return 7;
     if (!strncmp(buf, "GPBICGplus", 10)) return 9;
     if (!strncmp(buf, "GPBICGAR", 8)) return 10;  // 'GPBICGAR2' too: (1:8) is tested first
-    if (!strncmp(buf, "BICGSTARPLUS", 12) || !strncmp(buf, "QMRCLA", 6)) return 0;
+    if (!strncmp(buf, "BICGSTARPLUS", 12)) return 11;
+    if (!strncmp(buf, "QMRCLA", 6)) return 0;
     if (!strncmp(buf, "TFQMR", 5)) return 6;
     if (!strncmp(buf, "CG   ", 5)) return 5;
     if (!strncmp(buf, "BICGSTAB", 8)) return 4;
     if (!strncmp(buf, "QMRBICGSTAB1", 12)) return 2;
     if (!strncmp(buf, "QMRBICGSTAB2", 12)) return 3;
+    if (!strncmp(buf, "GPBICOR", 7)) return 13;
+    if (!strncmp(buf, "CORS   ", 7)) return 12;
     return 0;
 }
 

@@ -133,7 +133,7 @@ template void cast_dev<double>(const double2*, double2*, long, cudaStream_t);
 int reduction_blocks(long n3) { return (int)std::max<long>(1, std::min<long>((n3 + KNT * 4 - 1) / (KNT * 4), 1024)); }
 
 template <class T> void KrylovWork<T>::ensure(int method, int nrhs_, long n3_) {
-    static const int nslots[] = {0, G_NSLOT, Q_NSLOT, 0, B_NSLOT, C_NSLOT, T_NSLOT, S_NSLOT, A_NSLOT};
+    static const int nslots[] = {0, G_NSLOT, Q_NSLOT, 0, B_NSLOT, C_NSLOT, T_NSLOT, S_NSLOT, A_NSLOT, P_NSLOT, R_NSLOT, O_NSLOT};
     nslot = nslots[method_family(method)];
     nrhs = nrhs_;
     n3 = n3_;
@@ -278,6 +278,27 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
             mv_solver<T>(G, sp, W, B_S, B_T, status, st);
             vec_launch<2>(BOmega<T>{V, S}, n3, nblk, nrhs, rs, status, st);
             vec_launch<1>(BUpdate<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+        } else if (sp.method == 12) {
+            mv_solver<T>(G, sp, W, R_R, R_AR, status, st);
+            vec_launch<1>(CsRho<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<0>(CsD<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            mv_solver<T>(G, sp, W, R_D, R_Q, status, st);
+            vec_launch<1>(CsAlpha<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<1>(CsUpdate<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+        } else if (sp.method == 13) {
+            mv_solver<T>(G, sp, W, O_R, O_AR, status, st);
+            vec_launch<1>(ORho<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<0>(OP<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            mv_solver<T>(G, sp, W, O_W4, O_AW4, status, st);
+            vec_launch<1>(OAlpha<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<5>(OZeta<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<1>(OUpdate<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+        } else if (sp.method == 11) {
+            mv_solver<T>(G, sp, W, P_R, P_AR, status, st);
+            vec_launch<8>(PsCoef<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<0>(PsW<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            mv_solver<T>(G, sp, W, P_W4, P_AW4, status, st);
+            vec_launch<1>(PsUpdate<T>{V, S}, n3, nblk, nrhs, rs, status, st);
         } else if (sp.method == 10) {
             vec_launch<6>(ArAlpha<T>{V, S}, n3, nblk, nrhs, rs, status, st);
             vec_launch<0>(ArU<T>{V, S}, n3, nblk, nrhs, rs, status, st);
@@ -331,6 +352,18 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
         vec_launch<1>(BStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
         if (!sp.zero_guess) mv_solver<T>(G, sp, W, B_X, B_XR, status, st);
         vec_launch<2>(BInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+    } else if (sp.method == 12) {
+        vec_launch<1>(CsStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
+        if (!sp.zero_guess) mv_solver<T>(G, sp, W, R_X, R_XR, status, st);
+        vec_launch<1>(CsInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+    } else if (sp.method == 13) {
+        vec_launch<1>(OStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
+        if (!sp.zero_guess) mv_solver<T>(G, sp, W, O_X, O_XR, status, st);
+        vec_launch<0>(OInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+    } else if (sp.method == 11) {
+        vec_launch<1>(PsStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
+        if (!sp.zero_guess) mv_solver<T>(G, sp, W, P_X, P_XR, status, st);
+        vec_launch<1>(PsInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
     } else if (sp.method == 10) {
         vec_launch<1>(ArStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
         if (!sp.zero_guess) mv_solver<T>(G, sp, W, A_X, A_XR, status, st);
@@ -488,7 +521,8 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
 
 // Method codes (capi.cu method_code) -> the state machine and slot layout
 // they run on: GPBICG2 runs on GPBiCG's (1), GPBICGplus on GPBiCGsafe's (7),
-// QMRBICGSTAB2 on QMRBICGSTAB1's (2), GPBICGAR has its own (8).
+// QMRBICGSTAB2 on QMRBICGSTAB1's (2); GPBICGAR (8), BICGSTARPLUS (9), CORS
+// (10) and GPBICOR (11) have their own.
 int method_family(int method) {
     switch (method) {
     case 1:
@@ -499,20 +533,23 @@ int method_family(int method) {
     case 7:
     case 9: return 7;
     case 10: return 8;
+    case 11: return 9;
+    case 12: return 10;
+    case 13: return 11;
     default: return 2;
     }
 }
 
 template <class T> int KrylovWork<T>::x_slot(int method) const {
-    static const int s[] = {0, G_X, Q_X, 0, B_X, C_X, T_X, S_X, A_X};
+    static const int s[] = {0, G_X, Q_X, 0, B_X, C_X, T_X, S_X, A_X, P_X, R_X, O_X};
     return s[method_family(method)];
 }
 template <class T> int KrylovWork<T>::b_slot(int method) const {
-    static const int s[] = {0, G_B, Q_B, 0, B_B, C_B, T_B, S_B, A_B};
+    static const int s[] = {0, G_B, Q_B, 0, B_B, C_B, T_B, S_B, A_B, P_B, R_B, O_B};
     return s[method_family(method)];
 }
 template <class T> int KrylovWork<T>::xr_slot(int method) const {
-    static const int s[] = {0, G_XR, Q_XR, 0, B_XR, C_XR, T_XR, S_XR, A_XR};
+    static const int s[] = {0, G_XR, Q_XR, 0, B_XR, C_XR, T_XR, S_XR, A_XR, P_XR, R_XR, O_XR};
     return s[method_family(method)];
 }
 
@@ -524,9 +561,11 @@ template <class T> int KrylovWork<T>::xr_slot(int method) const {
 // :676-742; TFQMR: one per pass plus A x0, A u0 and the residual one, and
 // the driver adds one to ITNO, :603-675).
 void method_counts(int method, int itno, int& nloop, int& ncompte) {
-    if (method == 1 || method >= 7) {
+    if (method == 1 || (method >= 7 && method != 13)) {
         // GPBICG1, GPBICGsafe (:174-237), GPBICG2 (:109-173), GPBICGplus
-        // (:238-301), GPBICGAR (:302-366)
+        // (:238-301), GPBICGAR (:302-366), BICGSTARPLUS (:431-498), CORS
+        // (:1009-1072); GPBICOR (:943-1008) counts ITNO from 1 and its driver
+        // does not add one, so it counts like QMR-BiCGSTAB
         nloop = itno + 1;
         ncompte = 1 + 2 * (itno + 1) + 1;
     } else if (method == 6) {

@@ -21,6 +21,8 @@ struct KState {
     double2 alpha, beta, eta, dzeta, r0rn, c2, c5;
     // QMR-BiCGSTAB
     double2 rho, omega, tau, taut, theta, thetat, etaq, etat, f1, qbeta;
+    // CORS, GPBiCOR: rho of the previous iteration
+    double2 rhoa;
     double norm, residu, tol;
     int itno, steperr, maxit, conv;
 };
@@ -1025,6 +1027,484 @@ template <class T> struct ArBeta {
         }
         s.beta = zdiv(zdiv(zmul(s.alpha, a[0]), s.dzeta), s.r0rn);
         s.r0rn = a[0];
+        if (s.itno <= s.maxit) {
+            s.itno += 1;
+        } else {
+            status = 1;
+            s.steperr = 0;
+        }
+    }
+};
+
+// ---------------------------------------------------------- BiCGStar-plus ----
+// cdmlib/bicgstarplus.f (subroutine GPBICGSTARPLUS): shadow conj(r0) with
+// unconjugated dots, mat-vecs A r and A w4, eight dot products per
+// iteration.  The reference's first pass adds into two accumulators it never
+// cleared; they start at zero here.  Ends like GPBICG past MAXIT.
+// slots: 0 conj(r0), 1 A r, 2 r, 3 w4, 4 w5, 5 w6, 6 w7, 7 w8, 8 w9,
+//        9 A w4, 10 x, 11 w12, 12 xr (mat-vec out), 13 b
+enum { P_R0S = 0, P_AR, P_R, P_W4, P_W5, P_W6, P_W7, P_W8, P_W9, P_AW4, P_X, P_W12, P_XR, P_B, P_NSLOT };
+
+template <class T> struct PsStart {
+    Slots<T> V;
+    KState* stt;
+    int zero_guess;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 b = ld(V.v(P_B, r), i);
+        st(V.v(P_X, r), i, zero_guess ? make_double2(0, 0) : b);
+        if (zero_guess) st(V.v(P_XR, r), i, make_double2(0, 0));
+        acc[0].x += b.x * b.x + b.y * b.y;
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.norm = sqrt(a[0].x);
+        s.itno = 0;
+        s.steperr = -1;
+    }
+};
+
+// label 10: r = b - A x0, shadow conj(r), w4 = w5 = w8 = w9 = w12 = 0
+template <class T> struct PsInit {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 rr = zsub(ld(V.v(P_B, r), i), ld(V.v(P_XR, r), i));
+        const double2 z = make_double2(0, 0), rs = zconj(rr);
+        st(V.v(P_R, r), i, rr);
+        st(V.v(P_R0S, r), i, rs);
+        st(V.v(P_W4, r), i, z);
+        st(V.v(P_W5, r), i, z);
+        st(V.v(P_W8, r), i, z);
+        st(V.v(P_W9, r), i, z);
+        st(V.v(P_W12, r), i, z);
+        acc[0] = zadd(acc[0], zmul(rs, rr));
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.r0rn = a[0];
+        s.itno = 0;
+    }
+};
+
+// label 20: the eight dot products, beta, alpha, zeta, eta
+template <class T> struct PsCoef {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 rs = ld(V.v(P_R0S, r), i), rr = ld(V.v(P_R, r), i), ar = ld(V.v(P_AR, r), i),
+                      w5 = ld(V.v(P_W5, r), i);
+        acc[0] = zadd(acc[0], zmul(rs, rr));
+        acc[1] = zadd(acc[1], zmul(rs, ar));
+        acc[2] = zadd(acc[2], zconjmul(w5, w5));
+        acc[3] = zadd(acc[3], zconjmul(ar, rr));
+        acc[4] = zadd(acc[4], zconjmul(ar, w5));
+        acc[5] = zadd(acc[5], zconjmul(w5, rr));
+        acc[6] = zadd(acc[6], zconjmul(ar, ar));
+        acc[7] = zadd(acc[7], zmul(rs, ld(V.v(P_W12, r), i)));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        const double2 c1 = a[0], c2 = a[1], c3 = a[2], c4 = a[3], c5 = a[4], c6 = a[5], c7 = a[6], c8 = a[7];
+        if (s.itno == 0) {
+            s.eta = make_double2(0, 0);
+            s.beta = make_double2(0, 0);
+            s.r0rn = c1;
+            if (zisnull(c7)) {
+                status = -1;
+                s.steperr = 2;
+                return;
+            }
+            s.dzeta = zdiv(c4, c7);
+            if (zisnull(c2)) {
+                status = -1;
+                s.steperr = 3;
+                return;
+            }
+            s.alpha = zdiv(c1, c2);
+            return;
+        }
+        if (zisnull(s.dzeta)) {
+            status = -1;
+            s.steperr = 4;
+            return;
+        }
+        if (zisnull(s.r0rn)) {
+            status = -1;
+            s.steperr = 5;
+            return;
+        }
+        s.beta = zdiv(zmul(zdiv(make_double2(-s.alpha.x, -s.alpha.y), s.dzeta), c1), s.r0rn);
+        const double2 c = zsub(c2, zmul(s.beta, c8));
+        if (zisnull(c)) {
+            status = -1;
+            s.steperr = 6;
+            return;
+        }
+        s.alpha = zdiv(c1, c);
+        const double2 d = zsub(zmul(c7, c3), zmul(c5, zconj(c5)));
+        if (zisnull(d)) {
+            status = -1;
+            s.steperr = 7;
+            return;
+        }
+        s.dzeta = zdiv(zsub(zmul(c3, c4), zmul(c5, c6)), d);
+        s.eta = zdiv(zsub(zmul(c7, c6), zmul(zconj(c5), c4)), d);
+        s.r0rn = c1;
+    }
+};
+
+// w7 = Ar - beta w12, w6 = zeta r + eta w9, w4 = zeta w7 + eta (w5 - beta w4); then A w4
+template <class T> struct PsW {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2*) const {
+        const double2 w7 = zsub(ld(V.v(P_AR, r), i), zmul(s.beta, ld(V.v(P_W12, r), i)));
+        st(V.v(P_W7, r), i, w7);
+        st(V.v(P_W6, r), i, zadd(zmul(s.dzeta, ld(V.v(P_R, r), i)), zmul(s.eta, ld(V.v(P_W9, r), i))));
+        const double2 q = zsub(ld(V.v(P_W5, r), i), zmul(s.beta, ld(V.v(P_W4, r), i)));
+        st(V.v(P_W4, r), i, zadd(zmul(s.dzeta, w7), zmul(s.eta, q)));
+    }
+    __device__ void finish(int, KState&, int&, const double2*) const {}
+};
+
+// label 30 and 40: w8, w12, w9, w5, x, r, the stop test, the iteration limit
+template <class T> struct PsUpdate {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2* acc) const {
+        const double2 rr = ld(V.v(P_R, r), i), w4 = ld(V.v(P_W4, r), i), aw4 = ld(V.v(P_AW4, r), i),
+                      w6 = ld(V.v(P_W6, r), i);
+        const double2 w8 = zsub(zsub(rr, zmul(s.beta, ld(V.v(P_W8, r), i))), w4);
+        const double2 w12 = zsub(ld(V.v(P_W7, r), i), aw4);
+        st(V.v(P_W8, r), i, w8);
+        st(V.v(P_W12, r), i, w12);
+        st(V.v(P_W9, r), i, zsub(w6, zmul(s.alpha, w4)));
+        const double2 tmp = zadd(zmul(s.dzeta, ld(V.v(P_AR, r), i)), zmul(s.eta, ld(V.v(P_W5, r), i)));
+        st(V.v(P_W5, r), i, zsub(tmp, zmul(s.alpha, aw4)));
+        st(V.v(P_X, r), i, zadd(zadd(ld(V.v(P_X, r), i), w6), zmul(s.alpha, w8)));
+        const double2 rn = zsub(zsub(rr, tmp), zmul(s.alpha, w12));
+        st(V.v(P_R, r), i, rn);
+        acc[0].x += rn.x * rn.x + rn.y * rn.y;
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        s.residu = sqrt(a[0].x) / s.norm;
+        if (s.residu <= s.tol) {
+            status = 1;
+            s.steperr = 0;
+            return;
+        }
+        if (s.itno <= s.maxit) {
+            s.itno += 1;
+        } else {
+            status = 1;
+            s.steperr = 0;
+        }
+    }
+};
+
+// ------------------------------------------------------------------- CORS ----
+// cdmlib/cors.f: shadow conj(A r0) with unconjugated dots, mat-vecs A r and
+// A d.  Past MAXIT the reference returns a work column it never writes;
+// here x.  KState: alpha, beta, rho, rhoa; itno = ITNO (from 0).
+// slots: 0 shadow, 1 r, 2 A r, 3 e, 4 h, 5 d, 6 f, 7 g, 8 q = A d, 9 x,
+//        10 xr (mat-vec out), 11 b
+enum { R_RS = 0, R_R, R_AR, R_E, R_H, R_D, R_F, R_G, R_Q, R_X, R_XR, R_B, R_NSLOT };
+
+// x = x0 (or 0), NORM summed as |b_i|^2 (cors.f)
+template <class T> struct CsStart {
+    Slots<T> V;
+    KState* stt;
+    int zero_guess;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 b = ld(V.v(R_B, r), i);
+        st(V.v(R_X, r), i, zero_guess ? make_double2(0, 0) : b);
+        if (zero_guess) st(V.v(R_XR, r), i, make_double2(0, 0));
+        const double a = hypot(b.x, b.y);
+        acc[0].x += a * a;
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.norm = sqrt(a[0].x);
+        s.itno = 0;
+        s.steperr = -1;
+    }
+};
+
+// label 10: r = b - A x0
+template <class T> struct CsInit {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2*) const {
+        st(V.v(R_R, r), i, zsub(ld(V.v(R_B, r), i), ld(V.v(R_XR, r), i)));
+    }
+    __device__ void finish(int, KState& s, int&, const double2*) const { s.itno = 0; }
+};
+
+// label 20: (first pass) shadow = conj(A r); rho = shadow^T A r; beta
+template <class T> struct CsRho {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2* acc) const {
+        const double2 ar = ld(V.v(R_AR, r), i);
+        double2 rs;
+        if (s.itno == 0) {
+            rs = zconj(ar);
+            st(V.v(R_RS, r), i, rs);
+        } else {
+            rs = ld(V.v(R_RS, r), i);
+        }
+        acc[0] = zadd(acc[0], zmul(rs, ar));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        s.rho = a[0];
+        if (a[0].x == 0.0 && a[0].y == 0.0) {
+            status = -1;
+            s.steperr = 1;
+            return;
+        }
+        if (s.itno != 0) s.beta = zdiv(s.rho, s.rhoa);
+    }
+};
+
+// e, h, d (first pass: e = r, h = d = A r); then A d
+template <class T> struct CsD {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2*) const {
+        const double2 rr = ld(V.v(R_R, r), i), ar = ld(V.v(R_AR, r), i);
+        if (s.itno == 0) {
+            st(V.v(R_E, r), i, rr);
+            st(V.v(R_H, r), i, ar);
+            st(V.v(R_D, r), i, ar);
+        } else {
+            const double2 g = ld(V.v(R_G, r), i);
+            st(V.v(R_E, r), i, zadd(rr, zmul(s.beta, ld(V.v(R_F, r), i))));
+            const double2 h = zadd(ar, zmul(s.beta, g));
+            st(V.v(R_H, r), i, h);
+            st(V.v(R_D, r), i, zadd(h, zmul(s.beta, zadd(g, zmul(s.beta, ld(V.v(R_D, r), i))))));
+        }
+    }
+    __device__ void finish(int, KState&, int&, const double2*) const {}
+};
+
+// label 30: alpha = rho / shadow^T q
+template <class T> struct CsAlpha {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        acc[0] = zadd(acc[0], zmul(ld(V.v(R_RS, r), i), ld(V.v(R_Q, r), i)));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        if (a[0].x == 0.0 && a[0].y == 0.0) {
+            status = -1;
+            s.steperr = 2;
+            return;
+        }
+        s.alpha = zdiv(s.rho, a[0]);
+    }
+};
+
+// f, g, x += alpha (2 e - alpha d), r -= alpha (2 h - alpha q), the stop
+// test (||r|| summed as |r_i|^2), label 40
+template <class T> struct CsUpdate {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2* acc) const {
+        const double2 e = ld(V.v(R_E, r), i), d = ld(V.v(R_D, r), i), h = ld(V.v(R_H, r), i),
+                      q = ld(V.v(R_Q, r), i);
+        st(V.v(R_F, r), i, zsub(e, zmul(s.alpha, d)));
+        st(V.v(R_G, r), i, zsub(h, zmul(s.alpha, q)));
+        const double2 two = make_double2(2, 0);
+        st(V.v(R_X, r), i, zadd(ld(V.v(R_X, r), i), zmul(s.alpha, zsub(zmul(two, e), zmul(s.alpha, d)))));
+        const double2 rn = zsub(ld(V.v(R_R, r), i), zmul(s.alpha, zsub(zmul(two, h), zmul(s.alpha, q))));
+        st(V.v(R_R, r), i, rn);
+        const double a = hypot(rn.x, rn.y);
+        acc[0].x += a * a;
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        s.residu = sqrt(a[0].x) / s.norm;
+        if (s.residu <= s.tol) {
+            status = 1;
+            s.steperr = 0;
+            return;
+        }
+        s.rhoa = s.rho;
+        if (s.itno <= s.maxit) {
+            s.itno += 1;
+        } else {
+            status = 1;
+            s.steperr = 0;
+        }
+    }
+};
+
+// ---------------------------------------------------------------- GPBiCOR ----
+// cdmlib/gpbicor.f: mat-vecs A r and A w4; ITNO counts from 1 and its driver
+// reports it as is.  Past MAXIT the reference sets no solution; here x.
+// KState: alpha, beta, eta, dzeta, rho, rhoa; itno = ITNO.
+// slots: 0 r0, 1 p, 2 A r, 3 w4, 4 w5, 5 w6, 6 t, 7 w8, 8 w9, 9 r, 10 z,
+//        11 w12, 12 q, 13 s, 14 A w4, 15 x, 16 xr (mat-vec out), 17 b
+enum { O_R0 = 0, O_P, O_AR, O_W4, O_W5, O_W6, O_T, O_W8, O_W9, O_R, O_Z, O_W12, O_Q, O_S, O_AW4, O_X, O_XR, O_B,
+       O_NSLOT };
+
+template <class T> struct OStart {
+    Slots<T> V;
+    KState* stt;
+    int zero_guess;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 b = ld(V.v(O_B, r), i);
+        st(V.v(O_X, r), i, zero_guess ? make_double2(0, 0) : b);
+        if (zero_guess) st(V.v(O_XR, r), i, make_double2(0, 0));
+        acc[0].x += b.x * b.x + b.y * b.y;
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.norm = sqrt(a[0].x);
+        s.itno = 1;
+        s.steperr = -1;
+    }
+};
+
+// label 10: r0 = r = b - A x0, z = 0
+template <class T> struct OInit {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2*) const {
+        const double2 rr = zsub(ld(V.v(O_B, r), i), ld(V.v(O_XR, r), i));
+        st(V.v(O_R0, r), i, rr);
+        st(V.v(O_R, r), i, rr);
+        st(V.v(O_Z, r), i, make_double2(0, 0));
+    }
+    __device__ void finish(int, KState&, int&, const double2*) const {}
+};
+
+// label 20: rho = r0^H A r, beta = rho / rhoa alpha / zeta (0 on the first pass)
+template <class T> struct ORho {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        acc[0] = zadd(acc[0], zconjmul(ld(V.v(O_R0, r), i), ld(V.v(O_AR, r), i)));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        s.rho = a[0];
+        if (a[0].x == 0.0 && a[0].y == 0.0) {
+            status = -1;
+            s.steperr = 1;
+            return;
+        }
+        s.beta = s.itno == 1 ? make_double2(0, 0) : zdiv(zmul(zdiv(s.rho, s.rhoa), s.alpha), s.dzeta);
+    }
+};
+
+// p, w4, w5 (first pass: p = r0, w4 = A r, the rest 0); then A w4
+template <class T> struct OP {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2*) const {
+        const double2 ar = ld(V.v(O_AR, r), i);
+        if (s.itno == 1) {
+            const double2 z = make_double2(0, 0);
+            st(V.v(O_P, r), i, ld(V.v(O_R0, r), i));
+            st(V.v(O_W4, r), i, ar);
+            st(V.v(O_W12, r), i, z);
+            st(V.v(O_W5, r), i, z);
+            st(V.v(O_W8, r), i, z);
+            st(V.v(O_W9, r), i, z);
+            st(V.v(O_W6, r), i, z);
+        } else {
+            const double2 w4 = ld(V.v(O_W4, r), i);
+            st(V.v(O_W5, r), i, zadd(ld(V.v(O_W6, r), i), zmul(s.beta, w4)));
+            st(V.v(O_P, r), i,
+               zadd(ld(V.v(O_R, r), i), zmul(s.beta, zsub(ld(V.v(O_P, r), i), ld(V.v(O_W8, r), i)))));
+            st(V.v(O_W4, r), i, zadd(ar, zmul(s.beta, zsub(w4, ld(V.v(O_W9, r), i)))));
+        }
+    }
+    __device__ void finish(int, KState&, int&, const double2*) const {}
+};
+
+// label 30: alpha = rho / r0^H A w4
+template <class T> struct OAlpha {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        acc[0] = zadd(acc[0], zconjmul(ld(V.v(O_R0, r), i), ld(V.v(O_AW4, r), i)));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        if (a[0].x == 0.0 && a[0].y == 0.0) {
+            status = -1;
+            s.steperr = 2;
+            return;
+        }
+        s.alpha = zdiv(s.rho, a[0]);
+    }
+};
+
+// q, t, s and the five dot products of zeta and eta
+template <class T> struct OZeta {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2* acc) const {
+        const double2 rr = ld(V.v(O_R, r), i), w4 = ld(V.v(O_W4, r), i);
+        const double2 q = zadd(zsub(ld(V.v(O_W12, r), i), rr), zmul(s.alpha, zsub(w4, ld(V.v(O_W5, r), i))));
+        const double2 t = zsub(rr, zmul(s.alpha, w4));
+        const double2 sv = zsub(ld(V.v(O_AR, r), i), zmul(s.alpha, ld(V.v(O_AW4, r), i)));
+        st(V.v(O_Q, r), i, q);
+        st(V.v(O_T, r), i, t);
+        st(V.v(O_S, r), i, sv);
+        acc[0] = zadd(acc[0], zconjmul(sv, sv));
+        acc[1] = zadd(acc[1], zconjmul(q, t));
+        acc[2] = zadd(acc[2], zconjmul(q, sv));
+        acc[3] = zadd(acc[3], zconjmul(sv, t));
+        acc[4] = zadd(acc[4], zconjmul(q, q));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        const double2 c1 = a[0], c2 = a[1], c3 = a[2], c4 = a[3], c5 = a[4];
+        if (s.itno == 1) {
+            s.eta = make_double2(0, 0);
+            if (c1.x == 0.0 && c1.y == 0.0) {
+                status = -1;
+                s.steperr = 3;
+                return;
+            }
+            s.dzeta = zdiv(c4, c1);
+            return;
+        }
+        const double2 c = zsub(zmul(c1, c5), zmul(c3, zconj(c3)));
+        if (c.x == 0.0 && c.y == 0.0) {
+            status = -1;
+            s.steperr = 4;
+            return;
+        }
+        s.eta = zdiv(zsub(zmul(c1, c2), zmul(c3, c4)), c);
+        s.dzeta = zdiv(zsub(zmul(c5, c4), zmul(c2, zconj(c3))), c);
+    }
+};
+
+// w8, w9, z, r = t - eta q - zeta s, x += alpha p + z, w6 = s, w12 = t;
+// the stop test, label 40
+template <class T> struct OUpdate {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2* acc) const {
+        const double2 rr = ld(V.v(O_R, r), i), w4 = ld(V.v(O_W4, r), i), w12 = ld(V.v(O_W12, r), i),
+                      ar = ld(V.v(O_AR, r), i), sv = ld(V.v(O_S, r), i), t = ld(V.v(O_T, r), i);
+        const double2 w8 = zadd(zmul(s.dzeta, w4), zmul(s.eta, zadd(zsub(w12, rr), zmul(s.beta, ld(V.v(O_W8, r), i)))));
+        const double2 w9 = zadd(zdiv(zmul(s.dzeta, zsub(ar, sv)), s.alpha),
+                                zmul(s.eta, zadd(zsub(ld(V.v(O_W6, r), i), ar), zmul(s.beta, ld(V.v(O_W9, r), i)))));
+        const double2 z = zsub(zadd(zmul(s.dzeta, rr), zmul(s.eta, ld(V.v(O_Z, r), i))), zmul(s.alpha, w8));
+        st(V.v(O_W8, r), i, w8);
+        st(V.v(O_W9, r), i, w9);
+        st(V.v(O_Z, r), i, z);
+        const double2 rn = zsub(zsub(t, zmul(s.eta, ld(V.v(O_Q, r), i))), zmul(s.dzeta, sv));
+        st(V.v(O_R, r), i, rn);
+        acc[0].x += rn.x * rn.x + rn.y * rn.y;
+        st(V.v(O_X, r), i, zadd(zadd(ld(V.v(O_X, r), i), zmul(s.alpha, ld(V.v(O_P, r), i))), z));
+        st(V.v(O_W6, r), i, sv);
+        st(V.v(O_W12, r), i, t);
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        s.residu = sqrt(a[0].x) / s.norm;
+        if (s.residu <= s.tol) {
+            status = 1;
+            s.steperr = 0;
+            return;
+        }
+        s.rhoa = s.rho;
         if (s.itno <= s.maxit) {
             s.itno += 1;
         } else {

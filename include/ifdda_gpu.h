@@ -108,8 +108,9 @@ int ifdda_matvec_noalloc(ifdda_green* g, int precision, int ndip, const int* tab
    "GPBICG1" | "QMRBICGSTAB1" | "QMRBICGSTAB2" | "BICGSTAB" (pimzbicgstab.f)
    | "CG" (zcg.f) | "TFQMR" (tfqmr.f) | "GPBICGsafe" (gpbicgsafe.f) | "GPBICG2"
    (gpbicg2.f) | "GPBICGplus" (gpbicgplus.f) | "GPBICGAR" (gpbicgar.f; also
-   "GPBICGAR2", as in the reference), matched by prefix in the reference's
-   order; the other
+   "GPBICGAR2", as in the reference) | "BICGSTARPLUS" (bicgstarplus.f) |
+   "GPBICOR" (gpbicor.f) | "CORS" (cors.f), matched by prefix in the
+   reference's order; the other
    methods of the reference answer nstop = 1, "Iterative method not
    correct!".  On return FFloc = E (local field), FF = polarisa . E (dipole
    moments), tol1 = ||A E - FF0|| / NORM in FP64 with the method's NORM

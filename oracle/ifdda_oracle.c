@@ -1240,6 +1240,400 @@ L50: {
 }
 
 /* ------------------------------------------------------------------------- */
+/* BiCGStar-plus reverse communication: cdmlib/bicgstarplus.f (subroutine     */
+/* GPBICGSTARPLUS).  The shadow vector is conj(r0) with unconjugated dots.    */
+/* Work columns: 0 conj(r0), 1 A r, 2 r, 3 w4, 4 w5, 5 w6, 6 w7, 7 w8, 8 w9,  */
+/* 9 A w4, 10 x, 11 w12.  On its first pass the reference adds into two       */
+/* accumulators it never cleared (bicgstarplus.f, label 20); they start at 0  */
+/* here.  Ends like GPBICG (status 1 with the iterate past MAXIT).            */
+/* ------------------------------------------------------------------------- */
+static void bicgstarplus(zc *xi, zc *xr, const zc *B, long n, int *nou, zc *W, int *itno, int maxit,
+                         double tol, gpsafe_state *S, int *status, int *steperr) {
+#define WK(c) (W + (size_t)(c) * n)
+    zc *r0s = WK(0), *ar = WK(1), *r = WK(2), *w4 = WK(3), *w5 = WK(4), *w6 = WK(5), *w7 = WK(6), *w8 = WK(7),
+       *w9 = WK(8), *aw4 = WK(9), *x = WK(10), *w12 = WK(11);
+#undef WK
+    if (*nou == 1) goto L10;
+    if (*nou == 2) goto L20;
+    if (*nou == 3) goto L30;
+    if (*nou == 4) goto L40;
+    *status = 0;
+    *steperr = -1;
+    {
+        double nrm = 0;
+#pragma omp parallel for reduction(+ : nrm)
+        for (long i = 0; i < n; i++) {
+            x[i] = xi[i];
+            nrm += creal(B[i] * conj(B[i]));
+        }
+        S->norm = sqrt(nrm);
+    }
+    *nou = 1;
+    return;
+L10:
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        r[i] = B[i] - xr[i];
+        r0s[i] = conj(r[i]);
+        w8[i] = w4[i] = w9[i] = w5[i] = w12[i] = 0;
+    }
+    S->r0rn = zsum(r0s, r, n, 0);
+    *itno = -1;
+L100:
+    *itno += 1;
+    for (long i = 0; i < n; i++) xi[i] = r[i];
+    *nou = 2;
+    return;
+L20: {
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) ar[i] = xr[i];
+    if (*itno == 0) {
+        S->eta = 0;
+        S->beta = 0;
+        const zc an = zsum(r0s, r, n, 0), zn = zsum(ar, r, n, 1), c1 = zsum(ar, ar, n, 1),
+                 c2 = zsum(r0s, ar, n, 0);
+        S->r0rn = an;
+        if (c1 == 0) {
+            *status = -1;
+            *steperr = 2;
+            return;
+        }
+        S->dzeta = zn / c1;
+        if (c2 == 0) {
+            *status = -1;
+            *steperr = 3;
+            return;
+        }
+        S->alpha = an / c2;
+    } else {
+        const zc c1 = zsum(r0s, r, n, 0), c2 = zsum(r0s, ar, n, 0), c3 = zsum(w5, w5, n, 1),
+                 c4 = zsum(ar, r, n, 1), c5 = zsum(ar, w5, n, 1), c6 = zsum(w5, r, n, 1),
+                 c7 = zsum(ar, ar, n, 1), c8 = zsum(r0s, w12, n, 0);
+        if (S->dzeta == 0) {
+            *status = -1;
+            *steperr = 4;
+            return;
+        }
+        if (S->r0rn == 0) {
+            *status = -1;
+            *steperr = 5;
+            return;
+        }
+        S->beta = -S->alpha / S->dzeta * c1 / S->r0rn;
+        const zc c = c2 - S->beta * c8;
+        if (c == 0) {
+            *status = -1;
+            *steperr = 6;
+            return;
+        }
+        S->alpha = c1 / c;
+        const zc d = c7 * c3 - c5 * conj(c5);
+        if (d == 0) {
+            *status = -1;
+            *steperr = 7;
+            return;
+        }
+        S->dzeta = (c3 * c4 - c5 * c6) / d;
+        S->eta = (c7 * c6 - conj(c5) * c4) / d;
+        S->r0rn = c1;
+    }
+    const zc be = S->beta, dz = S->dzeta, et = S->eta;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        w7[i] = ar[i] - be * w12[i];
+        w6[i] = dz * r[i] + et * w9[i];
+        w4[i] = dz * w7[i] + et * (w5[i] - be * w4[i]);
+        xi[i] = w4[i];
+    }
+    *nou = 3;
+    return;
+}
+L30: {
+    const zc al = S->alpha, be = S->beta, dz = S->dzeta, et = S->eta;
+    double res = 0;
+#pragma omp parallel for reduction(+ : res)
+    for (long i = 0; i < n; i++) {
+        aw4[i] = xr[i];
+        w8[i] = r[i] - be * w8[i] - w4[i];
+        w12[i] = w7[i] - aw4[i];
+        w9[i] = w6[i] - al * w4[i];
+        const zc tmp = dz * ar[i] + et * w5[i];
+        w5[i] = tmp - al * aw4[i];
+        x[i] = x[i] + w6[i] + al * w8[i];
+        r[i] = r[i] - tmp - al * w12[i];
+        res += creal(r[i] * conj(r[i]));
+    }
+    if (sqrt(res) / S->norm <= tol) {
+        *status = 1;
+        for (long i = 0; i < n; i++) xi[i] = x[i];
+        *nou = 4;
+        return;
+    }
+}
+L40:
+    if (*itno <= maxit) goto L100;
+    *status = 1;
+    *steperr = 0;
+    for (long i = 0; i < n; i++) xi[i] = x[i];
+    *nou = 4;
+}
+
+/* ------------------------------------------------------------------------- */
+/* CORS reverse communication: cdmlib/cors.f.  Shadow conj(A r0) with         */
+/* unconjugated dots; mat-vecs A r and A d.  Work columns: 0 shadow, 1 r,     */
+/* 2 A r, 3 e, 4 h, 5 d, 6 f, 7 g, 8 q = A d, 9 x.  Past MAXIT the reference  */
+/* returns work column 11, which it never writes; the restatement returns x.  */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    zc alpha, beta, rho, rhoa;
+    double norm;
+} cors_state;
+
+static void cors(zc *xi, zc *xr, const zc *B, long n, int *nou, zc *W, int *itno, int maxit, double tol,
+                 cors_state *S, int *status, int *steperr) {
+#define WK(c) (W + (size_t)(c) * n)
+    zc *rs = WK(0), *r = WK(1), *ar = WK(2), *e = WK(3), *h = WK(4), *d = WK(5), *f = WK(6), *g = WK(7),
+       *q = WK(8), *x = WK(9);
+#undef WK
+    if (*nou == 1) goto L10;
+    if (*nou == 2) goto L20;
+    if (*nou == 3) goto L30;
+    if (*nou == 4) goto L40;
+    *status = 0;
+    *steperr = -1;
+    {
+        double nrm = 0;
+#pragma omp parallel for reduction(+ : nrm)
+        for (long i = 0; i < n; i++) {
+            x[i] = xi[i];
+            nrm += cabs(B[i]) * cabs(B[i]);
+        }
+        S->norm = sqrt(nrm);
+    }
+    *nou = 1;
+    return;
+L10:
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) r[i] = B[i] - xr[i];
+    *itno = -1;
+L100:
+    *itno += 1;
+    for (long i = 0; i < n; i++) xi[i] = r[i];
+    *nou = 2;
+    return;
+L20:
+    if (*itno == 0)
+        for (long i = 0; i < n; i++) rs[i] = conj(xr[i]);
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) ar[i] = xr[i];
+    S->rho = zsum(rs, ar, n, 0);
+    if (S->rho == 0) {
+        *status = -1;
+        *steperr = 1;
+        return;
+    }
+    if (*itno == 0) {
+        for (long i = 0; i < n; i++) {
+            e[i] = r[i];
+            h[i] = ar[i];
+            d[i] = ar[i];
+            xi[i] = d[i];
+        }
+    } else {
+        S->beta = S->rho / S->rhoa;
+        const zc be = S->beta;
+#pragma omp parallel for
+        for (long i = 0; i < n; i++) {
+            e[i] = r[i] + be * f[i];
+            h[i] = ar[i] + be * g[i];
+            d[i] = h[i] + be * (g[i] + be * d[i]);
+            xi[i] = d[i];
+        }
+    }
+    *nou = 3;
+    return;
+L30: {
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) q[i] = xr[i];
+    const zc c = zsum(rs, q, n, 0);
+    if (c == 0) {
+        *status = -1;
+        *steperr = 2;
+        return;
+    }
+    S->alpha = S->rho / c;
+    const zc al = S->alpha;
+    double res = 0;
+#pragma omp parallel for reduction(+ : res)
+    for (long i = 0; i < n; i++) {
+        f[i] = e[i] - al * d[i];
+        g[i] = h[i] - al * q[i];
+        x[i] = x[i] + al * (2.0 * e[i] - al * d[i]);
+        r[i] = r[i] - al * (2.0 * h[i] - al * q[i]);
+        res += cabs(r[i]) * cabs(r[i]);
+    }
+    if (sqrt(res) / S->norm <= tol) {
+        *status = 1;
+        for (long i = 0; i < n; i++) xi[i] = x[i];
+        *nou = 4;
+        return;
+    }
+}
+L40:
+    S->rhoa = S->rho;
+    if (*itno <= maxit) goto L100;
+    *status = 1;
+    for (long i = 0; i < n; i++) xi[i] = x[i];
+    *nou = 4;
+}
+
+/* ------------------------------------------------------------------------- */
+/* GPBiCOR reverse communication: cdmlib/gpbicor.f.  x is the caller's       */
+/* solution array (FFloc).  ITNO counts from 1.  Work columns: 0 r0, 1 p,     */
+/* 2 A r, 3 w4, 4 w5, 5 w6, 6 t, 7 w8, 8 w9, 9 r, 10 z, 11 w12, 12 q, 13 s.   */
+/* The reference keeps q and s in the driver's xi and xr arrays (its driver   */
+/* overwrites both after the return); past MAXIT it returns status 1 without */
+/* setting the solution; the restatement returns x there.                    */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    zc alpha, beta, eta, dzeta, rho, rhoa;
+    double norm;
+} gpbicor_state;
+
+static void gpbicor(zc *xi, zc *xr, const zc *B, zc *x, long n, int *nou, zc *W, int *itno, int maxit,
+                    double tol, gpbicor_state *S, int *status, int *steperr) {
+#define WK(c) (W + (size_t)(c) * n)
+    zc *r0 = WK(0), *p = WK(1), *ar = WK(2), *w4 = WK(3), *w5 = WK(4), *w6 = WK(5), *t = WK(6), *w8 = WK(7),
+       *w9 = WK(8), *r = WK(9), *z = WK(10), *w12 = WK(11), *q = WK(12), *s = WK(13);
+#undef WK
+    if (*nou == 1) goto L10;
+    if (*nou == 2) goto L20;
+    if (*nou == 3) goto L30;
+    if (*nou == 4) goto L40;
+    *status = 0;
+    *steperr = -1;
+    {
+        double nrm = 0;
+#pragma omp parallel for reduction(+ : nrm)
+        for (long i = 0; i < n; i++) {
+            x[i] = xi[i];
+            nrm += creal(B[i] * conj(B[i]));
+        }
+        S->norm = sqrt(nrm);
+    }
+    *nou = 1;
+    return;
+L10:
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        r0[i] = B[i] - xr[i];
+        r[i] = r0[i];
+        z[i] = 0;
+    }
+    *itno = 0;
+L100:
+    *itno += 1;
+    for (long i = 0; i < n; i++) xi[i] = r[i];
+    *nou = 2;
+    return;
+L20:
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) ar[i] = xr[i];
+    S->rho = zsum(r0, ar, n, 1);
+    if (S->rho == 0) {
+        *status = -1;
+        *steperr = 1;
+        return;
+    }
+    if (*itno == 1) {
+        S->beta = 0;
+        for (long i = 0; i < n; i++) {
+            p[i] = r0[i];
+            w4[i] = ar[i];
+            w12[i] = w5[i] = w8[i] = w9[i] = w6[i] = 0;
+            xi[i] = w4[i];
+        }
+    } else {
+        S->beta = S->rho / S->rhoa * S->alpha / S->dzeta;
+        const zc be = S->beta;
+#pragma omp parallel for
+        for (long i = 0; i < n; i++) {
+            w5[i] = w6[i] + be * w4[i];
+            p[i] = r[i] + be * (p[i] - w8[i]);
+            w4[i] = ar[i] + be * (w4[i] - w9[i]);
+            xi[i] = w4[i];
+        }
+    }
+    *nou = 3;
+    return;
+L30: {
+    const zc c = zsum(r0, xr, n, 1);
+    if (c == 0) {
+        *status = -1;
+        *steperr = 2;
+        return;
+    }
+    S->alpha = S->rho / c;
+    const zc al = S->alpha;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        q[i] = w12[i] - r[i] + al * (w4[i] - w5[i]);
+        t[i] = r[i] - al * w4[i];
+        s[i] = ar[i] - al * xr[i];
+    }
+    if (*itno == 1) {
+        S->eta = 0;
+        const zc num = zsum(s, t, n, 1), den = zsum(s, s, n, 1);
+        if (den == 0) {
+            *status = -1;
+            *steperr = 3;
+            return;
+        }
+        S->dzeta = num / den;
+    } else {
+        const zc c1 = zsum(s, s, n, 1), c2 = zsum(q, t, n, 1), c3 = zsum(q, s, n, 1), c4 = zsum(s, t, n, 1),
+                 c5 = zsum(q, q, n, 1);
+        const zc cc = c1 * c5 - c3 * conj(c3);
+        if (cc == 0) {
+            *status = -1;
+            *steperr = 4;
+            return;
+        }
+        S->eta = (c1 * c2 - c3 * c4) / cc;
+        S->dzeta = (c5 * c4 - c2 * conj(c3)) / cc;
+    }
+    const zc be = S->beta, dz = S->dzeta, et = S->eta;
+#pragma omp parallel for
+    for (long i = 0; i < n; i++) {
+        w8[i] = dz * w4[i] + et * (w12[i] - r[i] + be * w8[i]);
+        w9[i] = dz * (ar[i] - s[i]) / al + et * (w6[i] - ar[i] + be * w9[i]);
+        z[i] = dz * r[i] + et * z[i] - al * w8[i];
+    }
+    double res = 0;
+#pragma omp parallel for reduction(+ : res)
+    for (long i = 0; i < n; i++) {
+        r[i] = t[i] - et * q[i] - dz * s[i];
+        res += creal(r[i] * conj(r[i]));
+        x[i] = x[i] + al * p[i] + z[i];
+        w6[i] = s[i];
+        w12[i] = t[i];
+    }
+    if (sqrt(res) / S->norm <= tol) {
+        for (long i = 0; i < n; i++) xi[i] = x[i];
+        *status = 1;
+        *nou = 4;
+        return;
+    }
+}
+L40:
+    S->rhoa = S->rho;
+    if (*itno <= maxit) goto L100;
+    *status = 1;
+    for (long i = 0; i < n; i++) xi[i] = x[i];
+    *nou = 4;
+}
+
+/* ------------------------------------------------------------------------- */
 /* Solver driver: cdmlib/inverserigopt.f:1-107 (GPBICG1), :811-942             */
 /* (QMRBICGSTAB1/2) and cdmlib/inverserig.f (tabdip != NULL).                  */
 /* Returns nstop; infostr receives the reference's messages (space padded to   */
@@ -1276,7 +1670,7 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
     int nou = 0, nstat = 0, steperr = 0;
     zc *xi = (zc *)malloc(sizeof(zc) * n3);
     zc *xr = (zc *)malloc(sizeof(zc) * n3);
-    zc *W = (zc *)calloc((size_t)n3 * 12, sizeof(zc));
+    zc *W = (zc *)calloc((size_t)n3 * 16, sizeof(zc)); /* GPBiCOR uses 14 columns */
     memcpy(xi, FF0, sizeof(zc) * n3);
     *nstop = 0;
     *ncompte = 0;
@@ -1294,12 +1688,15 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
     else if (strncmp(meth, "GPBICGsafe", 10) == 0) kind = 7;
     else if (strncmp(meth, "GPBICGplus", 10) == 0) kind = 9;
     else if (strncmp(meth, "GPBICGAR", 8) == 0) kind = 10;  /* 'GPBICGAR2' too: (1:8) is tested first */
-    else if (strncmp(meth, "BICGSTARPLUS", 12) == 0 || strncmp(meth, "QMRCLA", 6) == 0) kind = 0;
+    else if (strncmp(meth, "BICGSTARPLUS", 12) == 0) kind = 11;
+    else if (strncmp(meth, "QMRCLA", 6) == 0) kind = 0;
     else if (strncmp(meth, "TFQMR", 5) == 0) kind = 6;
     else if (strncmp(meth, "CG   ", 5) == 0) kind = 5;
     else if (strncmp(meth, "BICGSTAB", 8) == 0) kind = 4;
     else if (strncmp(meth, "QMRBICGSTAB1", 12) == 0) kind = 2;
     else if (strncmp(meth, "QMRBICGSTAB2", 12) == 0) kind = 3;
+    else if (strncmp(meth, "GPBICOR", 7) == 0) kind = 13;
+    else if (strncmp(meth, "CORS   ", 7) == 0) kind = 12;
     if (kind == 0) {
         *nstop = 1;
         set_info(infostr, "Iterative method not correct!");
@@ -1312,6 +1709,10 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
     cg_state cs;
     tfqmr_state ts;
     gpsafe_state ss;
+    cors_state rs;
+    gpbicor_state os;
+    memset(&rs, 0, sizeof rs);
+    memset(&os, 0, sizeof os);
     memset(&ts, 0, sizeof ts);
     memset(&ss, 0, sizeof ss);
     memset(&gs, 0, sizeof gs);
@@ -1331,6 +1732,12 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
             zcg(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &cs, &nstat);
         else if (kind == 6)
             tfqmr(FFloc, xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &ts, &nstat, &steperr);
+        else if (kind == 12)
+            cors(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &rs, &nstat, &steperr);
+        else if (kind == 13)
+            gpbicor(xi, xr, FF0, FFloc, n3, &nou, W, nloop, nlim, tol, &os, &nstat, &steperr);
+        else if (kind == 11)
+            bicgstarplus(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &ss, &nstat, &steperr);
         else if (kind == 10)
             gpbicgar(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &ss, &nstat, &steperr);
         else if (kind == 7 || kind == 9)
@@ -1339,7 +1746,7 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
             qmrbicgstab(FFloc, xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &qs,
                         kind == 2 ? 1 : 2, &nstat, &steperr);
         norm = kind == 1 || kind == 8 ? gs.norm : kind == 4 ? bs.norm : kind == 5 ? cs.norm : kind == 6 ? ts.norm
-             : kind == 7 || kind == 9 || kind == 10 ? ss.norm : qs.norm;
+             : kind == 12 ? rs.norm : kind == 13 ? os.norm : kind >= 7 ? ss.norm : qs.norm;
         if (nstat < 0) {
             *nstop = 1;
             /* the TFQMR branch prints it without '!' (inverserigopt.f:609) */
@@ -1372,7 +1779,7 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
         t += creal(xr[i] * conj(xr[i]));
     }
     *tol1 = sqrt(t) / norm;
-    if (kind == 1 || kind >= 6) *nloop += 1;
+    if (kind == 1 || (kind >= 6 && kind != 13)) *nloop += 1;  /* the GPBICOR branch does not */
     free(xi); free(xr); free(W);
     return *nstop;
 }

@@ -296,7 +296,8 @@ def test_anisotropy_only_in_the_tail_matches_oracle(gctx, orc):
     g.close()
 
 
-@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR", "GPBICGsafe", "GPBICG2", "GPBICGplus", "GPBICGAR"])
+@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR", "GPBICGsafe", "GPBICG2", "GPBICGplus", "GPBICGAR",
+                                  "BICGSTARPLUS", "CORS", "GPBICOR"])
 def test_other_methods_match_oracle(gctx, orc, meth):
     """The reference's other Krylov methods (pimzbicgstab.f, zcg.f, tfqmr.f,
     gpbicgsafe.f, gpbicg2.f, gpbicgplus.f, gpbicgar.f) on the sphere

@@ -121,7 +121,8 @@ def test_qmr_agrees_with_gpbicg(orc, meth):
     assert rel(b["FFloc"], a["FFloc"]) < 1e-8
 
 
-@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR", "GPBICGsafe", "GPBICG2", "GPBICGplus", "GPBICGAR"])
+@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR", "GPBICGsafe", "GPBICG2", "GPBICGplus", "GPBICGAR",
+                                  "BICGSTARPLUS", "CORS", "GPBICOR"])
 def test_other_methods_agree_with_gpbicg(orc, meth):
     """The other Krylov methods restated (pimzbicgstab.f, zcg.f, tfqmr.f,
     gpbicgsafe.f, gpbicg2.f, gpbicgplus.f, gpbicgar.f): on the homogeneous
@@ -138,7 +139,7 @@ def test_other_methods_agree_with_gpbicg(orc, meth):
     if meth in ("CG", "TFQMR"):
         assert b["ncompte"] == b["nloop"] + 2 and b["tol1"] < 1e-9
         assert rel(b["FFloc"], a["FFloc"]) < 1e-8
-    elif meth in ("GPBICGsafe", "GPBICG2", "GPBICGplus", "GPBICGAR"):
+    elif meth in ("GPBICGsafe", "GPBICG2", "GPBICGplus", "GPBICGAR", "BICGSTARPLUS", "CORS", "GPBICOR"):
         assert b["ncompte"] == 2 * b["nloop"] + 2 and b["tol1"] < 1e-10
         assert rel(b["FFloc"], a["FFloc"]) < 1e-8
     else:
@@ -149,8 +150,9 @@ def test_other_methods_agree_with_gpbicg(orc, meth):
 
 
 @pytest.mark.parametrize("name,works", [("CG", True), ("CGX", False), ("BICGSTAB", True), ("GPBICGAR2", True),
-                                        ("TFQMR", True), ("BICGSTARPLUS", False), ("QMRCLA", False),
-                                        ("GPBICGsafe", True), ("GPBICG2", True)])
+                                        ("TFQMR", True), ("BICGSTARPLUS", True), ("QMRCLA", False),
+                                        ("GPBICGsafe", True), ("GPBICG2", True),
+                                        ("CORS", True), ("CORSX", False), ("GPBICOR", True)])
 def test_method_prefixes(orc, name, works):
     """methodeit is matched by prefix in the reference's order: 'GPBICGAR2'
     meets the 'GPBICGAR' test first (and runs GPBICGAR), 'CGX' is not 'CG'
