@@ -295,6 +295,11 @@ int ifdda_ctx_synchronize(ifdda_ctx* ctx) {
 void* ifdda_ctx_stream(ifdda_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 int ifdda_green_create(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, ifdda_green** out) {
+    return ifdda_green_create_nquad(ctx, nx, ny, nz, aretecube, k0, 0, out);
+}
+
+int ifdda_green_create_nquad(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, int nquad,
+                             ifdda_green** out) {
     if (!ctx || !out) return 1;
     *out = nullptr;
     std::unique_ptr<ifdda_green> g(new ifdda_green());
@@ -303,7 +308,7 @@ int ifdda_green_create(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube,
     DeviceScope ds(ctx->device);
     AllocStreamScope as(ctx->stream);
     if (ctx->closing) throw EngineError{1, "context already destroyed"};
-    green_build(g->G, nx, ny, nz, aretecube, k0, ctx->stream);
+    green_build(g->G, nx, ny, nz, aretecube, k0, ctx->stream, nquad);
     *out = g.release();
     ctx->live_greens++;
     return 0;

@@ -118,6 +118,7 @@ struct Green {
     int device = 0;
     MvGeom g{};
     double d = 0, k0 = 0;
+    int nquad = 0;
     DevBuf<double2> gc64;
     DevBuf<float2> gc32;
     DevBuf<double2> tw64[3];
@@ -137,7 +138,8 @@ template <> inline MvWork<double>& Green::work<double>() { return w64; }
 
 MvGeom make_geom(int nx, int ny, int nz);
 // builds the spectrum (FP64, plus an FP32 copy) on `st`; throws EngineError
-void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStream_t st);
+// nquad > 0: the cube-averaged tensor at offsets within nquad (calculgreenquadfft.f)
+void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStream_t st, int nquad = 0);
 // full FFTTENSOR arrays (6 x 8N) on the host, expanded from the compressed octant
 void green_export(const Green& G, double2* const out[6], cudaStream_t st);
 

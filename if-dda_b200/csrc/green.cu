@@ -72,8 +72,9 @@ static void launch_gyz(const GreenGeom& gg, const double2* src, double2* d64, fl
     k_green_yz<L, AXIS><<<grid, TT::NT, TT::smem_y, st>>>(gg, src, d64, d32, tw);
 }
 
-void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStream_t st) {
+void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStream_t st, int nquad) {
     if (nx < 1 || ny < 1 || nz < 1) throw EngineError{1, "Green: lattice dimensions must be positive"};
+    if (nquad < 0 || nquad > 16) throw EngineError{1, "Green: nquad must be in [0, 16]"};
     G.g = make_geom(nx, ny, nz);
     if (!fft_length_supported(G.g.X) || !fft_length_supported(G.g.Y) || !fft_length_supported(G.g.Z))
         throw EngineError{1, "FFT size not supported: 2*nx, 2*ny and 2*nz must be compiled lengths"};
@@ -83,7 +84,31 @@ void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStre
     upload_twiddles(G.g.X, G.tw64[0], G.tw32[0], st);
     upload_twiddles(G.g.Y, G.tw64[1], G.tw32[1], st);
     upload_twiddles(G.g.Z, G.tw64[2], G.tw32[2], st);
-    GreenGeom gg{nx, ny, nz, G.g.X, G.g.Y, G.g.Z, d, k0};
+    G.nquad = nquad;
+    GreenGeom gg{nx, ny, nz, G.g.X, G.g.Y, G.g.Z, d, k0, nquad, nullptr};
+    // cube-averaged tensor on the offsets i, j, k >= 0 within nquad
+    DevBuf<double2> quad, qpart;
+    DevBuf<int3> qoffs;
+    if (nquad > 0) {
+        std::vector<int3> offs;
+        for (int k = 0; k <= nquad; k++)
+            for (int j = 0; j <= nquad; j++)
+                for (int i = 0; i <= nquad; i++)
+                    if (i * i + j * j + k * k <= nquad * nquad) offs.push_back(make_int3(i, j, k));
+        const int n1 = nquad + 1, nent = (int)offs.size();
+        quad.ensure((size_t)n1 * n1 * n1 * 6);
+        qpart.ensure((size_t)nent * QUAD_CHUNKS * 6);
+        qoffs.ensure(nent);
+        IFDDA_CUDA(cudaMemsetAsync(quad.p, 0, (size_t)n1 * n1 * n1 * 6 * sizeof(double2), st));
+        IFDDA_CUDA(cudaMemcpyAsync(qoffs.p, offs.data(), nent * sizeof(int3), cudaMemcpyHostToDevice, st));
+        count_launch();
+        k_green_quad_part<<<dim3(nent, QUAD_CHUNKS), QUAD_NT, 0, st>>>(gg, qoffs.p, qpart.p);
+        count_launch();
+        k_green_quad_final<<<(nent + 63) / 64, 64, 0, st>>>(gg, qoffs.p, nent, qpart.p, quad.p);
+        IFDDA_CUDA(cudaGetLastError());
+        gg.quad = quad.p;
+        IFDDA_CUDA(cudaStreamSynchronize(st));  // the offsets live on this stack frame
+    }
     const long W = nx + 1;
     DevBuf<double2> GA, GB;
     GA.ensure((size_t)6 * G.g.Z * G.g.Y * W);

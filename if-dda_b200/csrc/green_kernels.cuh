@@ -11,12 +11,18 @@
 // axis, so the rest of the spectrum is a mirror image (see matvec_kernels.cuh).
 #pragma once
 #include "fft_tile.cuh"
+#include "reduce.cuh"
 
 namespace ifdda {
 
 struct GreenGeom {
     int nx, ny, nz, X, Y, Z;
     double d, k0;
+    // integrated tensor (cdmlib/calculgreenquadfft.f): offsets with
+    // i^2 + j^2 + k^2 <= nquad^2 take quad[((|k| (nquad+1) + |j|) (nquad+1)
+    // + |i|) * 6 + c]; nquad = 0 is the plain tensor everywhere
+    int nquad;
+    const double2* quad;
 };
 
 template <int L> struct GreenTiles {
@@ -55,6 +61,93 @@ __device__ __forceinline__ void green_point(double rx, double ry, double rz, dou
     }
 }
 
+// T at lattice offset (i, j, k): the plain tensor, or inside the nquad sphere
+// the cube-averaged one, whose components keep T's parity (xy odd in x and y,
+// xz in x and z, yz in y and z)
+__device__ __forceinline__ void green_value(const GreenGeom& g, int i, int j, int k, double2 (&t)[6]) {
+    if (g.nquad > 0 && i * i + j * j + k * k <= g.nquad * g.nquad) {
+        const int n1 = g.nquad + 1;
+        const double2* q = g.quad + (((long)abs(k) * n1 + abs(j)) * n1 + abs(i)) * 6;
+        const double sx = i < 0 ? -1.0 : 1.0, sy = j < 0 ? -1.0 : 1.0, sz = k < 0 ? -1.0 : 1.0;
+        const double s[6] = {1.0, sx * sy, sx * sz, 1.0, sy * sz, 1.0};
+#pragma unroll
+        for (int c = 0; c < 6; c++) t[c] = make_double2(s[c] * q[c].x, s[c] * q[c].y);
+        return;
+    }
+    green_point(i * g.d, j * g.d, k * g.d, g.k0, t);
+}
+
+// Cube-averaged tensor, cdmlib/propaesplibreintsim.f: Simpson rule with 128
+// steps per axis over the source cube [-d/2, d/2]^3, 129^3 nodes per offset.
+// Stage 1: block (entry, chunk) sums the nodes of its chunk in a fixed order.
+constexpr int QUAD_STEPS = 128, QUAD_NODES = 129 * 129 * 129, QUAD_CHUNKS = 64, QUAD_NT = 256;
+__global__ void __launch_bounds__(QUAD_NT) k_green_quad_part(const GreenGeom g, const int3* __restrict__ offs,
+                                                             double2* __restrict__ part) {
+    const int3 o = offs[blockIdx.x];
+    const double pas = g.d / QUAD_STEPS, h = g.d / 2;
+    double2 acc[6];
+#pragma unroll
+    for (int c = 0; c < 6; c++) acc[c] = make_double2(0, 0);
+    const int per = (QUAD_NODES + QUAD_CHUNKS - 1) / QUAD_CHUNKS;
+    const int n0 = blockIdx.y * per, n1 = min(QUAD_NODES, n0 + per);
+    for (int n = n0 + threadIdx.x; n < n1; n += QUAD_NT) {
+        const int a = n / (129 * 129), b = (n / 129) % 129, c = n % 129;
+        const auto wt = [](int m) { return m == 0 || m == QUAD_STEPS ? 1.0 : (m & 1 ? 4.0 : 2.0); };
+        const double ww = wt(a) * wt(b) * wt(c);
+        double2 t[6];
+        green_point(-h + pas * a - o.x * g.d, -h + pas * b - o.y * g.d, -h + pas * c - o.z * g.d, g.k0, t);
+#pragma unroll
+        for (int q = 0; q < 6; q++) acc[q] = make_double2(acc[q].x + t[q].x * ww, acc[q].y + t[q].y * ww);
+    }
+    __shared__ double2 scratch[6 * 32];
+    block_sum<QUAD_NT, 6>(acc, scratch);
+    if (threadIdx.x == 0) {
+        double2* p = part + ((long)blockIdx.x * QUAD_CHUNKS + blockIdx.y) * 6;
+#pragma unroll
+        for (int q = 0; q < 6; q++) p[q] = acc[q];
+    }
+}
+
+// Stage 2: one thread per entry sums the chunks in order and scales; points
+// closer than d/10 give 0, points beyond one wavelength the plain tensor.
+__global__ void k_green_quad_final(const GreenGeom g, const int3* __restrict__ offs, int nent,
+                                   const double2* __restrict__ part, double2* __restrict__ quad) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nent) return;
+    const int3 o = offs[e];
+    const int n1 = g.nquad + 1;
+    double2* out = quad + (((long)o.z * n1 + o.y) * n1 + o.x) * 6;
+    const double rab = g.d * sqrt((double)(o.x * o.x + o.y * o.y + o.z * o.z));
+    const double lambda = 2.0 * 3.14159265358979323846 / g.k0;
+    if (rab <= 0.1 * g.d) {
+#pragma unroll
+        for (int q = 0; q < 6; q++) out[q] = make_double2(0, 0);
+        return;
+    }
+    if (rab >= lambda) {
+        double2 t[6];
+        green_point(o.x * g.d, o.y * g.d, o.z * g.d, g.k0, t);
+#pragma unroll
+        for (int q = 0; q < 6; q++) out[q] = t[q];
+        return;
+    }
+    double2 acc[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) acc[q] = make_double2(0, 0);
+    for (int ch = 0; ch < QUAD_CHUNKS; ch++)
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            const double2 v = part[((long)e * QUAD_CHUNKS + ch) * 6 + q];
+            acc[q] = make_double2(acc[q].x + v.x, acc[q].y + v.y);
+        }
+    const double pas = g.d / QUAD_STEPS;
+    const double tmp = pas / 3.0 * pas / 3.0 * pas / 3.0 / g.d / g.d / g.d;
+    const double fx = o.x == 0 ? 0.0 : 1.0, fy = o.y == 0 ? 0.0 : 1.0, fz = o.z == 0 ? 0.0 : 1.0;
+    const double f[6] = {1.0, fx * fy, fx * fz, 1.0, fy * fz, 1.0};
+#pragma unroll
+    for (int q = 0; q < 6; q++) out[q] = make_double2(acc[q].x * tmp * f[q], acc[q].y * tmp * f[q]);
+}
+
 template <int L>
 __global__ void __launch_bounds__(GreenTiles<L>::NT) k_green_x(const GreenGeom g, double2* __restrict__ GA,
                                                                const double2* __restrict__ twx) {
@@ -75,7 +168,7 @@ __global__ void __launch_bounds__(GreenTiles<L>::NT) k_green_x(const GreenGeom g
         if (jl < nl && ii != g.nx && jj != g.ny && kk != g.nz) {
             const int i = ii > g.nx ? ii - g.X : ii;
             const int j = jj > g.ny ? jj - g.Y : jj;
-            green_point(i * g.d, j * g.d, k * g.d, g.k0, t);
+            green_value(g, i, j, k, t);
         } else {
 #pragma unroll
             for (int q = 0; q < 6; q++) t[q] = make_double2(0, 0);

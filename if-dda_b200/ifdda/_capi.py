@@ -42,6 +42,8 @@ SIGNATURES = {
     "ifdda_ctx_synchronize": (C.c_int, [_vp]),
     "ifdda_ctx_stream": (_vp, [_vp]),
     "ifdda_green_create": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.POINTER(_vp)]),
+    "ifdda_green_create_nquad": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
+                                           C.POINTER(_vp)]),
     "ifdda_green_destroy": (C.c_int, [_vp]),
     "ifdda_green_release_workspace": (C.c_int, [_vp]),
     "ifdda_green_export": (C.c_int, [_vp] + [_vp] * 6),

@@ -75,8 +75,8 @@ class Context:
         if rc != 0:
             raise IfddaError(self.last_error() or f"ifdda call failed ({rc})")
 
-    def green(self, nx, ny, nz, aretecube, k0) -> "GreenSpectrum":
-        return GreenSpectrum(self, nx, ny, nz, aretecube, k0)
+    def green(self, nx, ny, nz, aretecube, k0, nquad=0) -> "GreenSpectrum":
+        return GreenSpectrum(self, nx, ny, nz, aretecube, k0, nquad)
 
     # -- post-step ------------------------------------------------------
     def local_macro(self, nbsphere, nmax, epsilon, FFloc, aretecube, k0) -> np.ndarray:
@@ -116,13 +116,15 @@ class GreenSpectrum:
     """Device-resident Green spectrum of one lattice (greencalculfft) plus the
     solver workspace that uses it."""
 
-    def __init__(self, ctx: Context, nx, ny, nz, aretecube, k0):
+    def __init__(self, ctx: Context, nx, ny, nz, aretecube, k0, nquad=0):
         self.ctx = ctx
         self.lib = ctx.lib
         self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         self.aretecube, self.k0 = float(aretecube), float(k0)
+        self.nquad = int(nquad)
         h = C.c_void_p()
-        rc = self.lib.ifdda_green_create(ctx.h, self.nx, self.ny, self.nz, self.aretecube, self.k0, C.byref(h))
+        rc = self.lib.ifdda_green_create_nquad(ctx.h, self.nx, self.ny, self.nz, self.aretecube, self.k0, self.nquad,
+                                               C.byref(h))
         if rc != 0:
             raise IfddaError(ctx.last_error() or "ifdda_green_create failed")
         self.h = h

@@ -8,7 +8,7 @@ field (:1172-1187), Green spectrum (:1518-1546), solve (:1555-1597), local and
 macroscopic fields (:2497-2655), cross sections (:2717-2778) -- and returns
 the reference's outputs in a dict together with nstop/infostr.  Only the
 options on the rigorous-solve path are implemented (trope 'iso', plane waves,
-nrig = 0, nquad = 0); anything else returns nstop = 1 with a message.
+nrig = 0, 0 <= nquad <= 16); anything else returns nstop = 1 with a message.
 """
 from __future__ import annotations
 
@@ -43,8 +43,8 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
         return _fail("only isotropic objects are handled by the GPU drop-in")
     if nrig != 0:
         return _fail("only the rigorous solve (nrig = 0) is handled by the GPU drop-in")
-    if nquad != 0:
-        return _fail("only nquad = 0 is handled by the GPU drop-in")
+    if not 0 <= nquad <= 16:
+        return _fail("nquad must be in [0, 16]")
     if beam != "pwavelinear":
         return _fail("Cross section only with plane wave" if nsection else "only plane waves are handled")
     if tolinit < 1e-12:
@@ -91,7 +91,7 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
                              [p for _, p, _ in inc], [q for _, _, q in inc])
         # ---- Green spectrum and solve (cdmlib.f:1518-1597) ---------------
         try:
-            g = ctx.green(ob.nx, ob.ny, ob.nz, ob.aretecube, k0)
+            g = ctx.green(ob.nx, ob.ny, ob.nz, ob.aretecube, k0, nquad)
         except IfddaError as e:
             return _fail(str(e)[:64])
         r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0 if len(inc) > 1 else ff0[0], methodeit, tolinit,

@@ -60,6 +60,14 @@ void* ifdda_ctx_stream(ifdda_ctx* ctx);
    the free-space dyadic on the (2nx,2ny,2nz) circulant grid, FFT sign +1.
    aretecube in metres, k0 in 1/m.  The spectrum stays on the device. */
 int ifdda_green_create(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, ifdda_green** out);
+/* The same with the integrated Green tensor (nquad = 1..16, 0 = plain):
+   replaces greencalculquadfft (cdmlib/calculgreenquadfft.f, called at
+   cdmlib/cdmlib.f:1532-1536 when nquad != 0) with propaesplibreintsim
+   (cdmlib/propaesplibreintsim.f): at lattice offsets i^2+j^2+k^2 <= nquad^2
+   the tensor averaged over the source cube (Simpson rule, 128 steps per axis),
+   zero at the origin, the plain tensor beyond one wavelength. */
+int ifdda_green_create_nquad(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, int nquad,
+                             ifdda_green** out);
 int ifdda_green_destroy(ifdda_green* g);
 /* Frees the solver and mat-vec workspaces held by g (they are re-created on
    the next solve); the spectrum stays.  For callers that cache many spectra.

@@ -201,6 +201,92 @@ void orc_greencalculfft(int nx, int ny, int nz, double d, double k0, zc *G6) {
 }
 
 /* ------------------------------------------------------------------------- */
+/* Green tensor averaged over the source cube: cdmlib/propaesplibreintsim.f.  */
+/* Zero when the points are closer than d/10, the plain tensor beyond lim    */
+/* wavelengths, otherwise a Simpson rule with 128 steps per axis over the     */
+/* cube of side d centred on (x,y,z); the off-diagonal terms are zeroed       */
+/* along the axes on which the two points coincide (closer than d/10).        */
+/* out is column-major 3x3.                                                   */
+/* ------------------------------------------------------------------------- */
+void orc_propaesplibreintsim(double x, double y, double z, double x0, double y0, double z0,
+                             double k0, double d, double lim, zc *out) {
+    const double pi = acos(-1.0), lambda = 2.0 * pi / k0, dm = d * 0.1;
+    const double rab = sqrt((x - x0) * (x - x0) + (y - y0) * (y - y0) + (z - z0) * (z - z0));
+    if (rab <= dm) {
+        for (int q = 0; q < 9; q++) out[q] = 0;
+        return;
+    }
+    if (rab >= lim * lambda) {
+        orc_propa_espace_libre(x, y, z, x0, y0, z0, k0, out);
+        return;
+    }
+    const int nstep = 128;
+    double w[129];
+    w[0] = w[nstep] = 1.0;
+    for (int i = 1; i < nstep; i++) w[i] = i % 2 ? 4.0 : 2.0;
+    const double pas = d / nstep, ax = x - d / 2, ay = y - d / 2, az = z - d / 2;
+    double acc[12] = {0};
+#pragma omp parallel for reduction(+ : acc[:12]) schedule(static)
+    for (int i = 0; i <= nstep; i++)
+        for (int j = 0; j <= nstep; j++)
+            for (int k = 0; k <= nstep; k++) {
+                zc t[9];
+                orc_propa_espace_libre(ax + pas * i, ay + pas * j, az + pas * k, x0, y0, z0, k0, t);
+                const double ww = w[i] * w[j] * w[k];
+                const int qs[6] = {0, 3, 6, 4, 7, 8};  /* xx xy xz yy yz zz */
+                for (int q = 0; q < 6; q++) {
+                    acc[2 * q] += creal(t[qs[q]]) * ww;
+                    acc[2 * q + 1] += cimag(t[qs[q]]) * ww;
+                }
+            }
+    const double tmp = pas / 3.0 * pas / 3.0 * pas / 3.0 / d / d / d;
+    const double fx = fabs(x - x0) <= dm ? 0.0 : 1.0, fy = fabs(y - y0) <= dm ? 0.0 : 1.0,
+                 fz = fabs(z - z0) <= dm ? 0.0 : 1.0;
+    zc v[6];
+    for (int q = 0; q < 6; q++) v[q] = (acc[2 * q] + I * acc[2 * q + 1]) * tmp;
+    v[1] *= fx * fy;
+    v[2] *= fx * fz;
+    v[4] *= fy * fz;
+    out[0] = v[0];
+    out[3] = out[1] = v[1];
+    out[6] = out[2] = v[2];
+    out[4] = v[3];
+    out[7] = out[5] = v[4];
+    out[8] = v[5];
+}
+
+/* Green spectrum with the integrated tensor at the offsets i^2+j^2+k^2 <=     */
+/* nquad^2: cdmlib/calculgreenquadfft.f (lim = 1 wavelength).                 */
+void orc_greencalculquadfft(int nx, int ny, int nz, int nquad, double d, double k0, zc *G6) {
+    int nx2 = 2 * nx, ny2 = 2 * ny, nz2 = 2 * nz;
+    long M = (long)nx2 * ny2 * nz2;
+    for (long idx = 0; idx < M; idx++) {
+        int ii = (int)(idx % nx2);
+        int jj = (int)((idx / nx2) % ny2);
+        int kk = (int)(idx / ((long)nx2 * ny2));
+        if (ii == nx || jj == ny || kk == nz) {
+            for (int c = 0; c < 6; c++) G6[c * M + idx] = 0;
+            continue;
+        }
+        int i = ii > nx ? ii - nx2 : ii;
+        int j = jj > ny ? jj - ny2 : jj;
+        int k = kk > nz ? kk - nz2 : kk;
+        zc t[9];
+        if (nquad != 0 && i * i + j * j + k * k <= nquad * nquad)
+            orc_propaesplibreintsim(0, 0, 0, i * d, j * d, k * d, k0, d, 1.0, t);
+        else
+            orc_propa_espace_libre(0, 0, 0, i * d, j * d, k * d, k0, t);
+        G6[0 * M + idx] = t[0 + 3 * 0];
+        G6[1 * M + idx] = t[0 + 3 * 1];
+        G6[2 * M + idx] = t[0 + 3 * 2];
+        G6[3 * M + idx] = t[1 + 3 * 1];
+        G6[4 * M + idx] = t[1 + 3 * 2];
+        G6[5 * M + idx] = t[2 + 3 * 2];
+    }
+    for (int c = 0; c < 6; c++) orc_fft3d(G6 + c * M, nx2, ny2, nz2, +1);
+}
+
+/* ------------------------------------------------------------------------- */
 /* FFT mat-vec: FFB <- FFB - (1/M) IFFT(G~ . FFT(pad(FFX)))                   */
 /* cdmlib/produitfftmatvectopt.f:3-121 (tabdip == NULL, full box) and         */
 /* cdmlib/produitfftmatvect3.f:2-127 (tabdip != NULL: lattice site s holds    */

@@ -84,6 +84,23 @@ def greencalculfft(nx, ny, nz, d, k0) -> np.ndarray:
     return g.reshape(6, 2 * nz, 2 * ny, 2 * nx)
 
 
+def greencalculquadfft(nx, ny, nz, nquad, d, k0) -> np.ndarray:
+    """greencalculfft with the cube-averaged tensor at offsets within nquad."""
+    M = 8 * nx * ny * nz
+    g = np.zeros(6 * M, np.complex128)
+    lib().orc_greencalculquadfft(C.c_int(nx), C.c_int(ny), C.c_int(nz), C.c_int(nquad), C.c_double(d),
+                                 C.c_double(k0), _p(g))
+    return g.reshape(6, 2 * nz, 2 * ny, 2 * nx)
+
+
+def propaesplibreintsim(x, y, z, x0, y0, z0, k0, d, lim=1.0) -> np.ndarray:
+    """Cube-averaged tensor, 3x3 (row a, column b)."""
+    out = np.zeros(9, np.complex128)
+    lib().orc_propaesplibreintsim(C.c_double(x), C.c_double(y), C.c_double(z), C.c_double(x0), C.c_double(y0),
+                                  C.c_double(z0), C.c_double(k0), C.c_double(d), C.c_double(lim), _p(out))
+    return out.reshape(3, 3).T
+
+
 def matvec(G6, nx, ny, nz, FFX, FFB, tabdip=None) -> np.ndarray:
     """FFB - (1/M) IFFT(G~ FFT(pad FFX)); returns the new FFB."""
     g = _z(G6)

@@ -334,3 +334,28 @@ def test_other_methods_mixed_precision(gctx, orc, meth):
     assert r.tol1[0] < 1e-4
     assert rel(r.FFloc, tight["FFloc"]) < 1e-3
     g.close()
+
+
+@pytest.mark.parametrize("nquad", [1, 2])
+def test_integrated_green_spectrum_matches_oracle(gctx, orc, nquad):
+    """Spectrum with the cube-averaged tensor inside nquad (calculgreenquadfft.f)."""
+    nx, ny, nz = 6, 5, 4
+    d, k0 = 11e-9, 2 * math.pi / 550e-9
+    g = gctx.green(nx, ny, nz, d, k0, nquad=nquad)
+    got = g.export()
+    ref = orc.greencalculquadfft(nx, ny, nz, nquad, d, k0)
+    for c in range(6):
+        assert np.abs(got[c] - ref[c]).max() <= 1e-11 * np.abs(ref[c]).max(), c
+    g.close()
+
+
+def test_solve_with_integrated_green_matches_oracle(gctx, orc):
+    ob, k0, E0, ff0, _ = _c1_inputs(orc, nnnr=10)
+    G = orc.greencalculquadfft(10, 10, 10, 2, ob.aretecube, k0)
+    ref = orc.inverserig(G, 10, 10, 10, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-6, tabdip=ob.tabdip)
+    g = gctx.green(10, 10, 10, ob.aretecube, k0, nquad=2)
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-6, tabdip=ob.tabdip)
+    assert r.nstop == ref["nstop"] == 0
+    assert int(r.nloop[0]) == ref["nloop"] and int(r.ncompte[0]) == ref["ncompte"]
+    assert rel(r.FFloc, ref["FFloc"]) < 1e-7
+    g.close()

@@ -258,3 +258,29 @@ def test_cube_matches_oracle(orc):
     a = objects.cube(200e-9, 2.0 + 0.3j, 8, k0, "CM")
     b = orc.object_cube(200e-9, 2.0 + 0.3j, 8, k0, "CM")
     assert np.array_equal(a.xs, b.xs) and rel(a.polarisa, b.polarisa) < 1e-15
+
+
+def test_integrated_green_tensor_properties(orc):
+    """propaesplibreintsim.f restated: zero at the origin, the plain tensor
+    beyond lim wavelengths, symmetric, off-diagonal terms zero where the
+    points share a coordinate, and close to the plain tensor a few cells
+    away (the cube average of a smooth field)."""
+    k0, d = 2 * math.pi / 600e-9, 10e-9
+    assert np.all(orc.propaesplibreintsim(0, 0, 0, 0, 0, 0, k0, d) == 0)
+    far = orc.propaesplibreintsim(0, 0, 0, 0, 0, 70 * d, k0, d)  # 700 nm > one wavelength
+    assert np.array_equal(far, orc.propaesplibreintsim(0, 0, 0, 0, 0, 70 * d, k0, d, lim=0.0))
+    t = orc.propaesplibreintsim(0, 0, 0, d, 2 * d, 0, k0, d)
+    assert np.allclose(t, t.T, rtol=0, atol=1e-12 * np.abs(t).max())
+    assert t[0, 2] == 0 and t[1, 2] == 0 and t[0, 1] != 0
+    plain = orc.propaesplibreintsim(0, 0, 0, 4 * d, 3 * d, 2 * d, k0, d, lim=0.0)
+    avg = orc.propaesplibreintsim(0, 0, 0, 4 * d, 3 * d, 2 * d, k0, d)
+    assert rel(avg, plain) < 0.02
+
+
+def test_quad_spectrum_without_quad_is_the_plain_one(orc):
+    k0, d = 2 * math.pi / 550e-9, 11e-9
+    a = orc.greencalculquadfft(4, 3, 2, 0, d, k0)
+    b = orc.greencalculfft(4, 3, 2, d, k0)
+    assert np.array_equal(a, b)
+    c = orc.greencalculquadfft(4, 3, 2, 1, d, k0)
+    assert not np.array_equal(c, b) and rel(c, b) < 0.5
