@@ -7,8 +7,9 @@ validation (:317-471), object (:661-805), padded grid (:1141-1148), incident
 field (:1172-1187), Green spectrum (:1518-1546), solve (:1555-1597), local and
 macroscopic fields (:2497-2655), cross sections (:2717-2778) -- and returns
 the reference's outputs in a dict together with nstop/infostr.  Only the
-options on the rigorous-solve path are implemented (trope 'iso', plane waves,
-nrig = 0, 0 <= nquad <= 16); anything else returns nstop = 1 with a message.
+options on the rigorous-solve path are implemented (trope 'iso' for every
+object here, trope 'ani' for the sphere and the cube, plane waves, nrig = 0,
+0 <= nquad <= 16); anything else returns nstop = 1 with a message.
 """
 from __future__ import annotations
 
@@ -29,7 +30,7 @@ def _fail(msg, **extra):
 
 
 def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, rayons=None, epss=None,
-           nx=None, ny=None, nz=None, aretecube=None, lc=None, hc=None, ng=0, positions=None, eps_site=None,
+           nx=None, ny=None, nz=None, aretecube=None, epsani=None, lc=None, hc=None, ng=0, positions=None, eps_site=None,
            beam="pwavelinear", theta=0.0, phi=0.0, pp=1.0, incidences=None, P0=1.0, w0=None,
            tolinit=1e-4, methodeit="GPBICG1", polarizability="RR", trope="iso", nproche=0, nrig=0, nquad=0,
            nlocal=1, nmacro=1, nsection=1, precision=0, ctx: Context | None = None, device=0):
@@ -39,8 +40,16 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
     the full box (inverserigopt).  precision: 0 plain FP64, 1 FP32 inner
     iterations with FP64 refinement."""
     lam = wavelength * 1e-9
-    if trope != "iso":
-        return _fail("only isotropic objects are handled by the GPU drop-in")
+    if trope not in ("iso", "ani"):
+        return _fail(f"trope {trope!r} is neither 'iso' nor 'ani'")
+    if trope == "ani":
+        # cdmlib.f:597-611
+        if epsani is None or float(np.sum(np.abs(np.asarray(epsani, np.complex128)))) == 0.0:
+            return _fail("No relative permittivity given")
+        if polarizability not in ("RR", "CM"):
+            return _fail("Polarizability should be CM or RR with anisotropy")
+        if object not in ("sphere", "cube"):
+            return _fail(f"anisotropic {object!r} not handled by the GPU drop-in")
     if nrig != 0:
         return _fail("only the rigorous solve (nrig = 0) is handled by the GPU drop-in")
     if not 0 <= nquad <= 16:
@@ -59,10 +68,12 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
     inside = nproche - 1 == -1  # cdmlib.f:627 decrements the GUI value
     # ---- object (cdmlib.f:661-805) -------------------------------------
     try:
+        ani = epsani if trope == "ani" else None
+        e_iso = complex(eps) if eps is not None else 0j
         if object == "sphere":
-            ob = objects.sphere(rayon * 1e-9, complex(eps), nnnr, k0, polarizability, na=-1 if inside else 0)
+            ob = objects.sphere(rayon * 1e-9, e_iso, nnnr, k0, polarizability, na=-1 if inside else 0, epsani=ani)
         elif object == "cube":
-            ob = objects.cube(side * 1e-9, complex(eps), nnnr, k0, polarizability)
+            ob = objects.cube(side * 1e-9, e_iso, nnnr, k0, polarizability, epsani=ani)
         elif object == "inhomocuboid2":
             ob = objects.inhomocuboid(nx, ny, nz, aretecube * 1e-9, complex(eps), lc * 1e-9, hc, ng, k0,
                                       polarizability)
@@ -77,9 +88,13 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
         return _fail(str(e))
     if ob.nbsphere == 0:
         return _fail("No dipole in the object!")
-    # mesh size check (cdmlib.f:994-999)
-    eps_max = np.max(np.abs(np.sqrt(ob.eps))) if len(ob.eps) else 1.0
-    if ob.aretecube > 2.5 * lam / 10.0 / eps_max:
+    # mesh size check (cdmlib.f:994-999); for an anisotropic object the
+    # reference tests the scalar eps argument, so none given passes
+    if trope == "ani":
+        eps_max = abs(np.sqrt(complex(eps))) if eps is not None else 0.0
+    else:
+        eps_max = np.max(np.abs(np.sqrt(ob.eps))) if len(ob.eps) else 1.0
+    if eps_max > 0 and ob.aretecube > 2.5 * lam / 10.0 / eps_max:
         return _fail("Meshsize larger than lambda/4!")
     own = ctx is None
     ctx = ctx or Context(device)

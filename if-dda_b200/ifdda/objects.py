@@ -3,8 +3,9 @@
 One-time host work that cdmlib does before the solve (cdmlib/cdmlib.f:661-805),
 restated with numpy so the GPU path gets its inputs without the oracle:
   poladiff          cdmlib/polarisabilite.f:1-62
-  sphere            cdmlib/objectsphere.f:94-195          (na = -1 or 0)
-  cube              cdmlib/objectcube.f:60-130
+  polaepstens       cdmlib/polaepstens.f:1-122 (anisotropic permittivity tensor)
+  sphere            cdmlib/objectsphere.f:94-195          (na = -1 or 0; trope 'ani')
+  cube              cdmlib/objectcube.f:60-130            (trope 'ani')
   inhomocuboid      cdmlib/objectparainhomonxnynz.f:85-237 (+ SUNIF, cdmlib/random.f:19-56)
   concentric        cdmlib/objectsphereconcentric.f:76-230
   arbitrary         cdmlib/objectarbitrary.f:81-157 (arrays instead of a file)
@@ -12,7 +13,8 @@ All lengths are in metres (the reference multiplies its nm inputs by 1e-9).
 A DipoleObject carries the reference's arrays: xs, ys, zs (nbsphere),
 tabdip (nx*ny*nz, 1-based, 0 = empty), polarisa and epsilon as (nmax,3,3)
 column-major flattened, plus ``alpha`` and ``eps`` (one isotropic value per
-dipole).
+dipole) or, for an anisotropic object, ``alpha_t`` and ``eps_t`` (the 3x3
+tensors every dipole of the object shares).
 """
 from __future__ import annotations
 
@@ -37,26 +39,36 @@ class DipoleObject:
     alpha: np.ndarray   # isotropic polarisability per dipole
     eps: np.ndarray     # isotropic permittivity per dipole
     inside_only: bool
+    alpha_t: np.ndarray = None  # anisotropic object: 3x3 polarisability (row a, column b)
+    eps_t: np.ndarray = None    # anisotropic object: 3x3 permittivity
+    # full box with an anisotropic object: which sites hold a dipole of it
+    occupied: np.ndarray = None
 
     @property
     def nmax(self) -> int:
         return self.nx * self.ny * self.nz
 
-    def _tensor(self, diag: np.ndarray) -> np.ndarray:
+    def _tensor(self, diag: np.ndarray, full: np.ndarray = None, vacuum: complex = 0.0) -> np.ndarray:
         n = self.nmax
         t = np.zeros((3, 3, n), np.complex128)
-        for a in range(3):
-            t[a, a, : self.nbsphere] = diag
+        if full is None:
+            for a in range(3):
+                t[a, a, : self.nbsphere] = diag
+        else:
+            on = np.ones(self.nbsphere, bool) if self.occupied is None else self.occupied
+            for a in range(3):
+                for b in range(3):
+                    t[a, b, : self.nbsphere] = np.where(on, full[a, b], vacuum if a == b else 0.0)
         # (nmax,3,3) column-major: (n,a,b) at n + nmax*(a + 3b)  ->  t[b, a, n]
         return np.ascontiguousarray(t.transpose(1, 0, 2)).reshape(-1)
 
     @property
     def polarisa(self) -> np.ndarray:
-        return self._tensor(self.alpha)
+        return self._tensor(self.alpha, self.alpha_t, 0.0)
 
     @property
     def epsilon(self) -> np.ndarray:
-        return self._tensor(self.eps)
+        return self._tensor(self.eps, self.eps_t, 1.0)
 
     @property
     def tabdip_or_none(self):
@@ -99,9 +111,56 @@ def poladiff(aretecube: float, eps, k0: float, methode: str, eps0: float = 1.0, 
     raise ValueError(f"incorrect method {methode!r}")
 
 
+def polaepstens(aretecube: float, epsani, k0: float, methode: str, eps0: float = 1.0, dis: int = 1,
+                inv: int = 1) -> np.ndarray:
+    """Polarisability tensor of a cube of anisotropic permittivity epsani (3x3)
+    (polaepstens.f:1-122): alpha0 = V (eps - eps0 I) (eps + 2 eps0 I)^-1,
+    CM: alpha0 eps0, RR: (I - 2/3 i k^3 alpha0)^-1 alpha0 eps0; inv = -1
+    returns the inverse.  Only CM and RR exist for a tensor."""
+    e = np.asarray(epsani, np.complex128).reshape(3, 3)
+    pi = math.acos(-1.0)
+    k03 = k0 ** 3 * math.sqrt(eps0) ** 3
+    if dis == 0:
+        volume = aretecube ** 3
+    elif dis == 1:
+        volume = (aretecube * (0.75 / pi) ** (1.0 / 3.0)) ** 3
+    else:
+        raise ValueError("Bad value of dis")
+    eye = np.eye(3)
+    a0 = (e - eps0 * eye) @ np.linalg.inv(e + 2.0 * eps0 * eye) * volume
+    m = methode[:2]
+    if m == "CM":
+        a = a0 * eps0
+    elif m == "RR":
+        a = np.linalg.inv(eye - 2.0 / 3.0 * 1j * k03 * a0) @ a0 * eps0
+    else:
+        raise ValueError(f"incorrect method for the polarizability {methode!r}")
+    return np.linalg.inv(a) if inv == -1 else a
+
+
 def _lattice(n1, n2, n3):
     k, j, i = np.meshgrid(np.arange(n3), np.arange(n2), np.arange(n1), indexing="ij")
     return i.ravel(), j.ravel(), k.ravel()
+
+
+def _finish_ani(nx, ny, nz, d, x, y, z, keep, epsani, k0, methode, inside_only) -> DipoleObject:
+    """Anisotropic object (trope = 'ani'): every dipole gets polaepstens of
+    epsani with dis = 1 (objectsphere.f:129-135); 'PS' is refused there."""
+    if methode[:2] == "PS":
+        raise ValueError("anisotrope with PS")
+    e = np.asarray(epsani, np.complex128).reshape(3, 3)
+    at = polaepstens(d, e, k0, methode, dis=1)
+    N = nx * ny * nz
+    if inside_only:
+        tab = np.zeros(N, np.int32)
+        idx = np.nonzero(keep)[0]
+        tab[idx] = np.arange(1, len(idx) + 1, dtype=np.int32)
+        nb = len(idx)
+        return DipoleObject(nx, ny, nz, d, nb, N, x[idx].copy(), y[idx].copy(), z[idx].copy(), tab,
+                            np.full(nb, at[0, 0]), np.full(nb, e[0, 0]), True, at, e)
+    tab = np.arange(1, N + 1, dtype=np.int32)
+    return DipoleObject(nx, ny, nz, d, N, N, x.copy(), y.copy(), z.copy(), tab, np.where(keep, at[0, 0], 0.0),
+                        np.where(keep, e[0, 0], 1.0 + 0j), False, at, e, keep.copy())
 
 
 def _finish(nx, ny, nz, d, x, y, z, keep, eps_site, k0, methode, inside_only) -> DipoleObject:
@@ -121,8 +180,9 @@ def _finish(nx, ny, nz, d, x, y, z, keep, eps_site, k0, methode, inside_only) ->
     return DipoleObject(nx, ny, nz, d, N, N, x.copy(), y.copy(), z.copy(), tab, alpha, eps, False)
 
 
-def sphere(rayon, eps, nnnr, k0, methode="RR", na=-1) -> DipoleObject:
-    """objetsphere: d = 2R/nnnr, dipole where |r| < R (objectsphere.f:94-113)."""
+def sphere(rayon, eps, nnnr, k0, methode="RR", na=-1, epsani=None) -> DipoleObject:
+    """objetsphere: d = 2R/nnnr, dipole where |r| < R (objectsphere.f:94-113);
+    epsani (3x3) makes it anisotropic (trope = 'ani')."""
     if rayon == 0.0:
         raise ValueError("object sphere: radius=0!")
     d = 2.0 * rayon / nnnr
@@ -131,11 +191,14 @@ def sphere(rayon, eps, nnnr, k0, methode="RR", na=-1) -> DipoleObject:
     y = -rayon + d * (j + 1 - 0.5)
     z = -rayon + d * (k + 1 - 0.5)
     keep = np.sqrt(x * x + y * y + z * z) < rayon
+    if epsani is not None:
+        return _finish_ani(nnnr, nnnr, nnnr, d, x, y, z, keep, epsani, k0, methode, na == -1)
     return _finish(nnnr, nnnr, nnnr, d, x, y, z, keep, eps, k0, methode, na == -1)
 
 
-def cube(side, eps, nnnr, k0, methode="RR") -> DipoleObject:
-    """objetcube: full box, d = side/nnnr (objectcube.f:91-117)."""
+def cube(side, eps, nnnr, k0, methode="RR", epsani=None) -> DipoleObject:
+    """objetcube: full box, d = side/nnnr (objectcube.f:91-117); epsani (3x3)
+    makes it anisotropic."""
     if side == 0.0:
         raise ValueError("object cube: side=0!")
     d = side / nnnr
@@ -145,6 +208,8 @@ def cube(side, eps, nnnr, k0, methode="RR") -> DipoleObject:
     y = (j + 1) * d - xc
     z = (k + 1) * d - xc
     keep = np.ones(nnnr ** 3, bool)
+    if epsani is not None:
+        return _finish_ani(nnnr, nnnr, nnnr, d, x, y, z, keep, epsani, k0, methode, False)
     return _finish(nnnr, nnnr, nnnr, d, x, y, z, keep, eps, k0, methode, False)
 
 

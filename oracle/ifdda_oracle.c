@@ -1986,6 +1986,56 @@ int orc_local_macro(zc *Eloc, zc *Em, const zc *eps, double d, double k0, int ns
     return 0;
 }
 
+/* ------------------------------------------------------------------------- */
+/* Anisotropic polarisability: cdmlib/polaepstens.f:1-122.  eps is a          */
+/* column-major 3x3 permittivity; alpha0 = V (eps - eps0 I)(eps + 2 eps0 I)^-1 */
+/* (:33-62), CM: alpha0 eps0 (:64-69), RR: (I - 2/3 i k^3 alpha0)^-1 alpha0    */
+/* eps0 (:70-99); inv = -1 inverts the result (:106-118).  Returns 1 on an    */
+/* unknown method, a bad dis or a singular matrix (the reference stops).      */
+/* ------------------------------------------------------------------------- */
+int orc_polaepstens(double rayon1, const zc *eps, double eps0, double k0, int dis,
+                    const char *methode, int inv, zc *out) {
+    const double pi = acos(-1.0);
+    double indice = sqrt(eps0);
+    double k03 = k0 * k0 * k0 * indice * indice * indice;
+    double rayon = rayon1, volume;
+    if (dis == 0) volume = rayon * rayon * rayon;
+    else if (dis == 1) {
+        rayon = rayon * pow(0.75 / pi, 1.0 / 3.0);
+        volume = rayon * rayon * rayon;
+    } else return 1;
+    zc m[9], m1[9], mi[9], a0[9], r[9];
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+            m[a + 3 * b] = eps[a + 3 * b] + (a == b ? 2.0 * eps0 : 0.0);
+            m1[a + 3 * b] = eps[a + 3 * b] - (a == b ? eps0 : 0.0);
+        }
+    if (inv33(m, mi)) return 1;
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+            zc acc = 0;
+            for (int c = 0; c < 3; c++) acc += m1[a + 3 * c] * mi[c + 3 * b];
+            a0[a + 3 * b] = acc * volume;
+        }
+    if (!strncmp(methode, "CM", 2)) {
+        for (int q = 0; q < 9; q++) r[q] = a0[q] * eps0;
+    } else if (!strncmp(methode, "RR", 2)) {
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++)
+                m[a + 3 * b] = -2.0 / 3.0 * I * k03 * a0[a + 3 * b] + (a == b ? 1.0 : 0.0);
+        if (inv33(m, mi)) return 1;
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) {
+                zc acc = 0;
+                for (int c = 0; c < 3; c++) acc += mi[a + 3 * c] * a0[c + 3 * b] * eps0;
+                r[a + 3 * b] = acc;
+            }
+    } else return 1;
+    if (inv == -1) return inv33(r, out);
+    for (int q = 0; q < 9; q++) out[q] = r[q];
+    return 0;
+}
+
 /* macroscopic field of every dipole (cdmlib/cdmlib.f:2595-2655), eps in the
    (nmax,3,3) column-major layout */
 int orc_macro_all(int nbsphere, int nmax, const zc *epsilon, const zc *FFloc, double d,
@@ -2185,19 +2235,41 @@ static void set_iso(zc *pol, zc *eps, long nmax, long n, zc a, zc e) {
     }
 }
 
-/* objetsphere (cdmlib/objectsphere.f:94-195), na = -1 (inside only) or 0 */
-int orc_object_sphere(double rayon, zc eps, int nnnr, int na, double k0, const char *methode,
-                      int nmax, double *xs, double *ys, double *zs, int *tabdip, zc *pol,
-                      zc *epsilon, int *nbsphere, int *ndipole, double *aretecube) {
+/* one dipole of an anisotropic object: epsilon(n,:,:) = epsani,
+   polarisa(n,:,:) = polaeps (objectsphere.f:128-135) */
+static void set_full(zc *pol, zc *eps, long nmax, long n, const zc *a9, const zc *e9) {
+    for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+            pol[n + nmax * a + 3 * nmax * b] = a9[a + 3 * b];
+            eps[n + nmax * a + 3 * nmax * b] = e9[a + 3 * b];
+        }
+}
+
+/* a dipole of the object: isotropic (epsani NULL) or anisotropic */
+static void set_obj(zc *pol, zc *eps, long nmax, long n, zc a, zc e, const zc *a9, const zc *epsani) {
+    if (epsani) set_full(pol, eps, nmax, n, a9, epsani);
+    else set_iso(pol, eps, nmax, n, a, e);
+}
+
+/* objetsphere (cdmlib/objectsphere.f:94-195), na = -1 (inside only) or 0;
+   epsani (column-major 3x3) non-NULL for trope = 'ani', where 'PS' is refused
+   (:64-67) and every dipole gets polaepstens with dis = 1, inv = 1 */
+static int sphere_impl(double rayon, zc eps, const zc *epsani, int nnnr, int na, double k0,
+                       const char *methode, int nmax, double *xs, double *ys, double *zs,
+                       int *tabdip, zc *pol, zc *epsilon, int *nbsphere, int *ndipole,
+                       double *aretecube) {
     if (rayon == 0.0) return 1;
+    if (epsani && !strncmp(methode, "PS", 2)) return 1;
     long cap = (long)nmax;
     memset(pol, 0, sizeof(zc) * 9 * cap);
     memset(epsilon, 0, sizeof(zc) * 9 * cap);
     double d = 2.0 * rayon / nnnr;
     *aretecube = d;
     int nb = 0, nd = 0;
-    zc a;
-    if (orc_poladiff(d, eps, 1.0, k0, 1, methode, &a)) return 1;
+    zc a = 0, a9[9];
+    if (epsani) {
+        if (orc_polaepstens(d, epsani, 1.0, k0, 1, methode, 1, a9)) return 1;
+    } else if (orc_poladiff(d, eps, 1.0, k0, 1, methode, &a)) return 1;
     for (int i = 1; i <= nnnr; i++)
         for (int j = 1; j <= nnnr; j++)
             for (int k = 1; k <= nnnr; k++) {
@@ -2212,12 +2284,12 @@ int orc_object_sphere(double rayon, zc eps, int nnnr, int na, double k0, const c
                     nb++;
                     tabdip[nd - 1] = nb;
                     xs[nb - 1] = x; ys[nb - 1] = y; zs[nb - 1] = z;
-                    set_iso(pol, epsilon, cap, nb - 1, a, eps);
+                    set_obj(pol, epsilon, cap, nb - 1, a, eps, a9, epsani);
                 } else {
                     nb++;
                     tabdip[nd - 1] = nb;
                     xs[nb - 1] = x; ys[nb - 1] = y; zs[nb - 1] = z;
-                    if (inside) set_iso(pol, epsilon, cap, nb - 1, a, eps);
+                    if (inside) set_obj(pol, epsilon, cap, nb - 1, a, eps, a9, epsani);
                     else set_iso(pol, epsilon, cap, nb - 1, 0, 1.0);
                 }
             }
@@ -2226,10 +2298,27 @@ int orc_object_sphere(double rayon, zc eps, int nnnr, int na, double k0, const c
     return 0;
 }
 
-/* objetcube (cdmlib/objectcube.f:60-130): full box of nnnr^3 dipoles */
-int orc_object_cube(double side, zc eps, int nnnr, double k0, const char *methode, int nmax,
-                    double *xs, double *ys, double *zs, int *tabdip, zc *pol, zc *epsilon,
-                    int *nbsphere, int *ndipole, double *aretecube) {
+int orc_object_sphere(double rayon, zc eps, int nnnr, int na, double k0, const char *methode,
+                      int nmax, double *xs, double *ys, double *zs, int *tabdip, zc *pol,
+                      zc *epsilon, int *nbsphere, int *ndipole, double *aretecube) {
+    return sphere_impl(rayon, eps, NULL, nnnr, na, k0, methode, nmax, xs, ys, zs, tabdip, pol,
+                       epsilon, nbsphere, ndipole, aretecube);
+}
+
+int orc_object_sphere_ani(double rayon, const zc *epsani, int nnnr, int na, double k0,
+                          const char *methode, int nmax, double *xs, double *ys, double *zs,
+                          int *tabdip, zc *pol, zc *epsilon, int *nbsphere, int *ndipole,
+                          double *aretecube) {
+    return sphere_impl(rayon, 0, epsani, nnnr, na, k0, methode, nmax, xs, ys, zs, tabdip, pol,
+                       epsilon, nbsphere, ndipole, aretecube);
+}
+
+/* objetcube (cdmlib/objectcube.f:60-130): full box of nnnr^3 dipoles;
+   epsani non-NULL for trope = 'ani' (:118-135) */
+static int cube_impl(double side, zc eps, const zc *epsani, int nnnr, double k0,
+                     const char *methode, int nmax, double *xs, double *ys, double *zs,
+                     int *tabdip, zc *pol, zc *epsilon, int *nbsphere, int *ndipole,
+                     double *aretecube) {
     if (side == 0.0) return 1;
     long cap = nmax;
     memset(pol, 0, sizeof(zc) * 9 * cap);
@@ -2237,8 +2326,10 @@ int orc_object_cube(double side, zc eps, int nnnr, double k0, const char *method
     double d = side / nnnr;
     *aretecube = d;
     double xc = (side + d) / 2.0;
-    zc a;
-    if (orc_poladiff(d, eps, 1.0, k0, 1, methode, &a)) return 1;
+    zc a = 0, a9[9];
+    if (epsani) {
+        if (orc_polaepstens(d, epsani, 1.0, k0, 1, methode, 1, a9)) return 1;
+    } else if (orc_poladiff(d, eps, 1.0, k0, 1, methode, &a)) return 1;
     int nb = 0;
     for (int i = 1; i <= nnnr; i++)
         for (int j = 1; j <= nnnr; j++)
@@ -2248,11 +2339,25 @@ int orc_object_cube(double side, zc eps, int nnnr, double k0, const char *method
                 xs[nb - 1] = k * d - xc;
                 ys[nb - 1] = j * d - xc;
                 zs[nb - 1] = i * d - xc;
-                set_iso(pol, epsilon, cap, nb - 1, a, eps);
+                set_obj(pol, epsilon, cap, nb - 1, a, eps, a9, epsani);
             }
     *nbsphere = nb;
     *ndipole = nb;
     return 0;
+}
+
+int orc_object_cube(double side, zc eps, int nnnr, double k0, const char *methode, int nmax,
+                    double *xs, double *ys, double *zs, int *tabdip, zc *pol, zc *epsilon,
+                    int *nbsphere, int *ndipole, double *aretecube) {
+    return cube_impl(side, eps, NULL, nnnr, k0, methode, nmax, xs, ys, zs, tabdip, pol, epsilon,
+                     nbsphere, ndipole, aretecube);
+}
+
+int orc_object_cube_ani(double side, const zc *epsani, int nnnr, double k0, const char *methode,
+                        int nmax, double *xs, double *ys, double *zs, int *tabdip, zc *pol,
+                        zc *epsilon, int *nbsphere, int *ndipole, double *aretecube) {
+    return cube_impl(side, 0, epsani, nnnr, k0, methode, nmax, xs, ys, zs, tabdip, pol, epsilon,
+                     nbsphere, ndipole, aretecube);
 }
 
 /* objetparainhomonxnynz (cdmlib/objectparainhomonxnynz.f:85-237): cuboid with

@@ -266,10 +266,31 @@ def _pack(nx, ny, nz, d, nb, nd, xs, ys, zs, tab, pol, eps, nmax):
                         polarisa=pol, epsilon=eps, nmax=nmax)
 
 
-def object_sphere(rayon, eps, nnnr, na, k0, methode):
+def polaepstens(rayon, epsani, k0, methode, eps0=1.0, dis=1, inv=1) -> np.ndarray:
+    """polaepstens (cdmlib/polaepstens.f:1-122): 3x3 polarisability of a cube
+    of anisotropic permittivity epsani (3x3, [row, column])."""
+    e = _z(np.asarray(epsani, np.complex128).T.ravel())  # column-major
+    out = np.zeros(9, np.complex128)
+    f = lib().orc_polaepstens
+    f.argtypes = [C.c_double, C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_char_p, C.c_int, C.c_void_p]
+    f.restype = C.c_int
+    if f(rayon, _p(e), eps0, k0, dis, methode.encode(), inv, _p(out)):
+        raise ValueError("polaepstens: bad method, dis or singular matrix")
+    return out.reshape(3, 3).T.copy()
+
+
+def object_sphere(rayon, eps, nnnr, na, k0, methode, epsani=None):
     nmax = nnnr ** 3
     xs, ys, zs, tab, pol, ep = _alloc(nmax)
     nb, nd, d = C.c_int(0), C.c_int(0), C.c_double(0)
+    if epsani is not None:
+        ea = _z(np.asarray(epsani, np.complex128).T.ravel())
+        rc = lib().orc_object_sphere_ani(C.c_double(rayon), _p(ea), C.c_int(nnnr), C.c_int(na), C.c_double(k0),
+                                         methode.encode(), C.c_int(nmax), _p(xs), _p(ys), _p(zs), _p(tab),
+                                         _p(pol), _p(ep), C.byref(nb), C.byref(nd), C.byref(d))
+        if rc:
+            raise ValueError("object sphere")
+        return _pack(nnnr, nnnr, nnnr, d.value, nb.value, nd.value, xs, ys, zs, tab, pol, ep, nmax)
     f = lib().orc_object_sphere
     f.argtypes = [C.c_double, _ZC, C.c_int, C.c_int, C.c_double, C.c_char_p, C.c_int] + \
         [C.c_void_p] * 6 + [c_int_p, c_int_p, c_double_p]
@@ -281,10 +302,18 @@ def object_sphere(rayon, eps, nnnr, na, k0, methode):
     return _pack(nnnr, nnnr, nnnr, d.value, nb.value, nd.value, xs, ys, zs, tab, pol, ep, nmax)
 
 
-def object_cube(side, eps, nnnr, k0, methode):
+def object_cube(side, eps, nnnr, k0, methode, epsani=None):
     nmax = nnnr ** 3
     xs, ys, zs, tab, pol, ep = _alloc(nmax)
     nb, nd, d = C.c_int(0), C.c_int(0), C.c_double(0)
+    if epsani is not None:
+        ea = _z(np.asarray(epsani, np.complex128).T.ravel())
+        rc = lib().orc_object_cube_ani(C.c_double(side), _p(ea), C.c_int(nnnr), C.c_double(k0), methode.encode(),
+                                       C.c_int(nmax), _p(xs), _p(ys), _p(zs), _p(tab), _p(pol), _p(ep),
+                                       C.byref(nb), C.byref(nd), C.byref(d))
+        if rc:
+            raise ValueError("object cube")
+        return _pack(nnnr, nnnr, nnnr, d.value, nb.value, nd.value, xs, ys, zs, tab, pol, ep, nmax)
     f = lib().orc_object_cube
     f.argtypes = [C.c_double, _ZC, C.c_int, C.c_double, C.c_char_p, C.c_int] + \
         [C.c_void_p] * 6 + [c_int_p, c_int_p, c_double_p]

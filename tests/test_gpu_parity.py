@@ -231,6 +231,35 @@ def test_cdmlib_driver_config1_matches_oracle(orc):
     assert abs(out["Cext"][0] - mie_ext) / mie_ext < 0.06
 
 
+@pytest.mark.parametrize("nproche", [0, 1])
+def test_cdmlib_anisotropic_sphere_matches_oracle(orc, nproche):
+    """trope = 'ani' (polaepstens.f, objectsphere.f:128-135): every dipole
+    carries the full 3x3 tensor; inside-only (nproche 0) and full box
+    (nproche 1) against the oracle pipeline with the oracle's own object."""
+    from ifdda.cdmlib import cdmlib
+    ani = np.array([[2.25, 0.1j, 0.0], [-0.1j, 2.5 + 0.02j, 0.05], [0.0, 0.05, 3.0]])
+    out = cdmlib(wavelength=632.8, object="sphere", rayon=100.0, eps=2.25, nnnr=16, tolinit=1e-6,
+                 methodeit="GPBICG1", polarizability="RR", trope="ani", epsani=ani, nproche=nproche, theta=20.0,
+                 phi=30.0, pp=0.5, P0=1.0, w0=6328.0)
+    assert out["nstop"] == 0, out["infostr"]
+    k0 = 2 * math.pi / 632.8e-9
+    na = -1 if nproche == 0 else 0
+    ob = orc.object_sphere(100e-9, 0, 16, na, k0, "RR", epsani=ani)
+    assert out["nbsphere"] == ob.nbsphere
+    E0, _ = orc.irradiance(1.0, 6328e-9)
+    ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 0.5, 0, 20.0, 30.0)
+    G = orc.greencalculfft(ob.nx, ob.ny, ob.nz, ob.aretecube, k0)
+    ref = orc.inverserig(G, 16, 16, 16, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-6,
+                         tabdip=ob.tabdip if na == -1 else None)
+    assert ref["nstop"] == 0
+    assert rel(out["localfield"], ref["FFloc"]) < 1e-9
+    assert rel(out["FF"], ref["FF"]) < 1e-9
+    em = orc.local_macro_all(ob.nbsphere, ob.nmax, ob.epsilon, ref["FFloc"], ob.aretecube, k0)
+    assert rel(out["macroscopicfield"][0], em) < 1e-9
+    ce, ca = orc.cross_sections(ff0, ref["FF"], ref["FFloc"], k0, E0 ** 2)
+    assert abs(out["Cext"][0] - ce) <= 1e-9 * abs(ce)
+    assert abs(out["Cabs"][0] - ca) <= 1e-8 * abs(ce)
+
 
 def test_context_closed_before_its_spectrum():
     """A context destroyed while a spectrum made on it is alive (finalisers

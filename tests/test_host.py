@@ -4,6 +4,7 @@ import os
 import socket
 import sys
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -23,6 +24,15 @@ def test_cdmlib_driver_rejects_like_the_reference():
     assert cdmlib(wavelength=632.8, object="torus", nnnr=8)["nstop"] == 1
     assert cdmlib(wavelength=632.8, object="sphere", rayon=100.0, eps=2.25, nnnr=8, nlocal=0, nmacro=0,
                   nsection=0)["infostr"] == "No calculation requested!"
+    # anisotropic objects (cdmlib.f:597-611)
+    ani = [[2.25, 0, 0], [0, 2.5, 0], [0, 0, 3.0]]
+    assert cdmlib(wavelength=632.8, object="sphere", rayon=100.0, nnnr=8, trope="ani",
+                  epsani=np.zeros((3, 3)))["infostr"] == "No relative permittivity given"
+    assert cdmlib(wavelength=632.8, object="sphere", rayon=100.0, nnnr=8, trope="ani", epsani=ani,
+                  polarizability="LA")["infostr"] == "Polarizability should be CM or RR with anisotropy"
+    assert cdmlib(wavelength=632.8, object="concentricsphere", nnnr=8, trope="ani", epsani=ani)["nstop"] == 1
+    assert cdmlib(wavelength=632.8, object="sphere", rayon=1000.0, eps=2.25, nnnr=4, trope="ani",
+                  epsani=ani)["infostr"] == "Meshsize larger than lambda/4!"
 
 
 def _free_port():

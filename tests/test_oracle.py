@@ -284,3 +284,60 @@ def test_quad_spectrum_without_quad_is_the_plain_one(orc):
     assert np.array_equal(a, b)
     c = orc.greencalculquadfft(4, 3, 2, 1, d, k0)
     assert not np.array_equal(c, b) and rel(c, b) < 0.5
+
+
+# ---- anisotropic permittivity (polaepstens.f, trope = 'ani') -------------
+EPSANI = np.array([[2.25, 0.1j, 0.0], [-0.1j, 2.5 + 0.02j, 0.05], [0.0, 0.05, 3.0]])
+
+
+@pytest.mark.parametrize("meth", ["CM", "RR"])
+def test_polaepstens_matches_oracle(orc, meth):
+    from ifdda import objects
+    k0 = 2 * math.pi / 500e-9
+    for dis in (0, 1):
+        a = objects.polaepstens(10e-9, EPSANI, k0, meth, dis=dis)
+        b = orc.polaepstens(10e-9, EPSANI, k0, meth, dis=dis)
+        assert rel(a, b) < 1e-14
+        # inv = -1 returns the inverse tensor
+        ai = orc.polaepstens(10e-9, EPSANI, k0, meth, dis=dis, inv=-1)
+        assert rel(ai @ b, np.eye(3)) < 1e-12
+        assert rel(objects.polaepstens(10e-9, EPSANI, k0, meth, dis=dis, inv=-1), ai) < 1e-13
+
+
+@pytest.mark.parametrize("meth", ["CM", "RR"])
+def test_polaepstens_of_a_scalar_is_poladiff(orc, meth):
+    """eps * I gives poladiff's value on the diagonal and zeros elsewhere."""
+    k0 = 2 * math.pi / 500e-9
+    for eps in (2.25, 3.0 + 0.01j, 12 + 1j):
+        t = orc.polaepstens(10e-9, eps * np.eye(3), k0, meth)
+        p = orc.poladiff(10e-9, eps, k0, meth)
+        assert np.allclose(t, p * np.eye(3), rtol=1e-13, atol=1e-13 * abs(p))
+
+
+def test_polaepstens_rejects_other_methods(orc):
+    from ifdda import objects
+    k0 = 2 * math.pi / 500e-9
+    for meth in ("LA", "GB", "PS"):
+        with pytest.raises(ValueError):
+            orc.polaepstens(10e-9, EPSANI, k0, meth)
+        with pytest.raises(ValueError):
+            objects.polaepstens(10e-9, EPSANI, k0, meth)
+
+
+def test_anisotropic_objects_match_oracle(orc):
+    from ifdda import objects
+    k0 = 2 * math.pi / 632.8e-9
+    for na in (-1, 0):
+        a = objects.sphere(100e-9, 0, 10, k0, "RR", na=na, epsani=EPSANI)
+        b = orc.object_sphere(100e-9, 0, 10, na, k0, "RR", epsani=EPSANI)
+        assert a.nbsphere == b.nbsphere and np.array_equal(a.tabdip, b.tabdip)
+        assert np.array_equal(a.xs, b.xs) and np.array_equal(a.zs, b.zs)
+        assert rel(a.polarisa, b.polarisa) < 1e-15
+        assert rel(a.epsilon, b.epsilon) < 1e-15
+    a = objects.cube(200e-9, 0, 8, k0, "CM", epsani=EPSANI)
+    b = orc.object_cube(200e-9, 0, 8, k0, "CM", epsani=EPSANI)
+    assert rel(a.polarisa, b.polarisa) < 1e-15 and rel(a.epsilon, b.epsilon) < 1e-15
+    with pytest.raises(ValueError, match="anisotrope with PS"):
+        objects.sphere(100e-9, 0, 10, k0, "PS", epsani=EPSANI)
+    with pytest.raises(ValueError):
+        orc.object_sphere(100e-9, 0, 10, -1, k0, "PS", epsani=EPSANI)
