@@ -8,6 +8,7 @@
 #include <string>
 #include "../../include/ifdda_gpu.h"
 #include "post.cuh"
+#include "microscope.cuh"
 
 using namespace ifdda;
 
@@ -143,9 +144,12 @@ SolveSpec make_spec(int method, int nrhs, int nb, double tol, const ifdda_solve_
 }
 
 // Runs a (batched) solve whose inputs are already on the device.
+// check_tol: report tol1 >= tol as "Converge do not reach!" (cdmlib.f:1586-1591;
+// the microscopes call the solver without that check).
 int solve_device(ifdda_green* g, int nrhs, int nb, int nmax, const int* tab_dev, const double2* alpha_dev, int amode,
                  const double2* ff0_dev, const char* methodeit, double tol, double2* ff_dev, double2* loc_dev,
-                 double* tol1, int* nloop, int* ncompte, int* nstop, char* infostr, const ifdda_solve_options* opt) {
+                 double* tol1, int* nloop, int* ncompte, int* nstop, char* infostr, const ifdda_solve_options* opt,
+                 bool check_tol = true) {
     ifdda_ctx* ctx = g->ctx;
     const int method = method_code(methodeit);
     if (method == 0) {
@@ -196,7 +200,7 @@ int solve_device(ifdda_green* g, int nrhs, int nb, int nmax, const int* tab_dev,
             // the TFQMR branch of the reference words it without '!'
             // (cdmlib/inverserigopt.f:609)
             msg = method == 6 ? "Problem to solve Ax=b" : "Problem to solve Ax=b!";
-        } else if (!(res[r].tol1 < tol)) {
+        } else if (check_tol && !(res[r].tol1 < tol)) {
             rc = 1;
             msg = "Converge do not reach!";
         }
@@ -640,6 +644,222 @@ int ifdda_incident_planewaves(ifdda_ctx* ctx, int nbsphere, const double* xs, co
     if (bad) throw EngineError{1, "problem in plance incident wave"};
     return 0;
     IFDDA_GUARD_END(ctx, nullptr)
+}
+
+int ifdda_microscope(ifdda_green* g, const double* xs, const double* ys, const double* zs,
+                     const ifdda_dcmplx* polarisa, const char* methodeit, double tol,
+                     const ifdda_microscope_options* mo, double* image, double* xy, double* kxy, int* ninc,
+                     double* kxinc, double* kyinc, double* tol1, int* nloop, int* ncompte, int* nstop,
+                     char* infostr, const ifdda_solve_options* opt) {
+    if (!g || !xs || !ys || !zs || !polarisa || !mo || !image || !ninc) {
+        if (nstop) *nstop = 1;
+        set_info(infostr, "invalid argument");
+        return 1;
+    }
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(g->ctx->device);
+    AllocStreamScope as(g->ctx->stream);
+    cudaStream_t st = g->ctx->stream;
+    const MvGeom& geo = g->G.g;
+    const int nx = geo.nx, ny = geo.ny, nz = geo.nz, N = geo.N, n = mo->nfft2d;
+    auto fail = [&](const char* msg) {
+        if (nstop) *nstop = 1;
+        set_info(infostr, msg);
+        return 1;
+    };
+    if (mo->ntypemic != 1 && mo->ntypemic != 2) return fail("ntypemic must be 1 (bright field) or 2 (dark field)");
+    if (!image_length_supported(n)) return fail("nfft2d not supported: a power of two from 32 to 4096");
+    if (nx > n || ny > n) return fail("nfft2d smaller than the object");
+    const double pi = 3.14159265358979323846;
+    const double k0 = g->G.k0, d = g->G.d;
+    const double numaper = mo->numaper * k0, numaperinc = mo->numaperinc, numaperk = k0 * numaperinc;
+    // microsbf.f:83-88 (the reference tests numaper, not numaperinc, for <= 0)
+    if (numaperinc >= 1.0 || numaper <= 0.0) return fail("NA inc strictly between 0 and 1");
+    // step of the incidences (microsbf.f:91-135): the object's extent sets deltakm
+    double xmax = -1e300, xmin = 1e300, ymax = -1e300, ymin = 1e300;
+    for (int i = 0; i < N; i++) {
+        xmax = std::max(xmax, xs[i]);
+        xmin = std::min(xmin, xs[i]);
+        ymax = std::max(ymax, ys[i]);
+        ymin = std::min(ymin, ys[i]);
+    }
+    const double deltakm = pi / std::max(xmax - xmin, ymax - ymin);
+    const double dkx = 2.0 * pi / (d * (double)n), dky = dkx;
+    if (dkx >= numaperk) return fail("In FFT lens nfft2d too small:Increase size of FFT 1");
+    int imul = (int)(deltakm / dkx);
+    if (imul == 0) return fail("In FFT lens nfft2d too small:Increase size of FFT 2");
+    double deltak;
+    int imaxinc;
+    for (;;) {
+        deltak = dkx * (double)imul;
+        imaxinc = (int)std::lround(k0 / deltak) + 1;
+        if (imaxinc > 3) break;
+        if (--imul == 0) return fail("In FFT lens nfft2d too small:Increase size of FFT 3");
+    }
+    // incidences of one polarisation: the grid inside the condenser's NA
+    // (microsbf.f:161-171) or the ring at its NA (microsdf.f:160-162, 204-212)
+    std::vector<double> kxi, kyi;
+    if (mo->ntypemic == 1) {
+        for (int id = -imaxinc; id <= imaxinc; id++)
+            for (int jd = -imaxinc; jd <= imaxinc; jd++) {
+                const double kx = id * deltak, ky = jd * deltak;
+                if (kx * kx + ky * ky <= numaperk * numaperk) {
+                    kxi.push_back(kx);
+                    kyi.push_back(ky);
+                }
+            }
+        if (deltak >= numaperk) return fail("In FFT lens nfft2d too small");
+    } else {
+        const double deltatheta = deltak / k0 * numaperinc;
+        const int m = std::max((int)(2.0 * pi / deltatheta) + 1, 8);
+        for (int id = 0; id < m; id++) {
+            const double phi = (double)id * 2.0 * pi / (double)m;
+            kxi.push_back(std::cos(phi) * k0 * numaperinc);
+            kyi.push_back(std::sin(phi) * k0 * numaperinc);
+        }
+    }
+    const int cnt = (int)kxi.size(), cap = *ninc;
+    *ninc = cnt;
+    for (int q = 0; q < cnt && q < cap; q++) {
+        if (kxinc) kxinc[q] = kxi[q] / k0;
+        if (kyinc) kyinc[q] = kyi[q] / k0;
+    }
+    // power shared by the 2 cnt illuminations (microsbf.f:206-207, irradiance.f)
+    const double c = 299792458.0, eps0 = 1.0 / (c * c * 4.0 * pi * 1e-7);
+    const double irra = mo->P0 / (double)(2 * cnt) / (mo->w0 * mo->w0 * pi);
+    const double2 E0 = make_double2(std::sqrt(2.0 * irra / c / eps0), 0.0);
+    // every incidence in the reference's order: s then p, then the list;
+    // grid index of its specular wave (deltakroutine.f; microsbf.f passes the
+    // incidence step, microsdf.f the pupil step)
+    const int total = 2 * cnt;
+    std::vector<double> a1(total), a2(total), ppv(total);
+    std::vector<int> ikv(total), jkv(total);
+    for (int t = 0; t < total; t++) {
+        const int q = t % cnt;
+        a1[t] = kxi[q];
+        a2[t] = kyi[q];
+        ppv[t] = t < cnt ? 0.0 : 1.0;
+        const double sx = mo->ntypemic == 1 ? deltak : dkx, sy = mo->ntypemic == 1 ? deltak : dky;
+        int i = (int)std::lround(a1[t] / sx), j = (int)std::lround(a2[t] / sy);
+        const double kx = sx * i, ky = sy * j;
+        if (!(kx * kx + ky * ky <= k0 * k0)) {
+            i = (int)(a1[t] / sx);
+            j = (int)(a2[t] / sy);
+        }
+        ikv[t] = i;
+        jkv[t] = j;
+    }
+    // FFT lens (diffractefft2dlens.f:29-73)
+    MicGeom m{};
+    m.nx = nx;
+    m.ny = ny;
+    m.nz = nz;
+    m.n = n;
+    m.imax = (int)std::lround(k0 / dkx) + 1;
+    m.ntypemic = mo->ntypemic;
+    m.k0 = k0;
+    m.dkx = dkx;
+    m.dky = dky;
+    m.numaper = numaper;
+    m.var1 = (xs[0] + (double)(n / 2) * d) * dkx;
+    m.var2 = (ys[0] + (double)(n / 2) * d) * dky;
+    m.zlens = mo->zlens;
+    m.gross = mo->gross;
+    const int S = 2 * m.imax + 1;
+    const char* lens_error = dkx >= numaper ? "In FFT lens nfft2d too small"
+                             : S > n        ? "In FFT diffraction for lens nfft2d too small!"
+                             : S < 7        ? "In FFT diffract nfft2d too small"
+                                            : nullptr;
+    const int B = std::max(1, std::min(total, mo->batch > 0 ? mo->batch : 32));
+    const long n3 = 3L * N;
+    DevBuf<double> dx, dy, dz, zpl, d1, d2, dpp, img;
+    DevBuf<int> dbeam, dik, djk;
+    DevBuf<double2> pol, alpha, ff0, ff, loc, tw, Q, Ed, F, T;
+    dx.ensure(N);
+    dy.ensure(N);
+    dz.ensure(N);
+    IFDDA_CUDA(cudaMemcpyAsync(dx.p, xs, N * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(dy.p, ys, N * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(dz.p, zs, N * sizeof(double), cudaMemcpyHostToDevice, st));
+    // the object on the full box: one alpha per dipole when isotropic
+    pol.ensure((size_t)9 * N);
+    alpha.ensure(N);
+    IFDDA_CUDA(cudaMemcpyAsync(pol.p, polarisa, (size_t)9 * N * sizeof(double2), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemsetAsync(g->ctx->flag.p, 0, sizeof(int), st));
+    pola_compact_dev(pol.p, N, N, alpha.p, g->ctx->flag.p, st);
+    int aniso = 0;
+    IFDDA_CUDA(cudaMemcpyAsync(&aniso, g->ctx->flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    // z of each lattice plane, the roots of unity of the pupil transforms
+    std::vector<double> zp(nz);
+    for (int k = 0; k < nz; k++) zp[k] = zs[(long)nx * ny * k];
+    std::vector<double2> twh(n);
+    for (int j = 0; j < n; j++) {
+        const double a = 2.0 * pi * (double)j / (double)n;
+        twh[j] = make_double2(std::cos(a), std::sin(a));
+        if (4 * j == n) twh[j] = make_double2(0.0, 1.0);
+        if (2 * j == n) twh[j] = make_double2(-1.0, 0.0);
+        if (4 * j == 3 * n) twh[j] = make_double2(0.0, -1.0);
+        if (j == 0) twh[j] = make_double2(1.0, 0.0);
+    }
+    zpl.ensure(nz);
+    tw.ensure(n);
+    IFDDA_CUDA(cudaMemcpyAsync(zpl.p, zp.data(), nz * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(tw.p, twh.data(), n * sizeof(double2), cudaMemcpyHostToDevice, st));
+    std::vector<int> beam(B, 1);
+    d1.ensure(B);
+    d2.ensure(B);
+    dpp.ensure(B);
+    dbeam.ensure(B);
+    dik.ensure(B);
+    djk.ensure(B);
+    IFDDA_CUDA(cudaMemcpyAsync(dbeam.p, beam.data(), B * sizeof(int), cudaMemcpyHostToDevice, st));
+    ff0.ensure(n3 * B);
+    ff.ensure(n3 * B);
+    loc.ensure(n3 * B);
+    Q.ensure((size_t)B * nz * ny * S * 3);
+    Ed.ensure((size_t)B * S * S * 3);
+    F.ensure((size_t)B * 6 * S * S);
+    T.ensure((size_t)B * 6 * S * n);
+    img.ensure((size_t)6 * n * n);
+    IFDDA_CUDA(cudaMemsetAsync(img.p, 0, (size_t)6 * n * n * sizeof(double), st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    const double2* al = aniso ? pol.p : alpha.p;
+    const int amode = aniso ? ALPHA_FULL : ALPHA_ISO;
+    std::vector<double> t1(B);
+    std::vector<int> nl(B), nc(B);
+    for (int t0 = 0; t0 < total; t0 += B) {
+        const int nb = std::min(B, total - t0);
+        IFDDA_CUDA(cudaMemcpyAsync(d1.p, a1.data() + t0, nb * sizeof(double), cudaMemcpyHostToDevice, st));
+        IFDDA_CUDA(cudaMemcpyAsync(d2.p, a2.data() + t0, nb * sizeof(double), cudaMemcpyHostToDevice, st));
+        IFDDA_CUDA(cudaMemcpyAsync(dpp.p, ppv.data() + t0, nb * sizeof(double), cudaMemcpyHostToDevice, st));
+        IFDDA_CUDA(cudaMemcpyAsync(dik.p, ikv.data() + t0, nb * sizeof(int), cudaMemcpyHostToDevice, st));
+        IFDDA_CUDA(cudaMemcpyAsync(djk.p, jkv.data() + t0, nb * sizeof(int), cudaMemcpyHostToDevice, st));
+        planewaves_dev(N, dx.p, dy.p, dz.p, k0, E0, nb, dbeam.p, d1.p, d2.p, dpp.p, ff0.p, g->ctx->flag.p, st);
+        const int rc = solve_device(g, nb, N, N, nullptr, al, amode, ff0.p, methodeit, tol, ff.p, loc.p, t1.data(),
+                                    nl.data(), nc.data(), nstop, infostr, opt, false);
+        if (tol1) *tol1 = t1[nb - 1];
+        if (nloop) *nloop = nl[nb - 1];
+        if (ncompte) *ncompte = nc[nb - 1];
+        if (rc) return rc;
+        // the lens checks of diffractefft2dlens.f run after the first solve
+        if (lens_error) return fail(lens_error);
+        mic_farfield_dev(m, nb, ff.p, zpl.p, tw.p, Q.p, Ed.p, st);
+        mic_lens_dev(m, nb, Ed.p, dik.p, djk.p, dpp.p, E0, F.p, st);
+        if (!mic_image_dev(m, nb, F.p, tw.p, T.p, img.p, st)) return fail("nfft2d not supported");
+    }
+    mic_sqrt_dev((long)6 * n * n, img.p, st);
+    IFDDA_CUDA(cudaMemcpyAsync(image, img.p, (size_t)6 * n * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    // image and pupil axes (microsbf.f:846-857)
+    const double deltax = 2.0 * pi / (double)n / dkx;
+    for (int i = -n / 2; i <= n / 2 - 1; i++) {
+        if (xy) xy[i + n / 2] = deltax * (double)i * mo->gross;
+        if (kxy) kxy[i + n / 2] = dkx * (double)i / k0;
+    }
+    if (nstop) *nstop = 0;
+    if (infostr) memset(infostr, ' ', 64);
+    return 0;
+    IFDDA_GUARD_END(g->ctx, infostr)
 }
 
 }  // extern "C"

@@ -4,6 +4,7 @@
 //   plane waves  : cdmlib/ondeplane.f:1-50, cdmlib/ondeplanekxky.f:1-60
 #include "post.cuh"
 #include "krylov_kernels.cuh"
+#include "planewave.cuh"
 
 namespace ifdda {
 
@@ -122,24 +123,7 @@ __global__ void k_planewaves(int nb, const double* __restrict__ xs, const double
     } else {
         kx = a1[r];
         ky = a2[r];
-        kz = sqrt(k0 * k0 - kx * kx - ky * ky);
-        const double2 E0s = make_double2(E0.x * s, E0.y * s), E0p = make_double2(E0.x * p, E0.y * p);
-        if (kz >= 0.99999 * k0) {
-            ex = E0p;
-            ey = E0s;
-            ez = make_double2(0, 0);
-        } else {
-            const double kp = sqrt(kx * kx + ky * ky);
-            const double nsx = -ky / kp, nsy = kx / kp;
-            double npx = kz * nsy, npy = -kz * nsx, npz = -kx * nsy + ky * nsx;
-            const double np = sqrt(npx * npx + npy * npy + npz * npz);
-            npx /= np;
-            npy /= np;
-            npz /= np;
-            ex = make_double2(E0s.x * nsx + E0p.x * npx, E0s.y * nsx + E0p.y * npx);
-            ey = make_double2(E0s.x * nsy + E0p.x * npy, E0s.y * nsy + E0p.y * npy);
-            ez = make_double2(E0p.x * npz, E0p.y * npz);
-        }
+        kxky_amplitude(k0, E0, ppr, kx, ky, ex, ey, ez, kz);
     }
     double2* o = out + (long)r * 3 * nb;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += (long)gridDim.x * blockDim.x) {

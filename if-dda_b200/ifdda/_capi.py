@@ -27,6 +27,12 @@ class SolveOptions(C.Structure):
                 ("inner_floor", C.c_double), ("maxit", C.c_int)]
 
 
+class MicroscopeOptions(C.Structure):
+    _fields_ = [("ntypemic", C.c_int), ("nfft2d", C.c_int), ("numaper", C.c_double), ("numaperinc", C.c_double),
+                ("gross", C.c_double), ("zlens", C.c_double), ("P0", C.c_double), ("w0", C.c_double),
+                ("batch", C.c_int)]
+
+
 _lib = None
 
 _vp = C.c_void_p
@@ -61,6 +67,9 @@ SIGNATURES = {
     "ifdda_cross_sections": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_double, C.c_double, _dp, _dp]),
     "ifdda_incident_planewaves": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_double, DComplex, C.c_int, _vp, _vp,
                                             _vp, _vp, _vp]),
+    "ifdda_microscope": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_char_p, C.c_double, C.POINTER(MicroscopeOptions),
+                                   _vp, _vp, _vp, _ip, _vp, _vp, _dp, _ip, _ip, _ip, C.c_char_p,
+                                   C.POINTER(SolveOptions)]),
     "ifdda_launch_count": (C.c_ulonglong, []),
     "ifdda_timing_enable": (C.c_int, [C.c_int, C.c_int]),
     "ifdda_timing_read": (C.c_int, [_ip, _dp]),

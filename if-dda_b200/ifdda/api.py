@@ -13,7 +13,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _capi
-from ._capi import IFDDA_FP32, IFDDA_FP64, IFDDA_MIXED, DComplex, SolveOptions
+from ._capi import IFDDA_FP32, IFDDA_FP64, IFDDA_MIXED, DComplex, MicroscopeOptions, SolveOptions
 
 
 class IfddaError(RuntimeError):
@@ -38,6 +38,20 @@ class SolveResult:
     nstop: int
     infostr: str
     extra: dict = field(default_factory=dict)
+
+
+@dataclass
+class MicroscopeResult:
+    image: np.ndarray   # (6, n, n): |E| of x, y, z, then with the incident wave
+    xy: np.ndarray      # image positions (m)
+    kxy: np.ndarray     # pupil kx / k0
+    kxinc: np.ndarray   # incidences of one polarisation, units of k0
+    kyinc: np.ndarray
+    tol1: float         # last solve
+    nloop: int
+    ncompte: int
+    nstop: int
+    infostr: str
 
 
 class Context:
@@ -211,6 +225,43 @@ class GreenSpectrum:
         r = SolveResult(FF=FF[0] if single else FF, FFloc=FFloc[0] if single else FFloc, tol1=tol1, nloop=nloop,
                         ncompte=ncompte, nstop=nstop.value, infostr=info.raw[:64].decode(errors="replace"))
         return r
+
+    def microscope(self, xs, ys, zs, polarisa, methodeit="GPBICG1", tol=1e-4, ntypemic=1, nfft2d=128, numaper=0.9,
+                   numaperinc=0.5, gross=100.0, zlens=0.0, P0=1.0, w0=1e-6, batch=0, precision=IFDDA_FP64):
+        """Bright-field (ntypemic 1, microsbf) or dark-field / phase
+        (ntypemic 2, microsdf) microscope in transmission with the FFT lens,
+        on the full box of this spectrum.  zlens and w0 in metres.  Returns a
+        MicroscopeResult: image (6, n, n) = |E| of the x, y, z image fields
+        and of the same with the incident wave (row v, column u), xy, kxy,
+        kxinc / kyinc (units of k0), the last solve's counters, nstop, infostr."""
+        n = int(nfft2d)
+        N = self.nx * self.ny * self.nz
+        xs = np.ascontiguousarray(xs, np.float64)
+        ys = np.ascontiguousarray(ys, np.float64)
+        zs = np.ascontiguousarray(zs, np.float64)
+        if len(xs) != N:
+            raise ValueError("the microscope works on the full box: nx*ny*nz positions")
+        pol = _zc(polarisa)
+        img = np.zeros((6, n, n), np.float64)
+        xy = np.zeros(n)
+        kxy = np.zeros(n)
+        cap = 4 * (n + 8) ** 2
+        kxi = np.zeros(cap)
+        kyi = np.zeros(cap)
+        ninc = C.c_int(cap)
+        tol1 = C.c_double(0)
+        nloop, ncompte, nstop = C.c_int(0), C.c_int(0), C.c_int(0)
+        info = C.create_string_buffer(b" " * 64, 65)
+        mo = MicroscopeOptions(int(ntypemic), n, float(numaper), float(numaperinc), float(gross), float(zlens),
+                               float(P0), float(w0), int(batch))
+        opt = SolveOptions(precision, 0, 0, 0.0, 0)
+        self.lib.ifdda_microscope(self.h, _p(xs), _p(ys), _p(zs), _p(pol), methodeit.encode(), tol, C.byref(mo),
+                                  _p(img), _p(xy), _p(kxy), C.byref(ninc), _p(kxi), _p(kyi), C.byref(tol1),
+                                  C.byref(nloop), C.byref(ncompte), C.byref(nstop), info, C.byref(opt))
+        m = min(ninc.value, cap)
+        return MicroscopeResult(image=img, xy=xy, kxy=kxy, kxinc=kxi[:m].copy(), kyinc=kyi[:m].copy(),
+                                tol1=tol1.value, nloop=nloop.value, ncompte=ncompte.value, nstop=nstop.value,
+                                infostr=info.raw[:64].decode(errors="replace"))
 
     def inverserig_device(self, nrhs, nbsphere, nmax, tabdip_ptr, polarisa_ptr, FF0_ptr, FF_ptr, FFloc_ptr,
                           methodeit="GPBICG1", tol=1e-4, precision=IFDDA_FP64, check_every=0, max_outer=0,

@@ -173,6 +173,43 @@ int ifdda_incident_planewaves(ifdda_ctx* ctx, int nbsphere, const double* xs, co
                               double k0, ifdda_dcmplx E0, int nrhs, const int* beam, const double* a1,
                               const double* a2, const double* pp, ifdda_dcmplx* FF0);
 
+/* Microscope options: the cdmlib arguments that the microscopes read
+   (cdmlib/cdmlib.f:3660-3800 with nlentille = 1, nquicklens = 1, nside = 0). */
+typedef struct {
+    int ntypemic;      /* 1 bright field (microsbf.f), 2 dark field and phase (microsdf.f) */
+    int nfft2d;        /* side n of the pupil and image grids: a power of two from 32 to 4096 */
+    double numaper;    /* numerical aperture of the objective, (0, 1] */
+    double numaperinc; /* numerical aperture of the condenser, < 1 */
+    double gross;      /* magnification */
+    double zlens;      /* focal-plane position in metres */
+    double P0, w0;     /* power (W) shared by all illuminations, waist (m) of irradiance.f */
+    int batch;         /* illuminations solved together; 0 = 32 */
+} ifdda_microscope_options;
+
+/* Bright-field or dark-field / phase microscope in transmission with the FFT
+   lens: replaces microsbf (cdmlib/microsbf.f:1-965) and microsdf
+   (cdmlib/microsdf.f:1-915) called at cdmlib/cdmlib.f:3735-3800, with
+   diffractefft2dlens.f, fouriertoimage.f and deltakroutine.f inside.  The
+   object fills the full box of the spectrum g (nbsphere = nx*ny*nz, the
+   reference forces it when nquicklens = 1, cdmlib.f:631); xs, ys, zs and
+   polarisa (nmax = nbsphere) as for ifdda_inverserig.  Every illumination
+   (both polarisations, s first) is solved in batches of mo->batch through the
+   batched solver, without the tol1 < tol check of cdmlib (microsbf does not
+   make it).  image receives 6 * n * n values: sqrt(sum |E|^2) over the
+   illuminations of the x, y, z image fields and of the same with the
+   incident wave (Eimagex..z, Eimageincx..z), pixel u + n v.  xy and kxy
+   (n values, may be NULL): image positions (m) and pupil kx / k0.  *ninc: on
+   entry the room in kxinc / kyinc (may be 0 with NULL arrays), on return the
+   number of incidences per polarisation; kxinc / kyinc receive them in
+   units of k0.  tol1, nloop, ncompte: those of the last solve, as the
+   reference leaves them.  Errors answer nstop = 1 with the reference's
+   messages. */
+int ifdda_microscope(ifdda_green* g, const double* xs, const double* ys, const double* zs,
+                     const ifdda_dcmplx* polarisa, const char* methodeit, double tol,
+                     const ifdda_microscope_options* mo, double* image, double* xy, double* kxy, int* ninc,
+                     double* kxinc, double* kyinc, double* tol1, int* nloop, int* ncompte, int* nstop,
+                     char* infostr, const ifdda_solve_options* opt);
+
 /* Diagnostics (no counterpart in the reference, whose only instrumentation
    is the wall/CPU-time printout of cdmlib/cdmlib.f:1956-1963 and the
    mat-vec count ncompte).

@@ -2498,6 +2498,287 @@ int orc_object_arbitrary(int nx, int ny, int nz, double d, const double *px, con
     return bad;
 }
 
+/* ------------------------------------------------------------------------- */
+/* Microscopes in transmission with the FFT lens (nquicklens = 1, nside = +1): */
+/* bright field cdmlib/microsbf.f (ntypemic = 1) and dark field / phase       */
+/* cdmlib/microsdf.f (ntypemic = 2) over the rigorous full-box solve; far     */
+/* field cdmlib/diffractefft2dlens.f, image cdmlib/fouriertoimage.f, grid     */
+/* index cdmlib/deltakroutine.f.  numaper is the objective's NA times k0, as  */
+/* cdmlib.f:3674 passes it.  image: 6 arrays of n*n (x, y, z, then the same   */
+/* with the incident field), pixel u + n v, each sqrt(sum |E|^2) over the     */
+/* incidences and both polarisations.  Returns nstop.                        */
+/* ------------------------------------------------------------------------- */
+
+/* deltakroutine.f:1-17: nearest grid index, truncated when outside na */
+static void orc_deltakroutine(double kxinc, double kyinc, double dkx, double dky, double na, int *i,
+                              int *j) {
+    *i = (int)lround(kxinc / dkx);
+    *j = (int)lround(kyinc / dky);
+    double kx = dkx * *i, ky = dky * *j;
+    if (kx * kx + ky * ky <= na * na) return;
+    *i = (int)(kxinc / dkx);
+    *j = (int)(kyinc / dky);
+}
+
+/* slot of 1-based index i in the FFT array (tabfft2, diffractefft2dlens.f:48-56) */
+static int orc_tabfft2(int i, int n) {
+    int n2 = n / 2;
+    return (i - n2 - 1 >= 0) ? i - n2 : n2 + i;
+}
+
+/* diffractefft2dlens.f:1-181 (nside = +1).  Ediff: (2 imax + 1)^2 x 3 with
+   entry ((jj * S + ii) * 3 + c), ii = imax + i, jj = imax + j. */
+static int orc_diffractefft2dlens(int nx, int ny, int nz, int n, double k0, const double *xs,
+                                  const double *ys, const double *zs, double d, const zc *FF,
+                                  double numaper, int *imax_out, zc **Ediff_out, char *infostr) {
+    const double pi = acos(-1.0);
+    double dkx = 2.0 * pi / ((double)n * d), dky = dkx;
+    if (n > 16384) { set_info(infostr, "nfft2d too large"); return 1; }
+    if (dkx >= numaper) { set_info(infostr, "In FFT lens nfft2d too small"); return 1; }
+    int n2 = n / 2;
+    double var1 = (xs[0] + (double)n2 * d) * dkx;
+    double var2 = (ys[0] + (double)n2 * d) * dky;
+    int imax = (int)lround(k0 / dkx) + 1;
+    if (2 * imax + 1 > n) {
+        set_info(infostr, "In FFT diffraction for lens nfft2d too small!");
+        return 1;
+    }
+    if (2 * imax + 1 < 7) { set_info(infostr, "In FFT diffract nfft2d too small"); return 1; }
+    int S = 2 * imax + 1;
+    zc *Ed = (zc *)calloc((size_t)S * S * 3, sizeof(zc));
+    zc *E = (zc *)malloc(sizeof(zc) * 3 * (size_t)n * n);
+    for (int k = 1; k <= nz; k++) {
+        memset(E, 0, sizeof(zc) * 3 * (size_t)n * n);
+        for (int i = 1; i <= nx; i++)
+            for (int j = 1; j <= ny; j++) {
+                long kk = i + (long)nx * (j - 1) + (long)nx * ny * (k - 1);
+                long ind = (orc_tabfft2(i, n) - 1) + (long)n * (orc_tabfft2(j, n) - 1);
+                for (int c = 0; c < 3; c++) E[c * (size_t)n * n + ind] = FF[3 * (kk - 1) + c];
+            }
+        for (int c = 0; c < 3; c++) orc_fft3d(E + c * (size_t)n * n, n, n, 1, -1);
+        long kk = 1 + (long)nx * ny * (k - 1);
+        for (int i = -imax; i <= imax; i++)
+            for (int j = -imax; j <= imax; j++) {
+                double kx = (double)i * dkx, ky = (double)j * dky;
+                if (kx * kx + ky * ky < numaper * numaper) {
+                    double kz = sqrt(k0 * k0 - kx * kx - ky * ky);
+                    long ind = (orc_tabfft2(i + n2 + 1, n) - 1) +
+                               (long)n * (orc_tabfft2(j + n2 + 1, n) - 1);
+                    zc ex = E[ind], ey = E[(size_t)n * n + ind], ez = E[2 * (size_t)n * n + ind];
+                    zc ctmp = (kx * ex + ky * ey + kz * ez) / k0;
+                    zc ctmp1 = cexp(-I * kz * zs[kk - 1]) * cexp(-I * (var1 * i + var2 * j)) /
+                               (-2.0 * pi * I * kz);
+                    zc *o = Ed + ((size_t)(imax + j) * S + (imax + i)) * 3;
+                    o[0] += (ex - kx * ctmp / k0) * ctmp1;
+                    o[1] += (ey - ky * ctmp / k0) * ctmp1;
+                    o[2] += (ez - kz * ctmp / k0) * ctmp1;
+                }
+            }
+    }
+    for (size_t q = 0; q < (size_t)S * S * 3; q++) Ed[q] = Ed[q] * k0 * k0;
+    free(E);
+    *imax_out = imax;
+    *Ediff_out = Ed;
+    return 0;
+}
+
+/* fouriertoimage.f:1-128: 2-D FFT (sign -1) of the six arrays, centred
+   (fftshift) and scaled by dkx dky / gross */
+static void orc_fouriertoimage(double dkx, double dky, double gross, zc *F, int n) {
+    int n2 = n / 2;
+    double tmp = dkx * dky / gross;
+    for (int c = 0; c < 6; c++) orc_fft3d(F + c * (size_t)n * n, n, n, 1, -1);
+    for (int c = 0; c < 6; c++) {
+        zc *a = F + c * (size_t)n * n;
+        for (int i = -n2; i <= n2 - 1; i++)
+            for (int j = -n2; j <= -1; j++) {
+                int ix = i >= 0 ? i + 1 : n + i + 1, iy = j >= 0 ? j + 1 : n + j + 1;
+                long ind = (ix - 1) + (long)n * (iy - 1);
+                long kk = (i + n2) + (long)n * (j + n2);
+                zc t = a[kk];
+                a[kk] = a[ind] * tmp;
+                a[ind] = t * tmp;
+            }
+    }
+}
+
+int orc_microscope(int ntypemic, const zc *G6, int nx, int ny, int nz, double d, double k0,
+                   const double *xs, const double *ys, const double *zs, const zc *pol,
+                   const char *methodeit, double tol, double numaper, double numaperinc, int n,
+                   double gross, double zlens, double P0, double w0, double *image, double *xy,
+                   double *kxy, int *ninc, double *kxinc_out, double *kyinc_out, double *tol1,
+                   int *nloop, int *ncompte, char *infostr) {
+    const double pi = acos(-1.0);
+    int N = nx * ny * nz;
+    long n3 = 3L * N;
+    int n2 = n / 2;
+    double numaperk = k0 * numaperinc;
+    set_info(infostr, "");
+    if (numaperinc >= 1.0 || numaper <= 0.0) {
+        set_info(infostr, "NA inc strictly between 0 and 1");
+        return 1;
+    }
+    double xmax = -1e300, xmin = 1e300, ymax = -1e300, ymin = 1e300;
+    for (int i = 0; i < N; i++) {
+        xmax = fmax(xmax, xs[i]); xmin = fmin(xmin, xs[i]);
+        ymax = fmax(ymax, ys[i]); ymin = fmin(ymin, ys[i]);
+    }
+    double deltakm = pi / fmax(xmax - xmin, ymax - ymin);
+    double dkx = 2.0 * pi / (d * (double)n), dky;
+    if (dkx >= numaperk) {
+        set_info(infostr, "In FFT lens nfft2d too small:Increase size of FFT 1");
+        return 1;
+    }
+    int imul = (int)(deltakm / dkx);
+    if (imul == 0) {
+        set_info(infostr, "In FFT lens nfft2d too small:Increase size of FFT 2");
+        return 1;
+    }
+    double deltak;
+    int imaxinc;
+    for (;;) {
+        deltak = dkx * (double)imul;
+        imaxinc = (int)lround(k0 / deltak) + 1;
+        if (imaxinc > 3) break;
+        imul--;
+        if (imul == 0) {
+            set_info(infostr, "In FFT lens nfft2d too small:Increase size of FFT 3");
+            return 1;
+        }
+    }
+    dky = dkx;
+    /* incidence list of one polarisation */
+    int cap = 0, cnt = 0;
+    double *kxi = NULL, *kyi = NULL;
+    if (ntypemic == 1) {
+        int m = imaxinc;
+        cap = (2 * m + 1) * (2 * m + 1);
+        kxi = (double *)malloc(sizeof(double) * cap);
+        kyi = (double *)malloc(sizeof(double) * cap);
+        for (int id = -m; id <= m; id++)
+            for (int jd = -m; jd <= m; jd++) {
+                double kx = id * deltak, ky = jd * deltak;
+                if (kx * kx + ky * ky <= numaperk * numaperk) { kxi[cnt] = kx; kyi[cnt] = ky; cnt++; }
+            }
+        if (n > 16384) { set_info(infostr, "nfft2d too large"); free(kxi); free(kyi); return 1; }
+        if (deltak >= numaperk) {
+            set_info(infostr, "In FFT lens nfft2d too small");
+            free(kxi); free(kyi);
+            return 1;
+        }
+    } else if (ntypemic == 2) {
+        double deltatheta = deltak / k0 * numaperinc;
+        int m = (int)(2.0 * pi / deltatheta) + 1;
+        if (m < 8) m = 8;
+        kxi = (double *)malloc(sizeof(double) * m);
+        kyi = (double *)malloc(sizeof(double) * m);
+        for (int id = 0; id < m; id++) {
+            double phi = (double)id * 2.0 * pi / (double)m;
+            kxi[cnt] = cos(phi) * k0 * numaperinc;
+            kyi[cnt] = sin(phi) * k0 * numaperinc;
+            cnt++;
+        }
+    } else {
+        set_info(infostr, "ntypemic must be 1 or 2");
+        return 1;
+    }
+    int cap_out = *ninc;
+    *ninc = cnt;
+    for (int q = 0; q < cnt && q < cap_out; q++) {
+        if (kxinc_out) kxinc_out[q] = kxi[q] / k0;
+        if (kyinc_out) kyinc_out[q] = kyi[q] / k0;
+    }
+    double E0r, irra;
+    orc_irradiance(P0 / (double)(2 * cnt), w0, &E0r, &irra);
+    zc E0 = E0r;
+    memset(image, 0, sizeof(double) * 6 * (size_t)n * n);
+    zc *FF0 = (zc *)malloc(sizeof(zc) * n3), *FF = (zc *)malloc(sizeof(zc) * n3),
+       *FFloc = (zc *)malloc(sizeof(zc) * n3);
+    zc *F = (zc *)malloc(sizeof(zc) * 6 * (size_t)n * n);
+    int nstop = 0, imax = 0;
+    for (int ipol = 1; ipol <= 2 && !nstop; ipol++) {
+        double pp = ipol == 1 ? 0.0 : 1.0;
+        for (int q = 0; q < cnt && !nstop; q++) {
+            double kxinc = kxi[q], kyinc = kyi[q];
+            for (int i = 0; i < N; i++) orc_ondeplanekxky(xs[i], ys[i], zs[i], k0, E0, pp, kxinc, kyinc, FF0 + 3L * i);
+            orc_inverserig(G6, nx, ny, nz, N, NULL, pol, N, FF0, methodeit, tol, FF, FFloc, tol1, nloop,
+                           ncompte, &nstop, infostr, NULL, 0);
+            if (nstop == 1) break;
+            zc *Ed = NULL;
+            if (orc_diffractefft2dlens(nx, ny, nz, n, k0, xs, ys, zs, d, FF, numaper, &imax, &Ed, infostr)) {
+                nstop = 1;
+                break;
+            }
+            int S = 2 * imax + 1;
+            memset(F, 0, sizeof(zc) * 6 * (size_t)n * n);
+            int ik, jk;
+            if (ntypemic == 1) orc_deltakroutine(kxinc, kyinc, deltak, deltak, k0, &ik, &jk);
+            else orc_deltakroutine(kxinc, kyinc, dkx, dky, k0, &ik, &jk);
+            double dkxy = dkx * dky;
+            for (int i = -imax; i <= imax; i++)
+                for (int j = -imax; j <= imax; j++) {
+                    int ix = i >= 0 ? i + 1 : n + i + 1, iy = j >= 0 ? j + 1 : n + j + 1;
+                    long ind = (ix - 1) + (long)n * (iy - 1);
+                    double kx = dkx * i, ky = dky * j, tmp = kx * kx + ky * ky;
+                    if (!(tmp <= numaper * numaper)) continue;
+                    double kz = sqrt(k0 * k0 - tmp);
+                    zc zf = cexp(I * kz * zlens);
+                    zc *e = Ed + ((size_t)(imax + j) * S + (imax + i)) * 3;
+                    zc f[6];
+                    for (int c = 0; c < 3; c++) f[c] = f[c + 3] = e[c] * zf;
+                    if (i == ik && j == jk) {
+                        zc Ei[3];
+                        orc_ondeplanekxky(0.0, 0.0, 0.0, k0, E0, pp, kx, ky, Ei);
+                        if (ntypemic == 1) {
+                            /* microsbf.f: z divided by deltaky alone, as the reference does */
+                            f[3] += Ei[0] / dkxy * zf;
+                            f[4] += Ei[1] / dkxy * zf;
+                            f[5] += Ei[2] / dky * zf;
+                        } else {
+                            for (int c = 0; c < 3; c++) f[3 + c] += Ei[c] / dkx / dky * zf * I;
+                        }
+                    }
+                    if (tmp != 0.0) {
+                        double u[3], v[3];
+                        u[0] = kx / k0; u[1] = ky / k0; u[2] = sqrt(1.0 - u[0] * u[0] - u[1] * u[1]);
+                        v[0] = -kx / k0 / gross; v[1] = -ky / k0 / gross;
+                        v[2] = sqrt(1.0 - v[0] * v[0] - v[1] * v[1]);
+                        double u1 = u[1] * v[2] - u[2] * v[1];
+                        double u2 = -u[0] * v[2] + u[2] * v[0];
+                        double cs = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+                        double sn = sqrt(u1 * u1 + u2 * u2);
+                        u1 = u1 / sn;
+                        u2 = u2 / sn;
+                        double t = sqrt(u[2] / v[2]);
+                        for (int h = 3; h >= 0; h -= 3) {
+                            zc X = f[h], Y = f[h + 1], Z = f[h + 2];
+                            zc tx = (u1 * u1 + (1.0 - u1 * u1) * cs) * X + u1 * u2 * (1.0 - cs) * Y + u2 * sn * Z;
+                            zc ty = u1 * u2 * (1.0 - cs) * X + (u2 * u2 + (1.0 - u2 * u2) * cs) * Y - u1 * sn * Z;
+                            zc tz = -u2 * sn * X + u1 * sn * Y + cs * Z;
+                            f[h] = tx * t;
+                            f[h + 1] = ty * t;
+                            f[h + 2] = tz * t;
+                        }
+                    }
+                    for (int c = 0; c < 6; c++) F[c * (size_t)n * n + ind] = f[c];
+                }
+            free(Ed);
+            orc_fouriertoimage(dkx, dky, gross, F, n);
+            for (size_t p = 0; p < 6 * (size_t)n * n; p++)
+                image[p] += creal(F[p] * conj(F[p]));
+        }
+    }
+    free(FF0); free(FF); free(FFloc); free(F); free(kxi); free(kyi);
+    if (nstop) return nstop;
+    for (size_t p = 0; p < 6 * (size_t)n * n; p++) image[p] = sqrt(image[p]);
+    double deltax = 2.0 * pi / (double)n / dkx;
+    for (int i = -n2; i <= n2 - 1; i++) {
+        xy[i + n2] = deltax * (double)i * gross;
+        kxy[i + n2] = dkx * (double)i / k0;
+    }
+    return 0;
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -370,3 +370,35 @@ def object_arbitrary(nx, ny, nz, d, px, py, pz, eps_site, k0, methode):
     if rc:
         raise ValueError("object arbitrary")
     return _pack(nx, ny, nz, d, nb.value, nd.value, xs, ys, zs, tab, pol, ep, nmax)
+
+
+def microscope(ntypemic, G6, nx, ny, nz, d, k0, xs, ys, zs, polarisa, methodeit, tol, numaper, numaperinc, nfft2d,
+               gross, zlens, P0, w0):
+    """Bright-field (ntypemic 1, cdmlib/microsbf.f) or dark-field/phase
+    (ntypemic 2, cdmlib/microsdf.f) microscope in transmission with the FFT
+    lens, full box.  numaper is the objective's NA (multiplied by k0 here as
+    cdmlib.f:3674 does); zlens in metres.  Returns a dict with image (6, n, n)
+    [x, y, z, incx, incy, incz; row v, column u], xy, kxy, kxinc/kyinc (in
+    units of k0), the last solve's tol1/nloop/ncompte, nstop, infostr."""
+    n = int(nfft2d)
+    img = np.zeros(6 * n * n, np.float64)
+    xy = np.zeros(n, np.float64)
+    kxy = np.zeros(n, np.float64)
+    cap = 100000
+    kxi = np.zeros(cap, np.float64)
+    kyi = np.zeros(cap, np.float64)
+    ninc = C.c_int(cap)
+    tol1, nloop, ncompte = C.c_double(0), C.c_int(0), C.c_int(0)
+    info = C.create_string_buffer(b" " * 64, 65)
+    f = lib().orc_microscope
+    f.restype = C.c_int
+    nstop = f(C.c_int(ntypemic), _p(_z(G6)), C.c_int(nx), C.c_int(ny), C.c_int(nz), C.c_double(d), C.c_double(k0),
+              _p(np.ascontiguousarray(xs, np.float64)), _p(np.ascontiguousarray(ys, np.float64)),
+              _p(np.ascontiguousarray(zs, np.float64)), _p(_z(polarisa)), methodeit.encode(), C.c_double(tol),
+              C.c_double(numaper * k0), C.c_double(numaperinc), C.c_int(n), C.c_double(gross), C.c_double(zlens),
+              C.c_double(P0), C.c_double(w0), _p(img), _p(xy), _p(kxy), C.byref(ninc), _p(kxi), _p(kyi),
+              C.byref(tol1), C.byref(nloop), C.byref(ncompte), info)
+    m = ninc.value
+    return dict(image=img.reshape(6, n, n), xy=xy, kxy=kxy, kxinc=kxi[:m].copy(), kyinc=kyi[:m].copy(),
+                tol1=tol1.value, nloop=nloop.value, ncompte=ncompte.value, nstop=nstop,
+                infostr=info.raw[:64].decode(errors="replace"))

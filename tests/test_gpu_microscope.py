@@ -1,0 +1,79 @@
+"""GPU: the microscopes (bright field, microsbf.f; dark field and phase,
+microsdf.f) with the FFT lens, through the C-ABI, against the oracle's
+restatement, which solves the illuminations one by one and forms the image
+with full 2-D FFTs as the reference does.
+
+The solves converge to the same iteration counts, so the dipole moments agree
+to ~1e-10 and the images, sums of squared FFT outputs, to the same order; the
+test allows 1e-8 (relative, per image component).  Incidence lists and axes
+come from the same double arithmetic on the host and must be identical."""
+import math
+
+import numpy as np
+import pytest
+
+from cases import rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _object(nnnr=8):
+    from ifdda import objects
+    k0 = 2 * math.pi / 632.8e-9
+    ob = objects.sphere(100e-9, 2.25 + 0j, nnnr, k0, "RR", na=0)  # full box
+    return ob, k0
+
+
+def _compare(r, ref, tol=1e-8):
+    assert r.nstop == 0 and ref["nstop"] == 0, (r.infostr, ref["infostr"])
+    assert np.array_equal(r.kxinc, ref["kxinc"]) and np.array_equal(r.kyinc, ref["kyinc"])
+    assert np.array_equal(r.xy, ref["xy"]) and np.array_equal(r.kxy, ref["kxy"])
+    assert r.nloop == ref["nloop"] and r.ncompte == ref["ncompte"]
+    for c in range(6):
+        assert rel(r.image[c], ref["image"][c]) < tol, c
+
+
+@pytest.mark.parametrize("ntypemic,nfft2d", [(1, 64), (1, 128), (2, 64)])
+def test_microscope_matches_oracle(gctx, orc, ntypemic, nfft2d):
+    ob, k0 = _object()
+    G = orc.greencalculfft(8, 8, 8, ob.aretecube, k0)
+    ref = orc.microscope(ntypemic, G, 8, 8, 8, ob.aretecube, k0, ob.xs, ob.ys, ob.zs, ob.polarisa, "GPBICG1", 1e-6,
+                         0.9, 0.5, nfft2d, 100.0, 50e-9, 1.0, 6328e-9)
+    g = gctx.green(8, 8, 8, ob.aretecube, k0)
+    r = g.microscope(ob.xs, ob.ys, ob.zs, ob.polarisa, "GPBICG1", 1e-6, ntypemic=ntypemic, nfft2d=nfft2d,
+                     numaper=0.9, numaperinc=0.5, gross=100.0, zlens=50e-9, P0=1.0, w0=6328e-9)
+    _compare(r, ref)
+    # the image carries the object: the scattered intensity is not zero
+    assert r.image[0].max() > 0 and r.image[3].max() > r.image[0].max()
+    g.close()
+
+
+def test_microscope_batches_agree(gctx, orc):
+    """Illuminations split over batches of 3 give the image of one batch."""
+    ob, k0 = _object()
+    g = gctx.green(8, 8, 8, ob.aretecube, k0)
+    kw = dict(ntypemic=1, nfft2d=64, numaper=0.9, numaperinc=0.5, gross=100.0, zlens=0.0, P0=1.0, w0=6328e-9)
+    a = g.microscope(ob.xs, ob.ys, ob.zs, ob.polarisa, "GPBICG1", 1e-6, batch=3, **kw)
+    b = g.microscope(ob.xs, ob.ys, ob.zs, ob.polarisa, "GPBICG1", 1e-6, batch=0, **kw)
+    assert a.nstop == 0 and b.nstop == 0
+    for c in range(6):
+        assert rel(a.image[c], b.image[c]) < 1e-12
+    g.close()
+
+
+def test_microscope_reports_the_references_errors(gctx, orc):
+    ob, k0 = _object()
+    g = gctx.green(8, 8, 8, ob.aretecube, k0)
+    kw = dict(nfft2d=64, numaper=0.9, gross=100.0, zlens=0.0, P0=1.0, w0=6328e-9)
+    r = g.microscope(ob.xs, ob.ys, ob.zs, ob.polarisa, "GPBICG1", 1e-6, numaperinc=1.0, **kw)
+    assert r.nstop == 1 and r.infostr.strip() == "NA inc strictly between 0 and 1"
+    # a pupil grid too coarse for the condenser (dkx >= NA_inc k0)
+    r = g.microscope(ob.xs, ob.ys, ob.zs, ob.polarisa, "GPBICG1", 1e-6, numaperinc=0.1, **kw)
+    ref = orc.microscope(1, orc.greencalculfft(8, 8, 8, ob.aretecube, k0), 8, 8, 8, ob.aretecube, k0, ob.xs, ob.ys,
+                         ob.zs, ob.polarisa, "GPBICG1", 1e-6, 0.9, 0.1, 64, 100.0, 0.0, 1.0, 6328e-9)
+    assert r.nstop == ref["nstop"] == 1 and r.infostr.strip() == ref["infostr"].strip()
+    # nfft2d outside the compiled lengths
+    r = g.microscope(ob.xs, ob.ys, ob.zs, ob.polarisa, "GPBICG1", 1e-6, ntypemic=1, nfft2d=96, numaper=0.9,
+                     numaperinc=0.5)
+    assert r.nstop == 1 and "nfft2d not supported" in r.infostr
+    g.close()
