@@ -10,7 +10,9 @@ Default workload (one step = one complete rigorous solve):
 Other workloads (--workload): c1 (sphere 16^3, inside-only dipoles), c3
 (128 plane waves on a 96x96x64 ellipsoid lattice, one batched solve per
 step), c5 (192^3 concentric spheres, GPBICG1), c4 (request stream
-through the continuous-batching server).
+through the continuous-batching server), mic (bright-field microscope image
+of the c3 object: every illumination of the condenser solved in batches, FFT
+lens, 512^2 image; one step = one image).
 Inputs are resident in HBM for `value`; `e2e` runs the same solve through the
 C-ABI (ifdda_inverserig) with pinned host inputs and the host<->device copies
 inside the timed region.  L2 is flushed (256 MiB write) before every timed
@@ -546,13 +548,79 @@ def run_serving(args):
     return 0
 
 
+def run_microscope(args):
+    """Bright-field microscope (microsbf.f with the FFT lens) of the c3
+    ellipsoid: one step = one complete image, every illumination solved.  The
+    call is the C-ABI's ifdda_microscope with host inputs and the image read
+    back, so the timed region is end to end; it is timed with CUDA events on
+    the library's stream (the call returns after its last kernel)."""
+    import torch
+    import ifdda
+    from ifdda import IFDDA_FP64, IFDDA_MIXED
+
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = wl_c3()
+    ob, k0 = w.ob, w.k0
+    lam = 2 * math.pi / k0
+    mo = dict(ntypemic=1, nfft2d=512, numaper=0.9, numaperinc=0.5, gross=100.0, zlens=0.0, P0=1.0, w0=10 * lam)
+    ctx = ifdda.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    g = ctx.green(ob.nx, ob.ny, ob.nz, ob.aretecube, k0)
+    lib = ctx.lib
+    out = {}
+    for name, prec in (("mixed", IFDDA_MIXED), ("fp64", IFDDA_FP64)):
+        steps = args.steps if name == "mixed" else max(1, min(args.steps, 3))
+        for _ in range(args.warmup if name == "mixed" else 1):
+            r = g.microscope(ob.xs, ob.ys, ob.zs, ob.polarisa, w.method, TOL, precision=prec, **mo)
+            if r.nstop != 0:
+                raise RuntimeError(r.infostr.strip())
+        times = []
+        l0 = lib.ifdda_launch_count()
+        with ClockSampler(local) as clk:
+            for _ in range(steps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                r = g.microscope(ob.xs, ob.ys, ob.zs, ob.polarisa, w.method, TOL, precision=prec, **mo)
+                e1.record(stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+        launches = (lib.ifdda_launch_count() - l0) // steps
+        ms = statistics.mean(times)
+        out[name] = dict(images_per_s=1e3 / ms, ms_per_image=ms, illuminations=2 * len(r.kxinc),
+                         last_ncompte=r.ncompte, launches_per_image=launches, clocks=clk.summary())
+    m = out["mixed"]
+    nill = m["illuminations"]
+    cpu = None
+    if not args.no_cpu and rank == 0:
+        v, cores, sample = cpu_oracle_sample(w, out["fp64"]["last_ncompte"])
+        cpu = {"value": v / nill, "unit": "images/s", "cores": cores, "kind": "port",
+               "sample": sample + f"; one image = {nill} such solves (the oracle's image formation not counted)"}
+    desc = (f"bright-field microscope (microsbf.f, FFT lens) of the c3 ellipsoid (96x96x64 full box, d=10 nm, "
+            f"lambda=500 nm): objective NA 0.9, condenser NA 0.5, {nill} illuminations (s and p), image "
+            f"512x512, magnification 100, GPBICG1 to 1e-4")
+    line = {"metric": "microscope images/s", "value": m["images_per_s"], "unit": "images/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms_per_image"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64 inner / c128 outer", "data": "synthetic (seeded)",
+            "config": {"workload": desc, "parallelism": "single GPU", "l2": "inputs > L2 (590k dipoles)"},
+            "gpu_launches": m["launches_per_image"], "clocks": m["clocks"], "microscope": out,
+            "cpu_baseline": cpu}
+    g.close()
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ifdda", choices=["ifdda", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5", "mic"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) measurement")
     ap.add_argument("--requests", type=int, default=2000, help="c4: stream length")
@@ -562,11 +630,13 @@ def main():
                     help="matvec: time the five mat-vec passes only")
     args = ap.parse_args()
     if args.impl == "reference":
-        if args.workload == "c4":
+        if args.workload in ("c4", "mic"):
             args.workload = "c2"
         return run_reference(args)
     if args.workload == "c4":
         return run_serving(args)
+    if args.workload == "mic":
+        return run_microscope(args)
     if args.mode == "matvec":
         return run_matvec(args)
     return run_gpu(args)

@@ -770,7 +770,7 @@ int ifdda_microscope(ifdda_green* g, const double* xs, const double* ys, const d
                              : S > n        ? "In FFT diffraction for lens nfft2d too small!"
                              : S < 7        ? "In FFT diffract nfft2d too small"
                                             : nullptr;
-    const int B = std::max(1, std::min(total, mo->batch > 0 ? mo->batch : 32));
+    const int B = std::max(1, std::min(total, mo->batch > 0 ? mo->batch : 64));
     const long n3 = 3L * N;
     DevBuf<double> dx, dy, dz, zpl, d1, d2, dpp, img;
     DevBuf<int> dbeam, dik, djk;

@@ -9,7 +9,10 @@ macroscopic fields (:2497-2655), cross sections (:2717-2778) -- and returns
 the reference's outputs in a dict together with nstop/infostr.  Only the
 options on the rigorous-solve path are implemented (trope 'iso' for every
 object here, trope 'ani' for the sphere and the cube, plane waves, nrig = 0,
-0 <= nquad <= 16); anything else returns nstop = 1 with a message.
+0 <= nquad <= 16), and the bright-field and dark-field microscopes in
+transmission with the FFT lens (nlentille = 1, ntypemic 1 or 2, nside = 0,
+nquicklens = 1, cdmlib.f:3660-3800); anything else returns nstop = 1 with a
+message.
 """
 from __future__ import annotations
 
@@ -33,12 +36,16 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
            nx=None, ny=None, nz=None, aretecube=None, epsani=None, lc=None, hc=None, ng=0, positions=None, eps_site=None,
            beam="pwavelinear", theta=0.0, phi=0.0, pp=1.0, incidences=None, P0=1.0, w0=None,
            tolinit=1e-4, methodeit="GPBICG1", polarizability="RR", trope="iso", nproche=0, nrig=0, nquad=0,
-           nlocal=1, nmacro=1, nsection=1, precision=0, ctx: Context | None = None, device=0):
+           nlocal=1, nmacro=1, nsection=1, precision=0, nlentille=0, ntypemic=1, nside=0, nquicklens=1,
+           nfft2d=128, numaper=0.9, numaperinc=0.5, gross=100.0, zlens=0.0, microscope_batch=0,
+           ctx: Context | None = None, device=0):
     """Rigorous solve of one object for one plane wave (theta, phi, pp) or a
     batch of them (incidences = [(theta, phi, pp), ...]).  nproche follows the
     GUI convention: 0 -> dipoles inside the object only (inverserig), >= 1 ->
     the full box (inverserigopt).  precision: 0 plain FP64, 1 FP32 inner
-    iterations with FP64 refinement."""
+    iterations with FP64 refinement.  nlentille = 1 adds the microscope's
+    images (Eimagex..z, Eimageincx..z as |E| on nfft2d^2 pixels, xy, kxy,
+    kxinc/kyinc); zlens in nm."""
     lam = wavelength * 1e-9
     if trope not in ("iso", "ani"):
         return _fail(f"trope {trope!r} is neither 'iso' nor 'ani'")
@@ -62,6 +69,17 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
         return _fail("Tolerance  for the iterative method too large!")
     if object not in _SUPPORTED_OBJECTS:
         return _fail(f"object {object!r} not handled by the GPU drop-in")
+    if nlentille:
+        # cdmlib.f:365-389
+        if not 0.0 < numaper <= 1.0:
+            return _fail("Problem with numerical aperture!")
+        if abs(gross) < 1.0:
+            return _fail("Problem with manification!")
+        if abs(theta) >= 90.0:
+            return _fail("Illumination on the wrong side with the options")
+        if ntypemic not in (1, 2) or nside != 0 or nquicklens != 1:
+            return _fail("only the bright-field and dark-field microscopes in transmission with the FFT lens")
+        nproche = max(nproche, 1)  # the FFT lens needs the full box (cdmlib.f:631)
     if not (nlocal or nmacro or nsection):
         return _fail("No calculation requested!")
     k0 = 2 * math.pi / lam
@@ -115,6 +133,19 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
                    aretecube=ob.aretecube, k0=k0, irra=irra, E0=E0, tol1=r.tol1, nloop=r.nloop,
                    ncompte=r.ncompte, incidentfield=ff0, FF=r.FF, localfield=r.FFloc, xs=ob.xs, ys=ob.ys,
                    zs=ob.zs)
+        if r.nstop == 0 and nlentille:
+            # ---- microscope (cdmlib.f:3660-3800) ---------------------------
+            m = g.microscope(ob.xs, ob.ys, ob.zs, ob.polarisa, methodeit, tolinit, ntypemic=ntypemic,
+                             nfft2d=nfft2d, numaper=numaper, numaperinc=numaperinc, gross=gross,
+                             zlens=zlens * 1e-9, P0=P0, w0=(w0 if w0 is not None else 10 * wavelength) * 1e-9,
+                             batch=microscope_batch, precision=precision)
+            if m.nstop != 0:
+                g.close()
+                out.update(nstop=m.nstop, infostr=m.infostr)
+                return out
+            for c, name in enumerate(("Eimagex", "Eimagey", "Eimagez", "Eimageincx", "Eimageincy", "Eimageincz")):
+                out[name] = m.image[c]
+            out.update(xy=m.xy, kxy=m.kxy, kxinc=m.kxinc, kyinc=m.kyinc)
         g.close()
         if r.nstop != 0:
             return out

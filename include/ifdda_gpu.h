@@ -183,7 +183,7 @@ typedef struct {
     double gross;      /* magnification */
     double zlens;      /* focal-plane position in metres */
     double P0, w0;     /* power (W) shared by all illuminations, waist (m) of irradiance.f */
-    int batch;         /* illuminations solved together; 0 = 32 */
+    int batch;         /* illuminations solved together; 0 = 64 */
 } ifdda_microscope_options;
 
 /* Bright-field or dark-field / phase microscope in transmission with the FFT

@@ -77,3 +77,21 @@ def test_microscope_reports_the_references_errors(gctx, orc):
                      numaperinc=0.5)
     assert r.nstop == 1 and "nfft2d not supported" in r.infostr
     g.close()
+
+
+def test_cdmlib_microscope_matches_oracle(orc):
+    """nlentille = 1 through the cdmlib-style entry: the object is put in its
+    full box (cdmlib.f:631) and the images follow the normal-incidence
+    solve; zlens in nm as the reference takes it."""
+    from ifdda.cdmlib import cdmlib
+    out = cdmlib(wavelength=632.8, object="sphere", rayon=100.0, eps=2.25 + 0j, nnnr=8, tolinit=1e-6,
+                 methodeit="GPBICG1", polarizability="RR", nproche=0, P0=1.0, w0=6328.0, nlentille=1, ntypemic=2,
+                 nfft2d=64, numaper=0.9, numaperinc=0.5, gross=100.0, zlens=50.0)
+    assert out["nstop"] == 0, out["infostr"]
+    assert out["nbsphere"] == 512  # full box
+    ob, k0 = _object()
+    G = orc.greencalculfft(8, 8, 8, ob.aretecube, k0)
+    ref = orc.microscope(2, G, 8, 8, 8, ob.aretecube, k0, ob.xs, ob.ys, ob.zs, ob.polarisa, "GPBICG1", 1e-6,
+                         0.9, 0.5, 64, 100.0, 50e-9, 1.0, 6328e-9)
+    for c, name in enumerate(("Eimagex", "Eimagey", "Eimagez", "Eimageincx", "Eimageincy", "Eimageincz")):
+        assert rel(out[name], ref["image"][c]) < 1e-8, name

@@ -33,6 +33,13 @@ def test_cdmlib_driver_rejects_like_the_reference():
     assert cdmlib(wavelength=632.8, object="concentricsphere", nnnr=8, trope="ani", epsani=ani)["nstop"] == 1
     assert cdmlib(wavelength=632.8, object="sphere", rayon=1000.0, eps=2.25, nnnr=4, trope="ani",
                   epsani=ani)["infostr"] == "Meshsize larger than lambda/4!"
+    # microscope options (cdmlib.f:365-389)
+    sph = dict(wavelength=632.8, object="sphere", rayon=100.0, eps=2.25, nnnr=8, nlentille=1)
+    assert cdmlib(numaper=1.5, **sph)["infostr"] == "Problem with numerical aperture!"
+    assert cdmlib(gross=0.5, **sph)["infostr"] == "Problem with manification!"
+    assert cdmlib(theta=95.0, **sph)["infostr"] == "Illumination on the wrong side with the options"
+    assert cdmlib(ntypemic=0, **sph)["nstop"] == 1  # holography is not built
+    assert cdmlib(nside=1, **sph)["nstop"] == 1     # nor the reflection side
 
 
 def _free_port():
