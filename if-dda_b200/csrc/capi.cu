@@ -646,6 +646,105 @@ int ifdda_incident_planewaves(ifdda_ctx* ctx, int nbsphere, const double* xs, co
     IFDDA_GUARD_END(ctx, nullptr)
 }
 
+int ifdda_nearfield_wide(ifdda_ctx* ctx, int nx, int ny, int nz, int nxmp, int nymp, int nzmp, double aretecube,
+                         double k0, int nquad, int nbsphere, int nmax, const double* xs, const double* ys,
+                         const double* zs, const ifdda_dcmplx* FF, const ifdda_dcmplx* FF0,
+                         const ifdda_dcmplx* epsilon, ifdda_dcmplx E0, double theta, double phi, double pp,
+                         double* xswf, double* yswf, double* zswf, ifdda_dcmplx* incident, ifdda_dcmplx* local,
+                         ifdda_dcmplx* macro) {
+    if (!ctx || !xs || !ys || !zs || !FF || !FF0 || !epsilon || nbsphere < 1 || nmax < nbsphere || nx < 1 ||
+        ny < 1 || nz < 1 || nxmp < 0 || nymp < 0 || nzmp < 0)
+        return 1;
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(ctx->device);
+    AllocStreamScope as(ctx->stream);
+    cudaStream_t st = ctx->stream;
+    const int nxw = nx + 2 * nxmp, nyw = ny + 2 * nymp, nzw = nz + 2 * nzmp;
+    const long nw = (long)nxw * nyw * nzw;
+    // the enlarged box starts nxmp cells before the object's smallest x
+    // (cdmlib.f:2034-2050, 2144-2150)
+    double xmin = 1e300, ymin = 1e300, zmin = 1e300;
+    for (int i = 0; i < nbsphere; i++) {
+        xmin = std::min(xmin, xs[i]);
+        ymin = std::min(ymin, ys[i]);
+        zmin = std::min(zmin, zs[i]);
+    }
+    // object dipoles sit on box sites in the same z, y, x order; a site takes
+    // the next dipole when their positions agree within lambda / 1000
+    // (comparaison.f:41-50)
+    const double err = 2.0 * 3.14159265358979323846 / k0 / 1000.0;
+    std::vector<double> px(nw), py(nw), pz(nw);
+    std::vector<int> map(nw, -1);
+    long l = 0, s = 0;
+    for (int i = 1; i <= nzw; i++)
+        for (int j = 1; j <= nyw; j++)
+            for (int k = 1; k <= nxw; k++, s++) {
+                const double x = xmin + (double)(k - nxmp - 1) * aretecube;
+                const double y = ymin + (double)(j - nymp - 1) * aretecube;
+                const double z = zmin + (double)(i - nzmp - 1) * aretecube;
+                px[s] = x;
+                py[s] = y;
+                pz[s] = z;
+                if (l < nbsphere && x >= xs[l] - err && x <= xs[l] + err && y >= ys[l] - err && y <= ys[l] + err &&
+                    z >= zs[l] - err && z <= zs[l] + err)
+                    map[s] = (int)l++;
+            }
+    if (xswf) std::copy(px.begin(), px.end(), xswf);
+    if (yswf) std::copy(py.begin(), py.end(), yswf);
+    if (zswf) std::copy(pz.begin(), pz.end(), zswf);
+    DevBuf<double> dx, dy, dz, a1, a2, dp;
+    DevBuf<int> dmap, beam;
+    DevBuf<double2> ff, ff0, eps, xr, xi, epsw, em;
+    dx.ensure(nw);
+    dy.ensure(nw);
+    dz.ensure(nw);
+    dmap.ensure(nw);
+    ff.ensure(3L * nbsphere);
+    ff0.ensure(3L * nbsphere);
+    eps.ensure((size_t)9 * nmax);
+    xr.ensure(3 * nw);
+    xi.ensure(3 * nw);
+    epsw.ensure((size_t)9 * nw);
+    em.ensure(3 * nw);
+    a1.ensure(1);
+    a2.ensure(1);
+    dp.ensure(1);
+    beam.ensure(1);
+    const int b0 = 0;
+    IFDDA_CUDA(cudaMemcpyAsync(dx.p, px.data(), nw * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(dy.p, py.data(), nw * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(dz.p, pz.data(), nw * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(dmap.p, map.data(), nw * sizeof(int), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(ff.p, FF, 3L * nbsphere * sizeof(double2), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(ff0.p, FF0, 3L * nbsphere * sizeof(double2), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(eps.p, epsilon, (size_t)9 * nmax * sizeof(double2), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(a1.p, &theta, sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(a2.p, &phi, sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(dp.p, &pp, sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(beam.p, &b0, sizeof(int), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemsetAsync(ctx->flag.p, 0, sizeof(int), st));
+    // incident field on every site (ondeplane), then the object's own
+    planewaves_dev((int)nw, dx.p, dy.p, dz.p, k0, make_double2(E0.re, E0.im), 1, beam.p, a1.p, a2.p, dp.p, xr.p,
+                   ctx->flag.p, st);
+    wide_fill_dev(nw, dmap.p, ff.p, ff0.p, eps.p, nmax, xr.p, xi.p, epsw.p, st);
+    if (incident) IFDDA_CUDA(cudaMemcpyAsync(incident, xr.p, 3 * nw * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    // E = E0 + G p on the enlarged box: one FP64 mat-vec (cdmlib.f:2274-2277)
+    Green G;
+    green_build(G, nxw, nyw, nzw, aretecube, k0, st, nquad);
+    MvArgs<double> a = mv_args<double>(G, 1, xi.p, xr.p, xr.p, 3 * nw, ALPHA_NONE, nullptr, 0, nullptr, nullptr);
+    if (!matvec_launch<double>(a, 1, false, st)) throw EngineError{1, "FFT size not supported"};
+    if (local) IFDDA_CUDA(cudaMemcpyAsync(local, xr.p, 3 * nw * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    // macroscopic field with the object's permittivity (identity elsewhere)
+    local_macro_dev((int)nw, nw, epsw.p, xr.p, aretecube, k0, em.p, ctx->flag.p, st);
+    if (macro) IFDDA_CUDA(cudaMemcpyAsync(macro, em.p, 3 * nw * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    int bad = 0;
+    IFDDA_CUDA(cudaMemcpyAsync(&bad, ctx->flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    if (bad) throw EngineError{1, "problem in local-macro: singular 3x3 matrix"};
+    return 0;
+    IFDDA_GUARD_END(ctx, nullptr)
+}
+
 int ifdda_microscope(ifdda_green* g, const double* xs, const double* ys, const double* zs,
                      const ifdda_dcmplx* polarisa, const char* methodeit, double tol,
                      const ifdda_microscope_options* mo, double* image, double* xy, double* kxy, int* ninc,

@@ -145,6 +145,36 @@ void planewaves_dev(int nb, const double* xs, const double* ys, const double* zs
     IFDDA_CUDA(cudaGetLastError());
 }
 
+// Sites of the enlarged box of the wide near field (cdmlib.f:2142-2216):
+// site s holding object dipole l = map[s] takes its incident field, -FF as
+// the source of the mat-vec and its permittivity; the other sites keep the
+// incident wave already in xr, no source and the identity.
+__global__ void k_wide_fill(long nw, const int* __restrict__ map, const double2* __restrict__ ff,
+                            const double2* __restrict__ ff0, const double2* __restrict__ eps, long nmax,
+                            double2* __restrict__ xr, double2* __restrict__ xi, double2* __restrict__ epsw) {
+    for (long s = (long)blockIdx.x * blockDim.x + threadIdx.x; s < nw; s += (long)gridDim.x * blockDim.x) {
+        const int l = map[s];
+        for (int a = 0; a < 3; a++) {
+            if (l >= 0) {
+                xr[3 * s + a] = ff0[3L * l + a];
+                xi[3 * s + a] = make_double2(-ff[3L * l + a].x, -ff[3L * l + a].y);
+            } else {
+                xi[3 * s + a] = make_double2(0, 0);
+            }
+            for (int b = 0; b < 3; b++)
+                epsw[s + nw * (a + 3 * b)] = l >= 0 ? eps[l + nmax * (a + 3 * b)] : make_double2(a == b ? 1.0 : 0.0, 0.0);
+        }
+    }
+}
+
+void wide_fill_dev(long nw, const int* map, const double2* ff, const double2* ff0, const double2* eps, long nmax,
+                   double2* xr, double2* xi, double2* epsw, cudaStream_t st) {
+    const int grid = (int)std::max(1L, std::min<long>((nw + 255) / 256, 148L * 8));
+    count_launch();
+    k_wide_fill<<<grid, 256, 0, st>>>(nw, map, ff, ff0, eps, nmax, xr, xi, epsw);
+    IFDDA_CUDA(cudaGetLastError());
+}
+
 // Compacts an isotropic (nmax,3,3) polarisability to one value per dipole;
 // sets *aniso when any tensor is not a multiple of the identity.
 __global__ void k_pola_compact(const double2* __restrict__ pol, long nb, long nmax, double2* __restrict__ alpha,

@@ -14,6 +14,10 @@ void planewaves_dev(int nb, const double* xs, const double* ys, const double* zs
                     const int* beam, const double* a1, const double* a2, const double* pp, double2* out, int* bad,
                     cudaStream_t st);
 
+// wide near field: fills the enlarged box from the object dipoles (map[s] = l or -1)
+void wide_fill_dev(long nw, const int* map, const double2* ff, const double2* ff0, const double2* eps, long nmax,
+                   double2* xr, double2* xi, double2* epsw, cudaStream_t st);
+
 // one alpha per dipole from an isotropic (nmax,3,3) tensor; *aniso = 1 if not isotropic
 void pola_compact_dev(const double2* pol, long nb, long nmax, double2* alpha, int* aniso, cudaStream_t st);
 

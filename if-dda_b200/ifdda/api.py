@@ -107,6 +107,25 @@ class Context:
                                                   C.byref(ca)))
         return ce.value, ca.value
 
+    def nearfield_wide(self, nx, ny, nz, nxmp, nymp, nzmp, aretecube, k0, xs, ys, zs, FF, FF0, epsilon, nmax, E0,
+                       theta, phi, pp, nquad=0) -> dict:
+        """Wide near field (cdmlib.f:1967-2492) around a solved object:
+        positions xswf/yswf/zswf and the incident, local and macroscopic
+        fields (3 per site) on the box enlarged by nxmp, nymp, nzmp layers."""
+        nw = (nx + 2 * nxmp) * (ny + 2 * nymp) * (nz + 2 * nzmp)
+        xs = np.ascontiguousarray(xs, np.float64)
+        ys = np.ascontiguousarray(ys, np.float64)
+        zs = np.ascontiguousarray(zs, np.float64)
+        px, py, pz = (np.zeros(nw) for _ in range(3))
+        inc, loc, mac = (np.zeros(3 * nw, np.complex128) for _ in range(3))
+        e0 = complex(E0)
+        ff, ff0, eps = _zc(FF), _zc(FF0), _zc(epsilon)
+        self._check(self.lib.ifdda_nearfield_wide(self.h, nx, ny, nz, nxmp, nymp, nzmp, aretecube, k0, nquad,
+                                                  len(xs), nmax, _p(xs), _p(ys), _p(zs), _p(ff), _p(ff0), _p(eps),
+                                                  DComplex(e0.real, e0.imag), theta, phi, pp, _p(px), _p(py),
+                                                  _p(pz), _p(inc), _p(loc), _p(mac)))
+        return dict(xswf=px, yswf=py, zswf=pz, incident=inc, local=loc, macro=mac)
+
     def planewaves(self, xs, ys, zs, k0, E0, beam, a1, a2, pp) -> np.ndarray:
         """FF0 for a batch of plane waves: beam 0 = ondeplane(theta, phi deg),
         1 = ondeplanekxky(kx, ky).  Returns (nrhs, 3*nbsphere)."""

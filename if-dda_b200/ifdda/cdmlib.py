@@ -37,12 +37,15 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
            beam="pwavelinear", theta=0.0, phi=0.0, pp=1.0, incidences=None, P0=1.0, w0=None,
            tolinit=1e-4, methodeit="GPBICG1", polarizability="RR", trope="iso", nproche=0, nrig=0, nquad=0,
            nlocal=1, nmacro=1, nsection=1, precision=0, nlentille=0, ntypemic=1, nside=0, nquicklens=1,
-           nfft2d=128, numaper=0.9, numaperinc=0.5, gross=100.0, zlens=0.0, microscope_batch=0,
+           nfft2d=128, numaper=0.9, numaperinc=0.5, gross=100.0, zlens=0.0, microscope_batch=0, nxmp=0, nymp=0,
+           nzmp=0,
            ctx: Context | None = None, device=0):
     """Rigorous solve of one object for one plane wave (theta, phi, pp) or a
     batch of them (incidences = [(theta, phi, pp), ...]).  nproche follows the
-    GUI convention: 0 -> dipoles inside the object only (inverserig), >= 1 ->
-    the full box (inverserigopt).  precision: 0 plain FP64, 1 FP32 inner
+    GUI convention: 0 -> dipoles inside the object only (inverserig), 1 ->
+    the full box (inverserigopt), >= 2 -> the full box and the wide near
+    field on the box enlarged by nxmp, nymp, nzmp layers (incidentfield_wf,
+    localfield_wf, macroscopicfield_wf, xswf, yswf, zswf).  precision: 0 plain FP64, 1 FP32 inner
     iterations with FP64 refinement.  nlentille = 1 adds the microscope's
     images (Eimagex..z, Eimageincx..z as |E| on nfft2d^2 pixels, xy, kxy,
     kxinc/kyinc); zlens in nm."""
@@ -84,6 +87,7 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
         return _fail("No calculation requested!")
     k0 = 2 * math.pi / lam
     inside = nproche - 1 == -1  # cdmlib.f:627 decrements the GUI value
+    wide = nproche - 1 >= 1     # cdmlib.f:636-640: nprochefft, solved on the full box
     # ---- object (cdmlib.f:661-805) -------------------------------------
     try:
         ani = epsani if trope == "ani" else None
@@ -151,6 +155,15 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
             return out
         FF = np.atleast_2d(r.FF)
         FFloc = np.atleast_2d(r.FFloc)
+        if wide:
+            # ---- wide near field (cdmlib.f:1967-2492) ----------------------
+            wf = [ctx.nearfield_wide(ob.nx, ob.ny, ob.nz, nxmp, nymp, nzmp, ob.aretecube, k0, ob.xs, ob.ys, ob.zs,
+                                     FF[q], ff0[q], ob.epsilon, ob.nmax, E0, t, p, s, nquad)
+                  for q, (t, p, s) in enumerate(inc)]
+            out.update(xswf=wf[0]["xswf"], yswf=wf[0]["yswf"], zswf=wf[0]["zswf"],
+                       incidentfield_wf=np.stack([w["incident"] for w in wf]),
+                       localfield_wf=np.stack([w["local"] for w in wf]),
+                       macroscopicfield_wf=np.stack([w["macro"] for w in wf]))
         # ---- macroscopic field (cdmlib.f:2595-2655) ----------------------
         if nmacro:
             out["macroscopicfield"] = np.stack([ctx.local_macro(ob.nbsphere, ob.nmax, ob.epsilon, FFloc[q],

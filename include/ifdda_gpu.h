@@ -173,6 +173,25 @@ int ifdda_incident_planewaves(ifdda_ctx* ctx, int nbsphere, const double* xs, co
                               double k0, ifdda_dcmplx E0, int nrhs, const int* beam, const double* a1,
                               const double* a2, const double* pp, ifdda_dcmplx* FF0);
 
+/* Wide near field (cdmlib/cdmlib.f:1967-2492, nprochefft >= 1): the fields
+   on the box enlarged by nxmp, nymp, nzmp layers on every side of the
+   object's nx*ny*nz box, after a solve.  Its (nx+2nxmp)(ny+2nymp)(nz+2nzmp)
+   = nw sites run in z, y, x order from the smallest object coordinate minus
+   the layers; a site takes object dipole l (the next one in order) when
+   their positions agree within lambda/1000 (comparaison.f).  The Green
+   spectrum of the enlarged box is built (nquad as for ifdda_green_create_nquad),
+   and one FP64 mat-vec gives E = E0 - A(-FF): incident receives E0 (FF0 at the
+   object's dipoles, the plane wave ondeplane(theta, phi [deg], pp, E0)
+   elsewhere), local the field, macro local_macro of it with the object's
+   epsilon (nmax,3,3) and the identity elsewhere; 3*nw values each (may be
+   NULL), positions in xswf, yswf, zswf (nw values, may be NULL). */
+int ifdda_nearfield_wide(ifdda_ctx* ctx, int nx, int ny, int nz, int nxmp, int nymp, int nzmp, double aretecube,
+                         double k0, int nquad, int nbsphere, int nmax, const double* xs, const double* ys,
+                         const double* zs, const ifdda_dcmplx* FF, const ifdda_dcmplx* FF0,
+                         const ifdda_dcmplx* epsilon, ifdda_dcmplx E0, double theta, double phi, double pp,
+                         double* xswf, double* yswf, double* zswf, ifdda_dcmplx* incident, ifdda_dcmplx* local,
+                         ifdda_dcmplx* macro);
+
 /* Microscope options: the cdmlib arguments that the microscopes read
    (cdmlib/cdmlib.f:3660-3800 with nlentille = 1, nquicklens = 1, nside = 0). */
 typedef struct {

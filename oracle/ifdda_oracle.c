@@ -2499,6 +2499,77 @@ int orc_object_arbitrary(int nx, int ny, int nz, double d, const double *px, con
 }
 
 /* ------------------------------------------------------------------------- */
+/* Wide near field: cdmlib/cdmlib.f:1967-2492 (nprochefft >= 1, nrig = 0,     */
+/* plane wave).  The box enlarged by nxmp, nymp, nzmp layers, the object's    */
+/* dipoles matched to its sites in order with comparaison.f:41-50 (within     */
+/* lambda/1000), xi = -FF there, xr = FF0 there and ondeplane elsewhere, the  */
+/* Green spectrum of the enlarged box, one mat-vec xr -= G xi, then           */
+/* local_macro with epsilon (identity off the object).  Outputs 3*nw values.  */
+/* ------------------------------------------------------------------------- */
+int orc_nearfield_wide(int nx, int ny, int nz, int nxmp, int nymp, int nzmp, double d, double k0,
+                       double lambda, int nquad, int nbsphere, int nmax, const double *xs,
+                       const double *ys, const double *zs, const zc *FF, const zc *FF0,
+                       const zc *epsilon, zc E0, double theta, double phi, double pp, double *xswf,
+                       double *yswf, double *zswf, zc *incident, zc *local, zc *macro) {
+    int nxw = nx + 2 * nxmp, nyw = ny + 2 * nymp, nzw = nz + 2 * nzmp;
+    long nw = (long)nxw * nyw * nzw;
+    double xmin = 1e300, ymin = 1e300, zmin = 1e300;
+    for (int i = 0; i < nbsphere; i++) {
+        xmin = fmin(xmin, xs[i]);
+        ymin = fmin(ymin, ys[i]);
+        zmin = fmin(zmin, zs[i]);
+    }
+    double err = lambda / 1000.0;
+    zc *xi = (zc *)calloc(3 * nw, sizeof(zc));
+    zc *xr = (zc *)calloc(3 * nw, sizeof(zc));
+    zc *eps = (zc *)calloc(9 * nw, sizeof(zc));
+    for (long s = 0; s < nw; s++)
+        for (int a = 0; a < 3; a++) eps[s + nw * (a + 3 * a)] = 1.0;
+    long l = 0, s = 0;
+    for (int i = 1; i <= nzw; i++)
+        for (int j = 1; j <= nyw; j++)
+            for (int k = 1; k <= nxw; k++, s++) {
+                double x = xmin + (double)(k - nxmp - 1) * d;
+                double y = ymin + (double)(j - nymp - 1) * d;
+                double z = zmin + (double)(i - nzmp - 1) * d;
+                xswf[s] = x;
+                yswf[s] = y;
+                zswf[s] = z;
+                if (l < nbsphere && x >= xs[l] - err && x <= xs[l] + err && y >= ys[l] - err &&
+                    y <= ys[l] + err && z >= zs[l] - err && z <= zs[l] + err) {
+                    for (int a = 0; a < 3; a++) {
+                        xi[3 * s + a] = -FF[3 * l + a];
+                        xr[3 * s + a] = FF0[3 * l + a];
+                        for (int b = 0; b < 3; b++)
+                            eps[s + nw * (a + 3 * b)] = epsilon[l + (long)nmax * (a + 3 * b)];
+                    }
+                    l++;
+                } else {
+                    orc_ondeplane(x, y, z, k0, E0, pp, theta, phi, xr + 3 * s);
+                }
+            }
+    memcpy(incident, xr, sizeof(zc) * 3 * nw);
+    zc *G6 = (zc *)malloc(sizeof(zc) * 6 * 8 * nw);
+    if (nquad > 0) orc_greencalculquadfft(nxw, nyw, nzw, nquad, d, k0, G6);
+    else orc_greencalculfft(nxw, nyw, nzw, d, k0, G6);
+    orc_matvec_opt(G6, nxw, nyw, nzw, xi, xr);
+    free(G6);
+    memcpy(local, xr, sizeof(zc) * 3 * nw);
+    int bad = 0;
+    for (long q = 0; q < nw; q++) {
+        zc e[9], loc[3];
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) e[a + 3 * b] = eps[q + nw * (a + 3 * b)];
+        for (int a = 0; a < 3; a++) loc[a] = xr[3 * q + a];
+        bad |= orc_local_macro(loc, macro + 3 * q, e, d, k0, 1);
+    }
+    free(xi);
+    free(xr);
+    free(eps);
+    return bad;
+}
+
+/* ------------------------------------------------------------------------- */
 /* Microscopes in transmission with the FFT lens (nquicklens = 1, nside = +1): */
 /* bright field cdmlib/microsbf.f (ntypemic = 1) and dark field / phase       */
 /* cdmlib/microsdf.f (ntypemic = 2) over the rigorous full-box solve; far     */

@@ -402,3 +402,24 @@ def microscope(ntypemic, G6, nx, ny, nz, d, k0, xs, ys, zs, polarisa, methodeit,
     return dict(image=img.reshape(6, n, n), xy=xy, kxy=kxy, kxinc=kxi[:m].copy(), kyinc=kyi[:m].copy(),
                 tol1=tol1.value, nloop=nloop.value, ncompte=ncompte.value, nstop=nstop,
                 infostr=info.raw[:64].decode(errors="replace"))
+
+
+def nearfield_wide(nx, ny, nz, nxmp, nymp, nzmp, d, k0, lam, nquad, nbsphere, nmax, xs, ys, zs, FF, FF0, epsilon,
+                   E0, theta, phi, pp):
+    """Wide near field (cdmlib/cdmlib.f:1967-2492): returns dict with xswf,
+    yswf, zswf, incident, local, macro on the enlarged box."""
+    nw = (nx + 2 * nxmp) * (ny + 2 * nymp) * (nz + 2 * nzmp)
+    px, py, pz = (np.zeros(nw) for _ in range(3))
+    inc, loc, mac = (np.zeros(3 * nw, np.complex128) for _ in range(3))
+    f = lib().orc_nearfield_wide
+    f.argtypes = [C.c_int] * 6 + [C.c_double] * 3 + [C.c_int] * 3 + [C.c_void_p] * 6 + [_ZC] + \
+        [C.c_double] * 3 + [C.c_void_p] * 6
+    f.restype = C.c_int
+    e0 = complex(E0)
+    rc = f(nx, ny, nz, nxmp, nymp, nzmp, d, k0, lam, nquad, nbsphere, nmax,
+           _p(np.ascontiguousarray(xs, np.float64)), _p(np.ascontiguousarray(ys, np.float64)),
+           _p(np.ascontiguousarray(zs, np.float64)), _p(_z(FF)), _p(_z(FF0)), _p(_z(epsilon)),
+           _ZC(e0.real, e0.imag), theta, phi, pp, _p(px), _p(py), _p(pz), _p(inc), _p(loc), _p(mac))
+    if rc:
+        raise ValueError("nearfield_wide: singular local-macro matrix")
+    return dict(xswf=px, yswf=py, zswf=pz, incident=inc, local=loc, macro=mac)

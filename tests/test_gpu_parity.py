@@ -388,3 +388,39 @@ def test_solve_with_integrated_green_matches_oracle(gctx, orc):
     assert int(r.nloop[0]) == ref["nloop"] and int(r.ncompte[0]) == ref["ncompte"]
     assert rel(r.FFloc, ref["FFloc"]) < 1e-7
     g.close()
+
+
+@pytest.mark.parametrize("nquad", [0, 1])
+def test_wide_near_field_matches_oracle(gctx, orc, nquad):
+    """ifdda_nearfield_wide against the oracle's restatement on the same
+    solved dipole moments (cdmlib.f:1967-2492)."""
+    from ifdda import objects
+    k0 = 2 * math.pi / 632.8e-9
+    ob = objects.sphere(100e-9, 2.25 + 0.1j, 8, k0, "RR", na=0)
+    E0, _ = orc.irradiance(1.0, 6328e-9)
+    ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 0.3, 0, 30.0, 40.0)
+    G = orc.greencalculfft(8, 8, 8, ob.aretecube, k0)
+    sol = orc.inverserig(G, 8, 8, 8, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-8)
+    ref = orc.nearfield_wide(8, 8, 8, 4, 2, 4, ob.aretecube, k0, 632.8e-9, nquad, ob.nbsphere, ob.nmax, ob.xs,
+                             ob.ys, ob.zs, sol["FF"], ff0, ob.epsilon, E0, 30.0, 40.0, 0.3)
+    got = gctx.nearfield_wide(8, 8, 8, 4, 2, 4, ob.aretecube, k0, ob.xs, ob.ys, ob.zs, sol["FF"], ff0, ob.epsilon,
+                              ob.nmax, E0, 30.0, 40.0, 0.3, nquad=nquad)
+    for key in ("xswf", "yswf", "zswf"):
+        assert np.array_equal(got[key], ref[key]), key
+    assert rel(got["incident"], ref["incident"]) < 1e-13
+    assert rel(got["local"], ref["local"]) < 1e-11
+    assert rel(got["macro"], ref["macro"]) < 1e-11
+
+
+def test_cdmlib_wide_near_field(orc):
+    """nproche = 2: full-box solve, then the wide field; on the object's sites
+    the wide local field is the solve's."""
+    from ifdda.cdmlib import cdmlib
+    out = cdmlib(wavelength=632.8, object="sphere", rayon=100.0, eps=2.25 + 0j, nnnr=8, tolinit=1e-8,
+                 methodeit="GPBICG1", nproche=2, nxmp=4, nymp=4, nzmp=4, theta=10.0, phi=0.0, pp=1.0, P0=1.0,
+                 w0=6328.0)
+    assert out["nstop"] == 0, out["infostr"]
+    assert out["nbsphere"] == 512 and len(out["xswf"]) == 16 ** 3
+    sites = [(k + 4) * 256 + (j + 4) * 16 + (i + 4) for k in range(8) for j in range(8) for i in range(8)]
+    loc = out["localfield_wf"][0].reshape(-1, 3)[sites].reshape(-1)
+    assert rel(loc, out["localfield"][0] if out["localfield"].ndim > 1 else out["localfield"]) < 1e-6

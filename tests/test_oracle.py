@@ -341,3 +341,34 @@ def test_anisotropic_objects_match_oracle(orc):
         objects.sphere(100e-9, 0, 10, k0, "PS", epsani=EPSANI)
     with pytest.raises(ValueError):
         orc.object_sphere(100e-9, 0, 10, -1, k0, "PS", epsani=EPSANI)
+
+
+# ---- wide near field (cdmlib.f:1967-2492) ----------------------------------
+def test_wide_near_field_reproduces_the_local_field(orc):
+    """On the object's own sites the wide field E0 + G p is the solve's local
+    field (the linear system itself), to the solve's residual; off the
+    object it is the incident wave plus the scattered one, and the
+    macroscopic field there equals the local one (eps = 1)."""
+    from ifdda import objects
+    k0 = 2 * math.pi / 632.8e-9
+    ob = objects.sphere(100e-9, 2.25 + 0.1j, 6, k0, "RR", na=0)
+    E0, _ = orc.irradiance(1.0, 6328e-9)
+    ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 0.3, 0, 30.0, 40.0)
+    G = orc.greencalculfft(6, 6, 6, ob.aretecube, k0)
+    ref = orc.inverserig(G, 6, 6, 6, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-11)
+    assert ref["nstop"] == 0
+    w = orc.nearfield_wide(6, 6, 6, 2, 3, 1, ob.aretecube, k0, 632.8e-9, 0, ob.nbsphere, ob.nmax, ob.xs, ob.ys,
+                           ob.zs, ref["FF"], ff0, ob.epsilon, E0, 30.0, 40.0, 0.3)
+    nxw, nyw, nzw = 10, 12, 8
+    assert len(w["xswf"]) == nxw * nyw * nzw
+    # object sites: offsets (2, 3, 1) in the enlarged box
+    sites = [(k + 1) * nxw * nyw + (j + 3) * nxw + (i + 2) for k in range(6) for j in range(6) for i in range(6)]
+    loc = w["local"].reshape(-1, 3)[sites].reshape(-1)
+    assert rel(loc, ref["FFloc"]) < 1e-9
+    assert np.allclose(w["xswf"][sites], ob.xs, rtol=0, atol=1e-15)
+    em = orc.local_macro_all(ob.nbsphere, ob.nmax, ob.epsilon, ref["FFloc"], ob.aretecube, k0)
+    assert rel(w["macro"].reshape(-1, 3)[sites].reshape(-1), em) < 1e-9
+    off = np.setdiff1d(np.arange(nxw * nyw * nzw), sites)
+    assert rel(w["macro"].reshape(-1, 3)[off], w["local"].reshape(-1, 3)[off]) < 1e-14
+    inc = orc.incident(w["xswf"][off], w["yswf"][off], w["zswf"][off], k0, E0, 0.3, 0, 30.0, 40.0)
+    assert np.array_equal(w["incident"].reshape(-1, 3)[off].reshape(-1), inc)
