@@ -646,6 +646,61 @@ int ifdda_incident_planewaves(ifdda_ctx* ctx, int nbsphere, const double* xs, co
     IFDDA_GUARD_END(ctx, nullptr)
 }
 
+int ifdda_farfield_csca(ifdda_ctx* ctx, int nbsphere, const double* xs, const double* ys, const double* zs,
+                        const ifdda_dcmplx* FF, double k0, double I0, double theta, double phi, int ntheta, int nphi,
+                        double* Cscai, double* gasym, double* poynting, double* thetafield, double* phifield) {
+    if (!ctx || !xs || !ys || !zs || !FF || !Cscai || !gasym || nbsphere < 1) return 1;
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(ctx->device);
+    AllocStreamScope as(ctx->stream);
+    cudaStream_t st = ctx->stream;
+    if (ntheta <= 10 || nphi <= 20) throw EngineError{1, "ntheta and nphi too small!"};
+    const int ndir = (ntheta + 1) * nphi;
+    DevBuf<double> dx, dy, dz, em;
+    DevBuf<double2> ff, part;
+    dx.ensure(nbsphere);
+    dy.ensure(nbsphere);
+    dz.ensure(nbsphere);
+    ff.ensure(3L * nbsphere);
+    part.ensure((size_t)ndir * farfield_chunks(nbsphere) * 3);
+    em.ensure(ndir);
+    IFDDA_CUDA(cudaMemcpyAsync(dx.p, xs, nbsphere * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(dy.p, ys, nbsphere * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(dz.p, zs, nbsphere * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(ff.p, FF, 3L * nbsphere * sizeof(double2), cudaMemcpyHostToDevice, st));
+    farfield_dev(nbsphere, dx.p, dy.p, dz.p, ff.p, k0, ntheta, nphi, part.p, em.p, st);
+    std::vector<double> emod(ndir);
+    IFDDA_CUDA(cudaMemcpyAsync(emod.data(), em.p, ndir * sizeof(double), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    // the integration of cdmlib.f:2797-2872, in its order
+    const double pi = 3.14159265358979323846, c = 299792458.0, quatpieps0 = 1.0 / (c * c * 1e-7);
+    const double deltatheta = pi / (double)ntheta, deltaphi = 2.0 * pi / (double)nphi;
+    const double k03 = k0 * k0 * k0;
+    double cs = 0.0, g = 0.0;
+    int cnt = 0;
+    for (int itheta = 0; itheta <= ntheta; itheta++) {
+        const double thetas = deltatheta * (double)itheta;
+        for (int iphi = 0; iphi < nphi; iphi++, cnt++) {
+            const double phis = deltaphi * (double)iphi;
+            const double n0 = std::sin(thetas) * std::cos(phis), n1 = std::sin(thetas) * std::sin(phis),
+                         n2 = std::cos(thetas);
+            const double Emod = emod[cnt];
+            if (poynting) poynting[cnt] = Emod * k0 * k0 * k0 * k0 * c / 8 / pi * quatpieps0;
+            if (thetafield) thetafield[cnt] = thetas * 180.0 / pi;
+            if (phifield) phifield[cnt] = phis * 180.0 / pi;
+            cs = cs + deltaphi * deltatheta * std::sin(thetas) * Emod;
+            g = g + deltaphi * deltatheta * std::sin(thetas) * Emod *
+                        (n0 * std::sin(theta * pi / 180.0) * std::cos(phi * pi / 180.0) +
+                         n1 * std::sin(theta * pi / 180.0) * std::sin(phi * pi / 180.0) +
+                         n2 * std::cos(theta * pi / 180.0));
+        }
+    }
+    *gasym = g / cs;
+    *Cscai = cs * k03 * k0 / I0;
+    return 0;
+    IFDDA_GUARD_END(ctx, nullptr)
+}
+
 int ifdda_nearfield_wide(ifdda_ctx* ctx, int nx, int ny, int nz, int nxmp, int nymp, int nzmp, double aretecube,
                          double k0, int nquad, int nbsphere, int nmax, const double* xs, const double* ys,
                          const double* zs, const ifdda_dcmplx* FF, const ifdda_dcmplx* FF0,

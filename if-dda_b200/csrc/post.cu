@@ -145,6 +145,62 @@ void planewaves_dev(int nb, const double* xs, const double* ys, const double* zs
     IFDDA_CUDA(cudaGetLastError());
 }
 
+// Far field by direct summation (cdmlib.f:2803-2836): for direction n(theta,
+// phi) of the (ntheta+1) x nphi grid, E = sum_i exp(-i k0 n.r_i)(p_i -
+// n (n.p_i)).  Stage 1: block (direction, chunk) sums its dipoles; stage 2:
+// one thread per direction adds the chunks in order and returns |E|^2.
+constexpr int FF_NT = 256;
+__global__ void __launch_bounds__(FF_NT) k_farfield_part(int nb, const double* __restrict__ xs,
+                                                         const double* __restrict__ ys, const double* __restrict__ zs,
+                                                         const double2* __restrict__ ff, double k0, int ntheta,
+                                                         int nphi, int nchunk, double2* __restrict__ part) {
+    const int dir = blockIdx.x, ch = blockIdx.y;
+    const double pi = 3.14159265358979323846;
+    const int itheta = dir / nphi, iphi = dir % nphi;
+    const double th = pi / (double)ntheta * (double)itheta, ph = 2.0 * pi / (double)nphi * (double)iphi;
+    const double n0 = sin(th) * cos(ph), n1 = sin(th) * sin(ph), n2 = cos(th);
+    const long per = ((long)nb + nchunk - 1) / nchunk;
+    const long i0 = (long)ch * per, i1 = min((long)nb, i0 + per);
+    double2 acc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+    for (long i = i0 + threadIdx.x; i < i1; i += FF_NT) {
+        double sn, cs;
+        sincos(-k0 * (n0 * xs[i] + n1 * ys[i] + n2 * zs[i]), &sn, &cs);
+        const double2 e = make_double2(cs, sn);
+        const double2 p0 = ff[3 * i], p1 = ff[3 * i + 1], p2 = ff[3 * i + 2];
+        const double2 np = make_double2(n0 * p0.x + n1 * p1.x + n2 * p2.x, n0 * p0.y + n1 * p1.y + n2 * p2.y);
+        acc[0] = zadd(acc[0], zmul(e, make_double2(p0.x - np.x * n0, p0.y - np.y * n0)));
+        acc[1] = zadd(acc[1], zmul(e, make_double2(p1.x - np.x * n1, p1.y - np.y * n1)));
+        acc[2] = zadd(acc[2], zmul(e, make_double2(p2.x - np.x * n2, p2.y - np.y * n2)));
+    }
+    __shared__ double2 scratch[3 * 32];
+    block_sum<FF_NT, 3>(acc, scratch);
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 3; c++) part[((long)dir * nchunk + ch) * 3 + c] = acc[c];
+}
+
+__global__ void k_farfield_final(int ndir, int nchunk, const double2* __restrict__ part, double* __restrict__ emod) {
+    const int dir = blockIdx.x * blockDim.x + threadIdx.x;
+    if (dir >= ndir) return;
+    double2 e[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+    for (int ch = 0; ch < nchunk; ch++)
+        for (int c = 0; c < 3; c++) e[c] = zadd(e[c], part[((long)dir * nchunk + ch) * 3 + c]);
+    emod[dir] = (e[0].x * e[0].x + e[0].y * e[0].y) + (e[1].x * e[1].x + e[1].y * e[1].y) +
+                (e[2].x * e[2].x + e[2].y * e[2].y);
+}
+
+int farfield_chunks(long nb) { return (int)std::max(1L, std::min(256L, (nb + 4095) / 4096)); }
+
+void farfield_dev(int nb, const double* xs, const double* ys, const double* zs, const double2* ff, double k0,
+                  int ntheta, int nphi, double2* part, double* emod, cudaStream_t st) {
+    const int ndir = (ntheta + 1) * nphi, nchunk = farfield_chunks(nb);
+    count_launch();
+    k_farfield_part<<<dim3(ndir, nchunk), FF_NT, 0, st>>>(nb, xs, ys, zs, ff, k0, ntheta, nphi, nchunk, part);
+    IFDDA_CUDA(cudaGetLastError());
+    count_launch();
+    k_farfield_final<<<(ndir + 127) / 128, 128, 0, st>>>(ndir, nchunk, part, emod);
+    IFDDA_CUDA(cudaGetLastError());
+}
+
 // Sites of the enlarged box of the wide near field (cdmlib.f:2142-2216):
 // site s holding object dipole l = map[s] takes its incident field, -FF as
 // the source of the mat-vec and its permittivity; the other sites keep the

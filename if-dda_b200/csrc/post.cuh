@@ -14,6 +14,12 @@ void planewaves_dev(int nb, const double* xs, const double* ys, const double* zs
                     const int* beam, const double* a1, const double* a2, const double* pp, double2* out, int* bad,
                     cudaStream_t st);
 
+// far field |E|^2 on the (ntheta+1) x nphi directions (direction itheta * nphi + iphi);
+// part holds farfield_chunks(nb) * 3 values per direction
+int farfield_chunks(long nb);
+void farfield_dev(int nb, const double* xs, const double* ys, const double* zs, const double2* ff, double k0,
+                  int ntheta, int nphi, double2* part, double* emod, cudaStream_t st);
+
 // wide near field: fills the enlarged box from the object dipoles (map[s] = l or -1)
 void wide_fill_dev(long nw, const int* map, const double2* ff, const double2* ff0, const double2* eps, long nmax,
                    double2* xr, double2* xi, double2* epsw, cudaStream_t st);

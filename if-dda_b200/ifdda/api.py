@@ -107,6 +107,20 @@ class Context:
                                                   C.byref(ca)))
         return ce.value, ca.value
 
+    def farfield_csca(self, xs, ys, zs, FF, k0, I0, theta, phi, ntheta, nphi) -> dict:
+        """Cscai, gasym and the far-field Poynting vector by direct summation
+        over (ntheta+1) x nphi directions (cdmlib.f:2784-2880)."""
+        xs = np.ascontiguousarray(xs, np.float64)
+        ys = np.ascontiguousarray(ys, np.float64)
+        zs = np.ascontiguousarray(zs, np.float64)
+        ff = _zc(FF)
+        nd = (ntheta + 1) * nphi
+        pf, tf, phf = np.zeros(nd), np.zeros(nd), np.zeros(nd)
+        cs, g = C.c_double(0), C.c_double(0)
+        self._check(self.lib.ifdda_farfield_csca(self.h, len(xs), _p(xs), _p(ys), _p(zs), _p(ff), k0, I0, theta, phi,
+                                                 ntheta, nphi, C.byref(cs), C.byref(g), _p(pf), _p(tf), _p(phf)))
+        return dict(Cscai=cs.value, gasym=g.value, poyntingfield=pf, thetafield=tf, phifield=phf)
+
     def nearfield_wide(self, nx, ny, nz, nxmp, nymp, nzmp, aretecube, k0, xs, ys, zs, FF, FF0, epsilon, nmax, E0,
                        theta, phi, pp, nquad=0) -> dict:
         """Wide near field (cdmlib.f:1967-2492) around a solved object:

@@ -11,8 +11,10 @@ options on the rigorous-solve path are implemented (trope 'iso' for every
 object here, trope 'ani' for the sphere and the cube, plane waves, nrig = 0,
 0 <= nquad <= 16), and the bright-field and dark-field microscopes in
 transmission with the FFT lens (nlentille = 1, ntypemic 1 or 2, nside = 0,
-nquicklens = 1, cdmlib.f:3660-3800); anything else returns nstop = 1 with a
-message.
+nquicklens = 1, cdmlib.f:3660-3800), the wide near field (nproche >= 2) and
+the scattering cross section / Poynting vector by direct summation
+(nsectionsca = 1, nquickdiffracte = 0); anything else returns nstop = 1 with
+a message.
 """
 from __future__ import annotations
 
@@ -38,7 +40,7 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
            tolinit=1e-4, methodeit="GPBICG1", polarizability="RR", trope="iso", nproche=0, nrig=0, nquad=0,
            nlocal=1, nmacro=1, nsection=1, precision=0, nlentille=0, ntypemic=1, nside=0, nquicklens=1,
            nfft2d=128, numaper=0.9, numaperinc=0.5, gross=100.0, zlens=0.0, microscope_batch=0, nxmp=0, nymp=0,
-           nzmp=0,
+           nzmp=0, nsectionsca=0, nquickdiffracte=0, ntheta=36, nphi=72,
            ctx: Context | None = None, device=0):
     """Rigorous solve of one object for one plane wave (theta, phi, pp) or a
     batch of them (incidences = [(theta, phi, pp), ...]).  nproche follows the
@@ -72,6 +74,14 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
         return _fail("Tolerance  for the iterative method too large!")
     if object not in _SUPPORTED_OBJECTS:
         return _fail(f"object {object!r} not handled by the GPU drop-in")
+    if nsectionsca:
+        # cdmlib.f:394-400
+        if abs(theta) >= 45.0:
+            return _fail("Angle too strong: Imprecise calculation with FFT")
+        if nquickdiffracte:
+            return _fail("only the direct-sum far field (nquickdiffracte = 0) is handled by the GPU drop-in")
+        if ntheta <= 10 or nphi <= 20:
+            return _fail("ntheta and nphi too small!")
     if nlentille:
         # cdmlib.f:365-389
         if not 0.0 < numaper <= 1.0:
@@ -168,6 +178,13 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
         if nmacro:
             out["macroscopicfield"] = np.stack([ctx.local_macro(ob.nbsphere, ob.nmax, ob.epsilon, FFloc[q],
                                                                 ob.aretecube, k0) for q in range(len(inc))])
+        # ---- Csca, g and Poynting by direct summation (cdmlib.f:2784-2880)
+        if nsectionsca:
+            sc = [ctx.farfield_csca(ob.xs, ob.ys, ob.zs, FF[q], k0, abs(E0) ** 2, t, p, ntheta, nphi)
+                  for q, (t, p, _) in enumerate(inc)]
+            out.update(Cscai=np.array([s["Cscai"] for s in sc]), gasym=np.array([s["gasym"] for s in sc]),
+                       poyntingfield=np.stack([s["poyntingfield"] for s in sc]), thetafield=sc[0]["thetafield"],
+                       phifield=sc[0]["phifield"])
         # ---- cross sections (cdmlib.f:2717-2778) -------------------------
         if nsection:
             cs = [ctx.cross_sections(ff0[q], FF[q], FFloc[q], k0, abs(E0) ** 2) for q in range(len(inc))]

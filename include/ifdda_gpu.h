@@ -173,6 +173,18 @@ int ifdda_incident_planewaves(ifdda_ctx* ctx, int nbsphere, const double* xs, co
                               double k0, ifdda_dcmplx E0, int nrhs, const int* beam, const double* a1,
                               const double* a2, const double* pp, ifdda_dcmplx* FF0);
 
+/* Scattering cross section Cscai, asymmetry factor gasym and far-field
+   Poynting vector by direct summation of the dipole moments FF over the
+   (ntheta+1) x nphi directions (cdmlib/cdmlib.f:2784-2880, nsectionsca = 1,
+   nquickdiffracte = 0); the |E|^2 of every direction on the device, the
+   integration on the host in the reference's order.  theta, phi: incidence
+   (deg) for gasym; I0 = |E0|^2.  poynting, thetafield, phifield ((ntheta+1)
+   nphi values each, may be NULL): the reference's poyntingfield (W/sr) and its
+   angles in degrees.  ntheta <= 10 or nphi <= 20: "ntheta and nphi too small!". */
+int ifdda_farfield_csca(ifdda_ctx* ctx, int nbsphere, const double* xs, const double* ys, const double* zs,
+                        const ifdda_dcmplx* FF, double k0, double I0, double theta, double phi, int ntheta, int nphi,
+                        double* Cscai, double* gasym, double* poynting, double* thetafield, double* phifield);
+
 /* Wide near field (cdmlib/cdmlib.f:1967-2492, nprochefft >= 1): the fields
    on the box enlarged by nxmp, nymp, nzmp layers on every side of the
    object's nx*ny*nz box, after a solve.  Its (nx+2nxmp)(ny+2nymp)(nz+2nzmp)

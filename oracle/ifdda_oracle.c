@@ -2499,6 +2499,50 @@ int orc_object_arbitrary(int nx, int ny, int nz, double d, const double *px, con
 }
 
 /* ------------------------------------------------------------------------- */
+/* Far field by direct summation: cdmlib/cdmlib.f:2784-2880 (nsectionsca = 1, */
+/* nquickdiffracte = 0): Poynting vector on (ntheta+1) x nphi directions,      */
+/* Cscai and the asymmetry factor gasym.  Returns 1 for too few directions.  */
+/* ------------------------------------------------------------------------- */
+int orc_farfield_csca(int nbsphere, const double *xs, const double *ys, const double *zs,
+                      const zc *FF, double k0, double I0, double theta, double phi, int ntheta,
+                      int nphi, double *Cscai, double *gasym, double *poynting, double *thetafield,
+                      double *phifield) {
+    if (ntheta <= 10 || nphi <= 20) return 1;
+    const double pi = acos(-1.0), c = 299792458.0, quatpieps0 = 1.0 / (c * c * 1e-7);
+    double deltatheta = pi / (double)ntheta, deltaphi = 2.0 * pi / (double)nphi;
+    double k03 = k0 * k0 * k0;
+    double cs = 0.0, g = 0.0;
+    int cnt = 0;
+    for (int itheta = 0; itheta <= ntheta; itheta++) {
+        double thetas = deltatheta * (double)itheta;
+        for (int iphi = 0; iphi < nphi; iphi++, cnt++) {
+            double phis = deltaphi * (double)iphi;
+            double n0 = sin(thetas) * cos(phis), n1 = sin(thetas) * sin(phis), n2 = cos(thetas);
+            zc Ex = 0, Ey = 0, Ez = 0;
+            for (int i = 0; i < nbsphere; i++) {
+                zc ctmp = cexp(-I * k0 * (n0 * xs[i] + n1 * ys[i] + n2 * zs[i]));
+                zc ctmp1 = n0 * FF[3 * i] + n1 * FF[3 * i + 1] + n2 * FF[3 * i + 2];
+                Ex += ctmp * (FF[3 * i] - ctmp1 * n0);
+                Ey += ctmp * (FF[3 * i + 1] - ctmp1 * n1);
+                Ez += ctmp * (FF[3 * i + 2] - ctmp1 * n2);
+            }
+            double Emod = creal(Ex * conj(Ex) + Ey * conj(Ey) + Ez * conj(Ez));
+            poynting[cnt] = Emod * k0 * k0 * k0 * k0 * c / 8 / pi * quatpieps0;
+            thetafield[cnt] = thetas * 180.0 / pi;
+            phifield[cnt] = phis * 180.0 / pi;
+            cs = cs + deltaphi * deltatheta * sin(thetas) * Emod;
+            g = g + deltaphi * deltatheta * sin(thetas) * Emod *
+                        (n0 * sin(theta * pi / 180.0) * cos(phi * pi / 180.0) +
+                         n1 * sin(theta * pi / 180.0) * sin(phi * pi / 180.0) +
+                         n2 * cos(theta * pi / 180.0));
+        }
+    }
+    *gasym = g / cs;
+    *Cscai = cs * k03 * k0 / I0;
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
 /* Wide near field: cdmlib/cdmlib.f:1967-2492 (nprochefft >= 1, nrig = 0,     */
 /* plane wave).  The box enlarged by nxmp, nymp, nzmp layers, the object's    */
 /* dipoles matched to its sites in order with comparaison.f:41-50 (within     */

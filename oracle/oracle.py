@@ -423,3 +423,19 @@ def nearfield_wide(nx, ny, nz, nxmp, nymp, nzmp, d, k0, lam, nquad, nbsphere, nm
     if rc:
         raise ValueError("nearfield_wide: singular local-macro matrix")
     return dict(xswf=px, yswf=py, zswf=pz, incident=inc, local=loc, macro=mac)
+
+
+def farfield_csca(xs, ys, zs, FF, k0, I0, theta, phi, ntheta, nphi):
+    """Cscai, gasym and the Poynting vector by direct summation
+    (cdmlib/cdmlib.f:2784-2880)."""
+    nd = (ntheta + 1) * nphi
+    pf, tf, phf = np.zeros(nd), np.zeros(nd), np.zeros(nd)
+    cs, g = C.c_double(0), C.c_double(0)
+    f = lib().orc_farfield_csca
+    f.argtypes = [C.c_int] + [C.c_void_p] * 4 + [C.c_double] * 4 + [C.c_int] * 2 + [C.c_void_p] * 5
+    f.restype = C.c_int
+    xs = np.ascontiguousarray(xs, np.float64)
+    if f(len(xs), _p(xs), _p(np.ascontiguousarray(ys, np.float64)), _p(np.ascontiguousarray(zs, np.float64)),
+         _p(_z(FF)), k0, I0, theta, phi, ntheta, nphi, C.byref(cs), C.byref(g), _p(pf), _p(tf), _p(phf)):
+        raise ValueError("ntheta and nphi too small!")
+    return dict(Cscai=cs.value, gasym=g.value, poyntingfield=pf, thetafield=tf, phifield=phf)

@@ -424,3 +424,36 @@ def test_cdmlib_wide_near_field(orc):
     sites = [(k + 4) * 256 + (j + 4) * 16 + (i + 4) for k in range(8) for j in range(8) for i in range(8)]
     loc = out["localfield_wf"][0].reshape(-1, 3)[sites].reshape(-1)
     assert rel(loc, out["localfield"][0] if out["localfield"].ndim > 1 else out["localfield"]) < 1e-6
+
+
+def test_farfield_csca_matches_oracle(gctx, orc):
+    """ifdda_farfield_csca against the oracle's direct sum on the same dipole
+    moments (cdmlib.f:2784-2880): Poynting per direction, Cscai, gasym."""
+    ob, k0, E0, ff0, G = _c1_inputs(orc)
+    sol = orc.inverserig(G, 16, 16, 16, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-6, tabdip=ob.tabdip)
+    ref = orc.farfield_csca(ob.xs, ob.ys, ob.zs, sol["FF"], k0, E0 ** 2, 20.0, 30.0, 30, 60)
+    got = gctx.farfield_csca(ob.xs, ob.ys, ob.zs, sol["FF"], k0, E0 ** 2, 20.0, 30.0, 30, 60)
+    assert np.array_equal(got["thetafield"], ref["thetafield"]) and np.array_equal(got["phifield"], ref["phifield"])
+    assert rel(got["poyntingfield"], ref["poyntingfield"]) < 1e-12
+    assert abs(got["Cscai"] - ref["Cscai"]) <= 1e-12 * ref["Cscai"]
+    assert abs(got["gasym"] - ref["gasym"]) <= 1e-11 * abs(ref["gasym"])
+    with pytest.raises(ifdda_error()):
+        gctx.farfield_csca(ob.xs, ob.ys, ob.zs, sol["FF"], k0, E0 ** 2, 0.0, 0.0, 10, 60)
+
+
+def ifdda_error():
+    import ifdda
+    return ifdda.IfddaError
+
+
+def test_cdmlib_scattering_cross_section(orc):
+    """nsectionsca = 1 through the cdmlib entry: Cscai agrees with Cext - Cabs
+    (optical theorem) and with Mie within the DDA error."""
+    from ifdda.cdmlib import cdmlib
+    out = cdmlib(wavelength=632.8, object="sphere", rayon=100.0, eps=2.25 + 0j, nnnr=16, tolinit=1e-8,
+                 methodeit="GPBICG1", nproche=0, P0=1.0, w0=6328.0, nsectionsca=1, ntheta=36, nphi=72)
+    assert out["nstop"] == 0, out["infostr"]
+    assert abs(out["Cscai"][0] - out["Csca"][0]) / out["Csca"][0] < 0.02
+    _, mie_sca, _ = orc.mie(2.25, 100e-9, 632.8e-9)
+    assert abs(out["Cscai"][0] - mie_sca) / mie_sca < 0.1
+    assert out["poyntingfield"].shape == (1, 37 * 72)

@@ -372,3 +372,23 @@ def test_wide_near_field_reproduces_the_local_field(orc):
     assert rel(w["macro"].reshape(-1, 3)[off], w["local"].reshape(-1, 3)[off]) < 1e-14
     inc = orc.incident(w["xswf"][off], w["yswf"][off], w["zswf"][off], k0, E0, 0.3, 0, 30.0, 40.0)
     assert np.array_equal(w["incident"].reshape(-1, 3)[off].reshape(-1), inc)
+
+
+# ---- far field by direct summation (cdmlib.f:2784-2880) --------------------
+def test_farfield_csca_matches_mie_and_optical_theorem(orc):
+    """Config 1 sphere: the integrated Cscai is Mie's scattering cross
+    section within the DDA error, equals Cext - Cabs of the same solve (the
+    optical theorem, to the quadrature error), and g lies in (0, 1)."""
+    ob, k0, E0 = c1(16)
+    ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 1.0, 0, 0.0, 0.0)
+    G = orc.greencalculfft(16, 16, 16, ob.aretecube, k0)
+    ref = orc.inverserig(G, 16, 16, 16, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-8, tabdip=ob.tabdip)
+    ff = orc.farfield_csca(ob.xs, ob.ys, ob.zs, ref["FF"], k0, E0 ** 2, 0.0, 0.0, 36, 72)
+    _, mie_sca, _ = orc.mie(2.25, 100e-9, 632.8e-9)
+    assert abs(ff["Cscai"] - mie_sca) / mie_sca < 0.1
+    ce, ca = orc.cross_sections(ff0, ref["FF"], ref["FFloc"], k0, E0 ** 2)
+    assert abs(ff["Cscai"] - (ce - ca)) / (ce - ca) < 0.02
+    assert 0.0 < ff["gasym"] < 1.0
+    assert ff["thetafield"][-1] == 180.0 and ff["phifield"][71] == 355.0
+    with pytest.raises(ValueError):
+        orc.farfield_csca(ob.xs, ob.ys, ob.zs, ref["FF"], k0, E0 ** 2, 0.0, 0.0, 10, 72)
