@@ -701,6 +701,134 @@ int ifdda_farfield_csca(ifdda_ctx* ctx, int nbsphere, const double* xs, const do
     IFDDA_GUARD_END(ctx, nullptr)
 }
 
+int ifdda_farfield_fft(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, const double* xs, const double* ys,
+                       const double* zs, const ifdda_dcmplx* FF, double k0, double I0, double theta, double phi,
+                       int nfft2d, int ntheta, int nphi, double* Cscai, double* gasym, double* poynting,
+                       double* thetafield, double* phifield, int* imaxk0, double* kpos, double* kneg) {
+    if (!ctx || !xs || !ys || !zs || !FF || !Cscai || !gasym || nx < 1 || ny < 1 || nz < 1 || nfft2d < 2) return 1;
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(ctx->device);
+    AllocStreamScope as(ctx->stream);
+    cudaStream_t st = ctx->stream;
+    const double pi = 3.14159265358979323846, c = 299792458.0, quatpieps0 = 1.0 / (c * c * 1e-7);
+    const int n = nfft2d, n2 = n / 2;
+    const long N = (long)nx * ny * nz;
+    // diffractefft2d.f:29-74
+    const double dkx = 2.0 * pi / ((double)n * aretecube), dky = dkx;
+    if (n > 16384) throw EngineError{1, "nfft2d too large"};
+    if (dkx >= k0) throw EngineError{1, "In FFT Poynting nfft2d too small"};
+    const int imax = (int)std::lround(k0 / dkx) + 1, S = 2 * imax + 1;
+    if (S > n || S < 7) throw EngineError{1, "In FFT diffract nfft2d too small"};
+    if (nx > n || ny > n) throw EngineError{1, "nfft2d smaller than the object"};
+    if (ntheta <= 10 || nphi <= 20) throw EngineError{1, "ntheta and nphi too small!"};
+    MicGeom m{};
+    m.nx = nx;
+    m.ny = ny;
+    m.nz = nz;
+    m.n = n;
+    m.imax = imax;
+    m.k0 = k0;
+    m.dkx = dkx;
+    m.dky = dky;
+    m.numaper = k0;
+    m.var1 = (xs[0] + (double)n2 * aretecube) * dkx;
+    m.var2 = (ys[0] + (double)n2 * aretecube) * dky;
+    m.gross = 1.0;
+    std::vector<double> zp(nz);
+    for (int k = 0; k < nz; k++) zp[k] = zs[(long)nx * ny * k];
+    std::vector<double2> twh(n);
+    for (int j = 0; j < n; j++) {
+        const double a = 2.0 * pi * (double)j / (double)n;
+        twh[j] = make_double2(std::cos(a), std::sin(a));
+        if (4 * j == n) twh[j] = make_double2(0.0, 1.0);
+        if (2 * j == n) twh[j] = make_double2(-1.0, 0.0);
+        if (4 * j == 3 * n) twh[j] = make_double2(0.0, -1.0);
+        if (j == 0) twh[j] = make_double2(1.0, 0.0);
+    }
+    DevBuf<double> zpl;
+    DevBuf<double2> ff, tw, Q, Ed;
+    zpl.ensure(nz);
+    tw.ensure(n);
+    ff.ensure(3 * N);
+    Q.ensure((size_t)nz * ny * S * 3);
+    Ed.ensure((size_t)2 * S * S * 3);
+    IFDDA_CUDA(cudaMemcpyAsync(zpl.p, zp.data(), nz * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(tw.p, twh.data(), n * sizeof(double2), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(ff.p, FF, 3 * N * sizeof(double2), cudaMemcpyHostToDevice, st));
+    mic_farfield_dev(m, 1, ff.p, zpl.p, tw.p, Q.p, Ed.p, st, true);
+    std::vector<double2> ed((size_t)2 * S * S * 3);
+    IFDDA_CUDA(cudaMemcpyAsync(ed.data(), Ed.p, ed.size() * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    // |E|^2 at pupil point (i, j) of side s (0: kz > 0, 1: kz < 0), as
+    // cdabs(.)**2 sums
+    auto emod = [&](int s, int i, int j) {
+        const double2* e = ed.data() + (((size_t)s * S + (j + imax)) * S + (i + imax)) * 3;
+        double v = 0.0;
+        for (int q = 0; q < 3; q++) {
+            const double a = std::hypot(e[q].x, e[q].y);
+            v += a * a;
+        }
+        return v;
+    };
+    // Csca and g over the propagating waves (computegcfft2d.f:16-46)
+    const double sth = std::sin(theta * pi / 180.0), cph = std::cos(phi * pi / 180.0),
+                 sph = std::sin(phi * pi / 180.0), cth = std::cos(theta * pi / 180.0);
+    double cs = 0.0, g = 0.0;
+    int k = 0;
+    for (int i = -imax; i <= imax; i++)
+        for (int j = -imax; j <= imax; j++, k++) {
+            const double kx = (double)i * dkx, ky = (double)j * dky;
+            const bool prop = k0 * k0 - kx * kx - ky * ky > 0.0;
+            if (kpos) kpos[k] = 0.0;
+            if (kneg) kneg[k] = 0.0;
+            if (!prop) continue;
+            const double kz = std::sqrt(k0 * k0 - kx * kx - ky * ky);
+            double e = emod(0, i, j);
+            if (kpos) kpos[k] = e * k0 * k0 * k0 * k0 * c / 8 / pi * quatpieps0;
+            cs = cs + dkx * dky * e / kz;
+            g = g + dkx * dky * e / kz * (kx * sth * cph + ky * sth * sph + kz * cth) / k0;
+            e = emod(1, i, j);
+            if (kneg) kneg[k] = e * k0 * k0 * k0 * k0 * c / 8 / pi * quatpieps0;
+            cs = cs + dkx * dky * e / kz;
+            g = g + dkx * dky * e / kz * (kx * sth * cph + ky * sth * sph - kz * cth) / k0;
+        }
+    *gasym = g / cs;
+    *Cscai = cs * (k0 * k0 * k0) / I0;
+    if (imaxk0) *imaxk0 = imax;
+    // Poynting vector on the (theta, phi) grid by bilinear interpolation of the
+    // pupil grid (cdmlib.f:2990-3075), the reference's zero-count fallback
+    // included
+    const double deltatheta = pi / (double)ntheta, deltaphi = 2.0 * pi / (double)nphi;
+    int cnt = 0;
+    for (int itheta = 0; itheta <= ntheta; itheta++) {
+        const double thetas = deltatheta * (double)itheta;
+        for (int iphi = 0; iphi < nphi; iphi++, cnt++) {
+            const double phis = deltaphi * (double)iphi;
+            if (thetafield) thetafield[cnt] = thetas * 180.0 / pi;
+            if (phifield) phifield[cnt] = phis * 180.0 / pi;
+            const double kx = k0 * std::sin(thetas) * std::cos(phis), ky = k0 * std::sin(thetas) * std::sin(phis);
+            int i2 = -imax, j2 = -imax;
+            for (int i = -imax; i <= imax; i++)
+                if (kx >= i * dkx) i2 = i;
+            for (int j = -imax; j <= imax; j++)
+                if (ky >= j * dkx) j2 = j;
+            const int s = thetas <= pi / 2.0 ? 0 : 1;
+            const double e11 = emod(s, i2, j2), e22 = emod(s, i2 + 1, j2 + 1), e21 = emod(s, i2 + 1, j2),
+                         e12 = emod(s, i2, j2 + 1);
+            const int test = (e11 == 0.0) + (e22 == 0.0) + (e21 == 0.0) + (e12 == 0.0);
+            double e;
+            if (test == 0)
+                e = (e21 - e11) * (kx - dkx * i2) / dkx + (e12 - e11) * (ky - dkx * j2) / dkx +
+                    (e11 + e22 - e12 - e21) * (kx - dkx * i2) / dkx * (ky - dkx * j2) / dkx + e11;
+            else
+                e = (e11 + e12 + e21 + e22) / (double)(4 - test);
+            if (poynting) poynting[cnt] = e * k0 * k0 * k0 * k0 * c / 8.0 / pi * quatpieps0;
+        }
+    }
+    return 0;
+    IFDDA_GUARD_END(ctx, nullptr)
+}
+
 int ifdda_nearfield_wide(ifdda_ctx* ctx, int nx, int ny, int nz, int nxmp, int nymp, int nzmp, double aretecube,
                          double k0, int nquad, int nbsphere, int nmax, const double* xs, const double* ys,
                          const double* zs, const ifdda_dcmplx* FF, const ifdda_dcmplx* FF0,

@@ -70,6 +70,29 @@ __global__ void __launch_bounds__(256) k_mic_xdft(const MicGeom m, int nb, const
     q[2] = a2;
 }
 
+// y-DFT of plane k at pupil column irow: P_c = sum_y Q[b][k][y][irow][c]
+// exp(-2 pi i j (y - n/2) / n), with ph0 / step the phase index of y = 0 and
+// its increment
+__device__ __forceinline__ void ydft_plane(const MicGeom& m, const double2* __restrict__ Q, const double2* __restrict__ tw,
+                                           int b, int k, int irow, int ph0, int step, double2& p0, double2& p1,
+                                           double2& p2) {
+    const int S = m.S(), n = m.n;
+    const double2* q = Q + (((long)b * m.nz + k) * m.ny * S + irow) * 3;
+    p0 = make_double2(0, 0);
+    p1 = p0;
+    p2 = p0;
+    int ph = ph0;
+    for (int y = 0; y < m.ny; y++) {
+        const double2 w = cconj(tw[ph]);
+        const double2* qy = q + (long)y * S * 3;
+        p0 = cadd(p0, cmul(qy[0], w));
+        p1 = cadd(p1, cmul(qy[1], w));
+        p2 = cadd(p2, cmul(qy[2], w));
+        ph += step;
+        if (ph >= n) ph -= n;
+    }
+}
+
 // y-DFT and the sum over planes (diffractefft2dlens.f:121-150): inside the
 // pupil (kx^2 + ky^2 < numaper^2)
 //   Ed_c = k0^2 sum_k (P_c - k_c (k.P) / k0^2) exp(-i kz z_k)
@@ -97,18 +120,8 @@ __global__ void __launch_bounds__(256) k_mic_far(const MicGeom m, int nb, const 
         const double2 den = make_double2(0.0, -2.0 * 3.14159265358979323846 * kz);
         const int step = posmod(j, n), ph0 = posmod((long)j * (-(n / 2)), n);
         for (int k = 0; k < m.nz; k++) {
-            const double2* q = Q + (((long)b * m.nz + k) * m.ny * S + irow) * 3;
-            double2 p0 = make_double2(0, 0), p1 = p0, p2 = p0;
-            int ph = ph0;
-            for (int y = 0; y < m.ny; y++) {
-                const double2 w = cconj(tw[ph]);
-                const double2* qy = q + (long)y * S * 3;
-                p0 = cadd(p0, cmul(qy[0], w));
-                p1 = cadd(p1, cmul(qy[1], w));
-                p2 = cadd(p2, cmul(qy[2], w));
-                ph += step;
-                if (ph >= n) ph -= n;
-            }
+            double2 p0, p1, p2;
+            ydft_plane(m, Q, tw, b, k, irow, ph0, step, p0, p1, p2);
             // ctmp = (kx P_x + ky P_y + kz P_z) / k0
             const double2 ct = make_double2((kx * p0.x + ky * p1.x + kz * p2.x) / m.k0,
                                             (kx * p0.y + ky * p1.y + kz * p2.y) / m.k0);
@@ -127,6 +140,58 @@ __global__ void __launch_bounds__(256) k_mic_far(const MicGeom m, int nb, const 
     e[0] = o0;
     e[1] = o1;
     e[2] = o2;
+}
+
+// Far field on both sides without a lens (diffractefft2d.f:104-170): for
+// every propagating wave (k0^2 - kx^2 - ky^2 > 0) the sums over planes
+//   E+_c = sum_k (P_c - k+_c (k+.P) / k0^2) exp(-i kz z_k) exp(-i (var1 i + var2 j))
+//   E-_c = sum_k (P_c - k-_c (k-.P) / k0^2) exp(+i kz z_k) exp(-i (var1 i + var2 j))
+// with k+- = (kx, ky, +-kz); Ed holds E+ for all nb, then E-.
+__global__ void __launch_bounds__(256) k_mic_far2(const MicGeom m, int nb, const double2* __restrict__ Q,
+                                                   const double* __restrict__ zplane, const double2* __restrict__ tw,
+                                                   double2* __restrict__ Ed) {
+    const int S = m.S();
+    const long total = (long)nb * S * S;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int irow = (int)(t % S);
+    const int jrow = (int)((t / S) % S);
+    const int b = (int)(t / ((long)S * S));
+    const int i = irow - m.imax, j = jrow - m.imax, n = m.n;
+    const double kx = (double)i * m.dkx, ky = (double)j * m.dky;
+    double2 a0 = make_double2(0, 0), a1 = a0, a2 = a0, c0 = a0, c1 = a0, c2 = a0;
+    const double kz2 = __dsub_rn(__dsub_rn(__dmul_rn(m.k0, m.k0), __dmul_rn(kx, kx)), __dmul_rn(ky, ky));
+    if (kz2 > 0.0) {
+        const double kz = sqrt(kz2);
+        double sn, cs;
+        sincos(-__dadd_rn(__dmul_rn(m.var1, (double)i), __dmul_rn(m.var2, (double)j)), &sn, &cs);
+        const double2 exy = make_double2(cs, sn);
+        const int step = posmod(j, n), ph0 = posmod((long)j * (-(n / 2)), n);
+        for (int k = 0; k < m.nz; k++) {
+            double2 p0, p1, p2;
+            ydft_plane(m, Q, tw, b, k, irow, ph0, step, p0, p1, p2);
+            sincos(kz * zplane[k], &sn, &cs);
+            const double2 up = cmul(make_double2(cs, -sn), exy), dn = cmul(make_double2(cs, sn), exy);
+            const double2 tp = make_double2((kx * p0.x + ky * p1.x + kz * p2.x) / m.k0,
+                                            (kx * p0.y + ky * p1.y + kz * p2.y) / m.k0);
+            const double2 tn = make_double2((kx * p0.x + ky * p1.x - kz * p2.x) / m.k0,
+                                            (kx * p0.y + ky * p1.y - kz * p2.y) / m.k0);
+            a0 = cadd(a0, cmul(csub(p0, make_double2(kx * tp.x / m.k0, kx * tp.y / m.k0)), up));
+            a1 = cadd(a1, cmul(csub(p1, make_double2(ky * tp.x / m.k0, ky * tp.y / m.k0)), up));
+            a2 = cadd(a2, cmul(csub(p2, make_double2(kz * tp.x / m.k0, kz * tp.y / m.k0)), up));
+            c0 = cadd(c0, cmul(csub(p0, make_double2(kx * tn.x / m.k0, kx * tn.y / m.k0)), dn));
+            c1 = cadd(c1, cmul(csub(p1, make_double2(ky * tn.x / m.k0, ky * tn.y / m.k0)), dn));
+            c2 = cadd(c2, cmul(cadd(p2, make_double2(kz * tn.x / m.k0, kz * tn.y / m.k0)), dn));
+        }
+    }
+    double2* e = Ed + (((long)b * S + jrow) * S + irow) * 3;
+    e[0] = a0;
+    e[1] = a1;
+    e[2] = a2;
+    double2* f = e + (long)nb * S * S * 3;
+    f[0] = c0;
+    f[1] = c1;
+    f[2] = c2;
 }
 
 // The lens (microsbf.f:699-795, microsdf.f:677-766): focus phase
@@ -333,13 +398,14 @@ bool image_length_supported(int n) {
 }
 
 void mic_farfield_dev(const MicGeom& m, int nb, const double2* FF, const double* zplane, const double2* tw,
-                      double2* Q, double2* Ed, cudaStream_t st) {
+                      double2* Q, double2* Ed, cudaStream_t st, bool both_sides) {
     const long nq = (long)nb * m.nz * m.ny * m.S(), ne = (long)nb * m.S() * m.S();
     count_launch();
     k_mic_xdft<<<(unsigned)((nq + 255) / 256), 256, 0, st>>>(m, nb, FF, tw, Q);
     IFDDA_CUDA(cudaGetLastError());
     count_launch();
-    k_mic_far<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(m, nb, Q, zplane, tw, Ed);
+    if (both_sides) k_mic_far2<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(m, nb, Q, zplane, tw, Ed);
+    else k_mic_far<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(m, nb, Q, zplane, tw, Ed);
     IFDDA_CUDA(cudaGetLastError());
 }
 

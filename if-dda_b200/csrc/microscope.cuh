@@ -30,8 +30,10 @@ struct MicGeom {
 // Far field Ed (nb x S x S x 3, entry ((b S + jrow) S + irow) 3 + c) of the
 // dipole moments FF (nb vectors of 3 nx ny nz, full box).  zplane: z of each
 // lattice plane; tw: exp(+2 pi i m / n), m < n; Q: nb nz ny S 3 scratch.
+// both_sides: the lens-free far field of diffractefft2d.f on the kz > 0
+// side, then the kz < 0 side (2 nb S S 3 values), instead of the lens's.
 void mic_farfield_dev(const MicGeom& m, int nb, const double2* FF, const double* zplane, const double2* tw,
-                      double2* Q, double2* Ed, cudaStream_t st);
+                      double2* Q, double2* Ed, cudaStream_t st, bool both_sides = false);
 // Fourier-plane fields F (nb x 6 x S x S: x, y, z, then with the incident
 // wave) after the lens: focus phase, the specular wave at grid point
 // (ik[b], jk[b]) with polarisation pp[b], and the rotation by the lens.

@@ -8,6 +8,7 @@ a failing library call (bad argument, CUDA error) raises IfddaError.
 from __future__ import annotations
 
 import ctypes as C
+import math
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -120,6 +121,27 @@ class Context:
         self._check(self.lib.ifdda_farfield_csca(self.h, len(xs), _p(xs), _p(ys), _p(zs), _p(ff), k0, I0, theta, phi,
                                                  ntheta, nphi, C.byref(cs), C.byref(g), _p(pf), _p(tf), _p(phf)))
         return dict(Cscai=cs.value, gasym=g.value, poyntingfield=pf, thetafield=tf, phifield=phf)
+
+    def farfield_fft(self, nx, ny, nz, aretecube, xs, ys, zs, FF, k0, I0, theta, phi, nfft2d, ntheta, nphi) -> dict:
+        """Cscai, gasym and the Poynting vector from the far field on the
+        pupil grid of nfft2d (diffractefft2d.f, computegcfft2d.f,
+        cdmlib.f:2990-3075); FF on the full box."""
+        xs = np.ascontiguousarray(xs, np.float64)
+        ys = np.ascontiguousarray(ys, np.float64)
+        zs = np.ascontiguousarray(zs, np.float64)
+        ff = _zc(FF)
+        nd = (ntheta + 1) * nphi
+        pf, tf, phf = np.zeros(nd), np.zeros(nd), np.zeros(nd)
+        imax = int(round(k0 * nfft2d * aretecube / (2 * math.pi))) + 2
+        S = 2 * imax + 1
+        kp, kn = np.zeros(S * S), np.zeros(S * S)
+        cs, g, im = C.c_double(0), C.c_double(0), C.c_int(0)
+        self._check(self.lib.ifdda_farfield_fft(self.h, nx, ny, nz, aretecube, _p(xs), _p(ys), _p(zs), _p(ff), k0, I0,
+                                                theta, phi, nfft2d, ntheta, nphi, C.byref(cs), C.byref(g), _p(pf),
+                                                _p(tf), _p(phf), C.byref(im), _p(kp), _p(kn)))
+        S = 2 * im.value + 1
+        return dict(Cscai=cs.value, gasym=g.value, poyntingfield=pf, thetafield=tf, phifield=phf, imaxk0=im.value,
+                    kpos=kp[:S * S].copy(), kneg=kn[:S * S].copy())
 
     def nearfield_wide(self, nx, ny, nz, nxmp, nymp, nzmp, aretecube, k0, xs, ys, zs, FF, FF0, epsilon, nmax, E0,
                        theta, phi, pp, nquad=0) -> dict:

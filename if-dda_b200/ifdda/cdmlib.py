@@ -12,9 +12,10 @@ object here, trope 'ani' for the sphere and the cube, plane waves, nrig = 0,
 0 <= nquad <= 16), and the bright-field and dark-field microscopes in
 transmission with the FFT lens (nlentille = 1, ntypemic 1 or 2, nside = 0,
 nquicklens = 1, cdmlib.f:3660-3800), the wide near field (nproche >= 2) and
-the scattering cross section / Poynting vector by direct summation
-(nsectionsca = 1, nquickdiffracte = 0); anything else returns nstop = 1 with
-a message.
+the scattering cross section / asymmetry factor / Poynting vector
+(nsectionsca = 1, by direct summation or, with nquickdiffracte = 1, from the
+far field on the nfft2d pupil grid); anything else returns nstop = 1 with a
+message.
 """
 from __future__ import annotations
 
@@ -78,10 +79,10 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
         # cdmlib.f:394-400
         if abs(theta) >= 45.0:
             return _fail("Angle too strong: Imprecise calculation with FFT")
-        if nquickdiffracte:
-            return _fail("only the direct-sum far field (nquickdiffracte = 0) is handled by the GPU drop-in")
         if ntheta <= 10 or nphi <= 20:
             return _fail("ntheta and nphi too small!")
+    if nquickdiffracte:
+        nproche = max(nproche, 1)  # the FFT far field needs the full box (cdmlib.f:630)
     if nlentille:
         # cdmlib.f:365-389
         if not 0.0 < numaper <= 1.0:
@@ -180,8 +181,12 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
                                                                 ob.aretecube, k0) for q in range(len(inc))])
         # ---- Csca, g and Poynting by direct summation (cdmlib.f:2784-2880)
         if nsectionsca:
-            sc = [ctx.farfield_csca(ob.xs, ob.ys, ob.zs, FF[q], k0, abs(E0) ** 2, t, p, ntheta, nphi)
-                  for q, (t, p, _) in enumerate(inc)]
+            if nquickdiffracte:
+                sc = [ctx.farfield_fft(ob.nx, ob.ny, ob.nz, ob.aretecube, ob.xs, ob.ys, ob.zs, FF[q], k0,
+                                       abs(E0) ** 2, t, p, nfft2d, ntheta, nphi) for q, (t, p, _) in enumerate(inc)]
+            else:
+                sc = [ctx.farfield_csca(ob.xs, ob.ys, ob.zs, FF[q], k0, abs(E0) ** 2, t, p, ntheta, nphi)
+                      for q, (t, p, _) in enumerate(inc)]
             out.update(Cscai=np.array([s["Cscai"] for s in sc]), gasym=np.array([s["gasym"] for s in sc]),
                        poyntingfield=np.stack([s["poyntingfield"] for s in sc]), thetafield=sc[0]["thetafield"],
                        phifield=sc[0]["phifield"])

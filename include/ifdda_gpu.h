@@ -185,6 +185,22 @@ int ifdda_farfield_csca(ifdda_ctx* ctx, int nbsphere, const double* xs, const do
                         const ifdda_dcmplx* FF, double k0, double I0, double theta, double phi, int ntheta, int nphi,
                         double* Cscai, double* gasym, double* poynting, double* thetafield, double* phifield);
 
+/* The same quantities from the far field on the pupil grid (nsectionsca = 1,
+   nquickdiffracte = 1): diffractefft2d (cdmlib/diffractefft2d.f:1-183) on
+   both sides, evaluated on the device at the (2 imaxk0 + 1)^2 propagating
+   frequencies (i dk, j dk), dk = 2 pi / (nfft2d aretecube), imaxk0 =
+   nint(k0 / dk) + 1; Cscai and gasym by computegcfft2d
+   (cdmlib/computegcfft2d.f:1-51); poynting on the (ntheta+1) x nphi grid by
+   the reference's bilinear interpolation (cdmlib/cdmlib.f:2990-3075).  FF
+   on the full nx*ny*nz box (cdmlib.f:630 forces it).  kpos / kneg ((2 imaxk0
+   + 1)^2 values, index (i + imaxk0)(2 imaxk0 + 1) + j + imaxk0, may be NULL):
+   the Poynting vector on the pupil grid for kz > 0 and kz < 0.  Any nfft2d up
+   to 16384 (the sums are evaluated at the pupil frequencies only). */
+int ifdda_farfield_fft(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, const double* xs, const double* ys,
+                       const double* zs, const ifdda_dcmplx* FF, double k0, double I0, double theta, double phi,
+                       int nfft2d, int ntheta, int nphi, double* Cscai, double* gasym, double* poynting,
+                       double* thetafield, double* phifield, int* imaxk0, double* kpos, double* kneg);
+
 /* Wide near field (cdmlib/cdmlib.f:1967-2492, nprochefft >= 1): the fields
    on the box enlarged by nxmp, nymp, nzmp layers on every side of the
    object's nx*ny*nz box, after a solve.  Its (nx+2nxmp)(ny+2nymp)(nz+2nzmp)

@@ -2894,6 +2894,123 @@ int orc_microscope(int ntypemic, const zc *G6, int nx, int ny, int nz, double d,
     return 0;
 }
 
+/* ------------------------------------------------------------------------- */
+/* Far field on the pupil grid: diffractefft2d.f:1-183 (both sides, full box), */
+/* computegcfft2d.f:1-51 (Cscai, gasym) and the Poynting interpolation of     */
+/* cdmlib.f:2990-3075 (nsectionsca = 1, nquickdiffracte = 1).                 */
+/* ------------------------------------------------------------------------- */
+int orc_farfield_fft(int nx, int ny, int nz, double d, const double *xs, const double *ys,
+                     const double *zs, const zc *FF, double k0, double I0, double theta, double phi,
+                     int n, int ntheta, int nphi, double *Cscai, double *gasym, double *poynting,
+                     double *thetafield, double *phifield, int *imax_out, double *kpos, double *kneg,
+                     char *infostr) {
+    const double pi = acos(-1.0), c = 299792458.0, quatpieps0 = 1.0 / (c * c * 1e-7);
+    double dkx = 2.0 * pi / ((double)n * d), dky = dkx;
+    int n2 = n / 2;
+    double var1 = (xs[0] + (double)n2 * d) * dkx, var2 = (ys[0] + (double)n2 * d) * dky;
+    if (n > 16384) { set_info(infostr, "nfft2d too large"); return 1; }
+    if (dkx >= k0) { set_info(infostr, "In FFT Poynting nfft2d too small"); return 1; }
+    int imax = (int)lround(k0 / dkx) + 1, S = 2 * imax + 1;
+    if (S > n || S < 7) { set_info(infostr, "In FFT diffract nfft2d too small"); return 1; }
+    if (ntheta <= 10 || nphi <= 20) { set_info(infostr, "ntheta and nphi too small!"); return 1; }
+    zc *Ep = (zc *)calloc((size_t)S * S * 3, sizeof(zc)), *En = (zc *)calloc((size_t)S * S * 3, sizeof(zc));
+    zc *E = (zc *)malloc(sizeof(zc) * 3 * (size_t)n * n);
+    for (int k = 1; k <= nz; k++) {
+        memset(E, 0, sizeof(zc) * 3 * (size_t)n * n);
+        for (int i = 1; i <= nx; i++)
+            for (int j = 1; j <= ny; j++) {
+                long kk = i + (long)nx * (j - 1) + (long)nx * ny * (k - 1);
+                long ind = (orc_tabfft2(i, n) - 1) + (long)n * (orc_tabfft2(j, n) - 1);
+                for (int q = 0; q < 3; q++) E[q * (size_t)n * n + ind] = FF[3 * (kk - 1) + q];
+            }
+        for (int q = 0; q < 3; q++) orc_fft3d(E + q * (size_t)n * n, n, n, 1, -1);
+        long kk = 1 + (long)nx * ny * (k - 1);
+        for (int i = -imax; i <= imax; i++)
+            for (int j = -imax; j <= imax; j++) {
+                double kx = (double)i * dkx, ky = (double)j * dky;
+                if (!(k0 * k0 - kx * kx - ky * ky > 0.0)) continue;
+                double kz = sqrt(k0 * k0 - kx * kx - ky * ky);
+                long ind = (orc_tabfft2(i + n2 + 1, n) - 1) + (long)n * (orc_tabfft2(j + n2 + 1, n) - 1);
+                zc ex = E[ind], ey = E[(size_t)n * n + ind], ez = E[2 * (size_t)n * n + ind];
+                zc ph = cexp(-I * (var1 * i + var2 * j));
+                zc ctmp = (kx * ex + ky * ey + kz * ez) / k0;
+                zc ctmp1 = cexp(-I * kz * zs[kk - 1]) * ph;
+                zc *o = Ep + ((size_t)(imax + j) * S + (imax + i)) * 3;
+                o[0] += (ex - kx * ctmp / k0) * ctmp1;
+                o[1] += (ey - ky * ctmp / k0) * ctmp1;
+                o[2] += (ez - kz * ctmp / k0) * ctmp1;
+                ctmp = (kx * ex + ky * ey - kz * ez) / k0;
+                ctmp1 = cexp(I * kz * zs[kk - 1]) * ph;
+                o = En + ((size_t)(imax + j) * S + (imax + i)) * 3;
+                o[0] += (ex - kx * ctmp / k0) * ctmp1;
+                o[1] += (ey - ky * ctmp / k0) * ctmp1;
+                o[2] += (ez + kz * ctmp / k0) * ctmp1;
+            }
+    }
+    free(E);
+#define EMOD(A, i, j)                                                                           \
+    (cabs((A)[((size_t)(imax + (j)) * S + (imax + (i))) * 3]) *                                 \
+         cabs((A)[((size_t)(imax + (j)) * S + (imax + (i))) * 3]) +                             \
+     cabs((A)[((size_t)(imax + (j)) * S + (imax + (i))) * 3 + 1]) *                             \
+         cabs((A)[((size_t)(imax + (j)) * S + (imax + (i))) * 3 + 1]) +                         \
+     cabs((A)[((size_t)(imax + (j)) * S + (imax + (i))) * 3 + 2]) *                             \
+         cabs((A)[((size_t)(imax + (j)) * S + (imax + (i))) * 3 + 2]))
+    double sth = sin(theta * pi / 180.0), cph = cos(phi * pi / 180.0), sph = sin(phi * pi / 180.0),
+           cth = cos(theta * pi / 180.0);
+    double cs = 0.0, g = 0.0;
+    int k = 0;
+    for (int i = -imax; i <= imax; i++)
+        for (int j = -imax; j <= imax; j++, k++) {
+            double kx = (double)i * dkx, ky = (double)j * dky;
+            kpos[k] = 0.0;
+            kneg[k] = 0.0;
+            if (!(k0 * k0 - kx * kx - ky * ky > 0.0)) continue;
+            double kz = sqrt(k0 * k0 - kx * kx - ky * ky);
+            double e = EMOD(Ep, i, j);
+            kpos[k] = e * k0 * k0 * k0 * k0 * c / 8 / pi * quatpieps0;
+            cs = cs + dkx * dky * e / kz;
+            g = g + dkx * dky * e / kz * (kx * sth * cph + ky * sth * sph + kz * cth) / k0;
+            e = EMOD(En, i, j);
+            kneg[k] = e * k0 * k0 * k0 * k0 * c / 8 / pi * quatpieps0;
+            cs = cs + dkx * dky * e / kz;
+            g = g + dkx * dky * e / kz * (kx * sth * cph + ky * sth * sph - kz * cth) / k0;
+        }
+    *gasym = g / cs;
+    *Cscai = cs * (k0 * k0 * k0) / I0;
+    *imax_out = imax;
+    double deltatheta = pi / (double)ntheta, deltaphi = 2.0 * pi / (double)nphi;
+    int cnt = 0;
+    for (int itheta = 0; itheta <= ntheta; itheta++) {
+        double thetas = deltatheta * (double)itheta;
+        for (int iphi = 0; iphi < nphi; iphi++, cnt++) {
+            double phis = deltaphi * (double)iphi;
+            thetafield[cnt] = thetas * 180.0 / pi;
+            phifield[cnt] = phis * 180.0 / pi;
+            double kx = k0 * sin(thetas) * cos(phis), ky = k0 * sin(thetas) * sin(phis);
+            int i2 = -imax, j2 = -imax;
+            for (int i = -imax; i <= imax; i++)
+                if (kx >= i * dkx) i2 = i;
+            for (int j = -imax; j <= imax; j++)
+                if (ky >= j * dkx) j2 = j;
+            zc *A = thetas <= pi / 2.0 ? Ep : En;
+            double e11 = EMOD(A, i2, j2), e22 = EMOD(A, i2 + 1, j2 + 1), e21 = EMOD(A, i2 + 1, j2),
+                   e12 = EMOD(A, i2, j2 + 1);
+            int test = (e11 == 0.0) + (e22 == 0.0) + (e21 == 0.0) + (e12 == 0.0);
+            double e;
+            if (test == 0)
+                e = (e21 - e11) * (kx - dkx * i2) / dkx + (e12 - e11) * (ky - dkx * j2) / dkx +
+                    (e11 + e22 - e12 - e21) * (kx - dkx * i2) / dkx * (ky - dkx * j2) / dkx + e11;
+            else
+                e = (e11 + e12 + e21 + e22) / (double)(4 - test);
+            poynting[cnt] = e * k0 * k0 * k0 * k0 * c / 8.0 / pi * quatpieps0;
+        }
+    }
+#undef EMOD
+    free(Ep);
+    free(En);
+    return 0;
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -439,3 +439,26 @@ def farfield_csca(xs, ys, zs, FF, k0, I0, theta, phi, ntheta, nphi):
          _p(_z(FF)), k0, I0, theta, phi, ntheta, nphi, C.byref(cs), C.byref(g), _p(pf), _p(tf), _p(phf)):
         raise ValueError("ntheta and nphi too small!")
     return dict(Cscai=cs.value, gasym=g.value, poyntingfield=pf, thetafield=tf, phifield=phf)
+
+
+def farfield_fft(nx, ny, nz, d, xs, ys, zs, FF, k0, I0, theta, phi, nfft2d, ntheta, nphi):
+    """Cscai, gasym and the Poynting vector from the pupil-grid far field
+    (diffractefft2d.f, computegcfft2d.f, cdmlib.f:2990-3075)."""
+    nd = (ntheta + 1) * nphi
+    pf, tf, phf = np.zeros(nd), np.zeros(nd), np.zeros(nd)
+    kmax = nfft2d * nfft2d
+    kp, kn = np.zeros(kmax), np.zeros(kmax)
+    cs, g, imax = C.c_double(0), C.c_double(0), C.c_int(0)
+    info = C.create_string_buffer(b" " * 64, 65)
+    f = lib().orc_farfield_fft
+    f.argtypes = [C.c_int] * 3 + [C.c_double] + [C.c_void_p] * 4 + [C.c_double] * 4 + [C.c_int] * 3 + \
+        [C.c_void_p] * 5 + [C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p]
+    f.restype = C.c_int
+    rc = f(nx, ny, nz, d, _p(np.ascontiguousarray(xs, np.float64)), _p(np.ascontiguousarray(ys, np.float64)),
+           _p(np.ascontiguousarray(zs, np.float64)), _p(_z(FF)), k0, I0, theta, phi, nfft2d, ntheta, nphi,
+           C.byref(cs), C.byref(g), _p(pf), _p(tf), _p(phf), C.byref(imax), _p(kp), _p(kn), info)
+    if rc:
+        raise ValueError(info.raw[:64].decode().strip())
+    S = 2 * imax.value + 1
+    return dict(Cscai=cs.value, gasym=g.value, poyntingfield=pf, thetafield=tf, phifield=phf, imaxk0=imax.value,
+                kpos=kp[:S * S].copy(), kneg=kn[:S * S].copy())

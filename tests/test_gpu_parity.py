@@ -457,3 +457,28 @@ def test_cdmlib_scattering_cross_section(orc):
     _, mie_sca, _ = orc.mie(2.25, 100e-9, 632.8e-9)
     assert abs(out["Cscai"][0] - mie_sca) / mie_sca < 0.1
     assert out["poyntingfield"].shape == (1, 37 * 72)
+
+
+@pytest.mark.parametrize("nfft2d", [128, 100])
+def test_farfield_fft_matches_oracle(gctx, orc, nfft2d):
+    """ifdda_farfield_fft against the oracle's 2-D FFT restatement
+    (diffractefft2d.f, computegcfft2d.f, the Poynting interpolation); any
+    nfft2d, the device evaluating the pupil frequencies only."""
+    from ifdda import objects
+    k0 = 2 * math.pi / 632.8e-9
+    ob = objects.sphere(100e-9, 2.25 + 0.1j, 8, k0, "RR", na=0)
+    E0, _ = orc.irradiance(1.0, 6328e-9)
+    ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 0.4, 0, 20.0, 30.0)
+    G = orc.greencalculfft(8, 8, 8, ob.aretecube, k0)
+    sol = orc.inverserig(G, 8, 8, 8, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-6)
+    ref = orc.farfield_fft(8, 8, 8, ob.aretecube, ob.xs, ob.ys, ob.zs, sol["FF"], k0, E0 ** 2, 20.0, 30.0, nfft2d,
+                           30, 60)
+    got = gctx.farfield_fft(8, 8, 8, ob.aretecube, ob.xs, ob.ys, ob.zs, sol["FF"], k0, E0 ** 2, 20.0, 30.0, nfft2d,
+                            30, 60)
+    assert got["imaxk0"] == ref["imaxk0"]
+    assert rel(got["kpos"], ref["kpos"]) < 1e-11 and rel(got["kneg"], ref["kneg"]) < 1e-11
+    assert abs(got["Cscai"] - ref["Cscai"]) <= 1e-11 * ref["Cscai"]
+    assert abs(got["gasym"] - ref["gasym"]) <= 1e-10 * abs(ref["gasym"])
+    ok = np.isfinite(ref["poyntingfield"])
+    assert np.array_equal(ok, np.isfinite(got["poyntingfield"]))
+    assert rel(got["poyntingfield"][ok], ref["poyntingfield"][ok]) < 1e-10

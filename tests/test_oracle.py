@@ -392,3 +392,22 @@ def test_farfield_csca_matches_mie_and_optical_theorem(orc):
     assert ff["thetafield"][-1] == 180.0 and ff["phifield"][71] == 355.0
     with pytest.raises(ValueError):
         orc.farfield_csca(ob.xs, ob.ys, ob.zs, ref["FF"], k0, E0 ** 2, 0.0, 0.0, 10, 72)
+
+
+def test_farfield_fft_converges_to_the_direct_sum(orc):
+    """The pupil-grid integration (computegcfft2d.f) approaches the direct
+    summation's Cscai as nfft2d grows (its 1/kz edge makes small grids
+    coarse); full box as cdmlib.f:630 requires."""
+    from ifdda import objects
+    k0 = 2 * math.pi / 632.8e-9
+    ob = objects.sphere(100e-9, 2.25 + 0j, 8, k0, "RR", na=0)
+    E0, _ = orc.irradiance(1.0, 6328e-9)
+    ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 1.0, 0, 0.0, 0.0)
+    G = orc.greencalculfft(8, 8, 8, ob.aretecube, k0)
+    sol = orc.inverserig(G, 8, 8, 8, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-8)
+    a = orc.farfield_csca(ob.xs, ob.ys, ob.zs, sol["FF"], k0, E0 ** 2, 0.0, 0.0, 36, 72)
+    b = orc.farfield_fft(8, 8, 8, ob.aretecube, ob.xs, ob.ys, ob.zs, sol["FF"], k0, E0 ** 2, 0.0, 0.0, 1024, 36, 72)
+    assert abs(b["Cscai"] - a["Cscai"]) / a["Cscai"] < 0.01
+    assert abs(b["gasym"] - a["gasym"]) < 0.01
+    with pytest.raises(ValueError, match="In FFT Poynting nfft2d too small"):
+        orc.farfield_fft(8, 8, 8, ob.aretecube, ob.xs, ob.ys, ob.zs, sol["FF"], k0, E0 ** 2, 0.0, 0.0, 16, 36, 72)
