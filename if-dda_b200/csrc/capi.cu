@@ -731,6 +731,7 @@ int ifdda_farfield_fft(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube,
     m.dkx = dkx;
     m.dky = dky;
     m.numaper = k0;
+    m.dside = 1.0;
     m.var1 = (xs[0] + (double)n2 * aretecube) * dkx;
     m.var2 = (ys[0] + (double)n2 * aretecube) * dky;
     m.gross = 1.0;
@@ -950,6 +951,9 @@ int ifdda_microscope(ifdda_green* g, const double* xs, const double* ys, const d
         return 1;
     };
     if (mo->ntypemic != 1 && mo->ntypemic != 2) return fail("ntypemic must be 1 (bright field) or 2 (dark field)");
+    if (mo->nside != 0 && mo->nside != 1) return fail("nside must be 0 (transmission) or 1 (reflection)");
+    // cdmlib.f:237-238, 389: the side's sign of kz, carried by zlens too
+    const double dside = mo->nside == 1 ? -1.0 : 1.0;
     if (!image_length_supported(n)) return fail("nfft2d not supported: a power of two from 32 to 4096");
     if (nx > n || ny > n) return fail("nfft2d smaller than the object");
     const double pi = 3.14159265358979323846;
@@ -1045,8 +1049,9 @@ int ifdda_microscope(ifdda_green* g, const double* xs, const double* ys, const d
     m.numaper = numaper;
     m.var1 = (xs[0] + (double)(n / 2) * d) * dkx;
     m.var2 = (ys[0] + (double)(n / 2) * d) * dky;
-    m.zlens = mo->zlens;
+    m.zlens = mo->zlens * dside;
     m.gross = mo->gross;
+    m.dside = dside;
     const int S = 2 * m.imax + 1;
     const char* lens_error = dkx >= numaper ? "In FFT lens nfft2d too small"
                              : S > n        ? "In FFT diffraction for lens nfft2d too small!"

@@ -122,14 +122,15 @@ __global__ void __launch_bounds__(256) k_mic_far(const MicGeom m, int nb, const 
         for (int k = 0; k < m.nz; k++) {
             double2 p0, p1, p2;
             ydft_plane(m, Q, tw, b, k, irow, ph0, step, p0, p1, p2);
-            // ctmp = (kx P_x + ky P_y + kz P_z) / k0
-            const double2 ct = make_double2((kx * p0.x + ky * p1.x + kz * p2.x) / m.k0,
-                                            (kx * p0.y + ky * p1.y + kz * p2.y) / m.k0);
-            sincos(-kz * zplane[k], &sn, &cs);
+            // ctmp = (kx P_x + ky P_y + kz dside P_z) / k0, on the side dside
+            const double kzs = kz * m.dside;
+            const double2 ct = make_double2((kx * p0.x + ky * p1.x + kzs * p2.x) / m.k0,
+                                            (kx * p0.y + ky * p1.y + kzs * p2.y) / m.k0);
+            sincos(-kzs * zplane[k], &sn, &cs);
             const double2 c1 = zdiv(cmul(make_double2(cs, sn), exy), den);
             o0 = cadd(o0, cmul(csub(p0, make_double2(kx * ct.x / m.k0, kx * ct.y / m.k0)), c1));
             o1 = cadd(o1, cmul(csub(p1, make_double2(ky * ct.x / m.k0, ky * ct.y / m.k0)), c1));
-            o2 = cadd(o2, cmul(csub(p2, make_double2(kz * ct.x / m.k0, kz * ct.y / m.k0)), c1));
+            o2 = cadd(o2, cmul(csub(p2, make_double2(kzs * ct.x / m.k0, kzs * ct.y / m.k0)), c1));
         }
         const double k02 = m.k0 * m.k0;
         o0 = cscale(o0, k02);
@@ -220,8 +221,12 @@ __global__ void __launch_bounds__(256) k_mic_lens(const MicGeom m, int nb, const
         sincos(kz * m.zlens, &sn, &cs);
         const double2 zf = make_double2(cs, sn);
         const double2* e = Ed + (((long)b * S + jrow) * S + irow) * 3;
-        for (int c = 0; c < 3; c++) f[c] = f[c + 3] = cmul(e[c], zf);
-        if (i == ik[b] && j == jk[b]) {
+        for (int c = 0; c < 3; c++) f[c] = cmul(e[c], zf);
+        // the reflection side (microssansinc.f) forms no image with the
+        // incident wave: those three fields stay zero
+        if (m.dside > 0)
+            for (int c = 0; c < 3; c++) f[c + 3] = f[c];
+        if (m.dside > 0 && i == ik[b] && j == jk[b]) {
             double2 ex, ey, ez;
             double kzi;
             kxky_amplitude(m.k0, E0, pp[b], kx, ky, ex, ey, ez, kzi);
@@ -243,9 +248,9 @@ __global__ void __launch_bounds__(256) k_mic_lens(const MicGeom m, int nb, const
         }
         if (tmp != 0.0) {
             const double u0 = kx / m.k0, u1v = ky / m.k0;
-            const double u2v = sqrt(__dsub_rn(__dsub_rn(1.0, __dmul_rn(u0, u0)), __dmul_rn(u1v, u1v)));
+            const double u2v = sqrt(__dsub_rn(__dsub_rn(1.0, __dmul_rn(u0, u0)), __dmul_rn(u1v, u1v))) * m.dside;
             const double v0 = -kx / m.k0 / m.gross, v1 = -ky / m.k0 / m.gross;
-            const double v2 = sqrt(__dsub_rn(__dsub_rn(1.0, __dmul_rn(v0, v0)), __dmul_rn(v1, v1)));
+            const double v2 = sqrt(__dsub_rn(__dsub_rn(1.0, __dmul_rn(v0, v0)), __dmul_rn(v1, v1))) * m.dside;
             double a1 = __dsub_rn(__dmul_rn(u1v, v2), __dmul_rn(u2v, v1));
             double a2 = __dadd_rn(__dmul_rn(-u0, v2), __dmul_rn(u2v, v0));
             const double co = __dadd_rn(__dadd_rn(__dmul_rn(u0, v0), __dmul_rn(u1v, v1)), __dmul_rn(u2v, v2));

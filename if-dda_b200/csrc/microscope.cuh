@@ -24,6 +24,7 @@ struct MicGeom {
     double numaper;   // numerical aperture of the objective times k0
     double var1, var2;  // phase origin of the lattice (diffractefft2dlens.f:45-46)
     double zlens, gross;
+    double dside;       // +1 transmission (kz > 0), -1 reflection (kz < 0)
     __host__ __device__ int S() const { return 2 * imax + 1; }
 };
 

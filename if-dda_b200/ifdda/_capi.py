@@ -30,7 +30,7 @@ class SolveOptions(C.Structure):
 class MicroscopeOptions(C.Structure):
     _fields_ = [("ntypemic", C.c_int), ("nfft2d", C.c_int), ("numaper", C.c_double), ("numaperinc", C.c_double),
                 ("gross", C.c_double), ("zlens", C.c_double), ("P0", C.c_double), ("w0", C.c_double),
-                ("batch", C.c_int)]
+                ("batch", C.c_int), ("nside", C.c_int)]
 
 
 _lib = None

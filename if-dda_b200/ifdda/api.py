@@ -282,10 +282,11 @@ class GreenSpectrum:
         return r
 
     def microscope(self, xs, ys, zs, polarisa, methodeit="GPBICG1", tol=1e-4, ntypemic=1, nfft2d=128, numaper=0.9,
-                   numaperinc=0.5, gross=100.0, zlens=0.0, P0=1.0, w0=1e-6, batch=0, precision=IFDDA_FP64):
+                   numaperinc=0.5, gross=100.0, zlens=0.0, P0=1.0, w0=1e-6, batch=0, precision=IFDDA_FP64, nside=0):
         """Bright-field (ntypemic 1, microsbf) or dark-field / phase
         (ntypemic 2, microsdf) microscope in transmission with the FFT lens,
-        on the full box of this spectrum.  zlens and w0 in metres.  Returns a
+        on the full box of this spectrum.  zlens and w0 in metres; nside 0
+        transmission, 1 reflection (no image with the incident wave).  Returns a
         MicroscopeResult: image (6, n, n) = |E| of the x, y, z image fields
         and of the same with the incident wave (row v, column u), xy, kxy,
         kxinc / kyinc (units of k0), the last solve's counters, nstop, infostr."""
@@ -308,7 +309,7 @@ class GreenSpectrum:
         nloop, ncompte, nstop = C.c_int(0), C.c_int(0), C.c_int(0)
         info = C.create_string_buffer(b" " * 64, 65)
         mo = MicroscopeOptions(int(ntypemic), n, float(numaper), float(numaperinc), float(gross), float(zlens),
-                               float(P0), float(w0), int(batch))
+                               float(P0), float(w0), int(batch), int(nside))
         opt = SolveOptions(precision, 0, 0, 0.0, 0)
         self.lib.ifdda_microscope(self.h, _p(xs), _p(ys), _p(zs), _p(pol), methodeit.encode(), tol, C.byref(mo),
                                   _p(img), _p(xy), _p(kxy), C.byref(ninc), _p(kxi), _p(kyi), C.byref(tol1),

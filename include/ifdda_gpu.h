@@ -221,21 +221,25 @@ int ifdda_nearfield_wide(ifdda_ctx* ctx, int nx, int ny, int nz, int nxmp, int n
                          ifdda_dcmplx* macro);
 
 /* Microscope options: the cdmlib arguments that the microscopes read
-   (cdmlib/cdmlib.f:3660-3800 with nlentille = 1, nquicklens = 1, nside = 0). */
+   (cdmlib/cdmlib.f:3660-3800 with nlentille = 1, nquicklens = 1). */
 typedef struct {
     int ntypemic;      /* 1 bright field (microsbf.f), 2 dark field and phase (microsdf.f) */
     int nfft2d;        /* side n of the pupil and image grids: a power of two from 32 to 4096 */
     double numaper;    /* numerical aperture of the objective, (0, 1] */
     double numaperinc; /* numerical aperture of the condenser, < 1 */
     double gross;      /* magnification */
-    double zlens;      /* focal-plane position in metres */
+    double zlens;      /* focal-plane position in metres, as given (the side's sign is applied inside) */
     double P0, w0;     /* power (W) shared by all illuminations, waist (m) of irradiance.f */
     int batch;         /* illuminations solved together; 0 = 64 */
+    int nside;         /* 0 transmission (microsbf / microsdf), 1 reflection (microsbfneg /
+                          microsdfneg, cdmlib/microssansinc.f: no image with the incident wave) */
 } ifdda_microscope_options;
 
-/* Bright-field or dark-field / phase microscope in transmission with the FFT
-   lens: replaces microsbf (cdmlib/microsbf.f:1-965) and microsdf
-   (cdmlib/microsdf.f:1-915) called at cdmlib/cdmlib.f:3735-3800, with
+/* Bright-field or dark-field / phase microscope with the FFT lens, in
+   transmission or reflection: replaces microsbf (cdmlib/microsbf.f:1-965),
+   microsdf (cdmlib/microsdf.f:1-915) and their reflection forms microsbfneg /
+   microsdfneg (cdmlib/microssansinc.f:1-1741), called at
+   cdmlib/cdmlib.f:3735-3800, with
    diffractefft2dlens.f, fouriertoimage.f and deltakroutine.f inside.  The
    object fills the full box of the spectrum g (nbsphere = nx*ny*nz, the
    reference forces it when nquicklens = 1, cdmlib.f:631); xs, ys, zs and

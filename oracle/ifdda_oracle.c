@@ -2645,7 +2645,8 @@ static int orc_tabfft2(int i, int n) {
    entry ((jj * S + ii) * 3 + c), ii = imax + i, jj = imax + j. */
 static int orc_diffractefft2dlens(int nx, int ny, int nz, int n, double k0, const double *xs,
                                   const double *ys, const double *zs, double d, const zc *FF,
-                                  double numaper, int *imax_out, zc **Ediff_out, char *infostr) {
+                                  double numaper, double dside, int *imax_out, zc **Ediff_out,
+                                  char *infostr) {
     const double pi = acos(-1.0);
     double dkx = 2.0 * pi / ((double)n * d), dky = dkx;
     if (n > 16384) { set_info(infostr, "nfft2d too large"); return 1; }
@@ -2680,13 +2681,13 @@ static int orc_diffractefft2dlens(int nx, int ny, int nz, int n, double k0, cons
                     long ind = (orc_tabfft2(i + n2 + 1, n) - 1) +
                                (long)n * (orc_tabfft2(j + n2 + 1, n) - 1);
                     zc ex = E[ind], ey = E[(size_t)n * n + ind], ez = E[2 * (size_t)n * n + ind];
-                    zc ctmp = (kx * ex + ky * ey + kz * ez) / k0;
-                    zc ctmp1 = cexp(-I * kz * zs[kk - 1]) * cexp(-I * (var1 * i + var2 * j)) /
+                    zc ctmp = (kx * ex + ky * ey + kz * dside * ez) / k0;
+                    zc ctmp1 = cexp(-I * dside * kz * zs[kk - 1]) * cexp(-I * (var1 * i + var2 * j)) /
                                (-2.0 * pi * I * kz);
                     zc *o = Ed + ((size_t)(imax + j) * S + (imax + i)) * 3;
                     o[0] += (ex - kx * ctmp / k0) * ctmp1;
                     o[1] += (ey - ky * ctmp / k0) * ctmp1;
-                    o[2] += (ez - kz * ctmp / k0) * ctmp1;
+                    o[2] += (ez - kz * dside * ctmp / k0) * ctmp1;
                 }
             }
     }
@@ -2717,7 +2718,7 @@ static void orc_fouriertoimage(double dkx, double dky, double gross, zc *F, int 
     }
 }
 
-int orc_microscope(int ntypemic, const zc *G6, int nx, int ny, int nz, double d, double k0,
+int orc_microscope(int ntypemic, int nside, const zc *G6, int nx, int ny, int nz, double d, double k0,
                    const double *xs, const double *ys, const double *zs, const zc *pol,
                    const char *methodeit, double tol, double numaper, double numaperinc, int n,
                    double gross, double zlens, double P0, double w0, double *image, double *xy,
@@ -2728,6 +2729,10 @@ int orc_microscope(int ntypemic, const zc *G6, int nx, int ny, int nz, double d,
     long n3 = 3L * N;
     int n2 = n / 2;
     double numaperk = k0 * numaperinc;
+    /* cdmlib.f:237-238, 389: nside 0 (transmission) -> +1, 1 (reflection,
+       microsbfneg / microsdfneg of microssansinc.f) -> -1; zlens takes the sign */
+    double dside = nside == 1 ? -1.0 : 1.0;
+    zlens = zlens * dside;
     set_info(infostr, "");
     if (numaperinc >= 1.0 || numaper <= 0.0) {
         set_info(infostr, "NA inc strictly between 0 and 1");
@@ -2820,7 +2825,8 @@ int orc_microscope(int ntypemic, const zc *G6, int nx, int ny, int nz, double d,
                            ncompte, &nstop, infostr, NULL, 0);
             if (nstop == 1) break;
             zc *Ed = NULL;
-            if (orc_diffractefft2dlens(nx, ny, nz, n, k0, xs, ys, zs, d, FF, numaper, &imax, &Ed, infostr)) {
+            if (orc_diffractefft2dlens(nx, ny, nz, n, k0, xs, ys, zs, d, FF, numaper, dside, &imax, &Ed,
+                                       infostr)) {
                 nstop = 1;
                 break;
             }
@@ -2841,7 +2847,10 @@ int orc_microscope(int ntypemic, const zc *G6, int nx, int ny, int nz, double d,
                     zc *e = Ed + ((size_t)(imax + j) * S + (imax + i)) * 3;
                     zc f[6];
                     for (int c = 0; c < 3; c++) f[c] = f[c + 3] = e[c] * zf;
-                    if (i == ik && j == jk) {
+                    /* the reflection side forms no image with the incident wave */
+                    if (dside < 0)
+                        for (int c = 3; c < 6; c++) f[c] = 0;
+                    if (dside > 0 && i == ik && j == jk) {
                         zc Ei[3];
                         orc_ondeplanekxky(0.0, 0.0, 0.0, k0, E0, pp, kx, ky, Ei);
                         if (ntypemic == 1) {
@@ -2855,9 +2864,10 @@ int orc_microscope(int ntypemic, const zc *G6, int nx, int ny, int nz, double d,
                     }
                     if (tmp != 0.0) {
                         double u[3], v[3];
-                        u[0] = kx / k0; u[1] = ky / k0; u[2] = sqrt(1.0 - u[0] * u[0] - u[1] * u[1]);
+                        u[0] = kx / k0; u[1] = ky / k0;
+                        u[2] = sqrt(1.0 - u[0] * u[0] - u[1] * u[1]) * dside;
                         v[0] = -kx / k0 / gross; v[1] = -ky / k0 / gross;
-                        v[2] = sqrt(1.0 - v[0] * v[0] - v[1] * v[1]);
+                        v[2] = sqrt(1.0 - v[0] * v[0] - v[1] * v[1]) * dside;
                         double u1 = u[1] * v[2] - u[2] * v[1];
                         double u2 = -u[0] * v[2] + u[2] * v[0];
                         double cs = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];

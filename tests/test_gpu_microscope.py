@@ -33,18 +33,22 @@ def _compare(r, ref, tol=1e-8):
         assert rel(r.image[c], ref["image"][c]) < tol, c
 
 
-@pytest.mark.parametrize("ntypemic,nfft2d", [(1, 64), (1, 128), (2, 64)])
-def test_microscope_matches_oracle(gctx, orc, ntypemic, nfft2d):
+@pytest.mark.parametrize("ntypemic,nfft2d,nside", [(1, 64, 0), (1, 128, 0), (2, 64, 0), (1, 64, 1), (2, 64, 1)])
+def test_microscope_matches_oracle(gctx, orc, ntypemic, nfft2d, nside):
     ob, k0 = _object()
     G = orc.greencalculfft(8, 8, 8, ob.aretecube, k0)
     ref = orc.microscope(ntypemic, G, 8, 8, 8, ob.aretecube, k0, ob.xs, ob.ys, ob.zs, ob.polarisa, "GPBICG1", 1e-6,
-                         0.9, 0.5, nfft2d, 100.0, 50e-9, 1.0, 6328e-9)
+                         0.9, 0.5, nfft2d, 100.0, 50e-9, 1.0, 6328e-9, nside=nside)
     g = gctx.green(8, 8, 8, ob.aretecube, k0)
     r = g.microscope(ob.xs, ob.ys, ob.zs, ob.polarisa, "GPBICG1", 1e-6, ntypemic=ntypemic, nfft2d=nfft2d,
-                     numaper=0.9, numaperinc=0.5, gross=100.0, zlens=50e-9, P0=1.0, w0=6328e-9)
+                     numaper=0.9, numaperinc=0.5, gross=100.0, zlens=50e-9, P0=1.0, w0=6328e-9, nside=nside)
     _compare(r, ref)
     # the image carries the object: the scattered intensity is not zero
-    assert r.image[0].max() > 0 and r.image[3].max() > r.image[0].max()
+    assert r.image[0].max() > 0
+    if nside == 0:
+        assert r.image[3].max() > r.image[0].max()
+    else:  # reflection: no image with the incident wave (microssansinc.f)
+        assert not r.image[3:].any()
     g.close()
 
 
