@@ -929,12 +929,12 @@ int ifdda_nearfield_wide(ifdda_ctx* ctx, int nx, int ny, int nz, int nxmp, int n
     IFDDA_GUARD_END(ctx, nullptr)
 }
 
-int ifdda_microscope(ifdda_green* g, const double* xs, const double* ys, const double* zs,
-                     const ifdda_dcmplx* polarisa, const char* methodeit, double tol,
+int ifdda_microscope(ifdda_green* g, int nbsphere, const int* tabdip, const double* xs, const double* ys,
+                     const double* zs, const ifdda_dcmplx* polarisa, const char* methodeit, double tol,
                      const ifdda_microscope_options* mo, double* image, double* xy, double* kxy, int* ninc,
                      double* kxinc, double* kyinc, double* tol1, int* nloop, int* ncompte, int* nstop,
                      char* infostr, const ifdda_solve_options* opt) {
-    if (!g || !xs || !ys || !zs || !polarisa || !mo || !image || !ninc) {
+    if (!g || !xs || !ys || !zs || !polarisa || !mo || !image || !ninc || nbsphere < 1) {
         if (nstop) *nstop = 1;
         set_info(infostr, "invalid argument");
         return 1;
@@ -944,13 +944,19 @@ int ifdda_microscope(ifdda_green* g, const double* xs, const double* ys, const d
     AllocStreamScope as(g->ctx->stream);
     cudaStream_t st = g->ctx->stream;
     const MvGeom& geo = g->G.g;
-    const int nx = geo.nx, ny = geo.ny, nz = geo.nz, N = geo.N, n = mo->nfft2d;
+    const int nx = geo.nx, ny = geo.ny, nz = geo.nz, nmax = geo.N, N = nbsphere, n = mo->nfft2d;
+    const bool quick = mo->nquicklens == 1;
     auto fail = [&](const char* msg) {
         if (nstop) *nstop = 1;
         set_info(infostr, msg);
         return 1;
     };
     if (mo->ntypemic != 1 && mo->ntypemic != 2) return fail("ntypemic must be 1 (bright field) or 2 (dark field)");
+    if (mo->nquicklens != 0 && mo->nquicklens != 1) return fail("nquicklens must be 0 or 1");
+    // the FFT lens reads the dipoles plane by plane: full box (cdmlib.f:631)
+    if (quick && (tabdip || nbsphere != nmax)) return fail("the FFT lens needs the full box (nbsphere = nx*ny*nz)");
+    if (!tabdip && nbsphere != nmax) return fail("full-box solve: nbsphere must equal nx*ny*nz (or pass tabdip)");
+    if (tabdip) check_tabdip(tabdip, nmax, nbsphere);
     if (mo->nside != 0 && mo->nside != 1) return fail("nside must be 0 (transmission) or 1 (reflection)");
     // cdmlib.f:237-238, 389: the side's sign of kz, carried by zlens too
     const double dside = mo->nside == 1 ? -1.0 : 1.0;
@@ -970,18 +976,36 @@ int ifdda_microscope(ifdda_green* g, const double* xs, const double* ys, const d
         ymin = std::min(ymin, ys[i]);
     }
     const double deltakm = pi / std::max(xmax - xmin, ymax - ymin);
-    const double dkx = 2.0 * pi / (d * (double)n), dky = dkx;
-    if (dkx >= numaperk) return fail("In FFT lens nfft2d too small:Increase size of FFT 1");
-    int imul = (int)(deltakm / dkx);
-    if (imul == 0) return fail("In FFT lens nfft2d too small:Increase size of FFT 2");
+    double dkx = 2.0 * pi / (d * (double)n);
     double deltak;
-    int imaxinc;
-    for (;;) {
-        deltak = dkx * (double)imul;
-        imaxinc = (int)std::lround(k0 / deltak) + 1;
-        if (imaxinc > 3) break;
-        if (--imul == 0) return fail("In FFT lens nfft2d too small:Increase size of FFT 3");
+    int imaxinc, imaxk0 = 0;
+    if (quick) {
+        if (dkx >= numaperk) return fail("In FFT lens nfft2d too small:Increase size of FFT 1");
+        int imul = (int)(deltakm / dkx);
+        if (imul == 0) return fail("In FFT lens nfft2d too small:Increase size of FFT 2");
+        for (;;) {
+            deltak = dkx * (double)imul;
+            imaxinc = (int)std::lround(k0 / deltak) + 1;
+            if (imaxinc > 3) break;
+            if (--imul == 0) return fail("In FFT lens nfft2d too small:Increase size of FFT 3");
+        }
+    } else {
+        // microsbf.f:139-157: halve the pupil step until more than 5 points
+        // cover k0, then the incidence step from the object's size
+        for (int k = 0;; k++) {
+            dkx = 2.0 * pi / ((double)n * d) / (double)(1 << k);
+            imaxk0 = (int)std::lround(k0 / dkx) + 1;
+            if (imaxk0 > 5) break;
+        }
+        for (int k = 0;; k++) {
+            deltak = dkx * std::round(deltakm / dkx) / (double)(1 << k);
+            imaxinc = (int)std::lround(k0 / deltak) + 1;
+            if (imaxinc > 2) break;
+        }
+        // the pupil must fit the image grid (the reference does not check)
+        if (2 * imaxk0 + 1 > n) return fail("In FFT lens nfft2d too small");
     }
+    const double dky = dkx;
     // incidences of one polarisation: the grid inside the condenser's NA
     // (microsbf.f:161-171) or the ring at its NA (microsdf.f:160-162, 204-212)
     std::vector<double> kxi, kyi;
@@ -1041,7 +1065,7 @@ int ifdda_microscope(ifdda_green* g, const double* xs, const double* ys, const d
     m.ny = ny;
     m.nz = nz;
     m.n = n;
-    m.imax = (int)std::lround(k0 / dkx) + 1;
+    m.imax = quick ? (int)std::lround(k0 / dkx) + 1 : imaxk0;
     m.ntypemic = mo->ntypemic;
     m.k0 = k0;
     m.dkx = dkx;
@@ -1053,14 +1077,15 @@ int ifdda_microscope(ifdda_green* g, const double* xs, const double* ys, const d
     m.gross = mo->gross;
     m.dside = dside;
     const int S = 2 * m.imax + 1;
-    const char* lens_error = dkx >= numaper ? "In FFT lens nfft2d too small"
-                             : S > n        ? "In FFT diffraction for lens nfft2d too small!"
-                             : S < 7        ? "In FFT diffract nfft2d too small"
-                                            : nullptr;
+    const char* lens_error = !quick         ? nullptr
+                             : dkx >= numaper ? "In FFT lens nfft2d too small"
+                             : S > n          ? "In FFT diffraction for lens nfft2d too small!"
+                             : S < 7          ? "In FFT diffract nfft2d too small"
+                                              : nullptr;
     const int B = std::max(1, std::min(total, mo->batch > 0 ? mo->batch : 64));
     const long n3 = 3L * N;
     DevBuf<double> dx, dy, dz, zpl, d1, d2, dpp, img;
-    DevBuf<int> dbeam, dik, djk;
+    DevBuf<int> dbeam, dik, djk, dtab;
     DevBuf<double2> pol, alpha, ff0, ff, loc, tw, Q, Ed, F, T;
     dx.ensure(N);
     dy.ensure(N);
@@ -1068,17 +1093,23 @@ int ifdda_microscope(ifdda_green* g, const double* xs, const double* ys, const d
     IFDDA_CUDA(cudaMemcpyAsync(dx.p, xs, N * sizeof(double), cudaMemcpyHostToDevice, st));
     IFDDA_CUDA(cudaMemcpyAsync(dy.p, ys, N * sizeof(double), cudaMemcpyHostToDevice, st));
     IFDDA_CUDA(cudaMemcpyAsync(dz.p, zs, N * sizeof(double), cudaMemcpyHostToDevice, st));
-    // the object on the full box: one alpha per dipole when isotropic
-    pol.ensure((size_t)9 * N);
+    // the object ((nmax,3,3) tensor): one alpha per dipole when isotropic
+    pol.ensure((size_t)9 * nmax);
     alpha.ensure(N);
-    IFDDA_CUDA(cudaMemcpyAsync(pol.p, polarisa, (size_t)9 * N * sizeof(double2), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(pol.p, polarisa, (size_t)9 * nmax * sizeof(double2), cudaMemcpyHostToDevice, st));
     IFDDA_CUDA(cudaMemsetAsync(g->ctx->flag.p, 0, sizeof(int), st));
-    pola_compact_dev(pol.p, N, N, alpha.p, g->ctx->flag.p, st);
+    pola_compact_dev(pol.p, N, nmax, alpha.p, g->ctx->flag.p, st);
+    if (tabdip) {
+        dtab.ensure(nmax);
+        IFDDA_CUDA(cudaMemcpyAsync(dtab.p, tabdip, nmax * sizeof(int), cudaMemcpyHostToDevice, st));
+    }
     int aniso = 0;
     IFDDA_CUDA(cudaMemcpyAsync(&aniso, g->ctx->flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-    // z of each lattice plane, the roots of unity of the pupil transforms
+    // z of each lattice plane (FFT lens, full box), the roots of unity of the
+    // pupil transforms
     std::vector<double> zp(nz);
-    for (int k = 0; k < nz; k++) zp[k] = zs[(long)nx * ny * k];
+    if (quick)
+        for (int k = 0; k < nz; k++) zp[k] = zs[(long)nx * ny * k];
     std::vector<double2> twh(n);
     for (int j = 0; j < n; j++) {
         const double a = 2.0 * pi * (double)j / (double)n;
@@ -1103,7 +1134,8 @@ int ifdda_microscope(ifdda_green* g, const double* xs, const double* ys, const d
     ff0.ensure(n3 * B);
     ff.ensure(n3 * B);
     loc.ensure(n3 * B);
-    Q.ensure((size_t)B * nz * ny * S * 3);
+    if (quick) Q.ensure((size_t)B * nz * ny * S * 3);
+    else Q.ensure((size_t)B * S * S * mic_direct_chunks(N) * 3);
     Ed.ensure((size_t)B * S * S * 3);
     F.ensure((size_t)B * 6 * S * S);
     T.ensure((size_t)B * 6 * S * n);
@@ -1122,15 +1154,16 @@ int ifdda_microscope(ifdda_green* g, const double* xs, const double* ys, const d
         IFDDA_CUDA(cudaMemcpyAsync(dik.p, ikv.data() + t0, nb * sizeof(int), cudaMemcpyHostToDevice, st));
         IFDDA_CUDA(cudaMemcpyAsync(djk.p, jkv.data() + t0, nb * sizeof(int), cudaMemcpyHostToDevice, st));
         planewaves_dev(N, dx.p, dy.p, dz.p, k0, E0, nb, dbeam.p, d1.p, d2.p, dpp.p, ff0.p, g->ctx->flag.p, st);
-        const int rc = solve_device(g, nb, N, N, nullptr, al, amode, ff0.p, methodeit, tol, ff.p, loc.p, t1.data(),
-                                    nl.data(), nc.data(), nstop, infostr, opt, false);
+        const int rc = solve_device(g, nb, N, nmax, tabdip ? dtab.p : nullptr, al, amode, ff0.p, methodeit, tol, ff.p,
+                                    loc.p, t1.data(), nl.data(), nc.data(), nstop, infostr, opt, false);
         if (tol1) *tol1 = t1[nb - 1];
         if (nloop) *nloop = nl[nb - 1];
         if (ncompte) *ncompte = nc[nb - 1];
         if (rc) return rc;
         // the lens checks of diffractefft2dlens.f run after the first solve
         if (lens_error) return fail(lens_error);
-        mic_farfield_dev(m, nb, ff.p, zpl.p, tw.p, Q.p, Ed.p, st);
+        if (quick) mic_farfield_dev(m, nb, ff.p, zpl.p, tw.p, Q.p, Ed.p, st);
+        else mic_direct_dev(m, nb, N, dx.p, dy.p, dz.p, ff.p, Q.p, Ed.p, st);
         mic_lens_dev(m, nb, Ed.p, dik.p, djk.p, dpp.p, E0, F.p, st);
         if (!mic_image_dev(m, nb, F.p, tw.p, T.p, img.p, st)) return fail("nfft2d not supported");
     }

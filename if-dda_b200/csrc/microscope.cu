@@ -20,6 +20,7 @@
 #include "microscope.cuh"
 #include "fft_tile.cuh"
 #include "planewave.cuh"
+#include "reduce.cuh"
 
 namespace ifdda {
 
@@ -193,6 +194,69 @@ __global__ void __launch_bounds__(256) k_mic_far2(const MicGeom m, int nb, const
     f[0] = c0;
     f[1] = c1;
     f[2] = c2;
+}
+
+// The lens's far field by direct summation over the dipoles (nquicklens = 0,
+// microsbf.f:627-666): pupil point (i, j) inside sqrt(kx^2 + ky^2) <=
+// numaper, n = (kx, ky, dside kz) / k0, E = sum exp(-i k0 n.r)(p - n (n.p)).
+// Stage 1: block (point, chunk, incidence) sums its dipoles; stage 2 adds
+// the chunks in order and applies k0^2 / (-2 pi i kz).
+constexpr int MD_NT = 256;
+__device__ __forceinline__ bool direct_point(const MicGeom& m, int irow, int jrow, double& kx, double& ky) {
+    kx = m.dkx * (double)(irow - m.imax);
+    ky = m.dkx * (double)(jrow - m.imax);
+    return sqrt(__dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky))) <= m.numaper;
+}
+__global__ void __launch_bounds__(MD_NT) k_mic_direct_part(const MicGeom m, int nd, const double* __restrict__ xs,
+                                                           const double* __restrict__ ys,
+                                                           const double* __restrict__ zs,
+                                                           const double2* __restrict__ FF, int nchunk,
+                                                           double2* __restrict__ part) {
+    const int S = m.S(), pt = blockIdx.x, ch = blockIdx.y, b = blockIdx.z;
+    const int irow = pt % S, jrow = pt / S;
+    double kx, ky;
+    double2 acc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+    if (direct_point(m, irow, jrow, kx, ky)) {
+        const double n0 = kx / m.k0, n1 = ky / m.k0;
+        const double n2 = sqrt(__dsub_rn(__dsub_rn(1.0, __dmul_rn(n0, n0)), __dmul_rn(n1, n1))) * m.dside;
+        const long per = ((long)nd + nchunk - 1) / nchunk;
+        const long i0 = (long)ch * per, i1 = min((long)nd, i0 + per);
+        const double2* p = FF + (long)b * 3 * nd;
+        for (long i = i0 + threadIdx.x; i < i1; i += MD_NT) {
+            double sn, cs;
+            sincos(-m.k0 * (n0 * xs[i] + n1 * ys[i] + n2 * zs[i]), &sn, &cs);
+            const double2 e = make_double2(cs, sn);
+            const double2 p0 = p[3 * i], p1 = p[3 * i + 1], p2 = p[3 * i + 2];
+            const double2 np = make_double2(n0 * p0.x + n1 * p1.x + n2 * p2.x, n0 * p0.y + n1 * p1.y + n2 * p2.y);
+            acc[0] = cadd(acc[0], cmul(e, make_double2(p0.x - np.x * n0, p0.y - np.y * n0)));
+            acc[1] = cadd(acc[1], cmul(e, make_double2(p1.x - np.x * n1, p1.y - np.y * n1)));
+            acc[2] = cadd(acc[2], cmul(e, make_double2(p2.x - np.x * n2, p2.y - np.y * n2)));
+        }
+    }
+    __shared__ double2 scratch[3 * 32];
+    block_sum<MD_NT, 3>(acc, scratch);
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 3; c++) part[(((long)b * S * S + pt) * nchunk + ch) * 3 + c] = acc[c];
+}
+__global__ void k_mic_direct_final(const MicGeom m, int nb, int nchunk, const double2* __restrict__ part,
+                                   double2* __restrict__ Ed) {
+    const int S = m.S();
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)nb * S * S) return;
+    const int pt = (int)(t % ((long)S * S)), b = (int)(t / ((long)S * S));
+    const int irow = pt % S, jrow = pt / S;
+    double kx, ky;
+    double2 e[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+    if (direct_point(m, irow, jrow, kx, ky)) {
+        const double kz = sqrt(__dsub_rn(__dsub_rn(__dmul_rn(m.k0, m.k0), __dmul_rn(kx, kx)), __dmul_rn(ky, ky)));
+        const double2 den = make_double2(0.0, -2.0 * 3.14159265358979323846 * kz);
+        for (int ch = 0; ch < nchunk; ch++)
+            for (int c = 0; c < 3; c++) e[c] = cadd(e[c], part[(((long)b * S * S + pt) * nchunk + ch) * 3 + c]);
+        const double k02 = m.k0 * m.k0;
+        for (int c = 0; c < 3; c++) e[c] = zdiv(cscale(e[c], k02), den);
+    }
+    double2* o = Ed + (((long)b * S + jrow) * S + irow) * 3;
+    for (int c = 0; c < 3; c++) o[c] = e[c];
 }
 
 // The lens (microsbf.f:699-795, microsdf.f:677-766): focus phase
@@ -411,6 +475,20 @@ void mic_farfield_dev(const MicGeom& m, int nb, const double2* FF, const double*
     count_launch();
     if (both_sides) k_mic_far2<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(m, nb, Q, zplane, tw, Ed);
     else k_mic_far<<<(unsigned)((ne + 255) / 256), 256, 0, st>>>(m, nb, Q, zplane, tw, Ed);
+    IFDDA_CUDA(cudaGetLastError());
+}
+
+int mic_direct_chunks(long nd) { return (int)std::max(1L, std::min(64L, (nd + 4095) / 4096)); }
+
+void mic_direct_dev(const MicGeom& m, int nb, int nd, const double* xs, const double* ys, const double* zs,
+                    const double2* FF, double2* part, double2* Ed, cudaStream_t st) {
+    const int S = m.S(), nchunk = mic_direct_chunks(nd);
+    count_launch();
+    k_mic_direct_part<<<dim3(S * S, nchunk, nb), MD_NT, 0, st>>>(m, nd, xs, ys, zs, FF, nchunk, part);
+    IFDDA_CUDA(cudaGetLastError());
+    const long ne = (long)nb * S * S;
+    count_launch();
+    k_mic_direct_final<<<(unsigned)((ne + 127) / 128), 128, 0, st>>>(m, nb, nchunk, part, Ed);
     IFDDA_CUDA(cudaGetLastError());
 }
 

@@ -35,6 +35,11 @@ struct MicGeom {
 // side, then the kz < 0 side (2 nb S S 3 values), instead of the lens's.
 void mic_farfield_dev(const MicGeom& m, int nb, const double2* FF, const double* zplane, const double2* tw,
                       double2* Q, double2* Ed, cudaStream_t st, bool both_sides = false);
+// The same far field by direct summation over nd dipoles at (xs, ys, zs)
+// (nquicklens = 0); part holds nb S^2 mic_direct_chunks(nd) 3 values.
+int mic_direct_chunks(long nd);
+void mic_direct_dev(const MicGeom& m, int nb, int nd, const double* xs, const double* ys, const double* zs,
+                    const double2* FF, double2* part, double2* Ed, cudaStream_t st);
 // Fourier-plane fields F (nb x 6 x S x S: x, y, z, then with the incident
 // wave) after the lens: focus phase, the specular wave at grid point
 // (ik[b], jk[b]) with polarisation pp[b], and the rotation by the lens.

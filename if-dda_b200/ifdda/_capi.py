@@ -30,7 +30,7 @@ class SolveOptions(C.Structure):
 class MicroscopeOptions(C.Structure):
     _fields_ = [("ntypemic", C.c_int), ("nfft2d", C.c_int), ("numaper", C.c_double), ("numaperinc", C.c_double),
                 ("gross", C.c_double), ("zlens", C.c_double), ("P0", C.c_double), ("w0", C.c_double),
-                ("batch", C.c_int), ("nside", C.c_int)]
+                ("batch", C.c_int), ("nside", C.c_int), ("nquicklens", C.c_int)]
 
 
 _lib = None
@@ -74,7 +74,8 @@ SIGNATURES = {
                                      _vp, _vp, _ip, _vp, _vp]),
     "ifdda_nearfield_wide": (C.c_int, [_vp] + [C.c_int] * 6 + [C.c_double, C.c_double] + [C.c_int] * 3 +
                              [_vp] * 6 + [DComplex, C.c_double, C.c_double, C.c_double] + [_vp] * 6),
-    "ifdda_microscope": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_char_p, C.c_double, C.POINTER(MicroscopeOptions),
+    "ifdda_microscope": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_char_p, C.c_double,
+                                   C.POINTER(MicroscopeOptions),
                                    _vp, _vp, _vp, _ip, _vp, _vp, _dp, _ip, _ip, _ip, C.c_char_p,
                                    C.POINTER(SolveOptions)]),
     "ifdda_launch_count": (C.c_ulonglong, []),

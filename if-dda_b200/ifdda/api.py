@@ -282,21 +282,22 @@ class GreenSpectrum:
         return r
 
     def microscope(self, xs, ys, zs, polarisa, methodeit="GPBICG1", tol=1e-4, ntypemic=1, nfft2d=128, numaper=0.9,
-                   numaperinc=0.5, gross=100.0, zlens=0.0, P0=1.0, w0=1e-6, batch=0, precision=IFDDA_FP64, nside=0):
+                   numaperinc=0.5, gross=100.0, zlens=0.0, P0=1.0, w0=1e-6, batch=0, precision=IFDDA_FP64, nside=0,
+                   nquicklens=1, tabdip=None):
         """Bright-field (ntypemic 1, microsbf) or dark-field / phase
         (ntypemic 2, microsdf) microscope in transmission with the FFT lens,
-        on the full box of this spectrum.  zlens and w0 in metres; nside 0
+        on the full box of this spectrum (nquicklens 1, the FFT lens) or on any
+        object (nquicklens 0, the lens's far field by direct summation;
+        tabdip for inside-only dipoles).  zlens and w0 in metres; nside 0
         transmission, 1 reflection (no image with the incident wave).  Returns a
         MicroscopeResult: image (6, n, n) = |E| of the x, y, z image fields
         and of the same with the incident wave (row v, column u), xy, kxy,
         kxinc / kyinc (units of k0), the last solve's counters, nstop, infostr."""
         n = int(nfft2d)
-        N = self.nx * self.ny * self.nz
         xs = np.ascontiguousarray(xs, np.float64)
         ys = np.ascontiguousarray(ys, np.float64)
         zs = np.ascontiguousarray(zs, np.float64)
-        if len(xs) != N:
-            raise ValueError("the microscope works on the full box: nx*ny*nz positions")
+        tab = None if tabdip is None else np.ascontiguousarray(tabdip, np.int32)
         pol = _zc(polarisa)
         img = np.zeros((6, n, n), np.float64)
         xy = np.zeros(n)
@@ -309,9 +310,10 @@ class GreenSpectrum:
         nloop, ncompte, nstop = C.c_int(0), C.c_int(0), C.c_int(0)
         info = C.create_string_buffer(b" " * 64, 65)
         mo = MicroscopeOptions(int(ntypemic), n, float(numaper), float(numaperinc), float(gross), float(zlens),
-                               float(P0), float(w0), int(batch), int(nside))
+                               float(P0), float(w0), int(batch), int(nside), int(nquicklens))
         opt = SolveOptions(precision, 0, 0, 0.0, 0)
-        self.lib.ifdda_microscope(self.h, _p(xs), _p(ys), _p(zs), _p(pol), methodeit.encode(), tol, C.byref(mo),
+        self.lib.ifdda_microscope(self.h, len(xs), _p(tab) if tab is not None else None, _p(xs), _p(ys), _p(zs),
+                                  _p(pol), methodeit.encode(), tol, C.byref(mo),
                                   _p(img), _p(xy), _p(kxy), C.byref(ninc), _p(kxi), _p(kyi), C.byref(tol1),
                                   C.byref(nloop), C.byref(ncompte), C.byref(nstop), info, C.byref(opt))
         m = min(ninc.value, cap)

@@ -10,8 +10,8 @@ the reference's outputs in a dict together with nstop/infostr.  Only the
 options on the rigorous-solve path are implemented (trope 'iso' for every
 object here, trope 'ani' for the sphere and the cube, plane waves, nrig = 0,
 0 <= nquad <= 16), and the bright-field and dark-field microscopes in
-transmission or reflection with the FFT lens (nlentille = 1, ntypemic 1 or
-2, nside 0 or 1, nquicklens = 1, cdmlib.f:3660-3800), the wide near field (nproche >= 2) and
+transmission or reflection with or without the FFT lens (nlentille = 1,
+ntypemic 1 or 2, nside 0 or 1, nquicklens 0 or 1, cdmlib.f:3660-3800), the wide near field (nproche >= 2) and
 the scattering cross section / asymmetry factor / Poynting vector
 (nsectionsca = 1, by direct summation or, with nquickdiffracte = 1, from the
 far field on the nfft2d pupil grid); anything else returns nstop = 1 with a
@@ -91,9 +91,10 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
             return _fail("Problem with manification!")
         if abs(theta) >= 90.0:
             return _fail("Illumination on the wrong side with the options")
-        if ntypemic not in (1, 2) or nside not in (0, 1) or nquicklens != 1:
-            return _fail("only the bright-field and dark-field microscopes with the FFT lens")
-        nproche = max(nproche, 1)  # the FFT lens needs the full box (cdmlib.f:631)
+        if ntypemic not in (1, 2) or nside not in (0, 1) or nquicklens not in (0, 1):
+            return _fail("only the bright-field and dark-field microscopes")
+        if nquicklens:
+            nproche = max(nproche, 1)  # the FFT lens needs the full box (cdmlib.f:631)
     if not (nlocal or nmacro or nsection):
         return _fail("No calculation requested!")
     k0 = 2 * math.pi / lam
@@ -153,7 +154,8 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
             m = g.microscope(ob.xs, ob.ys, ob.zs, ob.polarisa, methodeit, tolinit, ntypemic=ntypemic,
                              nfft2d=nfft2d, numaper=numaper, numaperinc=numaperinc, gross=gross,
                              zlens=zlens * 1e-9, P0=P0, w0=(w0 if w0 is not None else 10 * wavelength) * 1e-9,
-                             batch=microscope_batch, precision=precision, nside=nside)
+                             batch=microscope_batch, precision=precision, nside=nside, nquicklens=nquicklens,
+                             tabdip=ob.tabdip_or_none)
             if m.nstop != 0:
                 g.close()
                 out.update(nstop=m.nstop, infostr=m.infostr)

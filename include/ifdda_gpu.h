@@ -233,6 +233,8 @@ typedef struct {
     int batch;         /* illuminations solved together; 0 = 64 */
     int nside;         /* 0 transmission (microsbf / microsdf), 1 reflection (microsbfneg /
                           microsdfneg, cdmlib/microssansinc.f: no image with the incident wave) */
+    int nquicklens;    /* 1 the FFT lens (full box), 0 the lens's far field by direct summation
+                          over the dipoles (any object, microsbf.f:139-157, 627-666) */
 } ifdda_microscope_options;
 
 /* Bright-field or dark-field / phase microscope with the FFT lens, in
@@ -240,10 +242,12 @@ typedef struct {
    microsdf (cdmlib/microsdf.f:1-915) and their reflection forms microsbfneg /
    microsdfneg (cdmlib/microssansinc.f:1-1741), called at
    cdmlib/cdmlib.f:3735-3800, with
-   diffractefft2dlens.f, fouriertoimage.f and deltakroutine.f inside.  The
-   object fills the full box of the spectrum g (nbsphere = nx*ny*nz, the
-   reference forces it when nquicklens = 1, cdmlib.f:631); xs, ys, zs and
-   polarisa (nmax = nbsphere) as for ifdda_inverserig.  Every illumination
+   diffractefft2dlens.f, fouriertoimage.f and deltakroutine.f inside.  With
+   the FFT lens (nquicklens = 1) the object fills the full box of the
+   spectrum g (nbsphere = nx*ny*nz, tabdip NULL: the reference forces it,
+   cdmlib.f:631); with nquicklens = 0 tabdip may name inside-only dipoles as
+   for ifdda_inverserig.  xs, ys, zs: nbsphere positions; polarisa: the
+   (nx*ny*nz,3,3) tensor.  Every illumination
    (both polarisations, s first) is solved in batches of mo->batch through the
    batched solver, without the tol1 < tol check of cdmlib (microsbf does not
    make it).  image receives 6 * n * n values: sqrt(sum |E|^2) over the
@@ -255,8 +259,8 @@ typedef struct {
    units of k0.  tol1, nloop, ncompte: those of the last solve, as the
    reference leaves them.  Errors answer nstop = 1 with the reference's
    messages. */
-int ifdda_microscope(ifdda_green* g, const double* xs, const double* ys, const double* zs,
-                     const ifdda_dcmplx* polarisa, const char* methodeit, double tol,
+int ifdda_microscope(ifdda_green* g, int nbsphere, const int* tabdip, const double* xs, const double* ys,
+                     const double* zs, const ifdda_dcmplx* polarisa, const char* methodeit, double tol,
                      const ifdda_microscope_options* mo, double* image, double* xy, double* kxy, int* ninc,
                      double* kxinc, double* kyinc, double* tol1, int* nloop, int* ncompte, int* nstop,
                      char* infostr, const ifdda_solve_options* opt);

@@ -2718,14 +2718,47 @@ static void orc_fouriertoimage(double dkx, double dky, double gross, zc *F, int 
     }
 }
 
-int orc_microscope(int ntypemic, int nside, const zc *G6, int nx, int ny, int nz, double d, double k0,
-                   const double *xs, const double *ys, const double *zs, const zc *pol,
+/* the lens's far field by direct summation over the dipoles (nquicklens = 0,
+   microsbf.f:627-666): inside dsqrt(kx^2 + ky^2) <= numaper, Ed =
+   k0^2 / (-2 pi i kz) sum exp(-i k0 n.r) (p - n (n.p)), n = (kx, ky, dside kz) / k0 */
+static void orc_lens_direct(int nb, const double *xs, const double *ys, const double *zs, const zc *FF,
+                            double k0, double numaper, double dside, int imax, double dkx, zc *Ed) {
+    const double pi = acos(-1.0);
+    int S = 2 * imax + 1;
+    for (int i = -imax; i <= imax; i++) {
+        double kx = dkx * (double)i;
+        for (int j = -imax; j <= imax; j++) {
+            double ky = dkx * (double)j;
+            zc *o = Ed + ((size_t)(imax + j) * S + (imax + i)) * 3;
+            o[0] = o[1] = o[2] = 0;
+            if (!(sqrt(kx * kx + ky * ky) <= numaper)) continue;
+            double kz = sqrt(k0 * k0 - kx * kx - ky * ky);
+            double n0 = kx / k0, n1 = ky / k0, n2 = sqrt(1.0 - n0 * n0 - n1 * n1) * dside;
+            zc Ex = 0, Ey = 0, Ez = 0;
+            for (int q = 0; q < nb; q++) {
+                zc ctmp = cexp(-I * k0 * (n0 * xs[q] + n1 * ys[q] + n2 * zs[q]));
+                zc ctmp1 = n0 * FF[3 * q] + n1 * FF[3 * q + 1] + n2 * FF[3 * q + 2];
+                Ex += ctmp * (FF[3 * q] - ctmp1 * n0);
+                Ey += ctmp * (FF[3 * q + 1] - ctmp1 * n1);
+                Ez += ctmp * (FF[3 * q + 2] - ctmp1 * n2);
+            }
+            zc ct = -2.0 * pi * I * kz;
+            o[0] = Ex * k0 * k0 / ct;
+            o[1] = Ey * k0 * k0 / ct;
+            o[2] = Ez * k0 * k0 / ct;
+        }
+    }
+}
+
+int orc_microscope(int ntypemic, int nside, int nquicklens, const zc *G6, int nx, int ny, int nz,
+                   double d, double k0, int nbsphere, const int *tabdip, const double *xs,
+                   const double *ys, const double *zs, const zc *pol,
                    const char *methodeit, double tol, double numaper, double numaperinc, int n,
                    double gross, double zlens, double P0, double w0, double *image, double *xy,
                    double *kxy, int *ninc, double *kxinc_out, double *kyinc_out, double *tol1,
                    int *nloop, int *ncompte, char *infostr) {
     const double pi = acos(-1.0);
-    int N = nx * ny * nz;
+    int N = nbsphere, nmax = nx * ny * nz;
     long n3 = 3L * N;
     int n2 = n / 2;
     double numaperk = k0 * numaperinc;
@@ -2745,24 +2778,43 @@ int orc_microscope(int ntypemic, int nside, const zc *G6, int nx, int ny, int nz
     }
     double deltakm = pi / fmax(xmax - xmin, ymax - ymin);
     double dkx = 2.0 * pi / (d * (double)n), dky;
-    if (dkx >= numaperk) {
-        set_info(infostr, "In FFT lens nfft2d too small:Increase size of FFT 1");
-        return 1;
-    }
-    int imul = (int)(deltakm / dkx);
-    if (imul == 0) {
-        set_info(infostr, "In FFT lens nfft2d too small:Increase size of FFT 2");
-        return 1;
-    }
     double deltak;
-    int imaxinc;
-    for (;;) {
-        deltak = dkx * (double)imul;
-        imaxinc = (int)lround(k0 / deltak) + 1;
-        if (imaxinc > 3) break;
-        imul--;
+    int imaxinc, imaxk0 = 0;
+    if (nquicklens == 1) {
+        if (dkx >= numaperk) {
+            set_info(infostr, "In FFT lens nfft2d too small:Increase size of FFT 1");
+            return 1;
+        }
+        int imul = (int)(deltakm / dkx);
         if (imul == 0) {
-            set_info(infostr, "In FFT lens nfft2d too small:Increase size of FFT 3");
+            set_info(infostr, "In FFT lens nfft2d too small:Increase size of FFT 2");
+            return 1;
+        }
+        for (;;) {
+            deltak = dkx * (double)imul;
+            imaxinc = (int)lround(k0 / deltak) + 1;
+            if (imaxinc > 3) break;
+            imul--;
+            if (imul == 0) {
+                set_info(infostr, "In FFT lens nfft2d too small:Increase size of FFT 3");
+                return 1;
+            }
+        }
+    } else {
+        /* microsbf.f:139-157: halve the pupil step until more than 5 points
+           cover k0, then the incidence step from the object's size */
+        for (int k = 0;; k++) {
+            dkx = 2.0 * pi / ((double)n * d) / (double)(1 << k);
+            imaxk0 = (int)lround(k0 / dkx) + 1;
+            if (imaxk0 > 5) break;
+        }
+        for (int k = 0;; k++) {
+            deltak = dkx * round(deltakm / dkx) / (double)(1 << k);
+            imaxinc = (int)lround(k0 / deltak) + 1;
+            if (imaxinc > 2) break;
+        }
+        if (2 * imaxk0 + 1 > n) {
+            set_info(infostr, "In FFT lens nfft2d too small");
             return 1;
         }
     }
@@ -2821,12 +2873,16 @@ int orc_microscope(int ntypemic, int nside, const zc *G6, int nx, int ny, int nz
         for (int q = 0; q < cnt && !nstop; q++) {
             double kxinc = kxi[q], kyinc = kyi[q];
             for (int i = 0; i < N; i++) orc_ondeplanekxky(xs[i], ys[i], zs[i], k0, E0, pp, kxinc, kyinc, FF0 + 3L * i);
-            orc_inverserig(G6, nx, ny, nz, N, NULL, pol, N, FF0, methodeit, tol, FF, FFloc, tol1, nloop,
+            orc_inverserig(G6, nx, ny, nz, N, tabdip, pol, nmax, FF0, methodeit, tol, FF, FFloc, tol1, nloop,
                            ncompte, &nstop, infostr, NULL, 0);
             if (nstop == 1) break;
             zc *Ed = NULL;
-            if (orc_diffractefft2dlens(nx, ny, nz, n, k0, xs, ys, zs, d, FF, numaper, dside, &imax, &Ed,
-                                       infostr)) {
+            if (nquicklens == 0) {
+                imax = imaxk0;
+                Ed = (zc *)malloc(sizeof(zc) * (size_t)(2 * imax + 1) * (2 * imax + 1) * 3);
+                orc_lens_direct(N, xs, ys, zs, FF, k0, numaper, dside, imax, dkx, Ed);
+            } else if (orc_diffractefft2dlens(nx, ny, nz, n, k0, xs, ys, zs, d, FF, numaper, dside, &imax, &Ed,
+                                              infostr)) {
                 nstop = 1;
                 break;
             }

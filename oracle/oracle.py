@@ -373,12 +373,14 @@ def object_arbitrary(nx, ny, nz, d, px, py, pz, eps_site, k0, methode):
 
 
 def microscope(ntypemic, G6, nx, ny, nz, d, k0, xs, ys, zs, polarisa, methodeit, tol, numaper, numaperinc, nfft2d,
-               gross, zlens, P0, w0, nside=0):
+               gross, zlens, P0, w0, nside=0, nquicklens=1, tabdip=None):
     """Bright-field (ntypemic 1, cdmlib/microsbf.f) or dark-field/phase
     (ntypemic 2, cdmlib/microsdf.f) microscope in transmission with the FFT
     lens, full box.  numaper is the objective's NA (multiplied by k0 here as
     cdmlib.f:3674 does); zlens in metres; nside 0 transmission, 1 reflection
-    (microsbfneg / microsdfneg, cdmlib/microssansinc.f: no incident image).  Returns a dict with image (6, n, n)
+    (microsbfneg / microsdfneg, cdmlib/microssansinc.f: no incident image);
+    nquicklens 0: the lens's far field by direct summation, any object
+    (tabdip for inside-only dipoles), 1: the FFT lens on the full box.  Returns a dict with image (6, n, n)
     [x, y, z, incx, incy, incz; row v, column u], xy, kxy, kxinc/kyinc (in
     units of k0), the last solve's tol1/nloop/ncompte, nstop, infostr."""
     n = int(nfft2d)
@@ -393,7 +395,9 @@ def microscope(ntypemic, G6, nx, ny, nz, d, k0, xs, ys, zs, polarisa, methodeit,
     info = C.create_string_buffer(b" " * 64, 65)
     f = lib().orc_microscope
     f.restype = C.c_int
-    nstop = f(C.c_int(ntypemic), C.c_int(nside), _p(_z(G6)), C.c_int(nx), C.c_int(ny), C.c_int(nz), C.c_double(d), C.c_double(k0),
+    tab = None if tabdip is None else np.ascontiguousarray(tabdip, np.int32)
+    nstop = f(C.c_int(ntypemic), C.c_int(nside), C.c_int(nquicklens), _p(_z(G6)), C.c_int(nx), C.c_int(ny),
+              C.c_int(nz), C.c_double(d), C.c_double(k0), C.c_int(len(xs)), _p(tab) if tab is not None else None,
               _p(np.ascontiguousarray(xs, np.float64)), _p(np.ascontiguousarray(ys, np.float64)),
               _p(np.ascontiguousarray(zs, np.float64)), _p(_z(polarisa)), methodeit.encode(), C.c_double(tol),
               C.c_double(numaper * k0), C.c_double(numaperinc), C.c_int(n), C.c_double(gross), C.c_double(zlens),

@@ -52,6 +52,27 @@ def test_microscope_matches_oracle(gctx, orc, ntypemic, nfft2d, nside):
     g.close()
 
 
+@pytest.mark.parametrize("ntypemic,nside,inside", [(1, 0, True), (2, 0, False), (1, 1, True)])
+def test_microscope_direct_lens_matches_oracle(gctx, orc, ntypemic, nside, inside):
+    """nquicklens = 0: the lens's far field by direct summation over the
+    dipoles, on the inside-only object or the full box (microsbf.f:139-157,
+    627-666)."""
+    from ifdda import objects
+    k0 = 2 * math.pi / 632.8e-9
+    ob = objects.sphere(100e-9, 2.25 + 0j, 8, k0, "RR", na=-1 if inside else 0)
+    G = orc.greencalculfft(8, 8, 8, ob.aretecube, k0)
+    tab = ob.tabdip if inside else None
+    ref = orc.microscope(ntypemic, G, 8, 8, 8, ob.aretecube, k0, ob.xs, ob.ys, ob.zs, ob.polarisa, "GPBICG1", 1e-6,
+                         0.9, 0.5, 64, 100.0, 50e-9, 1.0, 6328e-9, nside=nside, nquicklens=0, tabdip=tab)
+    g = gctx.green(8, 8, 8, ob.aretecube, k0)
+    r = g.microscope(ob.xs, ob.ys, ob.zs, ob.polarisa, "GPBICG1", 1e-6, ntypemic=ntypemic, nfft2d=64, numaper=0.9,
+                     numaperinc=0.5, gross=100.0, zlens=50e-9, P0=1.0, w0=6328e-9, nside=nside, nquicklens=0,
+                     tabdip=tab)
+    _compare(r, ref)
+    assert r.image[0].max() > 0
+    g.close()
+
+
 def test_microscope_batches_agree(gctx, orc):
     """Illuminations split over batches of 3 give the image of one batch."""
     ob, k0 = _object()
