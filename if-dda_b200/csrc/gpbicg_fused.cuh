@@ -39,9 +39,9 @@ template <class T> struct PreGpP {
         upd_w = S[rhs].itno > 0;
     }
     template <class C> __device__ __forceinline__ C value(int e) {
-        const C pc = from_d<C>(zadd(ld(r, e), zmul(beta, zsub(ld(p, e), ld(u, e)))));
+        const C pc = from_d<C>(zadd(ldg(r, e), zmul(beta, zsub(ldg(p, e), ldg(u, e)))));
         p[e] = pc;
-        if (upd_w) st(w, e, zadd(ld(at, e), zmul(beta, ld(ap, e))));
+        if (upd_w) st(w, e, zadd(ldg(at, e), zmul(beta, ldg(ap, e))));
         return pc;
     }
 };
@@ -59,7 +59,7 @@ template <class T> struct EpiGpAlpha {
         acc[0] = make_double2(0, 0);
     }
     template <class C> __device__ __forceinline__ void elem(int e, C y) {
-        acc[0] = zadd(acc[0], zconjmul(ld(r0, e), to_d(y)));
+        acc[0] = zadd(acc[0], zconjmul(ldg(r0, e), to_d(y)));
     }
     __device__ __forceinline__ void finish(int rhs, const double2* tot) {
         GpAlpha<T>{V, S}.finish(rhs, S[rhs], status[rhs], tot);
@@ -89,8 +89,8 @@ template <class T> struct PreGpYT {
         acc[0] = acc[1] = make_double2(0, 0);
     }
     template <class C> __device__ __forceinline__ C value(int e) {
-        const double2 rr = ld(r, e), apv = ld(ap, e);
-        const double2 yv = zadd(zsub(ld(t, e), rr), zmul(alpha, zsub(apv, ld(w, e))));
+        const double2 rr = ldg(r, e), apv = ldg(ap, e);
+        const double2 yv = zadd(zsub(ldg(t, e), rr), zmul(alpha, zsub(apv, ldg(w, e))));
         const double2 tv = zsub(rr, zmul(alpha, apv));
         st(y, e, yv);
         const C tc = from_d<C>(tv);
@@ -120,8 +120,8 @@ template <class T> struct EpiGpZeta {
     template <class C> __device__ __forceinline__ void elem(int e, C atc) {
         const double2 a = to_d(atc);
         acc[0] = zadd(acc[0], zconjmul(a, a));
-        acc[1] = zadd(acc[1], zconjmul(a, ld(y, e)));
-        acc[2] = zadd(acc[2], zconjmul(a, ld(t, e)));
+        acc[1] = zadd(acc[1], zconjmul(a, ldg(y, e)));
+        acc[2] = zadd(acc[2], zconjmul(a, ldg(t, e)));
     }
     __device__ __forceinline__ void finish(int rhs, const double2* tot) {
         KState& s = S[rhs];

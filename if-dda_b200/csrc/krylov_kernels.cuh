@@ -53,6 +53,11 @@ template <class T> struct Slots {
 };
 
 template <class C> __device__ __forceinline__ double2 ld(const C* p, long i) { return to_d(p[i]); }
+// The same through the read-only path.  For vectors that a kernel reads at an
+// element before (or without) writing that element from the same thread: the
+// loads may then be issued ahead of the stores to other elements, instead of
+// waiting behind them for want of alias information.
+template <class C> __device__ __forceinline__ double2 ldg(const C* p, long i) { return to_d(__ldg(p + i)); }
 template <class C> __device__ __forceinline__ void st(C* p, long i, double2 v) { p[i] = from_d<C>(v); }
 
 constexpr int KNT = 256;
@@ -217,19 +222,19 @@ template <class T> struct GpUpdate {
     KState* stt;
     int tcur, tnew;  // tcur = t_old after GpYT
     __device__ void elem(const KState& s, int r, long i, double2* acc) const {
-        const double2 ap = ld(V.v(G_AP, r), i), told = ld(V.v(tcur, r), i), rr = ld(V.v(G_R, r), i);
-        const double2 u0 = ld(V.v(G_U, r), i), z0 = ld(V.v(G_Z, r), i);
+        const double2 ap = ldg(V.v(G_AP, r), i), told = ldg(V.v(tcur, r), i), rr = ldg(V.v(G_R, r), i);
+        const double2 u0 = ldg(V.v(G_U, r), i), z0 = ldg(V.v(G_Z, r), i);
         const double2 u = zadd(zmul(s.dzeta, ap), zmul(s.eta, zadd(zsub(told, rr), zmul(s.beta, u0))));
         const double2 z = zsub(zadd(zmul(s.dzeta, rr), zmul(s.eta, z0)), zmul(s.alpha, u));
-        const double2 x = zadd(zadd(ld(V.v(G_X, r), i), zmul(s.alpha, ld(V.v(G_P, r), i))), z);
-        const double2 rn = zsub(zsub(ld(V.v(tnew, r), i), zmul(s.eta, ld(V.v(G_Y, r), i))),
-                                zmul(s.dzeta, ld(V.v(G_AT, r), i)));
+        const double2 x = zadd(zadd(ldg(V.v(G_X, r), i), zmul(s.alpha, ldg(V.v(G_P, r), i))), z);
+        const double2 rn = zsub(zsub(ldg(V.v(tnew, r), i), zmul(s.eta, ldg(V.v(G_Y, r), i))),
+                                zmul(s.dzeta, ldg(V.v(G_AT, r), i)));
         st(V.v(G_U, r), i, u);
         st(V.v(G_Z, r), i, z);
         st(V.v(G_X, r), i, x);
         st(V.v(G_R, r), i, rn);
         acc[0].x += rn.x * rn.x + rn.y * rn.y;
-        acc[1] = zadd(acc[1], zconjmul(ld(V.v(G_R0, r), i), rn));
+        acc[1] = zadd(acc[1], zconjmul(ldg(V.v(G_R0, r), i), rn));
     }
     __device__ void finish(int, KState& s, int& status, const double2* a) const {
         s.residu = sqrt(a[0].x) / s.norm;

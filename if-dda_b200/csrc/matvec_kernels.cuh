@@ -152,7 +152,7 @@ template <class T> struct PreNone {
     const cplx<T>* x;
     double2 acc[1];
     __device__ __forceinline__ void bind(const MvArgs<T>& a, int rhs) { x = a.x + rhs * a.xstride; }
-    template <class C> __device__ __forceinline__ C value(int e) { return x[e]; }
+    template <class C> __device__ __forceinline__ C value(int e) { return __ldg(x + e); }
 };
 
 // Element offsets inside one right-hand side's vectors and scratch fit in 32
@@ -172,16 +172,16 @@ template <class T, bool TAB, class Pre> struct FwdXLoad {
         const int site = site0 + jl * nx + p;
         int d = site;
         if (TAB) {
-            const int t = tab[site];
+            const int t = __ldg(tab + site);
             if (t == 0) return czero<C>();
             d = t - 1;
         }
-        if (amode == ALPHA_ISO) return cmul(alpha[d], pre.template value<C>(3 * d + c));
+        if (amode == ALPHA_ISO) return cmul(__ldg(alpha + d), pre.template value<C>(3 * d + c));
         if (amode == ALPHA_FULL) {
             C acc = czero<C>();
 #pragma unroll
             for (int q = 0; q < 3; q++)
-                acc = cadd(acc, cmul(alpha[d + nmax * (c + 3 * q)], pre.template value<C>(3 * d + q)));
+                acc = cadd(acc, cmul(__ldg(alpha + d + nmax * (c + 3 * q)), pre.template value<C>(3 * d + q)));
             return acc;
         }
         return pre.template value<C>(3 * d + c);
@@ -520,11 +520,12 @@ template <class T, bool TAB, class Epi> struct InvXStore {
         const int site = site0 + jl * nx + p;
         int d = site;
         if (TAB) {
-            const int t = tab[site];
+            const int t = __ldg(tab + site);
             if (t == 0) return;
             d = t - 1;
         }
-        const C y = csub(bv[3 * d + c], cscale(v, inv_m));
+        // b is read at an element before this thread writes y there (b may be y)
+        const C y = csub(__ldg(bv + 3 * d + c), cscale(v, inv_m));
         yv[3 * d + c] = y;
         epi.elem(3 * d + c, y);
     }
