@@ -513,6 +513,73 @@ def run_matvec(args):
     return 0
 
 
+def run_solve_passes(args):
+    """The five mat-vec passes inside complete solves of the workload's first
+    right-hand side (mixed, then FP64): each pass's launches timed with CUDA
+    events (the library then runs the solver loop without CUDA graphs, so the
+    pass kernels carry their fused Krylov work as in the solve), next to the
+    solve time with graphs.  Also the target of the per-iteration launch list
+    in profiles/."""
+    import ctypes as C
+    import torch
+    import ifdda
+    from ifdda import IFDDA_FP32, IFDDA_FP64, IFDDA_MIXED
+
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    w = WORKLOADS[args.workload]()
+    ob = w.ob
+    ctx = ifdda.Context(local)
+    lib = ctx.lib
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    g = ctx.green(ob.nx, ob.ny, ob.nz, ob.aretecube, w.k0)
+    bm, a1, a2, pp = w.beams[0]
+    ff0 = ctx.planewaves(ob.xs, ob.ys, ob.zs, w.k0, w.E0, [bm], [a1], [a2], [pp])
+    ff0_d = torch.from_numpy(ff0).to(dev)
+    pol_d = torch.from_numpy(ob.polarisa).to(dev)
+    tab_d = torch.from_numpy(ob.tabdip).to(dev) if ob.inside_only else None
+    ff_d, loc_d = torch.empty_like(ff0_d), torch.empty_like(ff0_d)
+
+    def solve(prec):
+        r = g.inverserig_device(1, ob.nbsphere, ob.nmax, tab_d.data_ptr() if tab_d is not None else None,
+                                pol_d.data_ptr(), ff0_d.data_ptr(), ff_d.data_ptr(), loc_d.data_ptr(), w.method, TOL,
+                                precision=prec)
+        if r["nstop"] != 0:
+            raise RuntimeError(r["infostr"].strip())
+        return r
+
+    names = {1: "fwd_x", 2: "fwd_y", 3: "zconv", 4: "inv_y", 5: "inv_x"}
+    out = {}
+    for name, prec, pbits in (("mixed", IFDDA_MIXED, IFDDA_FP32), ("fp64", IFDDA_FP64, IFDDA_FP64)):
+        for _ in range(args.warmup):
+            solve(prec)
+        ts = []
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = solve(prec)
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        res = {"ms_per_solve": statistics.median(ts), "nloop": int(r["nloop"][0]), "ncompte": int(r["ncompte"][0])}
+        for ps in range(1, 6):
+            lib.ifdda_timing_enable(ps, pbits)
+            solve(prec)
+            torch.cuda.synchronize()
+            nl, ms = C.c_int(0), C.c_double(0)
+            lib.ifdda_timing_read(C.byref(nl), C.byref(ms))
+            res[names[ps]] = {"launches": nl.value, "us_per_launch": round(1e3 * ms.value / max(nl.value, 1), 2)}
+        lib.ifdda_timing_enable(0, -1)
+        out[name] = res
+    if rank == 0:
+        print(json.dumps({"mode": "passes", "workload": w.desc, "solve": out}), flush=True)
+    g.close()
+    ctx.close()
+    return 0
+
+
 def run_serving(args):
     """Config 4: a seeded request stream through the continuous-batching
     server, mixed precision then plain FP64 on the same stream."""
@@ -626,8 +693,8 @@ def main():
     ap.add_argument("--requests", type=int, default=2000, help="c4: stream length")
     ap.add_argument("--rate", type=float, default=100.0, help="c4: Poisson arrival rate (requests/s)")
     ap.add_argument("--slots", type=int, default=4, help="c4: concurrent solver slots")
-    ap.add_argument("--mode", default="solve", choices=["solve", "matvec"],
-                    help="matvec: time the five mat-vec passes only")
+    ap.add_argument("--mode", default="solve", choices=["solve", "matvec", "passes"],
+                    help="matvec: time the five mat-vec passes only; passes: the passes inside solves")
     args = ap.parse_args()
     if args.impl == "reference":
         if args.workload in ("c4", "mic"):
@@ -639,6 +706,8 @@ def main():
         return run_microscope(args)
     if args.mode == "matvec":
         return run_matvec(args)
+    if args.mode == "passes":
+        return run_solve_passes(args)
     return run_gpu(args)
 
 
