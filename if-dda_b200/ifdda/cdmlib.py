@@ -8,7 +8,9 @@ field (:1172-1187), Green spectrum (:1518-1546), solve (:1555-1597), local and
 macroscopic fields (:2497-2655), cross sections (:2717-2778) -- and returns
 the reference's outputs in a dict together with nstop/infostr.  Only the
 options on the rigorous-solve path are implemented (trope 'iso' for every
-object here, trope 'ani' for the sphere and the cube, plane waves, nrig = 0,
+object here, trope 'ani' for the sphere, the cube (epsani), the concentric
+spheres (epsanis, one tensor per shell) and the arbitrary object (epsani_site,
+one per dipole), plane waves, nrig = 0,
 0 <= nquad <= 16), and the bright-field and dark-field microscopes in
 transmission or reflection with or without the FFT lens (nlentille = 1,
 ntypemic 1 or 2, nside 0 or 1, nquicklens 0 or 1, cdmlib.f:3660-3800), the wide near field (nproche >= 2) and
@@ -36,7 +38,7 @@ def _fail(msg, **extra):
 
 
 def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, rayons=None, epss=None,
-           nx=None, ny=None, nz=None, aretecube=None, epsani=None, lc=None, hc=None, ng=0, positions=None, eps_site=None,
+           nx=None, ny=None, nz=None, aretecube=None, epsani=None, epsanis=None, epsani_site=None, lc=None, hc=None, ng=0, positions=None, eps_site=None,
            beam="pwavelinear", theta=0.0, phi=0.0, pp=1.0, incidences=None, P0=1.0, w0=None,
            tolinit=1e-4, methodeit="GPBICG1", polarizability="RR", trope="iso", nproche=0, nrig=0, nquad=0,
            nlocal=1, nmacro=1, nsection=1, precision=0, nlentille=0, ntypemic=1, nside=0, nquicklens=1,
@@ -56,13 +58,18 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
     if trope not in ("iso", "ani"):
         return _fail(f"trope {trope!r} is neither 'iso' nor 'ani'")
     if trope == "ani":
-        # cdmlib.f:597-611
-        if epsani is None or float(np.sum(np.abs(np.asarray(epsani, np.complex128)))) == 0.0:
+        # cdmlib.f:597-611 (the first object's tensor: epsanimulti(:,:,1))
+        first = epsani if epsani is not None else (epsanis[0] if epsanis is not None else epsani_site)
+        if first is None or float(np.sum(np.abs(np.asarray(first, np.complex128)))) == 0.0:
             return _fail("No relative permittivity given")
         if polarizability not in ("RR", "CM"):
             return _fail("Polarizability should be CM or RR with anisotropy")
-        if object not in ("sphere", "cube"):
+        if object not in ("sphere", "cube", "concentricsphere", "arbitrary"):
             return _fail(f"anisotropic {object!r} not handled by the GPU drop-in")
+        if object == "concentricsphere" and (epsanis is None or rayons is None or len(epsanis) != len(rayons)):
+            return _fail("epsanis: one 3x3 tensor per sphere")
+        if object == "arbitrary" and epsani_site is None:
+            return _fail("epsani_site: one 3x3 tensor per dipole")
     if nrig != 0:
         return _fail("only the rigorous solve (nrig = 0) is handled by the GPU drop-in")
     if not 0 <= nquad <= 16:
@@ -113,11 +120,12 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
                                       polarizability)
         elif object == "concentricsphere":
             ob = objects.concentric([r * 1e-9 for r in rayons], epss, nnnr, k0, polarizability,
-                                    na=-1 if inside else 0)
+                                    na=-1 if inside else 0, epsanis=epsanis if trope == "ani" else None)
         else:
             pos = np.asarray(positions, float) * 1e-9
-            ob = objects.arbitrary(nx, ny, nz, aretecube * 1e-9, pos[:, 0], pos[:, 1], pos[:, 2], eps_site, k0,
-                                   polarizability)
+            ob = objects.arbitrary(nx, ny, nz, aretecube * 1e-9, pos[:, 0], pos[:, 1], pos[:, 2],
+                                   eps_site if eps_site is not None else np.ones(len(pos)), k0, polarizability,
+                                   epsani_site=epsani_site if trope == "ani" else None)
     except ValueError as e:
         return _fail(str(e))
     if ob.nbsphere == 0:

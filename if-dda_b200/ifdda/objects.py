@@ -7,14 +7,15 @@ restated with numpy so the GPU path gets its inputs without the oracle:
   sphere            cdmlib/objectsphere.f:94-195          (na = -1 or 0; trope 'ani')
   cube              cdmlib/objectcube.f:60-130            (trope 'ani')
   inhomocuboid      cdmlib/objectparainhomonxnynz.f:85-237 (+ SUNIF, cdmlib/random.f:19-56)
-  concentric        cdmlib/objectsphereconcentric.f:76-230
-  arbitrary         cdmlib/objectarbitrary.f:81-157 (arrays instead of a file)
+  concentric        cdmlib/objectsphereconcentric.f:76-230 (trope 'ani': a tensor per shell)
+  arbitrary         cdmlib/objectarbitrary.f:81-157 (arrays instead of a file;
+                    trope 'ani': a tensor per dipole)
 All lengths are in metres (the reference multiplies its nm inputs by 1e-9).
 A DipoleObject carries the reference's arrays: xs, ys, zs (nbsphere),
 tabdip (nx*ny*nz, 1-based, 0 = empty), polarisa and epsilon as (nmax,3,3)
 column-major flattened, plus ``alpha`` and ``eps`` (one isotropic value per
 dipole) or, for an anisotropic object, ``alpha_t`` and ``eps_t`` (the 3x3
-tensors every dipole of the object shares).
+tensors every dipole of the object shares, or one per dipole).
 """
 from __future__ import annotations
 
@@ -39,8 +40,10 @@ class DipoleObject:
     alpha: np.ndarray   # isotropic polarisability per dipole
     eps: np.ndarray     # isotropic permittivity per dipole
     inside_only: bool
-    alpha_t: np.ndarray = None  # anisotropic object: 3x3 polarisability (row a, column b)
-    eps_t: np.ndarray = None    # anisotropic object: 3x3 permittivity
+    # anisotropic object: the 3x3 polarisability / permittivity (row a, column
+    # b) shared by all its dipoles, or one per dipole (nbsphere, 3, 3)
+    alpha_t: np.ndarray = None
+    eps_t: np.ndarray = None
     # full box with an anisotropic object: which sites hold a dipole of it
     occupied: np.ndarray = None
 
@@ -58,7 +61,8 @@ class DipoleObject:
             on = np.ones(self.nbsphere, bool) if self.occupied is None else self.occupied
             for a in range(3):
                 for b in range(3):
-                    t[a, b, : self.nbsphere] = np.where(on, full[a, b], vacuum if a == b else 0.0)
+                    v = full[:, a, b] if full.ndim == 3 else full[a, b]
+                    t[a, b, : self.nbsphere] = np.where(on, v, vacuum if a == b else 0.0)
         # (nmax,3,3) column-major: (n,a,b) at n + nmax*(a + 3b)  ->  t[b, a, n]
         return np.ascontiguousarray(t.transpose(1, 0, 2)).reshape(-1)
 
@@ -116,8 +120,10 @@ def polaepstens(aretecube: float, epsani, k0: float, methode: str, eps0: float =
     """Polarisability tensor of a cube of anisotropic permittivity epsani (3x3)
     (polaepstens.f:1-122): alpha0 = V (eps - eps0 I) (eps + 2 eps0 I)^-1,
     CM: alpha0 eps0, RR: (I - 2/3 i k^3 alpha0)^-1 alpha0 eps0; inv = -1
-    returns the inverse.  Only CM and RR exist for a tensor."""
-    e = np.asarray(epsani, np.complex128).reshape(3, 3)
+    returns the inverse.  Only CM and RR exist for a tensor.  epsani may
+    also be a stack (..., 3, 3), one tensor per dipole."""
+    e = np.asarray(epsani, np.complex128)
+    e = e.reshape(3, 3) if e.size == 9 else e.reshape(-1, 3, 3)
     pi = math.acos(-1.0)
     k03 = k0 ** 3 * math.sqrt(eps0) ** 3
     if dis == 0:
@@ -145,12 +151,31 @@ def _lattice(n1, n2, n3):
 
 def _finish_ani(nx, ny, nz, d, x, y, z, keep, epsani, k0, methode, inside_only) -> DipoleObject:
     """Anisotropic object (trope = 'ani'): every dipole gets polaepstens of
-    epsani with dis = 1 (objectsphere.f:129-135); 'PS' is refused there."""
+    its permittivity with dis = 1 (objectsphere.f:129-135); 'PS' is refused
+    there.  epsani: one 3x3 tensor for the object, or one per lattice site
+    (nx*ny*nz, 3, 3)."""
     if methode[:2] == "PS":
         raise ValueError("anisotrope with PS")
-    e = np.asarray(epsani, np.complex128).reshape(3, 3)
-    at = polaepstens(d, e, k0, methode, dis=1)
+    e = np.asarray(epsani, np.complex128)
     N = nx * ny * nz
+    if e.size != 9:
+        e = e.reshape(N, 3, 3)
+        if inside_only:
+            tab = np.zeros(N, np.int32)
+            idx = np.nonzero(keep)[0]
+            tab[idx] = np.arange(1, len(idx) + 1, dtype=np.int32)
+            es = e[idx].copy()
+            at = polaepstens(d, es, k0, methode, dis=1)
+            return DipoleObject(nx, ny, nz, d, len(idx), N, x[idx].copy(), y[idx].copy(), z[idx].copy(), tab,
+                                at[:, 0, 0].copy(), es[:, 0, 0].copy(), True, at, es)
+        es = np.where(keep[:, None, None], e, np.eye(3))
+        at = polaepstens(d, es, k0, methode, dis=1)
+        tab = np.arange(1, N + 1, dtype=np.int32)
+        return DipoleObject(nx, ny, nz, d, N, N, x.copy(), y.copy(), z.copy(), tab,
+                            np.where(keep, at[:, 0, 0], 0.0), np.where(keep, es[:, 0, 0], 1.0 + 0j), False, at, es,
+                            keep.copy())
+    e = e.reshape(3, 3)
+    at = polaepstens(d, e, k0, methode, dis=1)
     if inside_only:
         tab = np.zeros(N, np.int32)
         idx = np.nonzero(keep)[0]
@@ -259,9 +284,11 @@ def inhomocuboid(nx, ny, nz, d, eps, lc, hc, ng, k0, methode="RR") -> DipoleObje
     return _finish(nx, ny, nz, d, x, y, z, np.ones(N, bool), eps_site, k0, methode, False)
 
 
-def concentric(rayons, epss, nnnr, k0, methode="RR", na=-1) -> DipoleObject:
+def concentric(rayons, epss, nnnr, k0, methode="RR", na=-1, epsanis=None) -> DipoleObject:
     """objetsphereconcentric: d = 2 r_out / nnnr; shell l holds r in
-    [r_{l-1}, r_l] (objectsphereconcentric.f:112-167)."""
+    [r_{l-1}, r_l] (objectsphereconcentric.f:112-167); epsanis (one 3x3 per
+    shell) makes it anisotropic (trope = 'ani', objectsphereconcentric.f:
+    128-146)."""
     rayons = list(rayons)
     if rayons[0] == 0.0:
         raise ValueError("spheres concentrics: 1st rayon=0")
@@ -282,15 +309,25 @@ def concentric(rayons, epss, nnnr, k0, methode="RR", na=-1) -> DipoleObject:
         sel = (ray > rayons[0]) & (ray <= rayons[l - 1]) & (ray >= rayons[l - 2])
         shell[sel] = l
     keep = shell > 0
+    if epsanis is not None:
+        ea = np.asarray(epsanis, np.complex128).reshape(ns, 3, 3)
+        e_site = np.where(keep[:, None, None], ea[np.maximum(shell - 1, 0)], np.eye(3))
+        return _finish_ani(nnnr, nnnr, nnnr, d, x, y, z, keep, e_site, k0, methode, na == -1)
     epss = np.asarray(epss, np.complex128)
     eps_site = np.where(keep, epss[np.maximum(shell - 1, 0)], 1.0)
     return _finish(nnnr, nnnr, nnnr, d, x, y, z, keep, eps_site, k0, methode, na == -1)
 
 
-def arbitrary(nx, ny, nz, d, x, y, z, eps_site, k0, methode="RR") -> DipoleObject:
+def arbitrary(nx, ny, nz, d, x, y, z, eps_site, k0, methode="RR", epsani_site=None) -> DipoleObject:
     """objetarbitrary without the file: every lattice site is a dipole of its
-    own isotropic permittivity (vacuum sites have eps = 1, alpha = 0)."""
+    own isotropic permittivity (vacuum sites have eps = 1, alpha = 0), or of
+    its own 3x3 tensor epsani_site (nx*ny*nz, 3, 3) (trope = 'ani',
+    objectarbitrary.f:130-151)."""
     N = nx * ny * nz
+    if epsani_site is not None:
+        return _finish_ani(nx, ny, nz, d, np.asarray(x, float), np.asarray(y, float), np.asarray(z, float),
+                           np.ones(N, bool), np.asarray(epsani_site, np.complex128).reshape(N, 3, 3), k0, methode,
+                           False)
     eps_site = np.asarray(eps_site, np.complex128).reshape(N)
     return _finish(nx, ny, nz, d, np.asarray(x, float), np.asarray(y, float), np.asarray(z, float),
                    np.ones(N, bool), eps_site, k0, methode, False)

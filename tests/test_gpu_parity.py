@@ -482,3 +482,24 @@ def test_farfield_fft_matches_oracle(gctx, orc, nfft2d):
     ok = np.isfinite(ref["poyntingfield"])
     assert np.array_equal(ok, np.isfinite(got["poyntingfield"]))
     assert rel(got["poyntingfield"][ok], ref["poyntingfield"][ok]) < 1e-10
+
+
+def test_cdmlib_anisotropic_concentric_matches_oracle(orc):
+    """trope = 'ani' on the concentric spheres (one tensor per shell): the
+    solve with per-dipole tensors against the oracle's solve of the same
+    object (its tensors checked against polaepstens in the CPU tests)."""
+    from ifdda import objects
+    from ifdda.cdmlib import cdmlib
+    shells = [np.array([[2.25, 0.1j, 0.0], [-0.1j, 2.5 + 0.02j, 0.05], [0.0, 0.05, 3.0]]), 1.8 * np.eye(3)]
+    out = cdmlib(wavelength=632.8, object="concentricsphere", rayons=[60.0, 120.0], epss=[2.0, 2.0], nnnr=12,
+                 tolinit=1e-8, methodeit="GPBICG1", trope="ani", epsanis=shells, nproche=0, P0=1.0, w0=6328.0)
+    assert out["nstop"] == 0, out["infostr"]
+    k0 = 2 * math.pi / 632.8e-9
+    ob = objects.concentric([60e-9, 120e-9], [2.0, 2.0], 12, k0, "RR", na=-1, epsanis=shells)
+    E0, _ = orc.irradiance(1.0, 6328e-9)
+    ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 1.0, 0, 0.0, 0.0)
+    G = orc.greencalculfft(12, 12, 12, ob.aretecube, k0)
+    ref = orc.inverserig(G, 12, 12, 12, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-8, tabdip=ob.tabdip)
+    assert rel(out["localfield"], ref["FFloc"]) < 1e-9
+    em = orc.local_macro_all(ob.nbsphere, ob.nmax, ob.epsilon, ref["FFloc"], ob.aretecube, k0)
+    assert rel(out["macroscopicfield"][0], em) < 1e-9

@@ -30,7 +30,12 @@ def test_cdmlib_driver_rejects_like_the_reference():
                   epsani=np.zeros((3, 3)))["infostr"] == "No relative permittivity given"
     assert cdmlib(wavelength=632.8, object="sphere", rayon=100.0, nnnr=8, trope="ani", epsani=ani,
                   polarizability="LA")["infostr"] == "Polarizability should be CM or RR with anisotropy"
-    assert cdmlib(wavelength=632.8, object="concentricsphere", nnnr=8, trope="ani", epsani=ani)["nstop"] == 1
+    assert cdmlib(wavelength=632.8, object="inhomocuboid2", nnnr=8, trope="ani", epsani=ani)["nstop"] == 1
+    assert cdmlib(wavelength=632.8, object="concentricsphere", rayons=[90.0, 190.0], epss=[3.0, 2.0], nnnr=8,
+                  trope="ani", epsani=ani)["infostr"] == "epsanis: one 3x3 tensor per sphere"
+    assert cdmlib(wavelength=632.8, object="arbitrary", nx=2, ny=2, nz=2, aretecube=10.0,
+                  positions=np.zeros((8, 3)), trope="ani", epsani=ani)["infostr"] == \
+        "epsani_site: one 3x3 tensor per dipole"
     assert cdmlib(wavelength=632.8, object="sphere", rayon=1000.0, eps=2.25, nnnr=4, trope="ani",
                   epsani=ani)["infostr"] == "Meshsize larger than lambda/4!"
     # microscope options (cdmlib.f:365-389)

@@ -411,3 +411,41 @@ def test_farfield_fft_converges_to_the_direct_sum(orc):
     assert abs(b["gasym"] - a["gasym"]) < 0.01
     with pytest.raises(ValueError, match="In FFT Poynting nfft2d too small"):
         orc.farfield_fft(8, 8, 8, ob.aretecube, ob.xs, ob.ys, ob.zs, sol["FF"], k0, E0 ** 2, 0.0, 0.0, 16, 36, 72)
+
+
+def test_anisotropic_concentric_and_arbitrary(orc):
+    """trope = 'ani' for the concentric spheres (one tensor per shell,
+    objectsphereconcentric.f:128-146) and the arbitrary object (one tensor per
+    dipole, objectarbitrary.f:130-151): the geometry of the isotropic builders,
+    every dipole's tensors from the oracle's polaepstens."""
+    from ifdda import objects
+    k0 = 2 * math.pi / 632.8e-9
+    shells = [EPSANI, EPSANI.T + 0.5 * np.eye(3)]
+    for na in (-1, 0):
+        a = objects.concentric([0.9e-6, 1.9e-6], [3.0, 2.0], 12, k0, "RR", na=na, epsanis=shells)
+        iso = objects.concentric([0.9e-6, 1.9e-6], [3.0, 2.0], 12, k0, "RR", na=na)
+        assert a.nbsphere == iso.nbsphere and np.array_equal(a.tabdip, iso.tabdip)
+        pol = a.polarisa.reshape(3, 3, a.nmax)   # [b][a][n]
+        eps = a.epsilon.reshape(3, 3, a.nmax)
+        ref = [orc.polaepstens(a.aretecube, e, k0, "RR") for e in shells]
+        isoe = iso.epsilon.reshape(3, 3, iso.nmax)[0, 0, : a.nbsphere]
+        for n in range(a.nbsphere):
+            e = isoe[n]
+            if e == 1.0:  # vacuum site of the full box
+                assert np.array_equal(pol[:, :, n], np.zeros((3, 3)))
+                assert np.array_equal(eps[:, :, n], np.eye(3))
+                continue
+            s = 0 if e == 3.0 else 1
+            assert np.allclose(pol[:, :, n].T, ref[s], rtol=1e-13, atol=1e-13 * abs(ref[s]).max())
+            assert np.array_equal(eps[:, :, n].T, shells[s])
+    rng = np.random.default_rng(5)
+    nx = ny = nz = 4
+    N = nx * ny * nz
+    t = rng.uniform(1.5, 3.0, (N, 3, 3)) + 0.01j * rng.uniform(0, 1, (N, 3, 3))
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    x, y, z = (v.transpose(2, 1, 0).reshape(-1) * 10e-9 for v in (i, j, k))
+    ob = objects.arbitrary(nx, ny, nz, 10e-9, x, y, z, np.ones(N), k0, "CM", epsani_site=t)
+    pol = ob.polarisa.reshape(3, 3, N)
+    for n in range(N):
+        r = orc.polaepstens(10e-9, t[n], k0, "CM")
+        assert np.allclose(pol[:, :, n].T, r, rtol=1e-13, atol=1e-13 * abs(r).max())
