@@ -929,6 +929,105 @@ int ifdda_nearfield_wide(ifdda_ctx* ctx, int nx, int ny, int nz, int nxmp, int n
     IFDDA_GUARD_END(ctx, nullptr)
 }
 
+int ifdda_holography(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, const double* xs,
+                     const double* ys, const double* zs, const ifdda_dcmplx* FF, ifdda_dcmplx E0, double theta,
+                     double phi, double pp, int nfft2d, double numaper, double gross, double zlens, int nside,
+                     ifdda_dcmplx* image, ifdda_dcmplx* fourier, double* xy, double* kxy, int* imaxk0,
+                     char* infostr) {
+    if (!ctx || !xs || !ys || !zs || !FF || !image || nx < 1 || ny < 1 || nz < 1) {
+        set_info(infostr, "invalid argument");
+        return 1;
+    }
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(ctx->device);
+    AllocStreamScope as(ctx->stream);
+    cudaStream_t st = ctx->stream;
+    auto fail = [&](const char* msg) {
+        set_info(infostr, msg);
+        ctx->last_error = msg;
+        return 1;
+    };
+    const int n = nfft2d;
+    const long N = (long)nx * ny * nz;
+    if (nside != 0 && nside != 1) return fail("nside must be 0 (transmission) or 1 (reflection)");
+    if (!image_length_supported(n)) return fail("nfft2d not supported: a power of two from 32 to 4096");
+    if (nx > n || ny > n) return fail("nfft2d smaller than the object");
+    const double pi = 3.14159265358979323846, dside = nside == 1 ? -1.0 : 1.0;
+    const double na = numaper * k0, dkx = 2.0 * pi / ((double)n * aretecube);
+    // diffractefft2dlens.f:29-73
+    if (dkx >= na) return fail("In FFT lens nfft2d too small");
+    const int imax = (int)std::lround(k0 / dkx) + 1, S = 2 * imax + 1;
+    if (S > n) return fail("In FFT diffraction for lens nfft2d too small!");
+    if (S < 7) return fail("In FFT diffract nfft2d too small");
+    MicGeom m{};
+    m.nx = nx;
+    m.ny = ny;
+    m.nz = nz;
+    m.n = n;
+    m.imax = imax;
+    m.k0 = k0;
+    m.dkx = dkx;
+    m.dky = dkx;
+    m.numaper = na;
+    m.var1 = (xs[0] + (double)(n / 2) * aretecube) * dkx;
+    m.var2 = (ys[0] + (double)(n / 2) * aretecube) * dkx;
+    m.zlens = zlens * dside;
+    m.gross = gross;
+    m.dside = dside;
+    // grid point of the incident wave (diffractefft2dinc.f:75-83, deltakroutine.f)
+    const double kxinc = std::sin(theta * pi / 180.0) * std::cos(phi * pi / 180.0) * k0;
+    const double kyinc = std::sin(theta * pi / 180.0) * std::sin(phi * pi / 180.0) * k0;
+    int ik = (int)std::lround(kxinc / dkx), jk = (int)std::lround(kyinc / dkx);
+    {
+        const double kx = dkx * ik, ky = dkx * jk;
+        if (!(kx * kx + ky * ky <= k0 * k0)) {
+            ik = (int)(kxinc / dkx);
+            jk = (int)(kyinc / dkx);
+        }
+    }
+    std::vector<double> zp(nz);
+    for (int k = 0; k < nz; k++) zp[k] = zs[(long)nx * ny * k];
+    std::vector<double2> twh(n);
+    for (int j = 0; j < n; j++) {
+        const double a = 2.0 * pi * (double)j / (double)n;
+        twh[j] = make_double2(std::cos(a), std::sin(a));
+        if (4 * j == n) twh[j] = make_double2(0.0, 1.0);
+        if (2 * j == n) twh[j] = make_double2(-1.0, 0.0);
+        if (4 * j == 3 * n) twh[j] = make_double2(0.0, -1.0);
+        if (j == 0) twh[j] = make_double2(1.0, 0.0);
+    }
+    DevBuf<double> zpl;
+    DevBuf<double2> ff, tw, Q, Ed, F, four, T, cimg;
+    zpl.ensure(nz);
+    tw.ensure(n);
+    ff.ensure(3 * N);
+    Q.ensure((size_t)nz * ny * S * 3);
+    Ed.ensure((size_t)S * S * 3);
+    F.ensure((size_t)6 * S * S);
+    four.ensure((size_t)6 * S * S);
+    T.ensure((size_t)6 * S * n);
+    cimg.ensure((size_t)6 * n * n);
+    IFDDA_CUDA(cudaMemcpyAsync(zpl.p, zp.data(), nz * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(tw.p, twh.data(), n * sizeof(double2), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(ff.p, FF, 3 * N * sizeof(double2), cudaMemcpyHostToDevice, st));
+    mic_farfield_dev(m, 1, ff.p, zpl.p, tw.p, Q.p, Ed.p, st);
+    if (!mic_holo_dev(m, Ed.p, ik, jk, pp, make_double2(E0.re, E0.im), F.p, four.p, tw.p, T.p, cimg.p, st))
+        return fail("nfft2d not supported");
+    IFDDA_CUDA(cudaMemcpyAsync(image, cimg.p, (size_t)6 * n * n * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    if (fourier)
+        IFDDA_CUDA(cudaMemcpyAsync(fourier, four.p, (size_t)6 * S * S * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    const double deltax = 2.0 * pi / (double)n / dkx;
+    for (int i = -n / 2; i <= n / 2 - 1; i++) {
+        if (xy) xy[i + n / 2] = deltax * (double)i * gross;
+        if (kxy) kxy[i + n / 2] = dkx * (double)i / k0;
+    }
+    if (imaxk0) *imaxk0 = imax;
+    if (infostr) memset(infostr, ' ', 64);
+    return 0;
+    IFDDA_GUARD_END(ctx, infostr)
+}
+
 int ifdda_microscope(ifdda_green* g, int nbsphere, const int* tabdip, const double* xs, const double* ys,
                      const double* zs, const ifdda_dcmplx* polarisa, const char* methodeit, double tol,
                      const ifdda_microscope_options* mo, double* image, double* xy, double* kxy, int* ninc,

@@ -434,6 +434,116 @@ __global__ void __launch_bounds__(ImgTiles<L>::NT) k_mic_cols(const MicGeom m, i
     }
 }
 
+// Holographic image: the complex field of one incidence, transformed along
+// y, centred and scaled by dkx dky / gross (fouriertoimage.f:37-95),
+// written to cimg[c][v][u]
+template <int L>
+__global__ void __launch_bounds__(ImgTiles<L>::NT) k_mic_cols_field(const MicGeom m, const double2* __restrict__ T,
+                                                                    const double2* __restrict__ tw,
+                                                                    double2* __restrict__ cimg) {
+    using TT = ImgTiles<L>;
+    using Lay = Layout<TT::NB, 1, true>;
+    constexpr int NB = TT::NB, NT = TT::NT, PER = (L * NB + NT - 1) / NT;
+    extern __shared__ double2 sm[];
+    double2* tws = sm + NB * L;
+    load_twiddles<double2, L, NT>(tws, tw);
+    const int x0 = blockIdx.x * NB, c = blockIdx.y, S = m.S();
+    const double sc = m.dkx * m.dky / m.gross;
+    const ColSrc src{T + (long)c * S * L, x0, m.imax, L};
+    fft_tile<double2, L, NB, NT, -1, Lay, ColSrc, SmemIO>(sm, tws, src);
+    const int n2 = L / 2;
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+        const int idx = threadIdx.x + q * NT;
+        if (PER * NT == L * NB || idx < L * NB) {
+            const double2 v = sm[Lay::addr(idx / NB, idx % NB)];
+            const int u = (x0 + idx % NB + n2) % L, w = (idx / NB + n2) % L;
+            cimg[((long)c * L + w) * L + u] = make_double2(v.x * sc, v.y * sc);
+        }
+    }
+}
+
+template <int L> void launch_image_field(const MicGeom& m, const double2* F, const double2* tw, double2* T,
+                                         double2* cimg, cudaStream_t st) {
+    using TT = ImgTiles<L>;
+    IFDDA_CUDA(cudaFuncSetAttribute(k_mic_rows<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TT::smem));
+    IFDDA_CUDA(
+        cudaFuncSetAttribute(k_mic_cols_field<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TT::smem));
+    const int nlines = 6 * m.S();
+    count_launch();
+    k_mic_rows<L><<<(nlines + TT::NB - 1) / TT::NB, TT::NT, TT::smem, st>>>(m, nlines, F, tw, T);
+    IFDDA_CUDA(cudaGetLastError());
+    count_launch();
+    k_mic_cols_field<L><<<dim3(L / TT::NB, 6), TT::NT, TT::smem, st>>>(m, T, tw, cimg);
+    IFDDA_CUDA(cudaGetLastError());
+}
+
+// The holographic microscope's lens (cdmlib.f:4380-4560): every pupil point
+// with k0^2 - kx^2 - ky^2 >= 0 gets the focus phase; on the transmission side
+// the field with the incident wave adds E_inc / dkx^2 at the grid point (ik,
+// jk) (diffractefft2dinc.f:75-91); then the rotation by the lens, skipped
+// where its axis vanishes (the centre).  four: the pupil fields before the
+// rotation (6 x S x S); F: after it, as the image transform reads them.
+__global__ void __launch_bounds__(256) k_mic_holo(const MicGeom m, const double2* __restrict__ Ed, int ik, int jk,
+                                                   double pp, double2 E0, double2* __restrict__ F,
+                                                   double2* __restrict__ four) {
+    const int S = m.S();
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= S * S) return;
+    const int irow = t % S, jrow = t / S, i = irow - m.imax, j = jrow - m.imax;
+    const double kx = m.dkx * (double)i, ky = m.dkx * (double)j;
+    const double kz2 = __dsub_rn(__dsub_rn(__dmul_rn(m.k0, m.k0), __dmul_rn(kx, kx)), __dmul_rn(ky, ky));
+    double2 f[6], g[6];
+    for (int c = 0; c < 6; c++) f[c] = g[c] = make_double2(0, 0);
+    if (kz2 >= 0.0) {
+        const double kz = sqrt(kz2);
+        double sn, cs;
+        sincos(kz * m.zlens, &sn, &cs);
+        const double2 zf = make_double2(cs, sn);
+        const double2* e = Ed + ((long)jrow * S + irow) * 3;
+        double2 inc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+        if (m.dside > 0 && i == ik && j == jk) {
+            double2 ex, ey, ez;
+            double kzi;
+            kxky_amplitude(m.k0, E0, pp, kx, ky, ex, ey, ez, kzi);
+            const double2 a[3] = {ex, ey, ez};
+            for (int c = 0; c < 3; c++) inc[c] = make_double2(a[c].x / m.dkx / m.dkx, a[c].y / m.dkx / m.dkx);
+        }
+        for (int c = 0; c < 3; c++) {
+            f[c] = cmul(e[c], zf);
+            if (m.dside > 0) f[c + 3] = cmul(cadd(e[c], inc[c]), zf);
+        }
+        const double u0 = kx / m.k0, u1v = ky / m.k0;
+        const double u2v = sqrt(__dsub_rn(__dsub_rn(1.0, __dmul_rn(u0, u0)), __dmul_rn(u1v, u1v))) * m.dside;
+        const double v0 = -kx / m.k0 / m.gross, v1 = -ky / m.k0 / m.gross;
+        const double v2 = sqrt(__dsub_rn(__dsub_rn(1.0, __dmul_rn(v0, v0)), __dmul_rn(v1, v1))) * m.dside;
+        double a1 = __dsub_rn(__dmul_rn(u1v, v2), __dmul_rn(u2v, v1));
+        double a2 = __dadd_rn(__dmul_rn(-u0, v2), __dmul_rn(u2v, v0));
+        const double co = __dadd_rn(__dadd_rn(__dmul_rn(u0, v0), __dmul_rn(u1v, v1)), __dmul_rn(u2v, v2));
+        const double si = sqrt(__dadd_rn(__dmul_rn(a1, a1), __dmul_rn(a2, a2)));
+        if (si == 0.0) {
+            for (int c = 0; c < 6; c++) g[c] = f[c];
+        } else {
+            a1 = a1 / si;
+            a2 = a2 / si;
+            const double tt = sqrt(u2v / v2);
+            const double r00 = a1 * a1 + (1.0 - a1 * a1) * co, r01 = a1 * a2 * (1.0 - co), r02 = a2 * si;
+            const double r11 = a2 * a2 + (1.0 - a2 * a2) * co, r12 = -a1 * si;
+            const double r20 = -a2 * si, r21 = a1 * si;
+            for (int h = 0; h < 6; h += 3) {
+                const double2 X = f[h], Y = f[h + 1], Z = f[h + 2];
+                g[h] = cscale(cadd(cadd(cscale(X, r00), cscale(Y, r01)), cscale(Z, r02)), tt);
+                g[h + 1] = cscale(cadd(cadd(cscale(X, r01), cscale(Y, r11)), cscale(Z, r12)), tt);
+                g[h + 2] = cscale(cadd(cadd(cscale(X, r20), cscale(Y, r21)), cscale(Z, co)), tt);
+            }
+        }
+    }
+    for (int c = 0; c < 6; c++) {
+        four[((long)c * S + jrow) * S + irow] = f[c];
+        F[((long)c * S + jrow) * S + irow] = g[c];
+    }
+}
+
 __global__ void k_mic_sqrt(long cnt, double* __restrict__ img) {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (long)gridDim.x * blockDim.x)
         img[i] = sqrt(img[i]);
@@ -505,6 +615,22 @@ bool mic_image_dev(const MicGeom& m, int nb, const double2* F, const double2* tw
     switch (m.n) {
 #define IFDDA_CASE_IMG(L) \
     case L: launch_image<L>(m, nb, F, tw, T, img, st); return true;
+        IFDDA_IMG_LENGTHS(IFDDA_CASE_IMG)
+#undef IFDDA_CASE_IMG
+        default:
+            return false;
+    }
+}
+
+bool mic_holo_dev(const MicGeom& m, const double2* Ed, int ik, int jk, double pp, double2 E0, double2* F,
+                  double2* four, const double2* tw, double2* T, double2* cimg, cudaStream_t st) {
+    const int S = m.S();
+    count_launch();
+    k_mic_holo<<<(S * S + 255) / 256, 256, 0, st>>>(m, Ed, ik, jk, pp, E0, F, four);
+    IFDDA_CUDA(cudaGetLastError());
+    switch (m.n) {
+#define IFDDA_CASE_IMG(L) \
+    case L: launch_image_field<L>(m, F, tw, T, cimg, st); return true;
         IFDDA_IMG_LENGTHS(IFDDA_CASE_IMG)
 #undef IFDDA_CASE_IMG
         default:

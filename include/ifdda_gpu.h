@@ -265,6 +265,26 @@ int ifdda_microscope(ifdda_green* g, int nbsphere, const int* tabdip, const doub
                      double* kxinc, double* kyinc, double* tol1, int* nloop, int* ncompte, int* nstop,
                      char* infostr, const ifdda_solve_options* opt);
 
+/* Holographic microscope (ntypemic = 0) with the FFT lens, after the solve of
+   one plane wave (theta, phi in degrees, polarisation pp, amplitude E0):
+   replaces cdmlib/cdmlib.f:4075-4660 with nenergie = 0, that is
+   diffractefft2dlens (cdmlib/diffractefft2dlens.f:1-181) on the dipole
+   moments FF of the full nx*ny*nz box, the incident wave in the pupil
+   (cdmlib/diffractefft2dinc.f:75-91), the lens rotation and fouriertoimage
+   (cdmlib/fouriertoimage.f, fouriertoimage2.f on the reflection side).
+   numaper unitless, zlens in metres without the side's sign, nside 0
+   transmission / 1 reflection.  image: 6 complex n*n fields (Eimagex..z,
+   then Eimageincx..z, zero on the reflection side), pixel u + n v; fourier
+   (may be NULL): the pupil fields Efourierx..z, Efourierincx..z before the
+   rotation, 6 x (2 imaxk0 + 1)^2, row j, column i; xy, kxy (n values, may be
+   NULL).  nfft2d: a power of two from 32 to 4096.  Returns 1 with the
+   reference's message on an error. */
+int ifdda_holography(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, const double* xs,
+                     const double* ys, const double* zs, const ifdda_dcmplx* FF, ifdda_dcmplx E0, double theta,
+                     double phi, double pp, int nfft2d, double numaper, double gross, double zlens, int nside,
+                     ifdda_dcmplx* image, ifdda_dcmplx* fourier, double* xy, double* kxy, int* imaxk0,
+                     char* infostr);
+
 /* Diagnostics (no counterpart in the reference, whose only instrumentation
    is the wall/CPU-time printout of cdmlib/cdmlib.f:1956-1963 and the
    mat-vec count ncompte).

@@ -3077,6 +3077,109 @@ int orc_farfield_fft(int nx, int ny, int nz, double d, const double *xs, const d
     return 0;
 }
 
+/* ------------------------------------------------------------------------- */
+/* Holographic microscope (ntypemic = 0) with the FFT lens, after the solve of */
+/* one plane wave (cdmlib.f:4075-4660 with nenergie = 0 and the lens far      */
+/* field computed afresh): diffractefft2dlens, the incident wave in the pupil */
+/* (diffractefft2dinc.f:75-91 for 'pwavelinear': E / dk^2 at the grid point   */
+/* of deltakroutine), the lens rotation, then fouriertoimage (fouriertoimage2 */
+/* on the reflection side).  nside 0 transmission, 1 reflection.  image: 6    */
+/* complex arrays of n*n (x, y, z, then with the incident wave; the latter    */
+/* stay zero on the reflection side); fourier: 6 arrays of (2 imax + 1)^2     */
+/* (row j, column i), the pupil fields before the rotation.  Returns nstop.  */
+/* ------------------------------------------------------------------------- */
+int orc_holography(int nx, int ny, int nz, double d, double k0, const double *xs,
+                   const double *ys, const double *zs, const zc *FF, zc E0, double theta,
+                   double phi, double pp, int n, double numaper, double gross, double zlens,
+                   int nside, zc *image, zc *fourier, double *xy, double *kxy, int *imax_out,
+                   char *infostr) {
+    const double pi = acos(-1.0);
+    double dside = nside == 1 ? -1.0 : 1.0;
+    zlens = zlens * dside;
+    numaper = numaper * k0;
+    set_info(infostr, "");
+    int imax = 0;
+    zc *Ed = NULL;
+    if (orc_diffractefft2dlens(nx, ny, nz, n, k0, xs, ys, zs, d, FF, numaper, dside, &imax, &Ed, infostr))
+        return 1;
+    int S = 2 * imax + 1, n2 = n / 2;
+    double dkx = 2.0 * pi / ((double)n * d), dky = dkx;
+    /* the incident wave on the pupil grid (transmission only) */
+    zc *Ei = (zc *)calloc((size_t)S * S * 3, sizeof(zc));
+    if (dside > 0) {
+        if (dkx >= numaper) {
+            set_info(infostr, "In FFT lens inc nfft2d too small");
+            free(Ed); free(Ei);
+            return 1;
+        }
+        double kxinc = sin(theta * pi / 180.0) * cos(phi * pi / 180.0) * k0;
+        double kyinc = sin(theta * pi / 180.0) * sin(phi * pi / 180.0) * k0;
+        int ik, jk;
+        orc_deltakroutine(kxinc, kyinc, dkx, dky, k0, &ik, &jk);
+        double kx = dkx * (double)ik, ky = dkx * (double)jk;
+        zc E[3];
+        orc_ondeplanekxky(0.0, 0.0, 0.0, k0, E0, pp, kx, ky, E);
+        zc *o = Ei + ((size_t)(imax + jk) * S + (imax + ik)) * 3;
+        for (int c = 0; c < 3; c++) o[c] = E[c] / dkx / dkx;
+    }
+    zc *F = (zc *)calloc(6 * (size_t)n * n, sizeof(zc));
+    if (fourier) memset(fourier, 0, sizeof(zc) * 6 * (size_t)S * S);
+    for (int i = -imax; i <= imax; i++)
+        for (int j = -imax; j <= imax; j++) {
+            int ix = i >= 0 ? i + 1 : n + i + 1, iy = j >= 0 ? j + 1 : n + j + 1;
+            long ind = (ix - 1) + (long)n * (iy - 1);
+            double kx = dkx * (double)i, ky = dkx * (double)j;
+            double kz = k0 * k0 - kx * kx - ky * ky;
+            if (!(kz >= 0.0)) continue;
+            kz = sqrt(kz);
+            zc zf = cexp(I * kz * zlens);
+            zc *e = Ed + ((size_t)(imax + j) * S + (imax + i)) * 3;
+            zc *ei = Ei + ((size_t)(imax + j) * S + (imax + i)) * 3;
+            zc f[6];
+            for (int c = 0; c < 3; c++) {
+                f[c] = e[c] * zf;
+                f[c + 3] = dside > 0 ? (e[c] + ei[c]) * zf : 0;
+            }
+            if (fourier)
+                for (int c = 0; c < 6; c++) fourier[(size_t)c * S * S + (size_t)(imax + j) * S + (imax + i)] = f[c];
+            double u[3], v[3];
+            u[0] = kx / k0; u[1] = ky / k0; u[2] = sqrt(1.0 - u[0] * u[0] - u[1] * u[1]) * dside;
+            v[0] = -kx / k0 / gross; v[1] = -ky / k0 / gross;
+            v[2] = sqrt(1.0 - v[0] * v[0] - v[1] * v[1]) * dside;
+            double u1 = u[1] * v[2] - u[2] * v[1];
+            double u2 = -u[0] * v[2] + u[2] * v[0];
+            double cs = u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+            double sn = sqrt(u1 * u1 + u2 * u2);
+            if (sn == 0.0) {
+                for (int c = 0; c < 6; c++) F[(size_t)c * n * n + ind] = f[c];
+                continue;
+            }
+            u1 = u1 / sn;
+            u2 = u2 / sn;
+            double t = sqrt(u[2] / v[2]);
+            for (int h = 0; h < 6; h += 3) {
+                zc X = f[h], Y = f[h + 1], Z = f[h + 2];
+                F[(size_t)h * n * n + ind] =
+                    ((u1 * u1 + (1.0 - u1 * u1) * cs) * X + u1 * u2 * (1.0 - cs) * Y + u2 * sn * Z) * t;
+                F[(size_t)(h + 1) * n * n + ind] =
+                    (u1 * u2 * (1.0 - cs) * X + (u2 * u2 + (1.0 - u2 * u2) * cs) * Y - u1 * sn * Z) * t;
+                F[(size_t)(h + 2) * n * n + ind] = (-u2 * sn * X + u1 * sn * Y + cs * Z) * t;
+            }
+        }
+    free(Ed);
+    free(Ei);
+    orc_fouriertoimage(dkx, dky, gross, F, n);
+    memcpy(image, F, sizeof(zc) * 6 * (size_t)n * n);
+    free(F);
+    double deltax = 2.0 * pi / (double)n / dkx;
+    for (int i = -n2; i <= n2 - 1; i++) {
+        xy[i + n2] = deltax * (double)i * gross;
+        kxy[i + n2] = dkx * (double)i / k0;
+    }
+    *imax_out = imax;
+    return 0;
+}
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -120,3 +120,46 @@ def test_cdmlib_microscope_matches_oracle(orc):
                          0.9, 0.5, 64, 100.0, 50e-9, 1.0, 6328e-9)
     for c, name in enumerate(("Eimagex", "Eimagey", "Eimagez", "Eimageincx", "Eimageincy", "Eimageincz")):
         assert rel(out[name], ref["image"][c]) < 1e-8, name
+
+
+@pytest.mark.parametrize("nside,nfft2d", [(0, 64), (1, 64), (0, 128)])
+def test_holography_matches_oracle(gctx, orc, nside, nfft2d):
+    """ntypemic = 0 (cdmlib.f:4075-4660): the complex image fields of one
+    oblique plane-wave solve, and the pupil fields, against the oracle's
+    restatement with full 2-D FFTs."""
+    ob, k0 = _object()
+    E0, _ = orc.irradiance(1.0, 6328e-9)
+    ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 0.3, 0, 10.0, 30.0)
+    G = orc.greencalculfft(8, 8, 8, ob.aretecube, k0)
+    sol = orc.inverserig(G, 8, 8, 8, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-8)
+    args = (8, 8, 8, ob.aretecube, k0, ob.xs, ob.ys, ob.zs, sol["FF"], E0, 10.0, 30.0, 0.3)
+    ref = orc.holography(*args, nfft2d, 0.9, 100.0, 50e-9, nside=nside)
+    got = gctx.holography(*args, nfft2d=nfft2d, numaper=0.9, gross=100.0, zlens=50e-9, nside=nside)
+    assert got["nstop"] == ref["nstop"] == 0, (got["infostr"], ref["infostr"])
+    assert got["imaxk0"] == ref["imaxk0"]
+    assert np.array_equal(got["xy"], ref["xy"]) and np.array_equal(got["kxy"], ref["kxy"])
+    for c in range(3 if nside else 6):
+        assert rel(got["image"][c], ref["image"][c]) < 1e-10, c
+        assert rel(got["fourier"][c], ref["fourier"][c]) < 1e-10, c
+    if nside:
+        assert not got["image"][3:].any()
+    else:  # the incident wave dominates the image with it
+        assert np.abs(got["image"][3]).max() > np.abs(got["image"][0]).max()
+
+
+def test_cdmlib_holography_matches_oracle(orc):
+    """ntypemic = 0 through the cdmlib entry (the reference's test1 driver
+    runs this microscope): full box, then the holographic images of the
+    solve's plane wave."""
+    from ifdda.cdmlib import cdmlib
+    out = cdmlib(wavelength=632.8, object="sphere", rayon=100.0, eps=2.25 + 0j, nnnr=8, tolinit=1e-8,
+                 methodeit="GPBICG1", nproche=0, theta=10.0, phi=30.0, pp=0.3, P0=1.0, w0=6328.0, nlentille=1,
+                 ntypemic=0, nfft2d=64, numaper=0.9, gross=100.0, zlens=50.0)
+    assert out["nstop"] == 0, out["infostr"]
+    assert out["nbsphere"] == 512
+    ob, k0 = _object()
+    E0, _ = orc.irradiance(1.0, 6328e-9)
+    ref = orc.holography(8, 8, 8, ob.aretecube, k0, ob.xs, ob.ys, ob.zs, out["FF"], E0, 10.0, 30.0, 0.3, 64, 0.9,
+                         100.0, 50e-9)
+    for c, name in enumerate(("Eimagex", "Eimagey", "Eimagez", "Eimageincx", "Eimageincy", "Eimageincz")):
+        assert rel(out[name], ref["image"][c]) < 1e-10, name
