@@ -929,12 +929,12 @@ int ifdda_nearfield_wide(ifdda_ctx* ctx, int nx, int ny, int nz, int nxmp, int n
     IFDDA_GUARD_END(ctx, nullptr)
 }
 
-int ifdda_holography(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, const double* xs,
-                     const double* ys, const double* zs, const ifdda_dcmplx* FF, ifdda_dcmplx E0, double theta,
-                     double phi, double pp, int nfft2d, double numaper, double gross, double zlens, int nside,
-                     ifdda_dcmplx* image, ifdda_dcmplx* fourier, double* xy, double* kxy, int* imaxk0,
-                     char* infostr) {
-    if (!ctx || !xs || !ys || !zs || !FF || !image || nx < 1 || ny < 1 || nz < 1) {
+int ifdda_holography(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, int nbsphere,
+                     const double* xs, const double* ys, const double* zs, const ifdda_dcmplx* FF, ifdda_dcmplx E0,
+                     double theta, double phi, double pp, int nfft2d, double numaper, double gross, double zlens,
+                     int nside, int nquicklens, ifdda_dcmplx* image, ifdda_dcmplx* fourier, double* xy,
+                     double* kxy, int* imaxk0, char* infostr) {
+    if (!ctx || !xs || !ys || !zs || !FF || !image || nx < 1 || ny < 1 || nz < 1 || nbsphere < 1) {
         set_info(infostr, "invalid argument");
         return 1;
     }
@@ -949,16 +949,35 @@ int ifdda_holography(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, d
     };
     const int n = nfft2d;
     const long N = (long)nx * ny * nz;
+    const bool quick = nquicklens == 1;
     if (nside != 0 && nside != 1) return fail("nside must be 0 (transmission) or 1 (reflection)");
+    if (nquicklens != 0 && nquicklens != 1) return fail("nquicklens must be 0 or 1");
+    if (quick && nbsphere != N) return fail("the FFT lens needs the full box (nbsphere = nx*ny*nz)");
     if (!image_length_supported(n)) return fail("nfft2d not supported: a power of two from 32 to 4096");
     if (nx > n || ny > n) return fail("nfft2d smaller than the object");
     const double pi = 3.14159265358979323846, dside = nside == 1 ? -1.0 : 1.0;
-    const double na = numaper * k0, dkx = 2.0 * pi / ((double)n * aretecube);
-    // diffractefft2dlens.f:29-73
-    if (dkx >= na) return fail("In FFT lens nfft2d too small");
-    const int imax = (int)std::lround(k0 / dkx) + 1, S = 2 * imax + 1;
-    if (S > n) return fail("In FFT diffraction for lens nfft2d too small!");
-    if (S < 7) return fail("In FFT diffract nfft2d too small");
+    const double na = numaper * k0;
+    double dkx = 2.0 * pi / ((double)n * aretecube);
+    int imax;
+    if (quick) {
+        // diffractefft2dlens.f:29-73
+        if (dkx >= na) return fail("In FFT lens nfft2d too small");
+        imax = (int)std::lround(k0 / dkx) + 1;
+        if (2 * imax + 1 > n) return fail("In FFT diffraction for lens nfft2d too small!");
+        if (2 * imax + 1 < 7) return fail("In FFT diffract nfft2d too small");
+    } else {
+        // cdmlib.f:3818-3826: halve the pupil step until more than 20 points
+        // cover k0; the pupil must fit the image grid (unchecked there)
+        for (int k = 0;; k++) {
+            dkx = 2.0 * pi / ((double)n * aretecube) / (double)(1 << k);
+            imax = (int)std::lround(k0 / dkx) + 1;
+            if (imax > 20) break;
+        }
+        if (2 * imax + 1 > n) return fail("In FFT lens nfft2d too small");
+        // diffractefft2dinc.f:64-68 on the transmission side
+        if (nside == 0 && dkx >= na) return fail("In FFT lens inc nfft2d too small");
+    }
+    const int S = 2 * imax + 1;
     MicGeom m{};
     m.nx = nx;
     m.ny = ny;
@@ -986,7 +1005,8 @@ int ifdda_holography(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, d
         }
     }
     std::vector<double> zp(nz);
-    for (int k = 0; k < nz; k++) zp[k] = zs[(long)nx * ny * k];
+    if (quick)
+        for (int k = 0; k < nz; k++) zp[k] = zs[(long)nx * ny * k];
     std::vector<double2> twh(n);
     for (int j = 0; j < n; j++) {
         const double a = 2.0 * pi * (double)j / (double)n;
@@ -996,12 +1016,13 @@ int ifdda_holography(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, d
         if (4 * j == 3 * n) twh[j] = make_double2(0.0, -1.0);
         if (j == 0) twh[j] = make_double2(1.0, 0.0);
     }
-    DevBuf<double> zpl;
+    DevBuf<double> zpl, dx, dy, dz;
     DevBuf<double2> ff, tw, Q, Ed, F, four, T, cimg;
     zpl.ensure(nz);
     tw.ensure(n);
-    ff.ensure(3 * N);
-    Q.ensure((size_t)nz * ny * S * 3);
+    ff.ensure(3L * nbsphere);
+    if (quick) Q.ensure((size_t)nz * ny * S * 3);
+    else Q.ensure((size_t)S * S * mic_direct_chunks(nbsphere) * 3);
     Ed.ensure((size_t)S * S * 3);
     F.ensure((size_t)6 * S * S);
     four.ensure((size_t)6 * S * S);
@@ -1009,9 +1030,19 @@ int ifdda_holography(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, d
     cimg.ensure((size_t)6 * n * n);
     IFDDA_CUDA(cudaMemcpyAsync(zpl.p, zp.data(), nz * sizeof(double), cudaMemcpyHostToDevice, st));
     IFDDA_CUDA(cudaMemcpyAsync(tw.p, twh.data(), n * sizeof(double2), cudaMemcpyHostToDevice, st));
-    IFDDA_CUDA(cudaMemcpyAsync(ff.p, FF, 3 * N * sizeof(double2), cudaMemcpyHostToDevice, st));
-    mic_farfield_dev(m, 1, ff.p, zpl.p, tw.p, Q.p, Ed.p, st);
-    if (!mic_holo_dev(m, Ed.p, ik, jk, pp, make_double2(E0.re, E0.im), F.p, four.p, tw.p, T.p, cimg.p, st))
+    IFDDA_CUDA(cudaMemcpyAsync(ff.p, FF, 3L * nbsphere * sizeof(double2), cudaMemcpyHostToDevice, st));
+    if (quick) {
+        mic_farfield_dev(m, 1, ff.p, zpl.p, tw.p, Q.p, Ed.p, st);
+    } else {
+        dx.ensure(nbsphere);
+        dy.ensure(nbsphere);
+        dz.ensure(nbsphere);
+        IFDDA_CUDA(cudaMemcpyAsync(dx.p, xs, nbsphere * sizeof(double), cudaMemcpyHostToDevice, st));
+        IFDDA_CUDA(cudaMemcpyAsync(dy.p, ys, nbsphere * sizeof(double), cudaMemcpyHostToDevice, st));
+        IFDDA_CUDA(cudaMemcpyAsync(dz.p, zs, nbsphere * sizeof(double), cudaMemcpyHostToDevice, st));
+        mic_direct_dev(m, 1, nbsphere, dx.p, dy.p, dz.p, ff.p, Q.p, Ed.p, st);
+    }
+    if (!mic_holo_dev(m, Ed.p, ik, jk, pp, make_double2(E0.re, E0.im), !quick, F.p, four.p, tw.p, T.p, cimg.p, st))
         return fail("nfft2d not supported");
     IFDDA_CUDA(cudaMemcpyAsync(image, cimg.p, (size_t)6 * n * n * sizeof(double2), cudaMemcpyDeviceToHost, st));
     if (fourier)

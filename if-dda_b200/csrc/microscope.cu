@@ -484,8 +484,11 @@ template <int L> void launch_image_field(const MicGeom& m, const double2* F, con
 // jk) (diffractefft2dinc.f:75-91); then the rotation by the lens, skipped
 // where its axis vanishes (the centre).  four: the pupil fields before the
 // rotation (6 x S x S); F: after it, as the image transform reads them.
+// slow: the lens without FFT (cdmlib.f:3885-3960): only points inside the
+// objective's aperture, and the field with the incident wave formed as
+// E zf + E_inc zf.
 __global__ void __launch_bounds__(256) k_mic_holo(const MicGeom m, const double2* __restrict__ Ed, int ik, int jk,
-                                                   double pp, double2 E0, double2* __restrict__ F,
+                                                   double pp, double2 E0, int slow, double2* __restrict__ F,
                                                    double2* __restrict__ four) {
     const int S = m.S();
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -493,9 +496,10 @@ __global__ void __launch_bounds__(256) k_mic_holo(const MicGeom m, const double2
     const int irow = t % S, jrow = t / S, i = irow - m.imax, j = jrow - m.imax;
     const double kx = m.dkx * (double)i, ky = m.dkx * (double)j;
     const double kz2 = __dsub_rn(__dsub_rn(__dmul_rn(m.k0, m.k0), __dmul_rn(kx, kx)), __dmul_rn(ky, ky));
+    const bool in = slow ? sqrt(__dadd_rn(__dmul_rn(kx, kx), __dmul_rn(ky, ky))) <= m.numaper : kz2 >= 0.0;
     double2 f[6], g[6];
     for (int c = 0; c < 6; c++) f[c] = g[c] = make_double2(0, 0);
-    if (kz2 >= 0.0) {
+    if (in) {
         const double kz = sqrt(kz2);
         double sn, cs;
         sincos(kz * m.zlens, &sn, &cs);
@@ -511,7 +515,7 @@ __global__ void __launch_bounds__(256) k_mic_holo(const MicGeom m, const double2
         }
         for (int c = 0; c < 3; c++) {
             f[c] = cmul(e[c], zf);
-            if (m.dside > 0) f[c + 3] = cmul(cadd(e[c], inc[c]), zf);
+            if (m.dside > 0) f[c + 3] = slow ? cadd(f[c], cmul(inc[c], zf)) : cmul(cadd(e[c], inc[c]), zf);
         }
         const double u0 = kx / m.k0, u1v = ky / m.k0;
         const double u2v = sqrt(__dsub_rn(__dsub_rn(1.0, __dmul_rn(u0, u0)), __dmul_rn(u1v, u1v))) * m.dside;
@@ -622,11 +626,11 @@ bool mic_image_dev(const MicGeom& m, int nb, const double2* F, const double2* tw
     }
 }
 
-bool mic_holo_dev(const MicGeom& m, const double2* Ed, int ik, int jk, double pp, double2 E0, double2* F,
-                  double2* four, const double2* tw, double2* T, double2* cimg, cudaStream_t st) {
+bool mic_holo_dev(const MicGeom& m, const double2* Ed, int ik, int jk, double pp, double2 E0, bool slow,
+                  double2* F, double2* four, const double2* tw, double2* T, double2* cimg, cudaStream_t st) {
     const int S = m.S();
     count_launch();
-    k_mic_holo<<<(S * S + 255) / 256, 256, 0, st>>>(m, Ed, ik, jk, pp, E0, F, four);
+    k_mic_holo<<<(S * S + 255) / 256, 256, 0, st>>>(m, Ed, ik, jk, pp, E0, slow ? 1 : 0, F, four);
     IFDDA_CUDA(cudaGetLastError());
     switch (m.n) {
 #define IFDDA_CASE_IMG(L) \

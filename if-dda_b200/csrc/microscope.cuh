@@ -52,9 +52,10 @@ bool mic_image_dev(const MicGeom& m, int nb, const double2* F, const double2* tw
 // Holographic image of one incidence: the lens of cdmlib.f:4380-4560 on the
 // far field Ed (S x S x 3), the incident wave at (ik, jk) on the transmission
 // side, then the complex image cimg (6 x n x n, pixel u + n v); four receives
-// the pupil fields (6 x S x S); F (6 S S) and T (6 S n) are scratch.
-bool mic_holo_dev(const MicGeom& m, const double2* Ed, int ik, int jk, double pp, double2 E0, double2* F,
-                  double2* four, const double2* tw, double2* T, double2* cimg, cudaStream_t st);
+// the pupil fields (6 x S x S); F (6 S S) and T (6 S n) are scratch.  slow:
+// the lens without FFT (Ed by direct summation, points inside the aperture).
+bool mic_holo_dev(const MicGeom& m, const double2* Ed, int ik, int jk, double pp, double2 E0, bool slow,
+                  double2* F, double2* four, const double2* tw, double2* T, double2* cimg, cudaStream_t st);
 // img = sqrt(img), cnt values
 void mic_sqrt_dev(long cnt, double* img, cudaStream_t st);
 

@@ -74,9 +74,9 @@ SIGNATURES = {
                                      _vp, _vp, _ip, _vp, _vp]),
     "ifdda_nearfield_wide": (C.c_int, [_vp] + [C.c_int] * 6 + [C.c_double, C.c_double] + [C.c_int] * 3 +
                              [_vp] * 6 + [DComplex, C.c_double, C.c_double, C.c_double] + [_vp] * 6),
-    "ifdda_holography": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, _vp, _vp, _vp, _vp,
-                                   DComplex, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double, C.c_double,
-                                   C.c_double, C.c_int, _vp, _vp, _vp, _vp, _ip, C.c_char_p]),
+    "ifdda_holography": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, _vp, _vp, _vp,
+                                   _vp, DComplex, C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
+                                   C.c_double, C.c_double, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _ip, C.c_char_p]),
     "ifdda_microscope": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_char_p, C.c_double,
                                    C.POINTER(MicroscopeOptions),
                                    _vp, _vp, _vp, _ip, _vp, _vp, _dp, _ip, _ip, _ip, C.c_char_p,

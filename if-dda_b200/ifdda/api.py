@@ -109,7 +109,7 @@ class Context:
         return ce.value, ca.value
 
     def holography(self, nx, ny, nz, aretecube, k0, xs, ys, zs, FF, E0, theta, phi, pp, nfft2d=128, numaper=0.9,
-                   gross=100.0, zlens=0.0, nside=0) -> dict:
+                   gross=100.0, zlens=0.0, nside=0, nquicklens=1) -> dict:
         """Holographic microscope with the FFT lens after one plane-wave solve
         (cdmlib.f:4075-4660): complex image fields (6, n, n) [x, y, z, then
         with the incident wave], pupil fields (6, S, S), xy, kxy, imaxk0,
@@ -120,15 +120,15 @@ class Context:
         zs = np.ascontiguousarray(zs, np.float64)
         ff = _zc(FF)
         img = np.zeros((6, n, n), np.complex128)
-        imax_est = int(round(k0 * n * aretecube / (2 * math.pi))) + 2
+        imax_est = max(int(round(k0 * n * aretecube / (2 * math.pi))) + 2, n // 2)
         four = np.zeros(6 * (2 * imax_est + 1) ** 2, np.complex128)
         xy, kxy = np.zeros(n), np.zeros(n)
         im = C.c_int(0)
         info = C.create_string_buffer(b" " * 64, 65)
         e0 = complex(E0)
-        rc = self.lib.ifdda_holography(self.h, nx, ny, nz, aretecube, k0, _p(xs), _p(ys), _p(zs), _p(ff),
+        rc = self.lib.ifdda_holography(self.h, nx, ny, nz, aretecube, k0, len(xs), _p(xs), _p(ys), _p(zs), _p(ff),
                                        DComplex(e0.real, e0.imag), theta, phi, pp, n, numaper, gross, zlens, nside,
-                                       _p(img), _p(four), _p(xy), _p(kxy), C.byref(im), info)
+                                       nquicklens, _p(img), _p(four), _p(xy), _p(kxy), C.byref(im), info)
         S = 2 * im.value + 1
         return dict(nstop=rc, infostr=info.raw[:64].decode(errors="replace"), image=img,
                     fourier=four[:6 * S * S].reshape(6, S, S), xy=xy, kxy=kxy, imaxk0=im.value)

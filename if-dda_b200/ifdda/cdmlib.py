@@ -14,7 +14,7 @@ one per dipole), plane waves, nrig = 0,
 0 <= nquad <= 16), and the bright-field and dark-field microscopes in
 transmission or reflection with or without the FFT lens (nlentille = 1,
 ntypemic 1 or 2, nside 0 or 1, nquicklens 0 or 1, cdmlib.f:3660-3800), the
-holographic microscope with the FFT lens (ntypemic 0, cdmlib.f:4075-4660), the wide near field (nproche >= 2) and
+holographic microscope (ntypemic 0, cdmlib.f:3803-4660), the wide near field (nproche >= 2) and
 the scattering cross section / asymmetry factor / Poynting vector
 (nsectionsca = 1, by direct summation or, with nquickdiffracte = 1, from the
 far field on the nfft2d pupil grid); anything else returns nstop = 1 with a
@@ -101,8 +101,6 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
             return _fail("Illumination on the wrong side with the options")
         if ntypemic not in (0, 1, 2) or nside not in (0, 1) or nquicklens not in (0, 1):
             return _fail("ntypemic 0, 1 or 2, nside 0 or 1, nquicklens 0 or 1")
-        if ntypemic == 0 and nquicklens == 0:
-            return _fail("the holographic microscope is handled with the FFT lens (nquicklens = 1)")
         if nquicklens:
             nproche = max(nproche, 1)  # the FFT lens needs the full box (cdmlib.f:631)
     if not (nlocal or nmacro or nsection):
@@ -165,7 +163,8 @@ def cdmlib(*, wavelength, object, eps=None, nnnr=None, rayon=None, side=None, ra
             FFs = np.atleast_2d(r.FF)
             t, p, s = inc[0]
             h = ctx.holography(ob.nx, ob.ny, ob.nz, ob.aretecube, k0, ob.xs, ob.ys, ob.zs, FFs[0], E0, t, p, s,
-                               nfft2d=nfft2d, numaper=numaper, gross=gross, zlens=zlens * 1e-9, nside=nside)
+                               nfft2d=nfft2d, numaper=numaper, gross=gross, zlens=zlens * 1e-9, nside=nside,
+                               nquicklens=nquicklens)
             if h["nstop"] != 0:
                 g.close()
                 out.update(nstop=h["nstop"], infostr=h["infostr"])

@@ -273,17 +273,21 @@ int ifdda_microscope(ifdda_green* g, int nbsphere, const int* tabdip, const doub
    (cdmlib/diffractefft2dinc.f:75-91), the lens rotation and fouriertoimage
    (cdmlib/fouriertoimage.f, fouriertoimage2.f on the reflection side).
    numaper unitless, zlens in metres without the side's sign, nside 0
-   transmission / 1 reflection.  image: 6 complex n*n fields (Eimagex..z,
+   transmission / 1 reflection.  nquicklens 0: the lens without FFT
+   (cdmlib.f:3803-4074): a finer pupil grid (more than 20 points over k0),
+   the far field by direct summation over the nbsphere dipoles (any object;
+   FF and xs, ys, zs of those dipoles), only points inside the aperture; with
+   nquicklens = 1 the object is the full box (nbsphere = nx*ny*nz).  image: 6 complex n*n fields (Eimagex..z,
    then Eimageincx..z, zero on the reflection side), pixel u + n v; fourier
    (may be NULL): the pupil fields Efourierx..z, Efourierincx..z before the
    rotation, 6 x (2 imaxk0 + 1)^2, row j, column i; xy, kxy (n values, may be
    NULL).  nfft2d: a power of two from 32 to 4096.  Returns 1 with the
    reference's message on an error. */
-int ifdda_holography(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, const double* xs,
-                     const double* ys, const double* zs, const ifdda_dcmplx* FF, ifdda_dcmplx E0, double theta,
-                     double phi, double pp, int nfft2d, double numaper, double gross, double zlens, int nside,
-                     ifdda_dcmplx* image, ifdda_dcmplx* fourier, double* xy, double* kxy, int* imaxk0,
-                     char* infostr);
+int ifdda_holography(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, int nbsphere,
+                     const double* xs, const double* ys, const double* zs, const ifdda_dcmplx* FF, ifdda_dcmplx E0,
+                     double theta, double phi, double pp, int nfft2d, double numaper, double gross, double zlens,
+                     int nside, int nquicklens, ifdda_dcmplx* image, ifdda_dcmplx* fourier, double* xy,
+                     double* kxy, int* imaxk0, char* infostr);
 
 /* Diagnostics (no counterpart in the reference, whose only instrumentation
    is the wall/CPU-time printout of cdmlib/cdmlib.f:1956-1963 and the

@@ -3088,11 +3088,11 @@ int orc_farfield_fft(int nx, int ny, int nz, double d, const double *xs, const d
 /* stay zero on the reflection side); fourier: 6 arrays of (2 imax + 1)^2     */
 /* (row j, column i), the pupil fields before the rotation.  Returns nstop.  */
 /* ------------------------------------------------------------------------- */
-int orc_holography(int nx, int ny, int nz, double d, double k0, const double *xs,
+int orc_holography(int nx, int ny, int nz, double d, double k0, int nb, const double *xs,
                    const double *ys, const double *zs, const zc *FF, zc E0, double theta,
                    double phi, double pp, int n, double numaper, double gross, double zlens,
-                   int nside, zc *image, zc *fourier, double *xy, double *kxy, int *imax_out,
-                   char *infostr) {
+                   int nside, int nquicklens, zc *image, zc *fourier, double *xy, double *kxy,
+                   int *imax_out, char *infostr) {
     const double pi = acos(-1.0);
     double dside = nside == 1 ? -1.0 : 1.0;
     zlens = zlens * dside;
@@ -3100,10 +3100,28 @@ int orc_holography(int nx, int ny, int nz, double d, double k0, const double *xs
     set_info(infostr, "");
     int imax = 0;
     zc *Ed = NULL;
-    if (orc_diffractefft2dlens(nx, ny, nz, n, k0, xs, ys, zs, d, FF, numaper, dside, &imax, &Ed, infostr))
-        return 1;
+    double dkx = 2.0 * pi / ((double)n * d), dky;
+    if (nquicklens == 1) {
+        if (orc_diffractefft2dlens(nx, ny, nz, n, k0, xs, ys, zs, d, FF, numaper, dside, &imax, &Ed,
+                                   infostr))
+            return 1;
+    } else {
+        /* cdmlib.f:3818-3826: halve the pupil step until more than 20
+           points cover k0; the far field by direct summation */
+        for (int k = 0;; k++) {
+            dkx = 2.0 * pi / ((double)n * d) / (double)(1 << k);
+            imax = (int)lround(k0 / dkx) + 1;
+            if (imax > 20) break;
+        }
+        if (2 * imax + 1 > n) {
+            set_info(infostr, "In FFT lens nfft2d too small");
+            return 1;
+        }
+        Ed = (zc *)malloc(sizeof(zc) * (size_t)(2 * imax + 1) * (2 * imax + 1) * 3);
+        orc_lens_direct(nb, xs, ys, zs, FF, k0, numaper, dside, imax, dkx, Ed);
+    }
     int S = 2 * imax + 1, n2 = n / 2;
-    double dkx = 2.0 * pi / ((double)n * d), dky = dkx;
+    dky = dkx;
     /* the incident wave on the pupil grid (transmission only) */
     zc *Ei = (zc *)calloc((size_t)S * S * 3, sizeof(zc));
     if (dside > 0) {
@@ -3129,16 +3147,24 @@ int orc_holography(int nx, int ny, int nz, double d, double k0, const double *xs
             int ix = i >= 0 ? i + 1 : n + i + 1, iy = j >= 0 ? j + 1 : n + j + 1;
             long ind = (ix - 1) + (long)n * (iy - 1);
             double kx = dkx * (double)i, ky = dkx * (double)j;
-            double kz = k0 * k0 - kx * kx - ky * ky;
-            if (!(kz >= 0.0)) continue;
-            kz = sqrt(kz);
+            double kz;
+            if (nquicklens == 1) {
+                kz = k0 * k0 - kx * kx - ky * ky;
+                if (!(kz >= 0.0)) continue;
+                kz = sqrt(kz);
+            } else {
+                /* cdmlib.f:3885-3916: the objective's aperture */
+                if (!(sqrt(kx * kx + ky * ky) <= numaper)) continue;
+                kz = sqrt(k0 * k0 - kx * kx - ky * ky);
+            }
             zc zf = cexp(I * kz * zlens);
             zc *e = Ed + ((size_t)(imax + j) * S + (imax + i)) * 3;
             zc *ei = Ei + ((size_t)(imax + j) * S + (imax + i)) * 3;
             zc f[6];
             for (int c = 0; c < 3; c++) {
                 f[c] = e[c] * zf;
-                f[c + 3] = dside > 0 ? (e[c] + ei[c]) * zf : 0;
+                if (dside < 0) f[c + 3] = 0;
+                else f[c + 3] = nquicklens == 1 ? (e[c] + ei[c]) * zf : f[c] + ei[c] * zf;
             }
             if (fourier)
                 for (int c = 0; c < 6; c++) fourier[(size_t)c * S * S + (size_t)(imax + j) * S + (imax + i)] = f[c];

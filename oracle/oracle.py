@@ -469,7 +469,8 @@ def farfield_fft(nx, ny, nz, d, xs, ys, zs, FF, k0, I0, theta, phi, nfft2d, nthe
                 kpos=kp[:S * S].copy(), kneg=kn[:S * S].copy())
 
 
-def holography(nx, ny, nz, d, k0, xs, ys, zs, FF, E0, theta, phi, pp, nfft2d, numaper, gross, zlens, nside=0):
+def holography(nx, ny, nz, d, k0, xs, ys, zs, FF, E0, theta, phi, pp, nfft2d, numaper, gross, zlens, nside=0,
+               nquicklens=1):
     """Holographic microscope with the FFT lens after one plane-wave solve
     (cdmlib.f:4075-4660): complex image fields (6, n, n) [x, y, z, then with
     the incident wave], the pupil fields (6, S, S), xy, kxy, imaxk0."""
@@ -480,13 +481,13 @@ def holography(nx, ny, nz, d, k0, xs, ys, zs, FF, E0, theta, phi, pp, nfft2d, nu
     imax = C.c_int(0)
     info = C.create_string_buffer(b" " * 64, 65)
     f = lib().orc_holography
-    f.argtypes = [C.c_int] * 3 + [C.c_double] * 2 + [C.c_void_p] * 4 + [_ZC] + [C.c_double] * 3 + [C.c_int] + \
-        [C.c_double] * 3 + [C.c_int] + [C.c_void_p] * 5 + [C.c_char_p]
+    f.argtypes = [C.c_int] * 3 + [C.c_double] * 2 + [C.c_int] + [C.c_void_p] * 4 + [_ZC] + [C.c_double] * 3 + \
+        [C.c_int] + [C.c_double] * 3 + [C.c_int] * 2 + [C.c_void_p] * 5 + [C.c_char_p]
     f.restype = C.c_int
     e0 = complex(E0)
-    rc = f(nx, ny, nz, d, k0, _p(np.ascontiguousarray(xs, np.float64)), _p(np.ascontiguousarray(ys, np.float64)),
+    rc = f(nx, ny, nz, d, k0, len(xs), _p(np.ascontiguousarray(xs, np.float64)), _p(np.ascontiguousarray(ys, np.float64)),
            _p(np.ascontiguousarray(zs, np.float64)), _p(_z(FF)), _ZC(e0.real, e0.imag), theta, phi, pp, n, numaper,
-           gross, zlens, nside, _p(img), _p(four), _p(xy), _p(kxy), C.byref(imax), info)
+           gross, zlens, nside, nquicklens, _p(img), _p(four), _p(xy), _p(kxy), C.byref(imax), info)
     S = 2 * imax.value + 1
     return dict(nstop=rc, infostr=info.raw[:64].decode(errors="replace"), image=img.reshape(6, n, n),
                 fourier=four[:6 * S * S].reshape(6, S, S), xy=xy, kxy=kxy, imaxk0=imax.value)

@@ -163,3 +163,27 @@ def test_cdmlib_holography_matches_oracle(orc):
                          100.0, 50e-9)
     for c, name in enumerate(("Eimagex", "Eimagey", "Eimagez", "Eimageincx", "Eimageincy", "Eimageincz")):
         assert rel(out[name], ref["image"][c]) < 1e-10, name
+
+
+@pytest.mark.parametrize("nside,inside", [(0, True), (1, False)])
+def test_holography_direct_lens_matches_oracle(gctx, orc, nside, inside):
+    """Holography without the FFT lens (cdmlib.f:3803-4074): the finer pupil
+    grid and the far field by direct summation, on the inside-only object or
+    the full box."""
+    from ifdda import objects
+    k0 = 2 * math.pi / 632.8e-9
+    ob = objects.sphere(100e-9, 2.25 + 0j, 8, k0, "RR", na=-1 if inside else 0)
+    E0, _ = orc.irradiance(1.0, 6328e-9)
+    ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 0.3, 0, 10.0, 30.0)
+    G = orc.greencalculfft(8, 8, 8, ob.aretecube, k0)
+    sol = orc.inverserig(G, 8, 8, 8, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-8,
+                         tabdip=ob.tabdip_or_none)
+    args = (8, 8, 8, ob.aretecube, k0, ob.xs, ob.ys, ob.zs, sol["FF"], E0, 10.0, 30.0, 0.3)
+    ref = orc.holography(*args, 64, 0.9, 100.0, 50e-9, nside=nside, nquicklens=0)
+    got = gctx.holography(*args, nfft2d=64, numaper=0.9, gross=100.0, zlens=50e-9, nside=nside, nquicklens=0)
+    assert got["nstop"] == ref["nstop"] == 0, (got["infostr"], ref["infostr"])
+    assert got["imaxk0"] == ref["imaxk0"] > 20
+    assert np.array_equal(got["xy"], ref["xy"])
+    for c in range(3 if nside else 6):
+        assert rel(got["image"][c], ref["image"][c]) < 1e-10, c
+        assert rel(got["fourier"][c], ref["fourier"][c]) < 1e-10, c

@@ -43,7 +43,7 @@ def test_cdmlib_driver_rejects_like_the_reference():
     assert cdmlib(numaper=1.5, **sph)["infostr"] == "Problem with numerical aperture!"
     assert cdmlib(gross=0.5, **sph)["infostr"] == "Problem with manification!"
     assert cdmlib(theta=95.0, **sph)["infostr"] == "Illumination on the wrong side with the options"
-    assert cdmlib(ntypemic=0, nquicklens=0, **sph)["nstop"] == 1  # holography only with the FFT lens
+    assert cdmlib(ntypemic=3, **sph)["nstop"] == 1
     assert cdmlib(nquicklens=2, **sph)["nstop"] == 1
     # scattering cross section by integration (cdmlib.f:394-400, :2789-2793)
     sph = dict(wavelength=632.8, object="sphere", rayon=100.0, eps=2.25, nnnr=8, nsectionsca=1)
