@@ -350,10 +350,21 @@ def run_gpu(args):
     lib.ifdda_timing_enable(0, -1)
     zconv_ms = tot.value / max(nl.value, 1)
     g.release_workspace()
+    kacc = w.fp64_nrhs
+    loc_mixed, ff_mixed = loc_d[:kacc].cpu().numpy(), ff_d[:kacc].cpu().numpy()
 
     fp64_steps = max(1, min(args.steps, 5))
     t_fp64, info_fp64, _ = timed(IFDDA_FP64, fp64_steps, min(args.warmup, 2), k=w.fp64_nrhs)
     g.release_workspace()
+    # accuracy of the mixed solve against the plain FP64 drop-in (which the
+    # parity tests hold to the oracle): local field and Cext
+    loc64, ff64 = loc_d[:kacc].cpu().numpy(), ff_d[:kacc].cpu().numpy()
+    err_loc, err_cext = 0.0, 0.0
+    for r in range(kacc):
+        err_loc = max(err_loc, float(np.linalg.norm(loc_mixed[r] - loc64[r]) / np.linalg.norm(loc64[r])))
+        cm, _ = ctx.cross_sections(ff0_h[r], ff_mixed[r], loc_mixed[r], k0, abs(E0) ** 2)
+        c6, _ = ctx.cross_sections(ff0_h[r], ff64[r], loc64[r], k0, abs(E0) ** 2)
+        err_cext = max(err_cext, abs(cm - c6) / abs(c6))
 
     total_ms = max_over_ranks(sum(t_mixed), ws, dev)
     value = ws * args.steps * nrhs / (total_ms / 1e3)
@@ -443,6 +454,8 @@ def run_gpu(args):
         "fp64": {"solves_s": fp64_value, "nrhs": w.fp64_nrhs, "ms_per_solve": fp64_total / fp64_steps,
                  "nloop_max": int(np.max(i64["nloop"])), "ncompte_max": int(np.max(i64["ncompte"])),
                  "tol1_max": float(np.max(i64["tol1"]))},
+        "accuracy": {"local_field_rel_l2_mixed_vs_fp64": err_loc, "cext_rel_diff_mixed_vs_fp64": err_cext,
+                     "rhs_compared": kacc},
         "matvec": mv,
         "green_build_ms": green_ms,
         "roofline": {"bound": "hbm", "kernel": f"k_zconv<float,{Z}> (z FFT + 3x3 spectrum multiply + inverse z FFT)",
