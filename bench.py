@@ -1,6 +1,6 @@
 """Benchmark: solves/s of the FFT-accelerated dipole solve on one B200.
 
-Default workload (one step = one complete rigorous solve):
+Default workload (one step = one complete rigorous solve of the inhomogeneous cube):
   inhomogeneous cube 64x64x64 (262,144 dipoles), d = 10 nm, lambda 632.8 nm,
   permittivity from the seeded Gaussian random field (mean 2.25, std 0.1,
   lc = 50 nm, SUNIF seed 4*7+1), plane wave theta = 20 deg p-polarised, RR
