@@ -110,14 +110,14 @@ int method_code(const char* m) {
     if (m) memcpy(buf, m, std::min<size_t>(strnlen(m, 12), 12));
     // the reference's elseif chain (cdmlib/inverserigopt.f:42-1009) compares
     // prefixes of the blank-padded character(12) methodeit, in this order;
-    // the methods not built here answer "Iterative method not correct!"
+    // any other string answers "Iterative method not correct!"
     if (!strncmp(buf, "GPBICG1", 7)) return 1;
     if (!strncmp(buf, "GPBICG2", 7)) return 8;
     if (!strncmp(buf, "GPBICGsafe", 10)) return 7;
     if (!strncmp(buf, "GPBICGplus", 10)) return 9;
     if (!strncmp(buf, "GPBICGAR", 8)) return 10;  // 'GPBICGAR2' too: (1:8) is tested first
     if (!strncmp(buf, "BICGSTARPLUS", 12)) return 11;
-    if (!strncmp(buf, "QMRCLA", 6)) return 0;
+    if (!strncmp(buf, "QMRCLA", 6)) return 14;
     if (!strncmp(buf, "TFQMR", 5)) return 6;
     if (!strncmp(buf, "CG   ", 5)) return 5;
     if (!strncmp(buf, "BICGSTAB", 8)) return 4;

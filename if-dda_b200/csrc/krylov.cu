@@ -133,7 +133,8 @@ template void cast_dev<double>(const double2*, double2*, long, cudaStream_t);
 int reduction_blocks(long n3) { return (int)std::max<long>(1, std::min<long>((n3 + KNT * 4 - 1) / (KNT * 4), 1024)); }
 
 template <class T> void KrylovWork<T>::ensure(int method, int nrhs_, long n3_) {
-    static const int nslots[] = {0, G_NSLOT, Q_NSLOT, 0, B_NSLOT, C_NSLOT, T_NSLOT, S_NSLOT, A_NSLOT, P_NSLOT, R_NSLOT, O_NSLOT};
+    static const int nslots[] = {0,       G_NSLOT, Q_NSLOT, 0,       B_NSLOT, C_NSLOT, T_NSLOT,
+                                 S_NSLOT, A_NSLOT, P_NSLOT, R_NSLOT, O_NSLOT, L_NSLOT};
     nslot = nslots[method_family(method)];
     nrhs = nrhs_;
     n3 = n3_;
@@ -196,6 +197,22 @@ static void mv_solver(Green& G, const SolveSpec& sp, KrylovWork<T>& W, int sx, i
     MvArgs<T> a = mv_args<T>(G, W.nrhs, x, x, y, W.n3, sp.amode, (const cplx<T>*)sp.alpha, sp.nmax, sp.tabdip, status);
     if (!matvec_launch<T>(a, W.nrhs, sp.tabdip != nullptr, st))
         throw EngineError{1, "FFT size not supported by the compiled kernels"};
+}
+
+// y = A^T x for the QMRCLA branch (cdmlib/inverserigopt.f:555-584): the
+// scratch slot T gets x - G x from a mat-vec without the polarisability,
+// then y = alpha^T (T - x) + x.  No memset, so the pass stays a pair of
+// kernel nodes inside the captured loop body.
+template <class T>
+static void mv_transpose(Green& G, const SolveSpec& sp, KrylovWork<T>& W, int sx, int sy, int* status,
+                         const RedSlots& rs, cudaStream_t st) {
+    Slots<T> V = W.slots();
+    MvArgs<T> a = mv_args<T>(G, W.nrhs, V.v(sx, 0), V.v(sx, 0), V.v(L_T, 0), W.n3, ALPHA_NONE, nullptr, 0, sp.tabdip,
+                             status);
+    if (!matvec_launch<T>(a, W.nrhs, sp.tabdip != nullptr, st))
+        throw EngineError{1, "FFT size not supported by the compiled kernels"};
+    vec_launch<0>(LTrans<T>{V, W.st.p, sx, sy, sp.amode, (const cplx<T>*)sp.alpha, sp.nmax}, W.n3, W.nblk, W.nrhs, rs,
+                  status, st);
 }
 
 template <class T> static bool poll(KrylovWork<T>& W, const SolveSpec& sp, cudaStream_t st, bool& cancelled) {
@@ -328,6 +345,13 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
                 mv_solver<T>(G, sp, W, T_U, T_AU, status, st);
                 vec_launch<1>(TV<T, true>{V, S}, n3, nblk, nrhs, rs, status, st);
             }
+        } else if (sp.method == 14) {
+            vec_launch<1>(LA<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            mv_solver<T>(G, sp, W, L_W2, L_W3, status, st);
+            vec_launch<3>(LB<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            mv_transpose<T>(G, sp, W, L_W8, L_W9, status, rs, st);
+            vec_launch<1>(LC<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+            vec_launch<1>(LD<T>{V, S}, n3, nblk, nrhs, rs, status, st);
         } else if (sp.method == 5) {
             vec_launch<1>(CUpdate<T>{V, S}, n3, nblk, nrhs, rs, status, st);
             mv_solver<T>(G, sp, W, C_R, C_S, status, st);
@@ -379,6 +403,12 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
         vec_launch<0>(TInit1<T>{V, S}, n3, nblk, nrhs, rs, status, st);
         mv_solver<T>(G, sp, W, T_U, T_V, status, st);
         vec_launch<1>(TInit2<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+    } else if (sp.method == 14) {
+        vec_launch<1>(LStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
+        if (!sp.zero_guess) mv_solver<T>(G, sp, W, L_X, L_XR, status, st);
+        vec_launch<3>(LInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
+        mv_transpose<T>(G, sp, W, L_W8, L_W9, status, rs, st);
+        vec_launch<1>(LInit2<T>{V, S}, n3, nblk, nrhs, rs, status, st);
     } else if (sp.method == 5) {
         vec_launch<1>(CStart<T>{V, S, sp.zero_guess}, n3, nblk, nrhs, rs, status, st);
         if (!sp.zero_guess) mv_solver<T>(G, sp, W, C_X, C_XR, status, st);
@@ -536,20 +566,21 @@ int method_family(int method) {
     case 11: return 9;
     case 12: return 10;
     case 13: return 11;
+    case 14: return 12;
     default: return 2;
     }
 }
 
 template <class T> int KrylovWork<T>::x_slot(int method) const {
-    static const int s[] = {0, G_X, Q_X, 0, B_X, C_X, T_X, S_X, A_X, P_X, R_X, O_X};
+    static const int s[] = {0, G_X, Q_X, 0, B_X, C_X, T_X, S_X, A_X, P_X, R_X, O_X, L_X};
     return s[method_family(method)];
 }
 template <class T> int KrylovWork<T>::b_slot(int method) const {
-    static const int s[] = {0, G_B, Q_B, 0, B_B, C_B, T_B, S_B, A_B, P_B, R_B, O_B};
+    static const int s[] = {0, G_B, Q_B, 0, B_B, C_B, T_B, S_B, A_B, P_B, R_B, O_B, L_B};
     return s[method_family(method)];
 }
 template <class T> int KrylovWork<T>::xr_slot(int method) const {
-    static const int s[] = {0, G_XR, Q_XR, 0, B_XR, C_XR, T_XR, S_XR, A_XR, P_XR, R_XR, O_XR};
+    static const int s[] = {0, G_XR, Q_XR, 0, B_XR, C_XR, T_XR, S_XR, A_XR, P_XR, R_XR, O_XR, L_XR};
     return s[method_family(method)];
 }
 
@@ -561,7 +592,12 @@ template <class T> int KrylovWork<T>::xr_slot(int method) const {
 // :676-742; TFQMR: one per pass plus A x0, A u0 and the residual one, and
 // the driver adds one to ITNO, :603-675).
 void method_counts(int method, int itno, int& nloop, int& ncompte) {
-    if (method == 1 || (method >= 7 && method != 13)) {
+    if (method == 14) {
+        // QMRCLA (:499-598): A x0, A^T r0, two products per pass and the
+        // residual one; its branch does not add one to ITNO
+        nloop = itno;
+        ncompte = 2 * itno + 3;
+    } else if (method == 1 || (method >= 7 && method != 13)) {
         // GPBICG1, GPBICGsafe (:174-237), GPBICG2 (:109-173), GPBICGplus
         // (:238-301), GPBICGAR (:302-366), BICGSTARPLUS (:431-498), CORS
         // (:1009-1072); GPBICOR (:943-1008) counts ITNO from 1 and its driver
@@ -719,7 +755,10 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
             int its = 0, mvs = 0;
             method_counts(sp.method, hs[r].itno, its, mvs);
             inner_iters[r] += its;
-            inner_mv[r] += sp.method == 5 || sp.method == 6 ? its + 1 : 2 * its;  // zero initial guess: no A x0
+            // zero initial guess: no A x0 (QMRCLA still forms A^T r0)
+            if (sp.method == 5 || sp.method == 6) inner_mv[r] += its + 1;
+            else if (sp.method == 14) inner_mv[r] += 2 * its + 1;
+            else inner_mv[r] += 2 * its;
             inner_runs[r] += 1;
         }
         count_launch();

@@ -12,6 +12,7 @@
 // once, so the host may launch iterations ahead and check the status only now
 // and then.  Vectors may be FP32 or FP64 complex; scalars and sums are FP64.
 #pragma once
+#include "matvec_kernels.cuh"  // ALPHA_* modes of the transposed product
 #include "reduce.cuh"
 
 namespace ifdda {
@@ -1678,6 +1679,247 @@ template <class T, bool ODD> struct TV {
 };
 
 // ------------------------------------------------------------ shared ------
+// ---------------------------------------------------------------- QMRCLA ----
+// QMR without look-ahead (PIMZQMR, cdmlib/qmrpim.f:1-270), with products by
+// A and by A^T.  Slots: w1 .. w9 are the reference's WRK columns 1 .. 9, T the
+// scratch of the transposed product.  State: lambda = alpha, kappa = beta,
+// theta, gamma = dzeta, ksi = eta, rho, epsilon = omega, mu = etaq, tau, the
+// dot products DOTS1..3 in c2, c5, f1.
+enum { L_X = 0, L_W1, L_W2, L_W3, L_W4, L_W5, L_W6, L_W7, L_W8, L_W9, L_T, L_XR, L_B, L_NSLOT };
+
+// label 10 (qmrpim.f:45-64): NORM = ||b||, x = x0
+template <class T> struct LStart {
+    Slots<T> V;
+    KState* stt;
+    int zero_guess;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 b = ld(V.v(L_B, r), i);
+        st(V.v(L_X, r), i, zero_guess ? make_double2(0, 0) : b);
+        if (zero_guess) st(V.v(L_XR, r), i, make_double2(0, 0));
+        acc[0].x += b.x * b.x + b.y * b.y;
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.alpha = make_double2(1, 0);
+        s.beta = make_double2(-1, 0);
+        s.theta = make_double2(-1, 0);
+        s.norm = sqrt(a[0].x);
+        s.itno = 0;
+        s.steperr = -1;
+    }
+};
+
+// label 20 (:68-92): w3 = A x0, w1 = w7 = w8 = b - A x0, w2 = w4 = w5 = w6 = 0;
+// DOTS1 = w7^H w7, DOTS2 = w8^H w8, DOTS3 = w7^T w8
+template <class T> struct LInit {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        const double2 w3 = ld(V.v(L_XR, r), i), w1 = zsub(ld(V.v(L_B, r), i), w3);
+        st(V.v(L_W3, r), i, w3);
+        st(V.v(L_W1, r), i, w1);
+        st(V.v(L_W7, r), i, w1);
+        st(V.v(L_W8, r), i, w1);
+        const double2 z = make_double2(0, 0);
+        st(V.v(L_W2, r), i, z);
+        st(V.v(L_W4, r), i, z);
+        st(V.v(L_W5, r), i, z);
+        st(V.v(L_W6, r), i, z);
+        acc[0] = zadd(acc[0], zconjmul(w1, w1));
+        acc[1] = zadd(acc[1], zconjmul(w1, w1));
+        acc[2] = zadd(acc[2], zmul(w1, w1));
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.c2 = a[0];
+        s.c5 = a[1];
+        s.f1 = a[2];
+    }
+};
+
+// The transposed product's second half (inverserigopt.f:570-583): slot T
+// holds x - G x, and out = alpha^T (T - x) + x (A^T = I - alpha^T G, G being
+// symmetric)
+template <class T> struct LTrans {
+    Slots<T> V;
+    KState* stt;
+    int sin, sout;
+    int amode;
+    const cplx<T>* alpha;
+    long nmax;
+    __device__ void elem(const KState&, int r, long i, double2*) const {
+        const long d = i / 3;
+        const int c = (int)(i - 3 * d);
+        const cplx<T>* t = V.v(L_T, r);
+        const cplx<T>* x = V.v(sin, r);
+        const double2 xi = ld(x, i);
+        double2 acc;
+        if (amode == ALPHA_ISO) {
+            acc = zmul(to_d(alpha[d]), zsub(ld(t, i), xi));
+        } else if (amode == ALPHA_FULL) {
+            acc = make_double2(0, 0);
+            for (int b = 0; b < 3; b++)
+                acc = zadd(acc, zmul(to_d(alpha[d + nmax * (b + 3 * c)]), zsub(ld(t, 3 * d + b), ld(x, 3 * d + b))));
+        } else {
+            acc = zsub(ld(t, i), xi);
+        }
+        st(V.v(sout, r), i, zadd(acc, xi));
+    }
+    __device__ void finish(int, KState&, int&, const double2*) const {}
+};
+
+// label 30 (:96-121): DOTS4 = w7^T w9 (w9 = A^T w8), then gamma, ksi, rho,
+// epsilon, mu = 0, tau
+template <class T> struct LInit2 {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        acc[0] = zadd(acc[0], zmul(ld(V.v(L_W7, r), i), ld(V.v(L_W9, r), i)));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        s.dzeta = zsqrt(s.c2);
+        s.eta = zsqrt(s.c5);
+        s.rho = s.f1;
+        s.omega = a[0];
+        s.etaq = make_double2(0, 0);
+        if (zisnull(s.rho)) {
+            s.itno = 0;
+            s.steperr = 5;
+            status = -1;
+            return;
+        }
+        s.tau = zdiv(s.omega, s.rho);
+        // the checks that open label 100
+        if (zisnull(s.dzeta)) {
+            s.steperr = 6;
+            status = -1;
+        } else if (zisnull(s.eta)) {
+            s.steperr = 7;
+            status = -1;
+        }
+    }
+};
+
+// label 100 (:122-146): ITNO + 1, the zero checks, w2 = w7 / gamma - mu w2,
+// w4 = (w9 - gamma mu w4) / ksi (A w2 follows).  The checks of this pass are
+// made by the previous pass's finish (or LInit2's) on the new values, so the
+// pass itself only updates; its single sum is unused.
+template <class T> struct LA {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2*) const {
+        const double2 w2 = zsub(zdiv(ld(V.v(L_W7, r), i), s.dzeta), zmul(s.etaq, ld(V.v(L_W2, r), i)));
+        const double2 w4 = zdiv(zsub(ld(V.v(L_W9, r), i), zmul(zmul(s.dzeta, s.etaq), ld(V.v(L_W4, r), i))), s.eta);
+        st(V.v(L_W2, r), i, w2);
+        st(V.v(L_W4, r), i, w4);
+    }
+    __device__ void finish(int, KState& s, int&, const double2*) const { s.itno += 1; }
+};
+
+// label 40 (:148-166): w3 = A w2, w7 = w3 - tau / gamma w7, w8 = w4 - tau /
+// ksi w8, the three dots (A^T w8 follows)
+template <class T> struct LB {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2* acc) const {
+        const double2 w7 = zsub(ld(V.v(L_W3, r), i), zmul(zdiv(s.tau, s.dzeta), ld(V.v(L_W7, r), i)));
+        const double2 w8 = zsub(ld(V.v(L_W4, r), i), zmul(zdiv(s.tau, s.eta), ld(V.v(L_W8, r), i)));
+        st(V.v(L_W7, r), i, w7);
+        st(V.v(L_W8, r), i, w8);
+        acc[0] = zadd(acc[0], zconjmul(w7, w7));
+        acc[1] = zadd(acc[1], zconjmul(w8, w8));
+        acc[2] = zadd(acc[2], zmul(w7, w8));
+    }
+    __device__ void finish(int, KState& s, int&, const double2* a) const {
+        s.c2 = a[0];
+        s.c5 = a[1];
+        s.f1 = a[2];
+    }
+};
+
+// label 50, first half (:176-215): DOTS4 = w7^T w9, then gamma, ksi, rho,
+// epsilon, mu, tau, theta, kappa, lambda with the breakdown checks 12-14
+template <class T> struct LC {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState&, int r, long i, double2* acc) const {
+        acc[0] = zadd(acc[0], zmul(ld(V.v(L_W7, r), i), ld(V.v(L_W9, r), i)));
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        const double2 gamma0 = s.dzeta, ksi0 = s.eta, rho0 = s.rho;
+        s.dzeta = zsqrt(s.c2);
+        s.eta = zsqrt(s.c5);
+        s.rho = s.f1;
+        s.omega = a[0];
+        double2 den = zmul(zmul(s.dzeta, s.tau), rho0);
+        if (zisnull(den)) {
+            s.steperr = 12;
+            status = -1;
+            return;
+        }
+        s.etaq = zdiv(zmul(zmul(gamma0, ksi0), s.rho), den);
+        if (zisnull(s.rho)) {
+            s.steperr = 13;
+            status = -1;
+            return;
+        }
+        const double2 tau0 = s.tau;
+        s.tau = zsub(zdiv(s.omega, s.rho), zmul(s.dzeta, s.etaq));
+        const double at = hypot(tau0.x, tau0.y), ag = hypot(s.dzeta.x, s.dzeta.y);
+        const double abstau02 = at * at, absgamma2 = ag * ag;
+        den = make_double2(s.alpha.x * abstau02 + absgamma2, s.alpha.y * abstau02);
+        if (zisnull(den)) {
+            s.steperr = 14;
+            status = -1;
+            return;
+        }
+        s.theta = zdiv(make_double2(abstau02 * (1.0 - s.alpha.x), -abstau02 * s.alpha.y), den);
+        const double2 kappa0 = s.beta;
+        const double2 k = zmul(zmul(gamma0, zconj(tau0)), kappa0);
+        s.beta = zdiv(make_double2(-k.x, -k.y), den);
+        s.alpha = zdiv(make_double2(s.alpha.x * abstau02, s.alpha.y * abstau02), den);
+    }
+};
+
+// label 50, second half (:217-240): w5 = theta w5 + kappa w2, w6 = theta w6 +
+// kappa w3, x += w5, w1 -= w6; stop when ||w1|| / NORM <= tol; past the
+// iteration limit the reference fails (STATUS = -1)
+template <class T> struct LD {
+    Slots<T> V;
+    KState* stt;
+    __device__ void elem(const KState& s, int r, long i, double2* acc) const {
+        const double2 w5 = zadd(zmul(s.theta, ld(V.v(L_W5, r), i)), zmul(s.beta, ld(V.v(L_W2, r), i)));
+        const double2 w6 = zadd(zmul(s.theta, ld(V.v(L_W6, r), i)), zmul(s.beta, ld(V.v(L_W3, r), i)));
+        st(V.v(L_W5, r), i, w5);
+        st(V.v(L_W6, r), i, w6);
+        st(V.v(L_X, r), i, zadd(ld(V.v(L_X, r), i), w5));
+        const double2 w1 = zsub(ld(V.v(L_W1, r), i), w6);
+        st(V.v(L_W1, r), i, w1);
+        acc[0].x += w1.x * w1.x + w1.y * w1.y;
+    }
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
+        s.residu = sqrt(fabs(a[0].x)) / s.norm;
+        if (s.residu <= s.tol) {
+            status = 1;
+            s.steperr = 0;
+            return;
+        }
+        if (s.itno > s.maxit) {
+            // STATUS = -1, ITNO = MAXIT, then label 100 counts one more
+            s.itno = s.maxit + 1;
+            s.steperr = 0;
+            status = -1;
+            return;
+        }
+        // the checks that open label 100 for the next pass
+        if (zisnull(s.dzeta)) {
+            s.steperr = 6;
+            status = -1;
+        } else if (zisnull(s.eta)) {
+            s.steperr = 7;
+            status = -1;
+        }
+    }
+};
+
 // y = alpha . x (polarisability, cdmlib/inverserigopt.f:68-80) on FP64 vectors
 __global__ void k_apply_alpha(const double2* __restrict__ x, double2* __restrict__ y, long nd, int nrhs, long stride,
                               int amode, const double2* __restrict__ alpha, long nmax);

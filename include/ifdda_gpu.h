@@ -117,9 +117,9 @@ int ifdda_matvec_noalloc(ifdda_green* g, int precision, int ndip, const int* tab
    | "CG" (zcg.f) | "TFQMR" (tfqmr.f) | "GPBICGsafe" (gpbicgsafe.f) | "GPBICG2"
    (gpbicg2.f) | "GPBICGplus" (gpbicgplus.f) | "GPBICGAR" (gpbicgar.f; also
    "GPBICGAR2", as in the reference) | "BICGSTARPLUS" (bicgstarplus.f) |
-   "GPBICOR" (gpbicor.f) | "CORS" (cors.f), matched by prefix in the
-   reference's order; the other
-   methods of the reference answer nstop = 1, "Iterative method not
+   "GPBICOR" (gpbicor.f) | "CORS" (cors.f) | "QMRCLA" (qmrpim.f, with
+   products by A^T = I - alpha^T G), matched by prefix in the reference's
+   order; any other string answers nstop = 1, "Iterative method not
    correct!".  On return FFloc = E (local field), FF = polarisa . E (dipole
    moments), tol1 = ||A E - FF0|| / NORM in FP64 with the method's NORM
    (||FF0||; for BICGSTAB the squared norm of the initial residual, as the

@@ -1742,6 +1742,184 @@ static void apply_pola(long nbs, long nmax, const zc *pol, const zc *xr, zc *xi)
     }
 }
 
+/* ------------------------------------------------------------------------- */
+/* QMR without look-ahead, PIMZQMR (cdmlib/qmrpim.f:1-270), behind methodeit  */
+/* 'QMRCLA'.  Reverse communication: on return *nt = 1 asks for A xi, *nt = 2 */
+/* for A^T xi (inverserigopt.f:528-584).  W columns 1..9 (0-based here).      */
+/* xs is the solution (the reference passes FFloc).                           */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    zc lambda, kappa, theta, gamma, ksi, rho, eps, mu, tau, dots1, dots2, dots3, dots4;
+    double norm;
+} qmrcla_state;
+
+static void qmrcla(zc *xs, zc *xi, const zc *xr, const zc *B, long n, int *nou, int *nt, zc *W,
+                   int *itno, int maxit, double tol, qmrcla_state *s, int *status, int *steperr) {
+#define WC(c) (W + (size_t)(c - 1) * n)
+    zc *w1 = WC(1), *w2 = WC(2), *w3 = WC(3), *w4 = WC(4), *w5 = WC(5), *w6 = WC(6), *w7 = WC(7),
+       *w8 = WC(8), *w9 = WC(9);
+#undef WC
+    switch (*nou) {
+    case 0: {
+        s->lambda = 1.0;
+        s->kappa = -1.0;
+        s->theta = -1.0;
+        double nrm = 0;
+        for (long i = 0; i < n; i++) {
+            nrm += creal(B[i] * conj(B[i]));
+            xs[i] = xi[i];
+        }
+        s->norm = sqrt(nrm);
+        *status = 0;
+        *steperr = -1;
+        *itno = 0;
+        *nou = 1;
+        *nt = 1;
+        return;
+    }
+    case 1: {
+        zc d1 = 0, d2 = 0, d3 = 0;
+        for (long i = 0; i < n; i++) {
+            w3[i] = xr[i];
+            w1[i] = B[i] - w3[i];
+            w7[i] = w1[i];
+            w8[i] = w1[i];
+            w2[i] = w4[i] = w5[i] = w6[i] = 0;
+            d1 += w7[i] * conj(w7[i]);
+            d2 += w8[i] * conj(w8[i]);
+            d3 += w7[i] * w8[i];
+            xi[i] = w8[i];
+        }
+        s->dots1 = d1; s->dots2 = d2; s->dots3 = d3;
+        *nt = 2;
+        *nou = 2;
+        return;
+    }
+    case 2: {
+        zc d4 = 0;
+        for (long i = 0; i < n; i++) {
+            w9[i] = xr[i];
+            d4 += w7[i] * w9[i];
+        }
+        s->dots4 = d4;
+        s->gamma = csqrt(s->dots1);
+        s->ksi = csqrt(s->dots2);
+        s->rho = s->dots3;
+        s->eps = s->dots4;
+        s->mu = 0;
+        if (cabs(s->rho) == 0.0) {
+            *itno = 0;
+            *status = -3;
+            *steperr = 5;
+            return;
+        }
+        s->tau = s->eps / s->rho;
+        goto label100;
+    }
+    case 3: {
+        zc d1 = 0, d2 = 0, d3 = 0;
+        for (long i = 0; i < n; i++) {
+            w3[i] = xr[i];
+            w7[i] = w3[i] - s->tau / s->gamma * w7[i];
+            w8[i] = w4[i] - s->tau / s->ksi * w8[i];
+            d1 += w7[i] * conj(w7[i]);
+            d2 += w8[i] * conj(w8[i]);
+            d3 += w7[i] * w8[i];
+            xi[i] = w8[i];
+        }
+        s->dots1 = d1; s->dots2 = d2; s->dots3 = d3;
+        *nt = 2;
+        *nou = 4;
+        return;
+    }
+    case 4: {
+        zc d4 = 0;
+        for (long i = 0; i < n; i++) {
+            w9[i] = xr[i];
+            d4 += w7[i] * w9[i];
+        }
+        s->dots4 = d4;
+        zc gamma0 = s->gamma, ksi0 = s->ksi, rho0 = s->rho;
+        s->gamma = csqrt(s->dots1);
+        s->ksi = csqrt(s->dots2);
+        s->rho = s->dots3;
+        s->eps = s->dots4;
+        zc den = s->gamma * s->tau * rho0;
+        if (cabs(den) == 0.0) { *status = -3; *steperr = 12; return; }
+        s->mu = (gamma0 * ksi0 * s->rho) / den;
+        if (cabs(s->rho) == 0.0) { *status = -3; *steperr = 13; return; }
+        zc tau0 = s->tau;
+        s->tau = s->eps / s->rho - s->gamma * s->mu;
+        double abstau02 = pow(cabs(tau0), 2.0), absgamma2 = pow(cabs(s->gamma), 2.0);
+        den = s->lambda * abstau02 + absgamma2;
+        if (cabs(den) == 0.0) { *status = -3; *steperr = 14; return; }
+        s->theta = (abstau02 * (1.0 - s->lambda)) / den;
+        zc kappa0 = s->kappa;
+        s->kappa = -(gamma0 * conj(tau0) * kappa0) / den;
+        zc lambda0 = s->lambda;
+        s->lambda = lambda0 * abstau02 / den;
+        zc tmp1 = 0;
+        for (long i = 0; i < n; i++) {
+            w5[i] = s->theta * w5[i] + s->kappa * w2[i];
+            w6[i] = s->theta * w6[i] + s->kappa * w3[i];
+            xs[i] = xs[i] + w5[i];
+            w1[i] = w1[i] - w6[i];
+            tmp1 += w1[i] * conj(w1[i]);
+        }
+        double tole = sqrt(cabs(tmp1)) / s->norm;
+        if (tole <= tol) {
+            *nou = 5;
+            *status = 1;
+            return;
+        }
+        if (*itno > maxit) {
+            *status = -1;
+            *itno = maxit;
+        }
+        goto label100;
+    }
+    default:
+        goto label100;
+    }
+label100:
+    *itno += 1;
+    if (cabs(s->gamma) == 0.0) { *status = -3; *steperr = 6; return; }
+    if (cabs(s->ksi) == 0.0) { *status = -3; *steperr = 7; return; }
+    for (long i = 0; i < n; i++) {
+        w2[i] = w7[i] / s->gamma - s->mu * w2[i];
+        w4[i] = (w9[i] - s->gamma * s->mu * w4[i]) / s->ksi;
+        xi[i] = w2[i];
+    }
+    *nt = 1;
+    *nou = 3;
+}
+
+/* A^T xi for the QMRCLA branch (inverserigopt.f:555-584): xr = 0 - G xi,
+   then xr = alpha^T xr + xi (G is symmetric, so A^T = I - alpha^T G) */
+static void apply_transpose(const zc *G6, int nx, int ny, int nz, const int *tabdip, long nbs, long nmax,
+                            const zc *pol, const zc *xi, zc *xr) {
+    long n3 = 3 * nbs;
+    memset(xr, 0, sizeof(zc) * n3);
+    matvec_core(G6, nx, ny, nz, tabdip, xi, xr);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < nbs; i++) {
+        zc t[3];
+        for (int a = 0; a < 3; a++) {
+            zc acc = 0;
+            for (int b = 0; b < 3; b++) acc += pol[i + nmax * b + 3 * nmax * a] * xr[3 * i + b];
+            t[a] = acc;
+        }
+        for (int a = 0; a < 3; a++) xr[3 * i + a] = t[a] + xi[3 * i + a];
+    }
+}
+
+/* The transposed product on its own, for the tests of its identity
+   u^T (A v) = (A^T u)^T v */
+void orc_apply_transpose(const zc *G6, int nx, int ny, int nz, const int *tabdip, int nbs, int nmax,
+                         const zc *pol, const zc *xi, zc *xr) {
+    apply_transpose(G6, nx, ny, nz, tabdip, nbs, nmax, pol, xi, xr);
+}
+
 /* An optional callback lets the CPU baseline stop after a bounded number of
    mat-vecs; it is NULL in the parity tests. */
 typedef int (*orc_cancel_fn)(int ncompte);
@@ -1775,7 +1953,7 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
     else if (strncmp(meth, "GPBICGplus", 10) == 0) kind = 9;
     else if (strncmp(meth, "GPBICGAR", 8) == 0) kind = 10;  /* 'GPBICGAR2' too: (1:8) is tested first */
     else if (strncmp(meth, "BICGSTARPLUS", 12) == 0) kind = 11;
-    else if (strncmp(meth, "QMRCLA", 6) == 0) kind = 0;
+    else if (strncmp(meth, "QMRCLA", 6) == 0) kind = 14;
     else if (strncmp(meth, "TFQMR", 5) == 0) kind = 6;
     else if (strncmp(meth, "CG   ", 5) == 0) kind = 5;
     else if (strncmp(meth, "BICGSTAB", 8) == 0) kind = 4;
@@ -1797,6 +1975,9 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
     gpsafe_state ss;
     cors_state rs;
     gpbicor_state os;
+    qmrcla_state ls;
+    int nt = 1;
+    memset(&ls, 0, sizeof ls);
     memset(&rs, 0, sizeof rs);
     memset(&os, 0, sizeof os);
     memset(&ts, 0, sizeof ts);
@@ -1828,11 +2009,13 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
             gpbicgar(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &ss, &nstat, &steperr);
         else if (kind == 7 || kind == 9)
             gpbicgsafe(xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &ss, &nstat, &steperr, kind == 9);
+        else if (kind == 14)
+            qmrcla(FFloc, xi, xr, FF0, n3, &nou, &nt, W, nloop, nlim, tol, &ls, &nstat, &steperr);
         else
             qmrbicgstab(FFloc, xi, xr, FF0, n3, &nou, W, nloop, nlim, tol, &qs,
                         kind == 2 ? 1 : 2, &nstat, &steperr);
         norm = kind == 1 || kind == 8 ? gs.norm : kind == 4 ? bs.norm : kind == 5 ? cs.norm : kind == 6 ? ts.norm
-             : kind == 12 ? rs.norm : kind == 13 ? os.norm : kind >= 7 ? ss.norm : qs.norm;
+             : kind == 12 ? rs.norm : kind == 13 ? os.norm : kind == 14 ? ls.norm : kind >= 7 ? ss.norm : qs.norm;
         if (nstat < 0) {
             *nstop = 1;
             /* the TFQMR branch prints it without '!' (inverserigopt.f:609) */
@@ -1841,15 +2024,31 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
             return *nstop;
         }
         *ncompte += 1;
-        if (!x_in_floc) {
+        if (kind == 14) {
+            /* inverserigopt.f:516-584: the solution is in FFloc; nt = 1 asks
+               for A xi (xi becomes alpha xi), nt = 2 for A^T xi */
+            if (nstat == 1) {
+                memcpy(xi, FFloc, sizeof(zc) * n3);
+                nt = 1;
+            }
+            if (nt == 1) {
+                memcpy(xr, xi, sizeof(zc) * n3);
+                apply_pola(nbsphere, nmax, polarisa, xr, xi);
+                matvec_core(G6, nx, ny, nz, tabdip, xi, xr);
+            } else {
+                apply_transpose(G6, nx, ny, nz, tabdip, nbsphere, nmax, polarisa, xi, xr);
+            }
+        } else if (!x_in_floc) {
             memcpy(xr, xi, sizeof(zc) * n3);
             if (nstat == 1) memcpy(FFloc, xi, sizeof(zc) * n3);
         } else {
             if (nstat == 1) memcpy(xi, FFloc, sizeof(zc) * n3);
             memcpy(xr, xi, sizeof(zc) * n3);
         }
-        apply_pola(nbsphere, nmax, polarisa, xr, xi);
-        matvec_core(G6, nx, ny, nz, tabdip, xi, xr);
+        if (kind != 14) {
+            apply_pola(nbsphere, nmax, polarisa, xr, xi);
+            matvec_core(G6, nx, ny, nz, tabdip, xi, xr);
+        }
         if (cancel && cancel(*ncompte)) {
             *nstop = -1;
             set_info(infostr, "Calculation cancelled during iterative method");
@@ -1865,7 +2064,8 @@ int orc_inverserig(const zc *G6, int nx, int ny, int nz, int nbsphere, const int
         t += creal(xr[i] * conj(xr[i]));
     }
     *tol1 = sqrt(t) / norm;
-    if (kind == 1 || (kind >= 6 && kind != 13)) *nloop += 1;  /* the GPBICOR branch does not */
+    /* the GPBICOR and QMRCLA branches do not */
+    if (kind == 1 || (kind >= 6 && kind != 13 && kind != 14)) *nloop += 1;
     free(xi); free(xr); free(W);
     return *nstop;
 }

@@ -114,6 +114,17 @@ def matvec(G6, nx, ny, nz, FFX, FFB, tabdip=None) -> np.ndarray:
     return b
 
 
+def apply_transpose(G6, nx, ny, nz, nbsphere, polarisa, nmax, FFX, tabdip) -> np.ndarray:
+    """A^T FFX with A = I - G alpha (the QMRCLA product, inverserigopt.f:555-584)."""
+    g = _z(G6)
+    x = _z(FFX)
+    out = np.zeros(3 * nbsphere, dtype=np.complex128)
+    t = np.ascontiguousarray(tabdip, dtype=np.int32)
+    lib().orc_apply_transpose(_p(g), C.c_int(nx), C.c_int(ny), C.c_int(nz), _p(t), C.c_int(nbsphere), C.c_int(nmax),
+                              _p(_z(polarisa)), _p(x), _p(out))
+    return out
+
+
 def matvec_direct(xs, ys, zs, k0, FFX, FFB) -> np.ndarray:
     xs = np.ascontiguousarray(xs, np.float64)
     ys = np.ascontiguousarray(ys, np.float64)

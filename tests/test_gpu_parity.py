@@ -278,10 +278,12 @@ def test_context_closed_before_its_spectrum():
     ctx2.close()
 
 
-@pytest.mark.parametrize("meth,prec", [("GPBICG1", 0), ("QMRBICGSTAB1", 0), ("GPBICG1", 1)])
+@pytest.mark.parametrize("meth,prec", [("GPBICG1", 0), ("QMRBICGSTAB1", 0), ("GPBICG1", 1), ("QMRCLA", 0),
+                                       ("QMRCLA", 1)])
 def test_anisotropic_polarisability_matches_oracle(gctx, orc, meth, prec):
     """A full 3x3 polarisability per dipole (polarisa(n,a,b) with off-diagonal
-    terms) takes the mat-vec's full-tensor path and the unfused GPBiCG steps."""
+    terms) takes the mat-vec's full-tensor path and the unfused GPBiCG steps;
+    QMRCLA's transposed product then needs alpha^T, not alpha."""
     ob, k0, E0, ff0, G = _c1_inputs(orc, nnnr=10)
     nb, nmax = ob.nbsphere, ob.nmax
     pol = ob.polarisa.copy()
@@ -326,10 +328,10 @@ def test_anisotropy_only_in_the_tail_matches_oracle(gctx, orc):
 
 
 @pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR", "GPBICGsafe", "GPBICG2", "GPBICGplus", "GPBICGAR",
-                                  "BICGSTARPLUS", "CORS", "GPBICOR"])
+                                  "BICGSTARPLUS", "CORS", "GPBICOR", "QMRCLA"])
 def test_other_methods_match_oracle(gctx, orc, meth):
     """The reference's other Krylov methods (pimzbicgstab.f, zcg.f, tfqmr.f,
-    gpbicgsafe.f, gpbicg2.f, gpbicgplus.f, gpbicgar.f) on the sphere
+    gpbicgsafe.f, gpbicg2.f, gpbicgplus.f, gpbicgar.f, qmrpim.f) on the sphere
     (inside-only, Tabdip) and on a full-box GRF cube: identical counters,
     local field within 1e-7, the method's tol1."""
     ob, k0, E0, ff0, G = _c1_inputs(orc)
@@ -351,7 +353,7 @@ def test_other_methods_match_oracle(gctx, orc, meth):
     g.close()
 
 
-@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR", "GPBICGsafe", "GPBICG2"])
+@pytest.mark.parametrize("meth", ["BICGSTAB", "CG", "TFQMR", "GPBICGsafe", "GPBICG2", "QMRCLA"])
 def test_other_methods_mixed_precision(gctx, orc, meth):
     from ifdda import IFDDA_MIXED
     ob, k0, E0, ff0, G = _c1_inputs(orc)

@@ -149,8 +149,63 @@ def test_other_methods_agree_with_gpbicg(orc, meth):
         assert 0 < b["tol1"] < 1e-10
 
 
+def _nonsymmetric_pola(ob, seed=11):
+    pol = ob.polarisa.copy()
+    rng = np.random.default_rng(seed)
+    nb, nmax = ob.nbsphere, ob.nmax
+    for a in range(3):
+        for b in range(3):
+            pol[np.arange(nb) + nmax * (a + 3 * b)] += 0.1 * ob.alpha * (rng.standard_normal(nb) +
+                                                                       1j * rng.standard_normal(nb))
+    return pol
+
+
+def test_transpose_product_identity(orc):
+    """The QMRCLA branch's A^T (inverserigopt.f:555-584) with a full
+    non-symmetric polarisability: u^T (A v) = (A^T u)^T v without
+    conjugation, and A^T u = u - alpha^T G u written out with numpy."""
+    ob, k0, E0 = c1(nnnr=6)
+    G = orc.greencalculfft(6, 6, 6, ob.aretecube, k0)
+    pol = _nonsymmetric_pola(ob)
+    nb, nmax = ob.nbsphere, ob.nmax
+    rng = np.random.default_rng(3)
+    u, v = (rng.standard_normal(3 * nb) + 1j * rng.standard_normal(3 * nb) for _ in range(2))
+
+    def alpha(x, transpose):
+        y = np.zeros_like(x)
+        for a in range(3):
+            for b in range(3):
+                t = pol[np.arange(nb) + nmax * ((b + 3 * a) if transpose else (a + 3 * b))]
+                y[a::3] += t * x[b::3]
+        return y
+
+    av = orc.matvec(G, 6, 6, 6, alpha(v, False), v, tabdip=ob.tabdip)
+    atu = orc.apply_transpose(G, 6, 6, 6, nb, pol, nmax, u, ob.tabdip)
+    assert abs(u @ av - atu @ v) <= 1e-12 * abs(u @ av)
+    want = u + alpha(orc.matvec(G, 6, 6, 6, u, np.zeros_like(u), tabdip=ob.tabdip), True)
+    assert rel(atu, want) < 1e-13
+
+
+@pytest.mark.parametrize("aniso", [False, True])
+def test_qmrcla_agrees_with_gpbicg(orc, aniso):
+    """QMRCLA (qmrpim.f, PIMZQMR) reaches the GPBICG solution, with or
+    without a non-symmetric tensor; its driver counts nloop = ITNO and
+    2 ITNO + 3 mat-vecs (A x0, A^T r0, two a pass, and the final residual)."""
+    ob, k0, E0 = c1(nnnr=8)
+    G = orc.greencalculfft(8, 8, 8, ob.aretecube, k0)
+    ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 1.0, 0, 0.0, 0.0)
+    pol = _nonsymmetric_pola(ob) if aniso else ob.polarisa
+    a = orc.inverserig(G, 8, 8, 8, ob.nbsphere, pol, ob.nmax, ff0, "GPBICG1", 1e-10, tabdip=ob.tabdip)
+    b = orc.inverserig(G, 8, 8, 8, ob.nbsphere, pol, ob.nmax, ff0, "QMRCLA", 1e-10, tabdip=ob.tabdip)
+    assert b["nstop"] == 0, b["infostr"]
+    assert b["ncompte"] == 2 * b["nloop"] + 3
+    assert b["tol1"] < 1e-10
+    assert rel(b["FFloc"], a["FFloc"]) < 1e-8
+
+
 @pytest.mark.parametrize("name,works", [("CG", True), ("CGX", False), ("BICGSTAB", True), ("GPBICGAR2", True),
-                                        ("TFQMR", True), ("BICGSTARPLUS", True), ("QMRCLA", False),
+                                        ("TFQMR", True), ("BICGSTARPLUS", True), ("QMRCLA", True),
+                                        ("QMRCLAX", True),
                                         ("GPBICGsafe", True), ("GPBICG2", True),
                                         ("CORS", True), ("CORSX", False), ("GPBICOR", True)])
 def test_method_prefixes(orc, name, works):
