@@ -394,8 +394,15 @@ def run_gpu(args):
         e1.synchronize()
         ms = e0.elapsed_time(e1) / reps
         balg = s * (7 * N + 6 * Np + 6 * M)
+        # the unpruned algorithm's bytes (x, alpha, y; the full 6-component
+        # spectrum; the padded 3-component field written and read once)
+        bdense = s * (7 * N + 12 * M)
+        pk, _ = measured_peaks()
         mv["fp32" if prec == 2 else "fp64"] = {"ms": round(ms, 4), "alg_bytes": balg,
-                                                "GB_s": round(balg / ms / 1e6, 1)}
+                                                "GB_s": round(balg / ms / 1e6, 1),
+                                                "alg_bytes_unpruned": bdense,
+                                                "GB_s_unpruned": round(bdense / ms / 1e6, 1),
+                                                "frac_unpruned": round(bdense / ms / 1e6 / pk, 3)}
         del x, b
     g.release_workspace()
 
