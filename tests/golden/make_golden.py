@@ -35,6 +35,11 @@ def green_and_matvec():
                         G=G, x=x, b=b, y=y)
 
 
+# every methodeit branch of the reference's driver (cdmlib/inverserigopt.f)
+METHODS = ("GPBICG1", "QMRBICGSTAB1", "QMRBICGSTAB2", "GPBICG2", "GPBICGsafe", "GPBICGplus", "GPBICGAR",
+           "BICGSTARPLUS", "TFQMR", "CG", "BICGSTAB", "GPBICOR", "CORS", "QMRCLA")
+
+
 def sphere_solves():
     lam = 632.8e-9
     k0 = 2 * math.pi / lam
@@ -43,8 +48,8 @@ def sphere_solves():
     ff0 = oracle.incident(ob.xs, ob.ys, ob.zs, k0, E0, 1.0, 0, 0.0, 0.0)
     G = oracle.greencalculfft(8, 8, 8, ob.aretecube, k0)
     out = dict(tabdip=ob.tabdip, alpha=ob.alpha, eps=ob.eps, xs=ob.xs, ys=ob.ys, zs=ob.zs, ff0=ff0, k0=k0,
-               E0=E0, d=ob.aretecube)
-    for meth in ("GPBICG1", "QMRBICGSTAB1", "QMRBICGSTAB2"):
+               E0=E0, d=ob.aretecube, methods=np.array(METHODS))
+    for meth in METHODS:
         r = oracle.inverserig(G, 8, 8, 8, ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-4, tabdip=ob.tabdip)
         out[meth + "_FFloc"] = r["FFloc"]
         out[meth + "_FF"] = r["FF"]
