@@ -1678,7 +1678,6 @@ template <class T, bool ODD> struct TV {
     }
 };
 
-// ------------------------------------------------------------ shared ------
 // ---------------------------------------------------------------- QMRCLA ----
 // QMR without look-ahead (PIMZQMR, cdmlib/qmrpim.f:1-270), with products by
 // A and by A^T.  Slots: w1 .. w9 are the reference's WRK columns 1 .. 9, T the
@@ -1920,6 +1919,7 @@ template <class T> struct LD {
     }
 };
 
+// ------------------------------------------------------------ shared ------
 // y = alpha . x (polarisability, cdmlib/inverserigopt.f:68-80) on FP64 vectors
 __global__ void k_apply_alpha(const double2* __restrict__ x, double2* __restrict__ y, long nd, int nrhs, long stride,
                               int amode, const double2* __restrict__ alpha, long nmax);
