@@ -590,8 +590,9 @@ template <class T> int KrylovWork<T>::xr_slot(int method) const {
 // BiCGSTAB: two mat-vecs per iteration plus the first and the residual one,
 // :743-942; CG: one per iteration plus A x0, A p0 and the residual one,
 // :676-742; TFQMR: one per pass plus A x0, A u0 and the residual one, and
-// the driver adds one to ITNO, :603-675).
-void method_counts(int method, int itno, int& nloop, int& ncompte) {
+// the driver adds one to ITNO, :603-675).  atmax: TFQMR or GPBiCGAR stopped
+// past MAXIT, whose last pass made the product that a converging pass skips.
+void method_counts(int method, int itno, int& nloop, int& ncompte, bool atmax = false) {
     if (method == 14) {
         // QMRCLA (:499-598): A x0, A^T r0, two products per pass and the
         // residual one; its branch does not add one to ITNO
@@ -603,10 +604,10 @@ void method_counts(int method, int itno, int& nloop, int& ncompte) {
         // (:1009-1072); GPBICOR (:943-1008) counts ITNO from 1 and its driver
         // does not add one, so it counts like QMR-BiCGSTAB
         nloop = itno + 1;
-        ncompte = 1 + 2 * (itno + 1) + 1;
+        ncompte = 1 + 2 * (itno + 1) + 1 + (method == 10 && atmax ? 1 : 0);
     } else if (method == 6) {
         nloop = itno + 1;
-        ncompte = nloop + 2;
+        ncompte = nloop + 2 + (atmax ? 1 : 0);
     } else if (method == 5) {
         nloop = itno;
         ncompte = itno + 2;
@@ -664,7 +665,7 @@ void solve_fp64(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b_
         o.steperr = hs[r].steperr;
         o.cancelled = !ok;
         o.tol1 = hf[r].residu;
-        method_counts(sp.method, hs[r].itno, o.nloop, o.ncompte);
+        method_counts(sp.method, hs[r].itno, o.nloop, o.ncompte, hs[r].atmax != 0);
         o.ncompte64 = o.ncompte;
         o.outer = 0;
     }
@@ -753,12 +754,13 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
         for (int r = 0; r < nrhs; r++) {
             if (ost[r]) continue;
             int its = 0, mvs = 0;
-            method_counts(sp.method, hs[r].itno, its, mvs);
+            method_counts(sp.method, hs[r].itno, its, mvs, hs[r].atmax != 0);
             inner_iters[r] += its;
             // zero initial guess: no A x0 (QMRCLA still forms A^T r0)
             if (sp.method == 5 || sp.method == 6) inner_mv[r] += its + 1;
             else if (sp.method == 14) inner_mv[r] += 2 * its + 1;
             else inner_mv[r] += 2 * its;
+            if (hs[r].atmax && (sp.method == 6 || sp.method == 10)) inner_mv[r] += 1;
             inner_runs[r] += 1;
         }
         count_launch();

@@ -26,6 +26,7 @@ struct KState {
     double2 rhoa;
     double norm, residu, tol;
     int itno, steperr, maxit, conv;
+    int atmax;  // TFQMR, GPBiCGAR: stopped past MAXIT, after the pass's last product
 };
 
 __device__ __forceinline__ double2 zmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
@@ -925,6 +926,7 @@ template <class T> struct ArStart {
         s.norm = sqrt(a[0].x);
         s.itno = 0;
         s.steperr = -1;
+        s.atmax = 0;
     }
 };
 
@@ -1036,8 +1038,11 @@ template <class T> struct ArBeta {
         if (s.itno <= s.maxit) {
             s.itno += 1;
         } else {
+            // past MAXIT (gpbicgar.f:360) after the pass's A r: one product
+            // more than a pass that converges at label 40
             status = 1;
             s.steperr = 0;
+            s.atmax = 1;
         }
     }
 };
@@ -1546,6 +1551,7 @@ template <class T> struct TStart {
         s.itno = 0;
         s.steperr = -1;
         s.conv = 0;
+        s.atmax = 0;
     }
 };
 
@@ -1672,8 +1678,11 @@ template <class T, bool ODD> struct TV {
         if (s.itno <= s.maxit) {
             s.itno += 1;
         } else {
+            // past MAXIT after the pass's A u (tfqmr.f:216): one product more
+            // than a pass that converges
             status = 1;
             s.steperr = 0;
+            s.atmax = 1;
         }
     }
 };

@@ -137,6 +137,29 @@ def test_gpbicg_iteration_limit_matches_oracle(gctx, orc):
     g.close()
 
 
+@pytest.mark.parametrize("meth", ["GPBICG1", "QMRBICGSTAB1", "QMRBICGSTAB2", "GPBICG2", "GPBICGsafe", "GPBICGplus",
+                                  "GPBICGAR", "BICGSTARPLUS", "TFQMR", "CG", "BICGSTAB", "GPBICOR", "CORS",
+                                  "QMRCLA"])
+def test_iteration_limit_every_method_matches_oracle(gctx, orc, meth):
+    """Each method stopped by an iteration limit of 3 at tol 1e-12 ends as
+    its branch of the reference's driver does: the current iterate with the
+    counters of the passes made (then cdmlib's "Converge do not reach!"), or
+    STATUS = -1 and "Problem to solve Ax=b!" (CG, BiCGSTAB, QMRCLA)."""
+    ob, k0, E0, ff0, G = _c1_inputs(orc)
+    ref = orc.inverserig(G, 16, 16, 16, ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-12, tabdip=ob.tabdip,
+                         nlim=3)
+    g = gctx.green(16, 16, 16, ob.aretecube, k0)
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-12, tabdip=ob.tabdip, maxit=3)
+    if ref["nstop"] == 0:
+        assert ref["tol1"] >= 1e-12
+        assert (r.nstop, r.infostr.strip()) == (1, "Converge do not reach!")
+        assert int(r.nloop[0]) == ref["nloop"] and int(r.ncompte[0]) == ref["ncompte"]
+        assert rel(r.FFloc, ref["FFloc"]) < 1e-9
+    else:
+        assert (r.nstop, r.infostr.strip()) == (ref["nstop"], ref["infostr"].strip())
+    g.close()
+
+
 def test_mixed_precision_meets_fp64_residual(gctx, orc):
     from ifdda import IFDDA_MIXED
     ob, k0, E0, ff0, G = _c1_inputs(orc)
