@@ -160,6 +160,47 @@ def test_iteration_limit_every_method_matches_oracle(gctx, orc, meth):
     g.close()
 
 
+@pytest.mark.parametrize("meth", ["GPBICG1", "QMRBICGSTAB1", "QMRBICGSTAB2", "GPBICG2", "GPBICGsafe", "GPBICGplus",
+                                  "GPBICGAR", "BICGSTARPLUS", "CG", "BICGSTAB", "GPBICOR", "CORS", "QMRCLA"])
+def test_zero_rhs_every_method_matches_oracle(gctx, orc, meth):
+    """FF0 = 0 makes every method break down at its first test (NORM = 0 or
+    a zero inner product): nstop = 1, "Problem to solve Ax=b!", the same
+    counters.  (TFQMR is left out: its stopping test divides by NORM and the
+    reference's loop never ends.)"""
+    ob, k0, E0, ff0, _ = _c1_inputs(orc, nnnr=8)
+    G = orc.greencalculfft(8, 8, 8, ob.aretecube, k0)
+    zero = np.zeros(3 * ob.nbsphere, dtype=np.complex128)
+    ref = orc.inverserig(G, 8, 8, 8, ob.nbsphere, ob.polarisa, ob.nmax, zero, meth, 1e-4, tabdip=ob.tabdip)
+    g = gctx.green(8, 8, 8, ob.aretecube, k0)
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, zero, meth, 1e-4, tabdip=ob.tabdip)
+    assert (r.nstop, r.infostr.strip()) == (ref["nstop"], ref["infostr"].strip()) == (1, "Problem to solve Ax=b!")
+    g.close()
+
+
+@pytest.mark.parametrize("meth", ["GPBICG2", "GPBICGsafe", "GPBICGplus", "GPBICGAR", "BICGSTARPLUS", "TFQMR", "CG",
+                                  "BICGSTAB", "QMRBICGSTAB2", "GPBICOR", "CORS"])
+def test_anisotropic_every_method_matches_oracle(gctx, orc, meth):
+    """The full-tensor mat-vec under each of the other methods (a
+    non-symmetric 3x3 polarisability per dipole): same counters, local field
+    within 1e-7."""
+    ob, k0, E0, ff0, G = _c1_inputs(orc, nnnr=10)
+    nb, nmax = ob.nbsphere, ob.nmax
+    pol = ob.polarisa.copy()
+    rng = np.random.default_rng(11)
+    for a in range(3):
+        for b in range(3):
+            pol[np.arange(nb) + nmax * (a + 3 * b)] += 0.1 * ob.alpha * (rng.standard_normal(nb) +
+                                                                       1j * rng.standard_normal(nb))
+    ref = orc.inverserig(G, 10, 10, 10, nb, pol, nmax, ff0, meth, 1e-6, tabdip=ob.tabdip)
+    assert ref["nstop"] == 0, ref["infostr"]
+    g = gctx.green(10, 10, 10, ob.aretecube, k0)
+    r = g.inverserig(nb, pol, nmax, ff0, meth, 1e-6, tabdip=ob.tabdip)
+    assert r.nstop == 0, r.infostr
+    assert int(r.nloop[0]) == ref["nloop"] and int(r.ncompte[0]) == ref["ncompte"]
+    assert rel(r.FFloc, ref["FFloc"]) < 1e-7
+    g.close()
+
+
 def test_mixed_precision_meets_fp64_residual(gctx, orc):
     from ifdda import IFDDA_MIXED
     ob, k0, E0, ff0, G = _c1_inputs(orc)
