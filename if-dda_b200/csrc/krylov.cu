@@ -71,9 +71,12 @@ struct NormOp {  // ||b|| of the outer problem, x = b
         x[o] = v;
         acc[0].x += v.x * v.x + v.y * v.y;
     }
-    __device__ void finish(int, KState& s, int&, const double2* a) const {
+    __device__ void finish(int, KState& s, int& status, const double2* a) const {
         s.norm = sqrt(a[0].x);
         s.itno = 0;
+        // b = 0: every method's first test fails on it (NORM = 0), so the
+        // right-hand side stops here instead of refining a 0/0 residual
+        if (s.norm == 0.0) status = -1;
     }
 };
 
@@ -773,7 +776,7 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
     IFDDA_CUDA(cudaStreamSynchronize(st));
     for (int r = 0; r < nrhs; r++) {
         SolveResult& o = res[r];
-        o.status = ost[r] ? 1 : 0;
+        o.status = ost[r] > 0 ? 1 : ost[r] < 0 ? -1 : 0;
         o.steperr = 0;
         o.cancelled = !ok;
         o.tol1 = hf[r].residu;

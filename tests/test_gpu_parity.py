@@ -177,6 +177,26 @@ def test_zero_rhs_every_method_matches_oracle(gctx, orc, meth):
     g.close()
 
 
+@pytest.mark.parametrize("prec", [0, 1])
+def test_zero_rhs_inside_a_batch(gctx, orc, prec):
+    """A zero right-hand side inside a batch stops at once ("Problem to solve
+    Ax=b!", the batch's nstop), and the others give what they give alone."""
+    ob, k0, E0, _, _ = _c1_inputs(orc, nnnr=10)
+    angles = [(0.0, 0.0, 1.0), (20.0, 10.0, 0.0), (35.0, 70.0, 1.0)]
+    ff0 = np.stack([orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, pp, 0, t, p) for t, p, pp in angles])
+    ff0[1] = 0
+    g = gctx.green(10, 10, 10, ob.aretecube, k0)
+    rb = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-5, tabdip=ob.tabdip, precision=prec)
+    assert rb.nstop == 1 and rb.infostr.strip() == "Problem to solve Ax=b!"
+    for q in (0, 2):
+        rs = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0[q], "GPBICG1", 1e-5, tabdip=ob.tabdip,
+                          precision=prec)
+        assert rs.nstop == 0
+        assert np.array_equal(rs.FFloc, rb.FFloc[q])
+        assert rs.nloop[0] == rb.nloop[q] and rs.ncompte[0] == rb.ncompte[q]
+    g.close()
+
+
 @pytest.mark.parametrize("meth", ["GPBICG2", "GPBICGsafe", "GPBICGplus", "GPBICGAR", "BICGSTARPLUS", "TFQMR", "CG",
                                   "BICGSTAB", "QMRBICGSTAB2", "GPBICOR", "CORS"])
 def test_anisotropic_every_method_matches_oracle(gctx, orc, meth):
