@@ -212,6 +212,36 @@ int solve_device(ifdda_green* g, int nrhs, int nb, int nmax, const int* tab_dev,
 }
 }  // namespace
 
+// Tabdip of a padded lattice (Green::padded): site (i, j, k) of the caller's
+// ux x uy x uz lattice maps to its dipole (src[site], or site + 1 for a full
+// box without src), the padding sites to none
+__global__ void k_pad_tab(const int* __restrict__ src, int* __restrict__ dst, int ux, int uy, int uz, int px, int py,
+                          long np) {
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < np; q += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(q % px);
+        const long r = q / px;
+        const int j = (int)(r % py), k = (int)(r / py);
+        int v = 0;
+        if (i < ux && j < uy && k < uz) {
+            const long s = i + (long)ux * (j + (long)uy * k);
+            v = src ? src[s] : (int)(s + 1);
+        }
+        dst[q] = v;
+    }
+}
+
+// The Tabdip the kernels use: src (device, caller's lattice, or null for a
+// full box) itself, or its padded form in g->ptab
+const int* lattice_tab(ifdda_green* g, const int* src, cudaStream_t st) {
+    if (!g->G.padded()) return src;
+    const long np = g->G.g.N;
+    count_launch();
+    k_pad_tab<<<(int)std::min<long>((np + 255) / 256, 148L * 16), 256, 0, st>>>(src, g->ptab.p, g->G.ux, g->G.uy,
+                                                                               g->G.uz, g->G.g.nx, g->G.g.ny, np);
+    IFDDA_CUDA(cudaGetLastError());
+    return g->ptab.p;
+}
+
 extern "C" {
 
 int ifdda_abi_version(void) { return IFDDA_GPU_ABI_VERSION; }
@@ -312,7 +342,8 @@ int ifdda_green_create_nquad(ifdda_ctx* ctx, int nx, int ny, int nz, double aret
     DeviceScope ds(ctx->device);
     AllocStreamScope as(ctx->stream);
     if (ctx->closing) throw EngineError{1, "context already destroyed"};
-    green_build(g->G, nx, ny, nz, aretecube, k0, ctx->stream, nquad);
+    green_build(g->G, nx, ny, nz, aretecube, k0, ctx->stream, nquad, /*pad=*/true);
+    if (g->G.padded()) g->ptab.ensure(g->G.g.N);
     *out = g.release();
     ctx->live_greens++;
     return 0;
@@ -368,6 +399,7 @@ int ifdda_green_export(ifdda_green* g, ifdda_dcmplx* xx, ifdda_dcmplx* xy, ifdda
     IFDDA_GUARD_BEGIN
     DeviceScope ds(g->ctx->device);
     AllocStreamScope as(g->ctx->stream);
+    if (g->G.padded()) throw EngineError{1, "export: the lattice was padded to compiled FFT lengths"};
     double2* out[6] = {(double2*)xx, (double2*)xy, (double2*)xz, (double2*)yy, (double2*)yz, (double2*)zz};
     green_export(g->G, out, g->ctx->stream);
     return 0;
@@ -381,16 +413,17 @@ int ifdda_matvec(ifdda_green* g, int precision, int ndip, const int* tabdip, con
     DeviceScope ds(g->ctx->device);
     AllocStreamScope as(g->ctx->stream);
     cudaStream_t st = g->ctx->stream;
-    const MvGeom& geo = g->G.g;
-    if (!tabdip && ndip != geo.N) throw EngineError{1, "ifdda_matvec: ndip must be nx*ny*nz without tabdip"};
+    const long uN = g->G.uN;
+    if (!tabdip && ndip != uN) throw EngineError{1, "ifdda_matvec: ndip must be nx*ny*nz without tabdip"};
     const long n3 = 3L * ndip;
     const int* tab = nullptr;
     if (tabdip) {
-        check_tabdip(tabdip, geo.N, ndip);
-        g->tab.ensure(geo.N);
-        IFDDA_CUDA(cudaMemcpyAsync(g->tab.p, tabdip, geo.N * sizeof(int), cudaMemcpyHostToDevice, st));
+        check_tabdip(tabdip, uN, ndip);
+        g->tab.ensure(uN);
+        IFDDA_CUDA(cudaMemcpyAsync(g->tab.p, tabdip, uN * sizeof(int), cudaMemcpyHostToDevice, st));
         tab = g->tab.p;
     }
+    tab = lattice_tab(g, tab, st);
     g->ffx.ensure(n3);
     g->ffb.ensure(n3);
     IFDDA_CUDA(cudaMemcpyAsync(g->ffx.p, FFX, n3 * sizeof(double2), cudaMemcpyHostToDevice, st));
@@ -425,8 +458,9 @@ int ifdda_matvec_device(ifdda_green* g, int precision, int nrhs, int ndip, const
     DeviceScope ds(g->ctx->device);
     AllocStreamScope as(g->ctx->stream);
     cudaStream_t st = g->ctx->stream;
-    if (!tabdip_dev && ndip != g->G.g.N) throw EngineError{1, "ifdda_matvec_device: ndip must be nx*ny*nz"};
+    if (!tabdip_dev && ndip != g->G.uN) throw EngineError{1, "ifdda_matvec_device: ndip must be nx*ny*nz"};
     const long n3 = 3L * ndip;
+    tabdip_dev = lattice_tab(g, tabdip_dev, st);
     bool ok;
     if (precision == IFDDA_FP32) {
         MvArgs<float> a = mv_args<float>(g->G, nrhs, (const float2*)FFX_dev, (const float2*)FFB_dev, (float2*)FFB_dev,
@@ -455,13 +489,13 @@ int ifdda_inverserig_batch(ifdda_green* g, int nrhs, int nbsphere, int nmax, con
     DeviceScope ds(g->ctx->device);
     AllocStreamScope as(g->ctx->stream);
     cudaStream_t st = g->ctx->stream;
-    const MvGeom& geo = g->G.g;
-    if (!tabdip && nbsphere != geo.N)
+    const long uN = g->G.uN;
+    if (!tabdip && nbsphere != uN)
         throw EngineError{1, "full-box solve: nbsphere must equal nx*ny*nz (or pass tabdip)"};
     if (nmax < nbsphere) throw EngineError{1, "nmax smaller than nbsphere"};
     const long n3 = 3L * nbsphere, tot = n3 * nrhs;
     const int* tab = nullptr;
-    if (tabdip) check_tabdip(tabdip, geo.N, nbsphere);
+    if (tabdip) check_tabdip(tabdip, uN, nbsphere);
     // the incident field goes first, so that its copy overlaps the host scan
     // of the polarisability below (when FF0 is pinned)
     g->ff0.ensure(tot);
@@ -469,10 +503,11 @@ int ifdda_inverserig_batch(ifdda_green* g, int nrhs, int nbsphere, int nmax, con
     g->ffb.ensure(tot);
     IFDDA_CUDA(cudaMemcpyAsync(g->ff0.p, FF0, tot * sizeof(double2), cudaMemcpyHostToDevice, st));
     if (tabdip) {
-        g->tab.ensure(geo.N);
-        IFDDA_CUDA(cudaMemcpyAsync(g->tab.p, tabdip, geo.N * sizeof(int), cudaMemcpyHostToDevice, st));
+        g->tab.ensure(uN);
+        IFDDA_CUDA(cudaMemcpyAsync(g->tab.p, tabdip, uN * sizeof(int), cudaMemcpyHostToDevice, st));
         tab = g->tab.p;
     }
+    tab = lattice_tab(g, tab, st);
     // Isotropy: the first dipoles are checked here (an anisotropic object is
     // almost always anisotropic there); if they are isotropic the solve starts
     // with one alpha per dipole while host threads scan the rest, and it is
@@ -540,10 +575,11 @@ int ifdda_inverserig_batch_device(ifdda_green* g, int nrhs, int nbsphere, int nm
     IFDDA_GUARD_BEGIN
     DeviceScope ds(g->ctx->device);
     AllocStreamScope as(g->ctx->stream);
-    if (!tabdip_dev && nbsphere != g->G.g.N)
+    if (!tabdip_dev && nbsphere != g->G.uN)
         throw EngineError{1, "full-box solve: nbsphere must equal nx*ny*nz (or pass tabdip)"};
     // isotropic tensors are compacted on the device (one alpha per dipole)
     cudaStream_t st = g->ctx->stream;
+    tabdip_dev = lattice_tab(g, tabdip_dev, st);
     g->alpha.ensure(nbsphere);
     IFDDA_CUDA(cudaMemsetAsync(g->ctx->flag.p, 0, sizeof(int), st));
     pola_compact_dev((const double2*)polarisa_dev, nbsphere, nmax, g->alpha.p, g->ctx->flag.p, st);
@@ -1073,8 +1109,8 @@ int ifdda_microscope(ifdda_green* g, int nbsphere, const int* tabdip, const doub
     DeviceScope ds(g->ctx->device);
     AllocStreamScope as(g->ctx->stream);
     cudaStream_t st = g->ctx->stream;
-    const MvGeom& geo = g->G.g;
-    const int nx = geo.nx, ny = geo.ny, nz = geo.nz, nmax = geo.N, N = nbsphere, n = mo->nfft2d;
+    // the caller's lattice (the solve maps it onto a padded one, if any)
+    const int nx = g->G.ux, ny = g->G.uy, nz = g->G.uz, nmax = (int)g->G.uN, N = nbsphere, n = mo->nfft2d;
     const bool quick = mo->nquicklens == 1;
     auto fail = [&](const char* msg) {
         if (nstop) *nstop = 1;
@@ -1233,6 +1269,7 @@ int ifdda_microscope(ifdda_green* g, int nbsphere, const int* tabdip, const doub
         dtab.ensure(nmax);
         IFDDA_CUDA(cudaMemcpyAsync(dtab.p, tabdip, nmax * sizeof(int), cudaMemcpyHostToDevice, st));
     }
+    const int* stab = lattice_tab(g, tabdip ? dtab.p : nullptr, st);
     int aniso = 0;
     IFDDA_CUDA(cudaMemcpyAsync(&aniso, g->ctx->flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     // z of each lattice plane (FFT lens, full box), the roots of unity of the
@@ -1284,8 +1321,8 @@ int ifdda_microscope(ifdda_green* g, int nbsphere, const int* tabdip, const doub
         IFDDA_CUDA(cudaMemcpyAsync(dik.p, ikv.data() + t0, nb * sizeof(int), cudaMemcpyHostToDevice, st));
         IFDDA_CUDA(cudaMemcpyAsync(djk.p, jkv.data() + t0, nb * sizeof(int), cudaMemcpyHostToDevice, st));
         planewaves_dev(N, dx.p, dy.p, dz.p, k0, E0, nb, dbeam.p, d1.p, d2.p, dpp.p, ff0.p, g->ctx->flag.p, st);
-        const int rc = solve_device(g, nb, N, nmax, tabdip ? dtab.p : nullptr, al, amode, ff0.p, methodeit, tol, ff.p,
-                                    loc.p, t1.data(), nl.data(), nc.data(), nstop, infostr, opt, false);
+        const int rc = solve_device(g, nb, N, nmax, stab, al, amode, ff0.p, methodeit, tol, ff.p, loc.p, t1.data(),
+                                    nl.data(), nc.data(), nstop, infostr, opt, false);
         if (tol1) *tol1 = t1[nb - 1];
         if (nloop) *nloop = nl[nb - 1];
         if (ncompte) *ncompte = nc[nb - 1];

@@ -26,6 +26,13 @@ struct ifdda_green {
     ifdda::SolverWork SW;
     // per-call device copies
     ifdda::DevBuf<int> tab;
+    // Tabdip of the padded box (G.padded()): allocated with the handle
+    ifdda::DevBuf<int> ptab;
     ifdda::DevBuf<double2> alpha, ff0, x, ffx, ffb;
     ifdda::DevBuf<float2> ffx32, ffb32, alpha32;
 };
+
+// The Tabdip the mat-vec kernels use for a lattice Tabdip src (device,
+// caller's lattice; null for a full box): src itself, or, when the handle's
+// lattice was padded to compiled FFT lengths, its padded form in g->ptab
+const int* lattice_tab(ifdda_green* g, const int* src, cudaStream_t st);

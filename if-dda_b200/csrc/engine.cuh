@@ -117,6 +117,11 @@ template <class T> struct MvWork {
 struct Green {
     int device = 0;
     MvGeom g{};
+    // the caller's lattice; g is larger where 2 nx, 2 ny or 2 nz is not a
+    // compiled FFT length, the lattice then sitting at the corner of g's
+    int ux = 0, uy = 0, uz = 0;
+    long uN = 0;
+    bool padded() const { return ux != g.nx || uy != g.ny || uz != g.nz; }
     double d = 0, k0 = 0;
     int nquad = 0;
     DevBuf<double2> gc64;
@@ -139,7 +144,11 @@ template <> inline MvWork<double>& Green::work<double>() { return w64; }
 MvGeom make_geom(int nx, int ny, int nz);
 // builds the spectrum (FP64, plus an FP32 copy) on `st`; throws EngineError
 // nquad > 0: the cube-averaged tensor at offsets within nquad (calculgreenquadfft.f)
-void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStream_t st, int nquad = 0);
+// pad: a lattice side n whose 2 n is not a compiled length is padded to the
+// smallest n' > n whose 2 n' is (the spectrum of the larger box holds the same
+// tensor at every offset between the caller's sites)
+void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStream_t st, int nquad = 0,
+                 bool pad = false);
 // full FFTTENSOR arrays (6 x 8N) on the host, expanded from the compressed octant
 void green_export(const Green& G, double2* const out[6], cudaStream_t st);
 

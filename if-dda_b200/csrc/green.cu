@@ -72,12 +72,28 @@ static void launch_gyz(const GreenGeom& gg, const double2* src, double2* d64, fl
     k_green_yz<L, AXIS><<<grid, TT::NT, TT::smem_y, st>>>(gg, src, d64, d32, tw);
 }
 
-void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStream_t st, int nquad) {
+// smallest n' >= n with 2 n' a compiled FFT length (n itself when none is)
+static int padded_side(int n) {
+    for (int m = n; m <= 4 * n && m <= 4096; m++)
+        if (fft_length_supported(2 * m)) return m;
+    return n;
+}
+
+void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStream_t st, int nquad, bool pad) {
     if (nx < 1 || ny < 1 || nz < 1) throw EngineError{1, "Green: lattice dimensions must be positive"};
     if (nquad < 0 || nquad > 16) throw EngineError{1, "Green: nquad must be in [0, 16]"};
+    G.ux = nx;
+    G.uy = ny;
+    G.uz = nz;
+    G.uN = (long)nx * ny * nz;
+    if (pad) {
+        nx = padded_side(nx);
+        ny = padded_side(ny);
+        nz = padded_side(nz);
+    }
     G.g = make_geom(nx, ny, nz);
     if (!fft_length_supported(G.g.X) || !fft_length_supported(G.g.Y) || !fft_length_supported(G.g.Z))
-        throw EngineError{1, "FFT size not supported: 2*nx, 2*ny and 2*nz must be compiled lengths"};
+        throw EngineError{1, "FFT size not supported: 2*nx, 2*ny and 2*nz must be compiled lengths (up to 384)"};
     G.d = d;
     G.k0 = k0;
     cudaGetDevice(&G.device);

@@ -86,8 +86,10 @@ extern "C" int ifdda_matvec_noalloc(ifdda_green* g, int precision, int ndip, con
             }
         } restore{ctx->device, prev};
         const ifdda::MvGeom& geo = g->G.g;
-        if (!tabdip_dev && ndip != geo.N)
+        if (!tabdip_dev && ndip != g->G.uN)
             throw ifdda::EngineError{1, "ifdda_matvec_noalloc: ndip must be nx*ny*nz without tabdip"};
+        // a padded lattice: its Tabdip goes to the buffer the handle holds
+        tabdip_dev = lattice_tab(g, tabdip_dev, ctx->stream);
         const size_t elem = precision == IFDDA_FP32 ? sizeof(float2) : sizeof(double2);
         const size_t need = (size_t)(geo.b1_rhs + geo.b2_rhs) * elem;
         if (need > IFDDA_NOALLOC_SCRATCH_BYTES)

@@ -58,7 +58,14 @@ void* ifdda_ctx_stream(ifdda_ctx* ctx);
 /* Green spectrum.  Replaces greencalculfft (cdmlib/calculgreenfft.f:1-104,
    called at cdmlib/cdmlib.f:1529-1531) with nquad = 0: the six components of
    the free-space dyadic on the (2nx,2ny,2nz) circulant grid, FFT sign +1.
-   aretecube in metres, k0 in 1/m.  The spectrum stays on the device. */
+   aretecube in metres, k0 in 1/m.  The spectrum stays on the device.
+   Every side from 1 to 192 is accepted, as the reference accepts any
+   (cdmlib/primefactor.f only warns).  2n in {2,4,6,8,10,12,16,20,24,32,40,
+   48,64,80,96,128,160,192,256,320,384} is computed as is; any other side n
+   is padded to the smallest n' > n with 2n' in that set.  The lattice then
+   sits at the corner of the larger box, and the mat-vecs and solves map the
+   caller's sites onto it.  The results are those of the caller's lattice, up
+   to the rounding of a longer FFT. */
 int ifdda_green_create(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, ifdda_green** out);
 /* The same with the integrated Green tensor (nquad = 1..16, 0 = plain):
    replaces greencalculquadfft (cdmlib/calculgreenquadfft.f, called at
@@ -74,7 +81,8 @@ int ifdda_green_destroy(ifdda_green* g);
    No counterpart in the reference. */
 int ifdda_green_release_workspace(ifdda_green* g);
 /* Writes the six FFTTENSOR arrays (xx,xy,xz,yy,yz,zz, 8*nx*ny*nz each, x
-   fastest) exactly as greencalculfft leaves them. */
+   fastest) exactly as greencalculfft leaves them.  Returns 1 for a padded
+   lattice, whose spectrum is on another grid. */
 int ifdda_green_export(ifdda_green* g, ifdda_dcmplx* xx, ifdda_dcmplx* xy, ifdda_dcmplx* xz, ifdda_dcmplx* yy,
                        ifdda_dcmplx* yz, ifdda_dcmplx* zz);
 

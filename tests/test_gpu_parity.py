@@ -177,6 +177,61 @@ def test_zero_rhs_every_method_matches_oracle(gctx, orc, meth):
     g.close()
 
 
+@pytest.mark.parametrize("dims", [(7, 5, 3), (15, 9, 11)])
+def test_padded_lattice_matvec_matches_oracle(gctx, orc, dims):
+    """A lattice side n whose 2n is not a compiled FFT length (14, 30, 18, 22
+    here) runs on the smallest larger compiled box, the lattice at its
+    corner: the mat-vec of the caller's lattice, full box and through a
+    Tabdip, matches the oracle's on the caller's own 2n grid."""
+    nx, ny, nz = dims
+    d, k0 = 10e-9, 2 * math.pi / 600e-9
+    G = orc.greencalculfft(nx, ny, nz, d, k0)
+    rng = np.random.default_rng(5)
+    N = nx * ny * nz
+    x = rng.standard_normal(3 * N) + 1j * rng.standard_normal(3 * N)
+    b = rng.standard_normal(3 * N) + 1j * rng.standard_normal(3 * N)
+    g = gctx.green(nx, ny, nz, d, k0)
+    assert rel(g.matvec(x, b), orc.matvec(G, nx, ny, nz, x, b)) < 1e-11
+    occ = rng.random(N) < 0.6
+    tab = np.zeros(N, np.int32)
+    tab[occ] = np.arange(1, occ.sum() + 1)
+    nd = int(occ.sum())
+    xt, bt = x[:3 * nd], b[:3 * nd]
+    assert rel(g.matvec(xt, bt, tabdip=tab), orc.matvec(G, nx, ny, nz, xt, bt, tabdip=tab)) < 1e-11
+    assert rel(g.matvec(x, b, precision=1), orc.matvec(G, nx, ny, nz, x, b)) < 2e-5
+    with pytest.raises(Exception, match="padded"):
+        g.export()
+    g.close()
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_padded_lattice_solve_matches_oracle(gctx, orc, prec):
+    """Solves on 15^3 lattices (2n = 30, not compiled): the sphere through
+    its Tabdip and the full-box GRF cube."""
+    ob, k0, E0, ff0, G = _c1_inputs(orc, nnnr=15)
+    ref = orc.inverserig(G, 15, 15, 15, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-6, tabdip=ob.tabdip)
+    g = gctx.green(15, 15, 15, ob.aretecube, k0)
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-6, tabdip=ob.tabdip, precision=prec)
+    assert r.nstop == ref["nstop"] == 0, r.infostr
+    if prec == 0:
+        assert int(r.nloop[0]) == ref["nloop"] and int(r.ncompte[0]) == ref["ncompte"]
+        assert rel(r.FFloc, ref["FFloc"]) < 1e-7
+    else:
+        assert r.tol1[0] < 1e-6 and rel(r.FFloc, ref["FFloc"]) < 1e-4
+    g.close()
+    ob, k0, ff0, G = _grf(orc, 15)
+    ref = orc.inverserig(G, 15, 15, 15, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "QMRBICGSTAB1", 1e-6)
+    g = gctx.green(15, 15, 15, ob.aretecube, k0)
+    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, "QMRBICGSTAB1", 1e-6, precision=prec)
+    assert r.nstop == ref["nstop"] == 0, r.infostr
+    if prec == 0:
+        assert int(r.nloop[0]) == ref["nloop"] and int(r.ncompte[0]) == ref["ncompte"]
+        assert rel(r.FFloc, ref["FFloc"]) < 1e-7
+    else:
+        assert r.tol1[0] < 1e-6 and rel(r.FFloc, ref["FFloc"]) < 1e-4
+    g.close()
+
+
 @pytest.mark.parametrize("prec", [0, 1])
 def test_zero_rhs_inside_a_batch(gctx, orc, prec):
     """A zero right-hand side inside a batch stops at once ("Problem to solve
@@ -295,8 +350,9 @@ def test_error_paths(gctx, orc):
     assert r.nstop == -1 and r.infostr.strip() == "Calculation cancelled during iterative method"
     # unsupported FFT length: 2*7 = 14 has no compiled kernel
     import ifdda
+    # a side above 192 has no compiled FFT length to pad to (2 n <= 384)
     with pytest.raises(ifdda.IfddaError):
-        gctx.green(7, 7, 7, 10e-9, k0)
+        gctx.green(193, 2, 2, 10e-9, k0)
     g.close()
 
 
