@@ -231,15 +231,18 @@ __global__ void k_pad_tab(const int* __restrict__ src, int* __restrict__ dst, in
 }
 
 // The Tabdip the kernels use: src (device, caller's lattice, or null for a
-// full box) itself, or its padded form in g->ptab
-const int* lattice_tab(ifdda_green* g, const int* src, cudaStream_t st) {
-    if (!g->G.padded()) return src;
-    const long np = g->G.g.N;
+// full box) itself, or its padded form in buf (G.g.N entries)
+static const int* lattice_tab(const Green& G, int* buf, const int* src, cudaStream_t st) {
+    if (!G.padded()) return src;
+    const long np = G.g.N;
     count_launch();
-    k_pad_tab<<<(int)std::min<long>((np + 255) / 256, 148L * 16), 256, 0, st>>>(src, g->ptab.p, g->G.ux, g->G.uy,
-                                                                               g->G.uz, g->G.g.nx, g->G.g.ny, np);
+    k_pad_tab<<<(int)std::min<long>((np + 255) / 256, 148L * 16), 256, 0, st>>>(src, buf, G.ux, G.uy, G.uz, G.g.nx,
+                                                                               G.g.ny, np);
     IFDDA_CUDA(cudaGetLastError());
-    return g->ptab.p;
+    return buf;
+}
+const int* lattice_tab(ifdda_green* g, const int* src, cudaStream_t st) {
+    return lattice_tab(g->G, g->ptab.p, src, st);
 }
 
 extern "C" {
@@ -950,9 +953,12 @@ int ifdda_nearfield_wide(ifdda_ctx* ctx, int nx, int ny, int nz, int nxmp, int n
     if (incident) IFDDA_CUDA(cudaMemcpyAsync(incident, xr.p, 3 * nw * sizeof(double2), cudaMemcpyDeviceToHost, st));
     // E = E0 + G p on the enlarged box: one FP64 mat-vec (cdmlib.f:2274-2277)
     Green G;
-    green_build(G, nxw, nyw, nzw, aretecube, k0, st, nquad);
-    MvArgs<double> a = mv_args<double>(G, 1, xi.p, xr.p, xr.p, 3 * nw, ALPHA_NONE, nullptr, 0, nullptr, nullptr);
-    if (!matvec_launch<double>(a, 1, false, st)) throw EngineError{1, "FFT size not supported"};
+    green_build(G, nxw, nyw, nzw, aretecube, k0, st, nquad, /*pad=*/true);
+    DevBuf<int> wtab;
+    if (G.padded()) wtab.ensure(G.g.N);
+    const int* tab = lattice_tab(G, wtab.p, nullptr, st);
+    MvArgs<double> a = mv_args<double>(G, 1, xi.p, xr.p, xr.p, 3 * nw, ALPHA_NONE, nullptr, 0, tab, nullptr);
+    if (!matvec_launch<double>(a, 1, tab != nullptr, st)) throw EngineError{1, "FFT size not supported"};
     if (local) IFDDA_CUDA(cudaMemcpyAsync(local, xr.p, 3 * nw * sizeof(double2), cudaMemcpyDeviceToHost, st));
     // macroscopic field with the object's permittivity (identity elsewhere)
     local_macro_dev((int)nw, nw, epsw.p, xr.p, aretecube, k0, em.p, ctx->flag.p, st);

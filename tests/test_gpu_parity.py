@@ -536,10 +536,11 @@ def test_solve_with_integrated_green_matches_oracle(gctx, orc):
     g.close()
 
 
-@pytest.mark.parametrize("nquad", [0, 1])
-def test_wide_near_field_matches_oracle(gctx, orc, nquad):
+@pytest.mark.parametrize("margins,nquad", [((4, 2, 4), 0), ((4, 2, 4), 1), ((3, 2, 5), 0)])
+def test_wide_near_field_matches_oracle(gctx, orc, margins, nquad):
     """ifdda_nearfield_wide against the oracle's restatement on the same
-    solved dipole moments (cdmlib.f:1967-2492)."""
+    solved dipole moments (cdmlib.f:1967-2492); margins (3, 2, 5) give a 14 x
+    12 x 18 box, whose 28 and 36 are padded to compiled lengths."""
     from ifdda import objects
     k0 = 2 * math.pi / 632.8e-9
     ob = objects.sphere(100e-9, 2.25 + 0.1j, 8, k0, "RR", na=0)
@@ -547,9 +548,10 @@ def test_wide_near_field_matches_oracle(gctx, orc, nquad):
     ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 0.3, 0, 30.0, 40.0)
     G = orc.greencalculfft(8, 8, 8, ob.aretecube, k0)
     sol = orc.inverserig(G, 8, 8, 8, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-8)
-    ref = orc.nearfield_wide(8, 8, 8, 4, 2, 4, ob.aretecube, k0, 632.8e-9, nquad, ob.nbsphere, ob.nmax, ob.xs,
+    mx, my, mz = margins
+    ref = orc.nearfield_wide(8, 8, 8, mx, my, mz, ob.aretecube, k0, 632.8e-9, nquad, ob.nbsphere, ob.nmax, ob.xs,
                              ob.ys, ob.zs, sol["FF"], ff0, ob.epsilon, E0, 30.0, 40.0, 0.3)
-    got = gctx.nearfield_wide(8, 8, 8, 4, 2, 4, ob.aretecube, k0, ob.xs, ob.ys, ob.zs, sol["FF"], ff0, ob.epsilon,
+    got = gctx.nearfield_wide(8, 8, 8, mx, my, mz, ob.aretecube, k0, ob.xs, ob.ys, ob.zs, sol["FF"], ff0, ob.epsilon,
                               ob.nmax, E0, 30.0, 40.0, 0.3, nquad=nquad)
     for key in ("xswf", "yswf", "zswf"):
         assert np.array_equal(got[key], ref[key]), key
