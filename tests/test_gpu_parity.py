@@ -177,12 +177,13 @@ def test_zero_rhs_every_method_matches_oracle(gctx, orc, meth):
     g.close()
 
 
-@pytest.mark.parametrize("dims", [(7, 5, 3), (15, 9, 11)])
+@pytest.mark.parametrize("dims", [(7, 5, 3), (15, 9, 11), (256, 2, 3), (200, 3, 2)])
 def test_padded_lattice_matvec_matches_oracle(gctx, orc, dims):
-    """A lattice side n whose 2n is not a compiled FFT length (14, 30, 18, 22
-    here) runs on the smallest larger compiled box, the lattice at its
+    """A lattice side n whose 2n is not a compiled FFT length (14, 30, 18, 22,
+    400 here) runs on the smallest larger compiled box, the lattice at its
     corner: the mat-vec of the caller's lattice, full box and through a
-    Tabdip, matches the oracle's on the caller's own 2n grid."""
+    Tabdip, matches the oracle's on the caller's own 2n grid (and 256 x 2 x 3
+    checks the length 512 itself)."""
     nx, ny, nz = dims
     d, k0 = 10e-9, 2 * math.pi / 600e-9
     G = orc.greencalculfft(nx, ny, nz, d, k0)
@@ -199,15 +200,17 @@ def test_padded_lattice_matvec_matches_oracle(gctx, orc, dims):
     xt, bt = x[:3 * nd], b[:3 * nd]
     assert rel(g.matvec(xt, bt, tabdip=tab), orc.matvec(G, nx, ny, nz, xt, bt, tabdip=tab)) < 1e-11
     assert rel(g.matvec(x, b, precision=1), orc.matvec(G, nx, ny, nz, x, b)) < 2e-5
-    with pytest.raises(Exception, match="padded"):
-        g.export()
+    compiled = {2, 4, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256, 320, 384, 512}
+    if any(2 * n not in compiled for n in dims):
+        with pytest.raises(Exception, match="padded"):
+            g.export()
     g.close()
 
 
 @pytest.mark.parametrize("prec", [0, 1])
 def test_padded_lattice_solve_matches_oracle(gctx, orc, prec):
-    """Solves on 15^3 lattices (2n = 30, not compiled): the sphere through
-    its Tabdip and the full-box GRF cube."""
+    """Solves on lattices whose 2n is not compiled: the 15^3 sphere through
+    its Tabdip, the full-box 15^3 GRF cube and a 200 x 3 x 2 GRF rod."""
     ob, k0, E0, ff0, G = _c1_inputs(orc, nnnr=15)
     ref = orc.inverserig(G, 15, 15, 15, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-6, tabdip=ob.tabdip)
     g = gctx.green(15, 15, 15, ob.aretecube, k0)
@@ -219,17 +222,23 @@ def test_padded_lattice_solve_matches_oracle(gctx, orc, prec):
     else:
         assert r.tol1[0] < 1e-6 and rel(r.FFloc, ref["FFloc"]) < 1e-4
     g.close()
-    ob, k0, ff0, G = _grf(orc, 15)
-    ref = orc.inverserig(G, 15, 15, 15, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "QMRBICGSTAB1", 1e-6)
-    g = gctx.green(15, 15, 15, ob.aretecube, k0)
-    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, "QMRBICGSTAB1", 1e-6, precision=prec)
-    assert r.nstop == ref["nstop"] == 0, r.infostr
-    if prec == 0:
-        assert int(r.nloop[0]) == ref["nloop"] and int(r.ncompte[0]) == ref["ncompte"]
-        assert rel(r.FFloc, ref["FFloc"]) < 1e-7
-    else:
-        assert r.tol1[0] < 1e-6 and rel(r.FFloc, ref["FFloc"]) < 1e-4
-    g.close()
+    from ifdda import objects
+    # the GRF cube, and a 200 x 3 x 2 GRF rod (its 400 runs on 512)
+    for dims, meth in (((15, 15, 15), "QMRBICGSTAB1"), ((200, 3, 2), "GPBICG1")):
+        ob = objects.inhomocuboid(*dims, 10e-9, 2.25 + 0j, 50e-9, 0.1, 7, k0, "RR")
+        E0, _ = objects.irradiance(1.0, 10 * 632.8e-9)
+        ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, 1.0, 0, 20.0, 0.0)
+        G = orc.greencalculfft(*dims, ob.aretecube, k0)
+        ref = orc.inverserig(G, *dims, ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-6)
+        g = gctx.green(*dims, ob.aretecube, k0)
+        r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, meth, 1e-6, precision=prec)
+        assert r.nstop == ref["nstop"] == 0, r.infostr
+        if prec == 0:
+            assert int(r.nloop[0]) == ref["nloop"] and int(r.ncompte[0]) == ref["ncompte"]
+            assert rel(r.FFloc, ref["FFloc"]) < 1e-7
+        else:
+            assert r.tol1[0] < 1e-6 and rel(r.FFloc, ref["FFloc"]) < 1e-4
+        g.close()
 
 
 @pytest.mark.parametrize("prec", [0, 1])
@@ -350,9 +359,9 @@ def test_error_paths(gctx, orc):
     assert r.nstop == -1 and r.infostr.strip() == "Calculation cancelled during iterative method"
     # unsupported FFT length: 2*7 = 14 has no compiled kernel
     import ifdda
-    # a side above 192 has no compiled FFT length to pad to (2 n <= 384)
+    # a side above 256 has no compiled FFT length to pad to (2 n <= 512)
     with pytest.raises(ifdda.IfddaError):
-        gctx.green(193, 2, 2, 10e-9, k0)
+        gctx.green(257, 2, 2, 10e-9, k0)
     g.close()
 
 
