@@ -52,6 +52,21 @@ def test_microscope_matches_oracle(gctx, orc, ntypemic, nfft2d, nside):
     g.close()
 
 
+def test_microscope_on_a_padded_lattice_matches_oracle(gctx, orc):
+    """A 7^3 full-box sphere: 2 x 7 = 14 is not a compiled FFT length, so the
+    solves run on the 8^3 box through a padded Tabdip while the FFT lens
+    reads the caller's 7^3 lattice."""
+    ob, k0 = _object(nnnr=7)
+    G = orc.greencalculfft(7, 7, 7, ob.aretecube, k0)
+    ref = orc.microscope(1, G, 7, 7, 7, ob.aretecube, k0, ob.xs, ob.ys, ob.zs, ob.polarisa, "GPBICG1", 1e-6,
+                         0.9, 0.5, 64, 100.0, 50e-9, 1.0, 6328e-9)
+    g = gctx.green(7, 7, 7, ob.aretecube, k0)
+    r = g.microscope(ob.xs, ob.ys, ob.zs, ob.polarisa, "GPBICG1", 1e-6, ntypemic=1, nfft2d=64, numaper=0.9,
+                     numaperinc=0.5, gross=100.0, zlens=50e-9, P0=1.0, w0=6328e-9)
+    _compare(r, ref)
+    g.close()
+
+
 @pytest.mark.parametrize("ntypemic,nside,inside", [(1, 0, True), (2, 0, False), (1, 1, True)])
 def test_microscope_direct_lens_matches_oracle(gctx, orc, ntypemic, nside, inside):
     """nquicklens = 0: the lens's far field by direct summation over the
