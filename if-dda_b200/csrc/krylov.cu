@@ -423,15 +423,28 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
         if (!sp.zero_guess) mv_solver<T>(G, sp, W, Q_X, Q_XR, status, st);
         vec_launch<1>(QInit<T>{V, S}, n3, nblk, nrhs, rs, status, st);
     }
-    // the first two iterations run as plain launches (they also set the
-    // kernels' shared-memory limits before any capture)
+    const bool graphs = sp.use_graphs && !timing_active();
+    // the buffers and shapes a captured loop is bound to
+    std::vector<const void*> key;
+    if (graphs) {
+        MvWork<T>& mw = G.work<T>();
+        mw.ensure(G.g, nrhs);
+        W.loopcount.ensure(1);
+        key = {V.base, sp.alpha, sp.tabdip, G.gc<T>(), mw.B1.p, mw.B2.p, W.partials.p, W.tickets.p, status, S,
+               W.mvpart.p, W.mvtk.p, W.loopcount.p, (const void*)(long)fused,
+               (const void*)(long)sp.method, (const void*)(long)nrhs, (const void*)n3, (const void*)(long)sp.amode,
+               (const void*)sp.nmax, (const void*)(long)nblk};
+    }
+    const bool cached = graphs && W.graph.exec && W.graph.key == key;
+    // without a loop captured for these buffers, the first two iterations run
+    // as plain launches (they also set the kernels' shared-memory limits
+    // before any capture); with one, the device-side loop starts at once
     long it = 0;
     bool done = false;
-    for (; it < 2 && !done; it++) {
+    for (; it < 2 && !done && !cached; it++) {
         iteration((int)(it & 1));
         done = poll(W, sp, st, cancelled);
     }
-    const bool graphs = sp.use_graphs && !timing_active();
     // Builds the device-side loop: [clear counter] -> while(cond) { two
     // iterations; k_loop_ctl }.  Returns false (nothing kept) if the driver
     // cannot build it; the caller then replays plain two-iteration graphs.
@@ -496,15 +509,7 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
         return true;
     };
     if (!done && graphs) {
-        MvWork<T>& mw = G.work<T>();
-        mw.ensure(G.g, nrhs);
-        W.loopcount.ensure(1);
-        const std::vector<const void*> key = {
-            V.base, sp.alpha, sp.tabdip, G.gc<T>(), mw.B1.p, mw.B2.p, W.partials.p, W.tickets.p, status, S,
-            W.mvpart.p, W.mvtk.p, W.loopcount.p, (const void*)(long)fused,
-            (const void*)(long)sp.method, (const void*)(long)nrhs, (const void*)n3, (const void*)(long)sp.amode,
-            (const void*)sp.nmax, (const void*)(long)nblk};
-        if (!W.graph.exec || W.graph.key != key) {
+        if (!cached) {
             W.graph.reset();
             if (build_loop()) {
                 W.graph.key = key;
