@@ -60,6 +60,23 @@ struct ResidualOp {
     }
 };
 
+// Fresh solver state for nrhs right-hand sides, set on the device: a copy
+// from pageable host memory would wait for the stream first
+__global__ void k_init_state(KState* __restrict__ s, int* __restrict__ status, int nrhs, double tol, int maxit) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrhs) return;
+    KState k{};
+    k.tol = tol;
+    k.maxit = maxit;
+    s[r] = k;
+    if (status) status[r] = 0;
+}
+static void init_state(KState* s, int* status, int nrhs, double tol, int maxit, cudaStream_t st) {
+    count_launch();
+    k_init_state<<<(nrhs + 127) / 128, 128, 0, st>>>(s, status, nrhs, tol, maxit);
+    IFDDA_CUDA(cudaGetLastError());
+}
+
 struct NormOp {  // ||b|| of the outer problem, x = b
     const double2* b;
     double2* x;
@@ -238,16 +255,7 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
     const long n3 = W.n3;
     const int nrhs = W.nrhs, nblk = W.nblk;
     RedSlots rs{W.partials.p, W.tickets.p, nblk};
-    if (!sp.preset_state) {
-        std::vector<KState> h(nrhs);
-        for (auto& s : h) {
-            s = KState{};
-            s.tol = sp.tol;
-            s.maxit = sp.maxit;
-        }
-        IFDDA_CUDA(cudaMemcpyAsync(W.st.p, h.data(), nrhs * sizeof(KState), cudaMemcpyHostToDevice, st));
-        IFDDA_CUDA(cudaMemsetAsync(W.status.p, 0, nrhs * sizeof(int), st));
-    }
+    if (!sp.preset_state) init_state(W.st.p, W.status.p, nrhs, sp.tol, sp.maxit, st);
     IFDDA_CUDA(cudaMemsetAsync(W.tickets.p, 0, nrhs * sizeof(unsigned), st));
     int* status = W.status.p;
     KState* S = W.st.p;
@@ -643,16 +651,19 @@ void solve_fp64(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b_
     IFDDA_CUDA(cudaMemcpyAsync(V.v(bs, 0), b_dev, tot * sizeof(double2), cudaMemcpyDeviceToDevice, st));
     const bool ok = krylov_run<double>(G, sp, W, st);
     res.assign(sp.nrhs, SolveResult{});
-    std::vector<KState> hs(sp.nrhs);
-    IFDDA_CUDA(cudaMemcpyAsync(hs.data(), W.st.p, sp.nrhs * sizeof(KState), cudaMemcpyDeviceToHost, st));
-    IFDDA_CUDA(cudaMemcpyAsync(W.hstatus.data(), W.status.p, sp.nrhs * sizeof(int), cudaMemcpyDeviceToHost, st));
-    IFDDA_CUDA(cudaStreamSynchronize(st));
-    // BiCGSTAB's soft breakdown returns x = p (cdmlib/pimzbicgstab.f:145-156)
-    if (sp.method == 4)
+    // W.hstatus holds the statuses the loop's last poll read; they do not
+    // change after it.  BiCGSTAB's soft breakdown returns x = p
+    // (cdmlib/pimzbicgstab.f:145-156), which needs the state now; the other
+    // methods read it once, with tol1, below.
+    if (sp.method == 4) {
+        std::vector<KState> hs(sp.nrhs);
+        IFDDA_CUDA(cudaMemcpyAsync(hs.data(), W.st.p, sp.nrhs * sizeof(KState), cudaMemcpyDeviceToHost, st));
+        IFDDA_CUDA(cudaStreamSynchronize(st));
         for (int r = 0; r < sp.nrhs; r++)
             if (W.hstatus[r] < 0 && hs[r].steperr == 12)
                 IFDDA_CUDA(cudaMemcpyAsync(V.v(B_X, r), V.v(B_P, r), sp.n3 * sizeof(double2), cudaMemcpyDeviceToDevice,
                                            st));
+    }
     // final A x and true residual, for every right-hand side that did not break down
     IFDDA_CUDA(cudaMemsetAsync(W.zstatus.p, 0, sp.nrhs * sizeof(int), st));
     {
@@ -670,10 +681,10 @@ void solve_fp64(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b_
     for (int r = 0; r < sp.nrhs; r++) {
         SolveResult& o = res[r];
         o.status = W.hstatus[r];
-        o.steperr = hs[r].steperr;
+        o.steperr = hf[r].steperr;  // TrueResOp sets residu only
         o.cancelled = !ok;
         o.tol1 = hf[r].residu;
-        method_counts(sp.method, hs[r].itno, o.nloop, o.ncompte, hs[r].atmax != 0);
+        method_counts(sp.method, hf[r].itno, o.nloop, o.ncompte, hf[r].atmax != 0);
         o.ncompte64 = o.ncompte;
         o.outer = 0;
     }
@@ -702,23 +713,10 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
         const long na = sp.amode == ALPHA_FULL ? 9 * sp.nmax : sp.nmax;
         cast_dev<float>((const double2*)sp.alpha, M.alpha32.p, na, st);
     }
-    std::vector<KState> ho(nrhs);
-    for (auto& s : ho) {
-        s = KState{};
-        s.tol = sp.tol;
-        s.maxit = sp.maxit;
-    }
-    IFDDA_CUDA(cudaMemcpyAsync(M.ost.p, ho.data(), nrhs * sizeof(KState), cudaMemcpyHostToDevice, st));
-    IFDDA_CUDA(cudaMemsetAsync(M.ostatus.p, 0, nrhs * sizeof(int), st));
+    init_state(M.ost.p, M.ostatus.p, nrhs, sp.tol, sp.maxit, st);
     IFDDA_CUDA(cudaMemsetAsync(M.tickets.p, 0, nrhs * sizeof(unsigned), st));
     // inner state defaults
-    std::vector<KState> hi(nrhs);
-    for (auto& s : hi) {
-        s = KState{};
-        s.tol = sp.tol;
-        s.maxit = sp.maxit;
-    }
-    IFDDA_CUDA(cudaMemcpyAsync(W.st.p, hi.data(), nrhs * sizeof(KState), cudaMemcpyHostToDevice, st));
+    init_state(W.st.p, nullptr, nrhs, sp.tol, sp.maxit, st);
     vec_launch<1>(NormOp{b_dev, M.x.p, n3, M.ost.p}, n3, nblk, nrhs, rs, M.ostatus.p, st);
     Slots<float> V = W.slots();
     const int bs = W.b_slot(sp.method), xs = W.x_slot(sp.method);
