@@ -145,11 +145,13 @@ SolveSpec make_spec(int method, int nrhs, int nb, double tol, const ifdda_solve_
 
 // Runs a (batched) solve whose inputs are already on the device.
 // check_tol: report tol1 >= tol as "Converge do not reach!" (cdmlib.f:1586-1591;
-// the microscopes call the solver without that check).
+// the microscopes call the solver without that check).  sync_out: return with
+// FF computed; a caller that next copies the outputs on the same stream and
+// waits there passes false.
 int solve_device(ifdda_green* g, int nrhs, int nb, int nmax, const int* tab_dev, const double2* alpha_dev, int amode,
                  const double2* ff0_dev, const char* methodeit, double tol, double2* ff_dev, double2* loc_dev,
                  double* tol1, int* nloop, int* ncompte, int* nstop, char* infostr, const ifdda_solve_options* opt,
-                 bool check_tol = true) {
+                 bool check_tol = true, bool sync_out = true) {
     ifdda_ctx* ctx = g->ctx;
     const int method = method_code(methodeit);
     if (method == 0) {
@@ -184,7 +186,7 @@ int solve_device(ifdda_green* g, int nrhs, int nb, int nmax, const int* tab_dev,
     else solve_fp64(g->G, g->SW, sp, ff0_dev, loc_dev, res, ctx->stream);
     // FF = polarisa . E (cdmlib/inverserigopt.f:92-97)
     apply_alpha_dev(loc_dev, ff_dev, nb, nrhs, 3L * nb, amode, alpha_dev, sp.nmax, ctx->stream);
-    IFDDA_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (sync_out) IFDDA_CUDA(cudaStreamSynchronize(ctx->stream));
     int rc = 0;
     const char* msg = nullptr;
     for (int r = 0; r < nrhs; r++) {
@@ -542,13 +544,14 @@ int ifdda_inverserig_batch(ifdda_green* g, int nrhs, int nbsphere, int nmax, con
         }
     };
     upload_alpha(amode);
+    // the outputs are copied and waited for below, on the same stream
     int rc = solve_device(g, nrhs, nbsphere, nmax, tab, g->alpha.p, amode, g->ff0.p, methodeit, tol, g->ffb.p, g->x.p,
-                          tol1, nloop, ncompte, nstop, infostr, opt);
+                          tol1, nloop, ncompte, nstop, infostr, opt, true, false);
     if (scan.joinable()) scan.join();
     if (amode == ALPHA_ISO && tail.load() == ALPHA_FULL && rc != -1) {
         upload_alpha(ALPHA_FULL);
         rc = solve_device(g, nrhs, nbsphere, nmax, tab, g->alpha.p, ALPHA_FULL, g->ff0.p, methodeit, tol, g->ffb.p,
-                          g->x.p, tol1, nloop, ncompte, nstop, infostr, opt);
+                          g->x.p, tol1, nloop, ncompte, nstop, infostr, opt, true, false);
     }
     IFDDA_CUDA(cudaMemcpyAsync(FFloc, g->x.p, tot * sizeof(double2), cudaMemcpyDeviceToHost, st));
     IFDDA_CUDA(cudaMemcpyAsync(FF, g->ffb.p, tot * sizeof(double2), cudaMemcpyDeviceToHost, st));
