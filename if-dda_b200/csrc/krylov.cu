@@ -729,6 +729,27 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
     std::vector<long> inner_iters(nrhs, 0), inner_mv(nrhs, 0), outer_mv(nrhs, 0), inner_runs(nrhs, 0);
     bool ok = true;
     int outer = 0;
+    // The inner solve's counters are read with the next outer status (one
+    // wait instead of two): the residual step that runs between them changes
+    // only the inner tol and maxit.  mask: the outer status before that solve.
+    std::vector<KState> hs(nrhs);
+    std::vector<int> mask(nrhs, 0);
+    bool pending = false;
+    auto account = [&]() {
+        for (int r = 0; r < nrhs; r++) {
+            if (mask[r]) continue;
+            int its = 0, mvs = 0;
+            method_counts(sp.method, hs[r].itno, its, mvs, hs[r].atmax != 0);
+            inner_iters[r] += its;
+            // zero initial guess: no A x0 (QMRCLA still forms A^T r0)
+            if (sp.method == 5 || sp.method == 6) inner_mv[r] += its + 1;
+            else if (sp.method == 14) inner_mv[r] += 2 * its + 1;
+            else inner_mv[r] += 2 * its;
+            if (hs[r].atmax && (sp.method == 6 || sp.method == 10)) inner_mv[r] += 1;
+            inner_runs[r] += 1;
+        }
+        pending = false;
+    };
     for (;; outer++) {
         MvArgs<double> a = mv_args<double>(G, nrhs, M.x.p, M.x.p, M.ax.p, n3, sp.amode, (const double2*)sp.alpha,
                                            sp.nmax, sp.tabdip, M.ostatus.p);
@@ -737,7 +758,10 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
         vec_launch<1>(ResidualOp{b_dev, M.ax.p, V.v(bs, 0), n3, M.ost.p, W.st.p, W.status.p, sp.inner_floor}, n3,
                       nblk, nrhs, rs, M.ostatus.p, st);
         IFDDA_CUDA(cudaMemcpyAsync(ost.data(), M.ostatus.p, nrhs * sizeof(int), cudaMemcpyDeviceToHost, st));
+        if (pending)
+            IFDDA_CUDA(cudaMemcpyAsync(hs.data(), W.st.p, nrhs * sizeof(KState), cudaMemcpyDeviceToHost, st));
         IFDDA_CUDA(cudaStreamSynchronize(st));
+        if (pending) account();
         bool all = true;
         for (int r = 0; r < nrhs; r++) {
             if (!done_before[r]) outer_mv[r]++;
@@ -754,24 +778,16 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
             ok = false;
             break;
         }
-        std::vector<KState> hs(nrhs);
-        IFDDA_CUDA(cudaMemcpyAsync(hs.data(), W.st.p, nrhs * sizeof(KState), cudaMemcpyDeviceToHost, st));
-        IFDDA_CUDA(cudaStreamSynchronize(st));
-        for (int r = 0; r < nrhs; r++) {
-            if (ost[r]) continue;
-            int its = 0, mvs = 0;
-            method_counts(sp.method, hs[r].itno, its, mvs, hs[r].atmax != 0);
-            inner_iters[r] += its;
-            // zero initial guess: no A x0 (QMRCLA still forms A^T r0)
-            if (sp.method == 5 || sp.method == 6) inner_mv[r] += its + 1;
-            else if (sp.method == 14) inner_mv[r] += 2 * its + 1;
-            else inner_mv[r] += 2 * its;
-            if (hs[r].atmax && (sp.method == 6 || sp.method == 10)) inner_mv[r] += 1;
-            inner_runs[r] += 1;
-        }
+        mask = ost;
+        pending = true;
         count_launch();
         k_axpy_outer<float><<<grid_for(tot), 256, 0, st>>>(M.x.p, V.v(xs, 0), n3, nrhs, M.ostatus.p);
         IFDDA_CUDA(cudaGetLastError());
+    }
+    if (pending) {
+        IFDDA_CUDA(cudaMemcpyAsync(hs.data(), W.st.p, nrhs * sizeof(KState), cudaMemcpyDeviceToHost, st));
+        IFDDA_CUDA(cudaStreamSynchronize(st));
+        account();
     }
     std::vector<KState> hf(nrhs);
     IFDDA_CUDA(cudaMemcpyAsync(hf.data(), M.ost.p, nrhs * sizeof(KState), cudaMemcpyDeviceToHost, st));
