@@ -998,7 +998,7 @@ int ifdda_holography(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, d
     if (nside != 0 && nside != 1) return fail("nside must be 0 (transmission) or 1 (reflection)");
     if (nquicklens != 0 && nquicklens != 1) return fail("nquicklens must be 0 or 1");
     if (quick && nbsphere != N) return fail("the FFT lens needs the full box (nbsphere = nx*ny*nz)");
-    if (!image_length_supported(n)) return fail("nfft2d not supported: a power of two from 32 to 4096");
+    if (!image_length_supported(n)) return fail("nfft2d not supported: 32 to 4096, a power of two or 768, 1536, 3072");
     if (nx > n || ny > n) return fail("nfft2d smaller than the object");
     const double pi = 3.14159265358979323846, dside = nside == 1 ? -1.0 : 1.0;
     const double na = numaper * k0;
@@ -1135,7 +1135,7 @@ int ifdda_microscope(ifdda_green* g, int nbsphere, const int* tabdip, const doub
     if (mo->nside != 0 && mo->nside != 1) return fail("nside must be 0 (transmission) or 1 (reflection)");
     // cdmlib.f:237-238, 389: the side's sign of kz, carried by zlens too
     const double dside = mo->nside == 1 ? -1.0 : 1.0;
-    if (!image_length_supported(n)) return fail("nfft2d not supported: a power of two from 32 to 4096");
+    if (!image_length_supported(n)) return fail("nfft2d not supported: 32 to 4096, a power of two or 768, 1536, 3072");
     if (nx > n || ny > n) return fail("nfft2d smaller than the object");
     const double pi = 3.14159265358979323846;
     const double k0 = g->G.k0, d = g->G.d;

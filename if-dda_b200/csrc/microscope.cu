@@ -341,8 +341,10 @@ __global__ void __launch_bounds__(256) k_mic_lens(const MicGeom m, int nb, const
 
 template <int L> struct ImgTiles {
     static constexpr int NT = 256;
-    // lines per block: 4096 points of shared memory (64 KB), at most 32 lines
-    static constexpr int NB = (4096 / L) > 32 ? 32 : (4096 / L) < 1 ? 1 : 4096 / L;
+    // lines per block: about 4096 points of shared memory (64 KB), at most 32
+    // lines, a power of two so that it divides every compiled L
+    static constexpr int NB = clamp_pow2(4096 / L, 1, 32);
+    static_assert(L % NB == 0, "column blocks must tile the image");
     static constexpr size_t smem = (size_t)(NB * L + L) * sizeof(double2);
 };
 

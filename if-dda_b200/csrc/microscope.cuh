@@ -6,8 +6,10 @@
 #pragma once
 #include "engine.cuh"
 
-// image sides n (nfft2d) the lens transforms are compiled for
-#define IFDDA_IMG_LENGTHS(X) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
+// image sides n (nfft2d) the lens transforms are compiled for: the powers of
+// two and the reference's option list up to 4096 (cdm/cdmOptions.cpp:35 also
+// offers 768, 1536, 3072)
+#define IFDDA_IMG_LENGTHS(X) X(32) X(64) X(128) X(256) X(512) X(768) X(1024) X(1536) X(2048) X(3072) X(4096)
 
 namespace ifdda {
 

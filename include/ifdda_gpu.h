@@ -232,7 +232,8 @@ int ifdda_nearfield_wide(ifdda_ctx* ctx, int nx, int ny, int nz, int nxmp, int n
    (cdmlib/cdmlib.f:3660-3800 with nlentille = 1, nquicklens = 1). */
 typedef struct {
     int ntypemic;      /* 1 bright field (microsbf.f), 2 dark field and phase (microsdf.f) */
-    int nfft2d;        /* side n of the pupil and image grids: a power of two from 32 to 4096 */
+    int nfft2d;        /* side n of the pupil and image grids: a power of two from 32 to
+                          4096, or 768, 1536, 3072 (the reference's list up to 4096) */
     double numaper;    /* numerical aperture of the objective, (0, 1] */
     double numaperinc; /* numerical aperture of the condenser, < 1 */
     double gross;      /* magnification */
@@ -289,7 +290,7 @@ int ifdda_microscope(ifdda_green* g, int nbsphere, const int* tabdip, const doub
    then Eimageincx..z, zero on the reflection side), pixel u + n v; fourier
    (may be NULL): the pupil fields Efourierx..z, Efourierincx..z before the
    rotation, 6 x (2 imaxk0 + 1)^2, row j, column i; xy, kxy (n values, may be
-   NULL).  nfft2d: a power of two from 32 to 4096.  Returns 1 with the
+   NULL).  nfft2d: a power of two from 32 to 4096, or 768, 1536, 3072.  Returns 1 with the
    reference's message on an error. */
 int ifdda_holography(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, int nbsphere,
                      const double* xs, const double* ys, const double* zs, const ifdda_dcmplx* FF, ifdda_dcmplx E0,

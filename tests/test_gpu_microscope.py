@@ -33,7 +33,8 @@ def _compare(r, ref, tol=1e-8):
         assert rel(r.image[c], ref["image"][c]) < tol, c
 
 
-@pytest.mark.parametrize("ntypemic,nfft2d,nside", [(1, 64, 0), (1, 128, 0), (2, 64, 0), (1, 64, 1), (2, 64, 1)])
+@pytest.mark.parametrize("ntypemic,nfft2d,nside", [(1, 64, 0), (1, 128, 0), (2, 64, 0), (1, 64, 1), (2, 64, 1),
+                                                  (1, 768, 0)])
 def test_microscope_matches_oracle(gctx, orc, ntypemic, nfft2d, nside):
     ob, k0 = _object()
     G = orc.greencalculfft(8, 8, 8, ob.aretecube, k0)
@@ -137,7 +138,7 @@ def test_cdmlib_microscope_matches_oracle(orc):
         assert rel(out[name], ref["image"][c]) < 1e-8, name
 
 
-@pytest.mark.parametrize("nside,nfft2d", [(0, 64), (1, 64), (0, 128)])
+@pytest.mark.parametrize("nside,nfft2d", [(0, 64), (1, 64), (0, 128), (0, 768)])
 def test_holography_matches_oracle(gctx, orc, nside, nfft2d):
     """ntypemic = 0 (cdmlib.f:4075-4660): the complex image fields of one
     oblique plane-wave solve, and the pupil fields, against the oracle's
