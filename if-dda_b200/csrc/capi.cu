@@ -275,7 +275,7 @@ int ifdda_ctx_create(int device, ifdda_ctx** out) {
         c->tickets.ensure(1);
         IFDDA_CUDA(cudaMemset(c->zstatus.p, 0, sizeof(int)));
         IFDDA_CUDA(cudaMemset(c->tickets.p, 0, sizeof(unsigned)));
-        c->partials.ensure(1024 * 4);
+        c->partials.ensure(2048 * 8);  // reduction_blocks() partials of up to 8 sums
     } catch (const EngineError& e) {
         delete c;
         return 1;

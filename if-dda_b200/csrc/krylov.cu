@@ -150,7 +150,7 @@ template void cast_dev<float>(const double2*, float2*, long, cudaStream_t);
 template void cast_dev<double>(const double2*, double2*, long, cudaStream_t);
 
 // ------------------------------------------------------------- solver ----
-int reduction_blocks(long n3) { return (int)std::max<long>(1, std::min<long>((n3 + KNT * 4 - 1) / (KNT * 4), 1024)); }
+int reduction_blocks(long n3) { return (int)std::max<long>(1, std::min<long>((n3 + KNT * 2 - 1) / (KNT * 2), 2048)); }
 
 template <class T> void KrylovWork<T>::ensure(int method, int nrhs_, long n3_) {
     static const int nslots[] = {0,       G_NSLOT, Q_NSLOT, 0,       B_NSLOT, C_NSLOT, T_NSLOT,
