@@ -13,12 +13,12 @@
 
 // FFT lengths (padded grid edges 2n) with compiled kernels.  A lattice edge n
 // whose 2n is not in this list runs on the smallest larger edge whose 2n is
-// (green_build's pad), so every edge up to 256 is accepted, as the
+// (green_build's pad), so every edge up to 320 is accepted, as the
 // reference's own FFT accepts any length, warning above prime factor 5
 // (cdmlib/primefactor.f).
 #define IFDDA_FFT_LENGTHS(X) \
     X(2) X(4) X(6) X(8) X(10) X(12) X(16) X(20) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(160) X(192) X(256) X(320) X(384) \
-        X(512)
+        X(512) X(640)
 
 namespace ifdda {
 

@@ -93,7 +93,7 @@ void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStre
     }
     G.g = make_geom(nx, ny, nz);
     if (!fft_length_supported(G.g.X) || !fft_length_supported(G.g.Y) || !fft_length_supported(G.g.Z))
-        throw EngineError{1, "FFT size not supported: lattice sides above 256 (2*n above 512)"};
+        throw EngineError{1, "FFT size not supported: lattice sides above 320 (2*n above 640)"};
     G.d = d;
     G.k0 = k0;
     cudaGetDevice(&G.device);

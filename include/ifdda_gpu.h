@@ -59,9 +59,9 @@ void* ifdda_ctx_stream(ifdda_ctx* ctx);
    called at cdmlib/cdmlib.f:1529-1531) with nquad = 0: the six components of
    the free-space dyadic on the (2nx,2ny,2nz) circulant grid, FFT sign +1.
    aretecube in metres, k0 in 1/m.  The spectrum stays on the device.
-   Every side from 1 to 256 is accepted, as the reference accepts any
+   Every side from 1 to 320 is accepted, as the reference accepts any
    (cdmlib/primefactor.f only warns).  2n in {2,4,6,8,10,12,16,20,24,32,40,
-   48,64,80,96,128,160,192,256,320,384,512} is computed as is; any other side n
+   48,64,80,96,128,160,192,256,320,384,512,640} is computed as is; any other side n
    is padded to the smallest n' > n with 2n' in that set.  The lattice then
    sits at the corner of the larger box, and the mat-vecs and solves map the
    caller's sites onto it.  The results are those of the caller's lattice, up

@@ -177,7 +177,7 @@ def test_zero_rhs_every_method_matches_oracle(gctx, orc, meth):
     g.close()
 
 
-@pytest.mark.parametrize("dims", [(7, 5, 3), (15, 9, 11), (256, 2, 3), (200, 3, 2)])
+@pytest.mark.parametrize("dims", [(7, 5, 3), (15, 9, 11), (256, 2, 3), (200, 3, 2), (300, 2, 2), (320, 3, 2)])
 def test_padded_lattice_matvec_matches_oracle(gctx, orc, dims):
     """A lattice side n whose 2n is not a compiled FFT length (14, 30, 18, 22,
     400 here) runs on the smallest larger compiled box, the lattice at its
@@ -200,7 +200,7 @@ def test_padded_lattice_matvec_matches_oracle(gctx, orc, dims):
     xt, bt = x[:3 * nd], b[:3 * nd]
     assert rel(g.matvec(xt, bt, tabdip=tab), orc.matvec(G, nx, ny, nz, xt, bt, tabdip=tab)) < 1e-11
     assert rel(g.matvec(x, b, precision=1), orc.matvec(G, nx, ny, nz, x, b)) < 2e-5
-    compiled = {2, 4, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256, 320, 384, 512}
+    compiled = {2, 4, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256, 320, 384, 512, 640}
     if any(2 * n not in compiled for n in dims):
         with pytest.raises(Exception, match="padded"):
             g.export()
@@ -359,9 +359,9 @@ def test_error_paths(gctx, orc):
     assert r.nstop == -1 and r.infostr.strip() == "Calculation cancelled during iterative method"
     # unsupported FFT length: 2*7 = 14 has no compiled kernel
     import ifdda
-    # a side above 256 has no compiled FFT length to pad to (2 n <= 512)
+    # a side above 320 has no compiled FFT length to pad to (2 n <= 640)
     with pytest.raises(ifdda.IfddaError):
-        gctx.green(257, 2, 2, 10e-9, k0)
+        gctx.green(321, 2, 2, 10e-9, k0)
     g.close()
 
 
