@@ -217,56 +217,65 @@ def barrier(ws):
 
 
 # ----------------------------------------------------------------- CPU arm --
-def cpu_oracle_sample(w: Workload, ncompte_full: int, n_mv=None):
+def cpu_oracle_solves(w: Workload, max_solves: int, budget_s: float):
     """Times the oracle (C restatement of the reference path, FP64, OpenMP on
-    every host thread) on one right-hand side of the workload: the Green
-    spectrum once, then the solve stopped after n_mv mat-vecs; a full solve is
-    extrapolated with the solve's mat-vec count.  Returns (solves/s for one
-    right-hand side, cores, sample string)."""
+    every host thread) doing what one cdmlib call does for one right-hand
+    side of the workload: greencalculfft, then the complete solve
+    (inverserig / inverserigopt with the workload's method) to TOL.  Runs
+    whole solves, at least one, until max_solves or budget_s seconds.
+    Returns (seconds per solve list, cores, info of the last solve)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    n_mv = n_mv or w.cpu_mv
     cores = os.cpu_count() or 1
     oracle.set_threads(cores)
     ob = w.ob
-    t0 = time.perf_counter()
-    G = oracle.greencalculfft(ob.nx, ob.ny, ob.nz, ob.aretecube, w.k0)
-    t_green = time.perf_counter() - t0
-    bm, a1, a2, pp = w.beams[0]
-    ff0 = oracle.incident(ob.xs, ob.ys, ob.zs, w.k0, w.E0, pp, bm, a1, a2)
-    t0 = time.perf_counter()
-    oracle.inverserig(G, ob.nx, ob.ny, ob.nz, ob.nbsphere, ob.polarisa, ob.nmax, ff0, w.method, TOL,
-                      tabdip=ob.tabdip_or_none, max_matvecs=n_mv)
-    t_mv = (time.perf_counter() - t0) / n_mv
-    del G
-    t_solve = t_green + t_mv * ncompte_full
-    sample = (f"oracle FP64 on {cores} host threads, one right-hand side of {w.key}: greencalculfft "
-              f"({t_green:.2f} s) + {w.method} stopped after {n_mv} mat-vecs ({t_mv:.3f} s/mat-vec incl. Krylov "
-              f"vector work); full solve extrapolated to ncompte={ncompte_full} mat-vecs = {t_solve:.1f} s")
-    return 1.0 / t_solve, cores, sample
+    times, info = [], None
+    t_all = time.perf_counter()
+    for i in range(max_solves):
+        bm, a1, a2, pp = w.beams[i % len(w.beams)]
+        ff0 = oracle.incident(ob.xs, ob.ys, ob.zs, w.k0, w.E0, pp, bm, a1, a2)
+        t0 = time.perf_counter()
+        G = oracle.greencalculfft(ob.nx, ob.ny, ob.nz, ob.aretecube, w.k0)
+        t_green = time.perf_counter() - t0
+        r = oracle.inverserig(G, ob.nx, ob.ny, ob.nz, ob.nbsphere, ob.polarisa, ob.nmax, ff0, w.method, TOL,
+                              tabdip=ob.tabdip_or_none)
+        times.append(time.perf_counter() - t0)
+        del G
+        info = {"green_s": t_green, "ncompte": int(r["ncompte"]), "nloop": int(r["nloop"]),
+                "tol1": float(r["tol1"]), "nstop": int(r["nstop"])}
+        if time.perf_counter() - t_all > budget_s:
+            break
+    return times, cores, info
 
 
-# number of mat-vecs of the FP64 GPBICG1 / QMR solve of each workload, the
-# same for the oracle and the GPU drop-in (tests check the equality)
-NCOMPTE_FP64 = {"c1": 8, "c2": 34}
+def cpu_sample_text(w, times, cores, info):
+    return (f"oracle FP64 on {cores} host threads: {len(times)} complete solve(s) of one right-hand side of "
+            f"{w.key}, each greencalculfft ({info['green_s']:.2f} s) + {w.method} to true residual {TOL:g} "
+            f"(nloop {info['nloop']}, ncompte {info['ncompte']}, tol1 {info['tol1']:.2e}); "
+            f"{statistics.mean(times):.2f} s per solve")
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of cdmlib's rigorous path timed
+    as whole solves (greencalculfft + the complete Krylov solve), one
+    right-hand side per step.  A full solve takes seconds, so the run is
+    bounded: one untimed warm-up solve, then timed solves until --steps or
+    about 150 s; the line's `steps` is the number actually timed."""
     ws, rank, _ = dist_setup()
     if rank != 0:
         return 0
     w = WORKLOADS[args.workload]()
-    ncompte = NCOMPTE_FP64.get(w.key, 40)
-    vals = []
-    for i in range(args.warmup + args.steps):
-        v, cores, sample = cpu_oracle_sample(w, ncompte, n_mv=2)
-        if i >= args.warmup:
-            vals.append(v)
-    value = statistics.mean(vals)
-    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded)", "impl": "reference",
-            "config": {"workload": w.desc, "precision": "fp64", "parallelism": "cpu"},
+    if args.warmup > 0:
+        cpu_oracle_solves(w, 1, 0.0)
+    times, cores, info = cpu_oracle_solves(w, max(1, args.steps), 150.0)
+    value = len(times) / sum(times)
+    sample = cpu_sample_text(w, times, cores, info)
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": len(times),
+            "steps_requested": args.steps, "warmup": min(args.warmup, 1), "ms_per_step": 1000.0 / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": w.desc, "precision": "fp64", "parallelism": "cpu",
+                       "step": "greencalculfft + complete solve of one right-hand side"},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -294,7 +303,7 @@ def run_gpu(args):
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
     t0 = time.perf_counter()
     g = ctx.green(ob.nx, ob.ny, ob.nz, ob.aretecube, k0)
-    green_ms = (time.perf_counter() - t0) * 1e3
+    green_ms = (time.perf_counter() - t0) * 1e3  # first build: allocation and twiddle tables included
     ff0_h = ctx.planewaves(ob.xs, ob.ys, ob.zs, k0, E0, [b[0] for b in w.beams], [b[1] for b in w.beams],
                            [b[2] for b in w.beams], [b[3] for b in w.beams])
     nb, nmax, nrhs = ob.nbsphere, ob.nmax, w.nrhs
@@ -314,8 +323,12 @@ def run_gpu(args):
             raise RuntimeError(f"solve failed: {r['infostr'].strip()}")
         return r
 
-    def timed(prec, steps, warmup, k=nrhs):
+    def timed(prec, steps, warmup, k=nrhs, green=False):
+        """steps complete solves; with green, each step first recomputes the
+        spectrum in place (greencalculfft, which cdmlib runs on every call)."""
         for _ in range(warmup):
+            if green:
+                g.recompute(ob.aretecube, k0)
             solve_dev(prec, k)
         torch.cuda.synchronize()
         barrier(ws)
@@ -328,6 +341,8 @@ def run_gpu(args):
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
+            if green:
+                g.recompute(ob.aretecube, k0)
             infos.append(solve_dev(prec, k))
             with torch.cuda.stream(stream):
                 e1.record(stream)
@@ -338,9 +353,13 @@ def run_gpu(args):
         barrier(ws)
         return times, infos, launches
 
-    # headline: mixed precision, iterations replayed as CUDA graphs
+    # headline: mixed precision, iterations replayed as CUDA graphs; a step
+    # is one object: its Green spectrum (recomputed in place, as cdmlib
+    # calls greencalculfft on every run) and the solve of its right-hand sides
     with ClockSampler(local) as clk:
-        t_mixed, info_mixed, launches = timed(IFDDA_MIXED, args.steps, args.warmup)
+        t_mixed, info_mixed, launches = timed(IFDDA_MIXED, args.steps, args.warmup, green=True)
+    # the same solves with the spectrum resident (a cached spectrum)
+    t_mixed_solve, _, _ = timed(IFDDA_MIXED, args.steps, 1)
     # the dominant kernel (zconv, FP32) bracketed by CUDA events on the
     # solver's stream during further complete solves (plain launches)
     lib.ifdda_timing_enable(_capi.PASS_ZCONV, _capi.IFDDA_FP32)
@@ -354,22 +373,65 @@ def run_gpu(args):
     loc_mixed, ff_mixed = loc_d[:kacc].cpu().numpy(), ff_d[:kacc].cpu().numpy()
 
     fp64_steps = max(1, min(args.steps, 5))
-    t_fp64, info_fp64, _ = timed(IFDDA_FP64, fp64_steps, min(args.warmup, 2), k=w.fp64_nrhs)
-    g.release_workspace()
-    # accuracy of the mixed solve against the plain FP64 drop-in (which the
-    # parity tests hold to the oracle): local field and Cext
+    t_fp64, info_fp64, _ = timed(IFDDA_FP64, fp64_steps, min(args.warmup, 2), k=w.fp64_nrhs, green=True)
     loc64, ff64 = loc_d[:kacc].cpu().numpy(), ff_d[:kacc].cpu().numpy()
-    err_loc, err_cext = 0.0, 0.0
-    for r in range(kacc):
-        err_loc = max(err_loc, float(np.linalg.norm(loc_mixed[r] - loc64[r]) / np.linalg.norm(loc64[r])))
-        cm, _ = ctx.cross_sections(ff0_h[r], ff_mixed[r], loc_mixed[r], k0, abs(E0) ** 2)
-        c6, _ = ctx.cross_sections(ff0_h[r], ff64[r], loc64[r], k0, abs(E0) ** 2)
-        err_cext = max(err_cext, abs(cm - c6) / abs(c6))
+    t_fp64_solve, _, _ = timed(IFDDA_FP64, fp64_steps, 0, k=w.fp64_nrhs)
+    # the plain FP64 drop-in called once per right-hand side, as the
+    # reference's incidence loop calls inverserig (microsbf.f:214-280)
+    serial = None
+    if nrhs > 1:
+        bytes_rhs = 3 * nb * 16
+        nser = w.fp64_nrhs
+
+        def serial_pass():
+            ts = []
+            for r in range(nser):
+                with torch.cuda.stream(stream):
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                rr = g.inverserig_device(1, nb, nmax, tab_d.data_ptr() if tab_d is not None else None,
+                                         pol_d.data_ptr(), ff0_d.data_ptr() + r * bytes_rhs,
+                                         ff_d.data_ptr() + r * bytes_rhs, loc_d.data_ptr() + r * bytes_rhs, w.method,
+                                         TOL, precision=IFDDA_FP64)
+                if rr["nstop"] != 0:
+                    raise RuntimeError(rr["infostr"].strip())
+                with torch.cuda.stream(stream):
+                    e1.record(stream)
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            return ts
+        serial_pass()
+        ts = serial_pass()
+        serial = {"solves_s": nser / (sum(ts) / 1e3), "rhs": nser, "ms_per_solve": statistics.mean(ts)}
+    # accuracy against a converged FP64 solve (true residual 1e-10; the FP64
+    # drop-in is the path the parity tests hold to the oracle): local field
+    # and Cext of the mixed solve, and of the FP64 solve stopped at TOL
+    rc = g.inverserig_device(kacc, nb, nmax, tab_d.data_ptr() if tab_d is not None else None, pol_d.data_ptr(),
+                             ff0_d.data_ptr(), ff_d.data_ptr(), loc_d.data_ptr(), w.method, 1e-10,
+                             precision=IFDDA_FP64)
+    if rc["nstop"] != 0:
+        raise RuntimeError(f"converged solve failed: {rc['infostr'].strip()}")
+    locc, ffc = loc_d[:kacc].cpu().numpy(), ff_d[:kacc].cpu().numpy()
+    g.release_workspace()
+    acc = {"reference": "FP64 drop-in solved to true residual 1e-10", "rhs_compared": kacc,
+           "converged_tol1_max": float(np.max(rc["tol1"]))}
+    for name, loc, ff in (("mixed", loc_mixed, ff_mixed), ("fp64", loc64, ff64)):
+        el, ec = 0.0, 0.0
+        for r in range(kacc):
+            el = max(el, float(np.linalg.norm(loc[r] - locc[r]) / np.linalg.norm(locc[r])))
+            cm, _ = ctx.cross_sections(ff0_h[r], ff[r], loc[r], k0, abs(E0) ** 2)
+            cc, _ = ctx.cross_sections(ff0_h[r], ffc[r], locc[r], k0, abs(E0) ** 2)
+            ec = max(ec, abs(cm - cc) / abs(cc))
+        acc[f"local_field_rel_l2_{name}"] = el
+        acc[f"cext_rel_diff_{name}"] = ec
 
     total_ms = max_over_ranks(sum(t_mixed), ws, dev)
     value = ws * args.steps * nrhs / (total_ms / 1e3)
+    solve_only = ws * args.steps * nrhs / (max_over_ranks(sum(t_mixed_solve), ws, dev) / 1e3)
     fp64_total = max_over_ranks(sum(t_fp64), ws, dev)
     fp64_value = ws * fp64_steps * w.fp64_nrhs / (fp64_total / 1e3)
+    fp64_solve_only = ws * fp64_steps * w.fp64_nrhs / (max_over_ranks(sum(t_fp64_solve), ws, dev) / 1e3)
 
     # mat-vec throughput (whole mat-vec, algorithmic bytes, one right-hand side)
     N = ob.nx * ob.ny * ob.nz
@@ -417,12 +479,15 @@ def run_gpu(args):
                    torch.empty(ff0_h.shape, dtype=torch.complex128).pin_memory().numpy())
         e2e_steps = max(1, min(args.steps, 20, int(10000.0 / max(total_ms / args.steps, 1.0))))  # ~10 s at most
         tab_h = ob.tabdip_or_none
+        g.recompute(ob.aretecube, k0)
         g.inverserig(nb, pol_pin.numpy(), nmax, ff0_pin.numpy(), w.method, TOL, tabdip=tab_h, precision=IFDDA_MIXED,
                      out=out_pin)
         barrier(ws)
         te = []
         for _ in range(e2e_steps):
             t0 = time.perf_counter()
+            # what one cdmlib call does on the path: greencalculfft, then the solve
+            g.recompute(ob.aretecube, k0)
             r = g.inverserig(nb, pol_pin.numpy(), nmax, ff0_pin.numpy(), w.method, TOL, tabdip=tab_h,
                              precision=IFDDA_MIXED, out=out_pin)
             te.append(time.perf_counter() - t0)
@@ -440,9 +505,9 @@ def run_gpu(args):
     achieved = zc_bytes / (zconv_ms * 1e6) if zconv_ms > 0 else None
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        ncompte64 = int(info_fp64[0]["ncompte"][0])
-        v, cores, sample = cpu_oracle_sample(w, ncompte64)
-        cpu = {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample}
+        times, cores, info = cpu_oracle_solves(w, 1, 0.0)
+        cpu = {"value": len(times) / sum(times), "unit": "solves/s", "cores": cores, "kind": "port",
+               "sample": cpu_sample_text(w, times, cores, info)}
 
     lat = sorted(t_mixed)
     p50 = statistics.median(lat)
@@ -454,15 +519,18 @@ def run_gpu(args):
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64 inner / c128 outer", "data": "synthetic (seeded)",
         "config": {"workload": w.desc, "nrhs_per_step": nrhs, "precision": "mixed FP32/FP64 refinement",
-                   "l2": "flushed before each step", "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+                   "step": "Green spectrum recomputed in place (greencalculfft) + solve of the step's right-hand "
+                           "sides, as one cdmlib call", "l2": "flushed before each step",
+                   "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
         "latency_ms": {"p50": p50, "p99": p99},
-        "mixed": {"solves_s": value, "nloop_max": int(np.max(im["nloop"])), "ncompte_max": int(np.max(im["ncompte"])),
-                  "tol1_max": float(np.max(im["tol1"]))},
-        "fp64": {"solves_s": fp64_value, "nrhs": w.fp64_nrhs, "ms_per_solve": fp64_total / fp64_steps,
-                 "nloop_max": int(np.max(i64["nloop"])), "ncompte_max": int(np.max(i64["ncompte"])),
-                 "tol1_max": float(np.max(i64["tol1"]))},
-        "accuracy": {"local_field_rel_l2_mixed_vs_fp64": err_loc, "cext_rel_diff_mixed_vs_fp64": err_cext,
-                     "rhs_compared": kacc},
+        "mixed": {"solves_s": value, "solves_s_spectrum_resident": solve_only, "nloop_max": int(np.max(im["nloop"])),
+                  "ncompte_max": int(np.max(im["ncompte"])), "tol1_max": float(np.max(im["tol1"]))},
+        "fp64": {"solves_s": fp64_value, "solves_s_spectrum_resident": fp64_solve_only, "nrhs": w.fp64_nrhs,
+                 "ms_per_step": fp64_total / fp64_steps, "nloop_max": int(np.max(i64["nloop"])),
+                 "ncompte_max": int(np.max(i64["ncompte"])), "tol1_max": float(np.max(i64["tol1"]))},
+        "accuracy": acc,
+        "fp64_one_rhs_per_call": serial,
+        "mixed_batched_over_fp64_one_rhs_per_call": (solve_only / serial["solves_s"]) if serial else None,
         "matvec": mv,
         "green_build_ms": green_ms,
         "roofline": {"bound": "hbm", "kernel": f"k_zconv<float,{Z}> (z FFT + 3x3 spectrum multiply + inverse z FFT)",
@@ -682,9 +750,10 @@ def run_microscope(args):
     nill = m["illuminations"]
     cpu = None
     if not args.no_cpu and rank == 0:
-        v, cores, sample = cpu_oracle_sample(w, out["fp64"]["last_ncompte"])
-        cpu = {"value": v / nill, "unit": "images/s", "cores": cores, "kind": "port",
-               "sample": sample + f"; one image = {nill} such solves (the oracle's image formation not counted)"}
+        times, cores, info = cpu_oracle_solves(w, 1, 0.0)
+        cpu = {"value": len(times) / sum(times) / nill, "unit": "images/s", "cores": cores, "kind": "port",
+               "sample": cpu_sample_text(w, times, cores, info) +
+               f"; one image = {nill} such solves (the oracle's image formation not counted)"}
     desc = (f"bright-field microscope (microsbf.f, FFT lens) of the c3 ellipsoid (96x96x64 full box, d=10 nm, "
             f"lambda=500 nm): objective NA 0.9, condenser NA 0.5, {nill} illuminations (s and p), image "
             f"512x512, magnification 100, GPBICG1 to 1e-4")

@@ -355,6 +355,17 @@ int ifdda_green_create_nquad(ifdda_ctx* ctx, int nx, int ny, int nz, double aret
     IFDDA_GUARD_END(ctx, nullptr)
 }
 
+int ifdda_green_recompute(ifdda_green* g, double aretecube, double k0) {
+    if (!g) return 1;
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(g->ctx->device);
+    AllocStreamScope as(g->ctx->stream);
+    if (!(aretecube > 0) || !(k0 > 0)) throw EngineError{1, "ifdda_green_recompute: aretecube and k0 must be > 0"};
+    green_recompute(g->G, aretecube, k0, g->ctx->stream);
+    return 0;
+    IFDDA_GUARD_END(g->ctx, nullptr)
+}
+
 int ifdda_green_destroy(ifdda_green* g) {
     if (!g) return 0;
     ifdda_ctx* ctx = g->ctx;
@@ -415,6 +426,8 @@ int ifdda_matvec(ifdda_green* g, int precision, int ndip, const int* tabdip, con
                  ifdda_dcmplx* FFB) {
     if (!g || !FFX || !FFB) return 1;
     IFDDA_GUARD_BEGIN
+    if (precision != IFDDA_FP32 && precision != IFDDA_FP64)
+        throw EngineError{1, "ifdda_matvec: precision must be IFDDA_FP32 or IFDDA_FP64"};
     DeviceScope ds(g->ctx->device);
     AllocStreamScope as(g->ctx->stream);
     cudaStream_t st = g->ctx->stream;
@@ -460,6 +473,8 @@ int ifdda_matvec_device(ifdda_green* g, int precision, int nrhs, int ndip, const
                         const void* FFX_dev, void* FFB_dev) {
     if (!g || !FFX_dev || !FFB_dev || nrhs < 1 || ndip < 1) return 1;
     IFDDA_GUARD_BEGIN
+    if (precision != IFDDA_FP32 && precision != IFDDA_FP64)
+        throw EngineError{1, "ifdda_matvec_device: precision must be IFDDA_FP32 or IFDDA_FP64"};
     DeviceScope ds(g->ctx->device);
     AllocStreamScope as(g->ctx->stream);
     cudaStream_t st = g->ctx->stream;

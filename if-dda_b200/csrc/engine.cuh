@@ -152,6 +152,9 @@ MvGeom make_geom(int nx, int ny, int nz);
 // tensor at every offset between the caller's sites)
 void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStream_t st, int nquad = 0,
                  bool pad = false);
+// the spectrum of G's lattice (and nquad, padding) for another spacing and
+// wavenumber, into G's own buffers (its solver workspaces stay valid)
+void green_recompute(Green& G, double d, double k0, cudaStream_t st);
 // full FFTTENSOR arrays (6 x 8N) on the host, expanded from the compressed octant
 void green_export(const Green& G, double2* const out[6], cudaStream_t st);
 

@@ -79,29 +79,11 @@ static int padded_side(int n) {
     return n;
 }
 
-void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStream_t st, int nquad, bool pad) {
-    if (nx < 1 || ny < 1 || nz < 1) throw EngineError{1, "Green: lattice dimensions must be positive"};
-    if (nquad < 0 || nquad > 16) throw EngineError{1, "Green: nquad must be in [0, 16]"};
-    G.ux = nx;
-    G.uy = ny;
-    G.uz = nz;
-    G.uN = (long)nx * ny * nz;
-    if (pad) {
-        nx = padded_side(nx);
-        ny = padded_side(ny);
-        nz = padded_side(nz);
-    }
-    G.g = make_geom(nx, ny, nz);
-    if (!fft_length_supported(G.g.X) || !fft_length_supported(G.g.Y) || !fft_length_supported(G.g.Z))
-        throw EngineError{1, "FFT size not supported: lattice sides above 320 (2*n above 640)"};
-    G.d = d;
-    G.k0 = k0;
-    cudaGetDevice(&G.device);
-    upload_twiddles(G.g.X, G.tw64[0], G.tw32[0], st);
-    upload_twiddles(G.g.Y, G.tw64[1], G.tw32[1], st);
-    upload_twiddles(G.g.Z, G.tw64[2], G.tw32[2], st);
-    G.nquad = nquad;
-    GreenGeom gg{nx, ny, nz, G.g.X, G.g.Y, G.g.Z, d, k0, nquad, nullptr};
+// The spectrum of G's lattice for its current (d, k0, nquad) into G.gc64 /
+// G.gc32, which are allocated; the twiddle tables are uploaded.
+static void green_compute(Green& G, cudaStream_t st) {
+    const int nx = G.g.nx, ny = G.g.ny, nz = G.g.nz, nquad = G.nquad;
+    GreenGeom gg{nx, ny, nz, G.g.X, G.g.Y, G.g.Z, G.d, G.k0, nquad, nullptr};
     // cube-averaged tensor on the offsets i, j, k >= 0 within nquad
     DevBuf<double2> quad, qpart;
     DevBuf<int3> qoffs;
@@ -126,11 +108,10 @@ void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStre
         IFDDA_CUDA(cudaStreamSynchronize(st));  // the offsets live on this stack frame
     }
     const long W = nx + 1;
+    // the intermediate spectra are freed stream-ordered, after the kernels
     DevBuf<double2> GA, GB;
     GA.ensure((size_t)6 * G.g.Z * G.g.Y * W);
     GB.ensure((size_t)6 * G.g.Z * (ny + 1) * W);
-    G.gc64.ensure((size_t)6 * G.g.gc_comp);
-    G.gc32.ensure((size_t)6 * G.g.gc_comp);
     switch (G.g.X) {
 #define IFDDA_CASE_GX(L) \
     case L: launch_gx<L>(gg, GA.p, G.tw64[0].p, st); break;
@@ -151,6 +132,40 @@ void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStre
     }
     IFDDA_CUDA(cudaGetLastError());
     IFDDA_CUDA(cudaStreamSynchronize(st));
+}
+
+void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStream_t st, int nquad, bool pad) {
+    if (nx < 1 || ny < 1 || nz < 1) throw EngineError{1, "Green: lattice dimensions must be positive"};
+    if (nquad < 0 || nquad > 16) throw EngineError{1, "Green: nquad must be in [0, 16]"};
+    G.ux = nx;
+    G.uy = ny;
+    G.uz = nz;
+    G.uN = (long)nx * ny * nz;
+    if (pad) {
+        nx = padded_side(nx);
+        ny = padded_side(ny);
+        nz = padded_side(nz);
+    }
+    G.g = make_geom(nx, ny, nz);
+    if (!fft_length_supported(G.g.X) || !fft_length_supported(G.g.Y) || !fft_length_supported(G.g.Z))
+        throw EngineError{1, "FFT size not supported: lattice sides above 320 (2*n above 640)"};
+    G.d = d;
+    G.k0 = k0;
+    cudaGetDevice(&G.device);
+    upload_twiddles(G.g.X, G.tw64[0], G.tw32[0], st);
+    upload_twiddles(G.g.Y, G.tw64[1], G.tw32[1], st);
+    upload_twiddles(G.g.Z, G.tw64[2], G.tw32[2], st);
+    G.nquad = nquad;
+    G.gc64.ensure((size_t)6 * G.g.gc_comp);
+    G.gc32.ensure((size_t)6 * G.g.gc_comp);
+    green_compute(G, st);
+}
+
+void green_recompute(Green& G, double d, double k0, cudaStream_t st) {
+    if (!G.gc64.p || !G.gc32.p) throw EngineError{1, "Green: no spectrum to recompute"};
+    G.d = d;
+    G.k0 = k0;
+    green_compute(G, st);
 }
 
 // parity of component c along axis a: +1 even, -1 odd (xx,xy,xz,yy,yz,zz)

@@ -775,7 +775,11 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
             break;
         }
         if (!krylov_run<float>(G, isp, W, st)) {
+            // cancelled: the iterations and mat-vecs the partial inner run
+            // made still count (read after the loop)
             ok = false;
+            mask = ost;
+            pending = true;
             break;
         }
         mask = ost;

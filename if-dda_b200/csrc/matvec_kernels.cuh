@@ -357,8 +357,11 @@ template <class LZ> constexpr int zmid_cost(int order, int TL, int NJ, int RK, i
 // transform run on the reversed plan, so the inverse starts from the values
 // the forward one ended with (its pass 0 reads exactly the points
 // j + r L/R the forward last pass produced), then inverse passes 1 .. n-1.
+// A block keeps its slice of the spectrum in shared memory and convolves the
+// right-hand sides rpb * blockIdx.z .. + rpb - 1 in turn, so a batch reads
+// each spectrum value once per rpb right-hand sides.
 template <class T, int L, class TT = MvTiles<T, L>>
-__global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a) {
+__global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a, const int nrhs, const int rpb) {
     using C = cplx<T>;
     using LZ = typename TT::LayZ;
     constexpr int TL = TT::TLZ, NB = TT::NBZ, NT = TT::NTZ;
@@ -370,7 +373,6 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
     constexpr int S = (int)sizeof(C);
     constexpr int ORDER = zmid_cost<LZ>(1, TL, NJ, RK, NG, S) < zmid_cost<LZ>(0, TL, NJ, RK, NG, S) ? 1 : 0;
     constexpr int NQ = L / 2 + 1;
-    const int rhs = blockIdx.z;
     C* tw = smem_base<C>();
     C* sm = tw + L;
     C* gs = sm + LZ::span(L) * TT::PSZ;
@@ -398,10 +400,11 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
     // the spectrum and the twiddles are constant: only B2 waits for the y pass
     pdl_trigger();
     pdl_wait();
-    if (a.status && a.status[rhs]) {
-        cp_async_wait_all();
-        return;
-    }
+    const int r1 = min(nrhs, (int)(blockIdx.z + 1) * rpb);
+    for (int rhs = blockIdx.z * rpb; rhs < r1; rhs++) {
+    // the status is the same for every thread of the block
+    if (a.status && a.status[rhs]) continue;
+    __syncthreads();  // the previous right-hand side's last reads of the tile are done
     C* B2 = a.B2 + rhs * a.g.b2_rhs + (long)qy * X + i0;
     const int rs = Y * X, comp = nz * Y * X, drow = (Y - 2 * qy) * X, nv = min(TL, X - i0);
     const ZLoad<T, TL> zload{B2, rs, comp, drow, nv, two};
@@ -491,6 +494,8 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
         __syncthreads();
         stockham_range<C, L, NB, NT, -1, LZ, true, NP, 1, RK>(sm, tw, SmemIO{}, zstore);
     }
+    }  // right-hand sides
+    cp_async_wait_all();  // every right-hand side may have been finished already
 }
 
 // ---- pass 5 -----------------------------------------------------------------

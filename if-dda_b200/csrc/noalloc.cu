@@ -15,6 +15,7 @@
 // needs to start at zero, because each pass writes every element the next
 // pass reads.  Two calls whose kernels overlap on the GPU (different streams
 // or different host threads on one device) race on the array.
+#include <exception>
 #include <mutex>
 #include "capi_types.cuh"
 
@@ -76,6 +77,8 @@ extern "C" int ifdda_matvec_noalloc(ifdda_green* g, int precision, int ndip, con
     if (!g || !FFX_dev || !FFB_dev || ndip < 1) return 1;
     ifdda_ctx* ctx = g->ctx;
     try {
+        if (precision != IFDDA_FP32 && precision != IFDDA_FP64)
+            throw ifdda::EngineError{1, "ifdda_matvec_noalloc: precision must be IFDDA_FP32 or IFDDA_FP64"};
         int prev = -1;
         IFDDA_CUDA(cudaGetDevice(&prev));
         if (prev != ctx->device) IFDDA_CUDA(cudaSetDevice(ctx->device));
@@ -103,6 +106,10 @@ extern "C" int ifdda_matvec_noalloc(ifdda_green* g, int precision, int ndip, con
         return 0;
     } catch (const ifdda::EngineError& e) {
         ctx->last_error = e.msg;
+        return 1;
+    } catch (const std::exception& e) {
+        // e.g. std::bad_alloc from an error message, std::system_error from the mutex
+        ctx->last_error = e.what();
         return 1;
     }
 }

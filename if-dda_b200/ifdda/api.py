@@ -234,6 +234,12 @@ class GreenSpectrum:
         except Exception:
             pass
 
+    def recompute(self, aretecube, k0):
+        """Recompute the spectrum in place for another spacing / wavenumber
+        (greencalculfft called again into the same FFTTENSOR arrays)."""
+        self.ctx._check(self.lib.ifdda_green_recompute(self.h, float(aretecube), float(k0)))
+        self.aretecube, self.k0 = float(aretecube), float(k0)
+
     def release_workspace(self):
         """Free the solver / mat-vec workspaces; the spectrum stays."""
         self.ctx._check(self.lib.ifdda_green_release_workspace(self.h))

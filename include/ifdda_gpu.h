@@ -75,6 +75,13 @@ int ifdda_green_create(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube,
    zero at the origin, the plain tensor beyond one wavelength. */
 int ifdda_green_create_nquad(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, int nquad,
                              ifdda_green** out);
+/* Recomputes g's spectrum in place for another lattice spacing and
+   wavenumber (same lattice sides, nquad and padding): the call cdmlib makes
+   at cdmlib/cdmlib.f:1529-1531 on every run, writing greencalculfft's result
+   into the FFTTENSOR arrays it already holds.  g's solver workspaces (and the
+   CUDA graphs captured on them) stay valid, so a solve that follows starts
+   without re-allocation.  Returns after the spectrum is complete. */
+int ifdda_green_recompute(ifdda_green* g, double aretecube, double k0);
 int ifdda_green_destroy(ifdda_green* g);
 /* Frees the solver and mat-vec workspaces held by g (they are re-created on
    the next solve); the spectrum stays.  For callers that cache many spectra.
@@ -89,14 +96,15 @@ int ifdda_green_export(ifdda_green* g, ifdda_dcmplx* xx, ifdda_dcmplx* xy, ifdda
 /* Mat-vec FFB <- FFB - (1/ntotal) IFFT(G~ . FFT(pad FFX)).  Replaces
    produitfftmatvectopt (cdmlib/produitfftmatvectopt.f:3-121, tabdip == NULL,
    ndip = nx*ny*nz) and produitfftmatvect3 (cdmlib/produitfftmatvect3.f:2-127,
-   tabdip != NULL, ndip = dipole count).  precision: IFDDA_FP64 or IFDDA_FP32. */
+   tabdip != NULL, ndip = dipole count).  precision: IFDDA_FP64 or IFDDA_FP32;
+   any other value returns 1. */
 int ifdda_matvec(ifdda_green* g, int precision, int ndip, const int* tabdip, const ifdda_dcmplx* FFX,
                  ifdda_dcmplx* FFB);
 
 /* Same operation on nrhs vectors already in device memory, in place on
    FFB_dev: complex128 vectors for IFDDA_FP64, complex64 for IFDDA_FP32
    (3*ndip per right-hand side, contiguous).  Asynchronous on the context's
-   stream. */
+   stream.  Any other precision returns 1. */
 int ifdda_matvec_device(ifdda_green* g, int precision, int nrhs, int ndip, const int* tabdip_dev,
                         const void* FFX_dev, void* FFB_dev);
 
@@ -107,10 +115,13 @@ int ifdda_matvec_device(ifdda_green* g, int precision, int nrhs, int ndip, const
    application that has handed its whole memory budget to another library.  It has no counterpart in the reference (whose
    buffers are static Fortran arrays).  The mat-vec scratch lives in one fixed
    16 MiB device array inside the library (held by every GPU that loads it
-   until the process exits), so 18*nx*ny*nz complex values of the chosen
-   precision must fit in 16 MiB (e.g. 32^3 sites fit in FP64 and 40^3 in FP32,
-   48^3 does not fit in FP64);
-   larger grids return 1 with the reason in ifdda_ctx_last_error.  The first
+   until the process exits), so 18*nx'*ny'*nz' complex values of the chosen
+   precision must fit in 16 MiB, where nx', ny', nz' are the sides the
+   spectrum was computed on: the caller's sides, or the larger padded ones
+   when a side n has 2n outside the compiled FFT lengths (e.g. 32^3 sites fit
+   in FP64 and 40^3 in FP32, 48^3 does not fit in FP64; 33^3 runs on the 40^3
+   box).  Larger grids, and a precision other than IFDDA_FP32 / IFDDA_FP64,
+   return 1 with the reason in ifdda_ctx_last_error.  The first
    call on a device looks up the array's device address; make that first call
    before any stream capture.  All calls share the array: calls whose kernels
    overlap on the GPU race.  The spectrum comes from ifdda_green_create, made

@@ -29,6 +29,32 @@ def test_green_spectrum_matches_oracle(gctx, orc, dims):
     g.close()
 
 
+def test_green_recompute_matches_a_new_spectrum(gctx, orc):
+    """ifdda_green_recompute (greencalculfft called again into the arrays the
+    caller holds, cdmlib.f:1529-1531): the spectrum at a new spacing and
+    wavelength matches the oracle's, and a solve after it (on workspaces and
+    captured loops made for the old spectrum) equals a fresh handle's solve
+    bit for bit."""
+    ob, k0, E0, ff0, _ = _c1_inputs(orc, nnnr=10)
+    g = gctx.green(10, 10, 10, ob.aretecube, k0)
+    g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-6, tabdip=ob.tabdip)
+    d2, k2 = 0.9 * ob.aretecube, 1.1 * k0
+    g.recompute(d2, k2)
+    ref = orc.greencalculfft(10, 10, 10, d2, k2)
+    got = g.export()
+    for c in range(6):
+        assert np.abs(got[c] - ref[c]).max() <= 1e-11 * np.abs(ref[c]).max(), c
+    for prec in (0, 1):
+        r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-6, tabdip=ob.tabdip, precision=prec)
+        fresh = gctx.green(10, 10, 10, d2, k2)
+        f = fresh.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-6, tabdip=ob.tabdip,
+                             precision=prec)
+        fresh.close()
+        assert r.nstop == f.nstop == 0
+        assert np.array_equal(r.FFloc, f.FFloc) and int(r.ncompte[0]) == int(f.ncompte[0])
+    g.close()
+
+
 @pytest.mark.parametrize("dims", SIZES)
 @pytest.mark.parametrize("inside", [False, True])
 def test_matvec_fp64_matches_oracle(gctx, orc, dims, inside):
@@ -177,13 +203,16 @@ def test_zero_rhs_every_method_matches_oracle(gctx, orc, meth):
     g.close()
 
 
-@pytest.mark.parametrize("dims", [(7, 5, 3), (15, 9, 11), (256, 2, 3), (200, 3, 2), (300, 2, 2), (320, 3, 2)])
+@pytest.mark.parametrize("dims", [(7, 5, 3), (15, 9, 11), (256, 2, 3), (200, 3, 2), (300, 2, 2), (320, 3, 2),
+                                  (2, 300, 2), (3, 2, 320), (2, 256, 3), (3, 2, 200), (2, 320, 3), (2, 3, 300)])
 def test_padded_lattice_matvec_matches_oracle(gctx, orc, dims):
     """A lattice side n whose 2n is not a compiled FFT length (14, 30, 18, 22,
-    400 here) runs on the smallest larger compiled box, the lattice at its
+    400, 600 here) runs on the smallest larger compiled box, the lattice at its
     corner: the mat-vec of the caller's lattice, full box and through a
-    Tabdip, matches the oracle's on the caller's own 2n grid (and 256 x 2 x 3
-    checks the length 512 itself)."""
+    Tabdip, matches the oracle's on the caller's own 2n grid.  The long side
+    sits on x, on y and on z in turn, so the x passes, the y passes and the z
+    convolution each run at the lengths 512 (256 and 200 -> 512) and 640
+    (300 and 320 -> 640)."""
     nx, ny, nz = dims
     d, k0 = 10e-9, 2 * math.pi / 600e-9
     G = orc.greencalculfft(nx, ny, nz, d, k0)
@@ -362,6 +391,11 @@ def test_error_paths(gctx, orc):
     # a side above 320 has no compiled FFT length to pad to (2 n <= 640)
     with pytest.raises(ifdda.IfddaError):
         gctx.green(321, 2, 2, 10e-9, k0)
+    # a mat-vec precision other than FP32 / FP64 is an error, not a silent FP64
+    x = np.zeros(3 * ob.nbsphere, np.complex128)
+    for prec in (1, 3, -1):
+        with pytest.raises(ifdda.IfddaError, match="precision"):
+            g.matvec(x, x.copy(), tabdip=ob.tabdip, precision=prec)
     g.close()
 
 
