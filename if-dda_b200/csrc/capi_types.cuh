@@ -30,6 +30,14 @@ struct ifdda_green {
     ifdda::DevBuf<int> ptab;
     ifdda::DevBuf<double2> alpha, ff0, x, ffx, ffb;
     ifdda::DevBuf<float2> ffx32, ffb32, alpha32;
+    // a ragged batch solved with this handle's workspaces (the first object
+    // of ifdda_inverserig_ragged): concatenated Tabdips and polarisabilities,
+    // per right-hand side spectra and offsets
+    ifdda::DevBuf<int> rtab, rtab_in;
+    ifdda::DevBuf<double2> ralpha;
+    ifdda::DevBuf<const double2*> rgc64;
+    ifdda::DevBuf<const float2*> rgc32;
+    ifdda::DevBuf<long> roff;
 };
 
 // The Tabdip the mat-vec kernels use for a lattice Tabdip src (device,

@@ -150,8 +150,10 @@ MvGeom make_geom(int nx, int ny, int nz);
 // pad: a lattice side n whose 2 n is not a compiled length is padded to the
 // smallest n' > n whose 2 n' is (the spectrum of the larger box holds the same
 // tensor at every offset between the caller's sites)
+// box: explicit sides (bx, by, bz) of the grid's box, each at least the
+// lattice's, instead of the padding rule (a ragged batch's common box)
 void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStream_t st, int nquad = 0,
-                 bool pad = false);
+                 bool pad = false, const int* box = nullptr);
 // the spectrum of G's lattice (and nquad, padding) for another spacing and
 // wavenumber, into G's own buffers (its solver workspaces stay valid)
 void green_recompute(Green& G, double d, double k0, cudaStream_t st);

@@ -134,14 +134,21 @@ static void green_compute(Green& G, cudaStream_t st) {
     IFDDA_CUDA(cudaStreamSynchronize(st));
 }
 
-void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStream_t st, int nquad, bool pad) {
+void green_build(Green& G, int nx, int ny, int nz, double d, double k0, cudaStream_t st, int nquad, bool pad,
+                 const int* box) {
     if (nx < 1 || ny < 1 || nz < 1) throw EngineError{1, "Green: lattice dimensions must be positive"};
     if (nquad < 0 || nquad > 16) throw EngineError{1, "Green: nquad must be in [0, 16]"};
     G.ux = nx;
     G.uy = ny;
     G.uz = nz;
     G.uN = (long)nx * ny * nz;
-    if (pad) {
+    if (box) {
+        if (box[0] < nx || box[1] < ny || box[2] < nz)
+            throw EngineError{1, "Green: the box must hold the lattice (each side at least the lattice's)"};
+        nx = box[0];
+        ny = box[1];
+        nz = box[2];
+    } else if (pad) {
         nx = padded_side(nx);
         ny = padded_side(ny);
         nz = padded_side(nz);

@@ -215,6 +215,7 @@ static void mv_solver(Green& G, const SolveSpec& sp, KrylovWork<T>& W, int sx, i
     const cplx<T>* x = V.base + (long)sx * W.nrhs * W.n3;
     cplx<T>* y = V.base + (long)sy * W.nrhs * W.n3;
     MvArgs<T> a = mv_args<T>(G, W.nrhs, x, x, y, W.n3, sp.amode, (const cplx<T>*)sp.alpha, sp.nmax, sp.tabdip, status);
+    set_ragged(a, sp);
     if (!matvec_launch<T>(a, W.nrhs, sp.tabdip != nullptr, st))
         throw EngineError{1, "FFT size not supported by the compiled kernels"};
 }
@@ -229,6 +230,7 @@ static void mv_transpose(Green& G, const SolveSpec& sp, KrylovWork<T>& W, int sx
     Slots<T> V = W.slots();
     MvArgs<T> a = mv_args<T>(G, W.nrhs, V.v(sx, 0), V.v(sx, 0), V.v(L_T, 0), W.n3, ALPHA_NONE, nullptr, 0, sp.tabdip,
                              status);
+    set_ragged(a, sp);
     if (!matvec_launch<T>(a, W.nrhs, sp.tabdip != nullptr, st))
         throw EngineError{1, "FFT size not supported by the compiled kernels"};
     vec_launch<0>(LTrans<T>{V, W.st.p, sx, sy, sp.amode, (const cplx<T>*)sp.alpha, sp.nmax}, W.n3, W.nblk, W.nrhs, rs,
@@ -280,10 +282,12 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
     auto iteration = [&](int par) {
         if (fused) {
             const int tcur = par ? G_TB : G_TA, tnew = par ? G_TA : G_TB;
-            const MvArgs<T> a1 = mv_args<T>(G, nrhs, V.v(G_P, 0), V.v(G_P, 0), V.v(G_AP, 0), n3, sp.amode, alpha,
-                                            sp.nmax, sp.tabdip, status);
-            const MvArgs<T> a2 = mv_args<T>(G, nrhs, V.v(tnew, 0), V.v(tnew, 0), V.v(G_AT, 0), n3, sp.amode, alpha,
-                                            sp.nmax, sp.tabdip, status);
+            MvArgs<T> a1 = mv_args<T>(G, nrhs, V.v(G_P, 0), V.v(G_P, 0), V.v(G_AP, 0), n3, sp.amode, alpha,
+                                      sp.nmax, sp.tabdip, status);
+            MvArgs<T> a2 = mv_args<T>(G, nrhs, V.v(tnew, 0), V.v(tnew, 0), V.v(G_AT, 0), n3, sp.amode, alpha,
+                                      sp.nmax, sp.tabdip, status);
+            set_ragged(a1, sp);
+            set_ragged(a2, sp);
             if (!matvec_launch_fused<T>(a1, PreGpP<T>{V, S}, EpiGpAlpha<T>{V, S, status}, red, nrhs, tab, st) ||
                 !matvec_launch_fused<T>(a2, PreGpYT<T>{V, S, tcur, tnew}, EpiGpZeta<T>{V, S, status, tnew, every2}, red, nrhs,
                                         tab, st))
@@ -441,7 +445,7 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
         key = {V.base, sp.alpha, sp.tabdip, G.gc<T>(), mw.B1.p, mw.B2.p, W.partials.p, W.tickets.p, status, S,
                W.mvpart.p, W.mvtk.p, W.loopcount.p, (const void*)(long)fused,
                (const void*)(long)sp.method, (const void*)(long)nrhs, (const void*)n3, (const void*)(long)sp.amode,
-               (const void*)sp.nmax, (const void*)(long)nblk};
+               (const void*)sp.nmax, (const void*)(long)nblk, sp.gc64_r, sp.gc32_r, sp.alpha_off, sp.tab_off};
     }
     const bool cached = graphs && W.graph.exec && W.graph.key == key;
     // without a loop captured for these buffers, the first two iterations run
@@ -645,6 +649,9 @@ void solve_fp64(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b_
                 cudaStream_t st) {
     KrylovWork<double>& W = SW.kw64;
     W.ensure(sp.method, sp.nrhs, sp.n3);
+    // a ragged batch pads shorter objects' vectors with entries no kernel
+    // writes: they start at zero and stay zero
+    if (sp.tab_off) IFDDA_CUDA(cudaMemsetAsync(W.vecs.p, 0, W.vecs.n * sizeof(double2), st));
     const long tot = (long)sp.nrhs * sp.n3;
     Slots<double> V = W.slots();
     const int bs = W.b_slot(sp.method), xs = W.x_slot(sp.method), xrs = W.xr_slot(sp.method);
@@ -669,6 +676,7 @@ void solve_fp64(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b_
     {
         MvArgs<double> a = mv_args<double>(G, sp.nrhs, V.v(xs, 0), V.v(xs, 0), V.v(xrs, 0), sp.n3, sp.amode,
                                            (const double2*)sp.alpha, sp.nmax, sp.tabdip, W.zstatus.p);
+        set_ragged(a, sp);
         if (!matvec_launch<double>(a, sp.nrhs, sp.tabdip != nullptr, st))
             throw EngineError{1, "FFT size not supported by the compiled kernels"};
         RedSlots rs{W.partials.p, W.tickets.p, W.nblk};
@@ -706,6 +714,10 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
     M.tickets.ensure(nrhs);
     KrylovWork<float>& W = SW.kw32;
     W.ensure(sp.method, nrhs, n3);
+    if (sp.tab_off) {  // ragged batch: padding entries start at zero (see solve_fp64)
+        IFDDA_CUDA(cudaMemsetAsync(W.vecs.p, 0, W.vecs.n * sizeof(float2), st));
+        IFDDA_CUDA(cudaMemsetAsync(M.ax.p, 0, tot * sizeof(double2), st));
+    }
     const int nblk = reduction_blocks(n3);
     RedSlots rs{M.partials.p, M.tickets.p, nblk};
     // FP32 copy of the polarisability
@@ -753,6 +765,7 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
     for (;; outer++) {
         MvArgs<double> a = mv_args<double>(G, nrhs, M.x.p, M.x.p, M.ax.p, n3, sp.amode, (const double2*)sp.alpha,
                                            sp.nmax, sp.tabdip, M.ostatus.p);
+        set_ragged(a, sp);
         if (!matvec_launch<double>(a, nrhs, sp.tabdip != nullptr, st))
             throw EngineError{1, "FFT size not supported by the compiled kernels"};
         vec_launch<1>(ResidualOp{b_dev, M.ax.p, V.v(bs, 0), n3, M.ost.p, W.st.p, W.status.p, sp.inner_floor}, n3,

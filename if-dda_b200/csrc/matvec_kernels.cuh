@@ -63,6 +63,15 @@ template <class T> struct MvArgs {
     const C* twz;
     const int* status;   // per rhs: nonzero -> skip (solve finished)
     T inv_m;             // 1 / (X Y Z)
+    // Ragged batch (objects of different lattices, spacings and wavelengths
+    // on one common box): per right-hand side, its object's spectrum and the
+    // offsets of its polarisability (dipoles) and Tabdip (box sites) in the
+    // concatenated alpha / tabdip arrays.  Null: one object for every rhs.
+    const C* const* gc_r;
+    const long* alpha_off;
+    const long* tab_off;
+    __device__ __forceinline__ const int* tab_of(int rhs) const { return tab_off ? tabdip + tab_off[rhs] : tabdip; }
+    __device__ __forceinline__ const C* alpha_of(int rhs) const { return alpha_off ? alpha + alpha_off[rhs] : alpha; }
 };
 
 // Tile shapes: lines per block, threads per block and the register cap of
@@ -221,7 +230,8 @@ __global__ void __launch_bounds__(TT::NTX, TT::MINBX) k_fwd_x(const MvArgs<T> a,
     pdl_trigger();
     pdl_wait();
     if (a.status && a.status[rhs]) return;
-    FwdXLoad<T, TAB, Pre> src{a.tabdip, a.alpha, a.amode, (int)a.nmax, nx, pre, k * nx * ny + j0 * nx, nl, TL};
+    FwdXLoad<T, TAB, Pre> src{a.tab_of(rhs), a.alpha_of(rhs), a.amode, (int)a.nmax, nx, pre, k * nx * ny + j0 * nx,
+                              nl, TL};
     src.pre.bind(a, rhs);
     B1RowIO<T, L, TL> dst{a.B1 + rhs * a.g.b1_rhs + ((long)k * ny + j0) * L, nl, nz * ny * L};
     fft_tile<C, L, NB, NT, +1, typename TT::LayX>(sm, tw, src, dst);
@@ -389,7 +399,8 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a,
         const int il = threadIdx.x % TL;
         const int i = min(i0 + il, X - 1);
         const int qxc = i <= nx ? i : X - i;
-        const C* gsrc = a.Gc + qy * (nx + 1) + qxc;
+        // a ragged batch runs one right-hand side per block (rpb = 1)
+        const C* gsrc = (a.gc_r ? a.gc_r[blockIdx.z] : a.Gc) + qy * (nx + 1) + qxc;
         const int gcs = (int)a.g.gc_comp, qzs = (ny + 1) * (nx + 1);
         for (int cq = threadIdx.x / TL; cq < 6 * NQ; cq += NT / TL) {
             const int c6 = cq / NQ, qz = cq - c6 * NQ;
@@ -551,7 +562,7 @@ __global__ void __launch_bounds__(TT::NTX, TT::MINBX) k_inv_x(const MvArgs<T> a,
     pdl_wait();
     if (a.status && a.status[rhs]) return;
     B1RowIO<T, L, TL> src{a.B1 + rhs * a.g.b1_rhs + ((long)k * ny + j0) * L, nl, nz * ny * L};
-    InvXStore<T, TAB, Epi> dst{a.tabdip, a.b + rhs * a.xstride, a.y + rhs * a.xstride, a.inv_m, nx,
+    InvXStore<T, TAB, Epi> dst{a.tab_of(rhs), a.b + rhs * a.xstride, a.y + rhs * a.xstride, a.inv_m, nx,
                                k * nx * ny + j0 * nx, nl, TL, epi};
     dst.epi.bind(a, rhs);
     fft_tile<C, L, NB, NT, -1, typename TT::LayX>(sm, tw, src, dst);

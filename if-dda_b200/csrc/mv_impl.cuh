@@ -50,7 +50,7 @@ inline int zconv_rhs_per_block(long blocks_per_rhs, int nrhs) {
 template <class T, int L> void launch_zconv(const MvArgs<T>& a, int nrhs, cudaStream_t st) {
     using TT = MvTiles<T, L>;
     const int gx = (a.g.X + TT::TLZ - 1) / TT::TLZ, gy = a.g.ny + 1;
-    const int rpb = zconv_rhs_per_block((long)gx * gy, nrhs);
+    const int rpb = a.gc_r ? 1 : zconv_rhs_per_block((long)gx * gy, nrhs);
     dim3 grid(gx, gy, (nrhs + rpb - 1) / rpb);
     PassScope ps(PASS_ZCONV, TT::S, st);
     ensure_smem(k_zconv<T, L>, TT::smem_z);

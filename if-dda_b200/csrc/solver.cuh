@@ -24,7 +24,26 @@ struct SolveSpec {
     // mixed precision
     int max_outer = 12;
     double inner_floor = 1e-6;
+    // ragged batch (objects of different lattices on one common box, see
+    // MvArgs): per right-hand side spectra and offsets, device arrays; null
+    // when every right-hand side belongs to one object
+    const double2* const* gc64_r = nullptr;
+    const float2* const* gc32_r = nullptr;
+    const long* alpha_off = nullptr;
+    const long* tab_off = nullptr;
 };
+
+// a solver's mat-vec arguments carry the ragged-batch tables of its spec
+inline void set_ragged(MvArgs<double>& a, const SolveSpec& sp) {
+    a.gc_r = sp.gc64_r;
+    a.alpha_off = sp.alpha_off;
+    a.tab_off = sp.tab_off;
+}
+inline void set_ragged(MvArgs<float>& a, const SolveSpec& sp) {
+    a.gc_r = sp.gc32_r;
+    a.alpha_off = sp.alpha_off;
+    a.tab_off = sp.tab_off;
+}
 
 struct SolveResult {
     int status = 0;     // 1 converged, 0 not converged, -1 breakdown

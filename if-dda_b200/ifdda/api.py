@@ -93,6 +93,52 @@ class Context:
     def green(self, nx, ny, nz, aretecube, k0, nquad=0) -> "GreenSpectrum":
         return GreenSpectrum(self, nx, ny, nz, aretecube, k0, nquad)
 
+    def green_box(self, nx, ny, nz, box, aretecube, k0) -> "GreenSpectrum":
+        """Spectrum of an nx x ny x nz lattice on the larger box `box` (bx,
+        by, bz): the form every object of a ragged batch needs."""
+        return GreenSpectrum(self, nx, ny, nz, aretecube, k0, 0, box=box)
+
+    def inverserig_ragged(self, items, methodeit="GPBICG1", tol=1e-4, precision=IFDDA_FP64, maxit=0):
+        """Ragged batch: items = [(green, nbsphere, nmax, tabdip or None,
+        polarisa, FF0 (nrhs_i, 3 nbsphere))], every green from green_box on
+        one box.  Returns (per item (FF, FFloc), tol1, nloop, ncompte, nstop,
+        infostr) with the counters of every right-hand side in item order."""
+        n = len(items)
+        keep = []
+        ff0s, ffs, locs = [], [], []
+        for g, nb, nmax, tab, pol, ff0 in items:
+            f = _zc(ff0).reshape(-1, 3 * nb)
+            ff0s.append(f)
+            ffs.append(np.zeros_like(f))
+            locs.append(np.zeros_like(f))
+        R = sum(f.shape[0] for f in ff0s)
+        arr = lambda t, vals: (t * n)(*vals)
+        greens = arr(C.c_void_p, [it[0].h for it in items])
+        nrhs = arr(C.c_int, [f.shape[0] for f in ff0s])
+        nbs = arr(C.c_int, [int(it[1]) for it in items])
+        nmaxs = arr(C.c_int, [int(it[2]) for it in items])
+        tabs_np = [None if it[3] is None else np.ascontiguousarray(it[3], np.int32) for it in items]
+        pols_np = [_zc(it[4]) for it in items]
+        keep += tabs_np + pols_np
+        tabs = arr(C.c_void_p, [None if t is None else t.ctypes.data for t in tabs_np])
+        pols = arr(C.c_void_p, [p.ctypes.data for p in pols_np])
+        p_ff0 = arr(C.c_void_p, [f.ctypes.data for f in ff0s])
+        p_ff = arr(C.c_void_p, [f.ctypes.data for f in ffs])
+        p_loc = arr(C.c_void_p, [f.ctypes.data for f in locs])
+        tol1 = np.zeros(R)
+        nloop = np.zeros(R, np.int32)
+        ncompte = np.zeros(R, np.int32)
+        nstop = C.c_int(0)
+        info = C.create_string_buffer(b" " * 64, 65)
+        opt = SolveOptions(precision, 0, 0, 0.0, maxit)
+        rc = self.lib.ifdda_inverserig_ragged(n, greens, nrhs, nbs, nmaxs, tabs, pols, p_ff0, methodeit.encode(),
+                                              float(tol), p_ff, p_loc, _p(tol1), _p(nloop), _p(ncompte),
+                                              C.byref(nstop), info, C.byref(opt))
+        infostr = info.raw[:64].decode(errors="replace")
+        if rc == 1 and nstop.value == 0:
+            raise IfddaError(self.last_error() or infostr.strip())
+        return list(zip(ffs, locs)), tol1, nloop, ncompte, nstop.value, infostr
+
     # -- post-step ------------------------------------------------------
     def local_macro(self, nbsphere, nmax, epsilon, FFloc, aretecube, k0) -> np.ndarray:
         eps = _zc(epsilon)
@@ -210,15 +256,20 @@ class GreenSpectrum:
     """Device-resident Green spectrum of one lattice (greencalculfft) plus the
     solver workspace that uses it."""
 
-    def __init__(self, ctx: Context, nx, ny, nz, aretecube, k0, nquad=0):
+    def __init__(self, ctx: Context, nx, ny, nz, aretecube, k0, nquad=0, box=None):
         self.ctx = ctx
         self.lib = ctx.lib
         self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         self.aretecube, self.k0 = float(aretecube), float(k0)
         self.nquad = int(nquad)
         h = C.c_void_p()
-        rc = self.lib.ifdda_green_create_nquad(ctx.h, self.nx, self.ny, self.nz, self.aretecube, self.k0, self.nquad,
-                                               C.byref(h))
+        if box is not None:
+            bx, by, bz = (int(v) for v in box)
+            rc = self.lib.ifdda_green_create_box(ctx.h, self.nx, self.ny, self.nz, bx, by, bz, self.aretecube,
+                                                 self.k0, C.byref(h))
+        else:
+            rc = self.lib.ifdda_green_create_nquad(ctx.h, self.nx, self.ny, self.nz, self.aretecube, self.k0,
+                                                   self.nquad, C.byref(h))
         if rc != 0:
             raise IfddaError(ctx.last_error() or "ifdda_green_create failed")
         self.h = h

@@ -6,9 +6,19 @@ take the next request in arrival order as soon as they are free *and* the
 request's device footprint fits in the HBM budget next to the requests in
 flight; their solves then overlap on the GPU.  Each slot keeps an LRU cache of
 Green spectra keyed by (lattice, spacing, wavelength), so a repeated object
-size at the same wavelength skips the spectrum build.  Every request's result
-is computed by its own context with fixed-order reductions, so it is the same
-bit for bit alone and inside the mix.
+size at the same wavelength skips the spectrum build.
+
+With `ragged=True` a free slot also takes every other request that has
+arrived, whose object fits the head request's box (the smallest compiled box
+holding it, padded by at most `pad_ratio` in volume) and that fits the HBM
+budget, up to `max_batch_rhs` right-hand sides: they are solved as one ragged
+batch (ifdda_inverserig_ragged), one launch sequence per iteration for every
+right-hand side of every object, each object with its own spectrum, spacing,
+wavelength and polarisability.  A request's vectors are laid out on the box's
+sites, so its result does not depend on the requests it shares a batch with.
+
+Either way every request's result is computed with fixed-order reductions, so
+it is the same bit for bit alone and inside the mix.
 
 The reference solves one object at a time (cdmlib/cdmlib.f:3-60 called from
 the GUI's run thread, cdm/cdmRunWidget.cpp:162); this loop is the serving
@@ -70,6 +80,33 @@ def footprint_bytes(n: int, nrhs: int, precision: int) -> int:
     return green + scr64 + vec64 + io
 
 
+def ragged_footprint_bytes(box: int, nrhs: int, precision: int) -> int:
+    """Device bytes of nrhs right-hand sides in a ragged batch on a box of
+    side `box` (vectors on the box's sites), spectra not included."""
+    N = box ** 3
+    scr64 = 18 * N * 16 * nrhs
+    vec64 = 14 * 3 * N * 16 * nrhs
+    io = 3 * 3 * N * 16 * nrhs + 2 * N * 16
+    if precision == IFDDA_MIXED:
+        return scr64 + 18 * N * 8 * nrhs + 14 * 3 * N * 8 * nrhs + 2 * 3 * N * 16 * nrhs + io
+    return scr64 + vec64 + io
+
+
+def green_bytes(box: int) -> int:
+    return 6 * (box + 1) ** 3 * (16 + 8)
+
+
+COMPILED_SIDES = (1, 2, 3, 4, 5, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256, 320)
+
+
+def box_side(n: int) -> int:
+    """Smallest side >= n whose 2n is a compiled FFT length."""
+    for m in COMPILED_SIDES:
+        if m >= n:
+            return m
+    raise ValueError(f"lattice side {n} above 320")
+
+
 def make_stream(nreq: int, rate: float, seed: int = 4, edges=(16, 24, 32, 48, 64, 80, 96), max_inc: int = 32,
                 d: float = 10e-9):
     """Seeded synthetic request stream: Poisson arrivals at `rate` per second,
@@ -108,12 +145,15 @@ class _Slot:
         self.cache = collections.OrderedDict()
         self.cache_size = cache_size
 
-    def green(self, ob, k0):
-        key = (ob.nx, ob.ny, ob.nz, ob.aretecube, k0)
+    def green(self, ob, k0, box=None):
+        key = (ob.nx, ob.ny, ob.nz, ob.aretecube, k0, box)
         if key in self.cache:
             self.cache.move_to_end(key)
             return self.cache[key], True
-        g = self.ctx.green(ob.nx, ob.ny, ob.nz, ob.aretecube, k0)
+        if box is None:
+            g = self.ctx.green(ob.nx, ob.ny, ob.nz, ob.aretecube, k0)
+        else:
+            g = self.ctx.green_box(ob.nx, ob.ny, ob.nz, (box, box, box), ob.aretecube, k0)
         self.cache[key] = g
         while len(self.cache) > self.cache_size:
             _, old = self.cache.popitem(last=False)
@@ -142,16 +182,51 @@ def solve_request(slot: _Slot, req: Request, precision: int, tol: float = 1e-4, 
     return r, hit
 
 
+def solve_ragged(slot: _Slot, reqs, box: int, precision: int, tol: float = 1e-4, methodeit: str = "GPBICG1"):
+    """One ragged batch: every request's object on the common box side `box`.
+    Returns one (SolveResult-like dict, green_hit) per request."""
+    items, hits, shapes = [], [], []
+    for req in reqs:
+        ob, k0 = build_object(req)
+        E0, _ = objects.irradiance(1.0, 10 * req.wavelength)
+        kx = [a * k0 for a, _, _ in req.incidences]
+        ky = [b * k0 for _, b, _ in req.incidences]
+        pp = [c for _, _, c in req.incidences]
+        ff0 = slot.ctx.planewaves(ob.xs, ob.ys, ob.zs, k0, E0, [1] * len(kx), kx, ky, pp)
+        g, hit = slot.green(ob, k0, box)
+        items.append((g, ob.nbsphere, ob.nmax, ob.tabdip_or_none, ob.polarisa, ff0))
+        hits.append(hit)
+        shapes.append(len(kx))
+    fields, tol1, nloop, ncompte, nstop, info = slot.ctx.inverserig_ragged(items, methodeit, tol,
+                                                                           precision=precision)
+    items[0][0].release_workspace()
+    out, r0 = [], 0
+    for (FF, FFloc), nr, hit in zip(fields, shapes, hits):
+        sl = slice(r0, r0 + nr)
+        ok = bool(np.all(tol1[sl] < tol))
+        out.append((dict(FFloc=FFloc, tol1=tol1[sl].copy(), nloop=nloop[sl].copy(), ncompte=ncompte[sl].copy(),
+                         nstop=0 if (nstop == 0 or ok) else nstop, infostr=info), hit))
+        r0 += nr
+    return out
+
+
 class Server:
-    """Admission by HBM footprint + `slots` concurrent workers."""
+    """Admission by HBM footprint + `slots` concurrent workers; with `ragged`
+    each worker solves every compatible arrived request in one ragged batch."""
 
     def __init__(self, slots: int = 4, device: int = 0, hbm_budget: float = 120e9, precision: int = IFDDA_MIXED,
-                 cache_size: int = 4):
-        self.slots = [_Slot(i, device, cache_size) for i in range(slots)]
+                 cache_size: int = 4, ragged: bool = False, max_batch_rhs: int = 64, max_objects: int = 64,
+                 pad_ratio: float = 1.0):
+        self.slots = [_Slot(i, device, cache_size if not ragged else max(cache_size, max_objects))
+                      for i in range(slots)]
         self.budget = hbm_budget
         self.precision = precision
         self.in_use = 0.0
         self.cv = threading.Condition()
+        self.ragged = ragged
+        self.max_batch_rhs = max_batch_rhs
+        self.max_objects = max_objects
+        self.pad_ratio = pad_ratio
 
     def close(self):
         for s in self.slots:
@@ -184,6 +259,63 @@ class Server:
                     wait = max(0.0005, head.arrival - now) if not arrived else 0.05
                     self.cv.wait(timeout=wait)
 
+        def next_batch():
+            # the head request as above, then every arrived request that fits
+            # its box (volume padding <= pad_ratio), the budget and the caps
+            with self.cv:
+                while True:
+                    if not pending:
+                        return [], 0, 0.0
+                    head = pending[0]
+                    now = time.perf_counter() - t0
+                    box = box_side(head.n)
+                    fp = ragged_footprint_bytes(box, len(head.incidences), self.precision) + green_bytes(box)
+                    arrived = (not realtime) or head.arrival <= now
+                    fits = self.in_use + fp <= self.budget or self.in_use == 0
+                    if arrived and fits:
+                        break
+                    wait = max(0.0005, head.arrival - now) if not arrived else 0.05
+                    self.cv.wait(timeout=wait)
+                batch = [pending.popleft()]
+                nr = len(head.incidences)
+                keep = collections.deque()
+                while pending and len(batch) < self.max_objects:
+                    q = pending.popleft()
+                    if realtime and q.arrival > now:
+                        keep.append(q)
+                        break
+                    qfp = ragged_footprint_bytes(box, len(q.incidences), self.precision) + green_bytes(box)
+                    ok = (box_side(q.n) == box or (q.n <= box and box ** 3 <= self.pad_ratio * q.n ** 3))
+                    if ok and nr + len(q.incidences) <= self.max_batch_rhs and self.in_use + fp + qfp <= self.budget:
+                        batch.append(q)
+                        nr += len(q.incidences)
+                        fp += qfp
+                    else:
+                        keep.append(q)
+                while keep:
+                    pending.appendleft(keep.pop())
+                self.in_use += fp
+                return batch, box, fp
+
+        def worker_ragged(slot: _Slot):
+            while True:
+                batch, box, fp = next_batch()
+                if not batch:
+                    return
+                start = time.perf_counter() - t0
+                try:
+                    outs = solve_ragged(slot, batch, box, self.precision)
+                finally:
+                    with self.cv:
+                        self.in_use -= fp
+                        self.cv.notify_all()
+                end = time.perf_counter() - t0
+                with lock:
+                    for req, (r, hit) in zip(batch, outs):
+                        results[req.rid] = Result(req.rid, r["FFloc"], r["tol1"], r["nloop"], r["ncompte"],
+                                                  r["nstop"], r["infostr"], start, end,
+                                                  req.arrival if realtime else 0.0, slot.idx, hit)
+
         def worker(slot: _Slot):
             while True:
                 req, fp = next_request()
@@ -201,7 +333,8 @@ class Server:
                     results[req.rid] = Result(req.rid, r.FFloc, r.tol1, r.nloop, r.ncompte, r.nstop, r.infostr,
                                               start, end, req.arrival if realtime else 0.0, slot.idx, hit)
 
-        threads = [threading.Thread(target=worker, args=(s,), daemon=True) for s in self.slots]
+        target = worker_ragged if self.ragged else worker
+        threads = [threading.Thread(target=target, args=(s,), daemon=True) for s in self.slots]
         for th in threads:
             th.start()
         for th in threads:

@@ -75,6 +75,14 @@ int ifdda_green_create(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube,
    zero at the origin, the plain tensor beyond one wavelength. */
 int ifdda_green_create_nquad(ifdda_ctx* ctx, int nx, int ny, int nz, double aretecube, double k0, int nquad,
                              ifdda_green** out);
+/* Spectrum of an nx x ny x nz lattice computed on a given larger box
+   bx x by x bz (each side at least the lattice's, 2b a compiled FFT length),
+   the lattice at the box's corner: greencalculfft on the box.  Spectra of
+   different lattices, spacings and wavelengths made on one box can be solved
+   together by ifdda_inverserig_ragged.  No counterpart in the reference,
+   which solves one object per cdmlib call. */
+int ifdda_green_create_box(ifdda_ctx* ctx, int nx, int ny, int nz, int bx, int by, int bz, double aretecube,
+                           double k0, ifdda_green** out);
 /* Recomputes g's spectrum in place for another lattice spacing and
    wavenumber (same lattice sides, nquad and padding): the call cdmlib makes
    at cdmlib/cdmlib.f:1529-1531 on every run, writing greencalculfft's result
@@ -169,6 +177,28 @@ int ifdda_inverserig_batch_device(ifdda_green* g, int nrhs, int nbsphere, int nm
                                   const char* methodeit, double tol, ifdda_dcmplx* FF_dev, ifdda_dcmplx* FFloc_dev,
                                   double* tol1, int* nloop, int* ncompte, int* nstop, char* infostr,
                                   const ifdda_solve_options* opt);
+
+/* Ragged batch: nobj objects of uneven lattices, spacings and wavelengths,
+   object i with nrhs[i] right-hand sides, solved together in one launch
+   sequence per iteration (what the reference does as one cdmlib call per
+   object, cdmlib/cdmlib.f:1565-1581, each a serial incidence loop as in
+   cdmlib/microsbf.f:214-280).  greens[i] is object i's spectrum, every one
+   made by ifdda_green_create_box on the same box and context; the first
+   one's workspaces hold the batch.  Object i: nbsphere[i] dipoles, nmax[i],
+   tabdip[i] on its own lattice (tabdip may be NULL, or tabdip[i] NULL for a
+   full box), polarisa[i] (nmax[i],3,3) isotropic, FF0[i] / FF[i] / FFloc[i]
+   nrhs[i] vectors of 3*nbsphere[i].  tol1, nloop, ncompte hold one entry per
+   right-hand side, objects in order; nstop / infostr report the first
+   failing one.  Every right-hand side is laid out on the box's sites, so its
+   result does not depend on the other objects of the batch: bit for bit the
+   same alone (nobj = 1) and in any batch on that box, and the solo solve's
+   (ifdda_inverserig) up to rounding.  QMRCLA and anisotropic tensors return
+   1. */
+int ifdda_inverserig_ragged(int nobj, ifdda_green* const* greens, const int* nrhs, const int* nbsphere,
+                            const int* nmax, const int* const* tabdip, const ifdda_dcmplx* const* polarisa,
+                            const ifdda_dcmplx* const* FF0, const char* methodeit, double tol, ifdda_dcmplx* const* FF,
+                            ifdda_dcmplx* const* FFloc, double* tol1, int* nloop, int* ncompte, int* nstop,
+                            char* infostr, const ifdda_solve_options* opt);
 
 /* Local -> macroscopic field of every dipole (nsens = 1), replacing the loop
    of cdmlib/cdmlib.f:2595-2655 over local_macro (cdmlib/local-macro.f:3-71);

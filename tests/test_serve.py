@@ -1,8 +1,12 @@
 """GPU: the continuous-batching server gives each request the same result
 alone and inside a concurrent mix (own context per slot, fixed-order
-reductions), and every request converges to the FP64 true residual."""
+reductions), every request converges to the FP64 true residual, small
+requests match the oracle's solve of the same object, and the HBM footprint
+the admission uses covers what a request really holds on the device."""
 import numpy as np
 import pytest
+
+from cases import rel
 
 pytestmark = pytest.mark.gpu
 
@@ -24,6 +28,101 @@ def test_results_identical_alone_and_in_the_mix():
         assert np.array_equal(a.FFloc, b.FFloc)
         assert np.array_equal(a.nloop, b.nloop)
         assert np.all(b.tol1 < 1e-4)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_ragged_serving_identical_alone_and_in_batches(prec):
+    """Ragged serving: requests of several sizes batched per box (16, 24
+    and 32 sides, a 12 side padded into 16), each request alone (batches of
+    one object) against the mix (up to 8 objects per ragged batch): bit for
+    bit the same fields and counters."""
+    from ifdda import serve
+    reqs = serve.make_stream(12, rate=1000.0, seed=13, edges=(12, 16, 24, 32), max_inc=3)
+    alone = serve.Server(slots=1, precision=prec, ragged=True, max_objects=1, pad_ratio=2.5)
+    ra = alone.run(reqs, realtime=False)
+    alone.close()
+    mix = serve.Server(slots=2, precision=prec, ragged=True, max_objects=8, pad_ratio=2.5)
+    rm = mix.run(reqs, realtime=False)
+    mix.close()
+    assert len(ra) == len(rm) == len(reqs)
+    groups = {}
+    for r in rm:
+        groups.setdefault((r.slot, r.start), []).append(r.rid)
+    assert max(len(v) for v in groups.values()) > 1  # some batch held several objects
+    for a, b in zip(ra, rm):
+        assert a.rid == b.rid and a.nstop == b.nstop == 0, (a.infostr, b.infostr)
+        assert np.array_equal(a.FFloc, b.FFloc)
+        assert np.array_equal(a.ncompte, b.ncompte)
+        assert np.all(b.tol1 < 1e-4)
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_served_requests_match_the_oracle(orc, prec):
+    """Three small requests (sphere and cube, several incidences) served in a
+    mix; each right-hand side's local field against the oracle's inverserig
+    of the same object and incident field.  FP64 requests reproduce the
+    oracle's counters and field (1e-7); for mixed ones the oracle's own
+    operator (the produitfftmatvect3 restatement) confirms the true residual
+    ||E - G alpha E - E0|| / ||E0|| <= 1e-4."""
+    from ifdda import objects, serve
+    reqs = serve.make_stream(3, rate=1000.0, seed=21, edges=(12, 16), max_inc=3)
+    srv = serve.Server(slots=2, precision=prec)
+    res = srv.run(reqs, realtime=False)
+    srv.close()
+    for req, r in zip(reqs, res):
+        ob, k0 = serve.build_object(req)
+        E0, _ = objects.irradiance(1.0, 10 * req.wavelength)
+        G6 = orc.greencalculfft(ob.nx, ob.ny, ob.nz, ob.aretecube, k0)
+        floc = np.asarray(r.FFloc).reshape(len(req.incidences), -1)
+        for q, (a, b, pp) in enumerate(req.incidences):
+            ff0 = orc.incident(ob.xs, ob.ys, ob.zs, k0, E0, pp, 1, a * k0, b * k0)
+            ref = orc.inverserig(G6, ob.nx, ob.ny, ob.nz, ob.nbsphere, ob.polarisa, ob.nmax, ff0, "GPBICG1", 1e-4,
+                                 tabdip=ob.tabdip_or_none)
+            assert ref["nstop"] == 0 and r.nstop == 0
+            if prec == 0:
+                assert int(np.atleast_1d(r.ncompte)[q]) == ref["ncompte"]
+                assert rel(floc[q], ref["FFloc"]) < 1e-7
+            else:
+                E = floc[q]
+                p = np.repeat(ob.alpha, 3) * E  # isotropic: FF = alpha E per dipole
+                AE = orc.matvec(G6, ob.nx, ob.ny, ob.nz, p, E, tabdip=ob.tabdip_or_none)
+                assert np.linalg.norm(AE - ff0) / np.linalg.norm(ff0) <= 1e-4
+
+
+def _pool():
+    from cuda.bindings import driver
+    assert driver.cuInit(0)[0] == driver.CUresult.CUDA_SUCCESS
+    err, d = driver.cuDeviceGet(0)
+    err, pool = driver.cuDeviceGetDefaultMemPool(d)
+    assert err == driver.CUresult.CUDA_SUCCESS
+    return driver, pool
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_footprint_covers_the_device_memory_of_a_request(prec):
+    """footprint_bytes (the admission's estimate) against the high-water mark
+    of the device memory pool, from which the library takes every workspace,
+    over one request's Green build and solve: the estimate is an upper bound,
+    and no more than 3x the real use."""
+    from ifdda import serve
+    driver, pool = _pool()
+    A = driver.CUmemPool_attribute
+    for n, ninc in ((24, 4), (48, 8)):
+        req = serve.Request(rid=0, shape="cube", n=n, d=10e-9, eps=2.5 + 0.1j, wavelength=600e-9,
+                            incidences=[(0.1 * i, 0.05 * i, float(i % 2)) for i in range(ninc)])
+        slot = serve._Slot(0, 0, cache_size=1)
+        slot.ctx.synchronize()
+        base = int(driver.cuMemPoolGetAttribute(pool, A.CU_MEMPOOL_ATTR_USED_MEM_CURRENT)[1])
+        assert driver.cuMemPoolSetAttribute(pool, A.CU_MEMPOOL_ATTR_USED_MEM_HIGH, driver.cuuint64_t(0))[0] == \
+            driver.CUresult.CUDA_SUCCESS
+        r, hit = serve.solve_request(slot, req, prec)
+        slot.ctx.synchronize()
+        high = int(driver.cuMemPoolGetAttribute(pool, A.CU_MEMPOOL_ATTR_USED_MEM_HIGH)[1])
+        slot.close()
+        assert r.nstop == 0 and not hit
+        used = high - base
+        fp = serve.footprint_bytes(n, ninc, prec)
+        assert used <= fp <= 3 * used, (n, ninc, used, fp)
 
 
 def test_admission_respects_the_hbm_budget():
