@@ -367,11 +367,13 @@ template <class LZ> constexpr int zmid_cost(int order, int TL, int NJ, int RK, i
 // transform run on the reversed plan, so the inverse starts from the values
 // the forward one ended with (its pass 0 reads exactly the points
 // j + r L/R the forward last pass produced), then inverse passes 1 .. n-1.
-// A block keeps its slice of the spectrum in shared memory and convolves the
-// right-hand sides rpb * blockIdx.z .. + rpb - 1 in turn, so a batch reads
-// each spectrum value once per rpb right-hand sides.
+// Grid (right-hand side, column tile, mirror-row pair): the right-hand side
+// varies fastest, so the blocks that read one slice of the spectrum run
+// together and a batch takes that slice from HBM once (L2 serves the rest).
+// (A loop over right-hand sides inside the block, keeping the slice in shared
+// memory, needs about twice the registers and spills.)
 template <class T, int L, class TT = MvTiles<T, L>>
-__global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a, const int nrhs, const int rpb) {
+__global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a) {
     using C = cplx<T>;
     using LZ = typename TT::LayZ;
     constexpr int TL = TT::TLZ, NB = TT::NBZ, NT = TT::NTZ;
@@ -383,12 +385,13 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a,
     constexpr int S = (int)sizeof(C);
     constexpr int ORDER = zmid_cost<LZ>(1, TL, NJ, RK, NG, S) < zmid_cost<LZ>(0, TL, NJ, RK, NG, S) ? 1 : 0;
     constexpr int NQ = L / 2 + 1;
+    const int rhs = blockIdx.x;
     C* tw = smem_base<C>();
     C* sm = tw + L;
     C* gs = sm + LZ::span(L) * TT::PSZ;
     const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz, X = a.g.X, Y = a.g.Y;
-    const int i0 = blockIdx.x * TL;
-    const int qy = blockIdx.y;                    // 0 .. ny
+    const int i0 = blockIdx.y * TL;
+    const int qy = blockIdx.z;                    // 0 .. ny
     const int two = (qy > 0 && qy < ny) ? 2 : 1;  // rows qy and Y - qy
     load_twiddles<C, L, NT>(tw, a.twz);
     // this block's slice of the compressed spectrum (qy fixed, every qz, the
@@ -399,8 +402,7 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a,
         const int il = threadIdx.x % TL;
         const int i = min(i0 + il, X - 1);
         const int qxc = i <= nx ? i : X - i;
-        // a ragged batch runs one right-hand side per block (rpb = 1)
-        const C* gsrc = (a.gc_r ? a.gc_r[blockIdx.z] : a.Gc) + qy * (nx + 1) + qxc;
+        const C* gsrc = (a.gc_r ? a.gc_r[rhs] : a.Gc) + qy * (nx + 1) + qxc;
         const int gcs = (int)a.g.gc_comp, qzs = (ny + 1) * (nx + 1);
         for (int cq = threadIdx.x / TL; cq < 6 * NQ; cq += NT / TL) {
             const int c6 = cq / NQ, qz = cq - c6 * NQ;
@@ -411,11 +413,10 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a,
     // the spectrum and the twiddles are constant: only B2 waits for the y pass
     pdl_trigger();
     pdl_wait();
-    const int r1 = min(nrhs, (int)(blockIdx.z + 1) * rpb);
-    for (int rhs = blockIdx.z * rpb; rhs < r1; rhs++) {
-    // the status is the same for every thread of the block
-    if (a.status && a.status[rhs]) continue;
-    __syncthreads();  // the previous right-hand side's last reads of the tile are done
+    if (a.status && a.status[rhs]) {
+        cp_async_wait_all();
+        return;
+    }
     C* B2 = a.B2 + rhs * a.g.b2_rhs + (long)qy * X + i0;
     const int rs = Y * X, comp = nz * Y * X, drow = (Y - 2 * qy) * X, nv = min(TL, X - i0);
     const ZLoad<T, TL> zload{B2, rs, comp, drow, nv, two};
@@ -505,8 +506,6 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a,
         __syncthreads();
         stockham_range<C, L, NB, NT, -1, LZ, true, NP, 1, RK>(sm, tw, SmemIO{}, zstore);
     }
-    }  // right-hand sides
-    cp_async_wait_all();  // every right-hand side may have been finished already
 }
 
 // ---- pass 5 -----------------------------------------------------------------

@@ -35,26 +35,12 @@ template <class T, int L, int DIR> void launch_pass_y(const MvArgs<T>& a, int nr
     launch_pdl(k_pass_y<T, L, DIR>, grid, TT::NTY, TT::smem_y, st, a);
 }
 
-// right-hand sides per zconv block: a batch shares each block's spectrum
-// slice across up to 32 right-hand sides while the grid keeps about 8
-// blocks per SM
-inline int zconv_rhs_per_block(long blocks_per_rhs, int nrhs) {
-    const long want = 148L * 8;
-    long r = blocks_per_rhs * nrhs / want;
-    if (r < 1) r = 1;
-    if (r > 32) r = 32;
-    if (r > nrhs) r = nrhs;
-    return (int)r;
-}
-
 template <class T, int L> void launch_zconv(const MvArgs<T>& a, int nrhs, cudaStream_t st) {
     using TT = MvTiles<T, L>;
-    const int gx = (a.g.X + TT::TLZ - 1) / TT::TLZ, gy = a.g.ny + 1;
-    const int rpb = a.gc_r ? 1 : zconv_rhs_per_block((long)gx * gy, nrhs);
-    dim3 grid(gx, gy, (nrhs + rpb - 1) / rpb);
+    dim3 grid(nrhs, (a.g.X + TT::TLZ - 1) / TT::TLZ, a.g.ny + 1);
     PassScope ps(PASS_ZCONV, TT::S, st);
     ensure_smem(k_zconv<T, L>, TT::smem_z);
-    launch_pdl(k_zconv<T, L>, grid, TT::NTZ, TT::smem_z, st, a, nrhs, rpb);
+    launch_pdl(k_zconv<T, L>, grid, TT::NTZ, TT::smem_z, st, a);
 }
 
 template <class T, int L, class Epi>
