@@ -386,6 +386,39 @@ int ifdda_green_create_box(ifdda_ctx* ctx, int nx, int ny, int nz, int bx, int b
     IFDDA_GUARD_END(ctx, nullptr)
 }
 
+int ifdda_green_tiles(ifdda_green* g, int precision, int nrhs, int* zconv_variant, int* ypass_variant,
+                      float* times_ms) {
+    if (!g || nrhs < 1 || (precision != IFDDA_FP32 && precision != IFDDA_FP64)) return 1;
+    auto it = g->G.tiles.find({precision == IFDDA_FP32 ? 1 : 0, nrhs});
+    const bool have = it != g->G.tiles.end();
+    if (zconv_variant) *zconv_variant = have ? it->second.zvar : -1;
+    if (ypass_variant) *ypass_variant = have ? it->second.yvar : -1;
+    if (times_ms)
+        for (int v = 0; v < 2; v++) {
+            times_ms[v] = have ? it->second.z_ms[v] : 0.f;
+            times_ms[2 + v] = have ? it->second.y_ms[v] : 0.f;
+        }
+    return 0;
+}
+
+int ifdda_green_set_tiles(ifdda_green* g, int precision, int nrhs, int zconv_variant, int ypass_variant) {
+    if (!g || nrhs < 1 || (precision != IFDDA_FP32 && precision != IFDDA_FP64)) return 1;
+    const std::pair<int, int> key{precision == IFDDA_FP32 ? 1 : 0, nrhs};
+    if (zconv_variant < 0 || ypass_variant < 0) {
+        g->G.tiles.erase(key);
+        return 0;
+    }
+    if (zconv_variant >= tile_variants(g->G.g.Z) || ypass_variant >= tile_variants(g->G.g.Y)) {
+        g->ctx->last_error = "ifdda_green_set_tiles: no such tile variant for this grid";
+        return 1;
+    }
+    TileChoice tc{};
+    tc.zvar = zconv_variant;
+    tc.yvar = ypass_variant;
+    g->G.tiles[key] = tc;
+    return 0;
+}
+
 int ifdda_green_recompute(ifdda_green* g, double aretecube, double k0) {
     if (!g) return 1;
     IFDDA_GUARD_BEGIN
@@ -484,6 +517,7 @@ int ifdda_matvec(ifdda_green* g, int precision, int ndip, const int* tabdip, con
     IFDDA_CUDA(cudaMemcpyAsync(g->ffx.p, FFX, n3 * sizeof(double2), cudaMemcpyHostToDevice, st));
     IFDDA_CUDA(cudaMemcpyAsync(g->ffb.p, FFB, n3 * sizeof(double2), cudaMemcpyHostToDevice, st));
     if (precision == IFDDA_FP32) {
+        tune_tiles<float>(g->G, 1, st);
         g->ffx32.ensure(n3);
         g->ffb32.ensure(n3);
         cast_dev<float>(g->ffx.p, g->ffx32.p, n3, st);
@@ -496,6 +530,7 @@ int ifdda_matvec(ifdda_green* g, int precision, int ndip, const int* tabdip, con
         IFDDA_CUDA(cudaStreamSynchronize(st));
         for (long i = 0; i < n3; i++) FFB[i] = ifdda_dcmplx{h[i].x, h[i].y};
     } else {
+        tune_tiles<double>(g->G, 1, st);
         MvArgs<double> a = mv_args<double>(g->G, 1, g->ffx.p, g->ffb.p, g->ffb.p, n3, ALPHA_NONE, nullptr, 0, tab,
                                            nullptr);
         if (!matvec_launch<double>(a, 1, tab != nullptr, st)) throw EngineError{1, "FFT size not supported"};
@@ -520,10 +555,12 @@ int ifdda_matvec_device(ifdda_green* g, int precision, int nrhs, int ndip, const
     tabdip_dev = lattice_tab(g, tabdip_dev, st);
     bool ok;
     if (precision == IFDDA_FP32) {
+        tune_tiles<float>(g->G, nrhs, st);
         MvArgs<float> a = mv_args<float>(g->G, nrhs, (const float2*)FFX_dev, (const float2*)FFB_dev, (float2*)FFB_dev,
                                          n3, ALPHA_NONE, nullptr, 0, tabdip_dev, nullptr);
         ok = matvec_launch<float>(a, nrhs, tabdip_dev != nullptr, st);
     } else {
+        tune_tiles<double>(g->G, nrhs, st);
         MvArgs<double> a = mv_args<double>(g->G, nrhs, (const double2*)FFX_dev, (const double2*)FFB_dev,
                                            (double2*)FFB_dev, n3, ALPHA_NONE, nullptr, 0, tabdip_dev, nullptr);
         ok = matvec_launch<double>(a, nrhs, tabdip_dev != nullptr, st);

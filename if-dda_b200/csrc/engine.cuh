@@ -7,6 +7,7 @@
 #include <atomic>
 #include <mutex>
 #include <unordered_map>
+#include <map>
 #include <utility>
 #include "instrument.cuh"
 #include "matvec_kernels.cuh"
@@ -116,6 +117,13 @@ template <class T> struct MvWork {
     }
 };
 
+// Tile variants chosen by the tile chooser for one (precision, batch), with
+// the times it measured (ms; 0 where a variant was not timed).
+struct TileChoice {
+    int zvar = 0, yvar = 0;
+    float z_ms[2] = {0, 0}, y_ms[2] = {0, 0};
+};
+
 // Green spectrum of one (lattice, spacing, wavenumber), device resident.
 struct Green {
     int device = 0;
@@ -133,6 +141,12 @@ struct Green {
     DevBuf<float2> tw32[3];
     MvWork<float> w32;
     MvWork<double> w64;
+    // tile chooser's result per (precision: 0 FP64, 1 FP32; right-hand sides)
+    std::map<std::pair<int, int>, TileChoice> tiles;
+    template <class T> const TileChoice* tile_choice(int nrhs) const {
+        auto it = tiles.find({sizeof(T) == 4 ? 1 : 0, nrhs});
+        return it == tiles.end() ? nullptr : &it->second;
+    }
     template <class T> const cplx<T>* gc() const;
     template <class T> const cplx<T>* tw(int axis) const;
     template <class T> MvWork<T>& work();
@@ -192,7 +206,14 @@ MvArgs<T> mv_args(Green& G, int nrhs, const cplx<T>* x, const cplx<T>* b, cplx<T
     a.twz = G.tw<T>(2);
     a.status = status;
     a.inv_m = (T)(1.0 / ((double)G.g.X * G.g.Y * G.g.Z));
+    if (const TileChoice* tc = G.tile_choice<T>(nrhs)) {
+        a.zvar = tc->zvar;
+        a.yvar = tc->yvar;
+    }
     return a;
 }
+
+// time the tile variants for (T, nrhs) on G's grid once, see mv_impl.cuh
+template <class T> void tune_tiles(Green& G, int nrhs, cudaStream_t st);
 
 }  // namespace ifdda

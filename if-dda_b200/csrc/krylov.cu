@@ -445,7 +445,10 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
         key = {V.base, sp.alpha, sp.tabdip, G.gc<T>(), mw.B1.p, mw.B2.p, W.partials.p, W.tickets.p, status, S,
                W.mvpart.p, W.mvtk.p, W.loopcount.p, (const void*)(long)fused,
                (const void*)(long)sp.method, (const void*)(long)nrhs, (const void*)n3, (const void*)(long)sp.amode,
-               (const void*)sp.nmax, (const void*)(long)nblk, sp.gc64_r, sp.gc32_r, sp.alpha_off, sp.tab_off};
+               (const void*)sp.nmax, (const void*)(long)nblk, sp.gc64_r, sp.gc32_r, sp.alpha_off, sp.tab_off,
+               (const void*)(long)(G.tile_choice<T>(nrhs) ? 1 + G.tile_choice<T>(nrhs)->zvar +
+                                                                2 * G.tile_choice<T>(nrhs)->yvar
+                                                          : 0)};
     }
     const bool cached = graphs && W.graph.exec && W.graph.key == key;
     // without a loop captured for these buffers, the first two iterations run
@@ -648,6 +651,7 @@ template bool krylov_run<double>(Green&, const SolveSpec&, KrylovWork<double>&, 
 void solve_fp64(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b_dev, double2* x_out, std::vector<SolveResult>& res,
                 cudaStream_t st) {
     KrylovWork<double>& W = SW.kw64;
+    tune_tiles<double>(G, sp.nrhs, st);
     W.ensure(sp.method, sp.nrhs, sp.n3);
     // a ragged batch pads shorter objects' vectors with entries no kernel
     // writes: they start at zero and stay zero
@@ -713,6 +717,8 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
     M.partials.ensure((size_t)nrhs * reduction_blocks(n3) * 4);
     M.tickets.ensure(nrhs);
     KrylovWork<float>& W = SW.kw32;
+    tune_tiles<double>(G, nrhs, st);
+    tune_tiles<float>(G, nrhs, st);
     W.ensure(sp.method, nrhs, n3);
     if (sp.tab_off) {  // ragged batch: padding entries start at zero (see solve_fp64)
         IFDDA_CUDA(cudaMemsetAsync(W.vecs.p, 0, W.vecs.n * sizeof(float2), st));

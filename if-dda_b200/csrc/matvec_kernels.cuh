@@ -63,6 +63,7 @@ template <class T> struct MvArgs {
     const C* twz;
     const int* status;   // per rhs: nonzero -> skip (solve finished)
     T inv_m;             // 1 / (X Y Z)
+    int zvar, yvar;      // tile variants of zconv and of the y passes (MvTiles V)
     // Ragged batch (objects of different lattices, spacings and wavelengths
     // on one common box): per right-hand side, its object's spectrum and the
     // offsets of its polarisability (dipoles) and Tabdip (box sites) in the
@@ -85,11 +86,18 @@ template <class T> struct MvArgs {
 //  * zconv: as many columns as fit in ~80 KB (FP32) / ~160 KB (FP64) of
 //    shared memory, so that two blocks (FP32) share an SM, and a register
 //    cap near 72 (FP32) / 168 (FP64) to keep more blocks resident.
-template <class T, int L> struct MvTiles {
+//
+// Variant V = 1 (compiled for lengths of 64 and more, where the grid is large
+// enough for the choice to matter) halves the zconv and y tiles; the tile
+// chooser (tune_tiles) times both on the caller's grid and batch and keeps
+// the faster.  A line's arithmetic does not depend on the tile, so both give
+// the same bits.
+constexpr int tile_variants(int L) { return L >= 64 ? 2 : 1; }
+template <class T, int L, int V = 0> struct MvTiles {
     static constexpr int S = (int)sizeof(cplx<T>);
     static constexpr int SMEM_X = 16384;
     static constexpr int TLX = clamp_pow2(SMEM_X / (3 * (L + 1) * S), 1, 16);
-    static constexpr int TLY = 16;
+    static constexpr int TLY = V ? 8 : 16;
     static constexpr int NBX = 3 * TLX, NBY = TLY;
     // x tile: points contiguous with one pad word every 16, line pitch = 8 (mod 16)
     static constexpr int lpitch() {
@@ -118,7 +126,7 @@ template <class T, int L> struct MvTiles {
     static constexpr int ztile() {
         int tl = 16;
         while (tl > 1 && zbytes(tl) > (size_t)80 * 1024 * (S / 8)) tl /= 2;
-        return tl;
+        return V && tl > 1 ? tl / 2 : tl;
     }
     static constexpr int TLZ = ztile(), NBZ = 6 * TLZ;
     // y tile: odd point stride; z tile: point stride NBZ with one pad point every 16

@@ -3,6 +3,7 @@
 #include "gpbicg_fused.cuh"
 
 namespace ifdda {
+template <> void tune_tiles<float>(Green& G, int nrhs, cudaStream_t st) { tune_tiles_impl<float>(G, nrhs, st); }
 template <> bool matvec_launch<float>(const MvArgs<float>& a, int nrhs, bool tab, cudaStream_t st) {
     return matvec_launch_fused<float, PreNone<float>, EpiNone>(a, PreNone<float>{}, EpiNone{}, MvRed{}, nrhs, tab, st);
 }

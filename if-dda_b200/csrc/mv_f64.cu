@@ -3,6 +3,7 @@
 #include "gpbicg_fused.cuh"
 
 namespace ifdda {
+template <> void tune_tiles<double>(Green& G, int nrhs, cudaStream_t st) { tune_tiles_impl<double>(G, nrhs, st); }
 template <> bool matvec_launch<double>(const MvArgs<double>& a, int nrhs, bool tab, cudaStream_t st) {
     return matvec_launch_fused<double, PreNone<double>, EpiNone>(a, PreNone<double>{}, EpiNone{}, MvRed{}, nrhs, tab, st);
 }

@@ -27,20 +27,32 @@ void launch_fwd_x(const MvArgs<T>& a, const Pre& pre, const MvRed& red, int nrhs
     }
 }
 
-template <class T, int L, int DIR> void launch_pass_y(const MvArgs<T>& a, int nrhs, cudaStream_t st) {
-    using TT = MvTiles<T, L>;
+template <class T, int L, int DIR, int V> void launch_pass_y_v(const MvArgs<T>& a, int nrhs, cudaStream_t st) {
+    using TT = MvTiles<T, L, V>;
     dim3 grid((a.g.X + TT::TLY - 1) / TT::TLY, a.g.nz, 3 * nrhs);
     PassScope ps(DIR > 0 ? PASS_FWD_Y : PASS_INV_Y, TT::S, st);
-    ensure_smem(k_pass_y<T, L, DIR>, TT::smem_y);
-    launch_pdl(k_pass_y<T, L, DIR>, grid, TT::NTY, TT::smem_y, st, a);
+    ensure_smem(k_pass_y<T, L, DIR, TT>, TT::smem_y);
+    launch_pdl(k_pass_y<T, L, DIR, TT>, grid, TT::NTY, TT::smem_y, st, a);
+}
+template <class T, int L, int DIR> void launch_pass_y(const MvArgs<T>& a, int nrhs, cudaStream_t st) {
+    if constexpr (tile_variants(L) > 1) {
+        if (a.yvar == 1) return launch_pass_y_v<T, L, DIR, 1>(a, nrhs, st);
+    }
+    launch_pass_y_v<T, L, DIR, 0>(a, nrhs, st);
 }
 
-template <class T, int L> void launch_zconv(const MvArgs<T>& a, int nrhs, cudaStream_t st) {
-    using TT = MvTiles<T, L>;
+template <class T, int L, int V> void launch_zconv_v(const MvArgs<T>& a, int nrhs, cudaStream_t st) {
+    using TT = MvTiles<T, L, V>;
     dim3 grid(nrhs, (a.g.X + TT::TLZ - 1) / TT::TLZ, a.g.ny + 1);
     PassScope ps(PASS_ZCONV, TT::S, st);
-    ensure_smem(k_zconv<T, L>, TT::smem_z);
-    launch_pdl(k_zconv<T, L>, grid, TT::NTZ, TT::smem_z, st, a);
+    ensure_smem(k_zconv<T, L, TT>, TT::smem_z);
+    launch_pdl(k_zconv<T, L, TT>, grid, TT::NTZ, TT::smem_z, st, a);
+}
+template <class T, int L> void launch_zconv(const MvArgs<T>& a, int nrhs, cudaStream_t st) {
+    if constexpr (tile_variants(L) > 1) {
+        if (a.zvar == 1) return launch_zconv_v<T, L, 1>(a, nrhs, st);
+    }
+    launch_zconv_v<T, L, 0>(a, nrhs, st);
 }
 
 template <class T, int L, class Epi>
@@ -85,6 +97,62 @@ bool matvec_launch_fused(const MvArgs<T>& a, const Pre& pre, const Epi& epi, con
     switch (a.g.X) { IFDDA_FFT_LENGTHS(IFDDA_CASE_INVX) default: return false; }
     IFDDA_CUDA(cudaGetLastError());
     return true;
+}
+
+#define IFDDA_CASE_TY(L) \
+    case L: launch_pass_y<T, L, +1>(a, nrhs, st); launch_pass_y<T, L, -1>(a, nrhs, st); break;
+#define IFDDA_CASE_TZ(L) \
+    case L: launch_zconv<T, L>(a, nrhs, st); break;
+
+// Tile chooser: with G's mat-vec scratch for nrhs right-hand sides (whose
+// contents are about to be overwritten by the next mat-vec anyway), time each
+// tile variant of the y passes (forward then inverse) and of zconv, best of
+// three launches with CUDA events on st, and record the faster in G for
+// (precision, nrhs).  Never runs while st is being captured.
+template <class T> void tune_tiles_impl(Green& G, int nrhs, cudaStream_t st) {
+    const int pk = sizeof(T) == 4 ? 1 : 0;
+    if (G.tiles.count({pk, nrhs})) return;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    IFDDA_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return;
+    MvArgs<T> a = mv_args<T>(G, nrhs, nullptr, nullptr, nullptr, 0, ALPHA_NONE, nullptr, 0, nullptr, nullptr);
+    TileChoice tc{};
+    const int nyv = tile_variants(G.g.Y), nzv = tile_variants(G.g.Z);
+    if (nyv > 1 || nzv > 1) {
+        cudaEvent_t e0, e1;
+        IFDDA_CUDA(cudaEventCreate(&e0));
+        IFDDA_CUDA(cudaEventCreate(&e1));
+        auto time_it = [&](auto&& launch) {
+            float best = 1e30f;
+            for (int r = 0; r < 4; r++) {
+                IFDDA_CUDA(cudaEventRecord(e0, st));
+                launch();
+                IFDDA_CUDA(cudaEventRecord(e1, st));
+                IFDDA_CUDA(cudaEventSynchronize(e1));
+                float ms = 0;
+                IFDDA_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                if (r > 0) best = ms < best ? ms : best;  // the first launch sets up the kernel
+            }
+            return best;
+        };
+        for (int v = 0; v < nyv; v++) {
+            a.yvar = v;
+            tc.y_ms[v] = time_it([&] {
+                switch (G.g.Y) { IFDDA_FFT_LENGTHS(IFDDA_CASE_TY) default: break; }
+            });
+            if (tc.y_ms[v] < tc.y_ms[tc.yvar]) tc.yvar = v;
+        }
+        for (int v = 0; v < nzv; v++) {
+            a.zvar = v;
+            tc.z_ms[v] = time_it([&] {
+                switch (G.g.Z) { IFDDA_FFT_LENGTHS(IFDDA_CASE_TZ) default: break; }
+            });
+            if (tc.z_ms[v] < tc.z_ms[tc.zvar]) tc.zvar = v;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    G.tiles[{pk, nrhs}] = tc;
 }
 
 }  // namespace ifdda

@@ -55,6 +55,37 @@ def test_green_recompute_matches_a_new_spectrum(gctx, orc):
     g.close()
 
 
+def test_tile_chooser_variants_give_the_same_bits(gctx, orc):
+    """Both tile shapes of zconv and of the y passes give bit-identical
+    mat-vecs (a line's arithmetic does not depend on the tile), the chooser
+    times both on first use and keeps one, and the result matches the oracle."""
+    from ifdda import IFDDA_FP32, IFDDA_FP64
+    nx, ny, nz = 40, 32, 48  # FFT lengths 80, 64, 96: two variants on every axis
+    d, k0 = 10e-9, 2 * math.pi / 500e-9
+    N = nx * ny * nz
+    x, b = random_field(3 * N, 7), random_field(3 * N, 8)
+    g = gctx.green(nx, ny, nz, d, k0)
+    ref = orc.matvec(orc.greencalculfft(nx, ny, nz, d, k0), nx, ny, nz, x, b)
+    for prec, tol in ((IFDDA_FP64, 1e-11), (IFDDA_FP32, 2e-5)):
+        assert g.tiles(prec, 1)[:2] == (-1, -1)
+        outs = []
+        for zv, yv in ((0, 0), (1, 1), (0, 1), (1, 0)):
+            g.set_tiles(prec, 1, zv, yv)
+            assert g.tiles(prec, 1)[:2] == (zv, yv)
+            outs.append(g.matvec(x, b, precision=prec))
+        for o in outs[1:]:
+            assert np.array_equal(o, outs[0])
+        g.set_tiles(prec, 1, -1, -1)
+        got = g.matvec(x, b, precision=prec)
+        zv, yv, t = g.tiles(prec, 1)
+        assert zv in (0, 1) and yv in (0, 1) and min(t) > 0
+        assert np.array_equal(got, outs[0]) and rel(got, ref) < tol
+    import ifdda
+    with pytest.raises(ifdda.IfddaError):
+        gctx.green(4, 4, 4, d, k0).set_tiles(IFDDA_FP64, 1, 1, 0)  # length 8 has one variant
+    g.close()
+
+
 @pytest.mark.parametrize("dims", SIZES)
 @pytest.mark.parametrize("inside", [False, True])
 def test_matvec_fp64_matches_oracle(gctx, orc, dims, inside):
