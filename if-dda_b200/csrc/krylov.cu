@@ -51,9 +51,12 @@ struct ResidualOp {
             inner_status[r] = 1;
             return;
         }
-        // ask the inner solve for half of the remaining reduction, but no less
-        // than FP32 vectors can deliver
-        inner[r].tol = fmax(0.5 * s.tol / s.residu, inner_floor);
+        // ask the inner solve to bring the true residual to a fifth of tol,
+        // but for no more than FP32 vectors can deliver: the solve then stops
+        // with a residual well below tol, and its local field within tol of
+        // the converged field (a residual just under tol leaves an error of
+        // about tol times the operator's condition)
+        inner[r].tol = fmax(0.2 * s.tol / s.residu, inner_floor);
         inner[r].maxit = s.maxit;
         inner_status[r] = 0;
         s.itno += 1;

@@ -56,7 +56,7 @@ SIGNATURES = {
     "ifdda_green_create_box": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                          C.c_double, C.POINTER(_vp)]),
     "ifdda_inverserig_ragged": (C.c_int, [C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_char_p, C.c_double, _vp,
-                                          _vp, _dp, _ip, _ip, _ip, C.c_char_p, C.POINTER(SolveOptions)]),
+                                          _vp, _vp, _vp, _vp, _ip, C.c_char_p, C.POINTER(SolveOptions)]),
     "ifdda_green_destroy": (C.c_int, [_vp]),
     "ifdda_green_release_workspace": (C.c_int, [_vp]),
     "ifdda_green_export": (C.c_int, [_vp] + [_vp] * 6),

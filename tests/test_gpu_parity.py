@@ -259,7 +259,7 @@ def test_padded_lattice_matvec_matches_oracle(gctx, orc, dims):
     nd = int(occ.sum())
     xt, bt = x[:3 * nd], b[:3 * nd]
     assert rel(g.matvec(xt, bt, tabdip=tab), orc.matvec(G, nx, ny, nz, xt, bt, tabdip=tab)) < 1e-11
-    assert rel(g.matvec(x, b, precision=1), orc.matvec(G, nx, ny, nz, x, b)) < 2e-5
+    assert rel(g.matvec(x, b, precision=2), orc.matvec(G, nx, ny, nz, x, b)) < 2e-5
     compiled = {2, 4, 6, 8, 10, 12, 16, 20, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256, 320, 384, 512, 640}
     if any(2 * n not in compiled for n in dims):
         with pytest.raises(Exception, match="padded"):
