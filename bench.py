@@ -108,8 +108,9 @@ def wl_c5():
     E0, _ = objects.irradiance(1.0, 10 * lam)
     return Workload("c5", "C5 concentric spheres (core eps 3+0.01i r=0.9 um, shell eps 2 r=1.9 um) on the full "
                     "192^3 lattice (7.08M dipoles, d = 2 r_out/192 = 19.79 nm as the reference sizes it), "
-                    "lambda=632.8 nm, normal incidence, GPBICG1 to 1e-4 (QMR-BiCGSTAB, the configured method, "
-                    "stalls on this object in the restatement and on the GPU alike), FFT grid 384^3",
+                    "lambda=632.8 nm, normal incidence, GPBICG1 to 1e-4 (QMR-BiCGSTAB, the configured method, does "
+                    "not converge on this object: QMRBICGSTAB2 stands at true residual 4.2e-2 after 3000 FP64 "
+                    "iterations, QMRBICGSTAB1 breaks down), FFT grid 384^3",
                     ob, k0, E0, [(0, 0.0, 0.0, 1.0)], "GPBICG1", 1, cpu_mv=1)
 
 
@@ -378,32 +379,38 @@ def run_gpu(args):
     t_fp64_solve, _, _ = timed(IFDDA_FP64, fp64_steps, 0, k=w.fp64_nrhs)
     # the plain FP64 drop-in called once per right-hand side, as the
     # reference's incidence loop calls inverserig (microsbf.f:214-280)
-    serial = None
-    if nrhs > 1:
-        bytes_rhs = 3 * nb * 16
-        nser = w.fp64_nrhs
+    # the plain FP64 drop-in called once per right-hand side, as the
+    # reference's incidence loop calls inverserig (microsbf.f:214-280), at
+    # the bench tolerance and at a fifth of it (its local-field error is
+    # compared with the converged field below)
+    bytes_rhs = 3 * nb * 16
+    nser = w.fp64_nrhs
+    serial = {}
 
-        def serial_pass():
-            ts = []
-            for r in range(nser):
-                with torch.cuda.stream(stream):
-                    e0 = torch.cuda.Event(enable_timing=True)
-                    e1 = torch.cuda.Event(enable_timing=True)
-                    e0.record(stream)
-                rr = g.inverserig_device(1, nb, nmax, tab_d.data_ptr() if tab_d is not None else None,
-                                         pol_d.data_ptr(), ff0_d.data_ptr() + r * bytes_rhs,
-                                         ff_d.data_ptr() + r * bytes_rhs, loc_d.data_ptr() + r * bytes_rhs, w.method,
-                                         TOL, precision=IFDDA_FP64)
-                if rr["nstop"] != 0:
-                    raise RuntimeError(rr["infostr"].strip())
-                with torch.cuda.stream(stream):
-                    e1.record(stream)
-                e1.synchronize()
-                ts.append(e0.elapsed_time(e1))
-            return ts
-        serial_pass()
-        ts = serial_pass()
-        serial = {"solves_s": nser / (sum(ts) / 1e3), "rhs": nser, "ms_per_solve": statistics.mean(ts)}
+    def serial_pass(tol):
+        ts, locs = [], []
+        for r in range(nser):
+            with torch.cuda.stream(stream):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            rr = g.inverserig_device(1, nb, nmax, tab_d.data_ptr() if tab_d is not None else None,
+                                     pol_d.data_ptr(), ff0_d.data_ptr() + r * bytes_rhs,
+                                     ff_d.data_ptr() + r * bytes_rhs, loc_d.data_ptr() + r * bytes_rhs, w.method,
+                                     tol, precision=IFDDA_FP64)
+            if rr["nstop"] != 0:
+                raise RuntimeError(rr["infostr"].strip())
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+            locs.append(loc_d[r].cpu().numpy())
+        return ts, locs
+    for tol_s in (TOL, TOL / 5):
+        serial_pass(tol_s)
+        ts, locs = serial_pass(tol_s)
+        serial[f"tol_{tol_s:g}"] = {"solves_s": nser / (sum(ts) / 1e3), "rhs": nser, "ms_per_solve": statistics.mean(ts),
+                                    "_locs": locs}
     # accuracy against a converged FP64 solve (true residual 1e-10; the FP64
     # drop-in is the path the parity tests hold to the oracle): local field
     # and Cext of the mixed solve, and of the FP64 solve stopped at TOL
@@ -425,6 +432,14 @@ def run_gpu(args):
             ec = max(ec, abs(cm - cc) / abs(cc))
         acc[f"local_field_rel_l2_{name}"] = el
         acc[f"cext_rel_diff_{name}"] = ec
+    for key, blk in serial.items():
+        locs = blk.pop("_locs")
+        blk["local_field_rel_l2"] = max(float(np.linalg.norm(locs[r] - locc[r]) / np.linalg.norm(locc[r]))
+                                        for r in range(min(nser, kacc)))
+    # the north star's comparison: the mixed batched solver against the FP64
+    # drop-in one right-hand side per call, at matching accuracy (the loosest
+    # tolerance whose local field is within 1e-4 of the converged field)
+    match = next((k for k in serial if serial[k]["local_field_rel_l2"] <= 1e-4), None)
 
     total_ms = max_over_ranks(sum(t_mixed), ws, dev)
     value = ws * args.steps * nrhs / (total_ms / 1e3)
@@ -438,6 +453,7 @@ def run_gpu(args):
     Np = (ob.nx + 1) * (ob.ny + 1) * (ob.nz + 1)
     M = 8 * N
     mv = {}
+    pk, _ = measured_peaks()
     for prec, dt, s in ((2, torch.complex64, 8), (0, torch.complex128, 16)):
         x = torch.randn(3 * N, dtype=dt, device=dev)
         b = torch.randn(3 * N, dtype=dt, device=dev)
@@ -459,9 +475,9 @@ def run_gpu(args):
         # the unpruned algorithm's bytes (x, alpha, y; the full 6-component
         # spectrum; the padded 3-component field written and read once)
         bdense = s * (7 * N + 12 * M)
-        pk, _ = measured_peaks()
         mv["fp32" if prec == 2 else "fp64"] = {"ms": round(ms, 4), "alg_bytes": balg,
                                                 "GB_s": round(balg / ms / 1e6, 1),
+                                                "frac": round(balg / ms / 1e6 / pk, 3),
                                                 "alg_bytes_unpruned": bdense,
                                                 "GB_s_unpruned": round(bdense / ms / 1e6, 1),
                                                 "frac_unpruned": round(bdense / ms / 1e6 / pk, 3)}
@@ -530,8 +546,13 @@ def run_gpu(args):
                  "ncompte_max": int(np.max(i64["ncompte"])), "tol1_max": float(np.max(i64["tol1"]))},
         "accuracy": acc,
         "fp64_one_rhs_per_call": serial,
-        "mixed_batched_over_fp64_one_rhs_per_call": (solve_only / serial["solves_s"]) if serial else None,
+        "mixed_over_fp64_one_rhs_per_call": {
+            "at_bench_tol": solve_only / serial[f"tol_{TOL:g}"]["solves_s"],
+            "at_matching_accuracy": (solve_only / serial[match]["solves_s"]) if match else None,
+            "fp64_tol_matching": match, "spectrum": "resident in both"},
         "matvec": mv,
+        "tile_chooser": {name: dict(zip(("zconv_variant", "ypass_variant", "ms_z0_z1_y0_y1"), g.tiles(pr, nrhs)))
+                         for name, pr in (("fp32", _capi.IFDDA_FP32), ("fp64", _capi.IFDDA_FP64))},
         "green_build_ms": green_ms,
         "roofline": {"bound": "hbm", "kernel": f"k_zconv<float,{Z}> (z FFT + 3x3 spectrum multiply + inverse z FFT)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -680,7 +701,7 @@ def run_serving(args):
     reqs = serve.make_stream(args.requests, args.rate, seed=4)
     out = {}
     for name, prec in (("mixed", IFDDA_MIXED), ("fp64", IFDDA_FP64)):
-        srv = serve.Server(slots=args.slots, device=local, precision=prec)
+        srv = serve.Server(slots=args.slots, device=local, precision=prec, ragged=args.ragged)
         # warm-up: one request per lattice size compiles nothing but fills caches
         srv.run(reqs[:args.slots], realtime=False)
         t0 = time.perf_counter()
@@ -691,7 +712,8 @@ def run_serving(args):
         out[name]["wall_s"] = wall
     desc = (f"C4 serving stream: {args.requests} requests, Poisson arrivals at {args.rate}/s (seed 4), sphere or "
             f"cube, edge in {{16..96}}, d=10 nm, eps' U[1.5,4] eps'' U[0,0.5], lambda U[400,800] nm, 1-32 "
-            f"incidences on the NA 0.9 disk, GPBICG1 to 1e-4, {args.slots} concurrent slots, HBM-budget admission")
+            f"incidences on the NA 0.9 disk, GPBICG1 to 1e-4, {args.slots} concurrent slots, HBM-budget admission"
+            + (", ragged batches (every arrived request of the head's box in one solve)" if args.ragged else ""))
     m = out["mixed"]
     line = {"metric": METRIC, "value": m["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": args.requests,
             "warmup": args.slots, "ms_per_step": m["wall_s"] * 1e3 / args.requests, "higher_is_better": True,
@@ -782,6 +804,7 @@ def main():
     ap.add_argument("--requests", type=int, default=2000, help="c4: stream length")
     ap.add_argument("--rate", type=float, default=100.0, help="c4: Poisson arrival rate (requests/s)")
     ap.add_argument("--slots", type=int, default=4, help="c4: concurrent solver slots")
+    ap.add_argument("--ragged", action="store_true", help="c4: solve arrived requests of one box as ragged batches")
     ap.add_argument("--mode", default="solve", choices=["solve", "matvec", "passes"],
                     help="matvec: time the five mat-vec passes only; passes: the passes inside solves")
     args = ap.parse_args()

@@ -59,15 +59,31 @@ __host__ __device__ constexpr int clamp_pow2(int v, int lo, int hi) {
     while (p * 2 <= v && p * 2 <= hi) p *= 2;
     return p < lo ? lo : p;
 }
+// Radices with a register butterfly (Dft<R> below).
+__host__ __device__ constexpr bool has_dft(int r) {
+    return r == 2 || r == 3 || r == 4 || r == 5 || r == 8 || r == 12 || r == 16 || r == 32;
+}
+// Plan policy 1 (two passes): a first radix of 32 or 16 and one more radix of
+// at most 12, where such a pair exists; otherwise policy 0.  It halves the
+// shared-memory round trips of a three-pass length (160, 192, 256, 384) for
+// a kernel that can afford the registers of a 32-point butterfly.
+__host__ __device__ constexpr int two_pass_first(int L) {
+    return (L % 32 == 0 && has_dft(L / 32) && L / 32 <= 12) ? 32
+         : (L % 16 == 0 && has_dft(L / 16) && L / 16 <= 12) ? 16 : 0;
+}
+__host__ __device__ constexpr int pick_radix_p(int L, int rem, bool first, int policy) {
+    if (policy == 1 && two_pass_first(L)) return first ? two_pass_first(L) : rem;
+    return pick_radix(rem, first);
+}
 // The plan of L: radix of pass q (0-based) and number of passes.  A plan
 // runs forward (q = 0 .. n-1) or reversed; any order of the radices is a
 // valid Stockham transform, and the reversed plan lets an inverse transform
 // start from the registers the forward transform ended with.
-__host__ __device__ constexpr int plan_len(int L) {
+__host__ __device__ constexpr int plan_len(int L, int policy = 0) {
     int n = 0;
     bool first = true;
     for (int rem = L; rem > 1;) {
-        const int r = pick_radix(rem, first);
+        const int r = pick_radix_p(L, rem, first, policy);
         if (r == 0) return -1;
         rem /= r;
         first = false;
@@ -75,25 +91,25 @@ __host__ __device__ constexpr int plan_len(int L) {
     }
     return n;
 }
-__host__ __device__ constexpr int plan_radix(int L, int q) {
+__host__ __device__ constexpr int plan_radix(int L, int q, int policy = 0) {
     int rem = L;
     bool first = true;
     for (int i = 0; i < q; i++) {
-        rem /= pick_radix(rem, first);
+        rem /= pick_radix_p(L, rem, first, policy);
         first = false;
     }
-    return pick_radix(rem, first);
+    return pick_radix_p(L, rem, first, policy);
 }
-__host__ __device__ constexpr int plan_radix_dir(int L, int q, bool rev) {
-    return rev ? plan_radix(L, plan_len(L) - 1 - q) : plan_radix(L, q);
+__host__ __device__ constexpr int plan_radix_dir(int L, int q, bool rev, int policy = 0) {
+    return rev ? plan_radix(L, plan_len(L, policy) - 1 - q, policy) : plan_radix(L, q, policy);
 }
 
 // largest radix used by the plan of L (sets the register footprint)
-__host__ __device__ constexpr int max_radix(int L) {
+__host__ __device__ constexpr int max_radix(int L, int policy = 0) {
     int m = 1;
     bool first = true;
     for (int rem = L; rem > 1;) {
-        const int r = pick_radix(rem, first);
+        const int r = pick_radix_p(L, rem, first, policy);
         if (r == 0) return 0;
         m = r > m ? r : m;
         rem /= r;
@@ -193,6 +209,45 @@ template <int DIR, class C> struct Dft<16, DIR, C> {
     }
 };
 
+// 32 points as 2 x 16: DFT16 over the even and the odd points, the twiddles
+// w32^k on the odd half, then DFT2 across; X[k] and X[k + 16]
+#define IFDDA_COS_PI16 0.98078528040323044912618223613424   // cos(pi / 16)
+#define IFDDA_SIN_PI16 0.19509032201612826784828486847702   // sin(pi / 16)
+#define IFDDA_COS_3PI16 0.83146961230254523707878837761791  // cos(3 pi / 16)
+#define IFDDA_SIN_3PI16 0.55557023301960222474283081394853  // sin(3 pi / 16)
+template <int DIR, class C> struct Dft<32, DIR, C> {
+    __device__ __forceinline__ static void run(C* v) {
+        using T = decltype(C().x);
+        C e[16], o[16];
+#pragma unroll
+        for (int n = 0; n < 16; n++) {
+            e[n] = v[2 * n];
+            o[n] = v[2 * n + 1];
+        }
+        Dft<16, DIR, C>::run(e);
+        Dft<16, DIR, C>::run(o);
+        // cos and sin of k pi / 16, k = 0..8 (k pi / 16 for k > 8 by symmetry)
+        const T cs[9] = {(T)1, (T)IFDDA_COS_PI16, (T)IFDDA_COS_PI8, (T)IFDDA_COS_3PI16, (T)IFDDA_SQRT1_2,
+                         (T)IFDDA_SIN_3PI16, (T)IFDDA_SIN_PI8, (T)IFDDA_SIN_PI16, (T)0};
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            // w32^k = cos(k pi/16) + i DIR sin(k pi/16)
+            const T c = k <= 8 ? cs[k] : -cs[16 - k];
+            const T sn = k <= 8 ? cs[8 - k] : cs[k - 8];
+            const C w = mk(c, DIR > 0 ? sn : -sn);
+            const C t = k == 0 ? o[0] : cmul(o[k], w);
+            v[k] = cadd(e[k], t);
+            v[k + 16] = csub(e[k], t);
+        }
+    }
+};
+
+// 12 points as 4 x 3: DFT3 over the stride-4 subsequences, the twiddles
+// w12^(n2 k1), then DFT4 across them; X[k1 + 3 k2]
+template <int DIR, class C> struct Dft<12, DIR, C> {
+    __device__ __forceinline__ static void run(C* v);
+};
+
 template <int DIR, class C> struct Dft<3, DIR, C> {
     __device__ __forceinline__ static void run(C* v) {
         using T = decltype(C().x);
@@ -222,6 +277,34 @@ template <int DIR, class C> struct Dft<5, DIR, C> {
         v[3] = csub(a2, b2);
     }
 };
+
+template <int DIR, class C> __device__ __forceinline__ void Dft<12, DIR, C>::run(C* v) {
+    using T = decltype(C().x);
+    C a[4][3];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; n2++) {
+        C t[3] = {v[n2], v[4 + n2], v[8 + n2]};
+        Dft<3, DIR, C>::run(t);
+#pragma unroll
+        for (int k1 = 0; k1 < 3; k1++) a[n2][k1] = t[k1];
+    }
+    // w12^1 = (sqrt3/2, DIR/2), w12^2 = (1/2, DIR sqrt3/2), w12^4 = (-1/2, DIR sqrt3/2)
+    const T h = (T)0.5, r3 = (T)IFDDA_SQRT3_2;
+    const C w1 = mk(r3, DIR > 0 ? h : -h), w2 = mk(h, DIR > 0 ? r3 : -r3), w4 = mk(-h, DIR > 0 ? r3 : -r3);
+    a[1][1] = cmul(a[1][1], w1);
+    a[1][2] = cmul(a[1][2], w2);
+    a[2][1] = cmul(a[2][1], w2);
+    a[2][2] = cmul(a[2][2], w4);
+    a[3][1] = cmul_i<DIR>(a[3][1]);  // w12^3
+    a[3][2] = cscale(a[3][2], (T)-1);  // w12^6
+#pragma unroll
+    for (int k1 = 0; k1 < 3; k1++) {
+        C t[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+        Dft<4, DIR, C>::run(t);
+#pragma unroll
+        for (int k2 = 0; k2 < 4; k2++) v[k1 + 3 * k2] = t[k2];
+    }
+}
 
 // Source / destination that is the shared-memory tile itself.
 struct SmemIO {
@@ -334,12 +417,13 @@ __device__ __forceinline__ void stockham_pass(C* sm, const C* tw, const Src& src
 
 // Passes q in [q, Q1) of the plan (reversed when REV); Ns is the product of
 // the radices of the passes before q.
-template <class C, int L, int NB, int NT, int DIR, class Lay, bool REV, int Q1, int q, int Ns, class Src, class Dst>
+template <class C, int L, int NB, int NT, int DIR, class Lay, bool REV, int Q1, int q, int Ns, class Src, class Dst,
+          int PLAN = 0>
 __device__ __forceinline__ void stockham_range(C* sm, const C* tw, const Src& src, const Dst& dst) {
     if constexpr (q < Q1) {
-        constexpr int R = plan_radix_dir(L, q, REV);
+        constexpr int R = plan_radix_dir(L, q, REV, PLAN);
         stockham_pass<C, L, R, Ns, NB, NT, DIR, Lay, Src, Dst>(sm, tw, src, dst);
-        stockham_range<C, L, NB, NT, DIR, Lay, REV, Q1, q + 1, Ns * R, Src, Dst>(sm, tw, src, dst);
+        stockham_range<C, L, NB, NT, DIR, Lay, REV, Q1, q + 1, Ns * R, Src, Dst, PLAN>(sm, tw, src, dst);
     }
 }
 

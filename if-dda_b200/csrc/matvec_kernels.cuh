@@ -107,8 +107,8 @@ template <class T, int L, int V = 0> struct MvTiles {
     }
     static constexpr int LP = lpitch();
     // one butterfly of the widest radix per thread
-    static constexpr int nthreads(int nb) {
-        int t = nb * L / max_radix(L);
+    static constexpr int nthreads(int nb, int policy = 0) {
+        int t = nb * L / max_radix(L, policy);
         t = (t + 31) / 32 * 32;
         return t < 64 ? 64 : (t > 512 ? 512 : t);
     }
@@ -129,15 +129,20 @@ template <class T, int L, int V = 0> struct MvTiles {
         return V && tl > 1 ? tl / 2 : tl;
     }
     static constexpr int TLZ = ztile(), NBZ = 6 * TLZ;
+    // zconv's FFT plan in FP32: two passes (a 32- or 16-point first pass)
+    // where that saves a pass over the usual plan (lengths 96, 160, 192, 256,
+    // 384), at about 120 registers a thread; FP64 keeps the usual plan (its
+    // 12-point middle for three components would not fit the registers)
+    static constexpr int ZP = (S == 8 && plan_len(L, 1) > 0 && plan_len(L, 1) < plan_len(L, 0)) ? 1 : 0;
     // y tile: odd point stride; z tile: point stride NBZ with one pad point every 16
     static constexpr int PSY = NBY + 1, PSZ = NBZ;
     using LayX = Layout<1, LP, false, 4>;
     using LayY = Layout<PSY, 1, true>;
     using LayZ = Layout<PSZ, 1, true, 4>;
-    static constexpr int NTX = nthreads(NBX), NTY = nthreads(NBY), NTZ = nthreads(NBZ);
+    static constexpr int NTX = nthreads(NBX), NTY = nthreads(NBY), NTZ = nthreads(NBZ, ZP);
     static constexpr int MINBX = minblocks(NTX, S == 8 ? 80 : 96);
     static constexpr int MINBY = minblocks(NTY, S == 8 ? 80 : 112);
-    static constexpr int MINBZ = minblocks(NTZ, S == 8 ? 72 : 168);
+    static constexpr int MINBZ = minblocks(NTZ, S == 8 ? (ZP ? 128 : 72) : 168);
     static constexpr size_t smem_x = (size_t)L * S + (size_t)NBX * LP * S;
     static constexpr size_t smem_y = (size_t)L * S + (size_t)L * PSY * S;
     static constexpr size_t smem_z = (size_t)L * S + (size_t)LayZ::span(L) * PSZ * S + (size_t)6 * (L / 2 + 1) * TLZ * S;
@@ -385,8 +390,9 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
     using C = cplx<T>;
     using LZ = typename TT::LayZ;
     constexpr int TL = TT::TLZ, NB = TT::NBZ, NT = TT::NTZ;
-    constexpr int NP = plan_len(L);
-    constexpr int RK = plan_radix(L, NP - 1);  // last forward radix = first inverse radix
+    constexpr int ZP = TT::ZP;
+    constexpr int NP = plan_len(L, ZP);
+    constexpr int RK = plan_radix(L, NP - 1, ZP);  // last forward radix = first inverse radix
     constexpr int NJ = L / RK;                 // butterflies per line in that pass
     constexpr int NG = 2 * TL * NJ;            // (row half, column, butterfly) groups
     constexpr int PERM = (NG + NT - 1) / NT;
@@ -429,7 +435,8 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
     const int rs = Y * X, comp = nz * Y * X, drow = (Y - 2 * qy) * X, nv = min(TL, X - i0);
     const ZLoad<T, TL> zload{B2, rs, comp, drow, nv, two};
     const ZStore<T, TL> zstore{B2, rs, comp, drow, nv, two};
-    if constexpr (NP > 1) stockham_range<C, L, NB, NT, +1, LZ, false, NP - 1, 0, 1>(sm, tw, zload, SmemIO{});
+    if constexpr (NP > 1)
+        stockham_range<C, L, NB, NT, +1, LZ, false, NP - 1, 0, 1, ZLoad<T, TL>, SmemIO, ZP>(sm, tw, zload, SmemIO{});
     cp_async_wait_all();
     __syncthreads();
     // ---- fused middle: read, transform, multiply, transform (registers) ----
@@ -512,7 +519,7 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
     }
     if constexpr (NP > 1) {
         __syncthreads();
-        stockham_range<C, L, NB, NT, -1, LZ, true, NP, 1, RK>(sm, tw, SmemIO{}, zstore);
+        stockham_range<C, L, NB, NT, -1, LZ, true, NP, 1, RK, SmemIO, ZStore<T, TL>, ZP>(sm, tw, SmemIO{}, zstore);
     }
 }
 
