@@ -389,23 +389,23 @@ int ifdda_green_create_box(ifdda_ctx* ctx, int nx, int ny, int nz, int bx, int b
 int ifdda_green_tiles(ifdda_green* g, int precision, int nrhs, int* zconv_variant, int* ypass_variant,
                       float* times_ms) {
     if (!g || nrhs < 1 || (precision != IFDDA_FP32 && precision != IFDDA_FP64)) return 1;
-    auto it = g->G.tiles.find({precision == IFDDA_FP32 ? 1 : 0, nrhs});
-    const bool have = it != g->G.tiles.end();
-    if (zconv_variant) *zconv_variant = have ? it->second.zvar : -1;
-    if (ypass_variant) *ypass_variant = have ? it->second.yvar : -1;
+    TileChoice tc;
+    const bool have = tile_get(g->G.device, precision == IFDDA_FP32 ? 1 : 0, g->G.g, nrhs, tc);
+    if (zconv_variant) *zconv_variant = have ? tc.zvar : -1;
+    if (ypass_variant) *ypass_variant = have ? tc.yvar : -1;
     if (times_ms)
         for (int v = 0; v < 2; v++) {
-            times_ms[v] = have ? it->second.z_ms[v] : 0.f;
-            times_ms[2 + v] = have ? it->second.y_ms[v] : 0.f;
+            times_ms[v] = have ? tc.z_ms[v] : 0.f;
+            times_ms[2 + v] = have ? tc.y_ms[v] : 0.f;
         }
     return 0;
 }
 
 int ifdda_green_set_tiles(ifdda_green* g, int precision, int nrhs, int zconv_variant, int ypass_variant) {
     if (!g || nrhs < 1 || (precision != IFDDA_FP32 && precision != IFDDA_FP64)) return 1;
-    const std::pair<int, int> key{precision == IFDDA_FP32 ? 1 : 0, nrhs};
+    const int pk = precision == IFDDA_FP32 ? 1 : 0;
     if (zconv_variant < 0 || ypass_variant < 0) {
-        g->G.tiles.erase(key);
+        tile_erase(g->G.device, pk, g->G.g, nrhs);
         return 0;
     }
     if (zconv_variant >= tile_variants(g->G.g.Z) || ypass_variant >= tile_variants(g->G.g.Y)) {
@@ -415,7 +415,7 @@ int ifdda_green_set_tiles(ifdda_green* g, int precision, int nrhs, int zconv_var
     TileChoice tc{};
     tc.zvar = zconv_variant;
     tc.yvar = ypass_variant;
-    g->G.tiles[key] = tc;
+    tile_put(g->G.device, pk, g->G.g, nrhs, tc);
     return 0;
 }
 

@@ -124,6 +124,13 @@ struct TileChoice {
     float z_ms[2] = {0, 0}, y_ms[2] = {0, 0};
 };
 
+// Tile chooser results, one per (device, precision 0 FP64 / 1 FP32, grid
+// X x Y x Z, right-hand sides), shared by every spectrum on that grid: a
+// request stream of many spectra on few grids times each grid once.
+bool tile_get(int dev, int prec, const MvGeom& g, int nrhs, TileChoice& out);
+void tile_put(int dev, int prec, const MvGeom& g, int nrhs, const TileChoice& tc);
+void tile_erase(int dev, int prec, const MvGeom& g, int nrhs);
+
 // Green spectrum of one (lattice, spacing, wavenumber), device resident.
 struct Green {
     int device = 0;
@@ -141,12 +148,9 @@ struct Green {
     DevBuf<float2> tw32[3];
     MvWork<float> w32;
     MvWork<double> w64;
-    // tile chooser's result per (precision: 0 FP64, 1 FP32; right-hand sides)
-    std::map<std::pair<int, int>, TileChoice> tiles;
-    template <class T> const TileChoice* tile_choice(int nrhs) const {
-        auto it = tiles.find({sizeof(T) == 4 ? 1 : 0, nrhs});
-        return it == tiles.end() ? nullptr : &it->second;
-    }
+    // the tile chooser's result for this grid (shared with every spectrum on
+    // the same grid and device), precision T and nrhs right-hand sides
+    template <class T> bool tile_choice(int nrhs, TileChoice& out) const;
     template <class T> const cplx<T>* gc() const;
     template <class T> const cplx<T>* tw(int axis) const;
     template <class T> MvWork<T>& work();
@@ -157,6 +161,9 @@ template <> inline const float2* Green::tw<float>(int a) const { return tw32[a].
 template <> inline const double2* Green::tw<double>(int a) const { return tw64[a].p; }
 template <> inline MvWork<float>& Green::work<float>() { return w32; }
 template <> inline MvWork<double>& Green::work<double>() { return w64; }
+template <class T> inline bool Green::tile_choice(int nrhs, TileChoice& out) const {
+    return tile_get(device, sizeof(T) == 4 ? 1 : 0, g, nrhs, out);
+}
 
 MvGeom make_geom(int nx, int ny, int nz);
 // builds the spectrum (FP64, plus an FP32 copy) on `st`; throws EngineError
@@ -206,9 +213,10 @@ MvArgs<T> mv_args(Green& G, int nrhs, const cplx<T>* x, const cplx<T>* b, cplx<T
     a.twz = G.tw<T>(2);
     a.status = status;
     a.inv_m = (T)(1.0 / ((double)G.g.X * G.g.Y * G.g.Z));
-    if (const TileChoice* tc = G.tile_choice<T>(nrhs)) {
-        a.zvar = tc->zvar;
-        a.yvar = tc->yvar;
+    TileChoice tc;
+    if (G.tile_choice<T>(nrhs, tc)) {
+        a.zvar = tc.zvar;
+        a.yvar = tc.yvar;
     }
     return a;
 }

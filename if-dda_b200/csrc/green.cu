@@ -1,5 +1,8 @@
 // Green spectrum build (replaces greencalculfft, cdmlib/calculgreenfft.f:1-104).
+#include <array>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include "engine.cuh"
 #include "green_kernels.cuh"
 
@@ -14,6 +17,31 @@ bool fft_length_supported(int L) {
         default:
             return false;
     }
+}
+
+namespace {
+std::mutex g_tile_mu;
+std::map<std::array<int, 6>, TileChoice>& tile_map() {
+    static std::map<std::array<int, 6>, TileChoice> m;
+    return m;
+}
+std::array<int, 6> tile_key(int dev, int prec, const MvGeom& g, int nrhs) { return {dev, prec, g.X, g.Y, g.Z, nrhs}; }
+}  // namespace
+
+bool tile_get(int dev, int prec, const MvGeom& g, int nrhs, TileChoice& out) {
+    std::lock_guard<std::mutex> lk(g_tile_mu);
+    auto it = tile_map().find(tile_key(dev, prec, g, nrhs));
+    if (it == tile_map().end()) return false;
+    out = it->second;
+    return true;
+}
+void tile_put(int dev, int prec, const MvGeom& g, int nrhs, const TileChoice& tc) {
+    std::lock_guard<std::mutex> lk(g_tile_mu);
+    tile_map()[tile_key(dev, prec, g, nrhs)] = tc;
+}
+void tile_erase(int dev, int prec, const MvGeom& g, int nrhs) {
+    std::lock_guard<std::mutex> lk(g_tile_mu);
+    tile_map().erase(tile_key(dev, prec, g, nrhs));
 }
 
 MvGeom make_geom(int nx, int ny, int nz) {

@@ -442,6 +442,8 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
     // the buffers and shapes a captured loop is bound to
     std::vector<const void*> key;
     if (graphs) {
+        TileChoice tcur;
+        const long tile_code = G.tile_choice<T>(nrhs, tcur) ? 1 + tcur.zvar + 2 * tcur.yvar : 0;
         MvWork<T>& mw = G.work<T>();
         mw.ensure(G.g, nrhs);
         W.loopcount.ensure(1);
@@ -449,9 +451,7 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
                W.mvpart.p, W.mvtk.p, W.loopcount.p, (const void*)(long)fused,
                (const void*)(long)sp.method, (const void*)(long)nrhs, (const void*)n3, (const void*)(long)sp.amode,
                (const void*)sp.nmax, (const void*)(long)nblk, sp.gc64_r, sp.gc32_r, sp.alpha_off, sp.tab_off,
-               (const void*)(long)(G.tile_choice<T>(nrhs) ? 1 + G.tile_choice<T>(nrhs)->zvar +
-                                                                2 * G.tile_choice<T>(nrhs)->yvar
-                                                          : 0)};
+               (const void*)(long)tile_code};
     }
     const bool cached = graphs && W.graph.exec && W.graph.key == key;
     // without a loop captured for these buffers, the first two iterations run

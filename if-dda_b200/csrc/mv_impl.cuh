@@ -107,11 +107,13 @@ bool matvec_launch_fused(const MvArgs<T>& a, const Pre& pre, const Epi& epi, con
 // Tile chooser: with G's mat-vec scratch for nrhs right-hand sides (whose
 // contents are about to be overwritten by the next mat-vec anyway), time each
 // tile variant of the y passes (forward then inverse) and of zconv, best of
-// three launches with CUDA events on st, and record the faster in G for
-// (precision, nrhs).  Never runs while st is being captured.
+// three launches with CUDA events on st, and record the faster for G's grid,
+// device, precision and nrhs (tile_put: every spectrum on that grid then
+// uses it).  Never runs while st is being captured.
 template <class T> void tune_tiles_impl(Green& G, int nrhs, cudaStream_t st) {
     const int pk = sizeof(T) == 4 ? 1 : 0;
-    if (G.tiles.count({pk, nrhs})) return;
+    TileChoice have;
+    if (G.tile_choice<T>(nrhs, have)) return;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     IFDDA_CUDA(cudaStreamIsCapturing(st, &cs));
     if (cs != cudaStreamCaptureStatusNone) return;
@@ -152,7 +154,7 @@ template <class T> void tune_tiles_impl(Green& G, int nrhs, cudaStream_t st) {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
     }
-    G.tiles[{pk, nrhs}] = tc;
+    tile_put(G.device, pk, G.g, nrhs, tc);
 }
 
 }  // namespace ifdda

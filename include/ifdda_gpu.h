@@ -87,8 +87,9 @@ int ifdda_green_create_box(ifdda_ctx* ctx, int nx, int ny, int nz, int bx, int b
    shapes for FFT lengths of 64 and more; before the first mat-vec of a
    precision and a number of right-hand sides on g, the library times both on
    g's grid (best of three launches with CUDA events) and keeps the faster
-   for every later mat-vec of that (precision, nrhs).  The shapes give the
-   same bits.  ifdda_green_tiles reports the choice (-1: not made yet) and,
+   for every later mat-vec of that (precision, nrhs) on that grid: the choice
+   belongs to the grid and device, shared by every spectrum on them.  The
+   shapes give the same bits.  ifdda_green_tiles reports the choice (-1: not made yet) and,
    if times_ms is not NULL, the four times measured (zconv variants 0, 1,
    y passes 0, 1; 0 where not timed).  ifdda_green_set_tiles imposes a
    choice (-1: choose again at the next mat-vec).  No counterpart in the
