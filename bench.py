@@ -575,9 +575,10 @@ def run_gpu(args):
 
 
 def run_matvec(args):
-    """Mat-vec only: the five passes of one right-hand side on the workload's
-    grid, FP32 then FP64, each pass timed with CUDA events on the solver
-    stream (also the target of the ncu commands in profiles/)."""
+    """Mat-vec only: the five passes of --nrhs right-hand sides (one batched
+    launch sequence) on the workload's grid, FP32 then FP64 (--precs), each
+    pass timed with CUDA events on the solver stream (also the target of the
+    ncu commands in profiles/)."""
     import ctypes as C
     import torch
     import ifdda
@@ -595,18 +596,23 @@ def run_matvec(args):
     Np = (ob.nx + 1) * (ob.ny + 1) * (ob.nz + 1)
     names = {1: "fwd_x", 2: "fwd_y", 3: "zconv", 4: "inv_y", 5: "inv_x"}
     out = {}
+    R = args.nrhs
     for prec, dt, s in ((_capi.IFDDA_FP32, torch.complex64, 8), (_capi.IFDDA_FP64, torch.complex128, 16)):
-        x = torch.randn(3 * N, dtype=dt, device=dev)
-        b = torch.randn(3 * N, dtype=dt, device=dev)
+        if str(prec) not in args.precs.split(","):
+            continue
+        x = torch.randn(R * 3 * N, dtype=dt, device=dev)
+        b = torch.randn(R * 3 * N, dtype=dt, device=dev)
         for _ in range(args.warmup):
-            g.matvec_device(1, N, x.data_ptr(), b.data_ptr(), precision=prec)
+            g.matvec_device(R, N, x.data_ptr(), b.data_ptr(), precision=prec)
         ctx.synchronize()
-        balg = {1: 9 * N * s, 2: 18 * N * s, 3: (24 * N + 6 * Np) * s, 4: 18 * N * s, 5: 12 * N * s}
+        # per launch: every right-hand side's share, the spectrum once
+        balg = {1: 9 * N * s * R, 2: 18 * N * s * R, 3: (24 * N * R + 6 * Np) * s, 4: 18 * N * s * R,
+                5: 12 * N * s * R}
         passes = {}
         for ps in range(1, 6):
             lib.ifdda_timing_enable(ps, prec)
             for _ in range(args.steps):
-                g.matvec_device(1, N, x.data_ptr(), b.data_ptr(), precision=prec)
+                g.matvec_device(R, N, x.data_ptr(), b.data_ptr(), precision=prec)
             ctx.synchronize()
             nl, ms = C.c_int(0), C.c_double(0)
             lib.ifdda_timing_read(C.byref(nl), C.byref(ms))
@@ -616,7 +622,7 @@ def run_matvec(args):
         out["fp32" if s == 8 else "fp64"] = passes
         del x, b
     if rank == 0:
-        print(json.dumps({"mode": "matvec", "workload": w.desc, "passes": out}), flush=True)
+        print(json.dumps({"mode": "matvec", "workload": w.desc, "nrhs": R, "passes": out}), flush=True)
     g.close()
     ctx.close()
     return 0
@@ -805,6 +811,8 @@ def main():
     ap.add_argument("--rate", type=float, default=100.0, help="c4: Poisson arrival rate (requests/s)")
     ap.add_argument("--slots", type=int, default=4, help="c4: concurrent solver slots")
     ap.add_argument("--ragged", action="store_true", help="c4: solve arrived requests of one box as ragged batches")
+    ap.add_argument("--nrhs", type=int, default=1, help="matvec mode: right-hand sides per batched mat-vec")
+    ap.add_argument("--precs", default="2,0", help="matvec mode: precisions (2 FP32, 0 FP64)")
     ap.add_argument("--mode", default="solve", choices=["solve", "matvec", "passes"],
                     help="matvec: time the five mat-vec passes only; passes: the passes inside solves")
     args = ap.parse_args()

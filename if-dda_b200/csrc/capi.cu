@@ -259,6 +259,157 @@ const int* lattice_tab(ifdda_green* g, const int* src, cudaStream_t st) {
     return lattice_tab(g->G, g->ptab.p, src, st);
 }
 
+// Ragged batch; the per-object arrays are host memory (dev = false) or
+// device memory of the context's device (dev = true).
+static int ragged_solve(int nobj, ifdda_green* const* greens, const int* nrhs, const int* nbsphere, const int* nmax,
+                        const int* const* tabdip, const ifdda_dcmplx* const* polarisa, const ifdda_dcmplx* const* FF0,
+                        const char* methodeit, double tol, ifdda_dcmplx* const* FF, ifdda_dcmplx* const* FFloc,
+                        double* tol1, int* nloop, int* ncompte, int* nstop, char* infostr,
+                        const ifdda_solve_options* opt, bool dev) {
+    if (nobj < 1 || !greens || !greens[0] || !nrhs || !nbsphere || !nmax || !polarisa || !FF0 || !FF || !FFloc) {
+        if (nstop) *nstop = 1;
+        set_info(infostr, "invalid argument");
+        return 1;
+    }
+    ifdda_green* g0 = greens[0];
+    ifdda_ctx* ctx = g0->ctx;
+    IFDDA_GUARD_BEGIN
+    DeviceScope ds(ctx->device);
+    AllocStreamScope as(ctx->stream);
+    cudaStream_t st = ctx->stream;
+    const int method = method_code(methodeit);
+    if (method == 0) {
+        if (nstop) *nstop = 1;
+        set_info(infostr, "Iterative method not correct!");
+        return 1;
+    }
+    if (method == 14) throw EngineError{1, "ragged batch: QMRCLA is not supported (its A^T products)"};
+    if (tol < 1e-12 || tol > 0.5) throw EngineError{1, "ragged batch: tolerance outside [1e-12, 0.5]"};
+    const MvGeom& box = g0->G.g;
+    long R = 0, nbmax = 0, nalpha = 0;
+    for (int i = 0; i < nobj; i++) {
+        ifdda_green* g = greens[i];
+        if (!g || g->ctx != ctx) throw EngineError{1, "ragged batch: every spectrum must belong to one context"};
+        if (g->G.g.nx != box.nx || g->G.g.ny != box.ny || g->G.g.nz != box.nz || g->G.nquad != 0)
+            throw EngineError{1, "ragged batch: every spectrum must be on one box (ifdda_green_create_box), nquad 0"};
+        if (nrhs[i] < 1 || nbsphere[i] < 1 || nmax[i] < nbsphere[i] || !polarisa[i] || !FF0[i] || !FF[i] ||
+            !FFloc[i])
+            throw EngineError{1, "ragged batch: invalid object " + std::to_string(i)};
+        if (!(tabdip && tabdip[i]) && nbsphere[i] != g->G.uN)
+            throw EngineError{1, "ragged batch: a full-box object needs nbsphere = nx*ny*nz"};
+        if (!dev && tabdip && tabdip[i]) check_tabdip(tabdip[i], g->G.uN, nbsphere[i]);
+        if (!dev && pola_mode_range(polarisa[i], 0, nbsphere[i], nmax[i]) != ALPHA_ISO)
+            throw EngineError{1, "ragged batch: only isotropic polarisabilities are supported"};
+        R += nrhs[i];
+        nbmax = std::max<long>(nbmax, nbsphere[i]);
+        nalpha += nbsphere[i];
+    }
+    // every right-hand side is laid out on the box's sites (not on the batch's
+    // largest object), so its vector length, reductions and kernels' work do
+    // not depend on the other objects of the batch: a request gives the same
+    // bits alone and inside any ragged batch on that box
+    const long Nb = box.N, n3 = 3 * Nb, tot = R * n3;
+    if (nbmax > Nb) throw EngineError{1, "ragged batch: an object has more dipoles than the box has sites"};
+    g0->ff0.ensure(tot);
+    g0->x.ensure(tot);
+    g0->ffb.ensure(tot);
+    g0->ralpha.ensure(nalpha);
+    g0->rtab.ensure((size_t)nobj * Nb);
+    g0->rgc64.ensure(R);
+    g0->rgc32.ensure(R);
+    g0->roff.ensure(2 * R);
+    const cudaMemcpyKind in_kind = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const cudaMemcpyKind out_kind = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    if (dev) IFDDA_CUDA(cudaMemsetAsync(ctx->flag.p, 0, sizeof(int), st));
+    // right-hand sides of every object, each zero-padded to 3 Nbox
+    IFDDA_CUDA(cudaMemsetAsync(g0->ff0.p, 0, tot * sizeof(double2), st));
+    std::vector<const double2*> h64(R);
+    std::vector<const float2*> h32(R);
+    std::vector<long> hoff(2 * R);
+    std::vector<long> aoff(nobj), roff(nobj);
+    long r0 = 0, a0 = 0;
+    for (int i = 0; i < nobj; i++) {
+        ifdda_green* g = greens[i];
+        const long n3i = 3L * nbsphere[i];
+        for (int q = 0; q < nrhs[i]; q++) {
+            IFDDA_CUDA(cudaMemcpyAsync(g0->ff0.p + (r0 + q) * n3, FF0[i] + q * n3i, n3i * sizeof(double2), in_kind,
+                                       st));
+            h64[r0 + q] = g->G.gc64.p;
+            h32[r0 + q] = g->G.gc32.p;
+            hoff[r0 + q] = a0;
+            hoff[R + r0 + q] = (long)i * Nb;
+        }
+        // the isotropic value of dipole n is polarisa(n,1,1): the first
+        // nbsphere entries of the (nmax,3,3) array (on the device, checked
+        // for isotropy as it is compacted)
+        if (dev)
+            pola_compact_dev((const double2*)polarisa[i], nbsphere[i], nmax[i], g0->ralpha.p + a0, ctx->flag.p, st);
+        else
+            IFDDA_CUDA(cudaMemcpyAsync(g0->ralpha.p + a0, polarisa[i], nbsphere[i] * sizeof(double2),
+                                       cudaMemcpyHostToDevice, st));
+        // the object's Tabdip on the common box (identity for a full box)
+        const int* src = nullptr;
+        if (dev && tabdip && tabdip[i]) {
+            src = tabdip[i];
+        } else if (tabdip && tabdip[i]) {
+            g0->rtab_in.ensure(g->G.uN);
+            IFDDA_CUDA(cudaMemcpyAsync(g0->rtab_in.p, tabdip[i], g->G.uN * sizeof(int), cudaMemcpyHostToDevice, st));
+            src = g0->rtab_in.p;
+        }
+        count_launch();
+        k_pad_tab<<<(int)std::min<long>((Nb + 255) / 256, 148L * 16), 256, 0, st>>>(
+            src, g0->rtab.p + (long)i * Nb, g->G.ux, g->G.uy, g->G.uz, box.nx, box.ny, Nb);
+        IFDDA_CUDA(cudaGetLastError());
+        // rtab_in is reused by the next object: its copy must be done
+        if (src && !dev) IFDDA_CUDA(cudaStreamSynchronize(st));
+        aoff[i] = a0;
+        roff[i] = r0;
+        r0 += nrhs[i];
+        a0 += nbsphere[i];
+    }
+    IFDDA_CUDA(cudaMemcpyAsync(g0->rgc64.p, h64.data(), R * sizeof(const double2*), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(g0->rgc32.p, h32.data(), R * sizeof(const float2*), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(g0->roff.p, hoff.data(), 2 * R * sizeof(long), cudaMemcpyHostToDevice, st));
+    SolveSpec sp = make_spec(method, (int)R, (int)Nb, tol, opt);
+    sp.tabdip = g0->rtab.p;
+    sp.amode = ALPHA_ISO;
+    sp.alpha = g0->ralpha.p;
+    sp.nmax = nalpha;
+    sp.cancel = (volatile int*)nstop;
+    sp.gc64_r = g0->rgc64.p;
+    sp.gc32_r = g0->rgc32.p;
+    sp.alpha_off = g0->roff.p;
+    sp.tab_off = g0->roff.p + R;
+    if (dev) {
+        int aniso = 0;
+        IFDDA_CUDA(cudaMemcpyAsync(&aniso, ctx->flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        IFDDA_CUDA(cudaStreamSynchronize(st));
+        if (aniso) throw EngineError{1, "ragged batch: only isotropic polarisabilities are supported"};
+    }
+    if (nstop && *nstop == -1) {
+        set_info(infostr, "Calculation cancelled during iterative method");
+        return -1;
+    }
+    std::vector<SolveResult> res;
+    if (opt && opt->precision == IFDDA_MIXED) solve_mixed(g0->G, g0->SW, sp, g0->ff0.p, g0->x.p, res, st);
+    else solve_fp64(g0->G, g0->SW, sp, g0->ff0.p, g0->x.p, res, st);
+    for (int i = 0; i < nobj; i++) {
+        const long n3i = 3L * nbsphere[i];
+        // FF = polarisa . E (cdmlib/inverserigopt.f:92-97), per object
+        apply_alpha_dev(g0->x.p + roff[i] * n3, g0->ffb.p + roff[i] * n3, nbsphere[i], nrhs[i], n3, ALPHA_ISO,
+                        g0->ralpha.p + aoff[i], nbsphere[i], st);
+        for (int q = 0; q < nrhs[i]; q++) {
+            IFDDA_CUDA(cudaMemcpyAsync(FFloc[i] + q * n3i, g0->x.p + (roff[i] + q) * n3, n3i * sizeof(double2),
+                                       out_kind, st));
+            IFDDA_CUDA(cudaMemcpyAsync(FF[i] + q * n3i, g0->ffb.p + (roff[i] + q) * n3, n3i * sizeof(double2),
+                                       out_kind, st));
+        }
+    }
+    IFDDA_CUDA(cudaStreamSynchronize(st));
+    return report_results(res, method, tol, true, tol1, nloop, ncompte, nstop, infostr);
+    IFDDA_GUARD_END(ctx, infostr)
+}
+
 extern "C" {
 
 int ifdda_abi_version(void) { return IFDDA_GPU_ABI_VERSION; }
@@ -654,133 +805,48 @@ int ifdda_inverserig_ragged(int nobj, ifdda_green* const* greens, const int* nrh
                             const ifdda_dcmplx* const* FF0, const char* methodeit, double tol, ifdda_dcmplx* const* FF,
                             ifdda_dcmplx* const* FFloc, double* tol1, int* nloop, int* ncompte, int* nstop,
                             char* infostr, const ifdda_solve_options* opt) {
-    if (nobj < 1 || !greens || !greens[0] || !nrhs || !nbsphere || !nmax || !polarisa || !FF0 || !FF || !FFloc) {
-        if (nstop) *nstop = 1;
-        set_info(infostr, "invalid argument");
+    return ragged_solve(nobj, greens, nrhs, nbsphere, nmax, tabdip, polarisa, FF0, methodeit, tol, FF, FFloc, tol1,
+                        nloop, ncompte, nstop, infostr, opt, false);
+}
+
+int ifdda_inverserig_ragged_device(int nobj, ifdda_green* const* greens, const int* nrhs, const int* nbsphere,
+                                   const int* nmax, const int* const* tabdip_dev,
+                                   const ifdda_dcmplx* const* polarisa_dev, const ifdda_dcmplx* const* FF0_dev,
+                                   const char* methodeit, double tol, ifdda_dcmplx* const* FF_dev,
+                                   ifdda_dcmplx* const* FFloc_dev, double* tol1, int* nloop, int* ncompte, int* nstop,
+                                   char* infostr, const ifdda_solve_options* opt) {
+    return ragged_solve(nobj, greens, nrhs, nbsphere, nmax, tabdip_dev, polarisa_dev, FF0_dev, methodeit, tol, FF_dev,
+                        FFloc_dev, tol1, nloop, ncompte, nstop, infostr, opt, true);
+}
+
+int ifdda_incident_planewaves_device(ifdda_ctx* ctx, int nbsphere, const double* xs_dev, const double* ys_dev,
+                                     const double* zs_dev, double k0, ifdda_dcmplx E0, int nrhs, const int* beam,
+                                     const double* a1, const double* a2, const double* pp, ifdda_dcmplx* FF0_dev) {
+    if (!ctx || !xs_dev || !ys_dev || !zs_dev || !beam || !a1 || !a2 || !pp || !FF0_dev || nbsphere < 1 || nrhs < 1)
         return 1;
-    }
-    ifdda_green* g0 = greens[0];
-    ifdda_ctx* ctx = g0->ctx;
     IFDDA_GUARD_BEGIN
     DeviceScope ds(ctx->device);
     AllocStreamScope as(ctx->stream);
     cudaStream_t st = ctx->stream;
-    const int method = method_code(methodeit);
-    if (method == 0) {
-        if (nstop) *nstop = 1;
-        set_info(infostr, "Iterative method not correct!");
-        return 1;
-    }
-    if (method == 14) throw EngineError{1, "ragged batch: QMRCLA is not supported (its A^T products)"};
-    if (tol < 1e-12 || tol > 0.5) throw EngineError{1, "ragged batch: tolerance outside [1e-12, 0.5]"};
-    const MvGeom& box = g0->G.g;
-    long R = 0, nbmax = 0, nalpha = 0;
-    for (int i = 0; i < nobj; i++) {
-        ifdda_green* g = greens[i];
-        if (!g || g->ctx != ctx) throw EngineError{1, "ragged batch: every spectrum must belong to one context"};
-        if (g->G.g.nx != box.nx || g->G.g.ny != box.ny || g->G.g.nz != box.nz || g->G.nquad != 0)
-            throw EngineError{1, "ragged batch: every spectrum must be on one box (ifdda_green_create_box), nquad 0"};
-        if (nrhs[i] < 1 || nbsphere[i] < 1 || nmax[i] < nbsphere[i] || !polarisa[i] || !FF0[i] || !FF[i] ||
-            !FFloc[i])
-            throw EngineError{1, "ragged batch: invalid object " + std::to_string(i)};
-        if (!(tabdip && tabdip[i]) && nbsphere[i] != g->G.uN)
-            throw EngineError{1, "ragged batch: a full-box object needs nbsphere = nx*ny*nz"};
-        if (tabdip && tabdip[i]) check_tabdip(tabdip[i], g->G.uN, nbsphere[i]);
-        if (pola_mode_range(polarisa[i], 0, nbsphere[i], nmax[i]) != ALPHA_ISO)
-            throw EngineError{1, "ragged batch: only isotropic polarisabilities are supported"};
-        R += nrhs[i];
-        nbmax = std::max<long>(nbmax, nbsphere[i]);
-        nalpha += nbsphere[i];
-    }
-    // every right-hand side is laid out on the box's sites (not on the batch's
-    // largest object), so its vector length, reductions and kernels' work do
-    // not depend on the other objects of the batch: a request gives the same
-    // bits alone and inside any ragged batch on that box
-    const long Nb = box.N, n3 = 3 * Nb, tot = R * n3;
-    if (nbmax > Nb) throw EngineError{1, "ragged batch: an object has more dipoles than the box has sites"};
-    g0->ff0.ensure(tot);
-    g0->x.ensure(tot);
-    g0->ffb.ensure(tot);
-    g0->ralpha.ensure(nalpha);
-    g0->rtab.ensure((size_t)nobj * Nb);
-    g0->rgc64.ensure(R);
-    g0->rgc32.ensure(R);
-    g0->roff.ensure(2 * R);
-    // right-hand sides of every object, each zero-padded to 3 nbmax
-    IFDDA_CUDA(cudaMemsetAsync(g0->ff0.p, 0, tot * sizeof(double2), st));
-    std::vector<const double2*> h64(R);
-    std::vector<const float2*> h32(R);
-    std::vector<long> hoff(2 * R);
-    std::vector<long> aoff(nobj), roff(nobj);
-    long r0 = 0, a0 = 0;
-    for (int i = 0; i < nobj; i++) {
-        ifdda_green* g = greens[i];
-        const long n3i = 3L * nbsphere[i];
-        for (int q = 0; q < nrhs[i]; q++) {
-            IFDDA_CUDA(cudaMemcpyAsync(g0->ff0.p + (r0 + q) * n3, FF0[i] + q * n3i, n3i * sizeof(double2),
-                                       cudaMemcpyHostToDevice, st));
-            h64[r0 + q] = g->G.gc64.p;
-            h32[r0 + q] = g->G.gc32.p;
-            hoff[r0 + q] = a0;
-            hoff[R + r0 + q] = (long)i * Nb;
-        }
-        // the isotropic value of dipole n is polarisa(n,1,1): the first
-        // nbsphere entries of the (nmax,3,3) array
-        IFDDA_CUDA(cudaMemcpyAsync(g0->ralpha.p + a0, polarisa[i], nbsphere[i] * sizeof(double2),
-                                   cudaMemcpyHostToDevice, st));
-        // the object's Tabdip on the common box (identity for a full box)
-        const int* src = nullptr;
-        if (tabdip && tabdip[i]) {
-            g0->rtab_in.ensure(g->G.uN);
-            IFDDA_CUDA(cudaMemcpyAsync(g0->rtab_in.p, tabdip[i], g->G.uN * sizeof(int), cudaMemcpyHostToDevice, st));
-            src = g0->rtab_in.p;
-        }
-        count_launch();
-        k_pad_tab<<<(int)std::min<long>((Nb + 255) / 256, 148L * 16), 256, 0, st>>>(
-            src, g0->rtab.p + (long)i * Nb, g->G.ux, g->G.uy, g->G.uz, box.nx, box.ny, Nb);
-        IFDDA_CUDA(cudaGetLastError());
-        // rtab_in is reused by the next object: its copy must be done
-        if (src) IFDDA_CUDA(cudaStreamSynchronize(st));
-        aoff[i] = a0;
-        roff[i] = r0;
-        r0 += nrhs[i];
-        a0 += nbsphere[i];
-    }
-    IFDDA_CUDA(cudaMemcpyAsync(g0->rgc64.p, h64.data(), R * sizeof(const double2*), cudaMemcpyHostToDevice, st));
-    IFDDA_CUDA(cudaMemcpyAsync(g0->rgc32.p, h32.data(), R * sizeof(const float2*), cudaMemcpyHostToDevice, st));
-    IFDDA_CUDA(cudaMemcpyAsync(g0->roff.p, hoff.data(), 2 * R * sizeof(long), cudaMemcpyHostToDevice, st));
-    SolveSpec sp = make_spec(method, (int)R, (int)Nb, tol, opt);
-    sp.tabdip = g0->rtab.p;
-    sp.amode = ALPHA_ISO;
-    sp.alpha = g0->ralpha.p;
-    sp.nmax = nalpha;
-    sp.cancel = (volatile int*)nstop;
-    sp.gc64_r = g0->rgc64.p;
-    sp.gc32_r = g0->rgc32.p;
-    sp.alpha_off = g0->roff.p;
-    sp.tab_off = g0->roff.p + R;
-    if (nstop && *nstop == -1) {
-        set_info(infostr, "Calculation cancelled during iterative method");
-        return -1;
-    }
-    std::vector<SolveResult> res;
-    if (opt && opt->precision == IFDDA_MIXED) solve_mixed(g0->G, g0->SW, sp, g0->ff0.p, g0->x.p, res, st);
-    else solve_fp64(g0->G, g0->SW, sp, g0->ff0.p, g0->x.p, res, st);
-    for (int i = 0; i < nobj; i++) {
-        const long n3i = 3L * nbsphere[i];
-        // FF = polarisa . E (cdmlib/inverserigopt.f:92-97), per object
-        apply_alpha_dev(g0->x.p + roff[i] * n3, g0->ffb.p + roff[i] * n3, nbsphere[i], nrhs[i], n3, ALPHA_ISO,
-                        g0->ralpha.p + aoff[i], nbsphere[i], st);
-        for (int q = 0; q < nrhs[i]; q++) {
-            IFDDA_CUDA(cudaMemcpyAsync(FFloc[i] + q * n3i, g0->x.p + (roff[i] + q) * n3, n3i * sizeof(double2),
-                                       cudaMemcpyDeviceToHost, st));
-            IFDDA_CUDA(cudaMemcpyAsync(FF[i] + q * n3i, g0->ffb.p + (roff[i] + q) * n3, n3i * sizeof(double2),
-                                       cudaMemcpyDeviceToHost, st));
-        }
-    }
+    DevBuf<double> d1, d2, dp;
+    DevBuf<int> db;
+    d1.ensure(nrhs);
+    d2.ensure(nrhs);
+    dp.ensure(nrhs);
+    db.ensure(nrhs);
+    IFDDA_CUDA(cudaMemcpyAsync(d1.p, a1, nrhs * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(d2.p, a2, nrhs * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(dp.p, pp, nrhs * sizeof(double), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemcpyAsync(db.p, beam, nrhs * sizeof(int), cudaMemcpyHostToDevice, st));
+    IFDDA_CUDA(cudaMemsetAsync(ctx->flag.p, 0, sizeof(int), st));
+    planewaves_dev(nbsphere, xs_dev, ys_dev, zs_dev, k0, make_double2(E0.re, E0.im), nrhs, db.p, d1.p, d2.p, dp.p,
+                   (double2*)FF0_dev, ctx->flag.p, st);
+    int bad = 0;
+    IFDDA_CUDA(cudaMemcpyAsync(&bad, ctx->flag.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     IFDDA_CUDA(cudaStreamSynchronize(st));
-    return report_results(res, method, tol, true, tol1, nloop, ncompte, nstop, infostr);
-    IFDDA_GUARD_END(ctx, infostr)
+    if (bad) throw EngineError{1, "problem in plance incident wave"};
+    return 0;
+    IFDDA_GUARD_END(ctx, nullptr)
 }
 
 int ifdda_inverserig(ifdda_green* g, int nbsphere, int nmax, const int* tabdip, const ifdda_dcmplx* polarisa,

@@ -57,6 +57,8 @@ SIGNATURES = {
                                          C.c_double, C.POINTER(_vp)]),
     "ifdda_inverserig_ragged": (C.c_int, [C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_char_p, C.c_double, _vp,
                                           _vp, _vp, _vp, _vp, _ip, C.c_char_p, C.POINTER(SolveOptions)]),
+    "ifdda_inverserig_ragged_device": (C.c_int, [C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_char_p, C.c_double,
+                                                 _vp, _vp, _vp, _vp, _vp, _ip, C.c_char_p, C.POINTER(SolveOptions)]),
     "ifdda_green_destroy": (C.c_int, [_vp]),
     "ifdda_green_release_workspace": (C.c_int, [_vp]),
     "ifdda_green_export": (C.c_int, [_vp] + [_vp] * 6),
@@ -74,6 +76,8 @@ SIGNATURES = {
     "ifdda_cross_sections": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_double, C.c_double, _dp, _dp]),
     "ifdda_incident_planewaves": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_double, DComplex, C.c_int, _vp, _vp,
                                             _vp, _vp, _vp]),
+    "ifdda_incident_planewaves_device": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, C.c_double, DComplex, C.c_int, _vp,
+                                                   _vp, _vp, _vp, _vp]),
     "ifdda_farfield_csca": (C.c_int, [_vp, C.c_int, _vp, _vp, _vp, _vp, C.c_double, C.c_double, C.c_double,
                                       C.c_double, C.c_int, C.c_int, _dp, _dp, _vp, _vp, _vp]),
     "ifdda_farfield_fft": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_double, _vp, _vp, _vp, _vp, C.c_double,

@@ -233,6 +233,49 @@ class Context:
                                                   _p(pz), _p(inc), _p(loc), _p(mac)))
         return dict(xswf=px, yswf=py, zswf=pz, incident=inc, local=loc, macro=mac)
 
+    def planewaves_device(self, nbsphere, xs_ptr, ys_ptr, zs_ptr, k0, E0, beam, a1, a2, pp, out_ptr):
+        """planewaves with device positions and a device result (pointers,
+        e.g. torch data_ptr()); beam, a1, a2, pp are host sequences."""
+        beam = np.ascontiguousarray(np.atleast_1d(beam), np.int32)
+        a1 = np.ascontiguousarray(np.atleast_1d(a1), np.float64)
+        a2 = np.ascontiguousarray(np.atleast_1d(a2), np.float64)
+        pp = np.ascontiguousarray(np.atleast_1d(pp), np.float64)
+        e0 = complex(E0)
+        self._check(self.lib.ifdda_incident_planewaves_device(
+            self.h, int(nbsphere), C.c_void_p(xs_ptr), C.c_void_p(ys_ptr), C.c_void_p(zs_ptr), k0,
+            DComplex(e0.real, e0.imag), len(beam), _p(beam), _p(a1), _p(a2), _p(pp), C.c_void_p(out_ptr)))
+
+    def inverserig_ragged_device(self, items, methodeit="GPBICG1", tol=1e-4, precision=IFDDA_FP64, maxit=0):
+        """Ragged batch on device pointers: items = [(green, nbsphere, nmax,
+        tabdip_ptr or None, polarisa_ptr, FF0_ptr, FF_ptr, FFloc_ptr, nrhs)].
+        Returns (tol1, nloop, ncompte, nstop, infostr), counters per
+        right-hand side in item order."""
+        n = len(items)
+        arr = lambda t, vals: (t * n)(*vals)
+        greens = arr(C.c_void_p, [it[0].h for it in items])
+        nbs = arr(C.c_int, [int(it[1]) for it in items])
+        nmaxs = arr(C.c_int, [int(it[2]) for it in items])
+        tabs = arr(C.c_void_p, [it[3] for it in items])
+        pols = arr(C.c_void_p, [it[4] for it in items])
+        p_ff0 = arr(C.c_void_p, [it[5] for it in items])
+        p_ff = arr(C.c_void_p, [it[6] for it in items])
+        p_loc = arr(C.c_void_p, [it[7] for it in items])
+        nrhs = arr(C.c_int, [int(it[8]) for it in items])
+        R = sum(int(it[8]) for it in items)
+        tol1 = np.zeros(R)
+        nloop = np.zeros(R, np.int32)
+        ncompte = np.zeros(R, np.int32)
+        nstop = C.c_int(0)
+        info = C.create_string_buffer(b" " * 64, 65)
+        opt = SolveOptions(precision, 0, 0, 0.0, maxit)
+        rc = self.lib.ifdda_inverserig_ragged_device(n, greens, nrhs, nbs, nmaxs, tabs, pols, p_ff0,
+                                                     methodeit.encode(), float(tol), p_ff, p_loc, _p(tol1),
+                                                     _p(nloop), _p(ncompte), C.byref(nstop), info, C.byref(opt))
+        infostr = info.raw[:64].decode(errors="replace")
+        if rc == 1 and nstop.value == 0:
+            raise IfddaError(self.last_error() or infostr.strip())
+        return tol1, nloop, ncompte, nstop.value, infostr
+
     def planewaves(self, xs, ys, zs, k0, E0, beam, a1, a2, pp) -> np.ndarray:
         """FF0 for a batch of plane waves: beam 0 = ondeplane(theta, phi deg),
         1 = ondeplanekxky(kx, ky).  Returns (nrhs, 3*nbsphere)."""

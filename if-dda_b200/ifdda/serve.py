@@ -66,15 +66,22 @@ class Result:
     green_hit: bool
 
 
+def _request_inputs_bytes(N: int, nrhs: int) -> int:
+    """A request's device inputs and outputs (_DeviceRequest): incident,
+    dipole-moment and local fields, the (nmax,3,3) polarisability, positions,
+    Tabdip and the isotropic alpha."""
+    return 3 * (3 * N * 16) * nrhs + 9 * N * 16 + 3 * N * 8 + N * 4 + N * 16
+
+
 def footprint_bytes(n: int, nrhs: int, precision: int) -> int:
     """Device bytes one solve holds: the spectrum (FP64 + FP32), mat-vec
-    scratch, Krylov vectors and inputs."""
+    scratch, Krylov vectors and the request's inputs and outputs."""
     N = n ** 3
     Np = (n + 1) ** 3
     green = 6 * Np * (16 + 8)
     scr64 = 18 * N * 16 * nrhs
     vec64 = 14 * 3 * N * 16 * nrhs
-    io = 4 * 3 * N * 16 * nrhs + N * 16
+    io = _request_inputs_bytes(N, nrhs) + N * 16
     if precision == IFDDA_MIXED:
         return green + scr64 + 18 * N * 8 * nrhs + 14 * 3 * N * 8 * nrhs + 2 * 3 * N * 16 * nrhs + io
     return green + scr64 + vec64 + io
@@ -86,7 +93,8 @@ def ragged_footprint_bytes(box: int, nrhs: int, precision: int) -> int:
     N = box ** 3
     scr64 = 18 * N * 16 * nrhs
     vec64 = 14 * 3 * N * 16 * nrhs
-    io = 3 * 3 * N * 16 * nrhs + 2 * N * 16
+    # the batch's own field copies on the box, and the request's inputs
+    io = 3 * 3 * N * 16 * nrhs + 2 * N * 16 + _request_inputs_bytes(N, nrhs)
     if precision == IFDDA_MIXED:
         return scr64 + 18 * N * 8 * nrhs + 14 * 3 * N * 8 * nrhs + 2 * 3 * N * 16 * nrhs + io
     return scr64 + vec64 + io
@@ -140,8 +148,10 @@ def build_object(req: Request):
 
 class _Slot:
     def __init__(self, idx: int, device: int, cache_size: int):
+        import torch
         self.idx = idx
         self.ctx = Context(device)
+        self.dev = torch.device("cuda", device)
         self.cache = collections.OrderedDict()
         self.cache_size = cache_size
 
@@ -167,46 +177,82 @@ class _Slot:
         self.ctx.close()
 
 
-def solve_request(slot: _Slot, req: Request, precision: int, tol: float = 1e-4, methodeit: str = "GPBICG1"):
-    ob, k0 = build_object(req)
-    E0, _ = objects.irradiance(1.0, 10 * req.wavelength)
-    kx = [a * k0 for a, _, _ in req.incidences]
-    ky = [b * k0 for _, b, _ in req.incidences]
-    pp = [c for _, _, c in req.incidences]
-    ff0 = slot.ctx.planewaves(ob.xs, ob.ys, ob.zs, k0, E0, [1] * len(kx), kx, ky, pp)
-    g, hit = slot.green(ob, k0)
-    r = g.inverserig(ob.nbsphere, ob.polarisa, ob.nmax, ff0, methodeit, tol, tabdip=ob.tabdip_or_none,
-                     precision=precision)
-    # a cached spectrum keeps no workspace: the HBM budget covers in-flight solves only
-    g.release_workspace()
-    return r, hit
+class _DeviceRequest:
+    """One request's inputs on the device (torch tensors on the slot's
+    device): positions, incident fields built there, the (nmax,3,3)
+    polarisability with its diagonal set from the isotropic alpha, Tabdip,
+    and room for the fields.  Only the alpha, positions and Tabdip cross
+    from the host; the local field is the one result read back."""
 
-
-def solve_ragged(slot: _Slot, reqs, box: int, precision: int, tol: float = 1e-4, methodeit: str = "GPBICG1"):
-    """One ragged batch: every request's object on the common box side `box`.
-    Returns one (SolveResult-like dict, green_hit) per request."""
-    items, hits, shapes = [], [], []
-    for req in reqs:
+    def __init__(self, slot, req: Request):
+        import torch
         ob, k0 = build_object(req)
+        self.ob, self.k0 = ob, k0
         E0, _ = objects.irradiance(1.0, 10 * req.wavelength)
+        dev = slot.dev
+        nb, nmax = ob.nbsphere, ob.nmax
+        self.nrhs = len(req.incidences)
+        self.xs = torch.from_numpy(np.ascontiguousarray(ob.xs, np.float64)).to(dev)
+        self.ys = torch.from_numpy(np.ascontiguousarray(ob.ys, np.float64)).to(dev)
+        self.zs = torch.from_numpy(np.ascontiguousarray(ob.zs, np.float64)).to(dev)
+        alpha = torch.from_numpy(np.ascontiguousarray(ob.alpha, np.complex128)).to(dev)
+        self.pol = torch.zeros(9 * nmax, dtype=torch.complex128, device=dev)
+        for q in (0, 4, 8):  # (n,a,a) at n + nmax*(a + 3a)
+            self.pol[q * nmax:q * nmax + nb] = alpha
+        self.tab = (torch.from_numpy(np.ascontiguousarray(ob.tabdip, np.int32)).to(dev) if ob.inside_only
+                    else None)
+        self.ff0 = torch.empty((self.nrhs, 3 * nb), dtype=torch.complex128, device=dev)
+        self.ff = torch.empty_like(self.ff0)
+        self.loc = torch.empty_like(self.ff0)
+        torch.cuda.synchronize(dev)
         kx = [a * k0 for a, _, _ in req.incidences]
         ky = [b * k0 for _, b, _ in req.incidences]
         pp = [c for _, _, c in req.incidences]
-        ff0 = slot.ctx.planewaves(ob.xs, ob.ys, ob.zs, k0, E0, [1] * len(kx), kx, ky, pp)
-        g, hit = slot.green(ob, k0, box)
-        items.append((g, ob.nbsphere, ob.nmax, ob.tabdip_or_none, ob.polarisa, ff0))
+        slot.ctx.planewaves_device(nb, self.xs.data_ptr(), self.ys.data_ptr(), self.zs.data_ptr(), k0, E0,
+                                   [1] * len(kx), kx, ky, pp, self.ff0.data_ptr())
+
+    @property
+    def tab_ptr(self):
+        return self.tab.data_ptr() if self.tab is not None else None
+
+
+def solve_request(slot: _Slot, req: Request, precision: int, tol: float = 1e-4, methodeit: str = "GPBICG1"):
+    """One request on its own: incident fields built on the device, the
+    batched solve of its incidences on device buffers, the local field read
+    back.  Returns (result dict, green_hit)."""
+    d = _DeviceRequest(slot, req)
+    ob = d.ob
+    g, hit = slot.green(ob, d.k0)
+    r = g.inverserig_device(d.nrhs, ob.nbsphere, ob.nmax, d.tab_ptr, d.pol.data_ptr(), d.ff0.data_ptr(),
+                            d.ff.data_ptr(), d.loc.data_ptr(), methodeit, tol, precision=precision)
+    FFloc = d.loc.cpu().numpy()
+    # a cached spectrum keeps no workspace: the HBM budget covers in-flight solves only
+    g.release_workspace()
+    return dict(FFloc=FFloc, tol1=r["tol1"], nloop=r["nloop"], ncompte=r["ncompte"], nstop=r["nstop"],
+                infostr=r["infostr"]), hit
+
+
+def solve_ragged(slot: _Slot, reqs, box: int, precision: int, tol: float = 1e-4, methodeit: str = "GPBICG1"):
+    """One ragged batch on the device: every request's object on the common
+    box side `box`.  Returns one (result dict, green_hit) per request."""
+    items, hits, dreqs = [], [], []
+    for req in reqs:
+        d = _DeviceRequest(slot, req)
+        g, hit = slot.green(d.ob, d.k0, box)
+        items.append((g, d.ob.nbsphere, d.ob.nmax, d.tab_ptr, d.pol.data_ptr(), d.ff0.data_ptr(), d.ff.data_ptr(),
+                      d.loc.data_ptr(), d.nrhs))
         hits.append(hit)
-        shapes.append(len(kx))
-    fields, tol1, nloop, ncompte, nstop, info = slot.ctx.inverserig_ragged(items, methodeit, tol,
-                                                                           precision=precision)
+        dreqs.append(d)
+    tol1, nloop, ncompte, nstop, info = slot.ctx.inverserig_ragged_device(items, methodeit, tol,
+                                                                          precision=precision)
     items[0][0].release_workspace()
     out, r0 = [], 0
-    for (FF, FFloc), nr, hit in zip(fields, shapes, hits):
-        sl = slice(r0, r0 + nr)
+    for d, hit in zip(dreqs, hits):
+        sl = slice(r0, r0 + d.nrhs)
         ok = bool(np.all(tol1[sl] < tol))
-        out.append((dict(FFloc=FFloc, tol1=tol1[sl].copy(), nloop=nloop[sl].copy(), ncompte=ncompte[sl].copy(),
-                         nstop=0 if (nstop == 0 or ok) else nstop, infostr=info), hit))
-        r0 += nr
+        out.append((dict(FFloc=d.loc.cpu().numpy(), tol1=tol1[sl].copy(), nloop=nloop[sl].copy(),
+                         ncompte=ncompte[sl].copy(), nstop=0 if (nstop == 0 or ok) else nstop, infostr=info), hit))
+        r0 += d.nrhs
     return out
 
 
@@ -330,8 +376,9 @@ class Server:
                         self.cv.notify_all()
                 end = time.perf_counter() - t0
                 with lock:
-                    results[req.rid] = Result(req.rid, r.FFloc, r.tol1, r.nloop, r.ncompte, r.nstop, r.infostr,
-                                              start, end, req.arrival if realtime else 0.0, slot.idx, hit)
+                    results[req.rid] = Result(req.rid, r["FFloc"], r["tol1"], r["nloop"], r["ncompte"], r["nstop"],
+                                              r["infostr"], start, end, req.arrival if realtime else 0.0, slot.idx,
+                                              hit)
 
         target = worker_ragged if self.ragged else worker
         threads = [threading.Thread(target=target, args=(s,), daemon=True) for s in self.slots]

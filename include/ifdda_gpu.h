@@ -214,6 +214,18 @@ int ifdda_inverserig_ragged(int nobj, ifdda_green* const* greens, const int* nrh
                             ifdda_dcmplx* const* FFloc, double* tol1, int* nloop, int* ncompte, int* nstop,
                             char* infostr, const ifdda_solve_options* opt);
 
+/* The same with every per-object array in device memory of the context's
+   device (tabdip_dev[i] may be NULL): the polarisability is checked for
+   isotropy and compacted on the device.  For a request loop that builds its
+   incident fields on the device (ifdda_incident_planewaves_device) and reads
+   back only what a request returns. */
+int ifdda_inverserig_ragged_device(int nobj, ifdda_green* const* greens, const int* nrhs, const int* nbsphere,
+                                   const int* nmax, const int* const* tabdip_dev,
+                                   const ifdda_dcmplx* const* polarisa_dev, const ifdda_dcmplx* const* FF0_dev,
+                                   const char* methodeit, double tol, ifdda_dcmplx* const* FF_dev,
+                                   ifdda_dcmplx* const* FFloc_dev, double* tol1, int* nloop, int* ncompte, int* nstop,
+                                   char* infostr, const ifdda_solve_options* opt);
+
 /* Local -> macroscopic field of every dipole (nsens = 1), replacing the loop
    of cdmlib/cdmlib.f:2595-2655 over local_macro (cdmlib/local-macro.f:3-71);
    the 3x3 inverse is evaluated in closed form on the device.  epsilon is
@@ -235,6 +247,13 @@ int ifdda_cross_sections(ifdda_ctx* ctx, int nbsphere, const ifdda_dcmplx* FF0, 
 int ifdda_incident_planewaves(ifdda_ctx* ctx, int nbsphere, const double* xs, const double* ys, const double* zs,
                               double k0, ifdda_dcmplx E0, int nrhs, const int* beam, const double* a1,
                               const double* a2, const double* pp, ifdda_dcmplx* FF0);
+
+/* ifdda_incident_planewaves with the dipole positions (xs_dev, ys_dev,
+   zs_dev) and the result FF0_dev in device memory of the context's device;
+   beam, a1, a2, pp stay host arrays of nrhs entries. */
+int ifdda_incident_planewaves_device(ifdda_ctx* ctx, int nbsphere, const double* xs_dev, const double* ys_dev,
+                                     const double* zs_dev, double k0, ifdda_dcmplx E0, int nrhs, const int* beam,
+                                     const double* a1, const double* a2, const double* pp, ifdda_dcmplx* FF0_dev);
 
 /* Scattering cross section Cscai, asymmetry factor gasym and far-field
    Poynting vector by direct summation of the dipole moments FF over the

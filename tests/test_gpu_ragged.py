@@ -119,3 +119,41 @@ def test_ragged_batch_rejects_mismatched_boxes(gctx):
         gctx.green_box(8, 8, 8, (6, 8, 8), ob.aretecube, k0)
     ga.close()
     gb.close()
+
+
+def test_ragged_device_entry_matches_host_entry(gctx, orc):
+    """ifdda_inverserig_ragged_device (every per-object array on the device,
+    the polarisability compacted there) gives the host entry's bits, and
+    ifdda_incident_planewaves_device the host planewaves' bits."""
+    import torch
+    items, greens, ff0s = _items(gctx, orc)
+    fields, tol1, nloop, ncompte, nstop, info = gctx.inverserig_ragged(items, "GPBICG1", 1e-4, precision=1)
+    assert nstop == 0, info
+    keep, ditems = [], []
+    for (g, nb, nmax, tab, pol, ff0) in items:
+        t = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in
+             (("pol", pol), ("ff0", ff0)) }
+        t["tab"] = torch.from_numpy(np.ascontiguousarray(tab, np.int32)).cuda() if tab is not None else None
+        t["ff"] = torch.empty_like(t["ff0"])
+        t["loc"] = torch.empty_like(t["ff0"])
+        keep.append(t)
+        ditems.append((g, nb, nmax, t["tab"].data_ptr() if t["tab"] is not None else None, t["pol"].data_ptr(),
+                       t["ff0"].data_ptr(), t["ff"].data_ptr(), t["loc"].data_ptr(), ff0.shape[0]))
+    d1, dl, dc, ds, dinfo = gctx.inverserig_ragged_device(ditems, "GPBICG1", 1e-4, precision=1)
+    assert ds == 0, dinfo
+    assert np.array_equal(d1, tol1) and np.array_equal(dc, ncompte) and np.array_equal(dl, nloop)
+    for t, (FF, FFloc) in zip(keep, fields):
+        assert np.array_equal(t["loc"].cpu().numpy(), FFloc) and np.array_equal(t["ff"].cpu().numpy(), FF)
+    # incident fields built on the device
+    from ifdda import objects
+    ob, k0, _ = _objects()[0]
+    E0, _ = objects.irradiance(1.0, 10 * 2 * math.pi / k0)
+    kx, ky, pp = [0.1 * k0, -0.3 * k0], [0.2 * k0, 0.0], [0.0, 1.0]
+    host = gctx.planewaves(ob.xs, ob.ys, ob.zs, k0, E0, [1, 1], kx, ky, pp)
+    xs, ys, zs = (torch.from_numpy(np.ascontiguousarray(v, np.float64)).cuda() for v in (ob.xs, ob.ys, ob.zs))
+    out = torch.empty(host.shape, dtype=torch.complex128, device="cuda")
+    gctx.planewaves_device(ob.nbsphere, xs.data_ptr(), ys.data_ptr(), zs.data_ptr(), k0, E0, [1, 1], kx, ky, pp,
+                           out.data_ptr())
+    assert np.array_equal(out.cpu().numpy(), host)
+    for g in greens:
+        g.close()
