@@ -64,6 +64,9 @@ class Result:
     arrival: float
     slot: int
     green_hit: bool
+    # seconds spent in this request's (or its ragged batch's) phases: host
+    # object build and device inputs, Green spectra, solve, read-back
+    phases: dict = field(default_factory=dict)
 
 
 def _request_inputs_bytes(N: int, nrhs: int) -> int:
@@ -82,9 +85,12 @@ def footprint_bytes(n: int, nrhs: int, precision: int) -> int:
     scr64 = 18 * N * 16 * nrhs
     vec64 = 14 * 3 * N * 16 * nrhs
     io = _request_inputs_bytes(N, nrhs) + N * 16
+    # solver bookkeeping (reductions, states, captured loops) and allocator
+    # granularity: 8 MiB
+    extra = 8 << 20
     if precision == IFDDA_MIXED:
-        return green + scr64 + 18 * N * 8 * nrhs + 14 * 3 * N * 8 * nrhs + 2 * 3 * N * 16 * nrhs + io
-    return green + scr64 + vec64 + io
+        return green + scr64 + 18 * N * 8 * nrhs + 14 * 3 * N * 8 * nrhs + 2 * 3 * N * 16 * nrhs + io + extra
+    return green + scr64 + vec64 + io + extra
 
 
 def ragged_footprint_bytes(box: int, nrhs: int, precision: int) -> int:
@@ -220,38 +226,53 @@ def solve_request(slot: _Slot, req: Request, precision: int, tol: float = 1e-4, 
     """One request on its own: incident fields built on the device, the
     batched solve of its incidences on device buffers, the local field read
     back.  Returns (result dict, green_hit)."""
+    t0 = time.perf_counter()
     d = _DeviceRequest(slot, req)
     ob = d.ob
+    t1 = time.perf_counter()
     g, hit = slot.green(ob, d.k0)
+    t2 = time.perf_counter()
     r = g.inverserig_device(d.nrhs, ob.nbsphere, ob.nmax, d.tab_ptr, d.pol.data_ptr(), d.ff0.data_ptr(),
                             d.ff.data_ptr(), d.loc.data_ptr(), methodeit, tol, precision=precision)
+    t3 = time.perf_counter()
     FFloc = d.loc.cpu().numpy()
     # a cached spectrum keeps no workspace: the HBM budget covers in-flight solves only
     g.release_workspace()
+    t4 = time.perf_counter()
     return dict(FFloc=FFloc, tol1=r["tol1"], nloop=r["nloop"], ncompte=r["ncompte"], nstop=r["nstop"],
-                infostr=r["infostr"]), hit
+                infostr=r["infostr"], phases=dict(inputs=t1 - t0, green=t2 - t1, solve=t3 - t2,
+                                                  readback=t4 - t3)), hit
 
 
 def solve_ragged(slot: _Slot, reqs, box: int, precision: int, tol: float = 1e-4, methodeit: str = "GPBICG1"):
     """One ragged batch on the device: every request's object on the common
     box side `box`.  Returns one (result dict, green_hit) per request."""
     items, hits, dreqs = [], [], []
+    t_in = t_gr = 0.0
     for req in reqs:
+        t0 = time.perf_counter()
         d = _DeviceRequest(slot, req)
+        t1 = time.perf_counter()
         g, hit = slot.green(d.ob, d.k0, box)
+        t_in += t1 - t0
+        t_gr += time.perf_counter() - t1
         items.append((g, d.ob.nbsphere, d.ob.nmax, d.tab_ptr, d.pol.data_ptr(), d.ff0.data_ptr(), d.ff.data_ptr(),
                       d.loc.data_ptr(), d.nrhs))
         hits.append(hit)
         dreqs.append(d)
+    t2 = time.perf_counter()
     tol1, nloop, ncompte, nstop, info = slot.ctx.inverserig_ragged_device(items, methodeit, tol,
                                                                           precision=precision)
+    t3 = time.perf_counter()
     items[0][0].release_workspace()
     out, r0 = [], 0
-    for d, hit in zip(dreqs, hits):
+    locs = [d.loc.cpu().numpy() for d in dreqs]
+    ph = dict(inputs=t_in, green=t_gr, solve=t3 - t2, readback=time.perf_counter() - t3)
+    for d, hit, loc in zip(dreqs, hits, locs):
         sl = slice(r0, r0 + d.nrhs)
         ok = bool(np.all(tol1[sl] < tol))
-        out.append((dict(FFloc=d.loc.cpu().numpy(), tol1=tol1[sl].copy(), nloop=nloop[sl].copy(),
-                         ncompte=ncompte[sl].copy(), nstop=0 if (nstop == 0 or ok) else nstop, infostr=info), hit))
+        out.append((dict(FFloc=loc, tol1=tol1[sl].copy(), nloop=nloop[sl].copy(), ncompte=ncompte[sl].copy(),
+                         nstop=0 if (nstop == 0 or ok) else nstop, infostr=info, phases=ph), hit))
         r0 += d.nrhs
     return out
 
@@ -360,7 +381,7 @@ class Server:
                     for req, (r, hit) in zip(batch, outs):
                         results[req.rid] = Result(req.rid, r["FFloc"], r["tol1"], r["nloop"], r["ncompte"],
                                                   r["nstop"], r["infostr"], start, end,
-                                                  req.arrival if realtime else 0.0, slot.idx, hit)
+                                                  req.arrival if realtime else 0.0, slot.idx, hit, r["phases"])
 
         def worker(slot: _Slot):
             while True:
@@ -378,7 +399,7 @@ class Server:
                 with lock:
                     results[req.rid] = Result(req.rid, r["FFloc"], r["tol1"], r["nloop"], r["ncompte"], r["nstop"],
                                               r["infostr"], start, end, req.arrival if realtime else 0.0, slot.idx,
-                                              hit)
+                                              hit, r["phases"])
 
         target = worker_ragged if self.ragged else worker
         threads = [threading.Thread(target=target, args=(s,), daemon=True) for s in self.slots]
@@ -392,6 +413,15 @@ class Server:
 def latency_stats(results, wall: float):
     lat = np.array([r.end - r.arrival for r in results])
     nrhs = sum(len(np.atleast_1d(r.tol1)) for r in results)
+    # phase seconds summed over solves (a ragged batch counted once)
+    batches = {}
+    for r in results:
+        batches[(r.slot, r.start)] = r.phases
+    phase_s = {}
+    for ph in batches.values():
+        for k, v in ph.items():
+            phase_s[k] = phase_s.get(k, 0.0) + v
     return dict(p50_ms=float(np.percentile(lat, 50) * 1e3), p99_ms=float(np.percentile(lat, 99) * 1e3),
                 requests_per_s=len(results) / wall, solves_per_s=nrhs / wall,
-                failed=int(sum(r.nstop != 0 for r in results)))
+                failed=int(sum(r.nstop != 0 for r in results)), batches=len(batches),
+                phase_seconds={k: round(v, 3) for k, v in phase_s.items()})
