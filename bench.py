@@ -551,7 +551,7 @@ def run_gpu(args):
             "at_matching_accuracy": (solve_only / serial[match]["solves_s"]) if match else None,
             "fp64_tol_matching": match, "spectrum": "resident in both"},
         "matvec": mv,
-        "tile_chooser": {name: dict(zip(("zconv_variant", "ypass_variant", "ms_z0_z1_y0_y1"), g.tiles(pr, nrhs)))
+        "tile_chooser": {name: dict(zip(("zconv_variant", "ypass_variant", "ms_z0_z1_y0_y1"), g.tiles(pr)))
                          for name, pr in (("fp32", _capi.IFDDA_FP32), ("fp64", _capi.IFDDA_FP64))},
         "green_build_ms": green_ms,
         "roofline": {"bound": "hbm", "kernel": f"k_zconv<float,{Z}> (z FFT + 3x3 spectrum multiply + inverse z FFT)",

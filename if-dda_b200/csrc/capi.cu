@@ -537,11 +537,10 @@ int ifdda_green_create_box(ifdda_ctx* ctx, int nx, int ny, int nz, int bx, int b
     IFDDA_GUARD_END(ctx, nullptr)
 }
 
-int ifdda_green_tiles(ifdda_green* g, int precision, int nrhs, int* zconv_variant, int* ypass_variant,
-                      float* times_ms) {
-    if (!g || nrhs < 1 || (precision != IFDDA_FP32 && precision != IFDDA_FP64)) return 1;
+int ifdda_green_tiles(ifdda_green* g, int precision, int* zconv_variant, int* ypass_variant, float* times_ms) {
+    if (!g || (precision != IFDDA_FP32 && precision != IFDDA_FP64)) return 1;
     TileChoice tc;
-    const bool have = tile_get(g->G.device, precision == IFDDA_FP32 ? 1 : 0, g->G.g, nrhs, tc);
+    const bool have = tile_get(g->G.device, precision == IFDDA_FP32 ? 1 : 0, g->G.g, tc);
     if (zconv_variant) *zconv_variant = have ? tc.zvar : -1;
     if (ypass_variant) *ypass_variant = have ? tc.yvar : -1;
     if (times_ms)
@@ -552,11 +551,11 @@ int ifdda_green_tiles(ifdda_green* g, int precision, int nrhs, int* zconv_varian
     return 0;
 }
 
-int ifdda_green_set_tiles(ifdda_green* g, int precision, int nrhs, int zconv_variant, int ypass_variant) {
-    if (!g || nrhs < 1 || (precision != IFDDA_FP32 && precision != IFDDA_FP64)) return 1;
+int ifdda_green_set_tiles(ifdda_green* g, int precision, int zconv_variant, int ypass_variant) {
+    if (!g || (precision != IFDDA_FP32 && precision != IFDDA_FP64)) return 1;
     const int pk = precision == IFDDA_FP32 ? 1 : 0;
     if (zconv_variant < 0 || ypass_variant < 0) {
-        tile_erase(g->G.device, pk, g->G.g, nrhs);
+        tile_erase(g->G.device, pk, g->G.g);
         return 0;
     }
     if (zconv_variant >= tile_variants(g->G.g.Z) || ypass_variant >= tile_variants(g->G.g.Y)) {
@@ -566,7 +565,7 @@ int ifdda_green_set_tiles(ifdda_green* g, int precision, int nrhs, int zconv_var
     TileChoice tc{};
     tc.zvar = zconv_variant;
     tc.yvar = ypass_variant;
-    tile_put(g->G.device, pk, g->G.g, nrhs, tc);
+    tile_put(g->G.device, pk, g->G.g, tc);
     return 0;
 }
 

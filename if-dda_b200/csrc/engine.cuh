@@ -125,11 +125,14 @@ struct TileChoice {
 };
 
 // Tile chooser results, one per (device, precision 0 FP64 / 1 FP32, grid
-// X x Y x Z, right-hand sides), shared by every spectrum on that grid: a
-// request stream of many spectra on few grids times each grid once.
-bool tile_get(int dev, int prec, const MvGeom& g, int nrhs, TileChoice& out);
-void tile_put(int dev, int prec, const MvGeom& g, int nrhs, const TileChoice& tc);
-void tile_erase(int dev, int prec, const MvGeom& g, int nrhs);
+// X x Y x Z), shared by every spectrum on that grid and every batch size: a
+// request stream of many spectra on few grids times each grid once, and a
+// right-hand side runs the same kernels alone and in a batch (the shapes can
+// differ in the last bits where the compiler contracts multiply-adds
+// differently, so one grid keeps one shape).
+bool tile_get(int dev, int prec, const MvGeom& g, TileChoice& out);
+void tile_put(int dev, int prec, const MvGeom& g, const TileChoice& tc);
+void tile_erase(int dev, int prec, const MvGeom& g);
 
 // Green spectrum of one (lattice, spacing, wavenumber), device resident.
 struct Green {
@@ -149,8 +152,8 @@ struct Green {
     MvWork<float> w32;
     MvWork<double> w64;
     // the tile chooser's result for this grid (shared with every spectrum on
-    // the same grid and device), precision T and nrhs right-hand sides
-    template <class T> bool tile_choice(int nrhs, TileChoice& out) const;
+    // the same grid and device) and precision T
+    template <class T> bool tile_choice(TileChoice& out) const;
     template <class T> const cplx<T>* gc() const;
     template <class T> const cplx<T>* tw(int axis) const;
     template <class T> MvWork<T>& work();
@@ -161,8 +164,8 @@ template <> inline const float2* Green::tw<float>(int a) const { return tw32[a].
 template <> inline const double2* Green::tw<double>(int a) const { return tw64[a].p; }
 template <> inline MvWork<float>& Green::work<float>() { return w32; }
 template <> inline MvWork<double>& Green::work<double>() { return w64; }
-template <class T> inline bool Green::tile_choice(int nrhs, TileChoice& out) const {
-    return tile_get(device, sizeof(T) == 4 ? 1 : 0, g, nrhs, out);
+template <class T> inline bool Green::tile_choice(TileChoice& out) const {
+    return tile_get(device, sizeof(T) == 4 ? 1 : 0, g, out);
 }
 
 MvGeom make_geom(int nx, int ny, int nz);
@@ -214,14 +217,15 @@ MvArgs<T> mv_args(Green& G, int nrhs, const cplx<T>* x, const cplx<T>* b, cplx<T
     a.status = status;
     a.inv_m = (T)(1.0 / ((double)G.g.X * G.g.Y * G.g.Z));
     TileChoice tc;
-    if (G.tile_choice<T>(nrhs, tc)) {
+    if (G.tile_choice<T>(tc)) {
         a.zvar = tc.zvar;
         a.yvar = tc.yvar;
     }
     return a;
 }
 
-// time the tile variants for (T, nrhs) on G's grid once, see mv_impl.cuh
+// time the tile variants of T on G's grid once (with nrhs right-hand sides),
+// see mv_impl.cuh
 template <class T> void tune_tiles(Green& G, int nrhs, cudaStream_t st);
 
 }  // namespace ifdda

@@ -21,27 +21,27 @@ bool fft_length_supported(int L) {
 
 namespace {
 std::mutex g_tile_mu;
-std::map<std::array<int, 6>, TileChoice>& tile_map() {
-    static std::map<std::array<int, 6>, TileChoice> m;
+std::map<std::array<int, 5>, TileChoice>& tile_map() {
+    static std::map<std::array<int, 5>, TileChoice> m;
     return m;
 }
-std::array<int, 6> tile_key(int dev, int prec, const MvGeom& g, int nrhs) { return {dev, prec, g.X, g.Y, g.Z, nrhs}; }
+std::array<int, 5> tile_key(int dev, int prec, const MvGeom& g) { return {dev, prec, g.X, g.Y, g.Z}; }
 }  // namespace
 
-bool tile_get(int dev, int prec, const MvGeom& g, int nrhs, TileChoice& out) {
+bool tile_get(int dev, int prec, const MvGeom& g, TileChoice& out) {
     std::lock_guard<std::mutex> lk(g_tile_mu);
-    auto it = tile_map().find(tile_key(dev, prec, g, nrhs));
+    auto it = tile_map().find(tile_key(dev, prec, g));
     if (it == tile_map().end()) return false;
     out = it->second;
     return true;
 }
-void tile_put(int dev, int prec, const MvGeom& g, int nrhs, const TileChoice& tc) {
+void tile_put(int dev, int prec, const MvGeom& g, const TileChoice& tc) {
     std::lock_guard<std::mutex> lk(g_tile_mu);
-    tile_map()[tile_key(dev, prec, g, nrhs)] = tc;
+    tile_map()[tile_key(dev, prec, g)] = tc;
 }
-void tile_erase(int dev, int prec, const MvGeom& g, int nrhs) {
+void tile_erase(int dev, int prec, const MvGeom& g) {
     std::lock_guard<std::mutex> lk(g_tile_mu);
-    tile_map().erase(tile_key(dev, prec, g, nrhs));
+    tile_map().erase(tile_key(dev, prec, g));
 }
 
 MvGeom make_geom(int nx, int ny, int nz) {

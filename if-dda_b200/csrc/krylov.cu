@@ -443,7 +443,7 @@ template <class T> bool krylov_run(Green& G, const SolveSpec& sp, KrylovWork<T>&
     std::vector<const void*> key;
     if (graphs) {
         TileChoice tcur;
-        const long tile_code = G.tile_choice<T>(nrhs, tcur) ? 1 + tcur.zvar + 2 * tcur.yvar : 0;
+        const long tile_code = G.tile_choice<T>(tcur) ? 1 + tcur.zvar + 2 * tcur.yvar : 0;
         MvWork<T>& mw = G.work<T>();
         mw.ensure(G.g, nrhs);
         W.loopcount.ensure(1);

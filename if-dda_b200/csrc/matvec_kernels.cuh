@@ -89,9 +89,9 @@ template <class T> struct MvArgs {
 //
 // Variant V = 1 (compiled for lengths of 64 and more, where the grid is large
 // enough for the choice to matter) halves the zconv and y tiles; the tile
-// chooser (tune_tiles) times both on the caller's grid and batch and keeps
-// the faster.  A line's arithmetic does not depend on the tile, so both give
-// the same bits.
+// chooser (tune_tiles) times both on the caller's grid and keeps one per
+// grid.  The two agree to rounding (the compiler may contract multiply-adds
+// differently in the two instances).
 constexpr int tile_variants(int L) { return L >= 64 ? 2 : 1; }
 template <class T, int L, int V = 0> struct MvTiles {
     static constexpr int S = (int)sizeof(cplx<T>);

@@ -107,13 +107,15 @@ bool matvec_launch_fused(const MvArgs<T>& a, const Pre& pre, const Epi& epi, con
 // Tile chooser: with G's mat-vec scratch for nrhs right-hand sides (whose
 // contents are about to be overwritten by the next mat-vec anyway), time each
 // tile variant of the y passes (forward then inverse) and of zconv, best of
-// three launches with CUDA events on st, and record the faster for G's grid,
-// device, precision and nrhs (tile_put: every spectrum on that grid then
-// uses it).  Never runs while st is being captured.
+// three launches with CUDA events on st, and record the choice for G's grid,
+// device and precision (tile_put: every spectrum and batch size on that grid
+// then uses it).  Variant 1 is taken only when it is at least 5% faster, so
+// timing noise between near-equal shapes does not flip the choice.  Never
+// runs while st is being captured.
 template <class T> void tune_tiles_impl(Green& G, int nrhs, cudaStream_t st) {
     const int pk = sizeof(T) == 4 ? 1 : 0;
     TileChoice have;
-    if (G.tile_choice<T>(nrhs, have)) return;
+    if (G.tile_choice<T>(have)) return;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     IFDDA_CUDA(cudaStreamIsCapturing(st, &cs));
     if (cs != cudaStreamCaptureStatusNone) return;
@@ -142,19 +144,19 @@ template <class T> void tune_tiles_impl(Green& G, int nrhs, cudaStream_t st) {
             tc.y_ms[v] = time_it([&] {
                 switch (G.g.Y) { IFDDA_FFT_LENGTHS(IFDDA_CASE_TY) default: break; }
             });
-            if (tc.y_ms[v] < tc.y_ms[tc.yvar]) tc.yvar = v;
+            if (tc.y_ms[v] < 0.95f * tc.y_ms[tc.yvar]) tc.yvar = v;
         }
         for (int v = 0; v < nzv; v++) {
             a.zvar = v;
             tc.z_ms[v] = time_it([&] {
                 switch (G.g.Z) { IFDDA_FFT_LENGTHS(IFDDA_CASE_TZ) default: break; }
             });
-            if (tc.z_ms[v] < tc.z_ms[tc.zvar]) tc.zvar = v;
+            if (tc.z_ms[v] < 0.95f * tc.z_ms[tc.zvar]) tc.zvar = v;
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
     }
-    tile_put(G.device, pk, G.g, nrhs, tc);
+    tile_put(G.device, pk, G.g, tc);
 }
 
 }  // namespace ifdda

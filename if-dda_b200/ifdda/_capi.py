@@ -51,8 +51,8 @@ SIGNATURES = {
     "ifdda_green_create_nquad": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
                                            C.POINTER(_vp)]),
     "ifdda_green_recompute": (C.c_int, [_vp, C.c_double, C.c_double]),
-    "ifdda_green_tiles": (C.c_int, [_vp, C.c_int, C.c_int, _ip, _ip, C.POINTER(C.c_float)]),
-    "ifdda_green_set_tiles": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "ifdda_green_tiles": (C.c_int, [_vp, C.c_int, _ip, _ip, C.POINTER(C.c_float)]),
+    "ifdda_green_set_tiles": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int]),
     "ifdda_green_create_box": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                          C.c_double, C.POINTER(_vp)]),
     "ifdda_inverserig_ragged": (C.c_int, [C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_char_p, C.c_double, _vp,

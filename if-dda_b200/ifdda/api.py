@@ -334,16 +334,16 @@ class GreenSpectrum:
         self.ctx._check(self.lib.ifdda_green_recompute(self.h, float(aretecube), float(k0)))
         self.aretecube, self.k0 = float(aretecube), float(k0)
 
-    def tiles(self, precision, nrhs=1):
-        """The tile chooser's (zconv variant, y-pass variant, times ms) for
-        (precision, nrhs); variants are -1 before the first mat-vec."""
+    def tiles(self, precision):
+        """The tile chooser's (zconv shape, y-pass shape, times ms) for this
+        grid and precision; shapes are -1 before the first mat-vec."""
         zv, yv = C.c_int(0), C.c_int(0)
         t = (C.c_float * 4)()
-        self.ctx._check(self.lib.ifdda_green_tiles(self.h, precision, nrhs, C.byref(zv), C.byref(yv), t))
+        self.ctx._check(self.lib.ifdda_green_tiles(self.h, precision, C.byref(zv), C.byref(yv), t))
         return zv.value, yv.value, list(t)
 
-    def set_tiles(self, precision, nrhs, zconv_variant, ypass_variant):
-        self.ctx._check(self.lib.ifdda_green_set_tiles(self.h, precision, nrhs, zconv_variant, ypass_variant))
+    def set_tiles(self, precision, zconv_variant, ypass_variant):
+        self.ctx._check(self.lib.ifdda_green_set_tiles(self.h, precision, zconv_variant, ypass_variant))
 
     def release_workspace(self):
         """Free the solver / mat-vec workspaces; the spectrum stays."""

@@ -158,6 +158,10 @@ class _Slot:
         self.idx = idx
         self.ctx = Context(device)
         self.dev = torch.device("cuda", device)
+        # the slot's device inputs are made and read back on its context's
+        # stream, so a slot waits for its own work only (no device-wide sync
+        # that would wait on, or interfere with, the other slots' solves)
+        self.tstream = torch.cuda.ExternalStream(self.ctx.stream(), device=self.dev)
         self.cache = collections.OrderedDict()
         self.cache_size = cache_size
 
@@ -194,23 +198,25 @@ class _DeviceRequest:
         import torch
         ob, k0 = build_object(req)
         self.ob, self.k0 = ob, k0
+        self.slot = slot
         E0, _ = objects.irradiance(1.0, 10 * req.wavelength)
         dev = slot.dev
         nb, nmax = ob.nbsphere, ob.nmax
         self.nrhs = len(req.incidences)
-        self.xs = torch.from_numpy(np.ascontiguousarray(ob.xs, np.float64)).to(dev)
-        self.ys = torch.from_numpy(np.ascontiguousarray(ob.ys, np.float64)).to(dev)
-        self.zs = torch.from_numpy(np.ascontiguousarray(ob.zs, np.float64)).to(dev)
-        alpha = torch.from_numpy(np.ascontiguousarray(ob.alpha, np.complex128)).to(dev)
-        self.pol = torch.zeros(9 * nmax, dtype=torch.complex128, device=dev)
-        for q in (0, 4, 8):  # (n,a,a) at n + nmax*(a + 3a)
-            self.pol[q * nmax:q * nmax + nb] = alpha
-        self.tab = (torch.from_numpy(np.ascontiguousarray(ob.tabdip, np.int32)).to(dev) if ob.inside_only
-                    else None)
-        self.ff0 = torch.empty((self.nrhs, 3 * nb), dtype=torch.complex128, device=dev)
-        self.ff = torch.empty_like(self.ff0)
-        self.loc = torch.empty_like(self.ff0)
-        torch.cuda.synchronize(dev)
+        with torch.cuda.stream(slot.tstream):
+            self.xs = torch.from_numpy(np.ascontiguousarray(ob.xs, np.float64)).to(dev)
+            self.ys = torch.from_numpy(np.ascontiguousarray(ob.ys, np.float64)).to(dev)
+            self.zs = torch.from_numpy(np.ascontiguousarray(ob.zs, np.float64)).to(dev)
+            alpha = torch.from_numpy(np.ascontiguousarray(ob.alpha, np.complex128)).to(dev)
+            self.pol = torch.zeros(9 * nmax, dtype=torch.complex128, device=dev)
+            for q in (0, 4, 8):  # (n,a,a) at n + nmax*(a + 3a)
+                self.pol[q * nmax:q * nmax + nb] = alpha
+            self.tab = (torch.from_numpy(np.ascontiguousarray(ob.tabdip, np.int32)).to(dev) if ob.inside_only
+                        else None)
+            self.ff0 = torch.empty((self.nrhs, 3 * nb), dtype=torch.complex128, device=dev)
+            self.ff = torch.empty_like(self.ff0)
+            self.loc = torch.empty_like(self.ff0)
+        slot.tstream.synchronize()
         kx = [a * k0 for a, _, _ in req.incidences]
         ky = [b * k0 for _, b, _ in req.incidences]
         pp = [c for _, _, c in req.incidences]
@@ -220,6 +226,13 @@ class _DeviceRequest:
     @property
     def tab_ptr(self):
         return self.tab.data_ptr() if self.tab is not None else None
+
+    def local_field(self) -> np.ndarray:
+        """The local field read back to the host, on the slot's stream."""
+        import torch
+        with torch.cuda.stream(self.slot.tstream):
+            out = self.loc.to("cpu", non_blocking=False)
+        return out.numpy()
 
 
 def solve_request(slot: _Slot, req: Request, precision: int, tol: float = 1e-4, methodeit: str = "GPBICG1"):
@@ -235,7 +248,7 @@ def solve_request(slot: _Slot, req: Request, precision: int, tol: float = 1e-4, 
     r = g.inverserig_device(d.nrhs, ob.nbsphere, ob.nmax, d.tab_ptr, d.pol.data_ptr(), d.ff0.data_ptr(),
                             d.ff.data_ptr(), d.loc.data_ptr(), methodeit, tol, precision=precision)
     t3 = time.perf_counter()
-    FFloc = d.loc.cpu().numpy()
+    FFloc = d.local_field()
     # a cached spectrum keeps no workspace: the HBM budget covers in-flight solves only
     g.release_workspace()
     t4 = time.perf_counter()
@@ -266,7 +279,7 @@ def solve_ragged(slot: _Slot, reqs, box: int, precision: int, tol: float = 1e-4,
     t3 = time.perf_counter()
     items[0][0].release_workspace()
     out, r0 = [], 0
-    locs = [d.loc.cpu().numpy() for d in dreqs]
+    locs = [d.local_field() for d in dreqs]
     ph = dict(inputs=t_in, green=t_gr, solve=t3 - t2, readback=time.perf_counter() - t3)
     for d, hit, loc in zip(dreqs, hits, locs):
         sl = slice(r0, r0 + d.nrhs)

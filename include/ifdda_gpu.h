@@ -85,18 +85,19 @@ int ifdda_green_create_box(ifdda_ctx* ctx, int nx, int ny, int nz, int bx, int b
                            double k0, ifdda_green** out);
 /* Tile chooser.  The zconv and y-pass kernels are compiled with two tile
    shapes for FFT lengths of 64 and more; before the first mat-vec of a
-   precision and a number of right-hand sides on g, the library times both on
-   g's grid (best of three launches with CUDA events) and keeps the faster
-   for every later mat-vec of that (precision, nrhs) on that grid: the choice
-   belongs to the grid and device, shared by every spectrum on them.  The
-   shapes give the same bits.  ifdda_green_tiles reports the choice (-1: not made yet) and,
-   if times_ms is not NULL, the four times measured (zconv variants 0, 1,
-   y passes 0, 1; 0 where not timed).  ifdda_green_set_tiles imposes a
-   choice (-1: choose again at the next mat-vec).  No counterpart in the
-   reference (whose FFT has no tiles). */
-int ifdda_green_tiles(ifdda_green* g, int precision, int nrhs, int* zconv_variant, int* ypass_variant,
-                      float* times_ms);
-int ifdda_green_set_tiles(ifdda_green* g, int precision, int nrhs, int zconv_variant, int ypass_variant);
+   precision on a grid, the library times both on that grid (best of three
+   launches with CUDA events) and keeps shape 1 if it is at least 5% faster,
+   for every later mat-vec of that precision on that grid and device, by
+   every spectrum and batch size: a right-hand side runs the same kernels
+   alone and in a batch.  The two shapes agree to rounding (the compiler may
+   contract multiply-adds differently), not always bit for bit.
+   ifdda_green_tiles reports the choice for g's grid (-1: not made yet) and,
+   if times_ms is not NULL, the four times measured (zconv shapes 0, 1, y
+   passes 0, 1; 0 where not timed).  ifdda_green_set_tiles imposes a choice
+   (-1: choose again at the next mat-vec).  No counterpart in the reference
+   (whose FFT has no tiles). */
+int ifdda_green_tiles(ifdda_green* g, int precision, int* zconv_variant, int* ypass_variant, float* times_ms);
+int ifdda_green_set_tiles(ifdda_green* g, int precision, int zconv_variant, int ypass_variant);
 /* Recomputes g's spectrum in place for another lattice spacing and
    wavenumber (same lattice sides, nquad and padding): the call cdmlib makes
    at cdmlib/cdmlib.f:1529-1531 on every run, writing greencalculfft's result
