@@ -162,6 +162,16 @@ class _Slot:
         # stream, so a slot waits for its own work only (no device-wide sync
         # that would wait on, or interfere with, the other slots' solves)
         self.tstream = torch.cuda.ExternalStream(self.ctx.stream(), device=self.dev)
+        # pinned staging for the local fields read back (grown on demand):
+        # device-to-host copies run at PCIe speed instead of through pageable
+        # memory
+        self.pinned = None
+
+    def staging(self, n: int):
+        import torch
+        if self.pinned is None or self.pinned.numel() < n:
+            self.pinned = torch.empty(int(n * 1.25) + 1, dtype=torch.complex128, pin_memory=True)
+        return self.pinned[:n]
         self.cache = collections.OrderedDict()
         self.cache_size = cache_size
 
@@ -228,11 +238,14 @@ class _DeviceRequest:
         return self.tab.data_ptr() if self.tab is not None else None
 
     def local_field(self) -> np.ndarray:
-        """The local field read back to the host, on the slot's stream."""
+        """The local field read back to the host (through the slot's pinned
+        staging, on the slot's stream) as an array the caller owns."""
         import torch
+        stage = self.slot.staging(self.loc.numel())
         with torch.cuda.stream(self.slot.tstream):
-            out = self.loc.to("cpu", non_blocking=False)
-        return out.numpy()
+            stage.copy_(self.loc.view(-1), non_blocking=True)
+        self.slot.tstream.synchronize()
+        return stage.numpy().reshape(self.loc.shape).copy()
 
 
 def solve_request(slot: _Slot, req: Request, precision: int, tol: float = 1e-4, methodeit: str = "GPBICG1"):
