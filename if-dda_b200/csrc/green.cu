@@ -83,7 +83,7 @@ static void upload_twiddles(int L, DevBuf<double2>& t64, DevBuf<float2>& t32, cu
 
 template <int L> static void launch_gx(const GreenGeom& gg, double2* GA, const double2* tw, cudaStream_t st) {
     using TT = GreenTiles<L>;
-    dim3 grid((gg.Y + TT::TLX - 1) / TT::TLX, gg.Z, 1);
+    dim3 grid((gg.ny + 1 + TT::TLX - 1) / TT::TLX, gg.nz + 1, 1);
     ensure_smem(k_green_x<L>, TT::smem_x);
     count_launch();
     k_green_x<L><<<grid, TT::NT, TT::smem_x, st>>>(gg, GA, tw);
@@ -94,7 +94,7 @@ static void launch_gyz(const GreenGeom& gg, const double2* src, double2* d64, fl
                        cudaStream_t st) {
     using TT = GreenTiles<L>;
     const int W = gg.nx + 1;
-    dim3 grid((W + TT::TLY - 1) / TT::TLY, AXIS == 1 ? gg.Z : gg.ny + 1, 6);
+    dim3 grid((W + TT::TLY - 1) / TT::TLY, AXIS == 1 ? gg.nz + 1 : gg.ny + 1, 6);
     ensure_smem(k_green_yz<L, AXIS>, TT::smem_y);
     count_launch();
     k_green_yz<L, AXIS><<<grid, TT::NT, TT::smem_y, st>>>(gg, src, d64, d32, tw);
@@ -138,8 +138,8 @@ static void green_compute(Green& G, cudaStream_t st) {
     const long W = nx + 1;
     // the intermediate spectra are freed stream-ordered, after the kernels
     DevBuf<double2> GA, GB;
-    GA.ensure((size_t)6 * G.g.Z * G.g.Y * W);
-    GB.ensure((size_t)6 * G.g.Z * (ny + 1) * W);
+    GA.ensure((size_t)6 * (nz + 1) * (ny + 1) * W);
+    GB.ensure((size_t)6 * (nz + 1) * (ny + 1) * W);
     switch (G.g.X) {
 #define IFDDA_CASE_GX(L) \
     case L: launch_gx<L>(gg, GA.p, G.tw64[0].p, st); break;

@@ -1,14 +1,21 @@
 // Green-tensor spectrum on sm_100a, FP64 (replaces cdmlib/calculgreenfft.f:1-104
 // with cdmlib/espace_libre.f:2-43 evaluated on the fly).
 //
-//   gx : for every (j, k) line of the padded grid, evaluate the 6 independent
-//        components of T(r) at r = (i, j, k) d with wrapped negative offsets
-//        and zero planes at i = nx, j = ny, k = nz (calculgreenfft.f:25-69),
-//        FFT along x (sign +1), keep qx in [0, nx]        -> GA[c][Z][Y][nx+1]
-//   gy : FFT along y, keep qy in [0, ny]                   -> GB[c][Z][ny+1][nx+1]
+//   gx : for every (j, k) line with j <= ny, k <= nz, evaluate the 6
+//        independent components of T(r) at r = (i, j, k) d with wrapped
+//        negative offsets along x and zero planes at i = nx, j = ny, k = nz
+//        (calculgreenfft.f:25-69), FFT along x (sign +1), keep qx in [0, nx]
+//                                                          -> GA[c][nz+1][ny+1][nx+1]
+//   gy : FFT along y, keep qy in [0, ny]                   -> GB[c][nz+1][ny+1][nx+1]
 //   gz : FFT along z, keep qz in [0, nz]                   -> Gc64, Gc32
 // Only the parity octant is kept: every component is even or odd along each
 // axis, so the rest of the spectrum is a mirror image (see matvec_kernels.cuh).
+// The same parity holds in real space, T_c(x, -y, z) = Py(c) T_c(x, y, z) and
+// T_c(x, y, -z) = Pz(c) T_c(x, y, z), so the x pass computes the lines with
+// j, k >= 0 only and the y and z passes read the negative offsets as signed
+// mirror images: a quarter of the x-pass lines and half of the y-pass lines,
+// with the same values as lines computed at negative offsets (only signs
+// change).
 #pragma once
 #include "fft_tile.cuh"
 #include "reduce.cuh"
@@ -148,6 +155,10 @@ __global__ void k_green_quad_final(const GreenGeom g, const int3* __restrict__ o
     for (int q = 0; q < 6; q++) out[q] = make_double2(acc[q].x * tmp * f[q], acc[q].y * tmp * f[q]);
 }
 
+// parity of component c (xx, xy, xz, yy, yz, zz) under y -> -y and z -> -z
+__device__ __forceinline__ double green_py(int c) { return (c == 1 || c == 4) ? -1.0 : 1.0; }
+__device__ __forceinline__ double green_pz(int c) { return (c == 2 || c == 4) ? -1.0 : 1.0; }
+
 template <int L>
 __global__ void __launch_bounds__(GreenTiles<L>::NT) k_green_x(const GreenGeom g, double2* __restrict__ GA,
                                                                const double2* __restrict__ twx) {
@@ -157,17 +168,17 @@ __global__ void __launch_bounds__(GreenTiles<L>::NT) k_green_x(const GreenGeom g
     extern __shared__ __align__(16) unsigned char raw[];
     C* tw = reinterpret_cast<C*>(raw);
     C* sm = tw + L;
-    const int j0 = blockIdx.x * TL, kk = blockIdx.y;
-    const int nl = min(TL, g.Y - j0);
+    const int j0 = blockIdx.x * TL, kk = blockIdx.y;  // j <= ny, k <= nz
+    const int nl = min(TL, g.ny + 1 - j0);
     load_twiddles<C, L, NT>(tw, twx);
-    const int k = kk > g.nz ? kk - g.Z : kk;
+    const int k = kk;
     for (int e = threadIdx.x; e < TL * L; e += NT) {
         const int jl = e / L, ii = e - jl * L;
         const int jj = j0 + jl;
         double2 t[6];
         if (jl < nl && ii != g.nx && jj != g.ny && kk != g.nz) {
             const int i = ii > g.nx ? ii - g.X : ii;
-            const int j = jj > g.ny ? jj - g.Y : jj;
+            const int j = jj;
             green_value(g, i, j, k, t);
         } else {
 #pragma unroll
@@ -182,11 +193,13 @@ __global__ void __launch_bounds__(GreenTiles<L>::NT) k_green_x(const GreenGeom g
     for (int e = threadIdx.x; e < NB * W; e += NT) {
         const int bl = e / W, q = e - bl * W;
         const int c = bl / TL, jl = bl - c * TL;
-        if (jl < nl) GA[(((long)c * g.Z + kk) * g.Y + j0 + jl) * W + q] = sm[q * LS + bl];
+        if (jl < nl) GA[(((long)c * (g.nz + 1) + kk) * (g.ny + 1) + j0 + jl) * W + q] = sm[q * LS + bl];
     }
 }
 
-// AXIS 1: GA[c][Z][Y][W] -> GB[c][Z][ny+1][W];  AXIS 2: GB -> Gc[c][nz+1][ny+1][W]
+// AXIS 1: GA[c][nz+1][ny+1][W] -> GB[c][nz+1][ny+1][W], rows y > ny read as
+// Py(c) times row Y - y;  AXIS 2: GB -> Gc[c][nz+1][ny+1][W], planes z > nz
+// read as Pz(c) times plane Z - z
 template <int L, int AXIS>
 __global__ void __launch_bounds__(GreenTiles<L>::NT) k_green_yz(const GreenGeom g, const double2* __restrict__ src,
                                                                 double2* __restrict__ dst64, float2* __restrict__ dst32,
@@ -200,18 +213,22 @@ __global__ void __launch_bounds__(GreenTiles<L>::NT) k_green_yz(const GreenGeom 
     const int W = g.nx + 1;
     const int q0 = blockIdx.x * TL, c = blockIdx.z;
     load_twiddles<C, L, NT>(tw, tw_axis);
-    // AXIS 1: blockIdx.y = kk (0..Z-1), lines along y;  AXIS 2: blockIdx.y = qy (0..ny), lines along z
+    // AXIS 1: blockIdx.y = kk (0..nz), lines along y;  AXIS 2: blockIdx.y = qy (0..ny), lines along z
     const int o = blockIdx.y;
     const int keep = AXIS == 1 ? g.ny + 1 : g.nz + 1;
+    const int half = AXIS == 1 ? g.ny : g.nz;
+    const double sgn = AXIS == 1 ? green_py(c) : green_pz(c);
     for (int e = threadIdx.x; e < TL * L; e += NT) {
         const int p = e / TL, il = e - p * TL;
         const int q = q0 + il;
         C v = make_double2(0, 0);
         if (q < W) {
+            const int pm = p <= half ? p : L - p;  // the mirror of a negative offset
             long idx;
-            if (AXIS == 1) idx = (((long)c * g.Z + o) * g.Y + p) * W + q;
-            else idx = (((long)c * g.Z + p) * (g.ny + 1) + o) * W + q;
+            if (AXIS == 1) idx = (((long)c * (g.nz + 1) + o) * (g.ny + 1) + pm) * W + q;
+            else idx = (((long)c * (g.nz + 1) + pm) * (g.ny + 1) + o) * W + q;
             v = src[idx];
+            if (p > half) v = make_double2(sgn * v.x, sgn * v.y);
         }
         sm[e] = v;
     }
@@ -222,7 +239,7 @@ __global__ void __launch_bounds__(GreenTiles<L>::NT) k_green_yz(const GreenGeom 
         const int q = q0 + il;
         if (q >= W) continue;
         long idx;
-        if (AXIS == 1) idx = (((long)c * g.Z + o) * (g.ny + 1) + p) * W + q;
+        if (AXIS == 1) idx = (((long)c * (g.nz + 1) + o) * (g.ny + 1) + p) * W + q;
         else idx = (((long)c * (g.nz + 1) + p) * (g.ny + 1) + o) * W + q;
         const C v = sm[e];
         dst64[idx] = v;
