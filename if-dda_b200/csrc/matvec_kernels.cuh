@@ -128,14 +128,17 @@ template <class T, int L, int V = 0> struct MvTiles {
     // 384), at about 120 registers a thread; FP64 keeps the usual plan (its
     // 12-point middle for three components would not fit the registers)
     static constexpr int ZP = (S == 8 && plan_len(L, 1) > 0 && plan_len(L, 1) < plan_len(L, 0)) ? 1 : 0;
-    // with the two-pass plan a wider tile (up to ~120 KB, one block per SM)
-    // measured faster: 384^3 took 1.11 ms with 4 columns against 1.37 ms
-    // with 2 (32-byte rows instead of 16)
+    // With the two-pass plan the tile is wider (up to ~120 KB, 32-byte rows
+    // at 384), one block per SM.  Its variant 1 keeps that tile but reads the
+    // spectrum from global memory (L2) instead of staging its slice in shared
+    // memory, and asks for two blocks per SM; otherwise variant 1 halves the
+    // columns.  The tile chooser times the two.
+    static constexpr bool GSLICE = !(ZP && V);
     static constexpr int ztile() {
         const size_t budget = (size_t)(ZP ? 120 : 80) * 1024 * (S / 8);
         int tl = 16;
         while (tl > 1 && zbytes(tl) > budget) tl /= 2;
-        return V && tl > 1 ? tl / 2 : tl;
+        return V && !ZP && tl > 1 ? tl / 2 : tl;
     }
     static constexpr int TLZ = ztile(), NBZ = 6 * TLZ;
     // y tile: odd point stride; z tile: point stride NBZ with one pad point every 16
@@ -146,11 +149,12 @@ template <class T, int L, int V = 0> struct MvTiles {
     static constexpr int NTX = nthreads(NBX), NTY = nthreads(NBY), NTZ = nthreads(NBZ, ZP);
     static constexpr int MINBX = minblocks(NTX, S == 8 ? 80 : 96);
     static constexpr int MINBY = minblocks(NTY, S == 8 ? 80 : 112);
-    static constexpr int MINBZ = minblocks(NTZ, S == 8 ? (ZP ? 128 : 72) : 168);
+    static constexpr int MINBZ = minblocks(NTZ, S == 8 ? (ZP ? (V ? 112 : 128) : 72) : 168);
     static constexpr size_t smem_x = (size_t)L * S + (size_t)NBX * LP * S;
     static constexpr size_t smem_y = (size_t)L * S + (size_t)L * PSY * S;
-    static constexpr size_t smem_z = (size_t)L * S + (size_t)LayZ::span(L) * PSZ * S + (size_t)6 * (L / 2 + 1) * TLZ * S;
-    static_assert(zbytes(TLZ) == smem_z, "z tile size rule and layout disagree");
+    static constexpr size_t smem_z = (size_t)L * S + (size_t)LayZ::span(L) * PSZ * S +
+                                     (GSLICE ? (size_t)6 * (L / 2 + 1) * TLZ * S : 0);
+    static_assert(!GSLICE || zbytes(TLZ) == smem_z, "z tile size rule and layout disagree");
 };
 
 // asynchronous global -> shared copy of one complex element (8 or 16 bytes)
@@ -412,15 +416,16 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
     const int qy = blockIdx.z;                    // 0 .. ny
     const int two = (qy > 0 && qy < ny) ? 2 : 1;  // rows qy and Y - qy
     load_twiddles<C, L, NT>(tw, a.twz);
+    const C* gbase = (a.gc_r ? a.gc_r[rhs] : a.Gc) + qy * (nx + 1);
     // this block's slice of the compressed spectrum (qy fixed, every qz, the
     // TL columns qx(i)) is copied into shared memory while the forward
-    // transform runs
-    {
+    // transform runs (without GSLICE the middle reads it from global memory)
+    if constexpr (TT::GSLICE) {
         static_assert(NT % TL == 0, "a thread keeps one column of the slice");
         const int il = threadIdx.x % TL;
         const int i = min(i0 + il, X - 1);
         const int qxc = i <= nx ? i : X - i;
-        const C* gsrc = (a.gc_r ? a.gc_r[rhs] : a.Gc) + qy * (nx + 1) + qxc;
+        const C* gsrc = gbase + qxc;
         const int gcs = (int)a.g.gc_comp, qzs = (ny + 1) * (nx + 1);
         for (int cq = threadIdx.x / TL; cq < 6 * NQ; cq += NT / TL) {
             const int c6 = cq / NQ, qz = cq - c6 * NQ;
@@ -481,13 +486,23 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
                 const int p = j + r * NJ;  // spectral index of this output
                 const int qzc = 2 * p <= L ? p : L - p;  // nz = L / 2
                 const T sz = 2 * p <= L ? (T)1 : (T)-1;
-                const C* gq = gs + qzc * TL + il;
-                const C gxx = gq[0];
-                const C gxy = cscale(gq[NQ * TL], sx * sy);
-                const C gxz = cscale(gq[2 * NQ * TL], sx * sz);
-                const C gyy = gq[3 * NQ * TL];
-                const C gyz = cscale(gq[4 * NQ * TL], sy * sz);
-                const C gzz = gq[5 * NQ * TL];
+                C g6[6];
+                if constexpr (TT::GSLICE) {
+                    const C* gq = gs + qzc * TL + il;
+#pragma unroll
+                    for (int c6 = 0; c6 < 6; c6++) g6[c6] = gq[c6 * NQ * TL];
+                } else {
+                    const int gcs = (int)a.g.gc_comp, qzs = (ny + 1) * (nx + 1);
+                    const C* gq = gbase + qzc * qzs + (i <= nx ? i : X - i);
+#pragma unroll
+                    for (int c6 = 0; c6 < 6; c6++) g6[c6] = __ldg(gq + c6 * gcs);
+                }
+                const C gxx = g6[0];
+                const C gxy = cscale(g6[1], sx * sy);
+                const C gxz = cscale(g6[2], sx * sz);
+                const C gyy = g6[3];
+                const C gyz = cscale(g6[4], sy * sz);
+                const C gzz = g6[5];
                 const C vx = v[q][0][r], vy = v[q][1][r], vz = v[q][2][r];
                 v[q][0][r] = cadd(cadd(cmul(gxx, vx), cmul(gxy, vy)), cmul(gxz, vz));
                 v[q][1][r] = cadd(cadd(cmul(gxy, vx), cmul(gyy, vy)), cmul(gyz, vz));

@@ -166,14 +166,14 @@ class _Slot:
         # device-to-host copies run at PCIe speed instead of through pageable
         # memory
         self.pinned = None
+        self.cache = collections.OrderedDict()
+        self.cache_size = cache_size
 
     def staging(self, n: int):
         import torch
         if self.pinned is None or self.pinned.numel() < n:
             self.pinned = torch.empty(int(n * 1.25) + 1, dtype=torch.complex128, pin_memory=True)
         return self.pinned[:n]
-        self.cache = collections.OrderedDict()
-        self.cache_size = cache_size
 
     def green(self, ob, k0, box=None):
         key = (ob.nx, ob.ny, ob.nz, ob.aretecube, k0, box)
