@@ -191,9 +191,17 @@ class _Slot:
         return g, False
 
     def close(self):
+        import torch
+        # every torch block that was used on the context's stream is released
+        # before the stream goes away: a cached block or pinned buffer freed
+        # later would otherwise be tied to a destroyed stream
+        self.tstream.synchronize()
+        self.pinned = None
         for g in self.cache.values():
             g.close()
         self.cache.clear()
+        torch.cuda.synchronize(self.dev)
+        torch.cuda.empty_cache()
         self.ctx.close()
 
 
@@ -242,9 +250,10 @@ class _DeviceRequest:
         staging, on the slot's stream) as an array the caller owns."""
         import torch
         stage = self.slot.staging(self.loc.numel())
+        # a blocking copy: torch ties no event of the slot's stream to the
+        # pinned buffer (the stream is destroyed with the slot)
         with torch.cuda.stream(self.slot.tstream):
-            stage.copy_(self.loc.view(-1), non_blocking=True)
-        self.slot.tstream.synchronize()
+            stage.copy_(self.loc.view(-1), non_blocking=False)
         return stage.numpy().reshape(self.loc.shape).copy()
 
 
