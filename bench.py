@@ -709,9 +709,10 @@ def run_serving(args):
     for name, prec in (("mixed", IFDDA_MIXED), ("fp64", IFDDA_FP64)):
         srv = serve.Server(slots=args.slots, device=local, precision=prec, ragged=args.ragged)
         # warm-up: one request per lattice size compiles nothing but fills caches
-        srv.run(reqs[:args.slots], realtime=False)
+        srv.run(reqs[:args.slots], realtime=False, keep_fields=False)
         t0 = time.perf_counter()
-        res = srv.run(reqs, realtime=True)
+        # every local field is read back to the host, then dropped
+        res = srv.run(reqs, realtime=True, keep_fields=False)
         wall = time.perf_counter() - t0
         srv.close()
         out[name] = serve.latency_stats(res, wall)

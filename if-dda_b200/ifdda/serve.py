@@ -162,18 +162,8 @@ class _Slot:
         # stream, so a slot waits for its own work only (no device-wide sync
         # that would wait on, or interfere with, the other slots' solves)
         self.tstream = torch.cuda.ExternalStream(self.ctx.stream(), device=self.dev)
-        # pinned staging for the local fields read back (grown on demand):
-        # device-to-host copies run at PCIe speed instead of through pageable
-        # memory
-        self.pinned = None
         self.cache = collections.OrderedDict()
         self.cache_size = cache_size
-
-    def staging(self, n: int):
-        import torch
-        if self.pinned is None or self.pinned.numel() < n:
-            self.pinned = torch.empty(int(n * 1.25) + 1, dtype=torch.complex128, pin_memory=True)
-        return self.pinned[:n]
 
     def green(self, ob, k0, box=None):
         key = (ob.nx, ob.ny, ob.nz, ob.aretecube, k0, box)
@@ -196,7 +186,6 @@ class _Slot:
         # before the stream goes away: a cached block or pinned buffer freed
         # later would otherwise be tied to a destroyed stream
         self.tstream.synchronize()
-        self.pinned = None
         for g in self.cache.values():
             g.close()
         self.cache.clear()
@@ -246,15 +235,19 @@ class _DeviceRequest:
         return self.tab.data_ptr() if self.tab is not None else None
 
     def local_field(self) -> np.ndarray:
-        """The local field read back to the host (through the slot's pinned
-        staging, on the slot's stream) as an array the caller owns."""
+        """The local field read back to the host, on the slot's stream, into
+        page-locked memory that the returned array owns: the copy runs at
+        PCIe speed and needs no second copy on the host (a pageable
+        destination would cost a host-side pass and first-touch page faults
+        over the whole field).  Freed arrays return their block to torch's
+        page-locked cache, so a steady stream of requests reuses them."""
         import torch
-        stage = self.slot.staging(self.loc.numel())
+        out = torch.empty(self.loc.shape, dtype=torch.complex128, pin_memory=True)
         # a blocking copy: torch ties no event of the slot's stream to the
-        # pinned buffer (the stream is destroyed with the slot)
+        # page-locked block (the stream is destroyed with the slot)
         with torch.cuda.stream(self.slot.tstream):
-            stage.copy_(self.loc.view(-1), non_blocking=False)
-        return stage.numpy().reshape(self.loc.shape).copy()
+            out.copy_(self.loc, non_blocking=False)
+        return out.numpy()
 
 
 def solve_request(slot: _Slot, req: Request, precision: int, tol: float = 1e-4, methodeit: str = "GPBICG1"):
@@ -334,9 +327,12 @@ class Server:
         for s in self.slots:
             s.close()
 
-    def run(self, requests, realtime: bool = True):
+    def run(self, requests, realtime: bool = True, keep_fields: bool = True):
         """Serve `requests` (sorted by arrival); returns the Results in id
-        order.  With realtime, a request becomes visible at its arrival time."""
+        order.  With realtime, a request becomes visible at its arrival time.
+        Without keep_fields every local field is still read back to the host
+        but dropped once its request completes (a long stream's fields would
+        otherwise all stay in host memory)."""
         pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
         results = {}
         t0 = time.perf_counter()
@@ -414,7 +410,7 @@ class Server:
                 end = time.perf_counter() - t0
                 with lock:
                     for req, (r, hit) in zip(batch, outs):
-                        results[req.rid] = Result(req.rid, r["FFloc"], r["tol1"], r["nloop"], r["ncompte"],
+                        results[req.rid] = Result(req.rid, r["FFloc"] if keep_fields else None, r["tol1"], r["nloop"], r["ncompte"],
                                                   r["nstop"], r["infostr"], start, end,
                                                   req.arrival if realtime else 0.0, slot.idx, hit, r["phases"])
 
@@ -432,7 +428,8 @@ class Server:
                         self.cv.notify_all()
                 end = time.perf_counter() - t0
                 with lock:
-                    results[req.rid] = Result(req.rid, r["FFloc"], r["tol1"], r["nloop"], r["ncompte"], r["nstop"],
+                    results[req.rid] = Result(req.rid, r["FFloc"] if keep_fields else None, r["tol1"], r["nloop"],
+                                              r["ncompte"], r["nstop"],
                                               r["infostr"], start, end, req.arrival if realtime else 0.0, slot.idx,
                                               hit, r["phases"])
 
