@@ -618,7 +618,25 @@ def run_matvec(args):
             lib.ifdda_timing_read(C.byref(nl), C.byref(ms))
             avg = ms.value / max(nl.value, 1)
             passes[names[ps]] = {"ms": round(avg, 5), "alg_GB_s": round(balg[ps] / avg / 1e6, 1)}
+        # every zconv variant the tile chooser weighs, timed the same way
+        zv, yv, tms = g.tiles(prec)
+        zvar = {}
+        for v in range(3):
+            try:
+                g.set_tiles(prec, v, yv)
+            except ifdda.IfddaError:  # the grid's z length has fewer variants
+                break
+            lib.ifdda_timing_enable(3, prec)
+            for _ in range(args.steps):
+                g.matvec_device(R, N, x.data_ptr(), b.data_ptr(), precision=prec)
+            ctx.synchronize()
+            nl, ms = C.c_int(0), C.c_double(0)
+            lib.ifdda_timing_read(C.byref(nl), C.byref(ms))
+            zvar[v] = round(ms.value / max(nl.value, 1), 5)
+        g.set_tiles(prec, zv, yv)
         lib.ifdda_timing_enable(0, -1)
+        passes["tile_chooser"] = {"zconv_variant": zv, "ypass_variant": yv, "ms_z0_z1_y0_y1": tms,
+                                  "zconv_ms_by_variant": zvar}
         out["fp32" if s == 8 else "fp64"] = passes
         del x, b
     if rank == 0:

@@ -264,12 +264,13 @@ def solve_request(slot: _Slot, req: Request, precision: int, tol: float = 1e-4, 
                             d.ff.data_ptr(), d.loc.data_ptr(), methodeit, tol, precision=precision)
     t3 = time.perf_counter()
     FFloc = d.local_field()
+    t4 = time.perf_counter()
     # a cached spectrum keeps no workspace: the HBM budget covers in-flight solves only
     g.release_workspace()
-    t4 = time.perf_counter()
+    t5 = time.perf_counter()
     return dict(FFloc=FFloc, tol1=r["tol1"], nloop=r["nloop"], ncompte=r["ncompte"], nstop=r["nstop"],
                 infostr=r["infostr"], phases=dict(inputs=t1 - t0, green=t2 - t1, solve=t3 - t2,
-                                                  readback=t4 - t3)), hit
+                                                  readback=t4 - t3, release=t5 - t4)), hit
 
 
 def solve_ragged(slot: _Slot, reqs, box: int, precision: int, tol: float = 1e-4, methodeit: str = "GPBICG1"):
@@ -292,10 +293,11 @@ def solve_ragged(slot: _Slot, reqs, box: int, precision: int, tol: float = 1e-4,
     tol1, nloop, ncompte, nstop, info = slot.ctx.inverserig_ragged_device(items, methodeit, tol,
                                                                           precision=precision)
     t3 = time.perf_counter()
-    items[0][0].release_workspace()
     out, r0 = [], 0
     locs = [d.local_field() for d in dreqs]
-    ph = dict(inputs=t_in, green=t_gr, solve=t3 - t2, readback=time.perf_counter() - t3)
+    t4 = time.perf_counter()
+    items[0][0].release_workspace()
+    ph = dict(inputs=t_in, green=t_gr, solve=t3 - t2, readback=t4 - t3, release=time.perf_counter() - t4)
     for d, hit, loc in zip(dreqs, hits, locs):
         sl = slice(r0, r0 + d.nrhs)
         ok = bool(np.all(tol1[sl] < tol))
