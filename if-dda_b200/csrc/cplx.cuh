@@ -41,6 +41,30 @@ template <int SIGN, class C> __host__ __device__ __forceinline__ C cmul_i(C a) {
 }
 template <class C> __host__ __device__ __forceinline__ C czero() { return mk(decltype(C().x)(0), decltype(C().x)(0)); }
 
+// Global load that asks L2 to fetch the PF bytes (64, 128 or 256) around the
+// address from DRAM (PTX ld .L2::<PF>B): for narrow rows that neighbouring
+// blocks read at the same time, the DRAM accesses become wider bursts.
+template <int PF> __device__ __forceinline__ float2 ld_l2pf(const float2* p) {
+    float2 v;
+    if constexpr (PF == 256)
+        asm volatile("ld.global.L2::256B.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+    else if constexpr (PF == 128)
+        asm volatile("ld.global.L2::128B.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+    else
+        v = *p;
+    return v;
+}
+template <int PF> __device__ __forceinline__ double2 ld_l2pf(const double2* p) {
+    double2 v;
+    if constexpr (PF == 256)
+        asm volatile("ld.global.L2::256B.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    else if constexpr (PF == 128)
+        asm volatile("ld.global.L2::128B.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    else
+        v = *p;
+    return v;
+}
+
 __host__ __device__ __forceinline__ double2 to_d(float2 a) { return make_double2(a.x, a.y); }
 __host__ __device__ __forceinline__ double2 to_d(double2 a) { return a; }
 template <class C> __host__ __device__ __forceinline__ C from_d(double2 a);

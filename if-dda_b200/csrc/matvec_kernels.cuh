@@ -118,10 +118,11 @@ template <class T, int L, int V = 0> struct MvTiles {
         if (m * nt > 2048) m = 2048 / nt;
         return m < 1 ? 1 : (m > 32 ? 32 : m);
     }
-    // z tile: shared memory of TL columns (twiddles, data tile with one pad
-    // point every 16, the block's slice of the compressed spectrum)
-    static constexpr size_t zbytes(int tl) {
-        return (size_t)L * S + (size_t)(L + (L >> 4)) * 6 * tl * S + (size_t)6 * (L / 2 + 1) * tl * S;
+    // z tile: shared memory of TL columns of mr mirror rows (twiddles, data
+    // tile with one pad point every 16, the block's slice of the compressed
+    // spectrum)
+    static constexpr size_t zbytes(int tl, int mr = 2) {
+        return (size_t)L * S + (size_t)(L + (L >> 4)) * 3 * mr * tl * S + (size_t)6 * (L / 2 + 1) * tl * S;
     }
     // zconv's FFT plan in FP32: two passes (a 32- or 16-point first pass)
     // where that saves a pass over the usual plan (lengths 96, 160, 192, 256,
@@ -129,18 +130,24 @@ template <class T, int L, int V = 0> struct MvTiles {
     // 12-point middle for three components would not fit the registers)
     static constexpr int ZP = (S == 8 && plan_len(L, 1) > 0 && plan_len(L, 1) < plan_len(L, 0)) ? 1 : 0;
     // With the two-pass plan the tile is wider (up to ~120 KB, 32-byte rows
-    // at 384), one block per SM.  Its variant 1 keeps that tile but reads the
-    // spectrum from global memory (L2) instead of staging its slice in shared
-    // memory, and asks for two blocks per SM; otherwise variant 1 halves the
-    // columns.  The tile chooser times the two.
-    static constexpr bool GSLICE = !(ZP && V);
+    // at 384), one block per SM.  Its variant 1 takes one of the two mirror
+    // rows per block (MRZ = 1) and twice the columns (up to ~160 KB): 64-byte
+    // rows at 384, whose DRAM accesses are half as scattered, the spectrum
+    // slice then read by the two blocks of a row pair back to back (L2
+    // serves the second).  Otherwise variant 1 halves the columns.  The tile
+    // chooser times the two.
+    static constexpr int MRZ = (ZP && V) ? 1 : 2;
     static constexpr int ztile() {
-        const size_t budget = (size_t)(ZP ? 120 : 80) * 1024 * (S / 8);
+        const size_t budget = (size_t)(ZP ? (MRZ == 1 ? 160 : 120) : 80) * 1024 * (S / 8);
         int tl = 16;
-        while (tl > 1 && zbytes(tl) > budget) tl /= 2;
+        while (tl > 1 && zbytes(tl, MRZ) > budget) tl /= 2;
         return V && !ZP && tl > 1 ? tl / 2 : tl;
     }
-    static constexpr int TLZ = ztile(), NBZ = 6 * TLZ;
+    static constexpr int TLZ = ztile(), NBZ = 3 * MRZ * TLZ;
+    // L2 prefetch size of the column reads of zconv and the y passes (rows of
+    // TLZ or TLY columns, 32 to 128 bytes, that neighbouring blocks read at
+    // the same time): 256-byte DRAM bursts, 4-5% faster at 192^2 x 128 and 384^3
+    static constexpr int ZPF = 256;
     // y tile: odd point stride; z tile: point stride NBZ with one pad point every 16
     static constexpr int PSY = NBY + 1, PSZ = NBZ;
     using LayX = Layout<1, LP, false, 4>;
@@ -149,18 +156,22 @@ template <class T, int L, int V = 0> struct MvTiles {
     static constexpr int NTX = nthreads(NBX), NTY = nthreads(NBY), NTZ = nthreads(NBZ, ZP);
     static constexpr int MINBX = minblocks(NTX, S == 8 ? 80 : 96);
     static constexpr int MINBY = minblocks(NTY, S == 8 ? 80 : 112);
-    static constexpr int MINBZ = minblocks(NTZ, S == 8 ? (ZP ? (V ? 112 : 128) : 72) : 168);
+    static constexpr int MINBZ = minblocks(NTZ, S == 8 ? (ZP ? 128 : 72) : 168);
     static constexpr size_t smem_x = (size_t)L * S + (size_t)NBX * LP * S;
     static constexpr size_t smem_y = (size_t)L * S + (size_t)L * PSY * S;
     static constexpr size_t smem_z = (size_t)L * S + (size_t)LayZ::span(L) * PSZ * S +
-                                     (GSLICE ? (size_t)6 * (L / 2 + 1) * TLZ * S : 0);
-    static_assert(!GSLICE || zbytes(TLZ) == smem_z, "z tile size rule and layout disagree");
+                                     (size_t)6 * (L / 2 + 1) * TLZ * S;
+    static_assert(zbytes(TLZ, MRZ) == smem_z, "z tile size rule and layout disagree");
 };
 
-// asynchronous global -> shared copy of one complex element (8 or 16 bytes)
-template <class C> __device__ __forceinline__ void cp_async_elem(C* dst_smem, const C* src) {
+// asynchronous global -> shared copy of one complex element (8 or 16 bytes);
+// PF = 256 asks L2 to fetch the 256 bytes around it from DRAM
+template <int PF = 0, class C> __device__ __forceinline__ void cp_async_elem(C* dst_smem, const C* src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"((int)sizeof(C)));
+    if constexpr (PF == 256)
+        asm volatile("cp.async.ca.shared.global.L2::256B [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"((int)sizeof(C)));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"((int)sizeof(C)));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
@@ -263,13 +274,13 @@ __global__ void __launch_bounds__(TT::NTX, TT::MINBX) k_fwd_x(const MvArgs<T> a,
 
 // ---- pass 2 and 4 ---------------------------------------------------------
 // DIR=+1: B1 (ny rows) -> B2 (Y rows);  DIR=-1: B2 (Y rows) -> B1 (ny rows)
-template <class T, int DIR> struct YLoad {
+template <class T, int DIR, int PF = 0> struct YLoad {
     static constexpr bool GLOBAL = true, HALF = DIR > 0;  // forward: rows >= ny are padding
     const cplx<T>* src;
     int X, i0;
     template <class C> __device__ __forceinline__ C load(int b, int p) const {
         const int i = i0 + b;
-        return i < X ? src[p * X + i] : czero<C>();
+        return i < X ? ld_l2pf<PF>(src + p * X + i) : czero<C>();
     }
 };
 template <class T, int DIR> struct YStore {
@@ -299,14 +310,14 @@ __global__ void __launch_bounds__(TT::NTY, TT::MINBY) k_pass_y(const MvArgs<T> a
     const int rows_out = DIR > 0 ? L : ny;
     const C* srcb = DIR > 0 ? a.B1 + rhs * a.g.b1_rhs : a.B2 + rhs * a.g.b2_rhs;
     C* dstb = DIR > 0 ? a.B2 + rhs * a.g.b2_rhs : a.B1 + rhs * a.g.b1_rhs;
-    YLoad<T, DIR> src{srcb + ((long)c * nz + k) * rows_in * X, X, i0};
+    YLoad<T, DIR, TT::ZPF> src{srcb + ((long)c * nz + k) * rows_in * X, X, i0};
     YStore<T, DIR> dst{dstb + ((long)c * nz + k) * rows_out * X, X, i0};
     fft_tile<C, L, TL, NT, DIR, typename TT::LayY>(sm, tw, src, dst);
 }
 
 // ---- pass 3 -----------------------------------------------------------------
 // lines b = (h * 3 + c) * TL + il: h = 0 row qy, h = 1 the mirror row Y - qy
-template <class T, int TL> struct ZLoad {
+template <class T, int TL, int PF = 0> struct ZLoad {
     static constexpr bool GLOBAL = true, HALF = true;  // rows >= nz are padding
     const cplx<T>* base;  // B2 of this right-hand side, column i0 of row qy
     int rs;    // elements between z rows (Y * X)
@@ -317,7 +328,7 @@ template <class T, int TL> struct ZLoad {
         const int hc = b / TL, il = b - hc * TL;
         const int h = hc / 3, c = hc - 3 * h;
         if (il >= nv || h >= two) return czero<C>();
-        return base[c * comp + p * rs + h * drow + il];
+        return ld_l2pf<PF>(base + c * comp + p * rs + h * drow + il);
     }
 };
 template <class T, int TL> struct ZStore {
@@ -402,25 +413,33 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
     constexpr int NP = plan_len(L, ZP);
     constexpr int RK = plan_radix(L, NP - 1, ZP);  // last forward radix = first inverse radix
     constexpr int NJ = L / RK;                 // butterflies per line in that pass
-    constexpr int NG = 2 * TL * NJ;            // (row half, column, butterfly) groups
+    constexpr int MR = TT::MRZ;                // mirror rows per block
+    constexpr int NG = MR * TL * NJ;           // (row half, column, butterfly) groups
     constexpr int PERM = (NG + NT - 1) / NT;
     constexpr int S = (int)sizeof(C);
-    constexpr int ORDER = zmid_cost<LZ>(1, TL, NJ, RK, NG, S) < zmid_cost<LZ>(0, TL, NJ, RK, NG, S) ? 1 : 0;
+    constexpr int ORDER =
+        MR == 2 && zmid_cost<LZ>(1, TL, NJ, RK, NG, S) < zmid_cost<LZ>(0, TL, NJ, RK, NG, S) ? 1 : 0;
     constexpr int NQ = L / 2 + 1;
-    const int rhs = blockIdx.x;
+    // with one mirror row per block, blockIdx.x = 2 rhs + hm: hm = 1 takes
+    // row Y - qy (which exists for 0 < qy < ny only)
+    const int rhs = MR == 2 ? (int)blockIdx.x : (int)blockIdx.x >> 1;
+    const int hm = MR == 2 ? 0 : (int)blockIdx.x & 1;
     C* tw = smem_base<C>();
     C* sm = tw + L;
     C* gs = sm + LZ::span(L) * TT::PSZ;
     const int nx = a.g.nx, ny = a.g.ny, nz = a.g.nz, X = a.g.X, Y = a.g.Y;
     const int i0 = blockIdx.y * TL;
     const int qy = blockIdx.z;                    // 0 .. ny
-    const int two = (qy > 0 && qy < ny) ? 2 : 1;  // rows qy and Y - qy
+    const bool pair = qy > 0 && qy < ny;
+    if (hm && !pair) return;
+    const int two = MR == 2 && pair ? 2 : 1;      // rows qy and Y - qy in the block
+    const int row = hm ? Y - qy : qy;             // the block's first row
     load_twiddles<C, L, NT>(tw, a.twz);
     const C* gbase = (a.gc_r ? a.gc_r[rhs] : a.Gc) + qy * (nx + 1);
     // this block's slice of the compressed spectrum (qy fixed, every qz, the
     // TL columns qx(i)) is copied into shared memory while the forward
-    // transform runs (without GSLICE the middle reads it from global memory)
-    if constexpr (TT::GSLICE) {
+    // transform runs
+    {
         static_assert(NT % TL == 0, "a thread keeps one column of the slice");
         const int il = threadIdx.x % TL;
         const int i = min(i0 + il, X - 1);
@@ -429,7 +448,7 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
         const int gcs = (int)a.g.gc_comp, qzs = (ny + 1) * (nx + 1);
         for (int cq = threadIdx.x / TL; cq < 6 * NQ; cq += NT / TL) {
             const int c6 = cq / NQ, qz = cq - c6 * NQ;
-            cp_async_elem(gs + cq * TL + il, gsrc + c6 * gcs + qz * qzs);
+            cp_async_elem<TT::ZPF>(gs + cq * TL + il, gsrc + c6 * gcs + qz * qzs);
         }
     }
     cp_async_commit();
@@ -440,12 +459,13 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
         cp_async_wait_all();
         return;
     }
-    C* B2 = a.B2 + rhs * a.g.b2_rhs + (long)qy * X + i0;
+    C* B2 = a.B2 + rhs * a.g.b2_rhs + (long)row * X + i0;
     const int rs = Y * X, comp = nz * Y * X, drow = (Y - 2 * qy) * X, nv = min(TL, X - i0);
-    const ZLoad<T, TL> zload{B2, rs, comp, drow, nv, two};
+    const ZLoad<T, TL, TT::ZPF> zload{B2, rs, comp, drow, nv, two};
     const ZStore<T, TL> zstore{B2, rs, comp, drow, nv, two};
     if constexpr (NP > 1)
-        stockham_range<C, L, NB, NT, +1, LZ, false, NP - 1, 0, 1, ZLoad<T, TL>, SmemIO, ZP>(sm, tw, zload, SmemIO{});
+        stockham_range<C, L, NB, NT, +1, LZ, false, NP - 1, 0, 1, ZLoad<T, TL, TT::ZPF>, SmemIO, ZP>(sm, tw, zload,
+                                                                                                    SmemIO{});
     cp_async_wait_all();
     __syncthreads();
     // ---- fused middle: read, transform, multiply, transform (registers) ----
@@ -480,23 +500,16 @@ __global__ void __launch_bounds__(TT::NTZ, TT::MINBZ) k_zconv(const MvArgs<T> a)
         }
         if (h < two && i < X) {
             const T sx = i <= nx ? (T)1 : (T)-1;
-            const T sy = h ? (T)-1 : (T)1;
+            const T sy = (h | hm) ? (T)-1 : (T)1;
 #pragma unroll
             for (int r = 0; r < RK; r++) {
                 const int p = j + r * NJ;  // spectral index of this output
                 const int qzc = 2 * p <= L ? p : L - p;  // nz = L / 2
                 const T sz = 2 * p <= L ? (T)1 : (T)-1;
                 C g6[6];
-                if constexpr (TT::GSLICE) {
-                    const C* gq = gs + qzc * TL + il;
+                const C* gq = gs + qzc * TL + il;
 #pragma unroll
-                    for (int c6 = 0; c6 < 6; c6++) g6[c6] = gq[c6 * NQ * TL];
-                } else {
-                    const int gcs = (int)a.g.gc_comp, qzs = (ny + 1) * (nx + 1);
-                    const C* gq = gbase + qzc * qzs + (i <= nx ? i : X - i);
-#pragma unroll
-                    for (int c6 = 0; c6 < 6; c6++) g6[c6] = __ldg(gq + c6 * gcs);
-                }
+                for (int c6 = 0; c6 < 6; c6++) g6[c6] = gq[c6 * NQ * TL];
                 const C gxx = g6[0];
                 const C gxy = cscale(g6[1], sx * sy);
                 const C gxz = cscale(g6[2], sx * sz);

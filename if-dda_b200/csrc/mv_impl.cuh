@@ -43,7 +43,7 @@ template <class T, int L, int DIR> void launch_pass_y(const MvArgs<T>& a, int nr
 
 template <class T, int L, int V> void launch_zconv_v(const MvArgs<T>& a, int nrhs, cudaStream_t st) {
     using TT = MvTiles<T, L, V>;
-    dim3 grid(nrhs, (a.g.X + TT::TLZ - 1) / TT::TLZ, a.g.ny + 1);
+    dim3 grid((3 - TT::MRZ) * nrhs, (a.g.X + TT::TLZ - 1) / TT::TLZ, a.g.ny + 1);
     PassScope ps(PASS_ZCONV, TT::S, st);
     ensure_smem(k_zconv<T, L, TT>, TT::smem_z);
     launch_pdl(k_zconv<T, L, TT>, grid, TT::NTZ, TT::smem_z, st, a);
