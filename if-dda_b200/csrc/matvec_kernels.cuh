@@ -130,18 +130,19 @@ template <class T, int L, int V = 0> struct MvTiles {
     // 12-point middle for three components would not fit the registers)
     static constexpr int ZP = (S == 8 && plan_len(L, 1) > 0 && plan_len(L, 1) < plan_len(L, 0)) ? 1 : 0;
     // With the two-pass plan the tile is wider (up to ~120 KB, 32-byte rows
-    // at 384), one block per SM.  Its variant 1 takes one of the two mirror
-    // rows per block (MRZ = 1) and twice the columns (up to ~160 KB): 64-byte
-    // rows at 384, whose DRAM accesses are half as scattered, the spectrum
-    // slice then read by the two blocks of a row pair back to back (L2
-    // serves the second).  Otherwise variant 1 halves the columns.  The tile
-    // chooser times the two.
-    static constexpr int MRZ = (ZP && V) ? 1 : 2;
+    // at 384), one block per SM.  Variant 1 takes one of the two mirror rows
+    // per block (MRZ = 1) and as many columns as fit (up to ~160 KB with the
+    // two-pass plan, 64-byte rows at 384; up to 112 KB otherwise, so that two
+    // blocks share an SM in FP64 too): wider rows, whose DRAM accesses are
+    // less scattered, the spectrum slice then read by the two blocks of a row
+    // pair back to back (L2 serves the second).  The tile chooser times the
+    // two.
+    static constexpr int MRZ = V ? 1 : 2;
     static constexpr int ztile() {
-        const size_t budget = (size_t)(ZP ? (MRZ == 1 ? 160 : 120) : 80) * 1024 * (S / 8);
+        const size_t budget = MRZ == 1 ? (size_t)(ZP ? 160 : 112) * 1024 : (size_t)(ZP ? 120 : 80) * 1024 * (S / 8);
         int tl = 16;
         while (tl > 1 && zbytes(tl, MRZ) > budget) tl /= 2;
-        return V && !ZP && tl > 1 ? tl / 2 : tl;
+        return tl;
     }
     static constexpr int TLZ = ztile(), NBZ = 3 * MRZ * TLZ;
     // L2 prefetch size of the column reads of zconv and the y passes (rows of
