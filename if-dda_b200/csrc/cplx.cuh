@@ -41,9 +41,10 @@ template <int SIGN, class C> __host__ __device__ __forceinline__ C cmul_i(C a) {
 }
 template <class C> __host__ __device__ __forceinline__ C czero() { return mk(decltype(C().x)(0), decltype(C().x)(0)); }
 
-// Global load that asks L2 to fetch the PF bytes (64, 128 or 256) around the
-// address from DRAM (PTX ld .L2::<PF>B): for narrow rows that neighbouring
-// blocks read at the same time, the DRAM accesses become wider bursts.
+// Global load that asks L2 to fetch the PF bytes (128 or 256; 0: a plain
+// load) around the address from DRAM (PTX ld .L2::<PF>B): for narrow rows
+// that neighbouring blocks read at the same time, the DRAM accesses become
+// wider bursts.
 template <int PF> __device__ __forceinline__ float2 ld_l2pf(const float2* p) {
     float2 v;
     if constexpr (PF == 256)
