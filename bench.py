@@ -725,9 +725,12 @@ def run_serving(args):
     ws, rank, local = dist_setup()
     torch.cuda.set_device(local)
     reqs = serve.make_stream(args.requests, args.rate, seed=4)
+    # page-locked read-back buffers for the largest local field of the
+    # stream, one per slot, made before the timed stream
+    serve.prewarm_readback(max(48 * r.n ** 3 * len(r.incidences) for r in reqs), args.slots)
     out = {}
     for name, prec in (("mixed", IFDDA_MIXED), ("fp64", IFDDA_FP64)):
-        srv = serve.Server(slots=args.slots, device=local, precision=prec, ragged=args.ragged)
+        srv = serve.Server(slots=args.slots, device=local, precision=prec, ragged=args.ragged, policy=args.policy)
         # warm-up: one request per lattice size compiles nothing but fills caches
         srv.run(reqs[:args.slots], realtime=False, keep_fields=False)
         t0 = time.perf_counter()
@@ -740,7 +743,8 @@ def run_serving(args):
     desc = (f"C4 serving stream: {args.requests} requests, Poisson arrivals at {args.rate}/s (seed 4), sphere or "
             f"cube, edge in {{16..96}}, d=10 nm, eps' U[1.5,4] eps'' U[0,0.5], lambda U[400,800] nm, 1-32 "
             f"incidences on the NA 0.9 disk, GPBICG1 to 1e-4, {args.slots} concurrent slots, HBM-budget admission"
-            + (", ragged batches (every arrived request of the head's box in one solve)" if args.ragged else ""))
+            + (", ragged batches (every arrived request of the head's box in one solve)" if args.ragged else "")
+            + (", least-work-first admission (5 s wait cap)" if args.policy == "sjf" else ", FIFO admission"))
     m = out["mixed"]
     line = {"metric": METRIC, "value": m["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "steps": args.requests,
             "warmup": args.slots, "ms_per_step": m["wall_s"] * 1e3 / args.requests, "higher_is_better": True,
@@ -829,7 +833,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) measurement")
     ap.add_argument("--requests", type=int, default=2000, help="c4: stream length")
-    ap.add_argument("--rate", type=float, default=100.0, help="c4: Poisson arrival rate (requests/s)")
+    ap.add_argument("--rate", type=float, default=3.0, help="c4: Poisson arrival rate (requests/s)")
+    ap.add_argument("--policy", default="fifo", choices=("fifo", "sjf"),
+                    help="c4: admission order (oldest first, or least work first with a 5 s wait cap)")
     ap.add_argument("--slots", type=int, default=4, help="c4: concurrent solver slots")
     ap.add_argument("--ragged", action="store_true", help="c4: solve arrived requests of one box as ragged batches")
     ap.add_argument("--nrhs", type=int, default=1, help="matvec mode: right-hand sides per batched mat-vec")

@@ -30,6 +30,7 @@ import collections
 import math
 import threading
 import time
+import weakref
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -74,6 +75,24 @@ def _request_inputs_bytes(N: int, nrhs: int) -> int:
     dipole-moment and local fields, the (nmax,3,3) polarisability, positions,
     Tabdip and the isotropic alpha."""
     return 3 * (3 * N * 16) * nrhs + 9 * N * 16 + 3 * N * 8 + N * 4 + N * 16
+
+
+def pick_next(pending, now: float, policy: str, max_wait: float):
+    """The request a server serves next from `pending` (sorted by arrival,
+    its head arrived by `now`): fifo takes the head; sjf takes the arrived
+    request with the least work (lattice sites x incidences; the earliest of
+    equals), or the head once it has waited max_wait seconds."""
+    head = pending[0]
+    if policy == "fifo" or now - head.arrival >= max_wait:
+        return head
+    best, cost = head, head.n ** 3 * len(head.incidences)
+    for q in pending:
+        if q.arrival > now:
+            break
+        c = q.n ** 3 * len(q.incidences)
+        if c < cost:
+            best, cost = q, c
+    return best
 
 
 def footprint_bytes(n: int, nrhs: int, precision: int) -> int:
@@ -150,6 +169,73 @@ def build_object(req: Request):
     else:
         ob = objects.cube(req.n * req.d, req.eps, req.n, k0, "RR")
     return ob, k0
+
+
+class _PinnedPool:
+    """Page-locked host buffers for the local fields read back, shared by
+    every slot and server of the process.  A read-back takes the smallest
+    free buffer that holds it (allocating one, rounded up to 64 MiB, only
+    when none does) and the returned array gives it back when it is freed.
+    Allocating page-locked memory is slow and holds the CUDA driver while it
+    runs, stalling the other slots' calls; a steady request stream reuses the
+    buffers instead, and prewarm() makes them before a timed stream starts."""
+
+    GRAIN = 64 << 20
+
+    def __init__(self, pin: bool = True):
+        self.lock = threading.Lock()
+        self.free = []
+        self.pin = pin
+
+    def acquire(self, nbytes: int):
+        import torch
+        with self.lock:
+            fit = [i for i, b in enumerate(self.free) if b.numel() >= nbytes]
+            if fit:
+                return self.free.pop(min(fit, key=lambda i: self.free[i].numel()))
+        size = -(-nbytes // self.GRAIN) * self.GRAIN
+        return torch.empty(size, dtype=torch.uint8, pin_memory=self.pin)
+
+    def release(self, buf):
+        with self.lock:
+            self.free.append(buf)
+
+    def array_view(self, shape):
+        """(tensor, array): a complex128 tensor of `shape` on a pool buffer
+        and the numpy array on the same memory.  The buffer returns to the
+        pool when the array (with every view of it) is freed, so the tensor
+        must not outlive the array."""
+        import torch
+        nbytes = int(np.prod(shape)) * 16
+        buf = self.acquire(nbytes)
+        out = buf[:nbytes].view(torch.complex128).view(tuple(shape))
+        arr = out.numpy()
+        weakref.finalize(arr, self.release, buf)
+        return out, arr
+
+    def prewarm(self, nbytes: int, count: int):
+        bufs = [self.acquire(nbytes) for _ in range(count)]
+        for b in bufs:
+            self.release(b)
+
+    def clear(self):
+        with self.lock:
+            self.free = []
+
+
+_PINNED = _PinnedPool()
+
+
+def prewarm_readback(nbytes: int, count: int):
+    """Make `count` page-locked read-back buffers of at least nbytes each
+    (a request's local field takes 3 x dipoles x incidences x 16 bytes)."""
+    _PINNED.prewarm(int(nbytes), int(count))
+
+
+def release_readback_buffers():
+    """Drop the free page-locked read-back buffers (those still held by
+    result arrays return to the pool when the arrays are freed)."""
+    _PINNED.clear()
 
 
 class _Slot:
@@ -236,18 +322,18 @@ class _DeviceRequest:
 
     def local_field(self) -> np.ndarray:
         """The local field read back to the host, on the slot's stream, into
-        page-locked memory that the returned array owns: the copy runs at
-        PCIe speed and needs no second copy on the host (a pageable
-        destination would cost a host-side pass and first-touch page faults
-        over the whole field).  Freed arrays return their block to torch's
-        page-locked cache, so a steady stream of requests reuses them."""
+        a page-locked buffer of the read-back pool that the returned array
+        holds: the copy runs at PCIe speed and needs no second copy on the
+        host (a pageable destination would cost a host-side pass and
+        first-touch page faults over the whole field).  When the array is
+        freed the buffer returns to the pool."""
         import torch
-        out = torch.empty(self.loc.shape, dtype=torch.complex128, pin_memory=True)
-        # a blocking copy: torch ties no event of the slot's stream to the
-        # page-locked block (the stream is destroyed with the slot)
+        out, arr = _PINNED.array_view(self.loc.shape)
+        # a blocking copy: no event of the slot's stream is tied to the
+        # buffer (the stream is destroyed with the slot)
         with torch.cuda.stream(self.slot.tstream):
             out.copy_(self.loc, non_blocking=False)
-        return out.numpy()
+        return arr
 
 
 def solve_request(slot: _Slot, req: Request, precision: int, tol: float = 1e-4, methodeit: str = "GPBICG1"):
@@ -313,9 +399,19 @@ class Server:
 
     def __init__(self, slots: int = 4, device: int = 0, hbm_budget: float = 120e9, precision: int = IFDDA_MIXED,
                  cache_size: int = 4, ragged: bool = False, max_batch_rhs: int = 64, max_objects: int = 64,
-                 pad_ratio: float = 1.0):
+                 pad_ratio: float = 1.0, policy: str = "fifo", max_wait: float = 5.0):
+        if policy not in ("fifo", "sjf"):
+            raise ValueError("policy must be 'fifo' or 'sjf'")
+        if policy == "sjf" and ragged:
+            raise ValueError("the sjf policy applies to per-request serving")
         self.slots = [_Slot(i, device, cache_size if not ragged else max(cache_size, max_objects))
                       for i in range(slots)]
+        # fifo: the oldest request first.  sjf: among the arrived requests the
+        # one with the least work (lattice sites x incidences) first, unless
+        # the oldest has waited max_wait seconds, which then goes first (so a
+        # large request is delayed by at most about max_wait)
+        self.policy = policy
+        self.max_wait = max_wait
         self.budget = hbm_budget
         self.precision = precision
         self.in_use = 0.0
@@ -341,19 +437,21 @@ class Server:
         lock = threading.Lock()
 
         def next_request():
-            # FIFO admission: the head of the queue waits until it has arrived
-            # and its footprint fits next to the work in flight
+            # admission: the policy's pick waits until it has arrived and its
+            # footprint fits next to the work in flight
             with self.cv:
                 while True:
                     if not pending:
                         return None, 0.0
-                    head = pending[0]
                     now = time.perf_counter() - t0
-                    fp = footprint_bytes(head.n, len(head.incidences), self.precision)
+                    head = pending[0]
                     arrived = (not realtime) or head.arrival <= now
+                    if arrived:
+                        head = pick_next(pending, now if realtime else math.inf, self.policy, self.max_wait)
+                    fp = footprint_bytes(head.n, len(head.incidences), self.precision)
                     fits = self.in_use + fp <= self.budget or self.in_use == 0
                     if arrived and fits:
-                        pending.popleft()
+                        pending.remove(head)
                         self.in_use += fp
                         return head, fp
                     wait = max(0.0005, head.arrival - now) if not arrived else 0.05
@@ -436,11 +534,26 @@ class Server:
                                               hit, r["phases"])
 
         target = worker_ragged if self.ragged else worker
-        threads = [threading.Thread(target=target, args=(s,), daemon=True) for s in self.slots]
+        errors = []
+
+        def guarded(slot: _Slot):
+            # a failing worker stops the stream: the other workers finish
+            # their request in flight, take no new one, and run() raises
+            try:
+                target(slot)
+            except BaseException as e:  # noqa: B902 - re-raised by run()
+                with self.cv:
+                    errors.append(e)
+                    pending.clear()
+                    self.cv.notify_all()
+
+        threads = [threading.Thread(target=guarded, args=(s,), daemon=True) for s in self.slots]
         for th in threads:
             th.start()
         for th in threads:
             th.join()
+        if errors:
+            raise errors[0]
         return [results[k] for k in sorted(results)]
 
 

@@ -28,6 +28,13 @@ def test_results_identical_alone_and_in_the_mix():
         assert np.array_equal(a.FFloc, b.FFloc)
         assert np.array_equal(a.nloop, b.nloop)
         assert np.all(b.tol1 < 1e-4)
+    # least-work-first admission serves the same results in another order
+    sjf = serve.Server(slots=2, precision=IFDDA_MIXED, policy="sjf")
+    rs = sjf.run(reqs, realtime=True)
+    sjf.close()
+    for a, b in zip(ra, rs):
+        assert a.rid == b.rid and b.nstop == 0
+        assert np.array_equal(a.FFloc, b.FFloc)
 
 
 @pytest.mark.parametrize("prec", [0, 1])
