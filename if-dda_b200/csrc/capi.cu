@@ -466,6 +466,7 @@ void ctx_free(ifdda_ctx* ctx) {
             cudaStreamSynchronize(ctx->stream);
             cudaStreamDestroy(ctx->stream);
         }
+        destroy_retired_graph_execs();
         if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     }
     delete ctx;

@@ -2,6 +2,9 @@
 // (FP32 inner / FP64 outer) iterative refinement.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <utility>
+#include <vector>
 #include "gpbicg_fused.cuh"
 #include "solver.cuh"
 
@@ -153,6 +156,43 @@ template void cast_dev<float>(const double2*, float2*, long, cudaStream_t);
 template void cast_dev<double>(const double2*, double2*, long, cudaStream_t);
 
 // ------------------------------------------------------------- solver ----
+namespace {
+std::mutex g_retired_mu;
+std::vector<std::pair<int, cudaGraphExec_t>> g_retired;  // (device, executable)
+
+void destroy_execs(const std::vector<std::pair<int, cudaGraphExec_t>>& v) {
+    if (v.empty()) return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    for (const auto& [dev, e] : v) {
+        cudaSetDevice(dev);
+        cudaGraphExecDestroy(e);
+    }
+    if (prev >= 0) cudaSetDevice(prev);
+}
+}  // namespace
+
+void retire_graph_exec(cudaGraphExec_t exec) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::vector<std::pair<int, cudaGraphExec_t>> now;
+    {
+        std::lock_guard<std::mutex> lk(g_retired_mu);
+        g_retired.emplace_back(dev, exec);
+        if (g_retired.size() >= 256) now.swap(g_retired);
+    }
+    destroy_execs(now);
+}
+
+void destroy_retired_graph_execs() {
+    std::vector<std::pair<int, cudaGraphExec_t>> now;
+    {
+        std::lock_guard<std::mutex> lk(g_retired_mu);
+        now.swap(g_retired);
+    }
+    destroy_execs(now);
+}
+
 int reduction_blocks(long n3) { return (int)std::max<long>(1, std::min<long>((n3 + KNT * 2 - 1) / (KNT * 2), 2048)); }
 
 template <class T> void KrylovWork<T>::ensure(int method, int nrhs_, long n3_) {
