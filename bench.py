@@ -436,7 +436,7 @@ def run_gpu(args):
         locs = blk.pop("_locs")
         blk["local_field_rel_l2"] = max(float(np.linalg.norm(locs[r] - locc[r]) / np.linalg.norm(locc[r]))
                                         for r in range(min(nser, kacc)))
-    # the north star's comparison: the mixed batched solver against the FP64
+    # the precision comparison: the mixed batched solver against the FP64
     # drop-in one right-hand side per call, at matching accuracy (the loosest
     # tolerance whose local field is as close to the converged field as the
     # mixed solve's, or within 1e-4 of it)

@@ -1,7 +1,7 @@
 /*
  * ifdda_oracle.c -- CPU restatement (FP64, OpenMP) of IF-DDA's FFT-accelerated
- * discrete-dipole solve.  TEST INFRASTRUCTURE ONLY: this library is the checker
- * for the CUDA path and the timed CPU baseline.  Nothing in the product links it.
+ * discrete-dipole solve.  TEST INFRASTRUCTURE ONLY: the parity tests hold the
+ * CUDA path to it, and it is the timed CPU baseline.  Nothing in the product links it.
  *
  * Parity status: the reference (Fortran 77/90) cannot be compiled where this was
  * written (no Fortran compiler, no FFTW3), and its own tests store no outputs.
