@@ -425,6 +425,8 @@ int ifdda_ctx_create(int device, ifdda_ctx** out) {
         c->device = device;
         DeviceScope ds(device);
         IFDDA_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        IFDDA_CUDA(cudaStreamCreateWithFlags(&c->upload_stream, cudaStreamNonBlocking));
+        IFDDA_CUDA(cudaEventCreateWithFlags(&c->upload_done, cudaEventDisableTiming));
         AllocStreamScope as(c->stream);
         // keep freed blocks in the device's memory pool: re-allocating a
         // workspace then costs neither a cudaMalloc nor a device synchronisation
@@ -466,6 +468,11 @@ void ctx_free(ifdda_ctx* ctx) {
             cudaStreamSynchronize(ctx->stream);
             cudaStreamDestroy(ctx->stream);
         }
+        if (ctx->upload_stream) {
+            cudaStreamSynchronize(ctx->upload_stream);
+            cudaStreamDestroy(ctx->upload_stream);
+        }
+        if (ctx->upload_done) cudaEventDestroy(ctx->upload_done);
         destroy_retired_graph_execs();
         if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     }
@@ -589,6 +596,7 @@ int ifdda_green_destroy(ifdda_green* g) {
     if (cudaSetDevice(ctx->device) == cudaSuccess) {
         AllocStreamScope as(ctx->stream);
         cudaStreamSynchronize(ctx->stream);
+        if (ctx->upload_stream) cudaStreamSynchronize(ctx->upload_stream);
         delete g;
         if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     } else {
@@ -604,6 +612,7 @@ int ifdda_green_release_workspace(ifdda_green* g) {
     DeviceScope ds(g->ctx->device);
     AllocStreamScope as(g->ctx->stream);
     IFDDA_CUDA(cudaStreamSynchronize(g->ctx->stream));
+    IFDDA_CUDA(cudaStreamSynchronize(g->ctx->upload_stream));
     g->SW.kw64.release();
     g->SW.kw32.release();
     g->SW.mixed.release();
@@ -613,6 +622,8 @@ int ifdda_green_release_workspace(ifdda_green* g) {
     g->G.w64.B2.release();
     g->alpha.release();
     g->ff0.release();
+    g->up_alpha.release();
+    g->up_ff0.release();
     g->x.release();
     g->ffx.release();
     g->ffb.release();
@@ -741,12 +752,30 @@ int ifdda_inverserig_batch(ifdda_green* g, int nrhs, int nbsphere, int nmax, con
     const long n3 = 3L * nbsphere, tot = n3 * nrhs;
     const int* tab = nullptr;
     if (tabdip) check_tabdip(tabdip, uN, nbsphere);
+    // The inputs are uploaded on the context's upload stream when their
+    // buffers need no allocation, so that the copies overlap the work already
+    // queued on the solve stream (in the reference's call sequence the
+    // spectrum, cdmlib/cdmlib.f:1529, comes right before the solve, :1565);
+    // the solve stream waits for them (upload_done) before the solve.  A
+    // buffer that must grow is allocated and filled on the solve stream,
+    // after the upload stream has drained (a pending upload may still target
+    // the old buffer after an error).
+    ifdda_ctx* ctx = g->ctx;
+    auto upload = [&](DevBuf<double2>& buf, const void* src, size_t n, bool side) {
+        cudaStream_t s = st;
+        if (side && n <= buf.n) {
+            s = ctx->upload_stream;
+        } else if (n > buf.n) {
+            IFDDA_CUDA(cudaStreamSynchronize(ctx->upload_stream));
+            buf.ensure(n);
+        }
+        IFDDA_CUDA(cudaMemcpyAsync(buf.p, src, n * sizeof(double2), cudaMemcpyHostToDevice, s));
+    };
     // the incident field goes first, so that its copy overlaps the host scan
     // of the polarisability below (when FF0 is pinned)
-    g->ff0.ensure(tot);
+    upload(g->up_ff0, FF0, (size_t)tot, true);
     g->x.ensure(tot);
     g->ffb.ensure(tot);
-    IFDDA_CUDA(cudaMemcpyAsync(g->ff0.p, FF0, tot * sizeof(double2), cudaMemcpyHostToDevice, st));
     if (tabdip) {
         g->tab.ensure(uN);
         IFDDA_CUDA(cudaMemcpyAsync(g->tab.p, tabdip, uN * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -770,28 +799,21 @@ int ifdda_inverserig_batch(ifdda_green* g, int nrhs, int nbsphere, int nmax, con
     } joiner{scan};
     if (amode == ALPHA_ISO && nbsphere > head)
         scan = std::thread([&] { tail.store(pola_mode_range(polarisa, head, nbsphere, nmax)); });
-    auto upload_alpha = [&](int mode) {
-        if (mode == ALPHA_ISO) {
-            // the isotropic value of dipole i is polarisa(i,1,1): the first nb
-            // entries of the (nmax,3,3) array, contiguous
-            g->alpha.ensure(nbsphere);
-            IFDDA_CUDA(
-                cudaMemcpyAsync(g->alpha.p, polarisa, nbsphere * sizeof(double2), cudaMemcpyHostToDevice, st));
-        } else {
-            g->alpha.ensure((size_t)9 * nmax);
-            IFDDA_CUDA(cudaMemcpyAsync(g->alpha.p, polarisa, (size_t)9 * nmax * sizeof(double2),
-                                       cudaMemcpyHostToDevice, st));
-        }
-    };
-    upload_alpha(amode);
+    // the isotropic value of dipole i is polarisa(i,1,1): the first nb
+    // entries of the (nmax,3,3) array, contiguous
+    upload(g->up_alpha, polarisa, amode == ALPHA_ISO ? (size_t)nbsphere : (size_t)9 * nmax, true);
+    IFDDA_CUDA(cudaEventRecord(ctx->upload_done, ctx->upload_stream));
+    IFDDA_CUDA(cudaStreamWaitEvent(st, ctx->upload_done, 0));
     // the outputs are copied and waited for below, on the same stream
-    int rc = solve_device(g, nrhs, nbsphere, nmax, tab, g->alpha.p, amode, g->ff0.p, methodeit, tol, g->ffb.p, g->x.p,
-                          tol1, nloop, ncompte, nstop, infostr, opt, true, false);
+    int rc = solve_device(g, nrhs, nbsphere, nmax, tab, g->up_alpha.p, amode, g->up_ff0.p, methodeit, tol, g->ffb.p,
+                          g->x.p, tol1, nloop, ncompte, nstop, infostr, opt, true, false);
     if (scan.joinable()) scan.join();
     if (amode == ALPHA_ISO && tail.load() == ALPHA_FULL && rc != -1) {
-        upload_alpha(ALPHA_FULL);
-        rc = solve_device(g, nrhs, nbsphere, nmax, tab, g->alpha.p, ALPHA_FULL, g->ff0.p, methodeit, tol, g->ffb.p,
-                          g->x.p, tol1, nloop, ncompte, nstop, infostr, opt, true, false);
+        // the first solve's kernels read up_alpha: the full tensor follows
+        // them on the solve stream
+        upload(g->up_alpha, polarisa, (size_t)9 * nmax, false);
+        rc = solve_device(g, nrhs, nbsphere, nmax, tab, g->up_alpha.p, ALPHA_FULL, g->up_ff0.p, methodeit, tol,
+                          g->ffb.p, g->x.p, tol1, nloop, ncompte, nstop, infostr, opt, true, false);
     }
     IFDDA_CUDA(cudaMemcpyAsync(FFloc, g->x.p, tot * sizeof(double2), cudaMemcpyDeviceToHost, st));
     IFDDA_CUDA(cudaMemcpyAsync(FF, g->ffb.p, tot * sizeof(double2), cudaMemcpyDeviceToHost, st));

@@ -8,6 +8,11 @@
 struct ifdda_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    // host-to-device uploads of ifdda_inverserig(_batch) that need no
+    // allocation run here, so that they overlap the work already queued on
+    // `stream`; `upload_done` orders the solve after them
+    cudaStream_t upload_stream = nullptr;
+    cudaEvent_t upload_done = nullptr;
     std::string last_error;
     ifdda::DevBuf<int> flag;  // device error flag for post kernels
     ifdda::DevBuf<double2> partials;
@@ -29,6 +34,10 @@ struct ifdda_green {
     // Tabdip of the padded box (G.padded()): allocated with the handle
     ifdda::DevBuf<int> ptab;
     ifdda::DevBuf<double2> alpha, ff0, x, ffx, ffb;
+    // incident fields and polarisabilities uploaded by ifdda_inverserig(_batch)
+    // alone (no other entry point queues work on them, so an upload on the
+    // context's upload stream cannot overwrite a buffer a queued kernel reads)
+    ifdda::DevBuf<double2> up_ff0, up_alpha;
     ifdda::DevBuf<float2> ffx32, ffb32, alpha32;
     // a ragged batch solved with this handle's workspaces (the first object
     // of ifdda_inverserig_ragged): concatenated Tabdips and polarisabilities,
