@@ -150,11 +150,16 @@ int report_results(const std::vector<SolveResult>& res, int method, double tol, 
 // check_tol: report tol1 >= tol as "Converge do not reach!" (cdmlib.f:1586-1591;
 // the microscopes call the solver without that check).  sync_out: return with
 // FF computed; a caller that next copies the outputs on the same stream and
-// waits there passes false.
+// waits there passes false.  early_loc: a page-locked host array for the
+// local field that a mixed solve fills on the context's upload stream after
+// each refinement step (SolveSpec::early_loc); *loc_on_host tells whether it
+// holds the result (the solve stream is ordered after that copy).
 int solve_device(ifdda_green* g, int nrhs, int nb, int nmax, const int* tab_dev, const double2* alpha_dev, int amode,
                  const double2* ff0_dev, const char* methodeit, double tol, double2* ff_dev, double2* loc_dev,
                  double* tol1, int* nloop, int* ncompte, int* nstop, char* infostr, const ifdda_solve_options* opt,
-                 bool check_tol = true, bool sync_out = true) {
+                 bool check_tol = true, bool sync_out = true, double2* early_loc = nullptr,
+                 bool* loc_on_host = nullptr) {
+    if (loc_on_host) *loc_on_host = false;
     ifdda_ctx* ctx = g->ctx;
     const int method = method_code(methodeit);
     if (method == 0) {
@@ -185,8 +190,15 @@ int solve_device(ifdda_green* g, int nrhs, int nb, int nmax, const int* tab_dev,
     }
     const int prec = opt ? opt->precision : IFDDA_FP64;
     std::vector<SolveResult> res;
+    if (prec == IFDDA_MIXED && early_loc) {
+        sp.early_loc = early_loc;
+        sp.early_stream = ctx->upload_stream;
+        sp.loc_ready = ctx->loc_ready;
+        sp.loc_copied = ctx->loc_copied;
+    }
     if (prec == IFDDA_MIXED) solve_mixed(g->G, g->SW, sp, ff0_dev, loc_dev, res, ctx->stream);
     else solve_fp64(g->G, g->SW, sp, ff0_dev, loc_dev, res, ctx->stream);
+    if (loc_on_host) *loc_on_host = !res.empty() && res[0].loc_on_host;
     // FF = polarisa . E (cdmlib/inverserigopt.f:92-97)
     apply_alpha_dev(loc_dev, ff_dev, nb, nrhs, 3L * nb, amode, alpha_dev, sp.nmax, ctx->stream);
     if (sync_out) IFDDA_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -427,6 +439,8 @@ int ifdda_ctx_create(int device, ifdda_ctx** out) {
         IFDDA_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
         IFDDA_CUDA(cudaStreamCreateWithFlags(&c->upload_stream, cudaStreamNonBlocking));
         IFDDA_CUDA(cudaEventCreateWithFlags(&c->upload_done, cudaEventDisableTiming));
+        IFDDA_CUDA(cudaEventCreateWithFlags(&c->loc_ready, cudaEventDisableTiming));
+        IFDDA_CUDA(cudaEventCreateWithFlags(&c->loc_copied, cudaEventDisableTiming));
         AllocStreamScope as(c->stream);
         // keep freed blocks in the device's memory pool: re-allocating a
         // workspace then costs neither a cudaMalloc nor a device synchronisation
@@ -473,6 +487,8 @@ void ctx_free(ifdda_ctx* ctx) {
             cudaStreamDestroy(ctx->upload_stream);
         }
         if (ctx->upload_done) cudaEventDestroy(ctx->upload_done);
+        if (ctx->loc_ready) cudaEventDestroy(ctx->loc_ready);
+        if (ctx->loc_copied) cudaEventDestroy(ctx->loc_copied);
         destroy_retired_graph_execs();
         if (prev >= 0 && prev != ctx->device) cudaSetDevice(prev);
     }
@@ -761,6 +777,12 @@ int ifdda_inverserig_batch(ifdda_green* g, int nrhs, int nbsphere, int nmax, con
     // after the upload stream has drained (a pending upload may still target
     // the old buffer after an error).
     ifdda_ctx* ctx = g->ctx;
+    // on every way out (errors included) the upload stream has finished with
+    // the caller's arrays before the call returns
+    struct UploadDrain {
+        cudaStream_t s;
+        ~UploadDrain() { cudaStreamSynchronize(s); }
+    } drain{ctx->upload_stream};
     auto upload = [&](DevBuf<double2>& buf, const void* src, size_t n, bool side) {
         cudaStream_t s = st;
         if (side && n <= buf.n) {
@@ -804,9 +826,18 @@ int ifdda_inverserig_batch(ifdda_green* g, int nrhs, int nbsphere, int nmax, con
     upload(g->up_alpha, polarisa, amode == ALPHA_ISO ? (size_t)nbsphere : (size_t)9 * nmax, true);
     IFDDA_CUDA(cudaEventRecord(ctx->upload_done, ctx->upload_stream));
     IFDDA_CUDA(cudaStreamWaitEvent(st, ctx->upload_done, 0));
+    // A page-locked FFloc receives the local field from the mixed solve after
+    // each refinement step, while the solve checks the new residual; the copy
+    // after the last step is the result.  (A pageable copy would block this
+    // thread, so a pageable FFloc gets the one copy at the end.)
+    cudaPointerAttributes pa{};
+    const bool loc_pinned = cudaPointerGetAttributes(&pa, FFloc) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();  // a host pointer the runtime does not know leaves no error behind
+    bool loc_done = false;
     // the outputs are copied and waited for below, on the same stream
     int rc = solve_device(g, nrhs, nbsphere, nmax, tab, g->up_alpha.p, amode, g->up_ff0.p, methodeit, tol, g->ffb.p,
-                          g->x.p, tol1, nloop, ncompte, nstop, infostr, opt, true, false);
+                          g->x.p, tol1, nloop, ncompte, nstop, infostr, opt, true, false,
+                          loc_pinned ? (double2*)FFloc : nullptr, &loc_done);
     if (scan.joinable()) scan.join();
     if (amode == ALPHA_ISO && tail.load() == ALPHA_FULL && rc != -1) {
         // the first solve's kernels read up_alpha: the full tensor follows
@@ -814,8 +845,10 @@ int ifdda_inverserig_batch(ifdda_green* g, int nrhs, int nbsphere, int nmax, con
         upload(g->up_alpha, polarisa, (size_t)9 * nmax, false);
         rc = solve_device(g, nrhs, nbsphere, nmax, tab, g->up_alpha.p, ALPHA_FULL, g->up_ff0.p, methodeit, tol,
                           g->ffb.p, g->x.p, tol1, nloop, ncompte, nstop, infostr, opt, true, false);
+        loc_done = false;
     }
-    IFDDA_CUDA(cudaMemcpyAsync(FFloc, g->x.p, tot * sizeof(double2), cudaMemcpyDeviceToHost, st));
+    if (!loc_done)
+        IFDDA_CUDA(cudaMemcpyAsync(FFloc, g->x.p, tot * sizeof(double2), cudaMemcpyDeviceToHost, st));
     IFDDA_CUDA(cudaMemcpyAsync(FF, g->ffb.p, tot * sizeof(double2), cudaMemcpyDeviceToHost, st));
     IFDDA_CUDA(cudaStreamSynchronize(st));
     return rc;

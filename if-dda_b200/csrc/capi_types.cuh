@@ -13,6 +13,9 @@ struct ifdda_ctx {
     // `stream`; `upload_done` orders the solve after them
     cudaStream_t upload_stream = nullptr;
     cudaEvent_t upload_done = nullptr;
+    // a mixed solve's copies of the local field to the caller's page-locked
+    // FFloc run on upload_stream too (SolveSpec::early_loc)
+    cudaEvent_t loc_ready = nullptr, loc_copied = nullptr;
     std::string last_error;
     ifdda::DevBuf<int> flag;  // device error flag for post kernels
     ifdda::DevBuf<double2> partials;

@@ -790,6 +790,7 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
     std::vector<long> inner_iters(nrhs, 0), inner_mv(nrhs, 0), outer_mv(nrhs, 0), inner_runs(nrhs, 0);
     bool ok = true;
     int outer = 0;
+    bool early = false;  // a copy of x to sp.early_loc has been issued
     // The inner solve's counters are read with the next outer status (one
     // wait instead of two): the residual step that runs between them changes
     // only the inner tol and maxit.  mask: the outer status before that solve.
@@ -846,10 +847,22 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
         }
         mask = ost;
         pending = true;
+        // the previous step's copy to the host reads x: it must end first
+        if (early) IFDDA_CUDA(cudaStreamWaitEvent(st, sp.loc_copied, 0));
         count_launch();
         k_axpy_outer<float><<<grid_for(tot), 256, 0, st>>>(M.x.p, V.v(xs, 0), n3, nrhs, M.ostatus.p);
         IFDDA_CUDA(cudaGetLastError());
+        if (sp.early_loc) {
+            IFDDA_CUDA(cudaEventRecord(sp.loc_ready, st));
+            IFDDA_CUDA(cudaStreamWaitEvent(sp.early_stream, sp.loc_ready, 0));
+            IFDDA_CUDA(cudaMemcpyAsync(sp.early_loc, M.x.p, tot * sizeof(double2), cudaMemcpyDeviceToHost,
+                                       sp.early_stream));
+            IFDDA_CUDA(cudaEventRecord(sp.loc_copied, sp.early_stream));
+            early = true;
+        }
     }
+    // whatever follows on the solve stream comes after the last host copy
+    if (early) IFDDA_CUDA(cudaStreamWaitEvent(st, sp.loc_copied, 0));
     if (pending) {
         IFDDA_CUDA(cudaMemcpyAsync(hs.data(), W.st.p, nrhs * sizeof(KState), cudaMemcpyDeviceToHost, st));
         IFDDA_CUDA(cudaStreamSynchronize(st));
@@ -869,6 +882,8 @@ void solve_mixed(Green& G, SolverWork& SW, const SolveSpec& sp, const double2* b
         o.ncompte = (int)(inner_mv[r] + outer_mv[r]);
         o.ncompte64 = (int)outer_mv[r];
         o.outer = (int)inner_runs[r];
+        // every step was followed by a copy, so the last one holds x
+        o.loc_on_host = early;
     }
 }
 

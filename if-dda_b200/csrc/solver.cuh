@@ -31,6 +31,14 @@ struct SolveSpec {
     const float2* const* gc32_r = nullptr;
     const long* alpha_off = nullptr;
     const long* tab_off = nullptr;
+    // mixed precision, optional: a page-locked host array (nrhs * n3, the
+    // layout of the solution) that receives the solution after every outer
+    // step, copied on early_stream while the solve checks the new residual;
+    // the copy after the last step is the result.  loc_ready / loc_copied
+    // order the copy after the step and the next step after the copy.
+    double2* early_loc = nullptr;
+    cudaStream_t early_stream = nullptr;
+    cudaEvent_t loc_ready = nullptr, loc_copied = nullptr;
 };
 
 // a solver's mat-vec arguments carry the ragged-batch tables of its spec
@@ -54,6 +62,7 @@ struct SolveResult {
     int ncompte = 0;    // mat-vecs
     int ncompte64 = 0;  // of which FP64
     int outer = 0;      // refinement steps (mixed)
+    bool loc_on_host = false;  // early_loc holds the returned solution
 };
 
 // Krylov iterations as one CUDA graph, reused while every pointer and size
