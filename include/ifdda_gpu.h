@@ -42,9 +42,12 @@ typedef struct {
 
 int ifdda_abi_version(void);
 
-/* Context: device ordinal, owns a CUDA stream.  No counterpart in the
-   reference (which has no device); cdmlib's FFTW plan set-up
-   (cdmlib/cdmlib.f:1150-1165) is the closest analogue. */
+/* Context: device ordinal, owns a CUDA stream for its work and a second
+   one on which ifdda_inverserig / ifdda_inverserig_batch move host data
+   while earlier work still runs (a call that returns host results has
+   finished with both).  No counterpart in the reference (which has no
+   device); cdmlib's FFTW plan set-up (cdmlib/cdmlib.f:1150-1165) is the
+   closest analogue. */
 int ifdda_ctx_create(int device, ifdda_ctx** out);
 /* Releases the context.  If spectra made on it are still alive, the release
    waits until the last of them is destroyed (they keep using its stream);
