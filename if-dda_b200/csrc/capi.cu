@@ -456,6 +456,10 @@ int ifdda_ctx_create(int device, ifdda_ctx** out) {
         IFDDA_CUDA(cudaMemset(c->tickets.p, 0, sizeof(unsigned)));
         c->partials.ensure(2048 * 8);  // reduction_blocks() partials of up to 8 sums
     } catch (const EngineError& e) {
+        for (cudaEvent_t ev : {c->upload_done, c->loc_ready, c->loc_copied})
+            if (ev) cudaEventDestroy(ev);
+        if (c->upload_stream) cudaStreamDestroy(c->upload_stream);
+        if (c->stream) cudaStreamDestroy(c->stream);
         delete c;
         return 1;
     }
