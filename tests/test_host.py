@@ -89,3 +89,15 @@ def test_replica_timing_max_over_two_gloo_ranks():
         assert p.exitcode == 0
     res = sorted(q.get(timeout=10) for _ in range(2))
     assert res == [(0, 2, 15.0), (1, 2, 15.0)]
+
+
+def test_product_path_fails_loudly_without_a_gpu():
+    """No CPU fallback: without a CUDA device the library's context creation
+    fails (and frees what it made) and the host API raises."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    import ifdda
+    for _ in range(3):
+        with pytest.raises(ifdda.IfddaError):
+            ifdda.Context(0)
